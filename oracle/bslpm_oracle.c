@@ -1,0 +1,781 @@
+/* CPU restatement of the reference's BVE backward semi-Lagrangian hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY: the checker for the CUDA path and the "port"
+ * CPU baseline.  The product library never links or calls this file.
+ *
+ * Every function cites the reference source (file:line, relative to the
+ * reference checkout) whose arithmetic it restates.  Expressions keep the
+ * reference's operand order and every accumulation keeps the reference's
+ * single-thread order (its atomics become owner-computes sums visited in the
+ * same order), so the results match the reference built by oracle/Makefile
+ * bit for bit when both use the same libm.  Parity is pinned by
+ * tests/test_oracle_golden.py against vectors that tests/golden/make_golden.py
+ * produced from the reference itself.
+ */
+#include "bslpm_oracle.h"
+
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define ORC_PI 3.14159265358979323846
+#define MAXQ 121
+
+static int g_orc_error = 0;
+int orc_error(void) { return g_orc_error; }
+void orc_clear_error(void) { g_orc_error = 0; }
+
+/* ---------------- geometry: src/cubed_sphere_transforms_impl.hpp ---------- */
+
+/* face_from_xyz: src/cubed_sphere_transforms_impl.hpp:8-32 */
+static int face_from_xyz(double x, double y, double z) {
+  double ax = fabs(x), ay = fabs(y), az = fabs(z);
+  if ((ax >= ay) && (ax >= az)) return x >= 0 ? 0 : 2;
+  if ((ay >= ax) && (ay >= az)) return y >= 0 ? 1 : 3;
+  return z >= 0 ? 4 : 5;
+}
+
+/* xyz_from_xieta: src/cubed_sphere_transforms_impl.hpp:34-65 */
+static void xyz_from_xieta(double xi, double eta, int face, double* xyz) {
+  double X = tan(xi), Y = tan(eta);
+  switch (face) {
+    case 0: xyz[0] = 1.0 / sqrt(1 + X * X + Y * Y); xyz[1] = X * xyz[0]; xyz[2] = Y * xyz[0]; break;
+    case 1: xyz[1] = 1.0 / sqrt(1 + X * X + Y * Y); xyz[0] = -X * xyz[1]; xyz[2] = Y * xyz[1]; break;
+    case 2: xyz[0] = -1.0 / sqrt(1 + X * X + Y * Y); xyz[1] = X * xyz[0]; xyz[2] = -Y * xyz[0]; break;
+    case 3: xyz[1] = -1.0 / sqrt(1 + X * X + Y * Y); xyz[0] = -X * xyz[1]; xyz[2] = -Y * xyz[1]; break;
+    case 4: xyz[2] = 1.0 / sqrt(1 + X * X + Y * Y); xyz[0] = -Y * xyz[2]; xyz[1] = X * xyz[2]; break;
+    case 5: xyz[2] = -1.0 / sqrt(1 + X * X + Y * Y); xyz[0] = -Y * xyz[2]; xyz[1] = -X * xyz[2]; break;
+    default: g_orc_error = 3; xyz[0] = xyz[1] = xyz[2] = 0; break;
+  }
+}
+
+/* xieta_from_xyz with a given face: src/cubed_sphere_transforms_impl.hpp:100-123 */
+static void xieta_from_xyz_face(double x, double y, double z, int face, double* xieta) {
+  switch (face) {
+    case 0: xieta[0] = atan(y / x); xieta[1] = atan(z / x); break;
+    case 1: xieta[0] = atan(-x / y); xieta[1] = atan(z / y); break;
+    case 2: xieta[0] = atan(y / x); xieta[1] = atan(-z / x); break;
+    case 3: xieta[0] = atan(-x / y); xieta[1] = atan(-z / y); break;
+    case 4: xieta[0] = atan(y / z); xieta[1] = atan(-x / z); break;
+    default: xieta[0] = atan(-y / z); xieta[1] = atan(-x / z); break;
+  }
+}
+
+/* xieta_from_xyz choosing the face itself: src/cubed_sphere_transforms_impl.hpp:67-98.
+ * Its branch structure picks the same face as face_from_xyz. */
+static void xieta_from_xyz(double x, double y, double z, double* xieta) {
+  xieta_from_xyz_face(x, y, z, face_from_xyz(x, y, z), xieta);
+}
+
+/* project_to_sphere: src/general_utils_impl.hpp:179-185 */
+static void project_to_sphere(double* x, double* y, double* z) {
+  double n = sqrt(*x * *x + *y * *y + *z * *z);
+  *x /= n;
+  *y /= n;
+  *z /= n;
+}
+
+/* gcdist, sphere_tri_area: src/general_utils.cpp:21-44 */
+static double gcdist(const double* p1, const double* p2) {
+  double dp = p1[0] * p2[0] + p1[1] * p2[1] + p1[2] * p2[2];
+  if (dp > 1.0) dp = 1.0;
+  if (dp < -1.0) dp = -1.0;
+  return acos(dp);
+}
+static double sphere_tri_area(const double* p1, const double* p2, const double* p3) {
+  double p1n[3], p2n[3], p3n[3], a, b, c, s, z;
+  memcpy(p1n, p1, sizeof p1n);
+  memcpy(p2n, p2, sizeof p2n);
+  memcpy(p3n, p3, sizeof p3n);
+  p2n[0] -= p3[0], p2n[1] -= p3[1], p2n[2] -= p3[2];
+  p3n[0] -= p1[0], p3n[1] -= p1[1], p3n[2] -= p1[2];
+  p1n[0] -= p2[0], p1n[1] -= p2[1], p1n[2] -= p2[2];
+  a = acos(1 - 0.5 * (p2n[0] * p2n[0] + p2n[1] * p2n[1] + p2n[2] * p2n[2]));
+  b = acos(1 - 0.5 * (p3n[0] * p3n[0] + p3n[1] * p3n[1] + p3n[2] * p3n[2]));
+  c = acos(1 - 0.5 * (p1n[0] * p1n[0] + p1n[1] * p1n[1] + p1n[2] * p1n[2]));
+  s = (a + b + c) / 2;
+  z = tan(s / 2) * tan((s - a) / 2) * tan((s - b) / 2) * tan((s - c) / 2);
+  return 4 * atan(sqrt(z));
+}
+
+/* ---------------- tree: src/initialize_cubed_sphere.cpp ------------------- */
+
+int orc_panel_count(int levels) { return 2 * ((1 << (2 * levels)) - 1); }
+int orc_leaf_count(int levels) { return 6 * (1 << (2 * (levels - 1))); }
+static int level_start(int level) { return 2 * ((1 << (2 * level)) - 1); }
+
+/* cubed_sphere_panels_init + refine_cube + cubed_sphere_init_2:
+ * src/initialize_cubed_sphere.cpp:64-234 */
+void orc_panels_init(int levels, orc_panel* p) {
+  int P = orc_panel_count(levels);
+  memset(p, 0, sizeof(orc_panel) * (size_t)P);
+  for (int i = 0; i < 6; i++) {
+    p[i].id = i;
+    p[i].face = i;
+    p[i].min_xi = -1;
+    p[i].max_xi = 1;
+    p[i].min_eta = -1;
+    p[i].max_eta = 1;
+    p[i].level = 0;
+    p[i].parent = -1;
+  }
+  for (int i = 0; i < 4; i++) {
+    p[i].top = 4;
+    p[i].bot = 5;
+  }
+  p[0].left = 3; p[0].right = 1;
+  p[1].left = 0; p[1].right = 2;
+  p[2].left = 1; p[2].right = 3;
+  p[3].left = 2; p[3].right = 0;
+  p[4].top = 2; p[4].left = 3; p[4].bot = 0; p[4].right = 1;
+  p[5].top = 0; p[5].left = 3; p[5].bot = 2; p[5].right = 1;
+
+  for (int level = 0; level < levels - 1; level++) {
+    int n = 6 * (1 << (2 * level));
+    int ls = level_start(level + 1), ps = level_start(level);
+    for (int i = 0; i < n; i++) {
+      int start = ls + 4 * i;
+      orc_panel* par = &p[ps + i];
+      for (int j = 0; j < 4; j++) {
+        p[start + j].id = start + j;
+        p[start + j].face = par->face;
+        p[start + j].parent = ps + i;
+        p[start + j].level = par->level + 1;
+      }
+      double max_xi = par->max_xi, min_xi = par->min_xi, max_eta = par->max_eta, min_eta = par->min_eta;
+      double mid_xi = 0.5 * (max_xi + min_xi), mid_eta = 0.5 * (max_eta + min_eta);
+      p[start].max_xi = max_xi; p[start].min_xi = mid_xi; p[start].max_eta = max_eta; p[start].min_eta = mid_eta;
+      p[start + 1].max_xi = mid_xi; p[start + 1].min_xi = min_xi; p[start + 1].max_eta = max_eta; p[start + 1].min_eta = mid_eta;
+      p[start + 2].max_xi = mid_xi; p[start + 2].min_xi = min_xi; p[start + 2].max_eta = mid_eta; p[start + 2].min_eta = min_eta;
+      p[start + 3].max_xi = max_xi; p[start + 3].min_xi = mid_xi; p[start + 3].max_eta = mid_eta; p[start + 3].min_eta = min_eta;
+      int pt = par->top - ps, pl = par->left - ps, pb = par->bot - ps, pr = par->right - ps;
+      p[start].top = ls + 4 * pt + 3; p[start].left = ls + 4 * i + 1; p[start].bot = ls + 4 * i + 3; p[start].right = ls + 4 * pr + 1;
+      p[start + 1].top = ls + 4 * pt + 2; p[start + 1].left = ls + 4 * pl; p[start + 1].bot = ls + 4 * i + 2; p[start + 1].right = ls + 4 * i;
+      p[start + 2].top = ls + 4 * i + 1; p[start + 2].left = ls + 4 * pl + 3; p[start + 2].bot = ls + 4 * pb + 1; p[start + 2].right = ls + 4 * i + 3;
+      p[start + 3].top = ls + 4 * i; p[start + 3].left = ls + 4 * i + 2; p[start + 3].bot = ls + 4 * pb; p[start + 3].right = ls + 4 * pr + 2;
+      for (int j = 0; j < 4; j++) par->child[j] = start + j;
+    }
+  }
+  for (int i = 0; i < P; i++) {
+    p[i].is_leaf = (p[i].level == levels - 1);
+    double max_xi = p[i].max_xi * ORC_PI / 4.0, min_xi = p[i].min_xi * ORC_PI / 4.0;
+    double max_eta = p[i].max_eta * ORC_PI / 4.0, min_eta = p[i].min_eta * ORC_PI / 4.0;
+    double mid_xi = 0.5 * (max_xi + min_xi), mid_eta = 0.5 * (max_eta + min_eta);
+    double p1[3], p2[3], p3[3], p4[3], pc[3];
+    xyz_from_xieta(max_xi, max_eta, p[i].face, p1);
+    xyz_from_xieta(max_xi, min_eta, p[i].face, p2);
+    xyz_from_xieta(min_xi, min_eta, p[i].face, p3);
+    xyz_from_xieta(min_xi, max_eta, p[i].face, p4);
+    xyz_from_xieta(mid_xi, mid_eta, p[i].face, pc);
+    double d1 = gcdist(p1, pc), d2 = gcdist(p2, pc), d3 = gcdist(p3, pc), d4 = gcdist(p4, pc);
+    p[i].radius = fmax(d1, fmax(d2, fmax(d3, d4)));
+    p[i].area = sphere_tri_area(p1, p2, p3) + sphere_tri_area(p1, p3, p4);
+  }
+}
+
+/* interp_init: src/interp_funcs.cpp:11-73.  With exact_cc the Clenshaw-Curtis
+ * weights are the exact ones (the reference's formula leaves the middle node
+ * weight at zero for odd degree and is not exact for even degree). */
+void orc_interp_init(int degree, int exact_cc, double* info) {
+  int d = degree, n = d + 1;
+  double cheb[11], bw[11], cc[11];
+  if (d == 0) {
+    cheb[0] = 0;
+    bw[0] = 1;
+  } else {
+    for (int i = 0; i < n; i++) {
+      cheb[i] = cos(ORC_PI / d * i);
+      if (fabs(cheb[i]) < 1e-16) cheb[i] = 0;
+      bw[i] = (i == 0) ? 0.5 : (i == d ? 0.5 * pow(-1, i) : pow(-1, i));
+    }
+  }
+  for (int i = 0; i < n; i++) cc[i] = 0;
+  if (!exact_cc) {
+    double vec[6];
+    for (int i = 0; i < d / 2 + 1; i++) vec[i] = 2;
+    vec[0] = 1;
+    for (int i = 1; i < d / 2 + 1; i++) vec[i] = 2.0 / (1 - 4 * i * i);
+    for (int i = 0; i < d / 2 + 1; i++) {
+      double sum = 0;
+      for (int j = 0; j < d / 2 + 1; j++) sum += 2 * cos(2 * i * j * ORC_PI / d) / d * vec[j];
+      cc[i] = sum;
+    }
+    cc[0] *= 0.5;
+    for (int i = 0; i < d / 2; i++) cc[d - i] = cc[i];
+  } else if (d == 0) {
+    cc[0] = 2;
+  } else {
+    /* w_i = (c_i/d) [1 - sum_{j=1}^{floor(d/2)} b_j cos(2 j theta_i) / (4 j^2 - 1)],
+     * c_i = 1 at the end nodes else 2, b_j = 1 for j = d/2 else 2. */
+    for (int i = 0; i < n; i++) {
+      double th = ORC_PI * i / d, s = 1.0;
+      for (int j = 1; j <= d / 2; j++) {
+        double b = (2 * j == d) ? 1.0 : 2.0;
+        s -= b * cos(2 * j * th) / (4.0 * j * j - 1);
+      }
+      cc[i] = ((i == 0 || i == d) ? 1.0 : 2.0) / d * s;
+    }
+  }
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < n; j++) {
+      int idx = i * n + j;
+      info[4 * idx + 0] = cheb[i];
+      info[4 * idx + 1] = cheb[j];
+      info[4 * idx + 2] = bw[i] * bw[j];
+      info[4 * idx + 3] = cc[i] * cc[j];
+    }
+}
+
+/* cube_sphere_spec_points / compute_point_panel: src/initialize_cubed_sphere.cpp:236-288 */
+void orc_spec_points(int levels, int degree, const orc_panel* p, const double* interp, double* x, double* y,
+                     double* z, double* area) {
+  int q = (degree + 1) * (degree + 1);
+  int off = level_start(levels - 1), P = orc_panel_count(levels);
+  for (int i = off; i < P; i++) {
+    double max_xi = ORC_PI / 4.0 * p[i].max_xi, min_xi = ORC_PI / 4.0 * p[i].min_xi;
+    double max_eta = ORC_PI / 4.0 * p[i].max_eta, min_eta = ORC_PI / 4.0 * p[i].min_eta;
+    double xi_range = 0.5 * (max_xi - min_xi), xi_offset = 0.5 * (max_xi + min_xi);
+    double eta_range = 0.5 * (max_eta - min_eta), eta_offset = 0.5 * (max_eta + min_eta);
+    for (int j = 0; j < q; j++) {
+      double xyz[3];
+      xyz_from_xieta(xi_offset + xi_range * interp[4 * j], eta_offset + eta_range * interp[4 * j + 1], p[i].face,
+                     xyz);
+      size_t o = (size_t)(i - off) * q + j;
+      x[o] = xyz[0];
+      y[o] = xyz[1];
+      z[o] = xyz[2];
+      area[o] = interp[4 * j + 3] * p[i].area / 4.0;
+    }
+  }
+}
+
+/* dual_tree_traversal: src/fmm_funcs.cpp:17-123 (FIFO queue of panel pairs). */
+long orc_dual_tree_traversal(int levels, const orc_panel* p, double theta, int* list, long cap) {
+  long qcap = 1 << 16, head = 0, tail = 0, count = 0;
+  int* qt = (int*)malloc(sizeof(int) * qcap);
+  int* qs = (int*)malloc(sizeof(int) * qcap);
+#define PUSH(t, s)                                                 \
+  do {                                                             \
+    if (tail == qcap) {                                            \
+      long live = tail - head;                                     \
+      memmove(qt, qt + head, sizeof(int) * live);                  \
+      memmove(qs, qs + head, sizeof(int) * live);                  \
+      head = 0;                                                    \
+      tail = live;                                                 \
+      if (tail + 8 > qcap) {                                       \
+        qcap *= 2;                                                 \
+        qt = (int*)realloc(qt, sizeof(int) * qcap);                \
+        qs = (int*)realloc(qs, sizeof(int) * qcap);                \
+      }                                                            \
+    }                                                              \
+    qt[tail] = (t);                                                \
+    qs[tail] = (s);                                                \
+    tail++;                                                        \
+  } while (0)
+#define EMIT(t, s, ty)              \
+  do {                              \
+    if (count < cap) {              \
+      list[3 * count] = (t);        \
+      list[3 * count + 1] = (s);    \
+      list[3 * count + 2] = (ty);   \
+    }                               \
+    count++;                        \
+  } while (0)
+  for (int i = 0; i < 6; i++)
+    for (int j = 0; j < 6; j++) PUSH(i, j);
+  while (tail > head) {
+    int t = qt[head], s = qs[head];
+    head++;
+    double xi1 = ORC_PI / 4.0 * 0.5 * (p[t].min_xi + p[t].max_xi);
+    double xi2 = ORC_PI / 4.0 * 0.5 * (p[s].min_xi + p[s].max_xi);
+    double eta1 = ORC_PI / 4.0 * 0.5 * (p[t].min_eta + p[t].max_eta);
+    double eta2 = ORC_PI / 4.0 * 0.5 * (p[s].min_eta + p[s].max_eta);
+    double c1[3], c2[3];
+    xyz_from_xieta(xi1, eta1, p[t].face, c1);
+    xyz_from_xieta(xi2, eta2, p[s].face, c2);
+    double dist = gcdist(c1, c2), sep = 100;
+    if (dist > 1e-16) sep = (p[t].radius + p[s].radius) / dist;
+    if (sep < theta) {
+      int ty = 0;
+      if (p[t].level < levels - 1) ty += 2;
+      if (p[s].level < levels - 1) ty += 1;
+      EMIT(t, s, ty);
+    } else if (p[t].is_leaf && p[s].is_leaf) {
+      EMIT(t, s, 0);
+    } else if (p[t].is_leaf) {
+      for (int c = 0; c < 4; c++) PUSH(t, p[s].child[c]);
+    } else if (p[s].is_leaf) {
+      for (int c = 0; c < 4; c++) PUSH(p[t].child[c], s);
+    } else if (p[t].level <= p[s].level) {
+      for (int c = 0; c < 4; c++) PUSH(p[t].child[c], s);
+    } else {
+      for (int c = 0; c < 4; c++) PUSH(t, p[s].child[c]);
+    }
+  }
+#undef PUSH
+#undef EMIT
+  free(qt);
+  free(qs);
+  return count;
+}
+
+/* ---------------- interpolation: src/interp_funcs_impl.hpp ---------------- */
+
+/* interp_vals_bli: src/interp_funcs_impl.hpp:11-112.  Out-of-panel input sets
+ * the oracle error flag (the reference aborts). */
+void orc_interp_vals_bli(double* basis, double xi, double eta, double min_xi, double max_xi, double min_eta,
+                         double max_eta, int d) {
+  double xi_range = 0.5 * (max_xi - min_xi), xi_offset = 0.5 * (max_xi + min_xi);
+  double eta_range = 0.5 * (max_eta - min_eta), eta_offset = 0.5 * (max_eta + min_eta);
+  double cheb_xi[11], cheb_eta[11], w[11], fx[11], fe[11], val;
+  if (xi < min_xi - 1e-15 || xi > max_xi + 1e-15 || eta < min_eta - 1e-15 || eta > max_eta + 1e-15) g_orc_error = 1;
+  for (int i = 0; i < (d + 1) * (d + 1); i++) basis[i] = 0.0;
+  if (d == 0) {
+    cheb_xi[0] = xi_offset;
+    cheb_eta[0] = eta_offset;
+    w[0] = 1;
+  } else {
+    for (int i = 0; i < d + 1; i++) {
+      cheb_xi[i] = cos(ORC_PI * i / d) * xi_range + xi_offset;
+      cheb_eta[i] = cos(ORC_PI * i / d) * eta_range + eta_offset;
+      w[i] = (i == 0) ? 0.5 : (i == d ? 0.5 * pow(-1, i) : pow(-1, i));
+    }
+  }
+  int found = 0;
+  for (int i = 0; i < d + 1; i++) {
+    if (fabs(xi - cheb_xi[i]) < 1e-15) {
+      found = 1;
+      for (int j = 0; j < d + 1; j++) fx[j] = 0;
+      fx[i] = 1;
+      break;
+    }
+  }
+  if (!found) {
+    double den = 0;
+    for (int i = 0; i < d + 1; i++) {
+      val = w[i] / (xi - cheb_xi[i]);
+      fx[i] = val;
+      den += val;
+    }
+    for (int i = 0; i < d + 1; i++) fx[i] /= den;
+  }
+  found = 0;
+  for (int i = 0; i < d + 1; i++) {
+    if (fabs(eta - cheb_eta[i]) < 1e-15) {
+      found = 1;
+      for (int j = 0; j < d + 1; j++) fe[j] = 0;
+      fe[i] = 1;
+      break;
+    }
+  }
+  if (!found) {
+    double den = 0;
+    for (int i = 0; i < d + 1; i++) {
+      val = w[i] / (eta - cheb_eta[i]);
+      fe[i] = val;
+      den += val;
+    }
+    for (int i = 0; i < d + 1; i++) fe[i] /= den;
+  }
+  for (int i = 0; i < d + 1; i++)
+    for (int j = 0; j < d + 1; j++) basis[i * (d + 1) + j] = fx[i] * fe[j];
+}
+
+/* point_locate_panel: src/interp_funcs_impl.hpp:114-142 */
+int orc_point_locate_panel(const orc_panel* p, double x, double y, double z) {
+  int cur = face_from_xyz(x, y, z);
+  double xe[2];
+  xieta_from_xyz_face(x, y, z, cur, xe);
+  double xi = xe[0], eta = xe[1];
+  while (!p[cur].is_leaf) {
+    double mid_xi = 0.5 * ORC_PI / 4.0 * (p[cur].max_xi + p[cur].min_xi);
+    double mid_eta = 0.5 * ORC_PI / 4.0 * (p[cur].max_eta + p[cur].min_eta);
+    if ((xi >= mid_xi) && (eta >= mid_eta)) cur = p[cur].child[0];
+    else if ((xi <= mid_xi) && (eta >= mid_eta)) cur = p[cur].child[1];
+    else if ((xi <= mid_xi) && (eta <= mid_eta)) cur = p[cur].child[2];
+    else if ((xi >= mid_xi) && (eta <= mid_eta)) cur = p[cur].child[3];
+    else {
+      g_orc_error = 2; /* NaN coordinates */
+      return cur;
+    }
+  }
+  return cur;
+}
+
+/* BLI of one point at the located leaf with bounds pi/4.0 * (panel bounds):
+ * the call pattern of src/bve_time_step.cpp:45-46, 143-144, 222-223. */
+static void bli_at_leaf(const orc_panel* p, int leaf, double xi, double eta, int d, double* basis) {
+  orc_interp_vals_bli(basis, xi, eta, ORC_PI / 4.0 * p[leaf].min_xi, ORC_PI / 4.0 * p[leaf].max_xi,
+                      ORC_PI / 4.0 * p[leaf].min_eta, ORC_PI / 4.0 * p[leaf].max_eta, d);
+}
+
+/* ---------------- FMM passes: src/fmm_funcs.cpp, src/fmm_funcs_impl.hpp --- */
+
+/* upward_pass + base_pots + child_to_parent: src/fmm_funcs.cpp:341-355,
+ * src/fmm_funcs_impl.hpp:17-71.  Parents accumulate children in ascending
+ * child index, then child point i, as the reference's sequential atomics do. */
+void orc_upward_pass(int levels, int degree, const orc_panel* p, const double* interp, const double* area,
+                     const double* pots, double* proxy) {
+  int q = (degree + 1) * (degree + 1), P = orc_panel_count(levels), A = orc_leaf_count(levels);
+  int off = P - A;
+  memset(proxy, 0, sizeof(double) * (size_t)P * q);
+  for (size_t i = 0; i < (size_t)A * q; i++) proxy[(size_t)off * q + i] = area[i] * pots[i];
+  for (int lev = levels - 1; lev >= 1; lev--) {
+    int plo = level_start(lev - 1), phi = level_start(lev);
+#pragma omp parallel for schedule(static)
+    for (int par = plo; par < phi; par++) {
+      double min_xi = p[par].min_xi * ORC_PI / 4.0, max_xi = p[par].max_xi * ORC_PI / 4.0;
+      double min_eta = p[par].min_eta * ORC_PI / 4.0, max_eta = p[par].max_eta * ORC_PI / 4.0;
+      double vals[MAXQ];
+      for (int c = 0; c < 4; c++) {
+        int k = p[par].child[c];
+        double xi_off = ORC_PI / 4.0 * 0.5 * (p[k].min_xi + p[k].max_xi);
+        double xi_scale = ORC_PI / 4.0 * 0.5 * (p[k].max_xi - p[k].min_xi);
+        double eta_off = ORC_PI / 4.0 * 0.5 * (p[k].min_eta + p[k].max_eta);
+        double eta_scale = ORC_PI / 4.0 * 0.5 * (p[k].max_eta - p[k].min_eta);
+        for (int i = 0; i < q; i++) {
+          double xi = interp[4 * i] * xi_scale + xi_off, eta = interp[4 * i + 1] * eta_scale + eta_off;
+          orc_interp_vals_bli(vals, xi, eta, min_xi, max_xi, min_eta, max_eta, degree);
+          for (int j = 0; j < q; j++) proxy[(size_t)par * q + j] += vals[j] * proxy[(size_t)k * q + i];
+        }
+      }
+    }
+  }
+}
+
+/* downward_pass_3 + parent_to_child_3 + child_panel_copy:
+ * src/fmm_funcs.cpp:374-392, src/fmm_funcs_impl.hpp:123-188 */
+void orc_downward_pass_3(int levels, int degree, const orc_panel* p, const double* interp, double* t1, double* t2,
+                         double* t3, double* s1, double* s2, double* s3) {
+  int q = (degree + 1) * (degree + 1), P = orc_panel_count(levels), A = orc_leaf_count(levels);
+  for (int lev = 0; lev < levels - 1; lev++) {
+    int plo = level_start(lev), phi = level_start(lev + 1);
+#pragma omp parallel for schedule(static)
+    for (int i = plo; i < phi; i++) {
+      double min_xi = p[i].min_xi * ORC_PI / 4.0, max_xi = p[i].max_xi * ORC_PI / 4.0;
+      double min_eta = p[i].min_eta * ORC_PI / 4.0, max_eta = p[i].max_eta * ORC_PI / 4.0;
+      double vals[MAXQ];
+      for (int c = 0; c < 4; c++) {
+        int ch = p[i].child[c];
+        double xi_off = ORC_PI / 4.0 * 0.5 * (p[ch].min_xi + p[ch].max_xi);
+        double xi_scale = ORC_PI / 4.0 * 0.5 * (p[ch].max_xi - p[ch].min_xi);
+        double eta_off = ORC_PI / 4.0 * 0.5 * (p[ch].min_eta + p[ch].max_eta);
+        double eta_scale = ORC_PI / 4.0 * 0.5 * (p[ch].max_eta - p[ch].min_eta);
+        for (int k = 0; k < q; k++) {
+          double xi = interp[4 * k] * xi_scale + xi_off, eta = interp[4 * k + 1] * eta_scale + eta_off;
+          orc_interp_vals_bli(vals, xi, eta, min_xi, max_xi, min_eta, max_eta, degree);
+          for (int l = 0; l < q; l++) {
+            t1[(size_t)ch * q + k] += vals[l] * t1[(size_t)i * q + l];
+            t2[(size_t)ch * q + k] += vals[l] * t2[(size_t)i * q + l];
+            t3[(size_t)ch * q + k] += vals[l] * t3[(size_t)i * q + l];
+          }
+        }
+      }
+    }
+  }
+  size_t off = (size_t)(P - A) * q;
+  for (size_t i = 0; i < (size_t)A * q; i++) {
+    s1[i] = t1[off + i];
+    s2[i] = t2[off + i];
+    s3[i] = t3[off + i];
+  }
+}
+
+/* Proxy point j of panel pn as the interaction kernel computes it:
+ * src/fmm_interactions/bve_vel_impl.hpp:90-108. */
+static void proxy_point(const orc_panel* p, int pn, const double* interp, int j, double* xyz) {
+  double xi_off = ORC_PI / 4 * 0.5 * (p[pn].max_xi + p[pn].min_xi);
+  double xi_scale = ORC_PI / 4 * 0.5 * (p[pn].max_xi - p[pn].min_xi);
+  double eta_off = ORC_PI / 4 * 0.5 * (p[pn].max_eta + p[pn].min_eta);
+  double eta_scale = ORC_PI / 4 * 0.5 * (p[pn].max_eta - p[pn].min_eta);
+  xyz_from_xieta(interp[4 * j] * xi_scale + xi_off, interp[4 * j + 1] * eta_scale + eta_off, p[pn].face, xyz);
+}
+
+/* One panel-pair block of bve_vel_panel_interaction:
+ * src/fmm_interactions/bve_vel_impl.hpp:85-122.  Sums for each target point
+ * run over source points k in order. */
+static void bve_pair_block(const orc_panel* p, const double* interp, int q, int t, int s, const double* dx,
+                           const double* dy, const double* dz, const double* src, double eps, double* t1,
+                           double* t2, double* t3) {
+  double xs[MAXQ], ys[MAXQ], zs[MAXQ];
+  for (int k = 0; k < q; k++) {
+    double xyz_s[3];
+    proxy_point(p, s, interp, k, xyz_s);
+    double x_s = xyz_s[0] + dx[(size_t)s * q + k], y_s = xyz_s[1] + dy[(size_t)s * q + k],
+           z_s = xyz_s[2] + dz[(size_t)s * q + k];
+    project_to_sphere(&x_s, &y_s, &z_s);
+    xs[k] = x_s;
+    ys[k] = y_s;
+    zs[k] = z_s;
+  }
+  for (int j = 0; j < q; j++) {
+    double xt[3];
+    proxy_point(p, t, interp, j, xt);
+    double a1 = t1[(size_t)t * q + j], a2 = t2[(size_t)t * q + j], a3 = t3[(size_t)t * q + j];
+    for (int k = 0; k < q; k++) {
+      double dp = xt[0] * xs[k] + xt[1] * ys[k] + xt[2] * zs[k];
+      double g = -0.07957747154594767 / (1.0 - dp + eps) * src[(size_t)s * q + k];
+      a1 += g * (xt[1] * zs[k] - xt[2] * ys[k]);
+      a2 += g * (xt[2] * xs[k] - xt[0] * zs[k]);
+      a3 += g * (xt[0] * ys[k] - xt[1] * xs[k]);
+    }
+    t1[(size_t)t * q + j] = a1;
+    t2[(size_t)t * q + j] = a2;
+    t3[(size_t)t * q + j] = a3;
+  }
+}
+
+/* bve_vel_interactions: src/fmm_interactions/bve_vel.cpp:9-37 with one rank.
+ * Entries are grouped by target panel (stable, so each target still sees its
+ * sources in list order) and target panels run in parallel. */
+void orc_bve_vel_interactions(int levels, int degree, const orc_panel* p, const double* interp, long n_list,
+                              const int* list, const double* disp_x, const double* disp_y, const double* disp_z,
+                              const double* source, double eps, double* t1, double* t2, double* t3) {
+  int q = (degree + 1) * (degree + 1), P = orc_panel_count(levels);
+  long* start = (long*)calloc((size_t)P + 1, sizeof(long));
+  long* order = (long*)malloc(sizeof(long) * (size_t)(n_list > 0 ? n_list : 1));
+  for (long i = 0; i < n_list; i++) start[list[3 * i] + 1]++;
+  for (int i = 0; i < P; i++) start[i + 1] += start[i];
+  long* fill = (long*)malloc(sizeof(long) * (size_t)P);
+  for (int i = 0; i < P; i++) fill[i] = start[i];
+  for (long i = 0; i < n_list; i++) order[fill[list[3 * i]]++] = i;
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int t = 0; t < P; t++)
+    for (long e = start[t]; e < start[t + 1]; e++)
+      bve_pair_block(p, interp, q, t, list[3 * order[e] + 1], disp_x, disp_y, disp_z, source, eps, t1, t2, t3);
+  free(start);
+  free(order);
+  free(fill);
+}
+
+void orc_bve_direct_velocity(int levels, int degree, const orc_panel* p, const double* interp, const double* disp_x,
+                             const double* disp_y, const double* disp_z, const double* source, double eps,
+                             double* t1, double* t2, double* t3) {
+  int q = (degree + 1) * (degree + 1), P = orc_panel_count(levels), A = orc_leaf_count(levels);
+  int off = P - A;
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int t = off; t < P; t++)
+    for (int s = off; s < P; s++) bve_pair_block(p, interp, q, t, s, disp_x, disp_y, disp_z, source, eps, t1, t2, t3);
+}
+
+/* ---------------- stepper: src/bve_time_step.cpp ------------------------- */
+
+/* BLI of a field at (x,y,z) in its located leaf: the locate + BLI + gather
+ * pattern of src/bve_time_step.cpp:220-237. */
+static int locate_and_basis(const orc_panel* p, int d, double x, double y, double z, double* basis) {
+  double xe[2];
+  xieta_from_xyz(x, y, z, xe);
+  int leaf = orc_point_locate_panel(p, x, y, z);
+  bli_at_leaf(p, leaf, xe[0], xe[1], d, basis);
+  return leaf;
+}
+
+/* bve_find_departure_points: src/bve_time_step.cpp:172-309.  v_k holds the
+ * x, y, z components as three consecutive A x q blocks. */
+void orc_bve_departure(int levels, int degree, const orc_panel* p, const double* x, const double* y,
+                       const double* z, const double* v0, const double* v1, const double* v2, const double* v3,
+                       double dt, double* dep_x, double* dep_y, double* dep_z) {
+  int q = (degree + 1) * (degree + 1), P = orc_panel_count(levels), A = orc_leaf_count(levels);
+  int off = P - A;
+  size_t n = (size_t)A * q;
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < A; i++) {
+    double b[MAXQ];
+    for (int j = 0; j < q; j++) {
+      size_t o = (size_t)i * q + j;
+      double k1x = v3[o], k1y = v3[n + o], k1z = v3[2 * n + o];
+      double xx = x[o] - 0.5 * dt * k1x, yy = y[o] - 0.5 * dt * k1y, zz = z[o] - 0.5 * dt * k1z;
+      project_to_sphere(&xx, &yy, &zz);
+      int leaf = locate_and_basis(p, degree, xx, yy, zz, b);
+      double k2x = 0, k2y = 0, k2z = 0;
+      for (int m = 0; m < q; m++) {
+        size_t g = (size_t)(leaf - off) * q + m;
+        k2x += v2[g] * b[m];
+        k2y += v2[n + g] * b[m];
+        k2z += v2[2 * n + g] * b[m];
+      }
+      xx = x[o] - 0.5 * dt * k2x, yy = y[o] - 0.5 * dt * k2y, zz = z[o] - 0.5 * dt * k2z;
+      project_to_sphere(&xx, &yy, &zz);
+      leaf = locate_and_basis(p, degree, xx, yy, zz, b);
+      double k3x = 0, k3y = 0, k3z = 0;
+      for (int m = 0; m < q; m++) {
+        size_t g = (size_t)(leaf - off) * q + m;
+        k3x += v1[g] * b[m];
+        k3y += v1[n + g] * b[m];
+        k3z += v1[2 * n + g] * b[m];
+      }
+      xx = x[o] - dt * k3x, yy = y[o] - dt * k3y, zz = z[o] - dt * k3z;
+      project_to_sphere(&xx, &yy, &zz);
+      leaf = locate_and_basis(p, degree, xx, yy, zz, b);
+      double k4x = 0, k4y = 0, k4z = 0;
+      for (int m = 0; m < q; m++) {
+        size_t g = (size_t)(leaf - off) * q + m;
+        k4x += v0[g] * b[m];
+        k4y += v0[n + g] * b[m];
+        k4z += v0[2 * n + g] * b[m];
+      }
+      xx = x[o] - 1.0 / 6.0 * dt * k1x, yy = y[o] - 1.0 / 6.0 * dt * k1y, zz = z[o] - 1.0 / 6.0 * dt * k1z;
+      project_to_sphere(&xx, &yy, &zz);
+      xx -= -1.0 / 3.0 * dt * k2x, yy -= -1.0 / 3.0 * dt * k2y, zz -= -1.0 / 3.0 * dt * k2z;
+      project_to_sphere(&xx, &yy, &zz);
+      xx -= -1.0 / 3.0 * dt * k3x, yy -= -1.0 / 3.0 * dt * k3y, zz -= -1.0 / 3.0 * dt * k3z;
+      project_to_sphere(&xx, &yy, &zz);
+      xx -= -1.0 / 6.0 * dt * k4x, yy -= -1.0 / 6.0 * dt * k4y, zz -= -1.0 / 6.0 * dt * k4z;
+      project_to_sphere(&xx, &yy, &zz);
+      dep_x[o] = xx;
+      dep_y[o] = yy;
+      dep_z[o] = zz;
+    }
+  }
+}
+
+/* bve_departure_to_target: src/bve_time_step.cpp:15-67 */
+void orc_bve_remap(int levels, int degree, const orc_panel* p, const double* z, const double* dep_x,
+                   const double* dep_y, const double* dep_z, const double* vors, int T, const double* tracers,
+                   double omega, double* new_vors, double* new_tracers) {
+  int q = (degree + 1) * (degree + 1), P = orc_panel_count(levels), A = orc_leaf_count(levels);
+  int off = P - A;
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < A; i++) {
+    double b[MAXQ];
+    for (int j = 0; j < q; j++) {
+      size_t o = (size_t)i * q + j;
+      int leaf = locate_and_basis(p, degree, dep_x[o], dep_y[o], dep_z[o], b);
+      for (int k = 0; k < T; k++) new_tracers[o * T + k] = 0;
+      double vor = 0;
+      for (int m = 0; m < q; m++) {
+        size_t g = (size_t)(leaf - off) * q + m;
+        vor += vors[g] * b[m];
+        for (int k = 0; k < T; k++) new_tracers[o * T + k] += tracers[g * T + k] * b[m];
+      }
+      vor += 2 * omega * dep_z[o];
+      new_vors[o] = vor - 2 * omega * z[o];
+    }
+  }
+}
+
+/* bve_disp_update: src/bve_time_step.cpp:69-105 (leaves; disp rows offset). */
+static void disp_update(int A, int q, int off, const double* x, const double* y, const double* z, const double* vel,
+                        const double* vor, double* new_vor, double* dx, double* dy, double* dz, double dt,
+                        double omega) {
+  size_t n = (size_t)A * q;
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < A; i++)
+    for (int j = 0; j < q; j++) {
+      size_t o = (size_t)i * q + j;
+      double xx = x[o] + vel[o] * dt, yy = y[o] + vel[n + o] * dt, zz = z[o] + vel[2 * n + o] * dt;
+      project_to_sphere(&xx, &yy, &zz);
+      new_vor[o] = vor[o] + 2 * omega * z[o] - 2 * omega * zz;
+      size_t d = (size_t)(i + off) * q + j;
+      dx[d] = dt * vel[o];
+      dy[d] = dt * vel[n + o];
+      dz[d] = dt * vel[2 * n + o];
+    }
+}
+
+/* bve_disp_interp: src/bve_time_step.cpp:107-160 (non-leaf panels). */
+static void disp_interp(const orc_panel* p, int off, int d, const double* interp, double* dx, double* dy,
+                        double* dz) {
+  int q = (d + 1) * (d + 1);
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < off; i++) {
+    double xi_off = ORC_PI / 4 * 0.5 * (p[i].max_xi + p[i].min_xi);
+    double xi_scale = ORC_PI / 4 * 0.5 * (p[i].max_xi - p[i].min_xi);
+    double eta_off = ORC_PI / 4 * 0.5 * (p[i].max_eta + p[i].min_eta);
+    double eta_scale = ORC_PI / 4 * 0.5 * (p[i].max_eta - p[i].min_eta);
+    double b[MAXQ], xyz[3];
+    for (int j = 0; j < q; j++) {
+      double xi = interp[4 * j] * xi_scale + xi_off, eta = interp[4 * j + 1] * eta_scale + eta_off;
+      xyz_from_xieta(xi, eta, p[i].face, xyz);
+      int leaf = orc_point_locate_panel(p, xyz[0], xyz[1], xyz[2]);
+      bli_at_leaf(p, leaf, xi, eta, d, b);
+      double ax = 0, ay = 0, az = 0;
+      for (int m = 0; m < q; m++) {
+        ax += dx[(size_t)leaf * q + m] * b[m];
+        ay += dy[(size_t)leaf * q + m] * b[m];
+        az += dz[(size_t)leaf * q + m] * b[m];
+      }
+      dx[(size_t)i * q + j] = ax;
+      dy[(size_t)i * q + j] = ay;
+      dz[(size_t)i * q + j] = az;
+    }
+  }
+}
+
+/* One velocity evaluation (one RK4 stage): up pass, interactions, down pass.
+ * src/bve_time_step.cpp:321-348 and the repeated stage blocks after it. */
+static void velocity_eval(const orc_bve_problem* pb, const double* eff_vor, const double* dx, const double* dy,
+                          const double* dz, double* proxy, double* t1, double* t2, double* t3, double* vel) {
+  int q = (pb->degree + 1) * (pb->degree + 1), P = orc_panel_count(pb->levels), A = orc_leaf_count(pb->levels);
+  size_t n = (size_t)A * q, pq = (size_t)P * q;
+  orc_upward_pass(pb->levels, pb->degree, pb->panels, pb->interp, pb->area, eff_vor, proxy);
+  memset(t1, 0, sizeof(double) * pq);
+  memset(t2, 0, sizeof(double) * pq);
+  memset(t3, 0, sizeof(double) * pq);
+  if (pb->mode == 1)
+    orc_bve_direct_velocity(pb->levels, pb->degree, pb->panels, pb->interp, dx, dy, dz, proxy, pb->kernel_eps, t1,
+                            t2, t3);
+  else
+    orc_bve_vel_interactions(pb->levels, pb->degree, pb->panels, pb->interp, pb->n_list, pb->list, dx, dy, dz,
+                             proxy, pb->kernel_eps, t1, t2, t3);
+  orc_downward_pass_3(pb->levels, pb->degree, pb->panels, pb->interp, t1, t2, t3, vel, vel + n, vel + 2 * n);
+}
+
+/* bve_back_rk4_step: src/bve_time_step.cpp:311-419 (forcing off, so the
+ * effective vorticity is the (displaced) relative vorticity:
+ * src/forcing_funcs.cpp:82-96). */
+void orc_bve_step(const orc_bve_problem* pb, double* vors, double* vel_x, double* vel_y, double* vel_z,
+                  double* tracers) {
+  int d = pb->degree, q = (d + 1) * (d + 1), P = orc_panel_count(pb->levels), A = orc_leaf_count(pb->levels);
+  int off = P - A, T = pb->tracer_count;
+  size_t n = (size_t)A * q, pq = (size_t)P * q;
+  double* dx = (double*)calloc(pq, sizeof(double));
+  double* dy = (double*)calloc(pq, sizeof(double));
+  double* dz = (double*)calloc(pq, sizeof(double));
+  double* proxy = (double*)calloc(pq, sizeof(double));
+  double* t1 = (double*)calloc(pq, sizeof(double));
+  double* t2 = (double*)calloc(pq, sizeof(double));
+  double* t3 = (double*)calloc(pq, sizeof(double));
+  double* v[4];
+  for (int k = 0; k < 4; k++) v[k] = (double*)calloc(3 * n, sizeof(double));
+  double* dvor = (double*)calloc(n, sizeof(double));
+  double* dep = (double*)calloc(3 * n, sizeof(double));
+  double* nv = (double*)calloc(n, sizeof(double));
+  double* ntr = (double*)calloc(n * (T > 0 ? T : 1), sizeof(double));
+
+  velocity_eval(pb, vors, dx, dy, dz, proxy, t1, t2, t3, v[0]);
+  const double fr[3] = {0.5, 0.5, 1.0};
+  for (int s = 1; s < 4; s++) {
+    disp_update(A, q, off, pb->x, pb->y, pb->z, v[s - 1], vors, dvor, dx, dy, dz, fr[s - 1] * pb->dt, pb->omega);
+    disp_interp(pb->panels, off, d, pb->interp, dx, dy, dz);
+    velocity_eval(pb, dvor, dx, dy, dz, proxy, t1, t2, t3, v[s]);
+  }
+  orc_bve_departure(pb->levels, d, pb->panels, pb->x, pb->y, pb->z, v[0], v[1], v[2], v[3], pb->dt, dep, dep + n,
+                    dep + 2 * n);
+  orc_bve_remap(pb->levels, d, pb->panels, pb->z, dep, dep + n, dep + 2 * n, vors, T, tracers, pb->omega, nv, ntr);
+  memcpy(vors, nv, sizeof(double) * n);
+  if (T > 0) memcpy(tracers, ntr, sizeof(double) * n * T);
+  memcpy(vel_x, v[0], sizeof(double) * n);
+  memcpy(vel_y, v[0] + n, sizeof(double) * n);
+  memcpy(vel_z, v[0] + 2 * n, sizeof(double) * n);
+  free(dx); free(dy); free(dz); free(proxy); free(t1); free(t2); free(t3);
+  for (int k = 0; k < 4; k++) free(v[k]);
+  free(dvor); free(dep); free(nv); free(ntr);
+}
+
+/* inv_lap: src/direct_sum_impl.hpp:20-27 (row i sums over j in order). */
+void orc_direct_sum_inv_lap(int n, const double* x, const double* y, const double* z, const double* area,
+                            const double* pots, double* soln) {
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < n; i++) {
+    double acc = soln[i];
+    for (int j = 0; j < n; j++) {
+      if (i != j) {
+        double dp = x[i] * x[j] + y[i] * y[j] + z[i] * z[j];
+        acc += -0.07957747154594767 * log(1 - dp) * area[j] * pots[j];
+      }
+    }
+    soln[i] = acc;
+  }
+}

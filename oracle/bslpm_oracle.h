@@ -1,0 +1,84 @@
+/* CPU restatement of the reference's BVE hot path (test infrastructure only).
+ *
+ * Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may load
+ * this library, and only as the checker or the timed CPU baseline; the product
+ * library never calls it.  Function-by-function citations of the reference are
+ * in bslpm_oracle.c.  The arithmetic and the accumulation order follow the
+ * reference, so with one thread the results agree bit for bit with the
+ * reference compiled by oracle/Makefile (checked by tests/test_oracle_golden.py).
+ */
+#ifndef SBSLPM_BSLPM_ORACLE_H
+#define SBSLPM_BSLPM_ORACLE_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Same fields as the reference's CubedSpherePanel
+ * (src/initialize_cubed_sphere.hpp:8-29); bounds are in [-1, 1], times pi/4
+ * on the sphere. */
+typedef struct {
+  int id, top, left, bot, right, face, level, parent;
+  int child[4];
+  int is_leaf;
+  double min_xi, max_xi, min_eta, max_eta, radius, area;
+} orc_panel;
+
+int orc_panel_count(int levels);
+int orc_leaf_count(int levels);
+void orc_panels_init(int levels, orc_panel* panels);
+/* interp: q x 4 = (xi node, eta node, BLI weight, CC weight).  exact_cc=0
+ * reproduces the reference's weights; exact_cc=1 gives exact
+ * Clenshaw-Curtis weights (the two agree only at the nodes' positions). */
+void orc_interp_init(int degree, int exact_cc, double* interp);
+void orc_spec_points(int levels, int degree, const orc_panel* panels, const double* interp, double* x,
+                     double* y, double* z, double* area);
+/* Returns the interaction count; writes at most cap triples. */
+long orc_dual_tree_traversal(int levels, const orc_panel* panels, double theta, int* list, long cap);
+
+void orc_interp_vals_bli(double* basis, double xi, double eta, double min_xi, double max_xi, double min_eta,
+                         double max_eta, int degree);
+int orc_point_locate_panel(const orc_panel* panels, double x, double y, double z);
+
+void orc_upward_pass(int levels, int degree, const orc_panel* panels, const double* interp, const double* area,
+                     const double* pots, double* proxy);
+void orc_downward_pass_3(int levels, int degree, const orc_panel* panels, const double* interp, double* t1,
+                         double* t2, double* t3, double* s1, double* s2, double* s3);
+void orc_bve_vel_interactions(int levels, int degree, const orc_panel* panels, const double* interp, long n_list,
+                              const int* list, const double* disp_x, const double* disp_y, const double* disp_z,
+                              const double* source, double kernel_eps, double* t1, double* t2, double* t3);
+/* Direct (all leaf x all leaf) velocity: the reference FMM in the theta -> 0
+ * limit, where every interaction is leaf-leaf.  Targets are undisplaced leaf
+ * proxies, sources are displaced leaf proxies. */
+void orc_bve_direct_velocity(int levels, int degree, const orc_panel* panels, const double* interp,
+                             const double* disp_x, const double* disp_y, const double* disp_z,
+                             const double* source, double kernel_eps, double* t1, double* t2, double* t3);
+void orc_bve_departure(int levels, int degree, const orc_panel* panels, const double* x, const double* y,
+                       const double* z, const double* v0, const double* v1, const double* v2, const double* v3,
+                       double dt, double* dep_x, double* dep_y, double* dep_z);
+void orc_bve_remap(int levels, int degree, const orc_panel* panels, const double* z, const double* dep_x,
+                   const double* dep_y, const double* dep_z, const double* vors, int tracer_count,
+                   const double* tracers, double omega, double* new_vors, double* new_tracers);
+
+/* One bve_back_rk4_step.  mode 0 = interaction list (FMM), 1 = direct.
+ * vors (A x q), vel_* (A x q, out = stage-0 velocity), tracers (A x q x T)
+ * are in-out. */
+typedef struct {
+  int levels, degree, tracer_count, mode;
+  double kernel_eps, omega, dt;
+  const orc_panel* panels;
+  const double* interp;
+  const double *x, *y, *z, *area;
+  long n_list;
+  const int* list;
+} orc_bve_problem;
+void orc_bve_step(const orc_bve_problem* pb, double* vors, double* vel_x, double* vel_y, double* vel_z,
+                  double* tracers);
+
+/* direct_sum_inv_lap (src/direct_sum_impl.hpp:20-27) over n points. */
+void orc_direct_sum_inv_lap(int n, const double* x, const double* y, const double* z, const double* area,
+                            const double* pots, double* soln);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,290 @@
+"""ctypes access to the two oracle libraries (test infrastructure only).
+
+* ``Port``: oracle/liboracle_port.so, the plain-C restatement of the
+  reference's BVE hot path (oracle/bslpm_oracle.c).  Builds from this
+  repository alone, so it is the checker on machines without the reference.
+* ``Ref``: oracle/_ref/libsbslpm_ref.so, the reference's own src/*.cpp built
+  against the shim headers by oracle/Makefile (present where it was built).
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg use
+this module, as the checker or as the timed CPU baseline.  The product
+package never imports it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PORT_PATH = os.path.join(HERE, "liboracle_port.so")
+REF_PATH = os.path.join(HERE, "_ref", "libsbslpm_ref.so")
+
+_D = ctypes.POINTER(ctypes.c_double)
+_I = ctypes.POINTER(ctypes.c_int)
+
+
+def _dp(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_D)
+
+
+def _ip(a: np.ndarray):
+    assert a.dtype == np.int32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_I)
+
+
+class OrcPanel(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int) for n in ("id", "top", "left", "bot", "right", "face", "level", "parent")] + [
+        ("child", ctypes.c_int * 4),
+        ("is_leaf", ctypes.c_int),
+    ] + [(n, ctypes.c_double) for n in ("min_xi", "max_xi", "min_eta", "max_eta", "radius", "area")]
+
+
+class OrcProblem(ctypes.Structure):
+    _fields_ = [
+        ("levels", ctypes.c_int),
+        ("degree", ctypes.c_int),
+        ("tracer_count", ctypes.c_int),
+        ("mode", ctypes.c_int),
+        ("kernel_eps", ctypes.c_double),
+        ("omega", ctypes.c_double),
+        ("dt", ctypes.c_double),
+        ("panels", ctypes.POINTER(OrcPanel)),
+        ("interp", _D),
+        ("x", _D),
+        ("y", _D),
+        ("z", _D),
+        ("area", _D),
+        ("n_list", ctypes.c_long),
+        ("list", _I),
+    ]
+
+
+def panels_to_arrays(panels) -> tuple[np.ndarray, np.ndarray]:
+    """(ints P x 13, dbls P x 6) in the column order of ref_get_panels."""
+    P = len(panels)
+    ints = np.zeros((P, 13), np.int32)
+    dbls = np.zeros((P, 6), np.float64)
+    for i, p in enumerate(panels):
+        ints[i] = [p.id, p.top, p.left, p.bot, p.right, p.face, p.level, p.parent, *p.child, p.is_leaf]
+        dbls[i] = [p.min_xi, p.max_xi, p.min_eta, p.max_eta, p.radius, p.area]
+    return ints, dbls
+
+
+class Port:
+    """The C restatement.  All arrays are float64 C-contiguous numpy arrays."""
+
+    def __init__(self, path: str = PORT_PATH):
+        self.lib = ctypes.CDLL(path)
+        L = self.lib
+        L.orc_dual_tree_traversal.restype = ctypes.c_long
+        L.orc_dual_tree_traversal.argtypes = [ctypes.c_int, ctypes.POINTER(OrcPanel), ctypes.c_double, _I, ctypes.c_long]
+        L.orc_point_locate_panel.restype = ctypes.c_int
+        L.orc_point_locate_panel.argtypes = [ctypes.POINTER(OrcPanel), ctypes.c_double, ctypes.c_double, ctypes.c_double]
+        L.orc_interp_vals_bli.argtypes = [_D] + [ctypes.c_double] * 6 + [ctypes.c_int]
+        L.orc_bve_step.argtypes = [ctypes.POINTER(OrcProblem), _D, _D, _D, _D, _D]
+
+    # ---- setup -------------------------------------------------------------
+    def build(self, levels: int, degree: int, theta: float | None, exact_cc: bool = False):
+        """Panels, interp table, points, areas and (if theta) interaction list."""
+        P = 2 * (4**levels - 1)
+        A = 6 * 4 ** (levels - 1)
+        q = (degree + 1) ** 2
+        panels = (OrcPanel * P)()
+        self.lib.orc_panels_init(levels, panels)
+        interp = np.zeros((q, 4))
+        self.lib.orc_interp_init(degree, int(exact_cc), _dp(interp))
+        x, y, z, area = (np.zeros((A, q)) for _ in range(4))
+        self.lib.orc_spec_points(levels, degree, panels, _dp(interp), _dp(x), _dp(y), _dp(z), _dp(area))
+        lst = np.zeros((0, 3), np.int32)
+        if theta is not None:
+            n = self.lib.orc_dual_tree_traversal(levels, panels, theta, None, 0)
+            lst = np.zeros((n, 3), np.int32)
+            self.lib.orc_dual_tree_traversal(levels, panels, theta, _ip(lst), n)
+        return dict(levels=levels, degree=degree, panels=panels, interp=interp, x=x, y=y, z=z, area=area, list=lst)
+
+    def bli(self, xi, eta, mnx, mxx, mne, mxe, degree):
+        out = np.zeros((degree + 1) ** 2)
+        self.lib.orc_interp_vals_bli(_dp(out), xi, eta, mnx, mxx, mne, mxe, degree)
+        return out
+
+    def locate(self, g, x, y, z) -> int:
+        return self.lib.orc_point_locate_panel(g["panels"], x, y, z)
+
+    # ---- passes ------------------------------------------------------------
+    def upward_pass(self, g, pots):
+        P = len(g["panels"])
+        out = np.zeros((P, g["interp"].shape[0]))
+        self.lib.orc_upward_pass(g["levels"], g["degree"], g["panels"], _dp(g["interp"]), _dp(g["area"]),
+                                 _dp(np.ascontiguousarray(pots)), _dp(out))
+        return out
+
+    def downward_pass_3(self, g, t1, t2, t3):
+        t1, t2, t3 = (np.array(t, dtype=np.float64, order="C") for t in (t1, t2, t3))
+        A, q = g["x"].shape
+        s = [np.zeros((A, q)) for _ in range(3)]
+        self.lib.orc_downward_pass_3(g["levels"], g["degree"], g["panels"], _dp(g["interp"]), _dp(t1), _dp(t2),
+                                     _dp(t3), _dp(s[0]), _dp(s[1]), _dp(s[2]))
+        return s
+
+    def vel_interactions(self, g, dx, dy, dz, src, eps):
+        P, q = src.shape
+        t = [np.zeros((P, q)) for _ in range(3)]
+        lst = np.ascontiguousarray(g["list"], dtype=np.int32)
+        self.lib.orc_bve_vel_interactions(g["levels"], g["degree"], g["panels"], _dp(g["interp"]),
+                                          ctypes.c_long(len(lst)), _ip(lst), _dp(dx), _dp(dy), _dp(dz), _dp(src),
+                                          ctypes.c_double(eps), _dp(t[0]), _dp(t[1]), _dp(t[2]))
+        return t
+
+    def direct_velocity(self, g, dx, dy, dz, src, eps):
+        P, q = src.shape
+        t = [np.zeros((P, q)) for _ in range(3)]
+        self.lib.orc_bve_direct_velocity(g["levels"], g["degree"], g["panels"], _dp(g["interp"]), _dp(dx), _dp(dy),
+                                         _dp(dz), _dp(src), ctypes.c_double(eps), _dp(t[0]), _dp(t[1]), _dp(t[2]))
+        return t
+
+    def departure(self, g, v0, v1, v2, v3, dt):
+        A, q = g["x"].shape
+        dep = [np.zeros((A, q)) for _ in range(3)]
+        vs = [np.ascontiguousarray(v, dtype=np.float64) for v in (v0, v1, v2, v3)]
+        self.lib.orc_bve_departure(g["levels"], g["degree"], g["panels"], _dp(g["x"]), _dp(g["y"]), _dp(g["z"]),
+                                   *[_dp(v) for v in vs], ctypes.c_double(dt), *[_dp(d) for d in dep])
+        return dep
+
+    def remap(self, g, dep, vors, tracers, omega):
+        A, q = g["x"].shape
+        T = 0 if tracers is None else tracers.shape[2]
+        tr = np.zeros(1) if tracers is None else np.ascontiguousarray(tracers)
+        nv = np.zeros((A, q))
+        ntr = np.zeros((A, q, max(T, 1)))
+        self.lib.orc_bve_remap(g["levels"], g["degree"], g["panels"], _dp(g["z"]), *[_dp(d) for d in dep],
+                               _dp(np.ascontiguousarray(vors)), T, _dp(tr), ctypes.c_double(omega), _dp(nv), _dp(ntr))
+        return nv, (ntr if T else None)
+
+    def bve_step(self, g, vors, tracers=None, *, dt, omega, eps, mode=0, nsteps=1):
+        """nsteps of bve_back_rk4_step; returns (vors, (vx, vy, vz), tracers)."""
+        A, q = g["x"].shape
+        T = 0 if tracers is None else tracers.shape[2]
+        lst = np.ascontiguousarray(g["list"], dtype=np.int32)
+        pb = OrcProblem(g["levels"], g["degree"], T, mode, eps, omega, dt, g["panels"], _dp(g["interp"]), _dp(g["x"]),
+                        _dp(g["y"]), _dp(g["z"]), _dp(g["area"]), len(lst), _ip(lst) if len(lst) else None)
+        v = np.array(vors, dtype=np.float64, order="C")
+        tr = np.zeros(1) if tracers is None else np.array(tracers, dtype=np.float64, order="C")
+        vx, vy, vz = (np.zeros((A, q)) for _ in range(3))
+        for _ in range(nsteps):
+            self.lib.orc_bve_step(ctypes.byref(pb), _dp(v), _dp(vx), _dp(vy), _dp(vz), _dp(tr))
+        return v, (vx, vy, vz), (tr if T else None)
+
+    def direct_sum_inv_lap(self, x, y, z, area, pots):
+        n = len(x)
+        out = np.zeros(n)
+        self.lib.orc_direct_sum_inv_lap(n, _dp(x), _dp(y), _dp(z), _dp(area), _dp(pots), _dp(out))
+        return out
+
+
+class Ref:
+    """The reference's own code (oracle/_ref/libsbslpm_ref.so)."""
+
+    def __init__(self, path: str = REF_PATH):
+        self.lib = ctypes.CDLL(path)
+        L = self.lib
+        L.ref_create.restype = ctypes.c_void_p
+        L.ref_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                 ctypes.c_int, ctypes.c_int]
+        for name in ("ref_destroy", "ref_sizes", "ref_get_panels", "ref_get_interactions", "ref_get_points",
+                     "ref_bve_initialize", "ref_bve_step", "ref_bve_vel_interactions", "ref_upward_pass",
+                     "ref_downward_pass_3", "ref_bve_departure", "ref_bve_remap"):
+            getattr(L, name).restype = None
+        L.ref_bve_step.argtypes = [ctypes.c_void_p, _D, _D, _D, _D, _D, ctypes.c_double, ctypes.c_int]
+        L.ref_bve_departure.argtypes = [ctypes.c_void_p, _D, _D, _D, _D, ctypes.c_double, _D, _D, _D]
+        L.ref_point_locate_panel.restype = ctypes.c_int
+        L.ref_point_locate_panel.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+        L.ref_interp_vals_bli.argtypes = [_D] + [ctypes.c_double] * 6 + [ctypes.c_int]
+        L.ref_num_threads.restype = ctypes.c_int
+
+    def create(self, levels, degree, theta, eps, omega, delta_t, tracer_count):
+        h = ctypes.c_void_p(self.lib.ref_create(levels, degree, theta, eps, omega, delta_t, tracer_count))
+        sz = np.zeros(5, np.int32)
+        self.lib.ref_sizes(h, _ip(sz))
+        P, A, q, I, _ = (int(v) for v in sz)
+        return dict(h=h, P=P, A=A, q=q, I=I, T=tracer_count, levels=levels, degree=degree)
+
+    def destroy(self, c):
+        self.lib.ref_destroy(c["h"])
+
+    def panels(self, c):
+        ints = np.zeros((c["P"], 13), np.int32)
+        dbls = np.zeros((c["P"], 6))
+        self.lib.ref_get_panels(c["h"], _ip(ints), _dp(dbls))
+        return ints, dbls
+
+    def interactions(self, c):
+        out = np.zeros((c["I"], 3), np.int32)
+        self.lib.ref_get_interactions(c["h"], _ip(out))
+        return out
+
+    def points(self, c):
+        A, q = c["A"], c["q"]
+        x, y, z, area = (np.zeros((A, q)) for _ in range(4))
+        interp = np.zeros((q, 4))
+        self.lib.ref_get_points(c["h"], _dp(x), _dp(y), _dp(z), _dp(area), _dp(interp))
+        return x, y, z, area, interp
+
+    def initialize(self, c, ic: str, balance: bool):
+        v = np.zeros((c["A"], c["q"]))
+        self.lib.ref_bve_initialize(c["h"], ic.encode(), int(balance), _dp(v))
+        return v
+
+    def bve_step(self, c, vors, tracers=None, time=0.0, nsteps=1):
+        A, q, T = c["A"], c["q"], c["T"]
+        v = np.array(vors, dtype=np.float64, order="C")
+        tr = np.zeros((A, q, max(T, 1))) if tracers is None else np.array(tracers, dtype=np.float64, order="C")
+        vx, vy, vz = (np.zeros((A, q)) for _ in range(3))
+        self.lib.ref_bve_step(c["h"], _dp(v), _dp(vx), _dp(vy), _dp(vz), _dp(tr), time, nsteps)
+        return v, (vx, vy, vz), (tr if T else None)
+
+    def vel_interactions(self, c, dx, dy, dz, src):
+        t = [np.zeros((c["P"], c["q"])) for _ in range(3)]
+        self.lib.ref_bve_vel_interactions(c["h"], _dp(dx), _dp(dy), _dp(dz), _dp(src), _dp(t[0]), _dp(t[1]), _dp(t[2]))
+        return t
+
+    def upward_pass(self, c, pots):
+        out = np.zeros((c["P"], c["q"]))
+        self.lib.ref_upward_pass(c["h"], _dp(np.ascontiguousarray(pots)), _dp(out))
+        return out
+
+    def downward_pass_3(self, c, t1, t2, t3):
+        t1, t2, t3 = (np.array(t, dtype=np.float64, order="C") for t in (t1, t2, t3))
+        s = [np.zeros((c["A"], c["q"])) for _ in range(3)]
+        self.lib.ref_downward_pass_3(c["h"], _dp(t1), _dp(t2), _dp(t3), _dp(s[0]), _dp(s[1]), _dp(s[2]))
+        return s
+
+    def departure(self, c, v0, v1, v2, v3, dt):
+        dep = [np.zeros((c["A"], c["q"])) for _ in range(3)]
+        vs = [np.ascontiguousarray(v, dtype=np.float64) for v in (v0, v1, v2, v3)]
+        self.lib.ref_bve_departure(c["h"], *[_dp(v) for v in vs], dt, *[_dp(d) for d in dep])
+        return dep
+
+    def remap(self, c, dep, vors, tracers):
+        A, q, T = c["A"], c["q"], c["T"]
+        tr = np.zeros((A, q, max(T, 1))) if tracers is None else np.ascontiguousarray(tracers)
+        nv = np.zeros((A, q))
+        ntr = np.zeros((A, q, max(T, 1)))
+        self.lib.ref_bve_remap(c["h"], *[_dp(d) for d in dep], _dp(np.ascontiguousarray(vors)), _dp(tr), _dp(nv), _dp(ntr))
+        return nv, (ntr if T else None)
+
+    def bli(self, xi, eta, mnx, mxx, mne, mxe, degree):
+        out = np.zeros((degree + 1) ** 2)
+        self.lib.ref_interp_vals_bli(_dp(out), xi, eta, mnx, mxx, mne, mxe, degree)
+        return out
+
+    def locate(self, c, x, y, z) -> int:
+        return self.lib.ref_point_locate_panel(c["h"], x, y, z)
+
+    def direct_sum_inv_lap(self, x, y, z, area, pots):
+        n = len(x)
+        out = np.zeros(n)
+        self.lib.ref_direct_sum_inv_lap(n, _dp(x), _dp(y), _dp(z), _dp(area), _dp(pots), _dp(out))
+        return out
