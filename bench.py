@@ -1,0 +1,326 @@
+#!/usr/bin/env python
+"""Benchmark of the BVE backward semi-Lagrangian RK4 step on B200.
+
+Workload (N=1): the 393,216-particle BVE configuration -- cubed sphere with
+6 x 64 x 64 leaf panels x 4 x 4 Chebyshev points (levels=7, interp_degree=3),
+unit sphere, Omega = 2*pi, Rossby-Haurwitz R=4 initial vorticity
+(omega0 = K = 0.5, mean removed), treecode/FMM velocity at MAC theta = 0.7,
+kernel_eps = 1e-4, dt = 0.005.  Synthetic inputs generated here; nothing is
+read from disk.
+
+  value     mixed-precision FMM steps/s (float32 pair kernels on
+            panel-relative coordinates, float64 everywhere else), inputs
+            resident in HBM, L2 flushed between steps, one device clock per
+            step (CUDA events), max over ranks.
+  e2e       the same steps through the C ABI with the step's inputs copied
+            from pinned host memory and the result read back every step.
+  extra     float64 "plain" FMM steps/s, their ratio, and the relative
+            L-infinity vorticity error after one step of both paths against
+            the float64 direct sum.
+
+With --gpus N under torchrun every rank runs an independent replica of the
+workload (the ensemble use: members share nothing), so scaling is weak and
+value = all ranks' steps / max-over-ranks time.
+
+--impl reference times the reference's own CPU step (oracle/_ref, the
+reference's unmodified sources on every host thread) on the same
+configuration; rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import csv
+import io
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+METRIC = "BVE RK4 steps/s at ≤1e-6 rel vort err: mixed+batched vs FP64 plain, 1 B200"
+LEVELS, DEGREE, THETA, EPS, OMEGA, DT = 7, 3, 0.7, 1e-4, 2 * np.pi, 0.005
+PAIR_FLOP = 17  # FLOP per Biot-Savart pair (division counted as 1)
+
+
+def workload_config():
+    return {"workload": "BVE RK4, 393,216 particles (6x64x64 panels x 4x4 points), RH4 IC, FMM theta=0.7",
+            "particles": 6 * 4 ** (LEVELS - 1) * (DEGREE + 1) ** 2, "levels": LEVELS, "interp_degree": DEGREE,
+            "theta": THETA, "kernel_eps": EPS, "omega": OMEGA, "dt": DT, "velocity": "fmm (reference spectral FMM)",
+            "precision": "mixed (f32 pairs, f64 positions/remap)", "l2": "flushed between timed steps"}
+
+
+def import_package():
+    sys.path.insert(0, ROOT)
+    from __graft_entry__ import _import_package
+
+    return _import_package()
+
+
+def rh4(g):
+    lat, lon = np.arcsin(np.clip(g.z, -1, 1)), np.arctan2(g.y, g.x)
+    vor = 2 * 0.5 * np.sin(lat) - 0.5 * np.sin(lat) * np.cos(lat) ** 4 * 30 * np.cos(4 * lon)
+    return vor - (vor * g.area).sum() / (4 * np.pi)
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.rows = []
+        if self.proc is None:
+            return False
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=10)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        for r in csv.reader(io.StringIO(out)):
+            if len(r) >= 9:
+                self.rows.append([c.strip() for c in r])
+        return False
+
+    def summary(self):
+        if not getattr(self, "rows", None):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    out = subprocess.run([sys.executable, "-m", "oracle.cpu_baseline", "--levels", str(LEVELS), "--theta",
+                          str(THETA), "--steps", str(args.steps), "--warmup", str(min(args.warmup, 1)),
+                          "--budget-s", "200"], cwd=ROOT, capture_output=True, text=True)
+    if out.returncode != 0:
+        print(json.dumps({"impl": "reference", "unavailable": "reference CPU step failed: " +
+                          (out.stderr.strip().splitlines() or ["?"])[-1]}))
+        return
+    r = json.loads(out.stdout.strip().splitlines()[-1])
+    v = r["steps_per_s"]
+    sample = (f"{r['steps_timed']} full bve_back_rk4_step calls of the {r['particles']}-particle problem "
+              f"(median), reference spectral FMM (interp_degree 3 proxies), float64")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": args.gpus,
+        "steps": r["steps_timed"], "warmup": min(args.warmup, 1), "ms_per_step": 1e3 / v, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload_config(),
+        "cpu_baseline": {"value": v, "unit": "steps/s", "cores": r["threads"], "kind": r["kind"], "sample": sample,
+                         "cpu": r["cpu"]},
+        "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def timed_steps(torch, ctx, f, steps, flush):
+    """Per-step device times (ms) of bve_run(nsteps=1) with an L2 flush between."""
+    st = torch.cuda.current_stream()
+    ts = []
+    for _ in range(steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        ctx.bve_run(*f, nsteps=1)
+        e1.record(st)
+        e1.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    return ts
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    sb = import_package()
+    dev = torch.device("cuda", local_rank)
+
+    g = sb.build_grid(LEVELS, DEGREE, exact_cc=True)
+    vor0 = rh4(g)
+    if world > 1:  # independent ensemble members: seeded perturbation per rank
+        vor0 = vor0 + np.random.default_rng(rank).standard_normal(vor0.shape) * 1e-3 * g.z
+
+    def T(a):
+        return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
+    def fields():
+        v = [torch.zeros_like(T(g.x)) for _ in range(3)]
+        return [T(g.x), T(g.y), T(g.z), T(g.area), T(vor0), *v, None]
+
+    def ctx_for(prec, vel=sb.VEL_FMM):
+        return sb.Context(sb.config_default(levels=LEVELS, interp_degree=DEGREE, fmm_theta=THETA, kernel_eps=EPS,
+                                            omega=OMEGA, dt=DT, precision=prec, velocity=vel))
+
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
+    ctx32, ctx64 = ctx_for(sb.MIXED), ctx_for(sb.FP64)
+    f32, f64 = fields(), fields()
+    for _ in range(args.warmup):
+        ctx32.bve_run(*f32, nsteps=1)
+        ctx64.bve_run(*f64, nsteps=1)
+    torch.cuda.synchronize()
+
+    # ---- headline: mixed precision, device-resident -----------------------
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = sb.kernel_launches()
+    with ClockSampler(local_rank) as clk:
+        ts32 = timed_steps(torch, ctx32, f32, args.steps, flush)
+    launches = sb.kernel_launches() - launches0
+    torch.cuda.synchronize()
+    t_total = sum(ts32)
+    if dist:
+        tt = torch.tensor([t_total], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_total = float(tt.item())
+        dist.barrier()
+    ms_per_step = t_total / args.steps
+    value = world * args.steps / (t_total * 1e-3)
+
+    # ---- float64 plain path --------------------------------------------------
+    ts64 = timed_steps(torch, ctx64, f64, args.steps, flush)
+    fp64_sps = 1e3 / (sum(ts64) / len(ts64))
+
+    # ---- accuracy after one step vs the float64 direct sum ------------------
+    ctxd = ctx_for(sb.FP64, sb.VEL_DIRECT)
+    fd, fa, fb = fields(), fields(), fields()
+    t0 = time.perf_counter()
+    ctxd.bve_back_rk4_step(*fd)
+    direct_s = time.perf_counter() - t0
+    ctx32.bve_back_rk4_step(*fa)
+    ctx64.bve_back_rk4_step(*fb)
+    ref = fd[4]
+    scale = ref.abs().max().item()
+    err32 = (fa[4] - ref).abs().max().item() / scale
+    err64 = (fb[4] - ref).abs().max().item() / scale
+    vel_ref = torch.stack(fd[5:8])
+    vscale = vel_ref.abs().max().item()
+    verr32 = (torch.stack(fa[5:8]) - vel_ref).abs().max().item() / vscale
+    del ctxd
+
+    # ---- roofline of the dominant kernel (interaction kernel, mixed) -------
+    ms_int, pairs = ctx32.time_interactions(reps=5)
+    achieved = PAIR_FLOP * pairs / (ms_int * 1e-3) / 1e12
+    peak_meas = sb.measure_fma_peak(0, 50.0) / 1e12
+    ms_int64, _ = ctx64.time_interactions(reps=3)
+    ach64 = PAIR_FLOP * pairs / (ms_int64 * 1e-3) / 1e12
+    peak64 = sb.measure_fma_peak(1, 50.0) / 1e12
+    share = 4 * ms_int / ms_per_step
+
+    # ---- end to end through the C ABI with host buffers ---------------------
+    host = [torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in (g.x, g.y, g.z, g.area, vor0)]
+    out_host = [torch.empty(g.x.shape, dtype=torch.float64).pin_memory() for _ in range(4)]
+    fe = fields()
+    st = torch.cuda.current_stream()
+    h2d = sum(h.numel() * 8 for h in host)
+    d2h = sum(o.numel() * 8 for o in out_host)
+    te = []
+    for _ in range(args.steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for d_, h_ in zip(fe[:5], host):
+            d_.copy_(h_, non_blocking=True)
+        ctx32.bve_back_rk4_step(*fe)
+        for o_, d_ in zip(out_host, [fe[4], *fe[5:8]]):
+            o_.copy_(d_, non_blocking=True)
+        e1.record(st)
+        e1.synchronize()
+        te.append(e0.elapsed_time(e1))
+    e2e_total = sum(te)
+    if dist:
+        tt = torch.tensor([e2e_total], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_total = float(tt.item())
+    e2e = world * args.steps / (e2e_total * 1e-3)
+
+    # ---- CPU baseline: the reference's own step on the host cores ----------
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out = subprocess.run([sys.executable, "-m", "oracle.cpu_baseline", "--levels", str(LEVELS), "--steps", "1",
+                              "--warmup", "0", "--budget-s", "60"], cwd=ROOT, capture_output=True, text=True)
+        if out.returncode == 0:
+            r = json.loads(out.stdout.strip().splitlines()[-1])
+            cpu = {"value": r["steps_per_s"], "unit": "steps/s", "cores": r["threads"], "kind": r["kind"],
+                   "sample": f"1 full bve_back_rk4_step of the {r['particles']}-particle problem (reference "
+                             f"spectral FMM, float64), {r['threads']} OpenMP threads", "cpu": r["cpu"]}
+        else:
+            cpu = {"value": None, "unit": "steps/s", "cores": os.cpu_count(), "kind": "reference",
+                   "sample": "failed: " + (out.stderr.strip().splitlines() or ["?"])[-1]}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 pairs / f64 positions+remap", "data": "synthetic",
+            "config": dict(workload_config(), parallelism=f"replicas x{world}" if world > 1 else "1 GPU"),
+            "e2e": {"value": e2e, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches,
+            "roofline": {"bound": "fp32", "kernel": "k_interact32 (pair interactions, q=16)", "achieved": achieved,
+                         "peak": peak_meas, "unit": "TFLOP/s", "frac": achieved / peak_meas, "traffic": None,
+                         "flop_per_pair": PAIR_FLOP, "pairs_per_launch": pairs, "ms_per_launch": ms_int,
+                         "step_share": share,
+                         "peak_source": "measured f32 FMA-chain throughput on this GPU (sbslpm_measure_fma_peak); "
+                                        "MEASURED_PEAKS.json has no CUDA-core peak"},
+            "fp64_plain": {"steps_per_s": fp64_sps, "ms_per_step": 1e3 / fp64_sps,
+                           "interaction_tflops": ach64, "fp64_fma_peak_tflops": peak64,
+                           "frac": ach64 / peak64},
+            "speedup_mixed_vs_fp64_plain": value / world / fp64_sps,
+            "accuracy_step1_vs_fp64_direct": {"mixed_rel_linf_vort": err32, "fp64_fmm_rel_linf_vort": err64,
+                                              "mixed_rel_linf_vel": verr32, "direct_step_s": direct_s},
+            "cpu_baseline": cpu, "clocks": clk.summary(),
+        }
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

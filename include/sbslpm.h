@@ -1,0 +1,216 @@
+/*
+ * sbslpm.h -- C ABI of the B200-native backward semi-Lagrangian (BSL) hot path
+ * of spectral-BSLPM: the barotropic vorticity equation (BVE) RK4 step on the
+ * cubed sphere, its Biot-Savart velocity (barycentric-Lagrange treecode/FMM or
+ * direct sum), the FMM passes, and the departure-point Lagrange remap.
+ *
+ * Plain pointers and sizes only.  Unless stated otherwise, field pointers are
+ * DEVICE pointers (cudaMalloc'd or torch CUDA tensors) in the reference's
+ * layout: row-major [panel][q] float64, q = (interp_degree+1)^2, point index
+ * i*(degree+1)+j with i the xi node and j the eta node
+ * (reference: src/interp_funcs.cpp:64-72).  Leaf-only fields are
+ * [leaf_count][q]; proxy fields over the whole tree are [panel_count][q].
+ *
+ * Every entry point returns an sbslpm_status.  Device code never traps: a
+ * point outside its panel (where the reference calls Kokkos::abort,
+ * src/interp_funcs_impl.hpp:22-33) or a non-finite input sets a device error
+ * word that the host turns into a status after the call.
+ *
+ * Threading: one host thread per context; calls on one context are ordered
+ * on the context's CUDA stream and are not re-entrant.  Separate contexts are
+ * independent.
+ */
+#ifndef SBSLPM_H
+#define SBSLPM_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  SBSLPM_OK = 0,
+  SBSLPM_ERR_CONFIG = 1,       /* invalid configuration / namelist */
+  SBSLPM_ERR_CUDA = 2,         /* CUDA runtime error (message: sbslpm_last_error) */
+  SBSLPM_ERR_OUT_OF_PANEL = 3, /* BLI point outside its panel (reference aborts) */
+  SBSLPM_ERR_NONFINITE = 4,    /* NaN/Inf met in a location step */
+  SBSLPM_ERR_ARG = 5,          /* bad argument (null pointer, size) */
+  SBSLPM_ERR_NO_DEVICE = 6     /* no CUDA device / library built without it */
+} sbslpm_status;
+
+/* Velocity evaluation used by the step. */
+enum { SBSLPM_VEL_FMM = 0, SBSLPM_VEL_DIRECT = 1 };
+/* Arithmetic of the pair kernels.  FP64: everything in float64.  MIXED: the
+ * pair kernels evaluate in float32 on panel-relative coordinates and
+ * accumulate per source panel in float32, then in float64; positions,
+ * projections, BLI weights, the RK4 update and the remap stay float64. */
+enum { SBSLPM_FP64 = 0, SBSLPM_MIXED = 1 };
+
+/* Mirrors the hot-path fields of the reference's RunConfig
+ * (src/run_config.hpp:6-44).  dt is a double (the reference's delta_t is an
+ * int number of seconds). */
+typedef struct {
+  int levels;        /* RunConfig::levels: tree depth; leaves at level levels-1 */
+  int interp_degree; /* RunConfig::interp_degree, 0..10 */
+  double fmm_theta;  /* RunConfig::fmm_theta, MAC parameter */
+  double kernel_eps; /* RunConfig::kernel_eps */
+  double omega;      /* RunConfig::omega, rotation rate */
+  double dt;         /* time step (RunConfig::delta_t as a double) */
+  int tracer_count;  /* RunConfig::tracer_count */
+  int velocity;      /* SBSLPM_VEL_FMM | SBSLPM_VEL_DIRECT */
+  int precision;     /* SBSLPM_FP64 | SBSLPM_MIXED */
+  int exact_cc;      /* setup helpers: 1 = exact Clenshaw-Curtis weights */
+} sbslpm_config;
+
+/* Same fields and order as the reference's CubedSpherePanel
+ * (src/initialize_cubed_sphere.hpp:8-29); is_leaf is an int here. */
+typedef struct {
+  int id, id_top_edge, id_left_edge, id_bot_edge, id_right_edge, face, level, parent_id;
+  int child1, child2, child3, child4;
+  int is_leaf;
+  double min_xi, max_xi, min_eta, max_eta, radius, area;
+  int point_count;
+} sbslpm_panel;
+
+/* The reference's interact_pair (src/fmm_funcs.hpp:10-14). */
+typedef struct {
+  int target_panel, source_panel, interact_type; /* 0 pp, 1 pc, 2 cp, 3 cc */
+} sbslpm_interact_pair;
+
+typedef struct sbslpm_ctx sbslpm_ctx;
+
+/* ---------------- configuration ---------------- */
+
+/* Defaults of the reference's RunConfig / namelist.txt (theta 0.7,
+ * kernel_eps 1e-4, Earth omega) with FMM velocity and float64. */
+sbslpm_status sbslpm_config_default(sbslpm_config* cfg);
+/* Replaces read_run_config (src/io_utils.cpp:11-92): key=value lines read
+ * until an unknown key.  Extra keys of this library: dt (double), velocity
+ * (fmm|direct), precision (fp64|mixed), exact_cc (0|1). */
+sbslpm_status sbslpm_read_run_config(const char* path, sbslpm_config* cfg);
+const char* sbslpm_status_string(sbslpm_status s);
+/* Last error message of the calling thread (CUDA errors, config errors). */
+const char* sbslpm_last_error(void);
+
+/* ---------------- host-side setup (host pointers) ---------------- */
+
+int sbslpm_panel_count(int levels); /* 2(4^levels - 1) */
+int sbslpm_leaf_count(int levels);  /* 6 * 4^(levels-1) */
+/* Replaces cubed_sphere_panels_init (src/initialize_cubed_sphere.cpp:185-234). */
+sbslpm_status sbslpm_cubed_sphere_panels_init(int levels, sbslpm_panel* panels);
+/* Replaces interp_init (src/interp_funcs.cpp:24-73); interp is q x 4. */
+sbslpm_status sbslpm_interp_init(int degree, int exact_cc, double* interp);
+/* Replaces cube_sphere_spec_points (src/initialize_cubed_sphere.cpp:280-288). */
+sbslpm_status sbslpm_cube_sphere_spec_points(int levels, int degree, const sbslpm_panel* panels,
+                                             const double* interp, double* xcos, double* ycos, double* zcos,
+                                             double* area);
+/* Replaces dual_tree_traversal (src/fmm_funcs.cpp:17-123).  Writes at most cap
+ * pairs to out (may be NULL) and returns the full count in *count. */
+sbslpm_status sbslpm_dual_tree_traversal(int levels, const sbslpm_panel* panels, double theta,
+                                         sbslpm_interact_pair* out, long cap, long* count);
+/* Host versions of interp_vals_bli / point_locate_panel
+ * (src/interp_funcs_impl.hpp:11-142). */
+sbslpm_status sbslpm_interp_vals_bli(double* basis, double xi, double eta, double min_xi, double max_xi,
+                                     double min_eta, double max_eta, int degree);
+int sbslpm_point_locate_panel(const sbslpm_panel* panels, double x, double y, double z);
+
+/* ---------------- context ---------------- */
+
+/* Builds the panel tree and interaction list for cfg, precomputes the static
+ * geometry on the device and allocates the step workspace (all device memory
+ * the step needs is owned by the context). */
+sbslpm_status sbslpm_create(const sbslpm_config* cfg, sbslpm_ctx** out);
+sbslpm_status sbslpm_destroy(sbslpm_ctx* ctx);
+/* Orders all later work of ctx on this cudaStream_t (NULL = the legacy
+ * default stream).  Until it is called, ctx uses a stream of its own. */
+sbslpm_status sbslpm_set_stream(sbslpm_ctx* ctx, void* cuda_stream);
+/* sizes[0..3] = panel_count, leaf_count, q, interaction_count */
+sbslpm_status sbslpm_get_sizes(const sbslpm_ctx* ctx, long* sizes);
+/* Host copies of the context's panel table (panel_count entries) and
+ * interaction list (interaction_count entries, reference order). */
+sbslpm_status sbslpm_get_panels(const sbslpm_ctx* ctx, sbslpm_panel* out);
+sbslpm_status sbslpm_get_interactions(const sbslpm_ctx* ctx, sbslpm_interact_pair* out);
+/* Number of kernels this library has launched in this process (graph
+ * replays count every kernel node). */
+long sbslpm_kernel_launches(void);
+
+/* ---------------- the step ---------------- */
+
+/* Replaces bve_back_rk4_step (src/bve_time_step.cpp:311-419; declared in
+ * src/bve_time_step.hpp:7-13).  Device pointers: xcos, ycos, zcos, area are
+ * [leaf][q]; vors is advanced in place; vel_x/y/z receive the stage-0
+ * velocity (the reference's vel_x/y/z); tracers [leaf][q][tracer_count] are
+ * remapped in place (may be NULL when tracer_count is 0).  time is accepted
+ * for interface parity (forcing is off, so it is unused). */
+sbslpm_status sbslpm_bve_step(sbslpm_ctx* ctx, const double* xcos, const double* ycos, const double* zcos,
+                              const double* area, double* vors, double* vel_x, double* vel_y, double* vel_z,
+                              double* tracers, double time);
+/* nsteps consecutive steps, captured once as a CUDA graph and replayed. */
+sbslpm_status sbslpm_bve_run(sbslpm_ctx* ctx, const double* xcos, const double* ycos, const double* zcos,
+                             const double* area, double* vors, double* vel_x, double* vel_y, double* vel_z,
+                             double* tracers, double time, int nsteps);
+
+/* ---------------- pieces of the step (device pointers) ---------------- */
+
+/* Replaces upward_pass (src/fmm_funcs.cpp:341-355): leaf strengths
+ * area*pots ([leaf][q]) anterpolated up the tree into proxy_source
+ * ([panel][q], overwritten). */
+sbslpm_status sbslpm_upward_pass(sbslpm_ctx* ctx, const double* area, const double* pots, double* proxy_source);
+/* Replaces bve_vel_interactions (src/fmm_interactions/bve_vel.cpp:9-37):
+ * proxy-target velocities of every pair in the interaction list with sources
+ * at proj(proxy + disp); disp_* and source are [panel][q]; target_1..3
+ * ([panel][q]) are accumulated into, as in the reference. */
+sbslpm_status sbslpm_bve_vel_interactions(sbslpm_ctx* ctx, const double* disp_x, const double* disp_y,
+                                          const double* disp_z, const double* source, double* target_1,
+                                          double* target_2, double* target_3);
+/* Replaces downward_pass_3 (src/fmm_funcs.cpp:374-392): targets ([panel][q],
+ * updated in place as in the reference) interpolated down the tree; sols_*
+ * ([leaf][q]) receive the leaf values. */
+sbslpm_status sbslpm_downward_pass_3(sbslpm_ctx* ctx, double* target_1, double* target_2, double* target_3,
+                                     double* sols_1, double* sols_2, double* sols_3);
+/* Replaces the bve_find_departure_points functor (src/bve_time_step.cpp:172-309):
+ * v0..v3 are [3][leaf][q] (x, y, z blocks); dep_* are [leaf][q]. */
+sbslpm_status sbslpm_bve_departure(sbslpm_ctx* ctx, const double* xcos, const double* ycos, const double* zcos,
+                                   const double* v0, const double* v1, const double* v2, const double* v3,
+                                   double dt, double* dep_x, double* dep_y, double* dep_z);
+/* Replaces the bve_departure_to_target functor (src/bve_time_step.cpp:15-67):
+ * new_vors = BLI(vors)(dep) + 2 omega (dep_z - zcos); tracers likewise. */
+sbslpm_status sbslpm_bve_remap(sbslpm_ctx* ctx, const double* zcos, const double* dep_x, const double* dep_y,
+                               const double* dep_z, const double* vors, const double* tracers, double* new_vors,
+                               double* new_tracers);
+
+/* ---------------- direct sums (device pointers, no context) ---------------- */
+
+/* Biot-Savart direct sum on the sphere (the reference's BVE kernel,
+ * src/fmm_interactions/bve_vel_impl.hpp:113-118, over all pairs):
+ *   u_i = -1/(4 pi) sum_j (x_i x y_j) s_j / (1 - x_i.y_j + eps)
+ * evaluated as x_i x sum_j s_j (y_j - x_i) / (|y_j - x_i|^2/2 + eps).
+ * Pairs with y_j == x_i contribute nothing.  precision: SBSLPM_FP64 or
+ * SBSLPM_MIXED.  stream: cudaStream_t or NULL. */
+sbslpm_status sbslpm_direct_sum_bve(long n_targets, const double* tx, const double* ty, const double* tz,
+                                    long n_sources, const double* sx, const double* sy, const double* sz,
+                                    const double* strength, double eps, int precision, double* u_x, double* u_y,
+                                    double* u_z, void* stream);
+/* Replaces direct_sum_inv_lap (src/direct_sum.cpp:8-15, inv_lap
+ * src/direct_sum_impl.hpp:20-27): soln_i += sum_{j != i}
+ * -1/(4 pi) log(1 - x_i.x_j) area_j pots_j (soln accumulated into). */
+sbslpm_status sbslpm_direct_sum_inv_lap(long n, const double* x, const double* y, const double* z,
+                                        const double* area, const double* pots, double* soln, void* stream);
+
+/* ---------------- measurement ---------------- */
+
+/* Average device time of one launch of the interaction kernel alone (the
+ * dominant kernel of the step), over reps launches on the current sources of
+ * the context (those of the last stage run), timed with CUDA events on the
+ * context's stream.  *pairs receives the pair evaluations per launch. */
+sbslpm_status sbslpm_time_interactions(sbslpm_ctx* ctx, int reps, double* ms_per_launch, double* pairs);
+/* CUDA-core fused multiply-add throughput of this GPU, measured with
+ * independent FMA chains on every SM for about ms milliseconds: kind 0 =
+ * float32, 1 = float64.  Returns FLOP/s (2 per FMA) in *flops. */
+sbslpm_status sbslpm_measure_fma_peak(int kind, double ms, double* flops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SBSLPM_H */

@@ -1,0 +1,359 @@
+"""B200-native backward semi-Lagrangian hot path of spectral-BSLPM.
+
+Python binding of the C ABI in include/sbslpm.h (libsbslpm.so, built in-tree
+by ``make -C spectral-bslpm_b200/csrc``).  The names mirror the reference's
+C++ entry points (bve_back_rk4_step, upward_pass, bve_vel_interactions,
+downward_pass_3, dual_tree_traversal, interp_init, ...).  Field arguments of
+the device entry points are torch CUDA float64 tensors in the reference's
+[panel][q] row-major layout; torch provides device memory and the stream,
+every computation runs in this library's sm_100a kernels.
+
+There is no CPU fallback: without the library or a GPU the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+__all__ = [
+    "SbslpmError", "Config", "Panel", "InteractPair", "FP64", "MIXED", "VEL_FMM", "VEL_DIRECT", "library_path",
+    "lib", "config_default", "read_run_config", "panel_count", "leaf_count", "cubed_sphere_panels_init",
+    "interp_init", "cube_sphere_spec_points", "dual_tree_traversal", "interp_vals_bli", "point_locate_panel",
+    "Context", "direct_sum_bve", "direct_sum_inv_lap", "kernel_launches", "Grid", "build_grid",
+]
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+FP64, MIXED = 0, 1
+VEL_FMM, VEL_DIRECT = 0, 1
+
+_D = ctypes.POINTER(ctypes.c_double)
+_VP = ctypes.c_void_p
+
+
+class SbslpmError(RuntimeError):
+    def __init__(self, status: int, where: str, message: str):
+        super().__init__(f"{where}: status {status} ({message})")
+        self.status = status
+
+
+class Config(ctypes.Structure):
+    """sbslpm_config: the hot-path fields of the reference's RunConfig."""
+
+    _fields_ = [
+        ("levels", ctypes.c_int),
+        ("interp_degree", ctypes.c_int),
+        ("fmm_theta", ctypes.c_double),
+        ("kernel_eps", ctypes.c_double),
+        ("omega", ctypes.c_double),
+        ("dt", ctypes.c_double),
+        ("tracer_count", ctypes.c_int),
+        ("velocity", ctypes.c_int),
+        ("precision", ctypes.c_int),
+        ("exact_cc", ctypes.c_int),
+    ]
+
+
+class Panel(ctypes.Structure):
+    """sbslpm_panel: the reference's CubedSpherePanel."""
+
+    _fields_ = [(n, ctypes.c_int) for n in (
+        "id", "id_top_edge", "id_left_edge", "id_bot_edge", "id_right_edge", "face", "level", "parent_id",
+        "child1", "child2", "child3", "child4", "is_leaf")] + [
+        (n, ctypes.c_double) for n in ("min_xi", "max_xi", "min_eta", "max_eta", "radius", "area")] + [
+        ("point_count", ctypes.c_int)]
+
+
+class InteractPair(ctypes.Structure):
+    _fields_ = [("target_panel", ctypes.c_int), ("source_panel", ctypes.c_int), ("interact_type", ctypes.c_int)]
+
+
+def library_path() -> str:
+    return os.path.join(HERE, "libsbslpm.so")
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded C ABI library; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = library_path()
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing: build it with `make -C {os.path.join(HERE, 'csrc')}`")
+    L = ctypes.CDLL(path)
+    L.sbslpm_status_string.restype = ctypes.c_char_p
+    L.sbslpm_last_error.restype = ctypes.c_char_p
+    L.sbslpm_kernel_launches.restype = ctypes.c_long
+    L.sbslpm_point_locate_panel.restype = ctypes.c_int
+    L.sbslpm_point_locate_panel.argtypes = [ctypes.POINTER(Panel), ctypes.c_double, ctypes.c_double, ctypes.c_double]
+    L.sbslpm_interp_vals_bli.argtypes = [_D] + [ctypes.c_double] * 6 + [ctypes.c_int]
+    L.sbslpm_dual_tree_traversal.argtypes = [ctypes.c_int, ctypes.POINTER(Panel), ctypes.c_double,
+                                             ctypes.POINTER(InteractPair), ctypes.c_long,
+                                             ctypes.POINTER(ctypes.c_long)]
+    L.sbslpm_create.argtypes = [ctypes.POINTER(Config), ctypes.POINTER(_VP)]
+    for name in ("sbslpm_destroy", "sbslpm_set_stream", "sbslpm_get_sizes", "sbslpm_get_panels",
+                 "sbslpm_get_interactions"):
+        getattr(L, name).argtypes = None
+    L.sbslpm_bve_step.argtypes = [_VP] + [_VP] * 9 + [ctypes.c_double]
+    L.sbslpm_bve_run.argtypes = [_VP] + [_VP] * 9 + [ctypes.c_double, ctypes.c_int]
+    L.sbslpm_upward_pass.argtypes = [_VP] * 4
+    L.sbslpm_bve_vel_interactions.argtypes = [_VP] * 8
+    L.sbslpm_downward_pass_3.argtypes = [_VP] * 7
+    L.sbslpm_bve_departure.argtypes = [_VP] * 8 + [ctypes.c_double] + [_VP] * 3
+    L.sbslpm_bve_remap.argtypes = [_VP] * 9
+    L.sbslpm_direct_sum_bve.argtypes = [ctypes.c_long, _VP, _VP, _VP, ctypes.c_long, _VP, _VP, _VP, _VP,
+                                        ctypes.c_double, ctypes.c_int, _VP, _VP, _VP, _VP]
+    L.sbslpm_direct_sum_inv_lap.argtypes = [ctypes.c_long] + [_VP] * 7
+    L.sbslpm_time_interactions.argtypes = [_VP, ctypes.c_int, _D, _D]
+    L.sbslpm_measure_fma_peak.argtypes = [ctypes.c_int, ctypes.c_double, _D]
+    _lib = L
+    return L
+
+
+def _check(status: int, where: str):
+    if status != 0:
+        L = lib()
+        msg = L.sbslpm_last_error().decode() or L.sbslpm_status_string(status).decode()
+        raise SbslpmError(status, where, msg)
+
+
+def kernel_launches() -> int:
+    return int(lib().sbslpm_kernel_launches())
+
+
+# ---------------------------------------------------------------- config ----
+
+def config_default(**overrides) -> Config:
+    cfg = Config()
+    _check(lib().sbslpm_config_default(ctypes.byref(cfg)), "sbslpm_config_default")
+    for k, v in overrides.items():
+        if not hasattr(cfg, k):
+            raise AttributeError(f"unknown config field {k}")
+        setattr(cfg, k, v)
+    return cfg
+
+
+def read_run_config(path: str, base: Config | None = None) -> Config:
+    """read_run_config (src/io_utils.cpp:11-92) into a Config."""
+    cfg = base if base is not None else config_default()
+    _check(lib().sbslpm_read_run_config(path.encode(), ctypes.byref(cfg)), "sbslpm_read_run_config")
+    return cfg
+
+
+# ----------------------------------------------------------------- setup ----
+
+def panel_count(levels: int) -> int:
+    return 2 * (4**levels - 1)
+
+
+def leaf_count(levels: int) -> int:
+    return 6 * 4 ** (levels - 1)
+
+
+def cubed_sphere_panels_init(levels: int):
+    panels = (Panel * panel_count(levels))()
+    _check(lib().sbslpm_cubed_sphere_panels_init(levels, panels), "sbslpm_cubed_sphere_panels_init")
+    return panels
+
+
+def interp_init(degree: int, exact_cc: bool = False) -> np.ndarray:
+    out = np.zeros(((degree + 1) ** 2, 4))
+    _check(lib().sbslpm_interp_init(degree, int(exact_cc), out.ctypes.data_as(_D)), "sbslpm_interp_init")
+    return out
+
+
+def cube_sphere_spec_points(levels: int, degree: int, panels, interp: np.ndarray):
+    A, q = leaf_count(levels), (degree + 1) ** 2
+    x, y, z, area = (np.zeros((A, q)) for _ in range(4))
+    interp = np.ascontiguousarray(interp, dtype=np.float64)
+    _check(lib().sbslpm_cube_sphere_spec_points(levels, degree, panels, interp.ctypes.data_as(_D),
+                                                *[a.ctypes.data_as(_D) for a in (x, y, z, area)]),
+           "sbslpm_cube_sphere_spec_points")
+    return x, y, z, area
+
+
+def dual_tree_traversal(levels: int, panels, theta: float) -> np.ndarray:
+    """Interaction list (I x 3 int32: target, source, type) in the reference's order."""
+    n = ctypes.c_long(0)
+    _check(lib().sbslpm_dual_tree_traversal(levels, panels, theta, None, 0, ctypes.byref(n)), "traversal")
+    out = (InteractPair * max(n.value, 1))()
+    _check(lib().sbslpm_dual_tree_traversal(levels, panels, theta, out, n.value, ctypes.byref(n)), "traversal")
+    return np.ctypeslib.as_array(ctypes.cast(out, ctypes.POINTER(ctypes.c_int)), (max(n.value, 1), 3))[: n.value].copy()
+
+
+def interp_vals_bli(xi, eta, min_xi, max_xi, min_eta, max_eta, degree) -> np.ndarray:
+    out = np.zeros((degree + 1) ** 2)
+    _check(lib().sbslpm_interp_vals_bli(out.ctypes.data_as(_D), xi, eta, min_xi, max_xi, min_eta, max_eta, degree),
+           "sbslpm_interp_vals_bli")
+    return out
+
+
+def point_locate_panel(panels, x, y, z) -> int:
+    return int(lib().sbslpm_point_locate_panel(panels, x, y, z))
+
+
+@dataclass
+class Grid:
+    """Leaf points of the cubed sphere (numpy, [leaf][q])."""
+
+    levels: int
+    degree: int
+    panels: object
+    interp: np.ndarray
+    x: np.ndarray
+    y: np.ndarray
+    z: np.ndarray
+    area: np.ndarray
+
+
+def build_grid(levels: int, degree: int, exact_cc: bool = True) -> Grid:
+    panels = cubed_sphere_panels_init(levels)
+    interp = interp_init(degree, exact_cc)
+    x, y, z, area = cube_sphere_spec_points(levels, degree, panels, interp)
+    return Grid(levels, degree, panels, interp, x, y, z, area)
+
+
+# --------------------------------------------------------------- device ----
+
+def _dev(t, name, shape=None):
+    """Device pointer of a contiguous float64 CUDA tensor (None -> NULL)."""
+    if t is None:
+        return None
+    import torch
+
+    if not isinstance(t, torch.Tensor) or not t.is_cuda or t.dtype != torch.float64 or not t.is_contiguous():
+        raise TypeError(f"{name} must be a contiguous float64 CUDA tensor")
+    if shape is not None and t.numel() != int(np.prod(shape)):
+        raise ValueError(f"{name} has {t.numel()} elements, expected {shape}")
+    return t.data_ptr()
+
+
+def _stream():
+    import torch
+
+    return torch.cuda.current_stream().cuda_stream
+
+
+class Context:
+    """sbslpm_ctx: tree, interaction list, static geometry and workspace on one GPU."""
+
+    def __init__(self, cfg: Config):
+        self.cfg = cfg
+        h = _VP()
+        _check(lib().sbslpm_create(ctypes.byref(cfg), ctypes.byref(h)), "sbslpm_create")
+        self._h = h
+        sizes = (ctypes.c_long * 4)()
+        _check(lib().sbslpm_get_sizes(self._h, sizes), "sbslpm_get_sizes")
+        self.panel_count, self.leaf_count, self.q, self.interaction_count = (int(v) for v in sizes)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().sbslpm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _sync_stream(self):
+        _check(lib().sbslpm_set_stream(self._h, _VP(_stream())), "sbslpm_set_stream")
+
+    def panels(self):
+        out = (Panel * self.panel_count)()
+        _check(lib().sbslpm_get_panels(self._h, out), "sbslpm_get_panels")
+        return out
+
+    def interactions(self) -> np.ndarray:
+        n = max(self.interaction_count, 1)
+        out = (InteractPair * n)()
+        _check(lib().sbslpm_get_interactions(self._h, out), "sbslpm_get_interactions")
+        arr = np.ctypeslib.as_array(ctypes.cast(out, ctypes.POINTER(ctypes.c_int)), (n, 3))
+        return arr[: self.interaction_count].copy()
+
+    # -- the step -------------------------------------------------------
+    def bve_back_rk4_step(self, xcos, ycos, zcos, area, vors, vel_x, vel_y, vel_z, tracers=None, time=0.0):
+        """bve_back_rk4_step (src/bve_time_step.cpp:311-419): vors, vel_*, tracers in place."""
+        lq = (self.leaf_count, self.q)
+        self._sync_stream()
+        _check(lib().sbslpm_bve_step(self._h, *[_dev(t, n, lq) for t, n in (
+            (xcos, "xcos"), (ycos, "ycos"), (zcos, "zcos"), (area, "area"), (vors, "vors"), (vel_x, "vel_x"),
+            (vel_y, "vel_y"), (vel_z, "vel_z"))], _dev(tracers, "tracers"), float(time)), "sbslpm_bve_step")
+
+    def bve_run(self, xcos, ycos, zcos, area, vors, vel_x, vel_y, vel_z, tracers=None, time=0.0, nsteps=1):
+        """nsteps steps replayed from one captured CUDA graph."""
+        lq = (self.leaf_count, self.q)
+        self._sync_stream()
+        _check(lib().sbslpm_bve_run(self._h, *[_dev(t, n, lq) for t, n in (
+            (xcos, "xcos"), (ycos, "ycos"), (zcos, "zcos"), (area, "area"), (vors, "vors"), (vel_x, "vel_x"),
+            (vel_y, "vel_y"), (vel_z, "vel_z"))], _dev(tracers, "tracers"), float(time), int(nsteps)),
+            "sbslpm_bve_run")
+
+    def time_interactions(self, reps: int = 5):
+        """(ms per launch, pair evaluations per launch) of the interaction kernel alone."""
+        ms, pairs = ctypes.c_double(), ctypes.c_double()
+        self._sync_stream()
+        _check(lib().sbslpm_time_interactions(self._h, int(reps), ctypes.byref(ms), ctypes.byref(pairs)),
+               "sbslpm_time_interactions")
+        return ms.value, pairs.value
+
+    # -- pieces ---------------------------------------------------------
+    def upward_pass(self, area, pots, proxy_source):
+        self._sync_stream()
+        _check(lib().sbslpm_upward_pass(self._h, _dev(area, "area"), _dev(pots, "pots"),
+                                        _dev(proxy_source, "proxy_source")), "sbslpm_upward_pass")
+
+    def bve_vel_interactions(self, disp_x, disp_y, disp_z, source, t1, t2, t3):
+        self._sync_stream()
+        _check(lib().sbslpm_bve_vel_interactions(self._h, *[_dev(t, "field") for t in (
+            disp_x, disp_y, disp_z, source, t1, t2, t3)]), "sbslpm_bve_vel_interactions")
+
+    def downward_pass_3(self, t1, t2, t3, s1, s2, s3):
+        self._sync_stream()
+        _check(lib().sbslpm_downward_pass_3(self._h, *[_dev(t, "field") for t in (t1, t2, t3, s1, s2, s3)]),
+               "sbslpm_downward_pass_3")
+
+    def bve_departure(self, xcos, ycos, zcos, v0, v1, v2, v3, dt, dep_x, dep_y, dep_z):
+        self._sync_stream()
+        _check(lib().sbslpm_bve_departure(self._h, *[_dev(t, "field") for t in (xcos, ycos, zcos, v0, v1, v2, v3)],
+                                          float(dt), *[_dev(t, "dep") for t in (dep_x, dep_y, dep_z)]),
+               "sbslpm_bve_departure")
+
+    def bve_remap(self, zcos, dep_x, dep_y, dep_z, vors, tracers, new_vors, new_tracers):
+        self._sync_stream()
+        _check(lib().sbslpm_bve_remap(self._h, *[_dev(t, "field") for t in (zcos, dep_x, dep_y, dep_z, vors)],
+                                      _dev(tracers, "tracers"), _dev(new_vors, "new_vors"),
+                                      _dev(new_tracers, "new_tracers")), "sbslpm_bve_remap")
+
+
+def measure_fma_peak(kind: int = 0, ms: float = 50.0) -> float:
+    """Measured CUDA-core FMA throughput in FLOP/s (kind 0 float32, 1 float64)."""
+    out = ctypes.c_double()
+    _check(lib().sbslpm_measure_fma_peak(int(kind), float(ms), ctypes.byref(out)), "sbslpm_measure_fma_peak")
+    return out.value
+
+
+def direct_sum_bve(tx, ty, tz, sx, sy, sz, strength, eps, precision=FP64, out=None):
+    """Biot-Savart direct sum on the sphere; returns (ux, uy, uz) tensors."""
+    import torch
+
+    nt, ns = tx.numel(), sx.numel()
+    if out is None:
+        out = tuple(torch.empty(nt, dtype=torch.float64, device=tx.device) for _ in range(3))
+    _check(lib().sbslpm_direct_sum_bve(nt, *[_dev(t, "target") for t in (tx, ty, tz)], ns,
+                                       *[_dev(t, "source") for t in (sx, sy, sz, strength)], float(eps),
+                                       int(precision), *[_dev(t, "out") for t in out], _VP(_stream())),
+           "sbslpm_direct_sum_bve")
+    return out
+
+
+def direct_sum_inv_lap(x, y, z, area, pots, soln):
+    """direct_sum_inv_lap (src/direct_sum.cpp:8-15): soln accumulated in place."""
+    _check(lib().sbslpm_direct_sum_inv_lap(x.numel(), *[_dev(t, "field") for t in (x, y, z, area, pots, soln)],
+                                           _VP(_stream())), "sbslpm_direct_sum_inv_lap")

@@ -1,0 +1,906 @@
+// Device kernels of the BVE backward semi-Lagrangian step, sm_100a.
+//
+// Data layout in HBM (all row-major, [panel][q] as in the reference):
+//   src   : double4 [panels*q]  displaced source position (x, y, z) and
+//           strength w = area * vorticity (leaves) or its anterpolation
+//           (non-leaf proxies).  32 B per proxy point, one load per pair block.
+//   srcf  : float4  [panels*q]  mixed precision: position relative to the
+//           panel centre (float) and strength (float).
+//   tgt   : double  [3][panels*q] proxy-target velocities.
+//   v_k   : double  [3][leaves*q] stage velocities (x, y, z blocks).
+// Every kernel is owner-computes (no atomics), so results are deterministic.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+
+#include "../../include/sbslpm.h"
+#include "bve_kernels.cuh"
+
+namespace sbslpm {
+
+long& launch_counter() {
+  static long n = 0;
+  return n;
+}
+
+namespace {
+
+constexpr int kWarpsPerBlock = 4;
+
+__device__ __forceinline__ void flag(unsigned* err, unsigned bits) {
+  if (bits) atomicOr(err, bits);
+}
+
+// 1/d from the hardware approximation refined by two Newton-Raphson steps
+// r <- r + r (1 - d r); each step squares the relative error.  d > 0.
+__device__ __forceinline__ double recip_nr(double d) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(d));
+  double e = fma(-d, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-d, r, 1.0);
+  return fma(r, e, r);
+}
+
+__device__ __forceinline__ float recip_f32(float d) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(d));
+  return r;
+}
+
+// One Biot-Savart pair in float64.  With d = y - x and |x| = |y| = 1,
+// 1 - x.y = |d|^2 / 2, and x cross y = x cross d, so the accumulated
+// a = sum g d gives u = -1/(4 pi) x cross a.  Coincident points add nothing.
+__device__ __forceinline__ void pair64(double tx, double ty, double tz, const double4 s, double eps, double& ax,
+                                       double& ay, double& az) {
+  double dx = s.x - tx, dy = s.y - ty, dz = s.z - tz;
+  double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+  double g = s.w * recip_nr(fma(0.5, r2, eps));
+  g = r2 > 0.0 ? g : 0.0;
+  ax = fma(g, dx, ax);
+  ay = fma(g, dy, ay);
+  az = fma(g, dz, az);
+}
+
+// The same pair in float32 on panel-relative coordinates: d = base + s.xyz
+// with base = (c_S - c_T) - delta_t.
+__device__ __forceinline__ void pair32(float bx, float by, float bz, const float4 s, float eps, float& ax, float& ay,
+                                       float& az) {
+  float dx = bx + s.x, dy = by + s.y, dz = bz + s.z;
+  float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+  float g = s.w * recip_f32(fmaf(0.5f, r2, eps));
+  g = r2 > 0.0f ? g : 0.0f;
+  ax = fmaf(g, dx, ax);
+  ay = fmaf(g, dy, ay);
+  az = fmaf(g, dz, az);
+}
+
+// ---------------------------------------------------------------------------
+// Source preparation.
+
+// Leaves (bve_disp_update, src/bve_time_step.cpp:69-105, with the forcing
+// copy of src/forcing_funcs.cpp:93-95 and base_pots, src/fmm_funcs_impl.hpp:17-34):
+// stage 0: strength area*vor at proj(proxy); stage s > 0: disp = dt_s v,
+// strength area*(vor + 2 Omega z - 2 Omega z'), z' from proj(x + v dt_s),
+// position proj(proxy + disp).
+__global__ void k_leaf_sources(StepGeom g, int stage, double dt_s, const double* __restrict__ vprev,
+                               const double* __restrict__ x, const double* __restrict__ y,
+                               const double* __restrict__ z, const double* __restrict__ vors,
+                               const double* __restrict__ area, double4* __restrict__ src) {
+  long n = (long)g.leaves * g.q;
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  long pn = (long)g.panels * g.q;
+  long o = (long)g.offset * g.q + i;
+  double px = g.px[o], py = g.px[pn + o], pz = g.px[2 * pn + o];
+  double w;
+  if (stage == 0) {
+    w = area[i] * vors[i];
+  } else {
+    double vx = vprev[i], vy = vprev[n + i], vz = vprev[2 * n + i];
+    double xx = x[i] + vx * dt_s, yy = y[i] + vy * dt_s, zz = z[i] + vz * dt_s;
+    project_to_sphere(xx, yy, zz);
+    double dvor = vors[i] + 2 * g.omega * z[i] - 2 * g.omega * zz;
+    w = area[i] * dvor;
+    px += dt_s * vx;
+    py += dt_s * vy;
+    pz += dt_s * vz;
+  }
+  project_to_sphere(px, py, pz);
+  src[o] = make_double4(px, py, pz, w);
+}
+
+// Non-leaf proxies (bve_disp_interp, src/bve_time_step.cpp:107-160): disp is
+// the BLI of the leaf displacements dt_s v at the proxy point (leaf row and
+// basis precomputed on the host); strength is filled by the upward pass.
+__global__ void k_nonleaf_sources(StepGeom g, int stage, double dt_s, const double* __restrict__ vprev,
+                                  double4* __restrict__ src) {
+  long n = (long)g.offset * g.q;
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  long pn = (long)g.panels * g.q, ln = (long)g.leaves * g.q;
+  double px = g.px[i], py = g.px[pn + i], pz = g.px[2 * pn + i];
+  if (stage > 0) {
+    const double* b = g.il_basis + i * g.q;
+    const long row = (long)g.il_row[i] * g.q;
+    double ax = 0, ay = 0, az = 0;
+    for (int m = 0; m < g.q; m++) {
+      double bm = b[m];
+      ax += (dt_s * vprev[row + m]) * bm;
+      ay += (dt_s * vprev[ln + row + m]) * bm;
+      az += (dt_s * vprev[2 * ln + row + m]) * bm;
+    }
+    px += ax;
+    py += ay;
+    pz += az;
+  }
+  project_to_sphere(px, py, pz);
+  src[i] = make_double4(px, py, pz, 0.0);
+}
+
+// Piecewise API: sources from explicit displacements and strengths
+// (the inputs of bve_vel_interactions).
+__global__ void k_sources_from_disp(StepGeom g, const double* __restrict__ dx, const double* __restrict__ dy,
+                                    const double* __restrict__ dz, const double* __restrict__ s,
+                                    double4* __restrict__ src) {
+  long pn = (long)g.panels * g.q;
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= pn) return;
+  double px = g.px[i] + dx[i], py = g.px[pn + i] + dy[i], pz = g.px[2 * pn + i] + dz[i];
+  project_to_sphere(px, py, pz);
+  src[i] = make_double4(px, py, pz, s[i]);
+}
+
+__global__ void k_leaf_strength(StepGeom g, const double* __restrict__ area, const double* __restrict__ pots,
+                                double4* __restrict__ src) {
+  long n = (long)g.leaves * g.q;
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  src[(long)g.offset * g.q + i].w = area[i] * pots[i];
+}
+
+__global__ void k_copy_strength(StepGeom g, const double4* __restrict__ src, double* __restrict__ out) {
+  long pn = (long)g.panels * g.q;
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= pn) return;
+  out[i] = src[i].w;
+}
+
+// ---------------------------------------------------------------------------
+// Tree passes (upward_pass / downward_pass_3, src/fmm_funcs.cpp:341-392).
+// child_mat[c][k][l] is the BLI basis of parent node l at child c's node k;
+// the uniform quadtree makes it the same matrix for every parent.
+
+// Parent node j = sum_c sum_k child_mat[c][k][j] * child_c node k
+// (child_to_parent, src/fmm_funcs_impl.hpp:36-71).
+__global__ void k_upward_level(StepGeom g, int parent_level, double4* __restrict__ src) {
+  int lo = level_start(parent_level), cnt = 6 << (2 * parent_level);
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= (long)cnt * g.q) return;
+  int p = lo + (int)(i / g.q), j = (int)(i % g.q);
+  int clo = level_start(parent_level + 1) + 4 * (p - lo);
+  double acc = 0;
+  for (int c = 0; c < 4; c++) {
+    const double4* cs = src + (long)(clo + c) * g.q;
+    const double* m = g.child_mat + (long)c * g.q * g.q + j;
+    for (int k = 0; k < g.q; k++) acc = fma(__ldg(m + (long)k * g.q), cs[k].w, acc);
+  }
+  src[(long)p * g.q + j].w = acc;
+}
+
+// Child node k += sum_l child_mat[c][k][l] * parent node l (parent_to_child_3,
+// src/fmm_funcs_impl.hpp:123-172).  At the leaf level the result goes to the
+// stage velocity (child_panel_copy, src/fmm_funcs_impl.hpp:174-188).
+__global__ void k_downward_level(StepGeom g, int child_level, double* __restrict__ tgt,
+                                 double* __restrict__ leaf_out) {
+  int lo = level_start(child_level), cnt = 6 << (2 * child_level);
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= (long)cnt * g.q) return;
+  int ch = lo + (int)(i / g.q), k = (int)(i % g.q);
+  int rel = ch - lo, c = rel & 3;
+  int par = level_start(child_level - 1) + (rel >> 2);
+  long pn = (long)g.panels * g.q;
+  const double* m = g.child_mat + ((long)c * g.q + k) * g.q;
+  const double* t0 = tgt + (long)par * g.q;
+  double a0 = 0, a1 = 0, a2 = 0;
+  for (int l = 0; l < g.q; l++) {
+    double ml = __ldg(m + l);
+    a0 = fma(ml, t0[l], a0);
+    a1 = fma(ml, t0[pn + l], a1);
+    a2 = fma(ml, t0[2 * pn + l], a2);
+  }
+  long o = (long)ch * g.q + k;
+  a0 += tgt[o];
+  a1 += tgt[pn + o];
+  a2 += tgt[2 * pn + o];
+  if (leaf_out != nullptr) {
+    long ln = (long)g.leaves * g.q, lo2 = o - (long)g.offset * g.q;
+    leaf_out[lo2] = a0;
+    leaf_out[ln + lo2] = a1;
+    leaf_out[2 * ln + lo2] = a2;
+  } else {
+    tgt[o] = a0;
+    tgt[pn + o] = a1;
+    tgt[2 * pn + o] = a2;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Interactions (bve_vel_panel_interaction, src/fmm_interactions/bve_vel_impl.hpp:85-122).
+//
+// One warp owns one target panel and walks its sources (CSR list, or all
+// leaves in direct mode).  For q <= 16 the warp's lanes are (split h,
+// target node j): split h takes every S-th source panel, stages its q
+// points in shared memory and every lane of the split runs over them.  For
+// q > 32 each lane owns ceil(q/32) target nodes and the whole warp stages
+// one source panel at a time.  Partial sums of the splits are combined in a
+// fixed order, so the result is deterministic.
+//
+// Direct mode (ALL_LEAVES) splits the source leaves into gridDim.y groups
+// and writes per-group partials that k_reduce_groups sums in order.
+
+template <int Q>
+struct WarpShape {
+  static constexpr int S = Q <= 16 ? 32 / Q : 1;          // source splits per warp
+  static constexpr int TPL = Q <= 32 ? 1 : (Q + 31) / 32;  // target nodes per lane
+  static constexpr int STAGE = (S * Q > Q ? S * Q : Q);    // staged points per warp
+};
+
+template <int Q, bool ALL_LEAVES, bool ACCUM>
+__global__ void __launch_bounds__(32 * kWarpsPerBlock) k_interact64(StepGeom g, const double4* __restrict__ src,
+                                                                    double* __restrict__ out, long out_stride) {
+  using W = WarpShape<Q>;
+  __shared__ double4 stage[kWarpsPerBlock][W::STAGE];
+  __shared__ double red[kWarpsPerBlock][3][32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int tp_first = ALL_LEAVES ? g.offset : 0;
+  const int tp_count = ALL_LEAVES ? g.leaves : g.panels;
+  const int tix = blockIdx.x * kWarpsPerBlock + warp;
+  if (tix >= tp_count) return;
+  const int t = tp_first + tix;
+  const long pn = (long)g.panels * g.q;
+
+  int e0, e1;
+  if (ALL_LEAVES) {
+    int per = (g.leaves + gridDim.y - 1) / gridDim.y;
+    e0 = blockIdx.y * per;
+    e1 = min(g.leaves, e0 + per);
+  } else {
+    e0 = g.tgt_start[t];
+    e1 = g.tgt_start[t + 1];
+  }
+  auto source_of = [&](int e) { return ALL_LEAVES ? g.offset + e : __ldg(g.src_panel + e); };
+
+  if constexpr (Q <= 32) {
+    const int h = lane / Q, j = lane % Q;
+    const bool active = h < W::S;
+    double tx = 0, ty = 0, tz = 0;
+    if (active) {
+      long o = (long)t * Q + j;
+      tx = g.px[o];
+      ty = g.px[pn + o];
+      tz = g.px[2 * pn + o];
+    }
+    double ax = 0, ay = 0, az = 0;
+    for (int e = e0; e < e1; e += W::S) {
+      if (active && e + h < e1) stage[warp][h * Q + j] = src[(long)source_of(e + h) * Q + j];
+      __syncwarp();
+      if (active && e + h < e1) {
+        const double4* sp = &stage[warp][h * Q];
+#pragma unroll
+        for (int k = 0; k < Q; k++) pair64(tx, ty, tz, sp[k], g.eps, ax, ay, az);
+      }
+      __syncwarp();
+    }
+    if (W::S > 1) {
+      red[warp][0][lane] = ax;
+      red[warp][1][lane] = ay;
+      red[warp][2][lane] = az;
+      __syncwarp();
+      if (h == 0) {
+        for (int hh = 1; hh < W::S; hh++) {
+          ax += red[warp][0][hh * Q + j];
+          ay += red[warp][1][hh * Q + j];
+          az += red[warp][2][hh * Q + j];
+        }
+      }
+    }
+    if (h == 0) {
+      double ux = kBiotSavart * (ty * az - tz * ay);
+      double uy = kBiotSavart * (tz * ax - tx * az);
+      double uz = kBiotSavart * (tx * ay - ty * ax);
+      long o = ALL_LEAVES ? (long)blockIdx.y * 3 * out_stride + (long)tix * Q + j : (long)t * Q + j;
+      long s = ALL_LEAVES ? out_stride : pn;
+      if (ACCUM) {
+        out[o] += ux;
+        out[s + o] += uy;
+        out[2 * s + o] += uz;
+      } else {
+        out[o] = ux;
+        out[s + o] = uy;
+        out[2 * s + o] = uz;
+      }
+    }
+  } else {
+    constexpr int TPL = W::TPL;
+    double tx[TPL], ty[TPL], tz[TPL], ax[TPL], ay[TPL], az[TPL];
+#pragma unroll
+    for (int r = 0; r < TPL; r++) {
+      int j = lane + 32 * r;
+      long o = (long)t * Q + (j < Q ? j : 0);
+      tx[r] = g.px[o];
+      ty[r] = g.px[pn + o];
+      tz[r] = g.px[2 * pn + o];
+      ax[r] = ay[r] = az[r] = 0;
+    }
+    for (int e = e0; e < e1; e++) {
+      const long sb = (long)source_of(e) * Q;
+      for (int k = lane; k < Q; k += 32) stage[warp][k] = src[sb + k];
+      __syncwarp();
+      for (int k = 0; k < Q; k++) {
+        const double4 s = stage[warp][k];
+#pragma unroll
+        for (int r = 0; r < TPL; r++) pair64(tx[r], ty[r], tz[r], s, g.eps, ax[r], ay[r], az[r]);
+      }
+      __syncwarp();
+    }
+#pragma unroll
+    for (int r = 0; r < TPL; r++) {
+      int j = lane + 32 * r;
+      if (j >= Q) continue;
+      double ux = kBiotSavart * (ty[r] * az[r] - tz[r] * ay[r]);
+      double uy = kBiotSavart * (tz[r] * ax[r] - tx[r] * az[r]);
+      double uz = kBiotSavart * (tx[r] * ay[r] - ty[r] * ax[r]);
+      long o = ALL_LEAVES ? (long)blockIdx.y * 3 * out_stride + (long)tix * Q + j : (long)t * Q + j;
+      long s = ALL_LEAVES ? out_stride : pn;
+      if (ACCUM) {
+        out[o] += ux;
+        out[s + o] += uy;
+        out[2 * s + o] += uz;
+      } else {
+        out[o] = ux;
+        out[s + o] = uy;
+        out[2 * s + o] = uz;
+      }
+    }
+  }
+}
+
+// Mixed precision: positions relative to panel centres in float, pair
+// arithmetic in float32, per-source-panel partial sums in float32 added into
+// float64 accumulators.
+__global__ void k_pack_mixed(StepGeom g, const double4* __restrict__ src, float4* __restrict__ srcf) {
+  long pn = (long)g.panels * g.q;
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= pn) return;
+  const double* c = g.pd_centre + 4 * (i / g.q);
+  double4 s = src[i];
+  srcf[i] = make_float4((float)(s.x - c[0]), (float)(s.y - c[1]), (float)(s.z - c[2]), (float)s.w);
+}
+
+template <int Q, bool ALL_LEAVES, bool ACCUM>
+__global__ void __launch_bounds__(32 * kWarpsPerBlock) k_interact32(StepGeom g, const float4* __restrict__ srcf,
+                                                                    double* __restrict__ out, long out_stride) {
+  static_assert(Q <= 32, "mixed kernel handles q <= 32");
+  using W = WarpShape<Q>;
+  __shared__ float4 stage[kWarpsPerBlock][W::STAGE];
+  __shared__ double red[kWarpsPerBlock][3][32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int tp_first = ALL_LEAVES ? g.offset : 0;
+  const int tp_count = ALL_LEAVES ? g.leaves : g.panels;
+  const int tix = blockIdx.x * kWarpsPerBlock + warp;
+  if (tix >= tp_count) return;
+  const int t = tp_first + tix;
+  const long pn = (long)g.panels * g.q;
+  int e0, e1;
+  if (ALL_LEAVES) {
+    int per = (g.leaves + gridDim.y - 1) / gridDim.y;
+    e0 = blockIdx.y * per;
+    e1 = min(g.leaves, e0 + per);
+  } else {
+    e0 = g.tgt_start[t];
+    e1 = g.tgt_start[t + 1];
+  }
+  const int h = lane / Q, j = lane % Q;
+  const bool active = h < W::S;
+  double tx = 0, ty = 0, tz = 0;
+  const double* ct = g.pd_centre + 4 * (long)t;
+  const double ctx = ct[0], cty = ct[1], ctz = ct[2];
+  float dtx = 0, dty = 0, dtz = 0;
+  if (active) {
+    long o = (long)t * Q + j;
+    tx = g.px[o];
+    ty = g.px[pn + o];
+    tz = g.px[2 * pn + o];
+    dtx = (float)(tx - ctx);
+    dty = (float)(ty - cty);
+    dtz = (float)(tz - ctz);
+  }
+  const float eps = (float)g.eps;
+  double ax = 0, ay = 0, az = 0;
+  for (int e = e0; e < e1; e += W::S) {
+    int sp = 0;
+    if (active && e + h < e1) {
+      sp = ALL_LEAVES ? g.offset + e + h : __ldg(g.src_panel + e + h);
+      stage[warp][h * Q + j] = srcf[(long)sp * Q + j];
+    }
+    __syncwarp();
+    if (active && e + h < e1) {
+      const double* cs = g.pd_centre + 4 * (long)sp;
+      float bx = (float)(cs[0] - ctx) - dtx, by = (float)(cs[1] - cty) - dty, bz = (float)(cs[2] - ctz) - dtz;
+      float fx = 0.f, fy = 0.f, fz = 0.f;
+      const float4* sb = &stage[warp][h * Q];
+#pragma unroll
+      for (int k = 0; k < Q; k++) pair32(bx, by, bz, sb[k], eps, fx, fy, fz);
+      ax += fx;
+      ay += fy;
+      az += fz;
+    }
+    __syncwarp();
+  }
+  if (W::S > 1) {
+    red[warp][0][lane] = ax;
+    red[warp][1][lane] = ay;
+    red[warp][2][lane] = az;
+    __syncwarp();
+    if (h == 0)
+      for (int hh = 1; hh < W::S; hh++) {
+        ax += red[warp][0][hh * Q + j];
+        ay += red[warp][1][hh * Q + j];
+        az += red[warp][2][hh * Q + j];
+      }
+  }
+  if (h == 0) {
+    double ux = kBiotSavart * (ty * az - tz * ay);
+    double uy = kBiotSavart * (tz * ax - tx * az);
+    double uz = kBiotSavart * (tx * ay - ty * ax);
+    long o = ALL_LEAVES ? (long)blockIdx.y * 3 * out_stride + (long)tix * Q + j : (long)t * Q + j;
+    long s = ALL_LEAVES ? out_stride : pn;
+    if (ACCUM) {
+      out[o] += ux;
+      out[s + o] += uy;
+      out[2 * s + o] += uz;
+    } else {
+      out[o] = ux;
+      out[s + o] = uy;
+      out[2 * s + o] = uz;
+    }
+  }
+}
+
+// Sum of per-group partials (group gi at partial + gi * gstride) in group order.
+__global__ void k_reduce_groups(const double* __restrict__ partial, int groups, long n, long gstride,
+                                double* __restrict__ out) {
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double a = 0;
+  for (int gi = 0; gi < groups; gi++) a += partial[(long)gi * gstride + i];
+  out[i] = a;
+}
+
+// ---------------------------------------------------------------------------
+// Departure points and remap.
+//
+// bve_find_departure_points (src/bve_time_step.cpp:172-309): backward RK4
+// with k1 = v3 at x, k2 = v2 at proj(x - dt/2 k1), k3 = v1 at
+// proj(x - dt/2 k2), k4 = v0 at proj(x - dt k3), and the re-projected
+// combination.  bve_departure_to_target (src/bve_time_step.cpp:15-67):
+// new vorticity = BLI(vor)(dep) + 2 Omega dep_z - 2 Omega z, tracers by BLI.
+// mode bit 1: compute departure points (else read dep); bit 2: remap (else
+// write dep).
+
+template <int D>
+struct Basis {
+  double fx[D + 1], fe[D + 1];
+  long row;  // (leaf - offset) * q
+};
+
+template <int D>
+__device__ __forceinline__ void locate_basis(const StepGeom& g, const BliTable& tab, double x, double y, double z,
+                                             Basis<D>& b, unsigned& err) {
+  double xi, eta;
+  Bounds bd;
+  int leaf = locate_leaf(x, y, z, g.levels, xi, eta, bd, err);
+  bli_1d(xi, kPi / 4.0 * bd.min_xi, kPi / 4.0 * bd.max_xi, D, tab.cosv, tab.w, b.fx, err);
+  bli_1d(eta, kPi / 4.0 * bd.min_eta, kPi / 4.0 * bd.max_eta, D, tab.cosv, tab.w, b.fe, err);
+  b.row = (long)(leaf - g.offset) * g.q;
+}
+
+// sum_m field[row + m] * fx[i] fe[j] with m = i (D+1) + j, in m order.
+template <int D>
+__device__ __forceinline__ double gather(const Basis<D>& b, const double* __restrict__ f, long stride = 1,
+                                         long base = 0) {
+  double acc = 0;
+  int m = 0;
+#pragma unroll
+  for (int i = 0; i <= D; i++)
+#pragma unroll
+    for (int j = 0; j <= D; j++, m++) acc += f[(b.row + m) * stride + base] * (b.fx[i] * b.fe[j]);
+  return acc;
+}
+
+template <int D>
+__device__ __forceinline__ void gather3(const Basis<D>& b, const double* __restrict__ v, long n, double& a,
+                                        double& c, double& e) {
+  a = 0;
+  c = 0;
+  e = 0;
+  int m = 0;
+#pragma unroll
+  for (int i = 0; i <= D; i++)
+#pragma unroll
+    for (int j = 0; j <= D; j++, m++) {
+      double bm = b.fx[i] * b.fe[j];
+      a += v[b.row + m] * bm;
+      c += v[n + b.row + m] * bm;
+      e += v[2 * n + b.row + m] * bm;
+    }
+}
+
+template <int D>
+__global__ void k_depart_remap(StepGeom g, BliTable tab, const double* __restrict__ x, const double* __restrict__ y,
+                               const double* __restrict__ z, const double* __restrict__ v0,
+                               const double* __restrict__ v1, const double* __restrict__ v2,
+                               const double* __restrict__ v3, double dt, double* __restrict__ dep,
+                               const double* __restrict__ vors, const double* __restrict__ tracers, int T,
+                               double* __restrict__ new_vors, double* __restrict__ new_tracers, int mode) {
+  const long n = (long)g.leaves * g.q;
+  const long o = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (o >= n) return;
+  unsigned err = 0;
+  Basis<D> b;
+  double dx, dy, dz;
+  if (mode & 1) {
+    const double x0 = x[o], y0 = y[o], z0 = z[o];
+    const double k1x = v3[o], k1y = v3[n + o], k1z = v3[2 * n + o];
+    double xx = x0 - 0.5 * dt * k1x, yy = y0 - 0.5 * dt * k1y, zz = z0 - 0.5 * dt * k1z;
+    project_to_sphere(xx, yy, zz);
+    locate_basis<D>(g, tab, xx, yy, zz, b, err);
+    double k2x, k2y, k2z;
+    gather3<D>(b, v2, n, k2x, k2y, k2z);
+    xx = x0 - 0.5 * dt * k2x, yy = y0 - 0.5 * dt * k2y, zz = z0 - 0.5 * dt * k2z;
+    project_to_sphere(xx, yy, zz);
+    locate_basis<D>(g, tab, xx, yy, zz, b, err);
+    double k3x, k3y, k3z;
+    gather3<D>(b, v1, n, k3x, k3y, k3z);
+    xx = x0 - dt * k3x, yy = y0 - dt * k3y, zz = z0 - dt * k3z;
+    project_to_sphere(xx, yy, zz);
+    locate_basis<D>(g, tab, xx, yy, zz, b, err);
+    double k4x, k4y, k4z;
+    gather3<D>(b, v0, n, k4x, k4y, k4z);
+    xx = x0 - 1.0 / 6.0 * dt * k1x, yy = y0 - 1.0 / 6.0 * dt * k1y, zz = z0 - 1.0 / 6.0 * dt * k1z;
+    project_to_sphere(xx, yy, zz);
+    xx -= -1.0 / 3.0 * dt * k2x, yy -= -1.0 / 3.0 * dt * k2y, zz -= -1.0 / 3.0 * dt * k2z;
+    project_to_sphere(xx, yy, zz);
+    xx -= -1.0 / 3.0 * dt * k3x, yy -= -1.0 / 3.0 * dt * k3y, zz -= -1.0 / 3.0 * dt * k3z;
+    project_to_sphere(xx, yy, zz);
+    xx -= -1.0 / 6.0 * dt * k4x, yy -= -1.0 / 6.0 * dt * k4y, zz -= -1.0 / 6.0 * dt * k4z;
+    project_to_sphere(xx, yy, zz);
+    dx = xx;
+    dy = yy;
+    dz = zz;
+    if (!(mode & 2)) {
+      dep[o] = dx;
+      dep[n + o] = dy;
+      dep[2 * n + o] = dz;
+    }
+  } else {
+    dx = dep[o];
+    dy = dep[n + o];
+    dz = dep[2 * n + o];
+  }
+  if (mode & 2) {
+    locate_basis<D>(g, tab, dx, dy, dz, b, err);
+    double vor = gather<D>(b, vors);
+    for (int k = 0; k < T; k++) new_tracers[o * T + k] = gather<D>(b, tracers, T, k);
+    vor += 2 * g.omega * dz;
+    new_vors[o] = vor - 2 * g.omega * z[o];
+  }
+  flag(g.err, err);
+}
+
+// ---------------------------------------------------------------------------
+// Stand-alone direct sums over arbitrary points: blocks own 128 targets and
+// stage 128 sources at a time in shared memory; gridDim.y source groups write
+// partials reduced by k_reduce_groups.
+
+constexpr int kDirectThreads = 128;
+
+__global__ void __launch_bounds__(kDirectThreads)
+    k_direct_bve64(long nt, const double* __restrict__ tx, const double* __restrict__ ty,
+                   const double* __restrict__ tz, long ns, const double* __restrict__ sx,
+                   const double* __restrict__ sy, const double* __restrict__ sz, const double* __restrict__ sw,
+                   double eps, double* __restrict__ partial) {
+  __shared__ double4 tile[kDirectThreads];
+  long i = blockIdx.x * (long)kDirectThreads + threadIdx.x;
+  double x = 0, y = 0, z = 0;
+  if (i < nt) {
+    x = tx[i];
+    y = ty[i];
+    z = tz[i];
+  }
+  long per = (ns + gridDim.y - 1) / gridDim.y;
+  long s0 = blockIdx.y * per, s1 = min(ns, s0 + per);
+  double ax = 0, ay = 0, az = 0;
+  for (long b = s0; b < s1; b += kDirectThreads) {
+    long k = b + threadIdx.x;
+    tile[threadIdx.x] = k < s1 ? make_double4(sx[k], sy[k], sz[k], sw[k]) : make_double4(0, 0, 0, 0);
+    __syncthreads();
+    int cnt = (int)min((long)kDirectThreads, s1 - b);
+    for (int m = 0; m < cnt; m++) pair64(x, y, z, tile[m], eps, ax, ay, az);
+    __syncthreads();
+  }
+  if (i < nt) {
+    long o = (long)blockIdx.y * 3 * nt + i;
+    partial[o] = kBiotSavart * (y * az - z * ay);
+    partial[nt + o] = kBiotSavart * (z * ax - x * az);
+    partial[2 * nt + o] = kBiotSavart * (x * ay - y * ax);
+  }
+}
+
+// Mixed: each block measures both tiles relative to their first point (in
+// float64), so float32 carries only the small in-tile offsets.
+__global__ void __launch_bounds__(kDirectThreads)
+    k_direct_bve32(long nt, const double* __restrict__ tx, const double* __restrict__ ty,
+                   const double* __restrict__ tz, long ns, const double* __restrict__ sx,
+                   const double* __restrict__ sy, const double* __restrict__ sz, const double* __restrict__ sw,
+                   double eps, double* __restrict__ partial) {
+  __shared__ float4 tile[kDirectThreads];
+  long i = blockIdx.x * (long)kDirectThreads + threadIdx.x;
+  long i0 = blockIdx.x * (long)kDirectThreads;
+  const double tcx = tx[i0], tcy = ty[i0], tcz = tz[i0];
+  double x = tcx, y = tcy, z = tcz;
+  if (i < nt) {
+    x = tx[i];
+    y = ty[i];
+    z = tz[i];
+  }
+  const float dtx = (float)(x - tcx), dty = (float)(y - tcy), dtz = (float)(z - tcz);
+  long per = (ns + gridDim.y - 1) / gridDim.y;
+  long s0 = blockIdx.y * per, s1 = min(ns, s0 + per);
+  double ax = 0, ay = 0, az = 0;
+  const float feps = (float)eps;
+  for (long b = s0; b < s1; b += kDirectThreads) {
+    const double scx = sx[b], scy = sy[b], scz = sz[b];
+    long k = b + threadIdx.x;
+    tile[threadIdx.x] = k < s1 ? make_float4((float)(sx[k] - scx), (float)(sy[k] - scy), (float)(sz[k] - scz),
+                                             (float)sw[k])
+                               : make_float4(0, 0, 0, 0);
+    __syncthreads();
+    float bx = (float)(scx - tcx) - dtx, by = (float)(scy - tcy) - dty, bz = (float)(scz - tcz) - dtz;
+    float fx = 0, fy = 0, fz = 0;
+    int cnt = (int)min((long)kDirectThreads, s1 - b);
+    for (int m = 0; m < cnt; m++) pair32(bx, by, bz, tile[m], feps, fx, fy, fz);
+    ax += fx;
+    ay += fy;
+    az += fz;
+    __syncthreads();
+  }
+  if (i < nt) {
+    long o = (long)blockIdx.y * 3 * nt + i;
+    partial[o] = kBiotSavart * (y * az - z * ay);
+    partial[nt + o] = kBiotSavart * (z * ax - x * az);
+    partial[2 * nt + o] = kBiotSavart * (x * ay - y * ax);
+  }
+}
+
+// inv_lap (src/direct_sum_impl.hpp:20-27): soln_i += sum_{j != i}
+// -1/(4 pi) log(1 - x_i.x_j) area_j pots_j.
+__global__ void __launch_bounds__(kDirectThreads)
+    k_inv_lap(long n, const double* __restrict__ x, const double* __restrict__ y, const double* __restrict__ z,
+              const double* __restrict__ area, const double* __restrict__ pots, double* __restrict__ soln) {
+  __shared__ double4 tile[kDirectThreads];
+  long i = blockIdx.x * (long)kDirectThreads + threadIdx.x;
+  double xi = 0, yi = 0, zi = 0;
+  if (i < n) {
+    xi = x[i];
+    yi = y[i];
+    zi = z[i];
+  }
+  double acc = 0;
+  for (long b = 0; b < n; b += kDirectThreads) {
+    long k = b + threadIdx.x;
+    tile[threadIdx.x] = k < n ? make_double4(x[k], y[k], z[k], area[k] * pots[k]) : make_double4(0, 0, 0, 0);
+    __syncthreads();
+    int cnt = (int)min((long)kDirectThreads, n - b);
+    for (int m = 0; m < cnt; m++) {
+      if (b + m == i) continue;
+      double4 s = tile[m];
+      double dp = xi * s.x + yi * s.y + zi * s.z;
+      acc += -0.07957747154594767 * log(1 - dp) * s.w;
+    }
+    __syncthreads();
+  }
+  if (i < n) soln[i] += acc;
+}
+
+inline unsigned blocks_for(long n, int t) { return (unsigned)((n + t - 1) / t); }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Launch wrappers.
+
+#define SB_LAUNCH(kernel, grid, block, shmem, st, ...)      \
+  do {                                                     \
+    kernel<<<grid, block, shmem, st>>>(__VA_ARGS__);       \
+    launch_counter()++;                                    \
+  } while (0)
+
+void launch_leaf_sources(const StepGeom& g, int stage, double dt_s, const double* vprev, const double* x,
+                         const double* y, const double* z, const double* vors, const double* area, double4* src,
+                         cudaStream_t st) {
+  long n = (long)g.leaves * g.q;
+  SB_LAUNCH(k_leaf_sources, blocks_for(n, 256), 256, 0, st, g, stage, dt_s, vprev, x, y, z, vors, area, src);
+}
+
+void launch_nonleaf_sources(const StepGeom& g, int stage, double dt_s, const double* vprev, double4* src,
+                            cudaStream_t st) {
+  long n = (long)g.offset * g.q;
+  if (n == 0) return;
+  SB_LAUNCH(k_nonleaf_sources, blocks_for(n, 256), 256, 0, st, g, stage, dt_s, vprev, src);
+}
+
+void launch_sources_from_disp(const StepGeom& g, const double* dx, const double* dy, const double* dz,
+                              const double* s, double4* src, cudaStream_t st) {
+  long n = (long)g.panels * g.q;
+  SB_LAUNCH(k_sources_from_disp, blocks_for(n, 256), 256, 0, st, g, dx, dy, dz, s, src);
+}
+
+void launch_leaf_strength(const StepGeom& g, const double* area, const double* pots, double4* src, cudaStream_t st) {
+  long n = (long)g.leaves * g.q;
+  SB_LAUNCH(k_leaf_strength, blocks_for(n, 256), 256, 0, st, g, area, pots, src);
+}
+
+void launch_copy_strength(const StepGeom& g, const double4* src, double* out, cudaStream_t st) {
+  long n = (long)g.panels * g.q;
+  SB_LAUNCH(k_copy_strength, blocks_for(n, 256), 256, 0, st, g, src, out);
+}
+
+void launch_upward_level(const StepGeom& g, int parent_level, double4* src, cudaStream_t st) {
+  long n = (long)(6 << (2 * parent_level)) * g.q;
+  SB_LAUNCH(k_upward_level, blocks_for(n, 128), 128, 0, st, g, parent_level, src);
+}
+
+void launch_downward_level(const StepGeom& g, int child_level, double* tgt, double* leaf_out, cudaStream_t st) {
+  long n = (long)(6 << (2 * child_level)) * g.q;
+  SB_LAUNCH(k_downward_level, blocks_for(n, 128), 128, 0, st, g, child_level, tgt, leaf_out);
+}
+
+namespace {
+template <int Q>
+void interact_q(const StepGeom& g, int precision, const double4* src, double* out, bool accumulate, bool all_leaves,
+                int groups, long out_stride, cudaStream_t st, bool pack = true) {
+  int tp = all_leaves ? g.leaves : g.panels;
+  dim3 grid(blocks_for(tp, kWarpsPerBlock), all_leaves ? groups : 1);
+  if (precision == SBSLPM_MIXED) {
+    if constexpr (Q <= 32) {
+      long pn = (long)g.panels * g.q;
+      if (pack) SB_LAUNCH(k_pack_mixed, blocks_for(pn, 256), 256, 0, st, g, src, g.srcf);
+      if (all_leaves)
+        SB_LAUNCH((k_interact32<Q, true, false>), grid, 32 * kWarpsPerBlock, 0, st, g, g.srcf, out, out_stride);
+      else if (accumulate)
+        SB_LAUNCH((k_interact32<Q, false, true>), grid, 32 * kWarpsPerBlock, 0, st, g, g.srcf, out, out_stride);
+      else
+        SB_LAUNCH((k_interact32<Q, false, false>), grid, 32 * kWarpsPerBlock, 0, st, g, g.srcf, out, out_stride);
+      return;
+    }
+  }
+  if (all_leaves)
+    SB_LAUNCH((k_interact64<Q, true, false>), grid, 32 * kWarpsPerBlock, 0, st, g, src, out, out_stride);
+  else if (accumulate)
+    SB_LAUNCH((k_interact64<Q, false, true>), grid, 32 * kWarpsPerBlock, 0, st, g, src, out, out_stride);
+  else
+    SB_LAUNCH((k_interact64<Q, false, false>), grid, 32 * kWarpsPerBlock, 0, st, g, src, out, out_stride);
+}
+
+void interact_dispatch(const StepGeom& g, int precision, const double4* src, double* out, bool accumulate,
+                       bool all_leaves, int groups, long out_stride, cudaStream_t st, bool pack = true) {
+#define SB_IQ(Q) \
+  case Q: interact_q<Q>(g, precision, src, out, accumulate, all_leaves, groups, out_stride, st, pack); break;
+  switch (g.q) {
+    SB_IQ(1) SB_IQ(4) SB_IQ(9) SB_IQ(16) SB_IQ(25) SB_IQ(36) SB_IQ(49) SB_IQ(64) SB_IQ(81) SB_IQ(100)
+    default: interact_q<121>(g, precision, src, out, accumulate, all_leaves, groups, out_stride, st, pack); break;
+  }
+#undef SB_IQ
+}
+
+// Independent FMA chains (8 per thread) so the pipe, not latency, limits throughput.
+__global__ void k_fma_probe32(int iters, float* out) {
+  float a[8];
+  for (int k = 0; k < 8; k++) a[k] = threadIdx.x * 1e-7f + k;
+  const float m = 0.999999f, c = 1e-7f;
+  for (int i = 0; i < iters; i++)
+#pragma unroll
+    for (int k = 0; k < 8; k++) a[k] = fmaf(a[k], m, c);
+  float s = 0;
+  for (int k = 0; k < 8; k++) s += a[k];
+  if (s == 12345.678f) out[0] = s;  // keeps the chains live
+}
+__global__ void k_fma_probe64(int iters, double* out) {
+  double a[8];
+  for (int k = 0; k < 8; k++) a[k] = threadIdx.x * 1e-7 + k;
+  const double m = 0.999999, c = 1e-7;
+  for (int i = 0; i < iters; i++)
+#pragma unroll
+    for (int k = 0; k < 8; k++) a[k] = fma(a[k], m, c);
+  double s = 0;
+  for (int k = 0; k < 8; k++) s += a[k];
+  if (s == 12345.678) out[0] = s;
+}
+}  // namespace
+
+void launch_interactions(const StepGeom& g, int precision, const double4* src, double* tgt, bool accumulate,
+                         cudaStream_t st) {
+  interact_dispatch(g, precision, src, tgt, accumulate, false, 1, 0, st);
+}
+
+void launch_interactions_only(const StepGeom& g, int precision, const double4* src, double* tgt, cudaStream_t st) {
+  interact_dispatch(g, precision, src, tgt, false, false, 1, 0, st, false);
+}
+
+void launch_pack_mixed(const StepGeom& g, const double4* src, cudaStream_t st) {
+  long pn = (long)g.panels * g.q;
+  SB_LAUNCH(k_pack_mixed, blocks_for(pn, 256), 256, 0, st, g, src, g.srcf);
+}
+
+void launch_fma_probe(int kind, int blocks, int iters, float* out32, double* out64, cudaStream_t st) {
+  if (kind == 0)
+    SB_LAUNCH(k_fma_probe32, blocks, 256, 0, st, iters, out32);
+  else
+    SB_LAUNCH(k_fma_probe64, blocks, 256, 0, st, iters, out64);
+}
+
+void launch_direct_leaves(const StepGeom& g, int precision, const double4* src, double* vout, double* partial,
+                          int groups, cudaStream_t st) {
+  long n = (long)g.leaves * g.q;
+  interact_dispatch(g, precision, src, partial, false, true, groups, n, st);
+  SB_LAUNCH(k_reduce_groups, blocks_for(3 * n, 256), 256, 0, st, partial, groups, 3 * n, 3 * n, vout);
+}
+
+void launch_depart_remap(const StepGeom& g, const BliTable* tab, const double* x, const double* y, const double* z,
+                         const double* v0, const double* v1, const double* v2, const double* v3, double dt,
+                         double* dep, const double* vors, const double* tracers, int T, double* new_vors,
+                         double* new_tracers, int mode, cudaStream_t st) {
+  long n = (long)g.leaves * g.q;
+  unsigned grid = blocks_for(n, 128);
+#define SB_DR(D)                                                                                                   \
+  case D:                                                                                                          \
+    SB_LAUNCH(k_depart_remap<D>, grid, 128, 0, st, g, *tab, x, y, z, v0, v1, v2, v3, dt, dep, vors, tracers, T,   \
+              new_vors, new_tracers, mode);                                                                        \
+    break;
+  switch (g.degree) {
+    SB_DR(0) SB_DR(1) SB_DR(2) SB_DR(3) SB_DR(4) SB_DR(5) SB_DR(6) SB_DR(7) SB_DR(8) SB_DR(9) SB_DR(10)
+  }
+#undef SB_DR
+}
+
+int direct_groups(long nt, long ns) {
+  // enough blocks to fill 148 SMs a few times over, without tiny groups
+  long tblocks = (nt + kDirectThreads - 1) / kDirectThreads;
+  long want = (4L * 148 * 8 + tblocks - 1) / tblocks;
+  long maxg = (ns + 1023) / 1024;
+  long gsel = want < maxg ? want : maxg;
+  return (int)(gsel < 1 ? 1 : (gsel > 64 ? 64 : gsel));
+}
+
+void launch_direct_bve(long nt, const double* tx, const double* ty, const double* tz, long ns, const double* sx,
+                       const double* sy, const double* sz, const double* s, double eps, int precision, double* partial,
+                       int groups, double* ux, double* uy, double* uz, cudaStream_t st) {
+  dim3 grid(blocks_for(nt, kDirectThreads), groups);
+  if (precision == SBSLPM_MIXED)
+    SB_LAUNCH(k_direct_bve32, grid, kDirectThreads, 0, st, nt, tx, ty, tz, ns, sx, sy, sz, s, eps, partial);
+  else
+    SB_LAUNCH(k_direct_bve64, grid, kDirectThreads, 0, st, nt, tx, ty, tz, ns, sx, sy, sz, s, eps, partial);
+  // reduce into the three output arrays (they need not be contiguous)
+  double* outs[3] = {ux, uy, uz};
+  for (int c = 0; c < 3; c++)
+    SB_LAUNCH(k_reduce_groups, blocks_for(nt, 256), 256, 0, st, partial + (long)c * nt, groups, nt, 3 * nt, outs[c]);
+}
+
+void launch_inv_lap(long n, const double* x, const double* y, const double* z, const double* area,
+                    const double* pots, double* soln, cudaStream_t st) {
+  SB_LAUNCH(k_inv_lap, blocks_for(n, kDirectThreads), kDirectThreads, 0, st, n, x, y, z, area, pots, soln);
+}
+
+}  // namespace sbslpm

@@ -1,0 +1,71 @@
+// Device kernels of the BVE step (sm_100a).  Launch wrappers are in
+// bve_kernels.cu; the step orchestration is in context.cu.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "geometry.cuh"
+
+namespace sbslpm {
+
+// Static per-problem constants used by the BLI code on the device.
+struct BliTable {
+  double cosv[kMaxDegree + 1];  // cos(pi*i/d), computed on the host with libm
+  double w[kMaxDegree + 1];     // barycentric weights of Chebyshev extrema
+};
+
+// Everything the stage kernels need, passed by value.
+struct StepGeom {
+  int levels, degree, q, panels, leaves, offset;  // offset = panels - leaves
+  double eps, omega;
+  const double* px;           // proxy positions [panels*q] x, y, z blocks (3 * panels*q)
+  const int* tgt_start;       // [panels+1] CSR of the interaction list by target
+  const int* src_panel;       // [interactions] source panel, list order within a target
+  const int* il_row;          // [(panels-leaves)*q] leaf row interpolating a non-leaf proxy
+  const double* il_basis;     // [(panels-leaves)*q*q] BLI basis at that leaf
+  const double* child_mat;    // [4][q][q]: basis of parent node l at child c's node k
+  const double* pd_centre;    // mixed: panel centres [panels][4] (double)
+  float4* srcf;               // mixed: packed sources [panels*q] (workspace)
+  unsigned* err;              // device error word
+};
+
+// Launch wrappers (stream-ordered).
+void launch_leaf_sources(const StepGeom& g, int stage, double dt_s, const double* vprev, const double* x,
+                         const double* y, const double* z, const double* vors, const double* area, double4* src,
+                         cudaStream_t st);
+void launch_nonleaf_sources(const StepGeom& g, int stage, double dt_s, const double* vprev, double4* src,
+                            cudaStream_t st);
+void launch_upward_level(const StepGeom& g, int parent_level, double4* src, cudaStream_t st);
+void launch_interactions(const StepGeom& g, int precision, const double4* src, double* tgt, bool accumulate,
+                         cudaStream_t st);
+void launch_downward_level(const StepGeom& g, int child_level, double* tgt, double* leaf_out, cudaStream_t st);
+void launch_direct_leaves(const StepGeom& g, int precision, const double4* src, double* vout, double* partial,
+                          int groups, cudaStream_t st);
+void launch_depart_remap(const StepGeom& g, const BliTable* tab, const double* x, const double* y, const double* z,
+                         const double* v0, const double* v1, const double* v2, const double* v3, double dt,
+                         double* dep, const double* vors, const double* tracers, int tracer_count, double* new_vors,
+                         double* new_tracers, int mode, cudaStream_t st);
+// Raw-array helpers for the piecewise API.
+void launch_sources_from_disp(const StepGeom& g, const double* dx, const double* dy, const double* dz,
+                              const double* source, double4* src, cudaStream_t st);
+void launch_leaf_strength(const StepGeom& g, const double* area, const double* pots, double4* src, cudaStream_t st);
+void launch_copy_strength(const StepGeom& g, const double4* src, double* out, cudaStream_t st);
+
+// Stand-alone direct sums (no tree).
+int direct_groups(long n_targets, long n_sources);
+void launch_direct_bve(long nt, const double* tx, const double* ty, const double* tz, long ns, const double* sx,
+                       const double* sy, const double* sz, const double* s, double eps, int precision, double* partial,
+                       int groups, double* ux, double* uy, double* uz, cudaStream_t st);
+void launch_inv_lap(long n, const double* x, const double* y, const double* z, const double* area,
+                    const double* pots, double* soln, cudaStream_t st);
+
+// The interaction kernel alone (no mixed-precision packing), for timing.
+void launch_interactions_only(const StepGeom& g, int precision, const double4* src, double* tgt, cudaStream_t st);
+void launch_pack_mixed(const StepGeom& g, const double4* src, cudaStream_t st);
+// FMA-chain throughput probe: kind 0 float32, 1 float64; iters per thread.
+void launch_fma_probe(int kind, int blocks, int iters, float* out32, double* out64, cudaStream_t st);
+
+// Counts every kernel launched through the wrappers above.
+long& launch_counter();
+
+}  // namespace sbslpm

@@ -1,0 +1,706 @@
+// C ABI of the BVE hot path: context set-up (tree, interaction list and the
+// static geometry precomputed on the host and uploaded once), the RK4 step
+// orchestration on one CUDA stream, CUDA-graph replay of whole steps, and the
+// piecewise entry points that mirror the reference's FMM functions.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "bve_kernels.cuh"
+#include "geometry.cuh"
+#include "internal.hpp"
+
+using namespace sbslpm;
+
+namespace sbslpm {
+namespace {
+thread_local std::string g_last_error;
+}
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace sbslpm
+
+#define SB_CUDA(call)                                                                      \
+  do {                                                                                     \
+    cudaError_t e_ = (call);                                                               \
+    if (e_ != cudaSuccess) {                                                               \
+      set_last_error(std::string(#call) + ": " + cudaGetErrorString(e_));                 \
+      return SBSLPM_ERR_CUDA;                                                              \
+    }                                                                                      \
+  } while (0)
+
+struct GraphKey {
+  const void* p[9];
+  bool operator==(const GraphKey& o) const { return std::memcmp(p, o.p, sizeof p) == 0; }
+};
+
+struct sbslpm_ctx {
+  sbslpm_config cfg{};
+  int L = 0, d = 0, q = 0, P = 0, A = 0, off = 0;
+  long I = 0;
+  std::vector<sbslpm_panel> panels;
+  std::vector<sbslpm_interact_pair> list;
+  cudaStream_t user_stream = nullptr, own_stream = nullptr;
+  bool user_stream_set = false;  // set_stream(NULL) selects the legacy default stream
+  // static device data
+  double *px = nullptr, *il_basis = nullptr, *child_mat = nullptr, *centre = nullptr;
+  int *tgt_start = nullptr, *src_panel = nullptr, *il_row = nullptr;
+  // workspace
+  double4* src = nullptr;
+  float4* srcf = nullptr;
+  double *tgt = nullptr, *vbuf = nullptr, *partial = nullptr, *newvor = nullptr, *newtr = nullptr, *dep = nullptr;
+  int groups = 1;
+  unsigned* err = nullptr;
+  unsigned* h_err = nullptr;
+  BliTable tab{};
+  StepGeom geom{};
+  cudaGraphExec_t graph = nullptr;
+  GraphKey graph_key{};
+  long launches_per_step = 0;
+
+  cudaStream_t stream() const { return user_stream_set ? user_stream : own_stream; }
+};
+
+namespace {
+
+template <class T>
+sbslpm_status dalloc(T** p, size_t count) {
+  *p = nullptr;
+  if (count == 0) return SBSLPM_OK;
+  SB_CUDA(cudaMalloc(reinterpret_cast<void**>(p), sizeof(T) * count));
+  return SBSLPM_OK;
+}
+
+template <class T>
+sbslpm_status upload(T** p, const std::vector<T>& h) {
+  sbslpm_status s = dalloc(p, h.size());
+  if (s != SBSLPM_OK) return s;
+  if (!h.empty()) SB_CUDA(cudaMemcpy(*p, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
+  return SBSLPM_OK;
+}
+
+#define SB_TRY(expr)                           \
+  do {                                         \
+    sbslpm_status s_ = (expr);                 \
+    if (s_ != SBSLPM_OK) return s_;            \
+  } while (0)
+
+sbslpm_status validate(const sbslpm_config& c) {
+  if (c.levels < 1 || c.levels > 12) return set_last_error("levels must be in 1..12"), SBSLPM_ERR_CONFIG;
+  if (c.interp_degree < 0 || c.interp_degree > kMaxDegree)
+    return set_last_error("interp_degree must be in 0..10"), SBSLPM_ERR_CONFIG;
+  if (c.tracer_count < 0) return set_last_error("tracer_count must be >= 0"), SBSLPM_ERR_CONFIG;
+  if (c.velocity != SBSLPM_VEL_FMM && c.velocity != SBSLPM_VEL_DIRECT)
+    return set_last_error("velocity must be SBSLPM_VEL_FMM or SBSLPM_VEL_DIRECT"), SBSLPM_ERR_CONFIG;
+  if (c.precision != SBSLPM_FP64 && c.precision != SBSLPM_MIXED)
+    return set_last_error("precision must be SBSLPM_FP64 or SBSLPM_MIXED"), SBSLPM_ERR_CONFIG;
+  if (c.precision == SBSLPM_MIXED && (c.interp_degree + 1) * (c.interp_degree + 1) > 32)
+    return set_last_error("mixed precision pair kernels support interp_degree <= 4"), SBSLPM_ERR_CONFIG;
+  if (!(c.kernel_eps >= 0) || !std::isfinite(c.dt) || !std::isfinite(c.omega))
+    return set_last_error("kernel_eps, dt and omega must be finite (kernel_eps >= 0)"), SBSLPM_ERR_CONFIG;
+  return SBSLPM_OK;
+}
+
+// Host precomputation of everything that does not change during a run.
+sbslpm_status precompute(sbslpm_ctx* c) {
+  const int q = c->q, P = c->P, off = c->off, d = c->d;
+  std::vector<double> interp;
+  build_interp(d, false, interp);
+
+  // proxy positions, exactly as the reference's interaction kernel places them
+  std::vector<double> px((size_t)3 * P * q);
+  const size_t pn = (size_t)P * q;
+  for (int p = 0; p < P; p++)
+    for (int j = 0; j < q; j++) {
+      double xyz[3];
+      proxy_point(c->panels[p], interp.data(), j, xyz);
+      px[(size_t)p * q + j] = xyz[0];
+      px[pn + (size_t)p * q + j] = xyz[1];
+      px[2 * pn + (size_t)p * q + j] = xyz[2];
+    }
+  SB_TRY(upload(&c->px, px));
+
+  // panel centres for the mixed-precision relative coordinates
+  std::vector<double> centre((size_t)4 * P, 0.0);
+  for (int p = 0; p < P; p++) {
+    const sbslpm_panel& pp = c->panels[p];
+    double xyz[3];
+    xyz_from_xieta(kPi / 4.0 * 0.5 * (pp.min_xi + pp.max_xi), kPi / 4.0 * 0.5 * (pp.min_eta + pp.max_eta), pp.face,
+                   xyz);
+    for (int k = 0; k < 3; k++) centre[4 * (size_t)p + k] = xyz[k];
+  }
+  SB_TRY(upload(&c->centre, centre));
+
+  // displacement interpolation at non-leaf proxies (bve_disp_interp,
+  // src/bve_time_step.cpp:131-159): located leaf row and BLI basis
+  std::vector<int> il_row((size_t)off * q);
+  std::vector<double> il_basis((size_t)off * q * q);
+  unsigned err = 0;
+  for (int i = 0; i < off; i++) {
+    const sbslpm_panel& p = c->panels[i];
+    double xo = kPi / 4 * 0.5 * (p.max_xi + p.min_xi), xs = kPi / 4 * 0.5 * (p.max_xi - p.min_xi);
+    double eo = kPi / 4 * 0.5 * (p.max_eta + p.min_eta), es = kPi / 4 * 0.5 * (p.max_eta - p.min_eta);
+    for (int j = 0; j < q; j++) {
+      double xi = interp[4 * j] * xs + xo, eta = interp[4 * j + 1] * es + eo, xyz[3], lxi, leta;
+      xyz_from_xieta(xi, eta, p.face, xyz);
+      Bounds b;
+      int leaf = locate_leaf(xyz[0], xyz[1], xyz[2], c->L, lxi, leta, b, err);
+      il_row[(size_t)i * q + j] = leaf - off;
+      host_bli(&il_basis[((size_t)i * q + j) * q], xi, eta, kPi / 4.0 * b.min_xi, kPi / 4.0 * b.max_xi,
+               kPi / 4.0 * b.min_eta, kPi / 4.0 * b.max_eta, d, err);
+    }
+  }
+  if (err) {
+    set_last_error("a non-leaf proxy point fell outside its located leaf (the reference aborts here too)");
+    return SBSLPM_ERR_OUT_OF_PANEL;
+  }
+  SB_TRY(upload(&c->il_row, il_row));
+  SB_TRY(upload(&c->il_basis, il_basis));
+
+  // child-in-parent BLI matrices (child_to_parent / parent_to_child_3,
+  // src/fmm_funcs_impl.hpp:47-70, 138-171), identical for every parent of
+  // the uniform quadtree; built from face 0 and its four children.
+  if (c->L > 1) {
+    std::vector<double> mat((size_t)4 * q * q);
+    const sbslpm_panel& par = c->panels[0];
+    for (int ch = 0; ch < 4; ch++) {
+      const sbslpm_panel& k = c->panels[child_of(par, ch)];
+      double xo = kPi / 4.0 * 0.5 * (k.min_xi + k.max_xi), xs = kPi / 4.0 * 0.5 * (k.max_xi - k.min_xi);
+      double eo = kPi / 4.0 * 0.5 * (k.min_eta + k.max_eta), es = kPi / 4.0 * 0.5 * (k.max_eta - k.min_eta);
+      for (int i = 0; i < q; i++)
+        host_bli(&mat[((size_t)ch * q + i) * q], interp[4 * i] * xs + xo, interp[4 * i + 1] * es + eo,
+                 par.min_xi * kPi / 4.0, par.max_xi * kPi / 4.0, par.min_eta * kPi / 4.0, par.max_eta * kPi / 4.0, d,
+                 err);
+    }
+    SB_TRY(upload(&c->child_mat, mat));
+  }
+
+  // interaction list grouped by target panel, list order kept within a target
+  if (c->cfg.velocity == SBSLPM_VEL_FMM) {
+    std::vector<int> start(P + 1, 0), srcs(c->list.size());
+    for (const auto& e : c->list) start[e.target_panel + 1]++;
+    for (int p = 0; p < P; p++) start[p + 1] += start[p];
+    std::vector<int> fill(start.begin(), start.end() - 1);
+    for (const auto& e : c->list) srcs[fill[e.target_panel]++] = e.source_panel;
+    SB_TRY(upload(&c->tgt_start, start));
+    SB_TRY(upload(&c->src_panel, srcs));
+  }
+
+  for (int i = 0; i <= d; i++) {
+    c->tab.cosv[i] = d == 0 ? 0.0 : std::cos(kPi * i / d);
+    c->tab.w[i] = d == 0 ? 1.0 : (i == 0 ? 0.5 : (i == d ? 0.5 * std::pow(-1, i) : std::pow(-1, i)));
+  }
+  return SBSLPM_OK;
+}
+
+sbslpm_status allocate_workspace(sbslpm_ctx* c) {
+  const size_t pn = (size_t)c->P * c->q, ln = (size_t)c->A * c->q;
+  SB_TRY(dalloc(&c->src, pn));
+  if (c->cfg.precision == SBSLPM_MIXED) SB_TRY(dalloc(&c->srcf, pn));
+  SB_TRY(dalloc(&c->tgt, 3 * pn));
+  SB_TRY(dalloc(&c->vbuf, 4 * 3 * ln));
+  SB_TRY(dalloc(&c->dep, 3 * ln));
+  SB_TRY(dalloc(&c->newvor, ln));
+  if (c->cfg.tracer_count > 0) SB_TRY(dalloc(&c->newtr, ln * c->cfg.tracer_count));
+  if (c->cfg.velocity == SBSLPM_VEL_DIRECT) {
+    long g = (148L * 64) / c->A;
+    c->groups = (int)(g < 1 ? 1 : (g > 64 ? 64 : g));
+    SB_TRY(dalloc(&c->partial, (size_t)c->groups * 3 * ln));
+  }
+  SB_TRY(dalloc(&c->err, 1));
+  SB_CUDA(cudaMemset(c->err, 0, sizeof(unsigned)));
+  SB_CUDA(cudaMallocHost(reinterpret_cast<void**>(&c->h_err), sizeof(unsigned)));
+  return SBSLPM_OK;
+}
+
+void fill_geom(sbslpm_ctx* c) {
+  StepGeom& g = c->geom;
+  g.levels = c->L;
+  g.degree = c->d;
+  g.q = c->q;
+  g.panels = c->P;
+  g.leaves = c->A;
+  g.offset = c->off;
+  g.eps = c->cfg.kernel_eps;
+  g.omega = c->cfg.omega;
+  g.px = c->px;
+  g.tgt_start = c->tgt_start;
+  g.src_panel = c->src_panel;
+  g.il_row = c->il_row;
+  g.il_basis = c->il_basis;
+  g.child_mat = c->child_mat;
+  g.pd_centre = c->centre;
+  g.srcf = c->srcf;
+  g.err = c->err;
+}
+
+// One velocity evaluation (one RK4 stage) into v (contiguous [3][leaves*q]).
+void velocity_eval(sbslpm_ctx* c, int stage, double dt_s, const double* vprev, const double* x, const double* y,
+                   const double* z, const double* area, const double* vors, double* v) {
+  cudaStream_t st = c->stream();
+  const StepGeom& g = c->geom;
+  launch_leaf_sources(g, stage, dt_s, vprev, x, y, z, vors, area, c->src, st);
+  if (c->cfg.velocity == SBSLPM_VEL_DIRECT) {
+    launch_direct_leaves(g, c->cfg.precision, c->src, v, c->partial, c->groups, st);
+    return;
+  }
+  launch_nonleaf_sources(g, stage, dt_s, vprev, c->src, st);
+  for (int lev = c->L - 2; lev >= 0; lev--) launch_upward_level(g, lev, c->src, st);
+  launch_interactions(g, c->cfg.precision, c->src, c->tgt, false, st);
+  if (c->L == 1) {
+    cudaMemcpyAsync(v, c->tgt, sizeof(double) * 3 * c->P * c->q, cudaMemcpyDeviceToDevice, st);
+    return;
+  }
+  for (int lev = 1; lev < c->L; lev++) launch_downward_level(g, lev, c->tgt, lev == c->L - 1 ? v : nullptr, st);
+}
+
+// The work of one bve_back_rk4_step (src/bve_time_step.cpp:311-419), enqueued on the stream.
+void enqueue_step(sbslpm_ctx* c, const double* x, const double* y, const double* z, const double* area, double* vors,
+                  double* vel_x, double* vel_y, double* vel_z, double* tracers) {
+  cudaStream_t st = c->stream();
+  const size_t ln = (size_t)c->A * c->q;
+  const double dt = c->cfg.dt;
+  double* v[4];
+  for (int k = 0; k < 4; k++) v[k] = c->vbuf + (size_t)k * 3 * ln;
+  const double stage_dt[4] = {0.0, 0.5 * dt, 0.5 * dt, dt};
+  for (int s = 0; s < 4; s++) velocity_eval(c, s, stage_dt[s], s ? v[s - 1] : nullptr, x, y, z, area, vors, v[s]);
+  const int T = c->cfg.tracer_count;
+  launch_depart_remap(c->geom, &c->tab, x, y, z, v[0], v[1], v[2], v[3], dt, c->dep, vors, tracers, T, c->newvor,
+                      c->newtr, 3, st);
+  cudaMemcpyAsync(vors, c->newvor, sizeof(double) * ln, cudaMemcpyDeviceToDevice, st);
+  if (T > 0) cudaMemcpyAsync(tracers, c->newtr, sizeof(double) * ln * T, cudaMemcpyDeviceToDevice, st);
+  cudaMemcpyAsync(vel_x, v[0], sizeof(double) * ln, cudaMemcpyDeviceToDevice, st);
+  cudaMemcpyAsync(vel_y, v[0] + ln, sizeof(double) * ln, cudaMemcpyDeviceToDevice, st);
+  cudaMemcpyAsync(vel_z, v[0] + 2 * ln, sizeof(double) * ln, cudaMemcpyDeviceToDevice, st);
+}
+
+// Waits for the stream, then turns launch errors and the device error word
+// into a status.
+sbslpm_status finish(sbslpm_ctx* c) {
+  cudaStream_t st = c->stream();
+  SB_CUDA(cudaGetLastError());
+  SB_CUDA(cudaMemcpyAsync(c->h_err, c->err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+  SB_CUDA(cudaStreamSynchronize(st));
+  unsigned e = *c->h_err;
+  if (e) {
+    SB_CUDA(cudaMemsetAsync(c->err, 0, sizeof(unsigned), st));
+    SB_CUDA(cudaStreamSynchronize(st));
+    if (e & kErrNonFinite) return set_last_error("non-finite point in a location step"), SBSLPM_ERR_NONFINITE;
+    return set_last_error("interpolation point outside its panel"), SBSLPM_ERR_OUT_OF_PANEL;
+  }
+  return SBSLPM_OK;
+}
+
+bool bad(const void* p) { return p == nullptr; }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+
+extern "C" {
+
+sbslpm_status sbslpm_config_default(sbslpm_config* cfg) {
+  if (!cfg) return SBSLPM_ERR_ARG;
+  *cfg = sbslpm_config{};
+  cfg->levels = 5;
+  cfg->interp_degree = 3;
+  cfg->fmm_theta = 0.7;
+  cfg->kernel_eps = 1e-4;
+  cfg->omega = 0.00007272205216643039;  // RunConfig::omega default, src/run_config.hpp:31
+  cfg->dt = 1.0;
+  cfg->tracer_count = 0;
+  cfg->velocity = SBSLPM_VEL_FMM;
+  cfg->precision = SBSLPM_FP64;
+  cfg->exact_cc = 0;
+  return SBSLPM_OK;
+}
+
+sbslpm_status sbslpm_read_run_config(const char* path, sbslpm_config* cfg) {
+  if (!path || !cfg) return SBSLPM_ERR_ARG;
+  std::string msg;
+  if (!read_namelist(path, cfg, msg)) {
+    set_last_error(msg);
+    return SBSLPM_ERR_CONFIG;
+  }
+  return SBSLPM_OK;  // combinations are validated by sbslpm_create
+}
+
+const char* sbslpm_status_string(sbslpm_status s) {
+  switch (s) {
+    case SBSLPM_OK: return "ok";
+    case SBSLPM_ERR_CONFIG: return "invalid configuration";
+    case SBSLPM_ERR_CUDA: return "CUDA error";
+    case SBSLPM_ERR_OUT_OF_PANEL: return "interpolation point outside its panel";
+    case SBSLPM_ERR_NONFINITE: return "non-finite value";
+    case SBSLPM_ERR_ARG: return "invalid argument";
+    case SBSLPM_ERR_NO_DEVICE: return "no CUDA device";
+  }
+  return "unknown status";
+}
+
+const char* sbslpm_last_error(void) { return g_last_error.c_str(); }
+
+int sbslpm_panel_count(int levels) { return 2 * ((1 << (2 * levels)) - 1); }
+int sbslpm_leaf_count(int levels) { return 6 * (1 << (2 * (levels - 1))); }
+
+sbslpm_status sbslpm_cubed_sphere_panels_init(int levels, sbslpm_panel* out) {
+  if (!out || levels < 1 || levels > 12) return SBSLPM_ERR_ARG;
+  std::vector<sbslpm_panel> p;
+  build_panels(levels, p);
+  std::memcpy(out, p.data(), sizeof(sbslpm_panel) * p.size());
+  return SBSLPM_OK;
+}
+
+sbslpm_status sbslpm_interp_init(int degree, int exact_cc, double* interp) {
+  if (!interp || degree < 0 || degree > kMaxDegree) return SBSLPM_ERR_ARG;
+  std::vector<double> v;
+  build_interp(degree, exact_cc != 0, v);
+  std::memcpy(interp, v.data(), sizeof(double) * v.size());
+  return SBSLPM_OK;
+}
+
+sbslpm_status sbslpm_cube_sphere_spec_points(int levels, int degree, const sbslpm_panel* panels, const double* interp,
+                                             double* x, double* y, double* z, double* area) {
+  if (!panels || !interp || !x || !y || !z || !area) return SBSLPM_ERR_ARG;
+  std::vector<sbslpm_panel> p(panels, panels + sbslpm_panel_count(levels));
+  build_points(levels, degree, p, interp, x, y, z, area);
+  return SBSLPM_OK;
+}
+
+sbslpm_status sbslpm_dual_tree_traversal(int levels, const sbslpm_panel* panels, double theta,
+                                         sbslpm_interact_pair* out, long cap, long* count) {
+  if (!panels || !count) return SBSLPM_ERR_ARG;
+  std::vector<sbslpm_panel> p(panels, panels + sbslpm_panel_count(levels));
+  std::vector<sbslpm_interact_pair> list;
+  build_interactions(levels, p, theta, list);
+  *count = (long)list.size();
+  if (out) std::memcpy(out, list.data(), sizeof(sbslpm_interact_pair) * std::min<size_t>(cap, list.size()));
+  return SBSLPM_OK;
+}
+
+sbslpm_status sbslpm_interp_vals_bli(double* basis, double xi, double eta, double min_xi, double max_xi,
+                                     double min_eta, double max_eta, int degree) {
+  if (!basis || degree < 0 || degree > kMaxDegree) return SBSLPM_ERR_ARG;
+  unsigned err = 0;
+  host_bli(basis, xi, eta, min_xi, max_xi, min_eta, max_eta, degree, err);
+  return err ? SBSLPM_ERR_OUT_OF_PANEL : SBSLPM_OK;
+}
+
+int sbslpm_point_locate_panel(const sbslpm_panel* panels, double x, double y, double z) {
+  if (!panels) return -1;
+  // depth of the uniform tree from the panel table (leaves are the last level)
+  int levels = 1;
+  while (!panels[level_start(levels - 1)].is_leaf) levels++;
+  double xi, eta;
+  Bounds b;
+  unsigned err = 0;
+  int leaf = locate_leaf(x, y, z, levels, xi, eta, b, err);
+  return err ? -1 : leaf;
+}
+
+sbslpm_status sbslpm_create(const sbslpm_config* cfg, sbslpm_ctx** out) {
+  if (!cfg || !out) return SBSLPM_ERR_ARG;
+  *out = nullptr;
+  SB_TRY(validate(*cfg));
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    set_last_error("no CUDA device available");
+    return SBSLPM_ERR_NO_DEVICE;
+  }
+  sbslpm_ctx* c = new sbslpm_ctx();
+  c->cfg = *cfg;
+  c->L = cfg->levels;
+  c->d = cfg->interp_degree;
+  c->q = (c->d + 1) * (c->d + 1);
+  c->P = sbslpm_panel_count(c->L);
+  c->A = sbslpm_leaf_count(c->L);
+  c->off = c->P - c->A;
+  build_panels(c->L, c->panels);
+  if (cfg->velocity == SBSLPM_VEL_FMM) build_interactions(c->L, c->panels, cfg->fmm_theta, c->list);
+  c->I = (long)c->list.size();
+  sbslpm_status s = SBSLPM_OK;
+  if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) s = SBSLPM_ERR_CUDA;
+  if (s == SBSLPM_OK) s = precompute(c);
+  if (s == SBSLPM_OK) s = allocate_workspace(c);
+  if (s != SBSLPM_OK) {
+    sbslpm_destroy(c);
+    return s;
+  }
+  fill_geom(c);
+  *out = c;
+  return SBSLPM_OK;
+}
+
+sbslpm_status sbslpm_destroy(sbslpm_ctx* c) {
+  if (!c) return SBSLPM_OK;
+  if (c->graph) cudaGraphExecDestroy(c->graph);
+  void* bufs[] = {c->px, c->il_basis, c->child_mat, c->centre, c->tgt_start, c->src_panel, c->il_row, c->src,
+                  c->srcf, c->tgt, c->vbuf, c->partial, c->newvor, c->newtr, c->dep, c->err};
+  for (void* b : bufs)
+    if (b) cudaFree(b);
+  if (c->h_err) cudaFreeHost(c->h_err);
+  if (c->own_stream) cudaStreamDestroy(c->own_stream);
+  delete c;
+  return SBSLPM_OK;
+}
+
+sbslpm_status sbslpm_set_stream(sbslpm_ctx* c, void* stream) {
+  if (!c) return SBSLPM_ERR_ARG;
+  c->user_stream = static_cast<cudaStream_t>(stream);
+  c->user_stream_set = true;
+  return SBSLPM_OK;
+}
+
+sbslpm_status sbslpm_get_sizes(const sbslpm_ctx* c, long* sizes) {
+  if (!c || !sizes) return SBSLPM_ERR_ARG;
+  sizes[0] = c->P;
+  sizes[1] = c->A;
+  sizes[2] = c->q;
+  sizes[3] = c->I;
+  return SBSLPM_OK;
+}
+
+sbslpm_status sbslpm_get_panels(const sbslpm_ctx* c, sbslpm_panel* out) {
+  if (!c || !out) return SBSLPM_ERR_ARG;
+  std::memcpy(out, c->panels.data(), sizeof(sbslpm_panel) * c->panels.size());
+  return SBSLPM_OK;
+}
+
+sbslpm_status sbslpm_get_interactions(const sbslpm_ctx* c, sbslpm_interact_pair* out) {
+  if (!c || !out) return SBSLPM_ERR_ARG;
+  if (!c->list.empty()) std::memcpy(out, c->list.data(), sizeof(sbslpm_interact_pair) * c->list.size());
+  return SBSLPM_OK;
+}
+
+long sbslpm_kernel_launches(void) { return launch_counter(); }
+
+sbslpm_status sbslpm_bve_step(sbslpm_ctx* c, const double* x, const double* y, const double* z, const double* area,
+                              double* vors, double* vel_x, double* vel_y, double* vel_z, double* tracers, double) {
+  if (!c || bad(x) || bad(y) || bad(z) || bad(area) || bad(vors) || bad(vel_x) || bad(vel_y) || bad(vel_z) ||
+      (c->cfg.tracer_count > 0 && bad(tracers)))
+    return SBSLPM_ERR_ARG;
+  enqueue_step(c, x, y, z, area, vors, vel_x, vel_y, vel_z, tracers);
+  return finish(c);
+}
+
+sbslpm_status sbslpm_bve_run(sbslpm_ctx* c, const double* x, const double* y, const double* z, const double* area,
+                             double* vors, double* vel_x, double* vel_y, double* vel_z, double* tracers, double,
+                             int nsteps) {
+  if (!c || bad(x) || bad(y) || bad(z) || bad(area) || bad(vors) || bad(vel_x) || bad(vel_y) || bad(vel_z) ||
+      (c->cfg.tracer_count > 0 && bad(tracers)) || nsteps < 0)
+    return SBSLPM_ERR_ARG;
+  GraphKey key{{x, y, z, area, vors, vel_x, vel_y, vel_z, tracers}};
+  cudaStream_t st = c->stream();
+  if (!c->graph || !(key == c->graph_key)) {
+    if (c->graph) {
+      cudaGraphExecDestroy(c->graph);
+      c->graph = nullptr;
+    }
+    // capture on the context's own stream (the legacy default stream cannot be captured)
+    cudaStream_t cap = c->own_stream;
+    if (st != cap) {
+      cudaEvent_t ev;
+      SB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+      SB_CUDA(cudaEventRecord(ev, st));
+      SB_CUDA(cudaStreamWaitEvent(cap, ev, 0));
+      cudaEventDestroy(ev);
+    }
+    const bool saved_set = c->user_stream_set;
+    c->user_stream_set = false;  // enqueue on the capturing stream
+    long before = launch_counter();
+    cudaGraph_t graph;
+    SB_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+    enqueue_step(c, x, y, z, area, vors, vel_x, vel_y, vel_z, tracers);
+    cudaError_t ce = cudaStreamEndCapture(cap, &graph);
+    c->user_stream_set = saved_set;
+    c->launches_per_step = launch_counter() - before;
+    launch_counter() = before;
+    SB_CUDA(ce);
+    SB_CUDA(cudaGraphInstantiate(&c->graph, graph, 0));
+    cudaGraphDestroy(graph);
+    c->graph_key = key;
+  }
+  for (int s = 0; s < nsteps; s++) {
+    SB_CUDA(cudaGraphLaunch(c->graph, st));
+    launch_counter() += c->launches_per_step;
+  }
+  return finish(c);
+}
+
+sbslpm_status sbslpm_upward_pass(sbslpm_ctx* c, const double* area, const double* pots, double* proxy_source) {
+  if (!c || bad(area) || bad(pots) || bad(proxy_source)) return SBSLPM_ERR_ARG;
+  cudaStream_t st = c->stream();
+  SB_CUDA(cudaMemsetAsync(c->src, 0, sizeof(double4) * c->P * c->q, st));
+  launch_leaf_strength(c->geom, area, pots, c->src, st);
+  for (int lev = c->L - 2; lev >= 0; lev--) launch_upward_level(c->geom, lev, c->src, st);
+  launch_copy_strength(c->geom, c->src, proxy_source, st);
+  return finish(c);
+}
+
+namespace sbslpm {
+// t_c[i] += tgt[c][i] for the three components (accumulating API of bve_vel_interactions).
+__global__ void k_add3(const double* __restrict__ t, long n, double* a, double* b, double* cc) {
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  a[i] += t[i];
+  b[i] += t[n + i];
+  cc[i] += t[2 * n + i];
+}
+}  // namespace sbslpm
+
+sbslpm_status sbslpm_bve_vel_interactions(sbslpm_ctx* c, const double* dx, const double* dy, const double* dz,
+                                          const double* source, double* t1, double* t2, double* t3) {
+  if (!c || bad(dx) || bad(dy) || bad(dz) || bad(source) || bad(t1) || bad(t2) || bad(t3)) return SBSLPM_ERR_ARG;
+  if (c->cfg.velocity != SBSLPM_VEL_FMM) return set_last_error("context has no interaction list"), SBSLPM_ERR_CONFIG;
+  cudaStream_t st = c->stream();
+  launch_sources_from_disp(c->geom, dx, dy, dz, source, c->src, st);
+  launch_interactions(c->geom, c->cfg.precision, c->src, c->tgt, false, st);
+  long n = (long)c->P * c->q;
+  k_add3<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(c->tgt, n, t1, t2, t3);
+  launch_counter()++;
+  return finish(c);
+}
+
+sbslpm_status sbslpm_downward_pass_3(sbslpm_ctx* c, double* t1, double* t2, double* t3, double* s1, double* s2,
+                                     double* s3) {
+  if (!c || bad(t1) || bad(t2) || bad(t3) || bad(s1) || bad(s2) || bad(s3)) return SBSLPM_ERR_ARG;
+  cudaStream_t st = c->stream();
+  size_t pn = (size_t)c->P * c->q, ln = (size_t)c->A * c->q, off = (size_t)c->off * c->q;
+  double* tin[3] = {t1, t2, t3};
+  double* sout[3] = {s1, s2, s3};
+  for (int k = 0; k < 3; k++)
+    SB_CUDA(cudaMemcpyAsync(c->tgt + k * pn, tin[k], sizeof(double) * pn, cudaMemcpyDeviceToDevice, st));
+  for (int lev = 1; lev < c->L; lev++) launch_downward_level(c->geom, lev, c->tgt, nullptr, st);
+  for (int k = 0; k < 3; k++) {
+    SB_CUDA(cudaMemcpyAsync(tin[k], c->tgt + k * pn, sizeof(double) * pn, cudaMemcpyDeviceToDevice, st));
+    SB_CUDA(cudaMemcpyAsync(sout[k], c->tgt + k * pn + off, sizeof(double) * ln, cudaMemcpyDeviceToDevice, st));
+  }
+  return finish(c);
+}
+
+sbslpm_status sbslpm_bve_departure(sbslpm_ctx* c, const double* x, const double* y, const double* z, const double* v0,
+                                   const double* v1, const double* v2, const double* v3, double dt, double* dep_x,
+                                   double* dep_y, double* dep_z) {
+  if (!c || bad(x) || bad(y) || bad(z) || bad(v0) || bad(v1) || bad(v2) || bad(v3) || bad(dep_x) || bad(dep_y) ||
+      bad(dep_z))
+    return SBSLPM_ERR_ARG;
+  cudaStream_t st = c->stream();
+  size_t ln = (size_t)c->A * c->q;
+  launch_depart_remap(c->geom, &c->tab, x, y, z, v0, v1, v2, v3, dt, c->dep, nullptr, nullptr, 0, nullptr, nullptr, 1,
+                      st);
+  double* outs[3] = {dep_x, dep_y, dep_z};
+  for (int k = 0; k < 3; k++)
+    SB_CUDA(cudaMemcpyAsync(outs[k], c->dep + k * ln, sizeof(double) * ln, cudaMemcpyDeviceToDevice, st));
+  return finish(c);
+}
+
+sbslpm_status sbslpm_bve_remap(sbslpm_ctx* c, const double* z, const double* dep_x, const double* dep_y,
+                               const double* dep_z, const double* vors, const double* tracers, double* new_vors,
+                               double* new_tracers) {
+  if (!c || bad(z) || bad(dep_x) || bad(dep_y) || bad(dep_z) || bad(vors) || bad(new_vors) ||
+      (c->cfg.tracer_count > 0 && (bad(tracers) || bad(new_tracers))))
+    return SBSLPM_ERR_ARG;
+  cudaStream_t st = c->stream();
+  size_t ln = (size_t)c->A * c->q;
+  const double* ins[3] = {dep_x, dep_y, dep_z};
+  for (int k = 0; k < 3; k++)
+    SB_CUDA(cudaMemcpyAsync(c->dep + k * ln, ins[k], sizeof(double) * ln, cudaMemcpyDeviceToDevice, st));
+  launch_depart_remap(c->geom, &c->tab, nullptr, nullptr, z, nullptr, nullptr, nullptr, nullptr, 0.0, c->dep, vors,
+                      tracers, c->cfg.tracer_count, new_vors, new_tracers, 2, st);
+  return finish(c);
+}
+
+sbslpm_status sbslpm_direct_sum_bve(long nt, const double* tx, const double* ty, const double* tz, long ns,
+                                    const double* sx, const double* sy, const double* sz, const double* s, double eps,
+                                    int precision, double* ux, double* uy, double* uz, void* stream) {
+  if (nt < 0 || ns < 0 || (nt > 0 && (bad(tx) || bad(ty) || bad(tz) || bad(ux) || bad(uy) || bad(uz))) ||
+      (ns > 0 && (bad(sx) || bad(sy) || bad(sz) || bad(s))) || (precision != SBSLPM_FP64 && precision != SBSLPM_MIXED))
+    return SBSLPM_ERR_ARG;
+  if (nt == 0) return SBSLPM_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (ns == 0) {
+    SB_CUDA(cudaMemsetAsync(ux, 0, sizeof(double) * nt, st));
+    SB_CUDA(cudaMemsetAsync(uy, 0, sizeof(double) * nt, st));
+    SB_CUDA(cudaMemsetAsync(uz, 0, sizeof(double) * nt, st));
+    SB_CUDA(cudaStreamSynchronize(st));
+    return SBSLPM_OK;
+  }
+  int groups = direct_groups(nt, ns);
+  double* partial = nullptr;
+  SB_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&partial), sizeof(double) * 3 * nt * groups, st));
+  launch_direct_bve(nt, tx, ty, tz, ns, sx, sy, sz, s, eps, precision, partial, groups, ux, uy, uz, st);
+  SB_CUDA(cudaGetLastError());
+  SB_CUDA(cudaFreeAsync(partial, st));
+  SB_CUDA(cudaStreamSynchronize(st));
+  return SBSLPM_OK;
+}
+
+sbslpm_status sbslpm_direct_sum_inv_lap(long n, const double* x, const double* y, const double* z, const double* area,
+                                        const double* pots, double* soln, void* stream) {
+  if (n < 0 || (n > 0 && (bad(x) || bad(y) || bad(z) || bad(area) || bad(pots) || bad(soln)))) return SBSLPM_ERR_ARG;
+  if (n == 0) return SBSLPM_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  launch_inv_lap(n, x, y, z, area, pots, soln, st);
+  SB_CUDA(cudaGetLastError());
+  SB_CUDA(cudaStreamSynchronize(st));
+  return SBSLPM_OK;
+}
+
+sbslpm_status sbslpm_time_interactions(sbslpm_ctx* c, int reps, double* ms_per_launch, double* pairs) {
+  if (!c || reps < 1 || !ms_per_launch) return SBSLPM_ERR_ARG;
+  if (c->cfg.velocity != SBSLPM_VEL_FMM) return set_last_error("context has no interaction list"), SBSLPM_ERR_CONFIG;
+  cudaStream_t st = c->stream();
+  if (c->cfg.precision == SBSLPM_MIXED) launch_pack_mixed(c->geom, c->src, st);
+  cudaEvent_t e0, e1;
+  SB_CUDA(cudaEventCreate(&e0));
+  SB_CUDA(cudaEventCreate(&e1));
+  SB_CUDA(cudaEventRecord(e0, st));
+  for (int r = 0; r < reps; r++) launch_interactions_only(c->geom, c->cfg.precision, c->src, c->tgt, st);
+  SB_CUDA(cudaEventRecord(e1, st));
+  SB_CUDA(cudaEventSynchronize(e1));
+  float ms = 0;
+  SB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *ms_per_launch = ms / reps;
+  if (pairs) *pairs = (double)c->I * c->q * c->q;
+  return finish(c);
+}
+
+sbslpm_status sbslpm_measure_fma_peak(int kind, double ms_target, double* flops) {
+  if ((kind != 0 && kind != 1) || !flops || !(ms_target > 0)) return SBSLPM_ERR_ARG;
+  int dev = 0, sms = 0;
+  SB_CUDA(cudaGetDevice(&dev));
+  SB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const int blocks = sms * 8;  // 8 x 256 threads per SM
+  float* o32 = nullptr;
+  double* o64 = nullptr;
+  SB_CUDA(cudaMalloc(&o32, sizeof(float)));
+  SB_CUDA(cudaMalloc(&o64, sizeof(double)));
+  cudaEvent_t e0, e1;
+  SB_CUDA(cudaEventCreate(&e0));
+  SB_CUDA(cudaEventCreate(&e1));
+  int iters = 1 << 12;
+  float ms = 0;
+  for (int attempt = 0; attempt < 12; attempt++) {  // grow iters until the launch lasts ms_target
+    launch_fma_probe(kind, blocks, iters, o32, o64, nullptr);
+    SB_CUDA(cudaEventRecord(e0, nullptr));
+    launch_fma_probe(kind, blocks, iters, o32, o64, nullptr);
+    SB_CUDA(cudaEventRecord(e1, nullptr));
+    SB_CUDA(cudaEventSynchronize(e1));
+    SB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    if (ms >= ms_target) break;
+    iters *= 2;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(o32);
+  cudaFree(o64);
+  *flops = 2.0 * 8.0 * (double)iters * blocks * 256 / (ms * 1e-3);
+  return SBSLPM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,28 @@
+// Internal declarations shared by the host setup code, the kernels and the
+// C ABI implementation.
+#pragma once
+
+#include <array>
+#include <string>
+#include <vector>
+
+#include "../../include/sbslpm.h"
+
+namespace sbslpm {
+
+// setup_host.cpp
+int child_of(const sbslpm_panel& p, int c);
+void build_panels(int levels, std::vector<sbslpm_panel>& panels);
+void build_interp(int degree, bool exact_cc, std::vector<double>& info);
+void build_interactions(int levels, const std::vector<sbslpm_panel>& panels, double theta,
+                        std::vector<sbslpm_interact_pair>& out);
+void build_points(int levels, int degree, const std::vector<sbslpm_panel>& panels, const double* interp, double* x,
+                  double* y, double* z, double* area);
+void proxy_point(const sbslpm_panel& p, const double* interp, int j, double* xyz);
+void host_bli(double* basis, double xi, double eta, double min_xi, double max_xi, double min_eta, double max_eta,
+              int degree, unsigned& err);
+bool read_namelist(const char* path, sbslpm_config* cfg, std::string& msg);
+
+void set_last_error(const std::string& msg);
+
+}  // namespace sbslpm
