@@ -29,8 +29,6 @@ configuration; rank 0 only.
 from __future__ import annotations
 
 import argparse
-import csv
-import io
 import json
 import os
 import subprocess
@@ -66,49 +64,73 @@ def rh4(g):
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle samples during the timed region."""
+    """SM clock, max clock, power and clock-event reasons sampled through NVML
+    in a thread during the timed region (one sample at start, every 20 ms,
+    one at stop).  Read-only: no GPU setting is changed."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-         "clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"),
+               ("hw_power_brake", "nvmlClocksEventReasonHwPowerBrakeSlowdown"))
 
     def __init__(self, index: int):
         self.index = index
-        self.proc = None
+        self.rows = []
+        self.err = None
+
+    def _sample(self):
+        nv = self.nv
+        sm = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+        mx = nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)
+        bits = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+        try:
+            pw = nv.nvmlDeviceGetPowerUsage(self.h) / 1000.0
+        except Exception:
+            pw = None
+        act = [n for n, c in self.REASONS if hasattr(nv, c) and bits & getattr(nv, c)]
+        self.rows.append((sm, mx, pw, act))
+
+    def _loop(self):
+        while not self.stop.wait(0.02):
+            self._sample()
 
     def __enter__(self):
+        import threading
+
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-        except OSError:
-            self.proc = None
+            import pynvml as nv
+
+            nv.nvmlInit()
+            self.nv = nv
+            # NVML enumerates all GPUs; map the visible CUDA device to its index
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+            idx = int(vis.split(",")[self.index]) if vis and vis.split(",")[self.index].isdigit() else self.index
+            self.h = nv.nvmlDeviceGetHandleByIndex(idx)
+            self._sample()
+            self.stop = threading.Event()
+            self.th = threading.Thread(target=self._loop, daemon=True)
+            self.th.start()
+        except Exception as e:  # no NVML: report it
+            self.err = repr(e)
+            self.nv = None
         return self
 
     def __exit__(self, *exc):
-        self.rows = []
-        if self.proc is None:
-            return False
-        self.proc.terminate()
-        try:
-            out, _ = self.proc.communicate(timeout=10)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-            out, _ = self.proc.communicate()
-        for r in csv.reader(io.StringIO(out)):
-            if len(r) >= 9:
-                self.rows.append([c.strip() for c in r])
+        if self.nv is not None:
+            self.stop.set()
+            self.th.join()
+            self._sample()
         return False
 
     def summary(self):
-        if not getattr(self, "rows", None):
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in self.rows for k in range(4) if r[5 + k].lower() == "active"})
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [f"no samples: {self.err}"], "samples": 0}
+        sm = [r[0] for r in self.rows]
+        pw = [r[2] for r in self.rows if r[2] is not None]
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(r[1] for r in self.rows),
+                "reasons": sorted({a for r in self.rows for a in r[3]}), "samples": len(self.rows),
+                "power_w_max": max(pw) if pw else None}
 
 
 def run_reference(args, rank):
@@ -153,7 +175,7 @@ def timed_steps(torch, ctx, f, steps, flush):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
