@@ -198,6 +198,27 @@ sbslpm_status sbslpm_direct_sum_bve(long n_targets, const double* tx, const doub
 sbslpm_status sbslpm_direct_sum_inv_lap(long n, const double* x, const double* y, const double* z,
                                         const double* area, const double* pots, double* soln, void* stream);
 
+/* No counterpart in the reference.  The same Biot-Savart direct sum as
+ * sbslpm_direct_sum_bve, for callers that cannot let a library allocate
+ * device memory: a host model that fixes its device footprint at start-up, or
+ * that routes every device allocation through its own allocator, cannot
+ * accept the cudaMallocAsync/cudaFreeAsync of scratch that
+ * sbslpm_direct_sum_bve makes on every call.  This entry point allocates
+ * nothing: its scratch is one fixed 16 MiB array compiled into the library,
+ * which each GPU that loads the library holds until the process exits.
+ * Limit: n_targets <= 699,050 (3 * n_targets doubles of scratch); larger
+ * calls return SBSLPM_ERR_ARG with a message and do nothing.  The first call
+ * on each device looks the array's device address up (cudaGetSymbolAddress,
+ * with that device current), so make that first call before any stream
+ * capture.  Every call on a device shares the one array and each call
+ * overwrites the parts it uses, so calls whose kernels overlap on the GPU
+ * (different streams or host threads) race: serialise them.  Synchronises
+ * the stream before returning. */
+sbslpm_status sbslpm_direct_sum_bve_noalloc(long n_targets, const double* tx, const double* ty, const double* tz,
+                                            long n_sources, const double* sx, const double* sy, const double* sz,
+                                            const double* strength, double eps, int precision, double* u_x,
+                                            double* u_y, double* u_z, void* stream);
+
 /* ---------------- measurement ---------------- */
 
 /* Average device time of one launch of the interaction kernel alone (the

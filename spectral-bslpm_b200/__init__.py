@@ -108,6 +108,7 @@ def lib() -> ctypes.CDLL:
     L.sbslpm_bve_remap.argtypes = [_VP] * 9
     L.sbslpm_direct_sum_bve.argtypes = [ctypes.c_long, _VP, _VP, _VP, ctypes.c_long, _VP, _VP, _VP, _VP,
                                         ctypes.c_double, ctypes.c_int, _VP, _VP, _VP, _VP]
+    L.sbslpm_direct_sum_bve_noalloc.argtypes = L.sbslpm_direct_sum_bve.argtypes
     L.sbslpm_direct_sum_inv_lap.argtypes = [ctypes.c_long] + [_VP] * 7
     L.sbslpm_time_interactions.argtypes = [_VP, ctypes.c_int, _D, _D]
     L.sbslpm_measure_fma_peak.argtypes = [ctypes.c_int, ctypes.c_double, _D]
@@ -350,6 +351,21 @@ def direct_sum_bve(tx, ty, tz, sx, sy, sz, strength, eps, precision=FP64, out=No
                                        *[_dev(t, "source") for t in (sx, sy, sz, strength)], float(eps),
                                        int(precision), *[_dev(t, "out") for t in out], _VP(_stream())),
            "sbslpm_direct_sum_bve")
+    return out
+
+
+def direct_sum_bve_noalloc(tx, ty, tz, sx, sy, sz, strength, eps, precision=FP64, out=None):
+    """direct_sum_bve through the entry point that allocates no device memory
+    (fixed scratch inside the library; at most 699,050 targets)."""
+    import torch
+
+    nt, ns = tx.numel(), sx.numel()
+    if out is None:
+        out = tuple(torch.empty(nt, dtype=torch.float64, device=tx.device) for _ in range(3))
+    _check(lib().sbslpm_direct_sum_bve_noalloc(nt, *[_dev(t, "target") for t in (tx, ty, tz)], ns,
+                                               *[_dev(t, "source") for t in (sx, sy, sz, strength)], float(eps),
+                                               int(precision), *[_dev(t, "out") for t in out], _VP(_stream())),
+           "sbslpm_direct_sum_bve_noalloc")
     return out
 
 
