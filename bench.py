@@ -4,19 +4,21 @@
 Workload (N=1): the 393,216-particle BVE configuration -- cubed sphere with
 6 x 64 x 64 leaf panels x 4 x 4 Chebyshev points (levels=7, interp_degree=3),
 unit sphere, Omega = 2*pi, Rossby-Haurwitz R=4 initial vorticity
-(omega0 = K = 0.5, mean removed), treecode/FMM velocity at MAC theta = 0.7,
-kernel_eps = 1e-4, dt = 0.005.  Synthetic inputs generated here; nothing is
-read from disk.
+(omega0 = K = 0.5, mean removed), barycentric-Lagrange treecode with MAC
+theta = 0.7, degree-8 proxies (81 per cluster), leaves of at most 256
+particles, kernel_eps = 1e-4, dt = 0.005.  Synthetic inputs generated here;
+nothing is read from disk.
 
-  value     mixed-precision FMM steps/s (float32 pair kernels on
-            panel-relative coordinates, float64 everywhere else), inputs
+  value     mixed-precision treecode steps/s (float32 pair kernels on
+            cluster-relative coordinates, float64 everywhere else), inputs
             resident in HBM, L2 flushed between steps, one device clock per
             step (CUDA events), max over ranks.
   e2e       the same steps through the C ABI with the step's inputs copied
             from pinned host memory and the result read back every step.
-  extra     float64 "plain" FMM steps/s, their ratio, and the relative
-            L-infinity vorticity error after one step of both paths against
-            the float64 direct sum.
+  extra     the float64 "plain" path on the same treecode, the reference's
+            own spectral FMM (proxy degree = particle degree) in both
+            precisions, and the relative L-infinity vorticity error after one
+            step of each against the float64 direct sum.
 
 With --gpus N under torchrun every rank runs an independent replica of the
 workload (the ensemble use: members share nothing), so scaling is weak and
@@ -40,14 +42,16 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 METRIC = "BVE RK4 steps/s at ≤1e-6 rel vort err: mixed+batched vs FP64 plain, 1 B200"
 LEVELS, DEGREE, THETA, EPS, OMEGA, DT = 7, 3, 0.7, 1e-4, 2 * np.pi, 0.005
+PROXY_DEGREE, LEAF_SIZE = 8, 256
 PAIR_FLOP = 17  # FLOP per Biot-Savart pair (division counted as 1)
 
 
 def workload_config():
-    return {"workload": "BVE RK4, 393,216 particles (6x64x64 panels x 4x4 points), RH4 IC, FMM theta=0.7",
+    return {"workload": "BVE RK4, 393,216 particles (6x64x64 panels x 4x4 points), RH4 IC, treecode theta=0.7, "
+                        "proxy degree 8, leaf <= 256",
             "particles": 6 * 4 ** (LEVELS - 1) * (DEGREE + 1) ** 2, "levels": LEVELS, "interp_degree": DEGREE,
-            "theta": THETA, "kernel_eps": EPS, "omega": OMEGA, "dt": DT, "velocity": "fmm (reference spectral FMM)",
-            "precision": "mixed (f32 pairs, f64 positions/remap)", "l2": "flushed between timed steps"}
+            "theta": THETA, "proxy_degree": PROXY_DEGREE, "leaf_size": LEAF_SIZE, "kernel_eps": EPS, "omega": OMEGA,
+            "dt": DT, "precision": "mixed (f32 pairs, f64 positions/remap)", "l2": "flushed between timed steps"}
 
 
 def import_package():
@@ -215,19 +219,21 @@ def main():
         v = [torch.zeros_like(T(g.x)) for _ in range(3)]
         return [T(g.x), T(g.y), T(g.z), T(g.area), T(vor0), *v, None]
 
-    def ctx_for(prec, vel=sb.VEL_FMM):
+    def ctx_for(prec, vel=sb.VEL_FMM, proxy=PROXY_DEGREE):
         return sb.Context(sb.config_default(levels=LEVELS, interp_degree=DEGREE, fmm_theta=THETA, kernel_eps=EPS,
-                                            omega=OMEGA, dt=DT, precision=prec, velocity=vel))
+                                            omega=OMEGA, dt=DT, precision=prec, velocity=vel, proxy_degree=proxy,
+                                            leaf_size=LEAF_SIZE))
 
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
     ctx32, ctx64 = ctx_for(sb.MIXED), ctx_for(sb.FP64)
-    f32, f64 = fields(), fields()
+    ctxr32, ctxr64 = ctx_for(sb.MIXED, proxy=0), ctx_for(sb.FP64, proxy=0)
+    f32, f64, fr32, fr64 = fields(), fields(), fields(), fields()
     for _ in range(args.warmup):
-        ctx32.bve_run(*f32, nsteps=1)
-        ctx64.bve_run(*f64, nsteps=1)
+        for c, f in ((ctx32, f32), (ctx64, f64), (ctxr32, fr32), (ctxr64, fr64)):
+            c.bve_run(*f, nsteps=1)
     torch.cuda.synchronize()
 
-    # ---- headline: mixed precision, device-resident -----------------------
+    # ---- headline: mixed-precision treecode, device-resident ---------------
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -245,33 +251,38 @@ def main():
     ms_per_step = t_total / args.steps
     value = world * args.steps / (t_total * 1e-3)
 
-    # ---- float64 plain path --------------------------------------------------
-    ts64 = timed_steps(torch, ctx64, f64, args.steps, flush)
-    fp64_sps = 1e3 / (sum(ts64) / len(ts64))
+    # ---- the other paths -----------------------------------------------------
+    def sps(c, f):
+        ts = timed_steps(torch, c, f, args.steps, flush)
+        return 1e3 / (sum(ts) / len(ts))
+
+    fp64_sps, r32_sps, r64_sps = sps(ctx64, f64), sps(ctxr32, fr32), sps(ctxr64, fr64)
 
     # ---- accuracy after one step vs the float64 direct sum ------------------
-    ctxd = ctx_for(sb.FP64, sb.VEL_DIRECT)
-    fd, fa, fb = fields(), fields(), fields()
+    ctxd = ctx_for(sb.FP64, sb.VEL_DIRECT, proxy=0)
+    fd = fields()
     t0 = time.perf_counter()
     ctxd.bve_back_rk4_step(*fd)
     direct_s = time.perf_counter() - t0
-    ctx32.bve_back_rk4_step(*fa)
-    ctx64.bve_back_rk4_step(*fb)
     ref = fd[4]
     scale = ref.abs().max().item()
-    err32 = (fa[4] - ref).abs().max().item() / scale
-    err64 = (fb[4] - ref).abs().max().item() / scale
     vel_ref = torch.stack(fd[5:8])
     vscale = vel_ref.abs().max().item()
-    verr32 = (torch.stack(fa[5:8]) - vel_ref).abs().max().item() / vscale
+    acc = {}
+    for name, c in (("treecode_mixed", ctx32), ("treecode_fp64", ctx64), ("spectral_fmm_mixed", ctxr32),
+                    ("spectral_fmm_fp64", ctxr64)):
+        fa = fields()
+        c.bve_back_rk4_step(*fa)
+        acc[name] = {"rel_linf_vort": (fa[4] - ref).abs().max().item() / scale,
+                     "rel_linf_vel": (torch.stack(fa[5:8]) - vel_ref).abs().max().item() / vscale}
     del ctxd
 
-    # ---- roofline of the dominant kernel (interaction kernel, mixed) -------
+    # ---- roofline of the dominant kernel (near-field pair kernel, mixed) ---
     ms_int, pairs = ctx32.time_interactions(reps=5)
     achieved = PAIR_FLOP * pairs / (ms_int * 1e-3) / 1e12
     peak_meas = sb.measure_fma_peak(0, 50.0) / 1e12
-    ms_int64, _ = ctx64.time_interactions(reps=3)
-    ach64 = PAIR_FLOP * pairs / (ms_int64 * 1e-3) / 1e12
+    ms_int64, pairs64 = ctx64.time_interactions(reps=3)
+    ach64 = PAIR_FLOP * pairs64 / (ms_int64 * 1e-3) / 1e12
     peak64 = sb.measure_fma_peak(1, 50.0) / 1e12
     share = 4 * ms_int / ms_per_step
 
@@ -324,18 +335,18 @@ def main():
             "config": dict(workload_config(), parallelism=f"replicas x{world}" if world > 1 else "1 GPU"),
             "e2e": {"value": e2e, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
-            "roofline": {"bound": "fp32", "kernel": "k_interact32 (pair interactions, q=16)", "achieved": achieved,
-                         "peak": peak_meas, "unit": "TFLOP/s", "frac": achieved / peak_meas, "traffic": None,
-                         "flop_per_pair": PAIR_FLOP, "pairs_per_launch": pairs, "ms_per_launch": ms_int,
-                         "step_share": share,
+            "roofline": {"bound": "fp32", "kernel": "k_bltc_near32 (near-field particle pairs, 256 x 256 tiles)",
+                         "achieved": achieved, "peak": peak_meas, "unit": "TFLOP/s", "frac": achieved / peak_meas,
+                         "traffic": None, "flop_per_pair": PAIR_FLOP, "pairs_per_launch": pairs,
+                         "ms_per_launch": ms_int, "step_share": share,
                          "peak_source": "measured f32 FMA-chain throughput on this GPU (sbslpm_measure_fma_peak); "
                                         "MEASURED_PEAKS.json has no CUDA-core peak"},
-            "fp64_plain": {"steps_per_s": fp64_sps, "ms_per_step": 1e3 / fp64_sps,
-                           "interaction_tflops": ach64, "fp64_fma_peak_tflops": peak64,
-                           "frac": ach64 / peak64},
+            "fp64_plain": {"steps_per_s": fp64_sps, "ms_per_step": 1e3 / fp64_sps, "near_kernel_tflops": ach64,
+                           "fp64_fma_peak_tflops": peak64, "frac": ach64 / peak64},
             "speedup_mixed_vs_fp64_plain": value / world / fp64_sps,
-            "accuracy_step1_vs_fp64_direct": {"mixed_rel_linf_vort": err32, "fp64_fmm_rel_linf_vort": err64,
-                                              "mixed_rel_linf_vel": verr32, "direct_step_s": direct_s},
+            "reference_spectral_fmm": {"mixed_steps_per_s": r32_sps, "fp64_steps_per_s": r64_sps,
+                                       "note": "the reference's own algorithm (proxy degree = particle degree 3)"},
+            "accuracy_step1_vs_fp64_direct": dict(acc, direct_step_s=direct_s),
             "cpu_baseline": cpu, "clocks": clk.summary(),
         }
         print(json.dumps(line))

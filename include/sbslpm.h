@@ -61,6 +61,15 @@ typedef struct {
   int velocity;      /* SBSLPM_VEL_FMM | SBSLPM_VEL_DIRECT */
   int precision;     /* SBSLPM_FP64 | SBSLPM_MIXED */
   int exact_cc;      /* setup helpers: 1 = exact Clenshaw-Curtis weights */
+  /* 0: the reference's spectral FMM, whose proxies are the panels' own
+   * interp_degree points (src/fmm_interactions/bve_vel_impl.hpp).  n > 0: a
+   * treecode with degree-n Chebyshev proxies (fixed, (n+1)^2 per panel) on the
+   * tree truncated so that a leaf holds at most leaf_size particles: near
+   * leaf pairs are summed particle by particle, every well-separated pair
+   * proxy by proxy (the typed-interaction design of the reference's
+   * irregular-point tree, src/fmm_interactions/swe_vel_impl.hpp:149-288). */
+  int proxy_degree;
+  int leaf_size; /* RunConfig::leaf_size: particles per treecode leaf (proxy_degree > 0) */
 } sbslpm_config;
 
 /* Same fields and order as the reference's CubedSpherePanel

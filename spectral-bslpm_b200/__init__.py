@@ -53,6 +53,8 @@ class Config(ctypes.Structure):
         ("velocity", ctypes.c_int),
         ("precision", ctypes.c_int),
         ("exact_cc", ctypes.c_int),
+        ("proxy_degree", ctypes.c_int),
+        ("leaf_size", ctypes.c_int),
     ]
 
 

@@ -50,13 +50,15 @@ __device__ __forceinline__ float recip_f32(float d) {
 
 // One Biot-Savart pair in float64.  With d = y - x and |x| = |y| = 1,
 // 1 - x.y = |d|^2 / 2, and x cross y = x cross d, so the accumulated
-// a = sum g d gives u = -1/(4 pi) x cross a.  Coincident points add nothing.
+// a = sum g d gives u = -1/(4 pi) x cross a.  Coincident points add nothing:
+// with eps > 0 because d = 0; with eps = 0 (GUARD) because g is zeroed.
+template <bool GUARD>
 __device__ __forceinline__ void pair64(double tx, double ty, double tz, const double4 s, double eps, double& ax,
                                        double& ay, double& az) {
   double dx = s.x - tx, dy = s.y - ty, dz = s.z - tz;
   double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
   double g = s.w * recip_nr(fma(0.5, r2, eps));
-  g = r2 > 0.0 ? g : 0.0;
+  if (GUARD) g = r2 > 0.0 ? g : 0.0;
   ax = fma(g, dx, ax);
   ay = fma(g, dy, ay);
   az = fma(g, dz, az);
@@ -64,12 +66,13 @@ __device__ __forceinline__ void pair64(double tx, double ty, double tz, const do
 
 // The same pair in float32 on panel-relative coordinates: d = base + s.xyz
 // with base = (c_S - c_T) - delta_t.
+template <bool GUARD>
 __device__ __forceinline__ void pair32(float bx, float by, float bz, const float4 s, float eps, float& ax, float& ay,
                                        float& az) {
   float dx = bx + s.x, dy = by + s.y, dz = bz + s.z;
   float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
   float g = s.w * recip_f32(fmaf(0.5f, r2, eps));
-  g = r2 > 0.0f ? g : 0.0f;
+  if (GUARD) g = r2 > 0.0f ? g : 0.0f;
   ax = fmaf(g, dx, ax);
   ay = fmaf(g, dy, ay);
   az = fmaf(g, dz, az);
@@ -110,16 +113,60 @@ __global__ void k_leaf_sources(StepGeom g, int stage, double dt_s, const double*
   src[o] = make_double4(px, py, pz, w);
 }
 
-// Non-leaf proxies (bve_disp_interp, src/bve_time_step.cpp:107-160): disp is
-// the BLI of the leaf displacements dt_s v at the proxy point (leaf row and
-// basis precomputed on the host); strength is filled by the upward pass.
-__global__ void k_nonleaf_sources(StepGeom g, int stage, double dt_s, const double* __restrict__ vprev,
-                                  double4* __restrict__ src) {
-  long n = (long)g.offset * g.q;
+// Piecewise API: sources from explicit displacements and strengths
+// (the inputs of bve_vel_interactions).
+__global__ void k_sources_from_disp(StepGeom g, const double* __restrict__ dx, const double* __restrict__ dy,
+                                    const double* __restrict__ dz, const double* __restrict__ s,
+                                    double4* __restrict__ src) {
+  long pn = (long)g.panels * g.q;
   long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  long pn = (long)g.panels * g.q, ln = (long)g.leaves * g.q;
-  double px = g.px[i], py = g.px[pn + i], pz = g.px[2 * pn + i];
+  if (i >= pn) return;
+  double px = g.px[i] + dx[i], py = g.px[pn + i] + dy[i], pz = g.px[2 * pn + i] + dz[i];
+  project_to_sphere(px, py, pz);
+  src[i] = make_double4(px, py, pz, s[i]);
+}
+
+__global__ void k_copy_strength(StepGeom g, const double4* __restrict__ src, double* __restrict__ out) {
+  long pn = (long)g.panels * g.q;
+  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= pn) return;
+  out[i] = src[i].w;
+}
+
+// ---------------------------------------------------------------------------
+// Tree passes (upward_pass / downward_pass_3, src/fmm_funcs.cpp:341-392;
+// child_to_parent / parent_to_child_3, src/fmm_funcs_impl.hpp:36-172).
+// child_mat[c][k][l] is the BLI basis of parent node l at child c's node k;
+// the uniform quadtree makes it the same matrix for every parent:
+//   upward:   parent node j  = sum_c sum_k child_mat[c][k][j] * child_c node k
+//   downward: child_c node k += sum_l child_mat[c][k][l] * parent node l
+//
+// One CTA owns the subtree of depth D below one panel of level r and keeps
+// the strengths (upward) or target values (downward) of all its levels in
+// shared memory, so a pass over the whole tree takes ceil((L-1)/3) launches.
+//
+// Upward, mode 0 (the step): when the subtree reaches the leaves, the leaf
+// sources are computed here (bve_disp_update, src/bve_time_step.cpp:69-105,
+// with the forcing copy and base_pots folded in); the non-leaf proxies of the
+// subtree get their displaced positions (bve_disp_interp,
+// src/bve_time_step.cpp:107-160, leaf row and BLI basis precomputed on the
+// host); strengths are anterpolated level by level; in mixed precision the
+// packed float4 sources are written for every panel the CTA owns.
+// Mode 1 (sbslpm_upward_pass): leaf strengths area * pots, positions untouched.
+// Mode 2 (treecode): leaf strengths already anterpolated into src, fixed
+// proxy positions untouched, mixed packing as in mode 0.
+
+__device__ __forceinline__ int subtree_first(int level, int root_rel, int k) {
+  return level_start(level + k) + (root_rel << (2 * k));
+}
+
+__device__ __forceinline__ void nonleaf_position(const StepGeom& g, long i, int stage, double dt_s,
+                                                 const double* __restrict__ vprev, double& px, double& py,
+                                                 double& pz) {
+  const long pn = (long)g.panels * g.q, ln = (long)g.leaves * g.q;
+  px = g.px[i];
+  py = g.px[pn + i];
+  pz = g.px[2 * pn + i];
   if (stage > 0) {
     const double* b = g.il_basis + i * g.q;
     const long row = (long)g.il_row[i] * g.q;
@@ -135,93 +182,150 @@ __global__ void k_nonleaf_sources(StepGeom g, int stage, double dt_s, const doub
     pz += az;
   }
   project_to_sphere(px, py, pz);
-  src[i] = make_double4(px, py, pz, 0.0);
 }
 
-// Piecewise API: sources from explicit displacements and strengths
-// (the inputs of bve_vel_interactions).
-__global__ void k_sources_from_disp(StepGeom g, const double* __restrict__ dx, const double* __restrict__ dy,
-                                    const double* __restrict__ dz, const double* __restrict__ s,
-                                    double4* __restrict__ src) {
-  long pn = (long)g.panels * g.q;
-  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (i >= pn) return;
-  double px = g.px[i] + dx[i], py = g.px[pn + i] + dy[i], pz = g.px[2 * pn + i] + dz[i];
-  project_to_sphere(px, py, pz);
-  src[i] = make_double4(px, py, pz, s[i]);
-}
+__global__ void k_upward_subtree(StepGeom g, int r, int D, int mode, int stage, double dt_s,
+                                 const double* __restrict__ vprev, const double* __restrict__ x,
+                                 const double* __restrict__ y, const double* __restrict__ z,
+                                 const double* __restrict__ vors, const double* __restrict__ area,
+                                 double4* __restrict__ src, int mixed) {
+  extern __shared__ double sh[];  // strengths of levels r..r+D, level k at offset q*(4^k-1)/3
+  const int q = g.q, root_rel = blockIdx.x;
+  const bool leaves_here = (r + D == g.levels - 1);
+  const long ln = (long)g.leaves * g.q, pn = (long)g.panels * g.q;
+  auto lvl = [&](int k) { return sh + q * (((1 << (2 * k)) - 1) / 3); };
 
-__global__ void k_leaf_strength(StepGeom g, const double* __restrict__ area, const double* __restrict__ pots,
-                                double4* __restrict__ src) {
-  long n = (long)g.leaves * g.q;
-  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  src[(long)g.offset * g.q + i].w = area[i] * pots[i];
-}
-
-__global__ void k_copy_strength(StepGeom g, const double4* __restrict__ src, double* __restrict__ out) {
-  long pn = (long)g.panels * g.q;
-  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (i >= pn) return;
-  out[i] = src[i].w;
-}
-
-// ---------------------------------------------------------------------------
-// Tree passes (upward_pass / downward_pass_3, src/fmm_funcs.cpp:341-392).
-// child_mat[c][k][l] is the BLI basis of parent node l at child c's node k;
-// the uniform quadtree makes it the same matrix for every parent.
-
-// Parent node j = sum_c sum_k child_mat[c][k][j] * child_c node k
-// (child_to_parent, src/fmm_funcs_impl.hpp:36-71).
-__global__ void k_upward_level(StepGeom g, int parent_level, double4* __restrict__ src) {
-  int lo = level_start(parent_level), cnt = 6 << (2 * parent_level);
-  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (i >= (long)cnt * g.q) return;
-  int p = lo + (int)(i / g.q), j = (int)(i % g.q);
-  int clo = level_start(parent_level + 1) + 4 * (p - lo);
-  double acc = 0;
-  for (int c = 0; c < 4; c++) {
-    const double4* cs = src + (long)(clo + c) * g.q;
-    const double* m = g.child_mat + (long)c * g.q * g.q + j;
-    for (int k = 0; k < g.q; k++) acc = fma(__ldg(m + (long)k * g.q), cs[k].w, acc);
+  // bottom level of the subtree: leaf sources, or strengths computed by the previous launch
+  {
+    const int first = subtree_first(r, root_rel, D), npts = (1 << (2 * D)) * q;
+    double* bot = lvl(D);
+    for (int t = threadIdx.x; t < npts; t += blockDim.x) {
+      const long o = (long)first * q + t;
+      if (leaves_here && mode != 2) {
+        const long i = o - (long)g.offset * q;
+        double w;
+        if (mode == 1) {
+          w = area[i] * vors[i];
+          src[o].w = w;
+        } else {
+          double px = g.px[o], py = g.px[pn + o], pz = g.px[2 * pn + o];
+          if (stage == 0) {
+            w = area[i] * vors[i];
+          } else {
+            double vx = vprev[i], vy = vprev[ln + i], vz = vprev[2 * ln + i];
+            double xx = x[i] + vx * dt_s, yy = y[i] + vy * dt_s, zz = z[i] + vz * dt_s;
+            project_to_sphere(xx, yy, zz);
+            double dvor = vors[i] + 2 * g.omega * z[i] - 2 * g.omega * zz;
+            w = area[i] * dvor;
+            px += dt_s * vx;
+            py += dt_s * vy;
+            pz += dt_s * vz;
+          }
+          project_to_sphere(px, py, pz);
+          src[o] = make_double4(px, py, pz, w);
+        }
+        bot[t] = w;
+      } else {
+        bot[t] = src[o].w;
+      }
+    }
   }
-  src[(long)p * g.q + j].w = acc;
+  // displaced positions of the subtree's non-leaf proxies (levels r..r+D-1)
+  if (mode == 0) {
+    for (int k = 0; k < D; k++) {
+      const int first = subtree_first(r, root_rel, k), npts = (1 << (2 * k)) * q;
+      for (int t = threadIdx.x; t < npts; t += blockDim.x) {
+        const long i = (long)first * q + t;
+        double px, py, pz;
+        nonleaf_position(g, i, stage, dt_s, vprev, px, py, pz);
+        src[i] = make_double4(px, py, pz, 0.0);
+      }
+    }
+  }
+  __syncthreads();
+  // anterpolation, deepest parents first
+  for (int k = D - 1; k >= 0; k--) {
+    const double* ch = lvl(k + 1);
+    double* pa = lvl(k);
+    const int npts = (1 << (2 * k)) * q, first = subtree_first(r, root_rel, k);
+    for (int t = threadIdx.x; t < npts; t += blockDim.x) {
+      const int p = t / q, j = t % q;
+      double acc = 0;
+      for (int c = 0; c < 4; c++) {
+        const double* cs = ch + (4 * p + c) * q;
+        const double* m = g.child_mat + (long)c * q * q + j;
+        for (int kk = 0; kk < q; kk++) acc = fma(__ldg(m + (long)kk * q), cs[kk], acc);
+      }
+      pa[t] = acc;
+      src[(long)first * q + t].w = acc;
+    }
+    __syncthreads();
+  }
+  // mixed precision: float4 sources relative to the panel centre, for every panel this CTA owns
+  if (mixed && mode != 1) {
+    const int kmax = leaves_here ? D : D - 1;
+    for (int k = 0; k <= kmax; k++) {
+      const int first = subtree_first(r, root_rel, k), npts = (1 << (2 * k)) * q;
+      for (int t = threadIdx.x; t < npts; t += blockDim.x) {
+        const long i = (long)first * q + t;
+        const double* cc = g.pd_centre + 4 * (i / q);
+        double4 sv = src[i];
+        g.srcf[i] = make_float4((float)(sv.x - cc[0]), (float)(sv.y - cc[1]), (float)(sv.z - cc[2]), (float)sv.w);
+      }
+    }
+  }
 }
 
-// Child node k += sum_l child_mat[c][k][l] * parent node l (parent_to_child_3,
-// src/fmm_funcs_impl.hpp:123-172).  At the leaf level the result goes to the
-// stage velocity (child_panel_copy, src/fmm_funcs_impl.hpp:174-188).
-__global__ void k_downward_level(StepGeom g, int child_level, double* __restrict__ tgt,
-                                 double* __restrict__ leaf_out) {
-  int lo = level_start(child_level), cnt = 6 << (2 * child_level);
-  long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (i >= (long)cnt * g.q) return;
-  int ch = lo + (int)(i / g.q), k = (int)(i % g.q);
-  int rel = ch - lo, c = rel & 3;
-  int par = level_start(child_level - 1) + (rel >> 2);
-  long pn = (long)g.panels * g.q;
-  const double* m = g.child_mat + ((long)c * g.q + k) * g.q;
-  const double* t0 = tgt + (long)par * g.q;
-  double a0 = 0, a1 = 0, a2 = 0;
-  for (int l = 0; l < g.q; l++) {
-    double ml = __ldg(m + l);
-    a0 = fma(ml, t0[l], a0);
-    a1 = fma(ml, t0[pn + l], a1);
-    a2 = fma(ml, t0[2 * pn + l], a2);
+// Downward: the root's targets are final; children of levels r+1..r+D get
+// own + interpolated parent values.  Leaves go to leaf_out when given (the
+// stage velocity), intermediate levels stay in shared memory, and the
+// deepest non-leaf level is written back for the next launch.
+__global__ void k_downward_subtree(StepGeom g, int r, int D, double* __restrict__ tgt,
+                                   double* __restrict__ leaf_out) {
+  extern __shared__ double sh[];  // 3 fields x levels r..r+D
+  const int q = g.q, root_rel = blockIdx.x;
+  const long pn = (long)g.panels * g.q, ln = (long)g.leaves * g.q;
+  const int per_field = q * (((1 << (2 * (D + 1))) - 1) / 3);
+  auto lvl = [&](int f, int k) { return sh + f * per_field + q * (((1 << (2 * k)) - 1) / 3); };
+  {
+    const int first = subtree_first(r, root_rel, 0);
+    for (int t = threadIdx.x; t < q; t += blockDim.x)
+      for (int f = 0; f < 3; f++) lvl(f, 0)[t] = tgt[f * pn + (long)first * q + t];
   }
-  long o = (long)ch * g.q + k;
-  a0 += tgt[o];
-  a1 += tgt[pn + o];
-  a2 += tgt[2 * pn + o];
-  if (leaf_out != nullptr) {
-    long ln = (long)g.leaves * g.q, lo2 = o - (long)g.offset * g.q;
-    leaf_out[lo2] = a0;
-    leaf_out[ln + lo2] = a1;
-    leaf_out[2 * ln + lo2] = a2;
-  } else {
-    tgt[o] = a0;
-    tgt[pn + o] = a1;
-    tgt[2 * pn + o] = a2;
+  __syncthreads();
+  for (int k = 1; k <= D; k++) {
+    const int level = r + k, npts = (1 << (2 * k)) * q, first = subtree_first(r, root_rel, k);
+    const bool is_leaf = (level == g.levels - 1);
+    for (int t = threadIdx.x; t < npts; t += blockDim.x) {
+      const int pc = t / q, kk = t % q, c = pc & 3, pp = pc >> 2;
+      const double* m = g.child_mat + ((long)c * q + kk) * q;
+      const double *t0 = lvl(0, k - 1) + pp * q, *t1 = lvl(1, k - 1) + pp * q, *t2 = lvl(2, k - 1) + pp * q;
+      double a0 = 0, a1 = 0, a2 = 0;
+      for (int l = 0; l < q; l++) {
+        double ml = __ldg(m + l);
+        a0 = fma(ml, t0[l], a0);
+        a1 = fma(ml, t1[l], a1);
+        a2 = fma(ml, t2[l], a2);
+      }
+      const long o = (long)first * q + t;
+      a0 += tgt[o];
+      a1 += tgt[pn + o];
+      a2 += tgt[2 * pn + o];
+      lvl(0, k)[t] = a0;
+      lvl(1, k)[t] = a1;
+      lvl(2, k)[t] = a2;
+      if (is_leaf && leaf_out != nullptr) {
+        const long lo = o - (long)g.offset * q;
+        leaf_out[lo] = a0;
+        leaf_out[ln + lo] = a1;
+        leaf_out[2 * ln + lo] = a2;
+      } else if (k == D || is_leaf || leaf_out == nullptr) {
+        tgt[o] = a0;
+        tgt[pn + o] = a1;
+        tgt[2 * pn + o] = a2;
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -246,7 +350,7 @@ struct WarpShape {
   static constexpr int STAGE = (S * Q > Q ? S * Q : Q);    // staged points per warp
 };
 
-template <int Q, bool ALL_LEAVES, bool ACCUM>
+template <int Q, bool ALL_LEAVES, bool GUARD>
 __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_interact64(StepGeom g, const double4* __restrict__ src,
                                                                     double* __restrict__ out, long out_stride) {
   using W = WarpShape<Q>;
@@ -288,7 +392,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_interact64(StepGeom g, 
       if (active && e + h < e1) {
         const double4* sp = &stage[warp][h * Q];
 #pragma unroll
-        for (int k = 0; k < Q; k++) pair64(tx, ty, tz, sp[k], g.eps, ax, ay, az);
+        for (int k = 0; k < Q; k++) pair64<GUARD>(tx, ty, tz, sp[k], g.eps, ax, ay, az);
       }
       __syncwarp();
     }
@@ -311,15 +415,9 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_interact64(StepGeom g, 
       double uz = kBiotSavart * (tx * ay - ty * ax);
       long o = ALL_LEAVES ? (long)blockIdx.y * 3 * out_stride + (long)tix * Q + j : (long)t * Q + j;
       long s = ALL_LEAVES ? out_stride : pn;
-      if (ACCUM) {
-        out[o] += ux;
-        out[s + o] += uy;
-        out[2 * s + o] += uz;
-      } else {
-        out[o] = ux;
-        out[s + o] = uy;
-        out[2 * s + o] = uz;
-      }
+      out[o] = ux;
+      out[s + o] = uy;
+      out[2 * s + o] = uz;
     }
   } else {
     constexpr int TPL = W::TPL;
@@ -340,7 +438,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_interact64(StepGeom g, 
       for (int k = 0; k < Q; k++) {
         const double4 s = stage[warp][k];
 #pragma unroll
-        for (int r = 0; r < TPL; r++) pair64(tx[r], ty[r], tz[r], s, g.eps, ax[r], ay[r], az[r]);
+        for (int r = 0; r < TPL; r++) pair64<GUARD>(tx[r], ty[r], tz[r], s, g.eps, ax[r], ay[r], az[r]);
       }
       __syncwarp();
     }
@@ -353,15 +451,9 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_interact64(StepGeom g, 
       double uz = kBiotSavart * (tx[r] * ay[r] - ty[r] * ax[r]);
       long o = ALL_LEAVES ? (long)blockIdx.y * 3 * out_stride + (long)tix * Q + j : (long)t * Q + j;
       long s = ALL_LEAVES ? out_stride : pn;
-      if (ACCUM) {
-        out[o] += ux;
-        out[s + o] += uy;
-        out[2 * s + o] += uz;
-      } else {
-        out[o] = ux;
-        out[s + o] = uy;
-        out[2 * s + o] = uz;
-      }
+      out[o] = ux;
+      out[s + o] = uy;
+      out[2 * s + o] = uz;
     }
   }
 }
@@ -378,10 +470,9 @@ __global__ void k_pack_mixed(StepGeom g, const double4* __restrict__ src, float4
   srcf[i] = make_float4((float)(s.x - c[0]), (float)(s.y - c[1]), (float)(s.z - c[2]), (float)s.w);
 }
 
-template <int Q, bool ALL_LEAVES, bool ACCUM>
+template <int Q, bool ALL_LEAVES, bool GUARD>
 __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_interact32(StepGeom g, const float4* __restrict__ srcf,
                                                                     double* __restrict__ out, long out_stride) {
-  static_assert(Q <= 32, "mixed kernel handles q <= 32");
   using W = WarpShape<Q>;
   __shared__ float4 stage[kWarpsPerBlock][W::STAGE];
   __shared__ double red[kWarpsPerBlock][3][32];
@@ -401,69 +492,116 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_interact32(StepGeom g, 
     e0 = g.tgt_start[t];
     e1 = g.tgt_start[t + 1];
   }
-  const int h = lane / Q, j = lane % Q;
-  const bool active = h < W::S;
-  double tx = 0, ty = 0, tz = 0;
   const double* ct = g.pd_centre + 4 * (long)t;
   const double ctx = ct[0], cty = ct[1], ctz = ct[2];
-  float dtx = 0, dty = 0, dtz = 0;
-  if (active) {
-    long o = (long)t * Q + j;
-    tx = g.px[o];
-    ty = g.px[pn + o];
-    tz = g.px[2 * pn + o];
-    dtx = (float)(tx - ctx);
-    dty = (float)(ty - cty);
-    dtz = (float)(tz - ctz);
-  }
   const float eps = (float)g.eps;
-  double ax = 0, ay = 0, az = 0;
-  for (int e = e0; e < e1; e += W::S) {
-    int sp = 0;
-    if (active && e + h < e1) {
-      sp = ALL_LEAVES ? g.offset + e + h : __ldg(g.src_panel + e + h);
-      stage[warp][h * Q + j] = srcf[(long)sp * Q + j];
+  if constexpr (Q <= 32) {
+    const int h = lane / Q, j = lane % Q;
+    const bool active = h < W::S;
+    double tx = 0, ty = 0, tz = 0;
+    float dtx = 0, dty = 0, dtz = 0;
+    if (active) {
+      long o = (long)t * Q + j;
+      tx = g.px[o];
+      ty = g.px[pn + o];
+      tz = g.px[2 * pn + o];
+      dtx = (float)(tx - ctx);
+      dty = (float)(ty - cty);
+      dtz = (float)(tz - ctz);
     }
-    __syncwarp();
-    if (active && e + h < e1) {
-      const double* cs = g.pd_centre + 4 * (long)sp;
-      float bx = (float)(cs[0] - ctx) - dtx, by = (float)(cs[1] - cty) - dty, bz = (float)(cs[2] - ctz) - dtz;
-      float fx = 0.f, fy = 0.f, fz = 0.f;
-      const float4* sb = &stage[warp][h * Q];
-#pragma unroll
-      for (int k = 0; k < Q; k++) pair32(bx, by, bz, sb[k], eps, fx, fy, fz);
-      ax += fx;
-      ay += fy;
-      az += fz;
-    }
-    __syncwarp();
-  }
-  if (W::S > 1) {
-    red[warp][0][lane] = ax;
-    red[warp][1][lane] = ay;
-    red[warp][2][lane] = az;
-    __syncwarp();
-    if (h == 0)
-      for (int hh = 1; hh < W::S; hh++) {
-        ax += red[warp][0][hh * Q + j];
-        ay += red[warp][1][hh * Q + j];
-        az += red[warp][2][hh * Q + j];
+    double ax = 0, ay = 0, az = 0;
+    for (int e = e0; e < e1; e += W::S) {
+      int sp = 0;
+      if (active && e + h < e1) {
+        sp = ALL_LEAVES ? g.offset + e + h : __ldg(g.src_panel + e + h);
+        stage[warp][h * Q + j] = srcf[(long)sp * Q + j];
       }
-  }
-  if (h == 0) {
-    double ux = kBiotSavart * (ty * az - tz * ay);
-    double uy = kBiotSavart * (tz * ax - tx * az);
-    double uz = kBiotSavart * (tx * ay - ty * ax);
-    long o = ALL_LEAVES ? (long)blockIdx.y * 3 * out_stride + (long)tix * Q + j : (long)t * Q + j;
-    long s = ALL_LEAVES ? out_stride : pn;
-    if (ACCUM) {
-      out[o] += ux;
-      out[s + o] += uy;
-      out[2 * s + o] += uz;
-    } else {
-      out[o] = ux;
-      out[s + o] = uy;
-      out[2 * s + o] = uz;
+      __syncwarp();
+      if (active && e + h < e1) {
+        const double* cs = g.pd_centre + 4 * (long)sp;
+        float bx = (float)(cs[0] - ctx) - dtx, by = (float)(cs[1] - cty) - dty, bz = (float)(cs[2] - ctz) - dtz;
+        float fx = 0.f, fy = 0.f, fz = 0.f;
+        const float4* sb = &stage[warp][h * Q];
+#pragma unroll
+        for (int k = 0; k < Q; k++) pair32<GUARD>(bx, by, bz, sb[k], eps, fx, fy, fz);
+        ax += fx;
+        ay += fy;
+        az += fz;
+      }
+      __syncwarp();
+    }
+    if (W::S > 1) {
+      red[warp][0][lane] = ax;
+      red[warp][1][lane] = ay;
+      red[warp][2][lane] = az;
+      __syncwarp();
+      if (h == 0)
+        for (int hh = 1; hh < W::S; hh++) {
+          ax += red[warp][0][hh * Q + j];
+          ay += red[warp][1][hh * Q + j];
+          az += red[warp][2][hh * Q + j];
+        }
+    }
+    if (h == 0) {
+      long o = ALL_LEAVES ? (long)blockIdx.y * 3 * out_stride + (long)tix * Q + j : (long)t * Q + j;
+      long s = ALL_LEAVES ? out_stride : pn;
+      out[o] = kBiotSavart * (ty * az - tz * ay);
+      out[s + o] = kBiotSavart * (tz * ax - tx * az);
+      out[2 * s + o] = kBiotSavart * (tx * ay - ty * ax);
+    }
+  } else {
+    constexpr int TPL = W::TPL;
+    double tx[TPL], ty[TPL], tz[TPL], ax[TPL], ay[TPL], az[TPL];
+    float dtx[TPL], dty[TPL], dtz[TPL];
+#pragma unroll
+    for (int r = 0; r < TPL; r++) {
+      int j = lane + 32 * r;
+      long o = (long)t * Q + (j < Q ? j : 0);
+      tx[r] = g.px[o];
+      ty[r] = g.px[pn + o];
+      tz[r] = g.px[2 * pn + o];
+      dtx[r] = (float)(tx[r] - ctx);
+      dty[r] = (float)(ty[r] - cty);
+      dtz[r] = (float)(tz[r] - ctz);
+      ax[r] = ay[r] = az[r] = 0;
+    }
+    for (int e = e0; e < e1; e++) {
+      const int sp = ALL_LEAVES ? g.offset + e : __ldg(g.src_panel + e);
+      const long sb = (long)sp * Q;
+      for (int k = lane; k < Q; k += 32) stage[warp][k] = srcf[sb + k];
+      const double* cs = g.pd_centre + 4 * (long)sp;
+      const float bx0 = (float)(cs[0] - ctx), by0 = (float)(cs[1] - cty), bz0 = (float)(cs[2] - ctz);
+      float fx[TPL], fy[TPL], fz[TPL], bx[TPL], by[TPL], bz[TPL];
+#pragma unroll
+      for (int r = 0; r < TPL; r++) {
+        fx[r] = fy[r] = fz[r] = 0.f;
+        bx[r] = bx0 - dtx[r];
+        by[r] = by0 - dty[r];
+        bz[r] = bz0 - dtz[r];
+      }
+      __syncwarp();
+      for (int k = 0; k < Q; k++) {
+        const float4 s = stage[warp][k];
+#pragma unroll
+        for (int r = 0; r < TPL; r++) pair32<GUARD>(bx[r], by[r], bz[r], s, eps, fx[r], fy[r], fz[r]);
+      }
+#pragma unroll
+      for (int r = 0; r < TPL; r++) {
+        ax[r] += fx[r];
+        ay[r] += fy[r];
+        az[r] += fz[r];
+      }
+      __syncwarp();
+    }
+#pragma unroll
+    for (int r = 0; r < TPL; r++) {
+      int j = lane + 32 * r;
+      if (j >= Q) continue;
+      long o = ALL_LEAVES ? (long)blockIdx.y * 3 * out_stride + (long)tix * Q + j : (long)t * Q + j;
+      long s = ALL_LEAVES ? out_stride : pn;
+      out[o] = kBiotSavart * (ty[r] * az[r] - tz[r] * ay[r]);
+      out[s + o] = kBiotSavart * (tz[r] * ax[r] - tx[r] * az[r]);
+      out[2 * s + o] = kBiotSavart * (tx[r] * ay[r] - ty[r] * ax[r]);
     }
   }
 }
@@ -627,7 +765,7 @@ __global__ void __launch_bounds__(kDirectThreads)
     tile[threadIdx.x] = k < s1 ? make_double4(sx[k], sy[k], sz[k], sw[k]) : make_double4(0, 0, 0, 0);
     __syncthreads();
     int cnt = (int)min((long)kDirectThreads, s1 - b);
-    for (int m = 0; m < cnt; m++) pair64(x, y, z, tile[m], eps, ax, ay, az);
+    for (int m = 0; m < cnt; m++) pair64<true>(x, y, z, tile[m], eps, ax, ay, az);
     __syncthreads();
   }
   if (i < nt) {
@@ -670,7 +808,7 @@ __global__ void __launch_bounds__(kDirectThreads)
     float bx = (float)(scx - tcx) - dtx, by = (float)(scy - tcy) - dty, bz = (float)(scz - tcz) - dtz;
     float fx = 0, fy = 0, fz = 0;
     int cnt = (int)min((long)kDirectThreads, s1 - b);
-    for (int m = 0; m < cnt; m++) pair32(bx, by, bz, tile[m], feps, fx, fy, fz);
+    for (int m = 0; m < cnt; m++) pair32<true>(bx, by, bz, tile[m], feps, fx, fy, fz);
     ax += fx;
     ay += fy;
     az += fz;
@@ -734,22 +872,10 @@ void launch_leaf_sources(const StepGeom& g, int stage, double dt_s, const double
   SB_LAUNCH(k_leaf_sources, blocks_for(n, 256), 256, 0, st, g, stage, dt_s, vprev, x, y, z, vors, area, src);
 }
 
-void launch_nonleaf_sources(const StepGeom& g, int stage, double dt_s, const double* vprev, double4* src,
-                            cudaStream_t st) {
-  long n = (long)g.offset * g.q;
-  if (n == 0) return;
-  SB_LAUNCH(k_nonleaf_sources, blocks_for(n, 256), 256, 0, st, g, stage, dt_s, vprev, src);
-}
-
 void launch_sources_from_disp(const StepGeom& g, const double* dx, const double* dy, const double* dz,
                               const double* s, double4* src, cudaStream_t st) {
   long n = (long)g.panels * g.q;
   SB_LAUNCH(k_sources_from_disp, blocks_for(n, 256), 256, 0, st, g, dx, dy, dz, s, src);
-}
-
-void launch_leaf_strength(const StepGeom& g, const double* area, const double* pots, double4* src, cudaStream_t st) {
-  long n = (long)g.leaves * g.q;
-  SB_LAUNCH(k_leaf_strength, blocks_for(n, 256), 256, 0, st, g, area, pots, src);
 }
 
 void launch_copy_strength(const StepGeom& g, const double4* src, double* out, cudaStream_t st) {
@@ -757,41 +883,84 @@ void launch_copy_strength(const StepGeom& g, const double4* src, double* out, cu
   SB_LAUNCH(k_copy_strength, blocks_for(n, 256), 256, 0, st, g, src, out);
 }
 
-void launch_upward_level(const StepGeom& g, int parent_level, double4* src, cudaStream_t st) {
-  long n = (long)(6 << (2 * parent_level)) * g.q;
-  SB_LAUNCH(k_upward_level, blocks_for(n, 128), 128, 0, st, g, parent_level, src);
+// Subtree depth per launch: 3 levels (85 panels) when the shared memory
+// allows, fewer for large q.
+static int subtree_depth(int q, int fields) {
+  for (int D = 3; D >= 1; D--)
+    if ((long)q * fields * 8 * (((1L << (2 * (D + 1))) - 1) / 3) <= 160 * 1024) return D;
+  return 1;
 }
 
-void launch_downward_level(const StepGeom& g, int child_level, double* tgt, double* leaf_out, cudaStream_t st) {
-  long n = (long)(6 << (2 * child_level)) * g.q;
-  SB_LAUNCH(k_downward_level, blocks_for(n, 128), 128, 0, st, g, child_level, tgt, leaf_out);
+static size_t subtree_smem(int q, int fields, int D) {
+  return (size_t)q * fields * 8 * (((1L << (2 * (D + 1))) - 1) / 3);
+}
+
+void launch_upward_fused(const StepGeom& g, int mode, int stage, double dt_s, const double* vprev, const double* x,
+                         const double* y, const double* z, const double* vors, const double* area, double4* src,
+                         bool mixed, cudaStream_t st) {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_upward_subtree, cudaFuncAttributeMaxDynamicSharedMemorySize, 164 * 1024);
+    attr = true;
+  }
+  const int Dmax = subtree_depth(g.q, 1);
+  int r = g.levels - 1;  // the bottom of the next subtree
+  bool first = true;
+  while (first || r > 0) {
+    int D = first ? (r < Dmax ? r : Dmax) : (r < Dmax ? r : Dmax);
+    int root = r - D;
+    SB_LAUNCH(k_upward_subtree, (unsigned)(6 << (2 * root)), 256, subtree_smem(g.q, 1, D), st, g, root, D, mode,
+              stage, dt_s, vprev, x, y, z, vors, area, src, mixed ? 1 : 0);
+    r = root;
+    first = false;
+  }
+}
+
+void launch_downward_fused(const StepGeom& g, double* tgt, double* leaf_out, cudaStream_t st) {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_downward_subtree, cudaFuncAttributeMaxDynamicSharedMemorySize, 164 * 1024);
+    attr = true;
+  }
+  const int Dmax = subtree_depth(g.q, 3);
+  int r = 0;
+  while (r < g.levels - 1) {
+    int D = (g.levels - 1 - r) < Dmax ? (g.levels - 1 - r) : Dmax;
+    SB_LAUNCH(k_downward_subtree, (unsigned)(6 << (2 * r)), 256, subtree_smem(g.q, 3, D), st, g, r, D, tgt,
+              leaf_out);
+    r += D;
+  }
 }
 
 namespace {
-template <int Q>
-void interact_q(const StepGeom& g, int precision, const double4* src, double* out, bool accumulate, bool all_leaves,
-                int groups, long out_stride, cudaStream_t st, bool pack = true) {
+template <int Q, bool GUARD>
+void interact_qg(const StepGeom& g, int precision, const double4* src, double* out, bool all_leaves, int groups,
+                 long out_stride, cudaStream_t st, bool pack) {
   int tp = all_leaves ? g.leaves : g.panels;
   dim3 grid(blocks_for(tp, kWarpsPerBlock), all_leaves ? groups : 1);
   if (precision == SBSLPM_MIXED) {
-    if constexpr (Q <= 32) {
-      long pn = (long)g.panels * g.q;
-      if (pack) SB_LAUNCH(k_pack_mixed, blocks_for(pn, 256), 256, 0, st, g, src, g.srcf);
-      if (all_leaves)
-        SB_LAUNCH((k_interact32<Q, true, false>), grid, 32 * kWarpsPerBlock, 0, st, g, g.srcf, out, out_stride);
-      else if (accumulate)
-        SB_LAUNCH((k_interact32<Q, false, true>), grid, 32 * kWarpsPerBlock, 0, st, g, g.srcf, out, out_stride);
-      else
-        SB_LAUNCH((k_interact32<Q, false, false>), grid, 32 * kWarpsPerBlock, 0, st, g, g.srcf, out, out_stride);
-      return;
-    }
+    long pn = (long)g.panels * g.q;
+    if (pack) SB_LAUNCH(k_pack_mixed, blocks_for(pn, 256), 256, 0, st, g, src, g.srcf);
+    if (all_leaves)
+      SB_LAUNCH((k_interact32<Q, true, GUARD>), grid, 32 * kWarpsPerBlock, 0, st, g, g.srcf, out, out_stride);
+    else
+      SB_LAUNCH((k_interact32<Q, false, GUARD>), grid, 32 * kWarpsPerBlock, 0, st, g, g.srcf, out, out_stride);
+    return;
   }
   if (all_leaves)
-    SB_LAUNCH((k_interact64<Q, true, false>), grid, 32 * kWarpsPerBlock, 0, st, g, src, out, out_stride);
-  else if (accumulate)
-    SB_LAUNCH((k_interact64<Q, false, true>), grid, 32 * kWarpsPerBlock, 0, st, g, src, out, out_stride);
+    SB_LAUNCH((k_interact64<Q, true, GUARD>), grid, 32 * kWarpsPerBlock, 0, st, g, src, out, out_stride);
   else
-    SB_LAUNCH((k_interact64<Q, false, false>), grid, 32 * kWarpsPerBlock, 0, st, g, src, out, out_stride);
+    SB_LAUNCH((k_interact64<Q, false, GUARD>), grid, 32 * kWarpsPerBlock, 0, st, g, src, out, out_stride);
+}
+
+// The coincident-point guard is compiled in only when kernel_eps = 0.
+template <int Q>
+void interact_q(const StepGeom& g, int precision, const double4* src, double* out, bool, bool all_leaves,
+                int groups, long out_stride, cudaStream_t st, bool pack = true) {
+  if (g.eps > 0)
+    interact_qg<Q, false>(g, precision, src, out, all_leaves, groups, out_stride, st, pack);
+  else
+    interact_qg<Q, true>(g, precision, src, out, all_leaves, groups, out_stride, st, pack);
 }
 
 void interact_dispatch(const StepGeom& g, int precision, const double4* src, double* out, bool accumulate,

@@ -29,16 +29,36 @@ struct StepGeom {
   unsigned* err;              // device error word
 };
 
+// Treecode with decoupled proxy degree (bltc_kernels.cu).  The treecode tree
+// itself is described by a StepGeom over its panels with q = (n+1)^2 proxies.
+struct TreeGeom {
+  int n;                  // proxy degree
+  int npl;                // particles per treecode leaf
+  long N;                 // particles
+  double eps, omega;
+  const double* lx;       // [npl][n+1]: leaf-box BLI basis of each particle's xi (same for every leaf)
+  const double* ly;       // [npl][n+1]: the same for eta
+  const double* fbounds;  // [tree panels][4]: min_xi, max_xi, min_eta, max_eta (radians)
+  const int* fface;       // [tree panels]
+  const int* near_start;  // [tree leaves + 1]: CSR of near leaf pairs by target leaf
+  const int* near_src;    // source leaf (relative to the first leaf)
+};
+
 // Launch wrappers (stream-ordered).
 void launch_leaf_sources(const StepGeom& g, int stage, double dt_s, const double* vprev, const double* x,
                          const double* y, const double* z, const double* vors, const double* area, double4* src,
                          cudaStream_t st);
-void launch_nonleaf_sources(const StepGeom& g, int stage, double dt_s, const double* vprev, double4* src,
-                            cudaStream_t st);
-void launch_upward_level(const StepGeom& g, int parent_level, double4* src, cudaStream_t st);
+// Fused passes: whole tree in ceil((levels-1)/3) launches.  mode 0 = the
+// step's sources (leaf sources, non-leaf positions, strengths, mixed
+// packing); mode 1 = strengths area*pots only; mode 2 = leaf strengths
+// already in src (treecode proxies), mixed packing.
+void launch_upward_fused(const StepGeom& g, int mode, int stage, double dt_s, const double* vprev, const double* x,
+                         const double* y, const double* z, const double* vors, const double* area, double4* src,
+                         bool mixed, cudaStream_t st);
+// leaf_out == nullptr: leaf values stay in tgt.
+void launch_downward_fused(const StepGeom& g, double* tgt, double* leaf_out, cudaStream_t st);
 void launch_interactions(const StepGeom& g, int precision, const double4* src, double* tgt, bool accumulate,
                          cudaStream_t st);
-void launch_downward_level(const StepGeom& g, int child_level, double* tgt, double* leaf_out, cudaStream_t st);
 void launch_direct_leaves(const StepGeom& g, int precision, const double4* src, double* vout, double* partial,
                           int groups, cudaStream_t st);
 void launch_depart_remap(const StepGeom& g, const BliTable* tab, const double* x, const double* y, const double* z,
@@ -48,7 +68,6 @@ void launch_depart_remap(const StepGeom& g, const BliTable* tab, const double* x
 // Raw-array helpers for the piecewise API.
 void launch_sources_from_disp(const StepGeom& g, const double* dx, const double* dy, const double* dz,
                               const double* source, double4* src, cudaStream_t st);
-void launch_leaf_strength(const StepGeom& g, const double* area, const double* pots, double4* src, cudaStream_t st);
 void launch_copy_strength(const StepGeom& g, const double4* src, double* out, cudaStream_t st);
 
 // Stand-alone direct sums (no tree).
@@ -64,6 +83,14 @@ void launch_interactions_only(const StepGeom& g, int precision, const double4* s
 void launch_pack_mixed(const StepGeom& g, const double4* src, cudaStream_t st);
 // FMA-chain throughput probe: kind 0 float32, 1 float64; iters per thread.
 void launch_fma_probe(int kind, int blocks, int iters, float* out32, double* out64, cudaStream_t st);
+
+void launch_bltc_sources(const TreeGeom& tg, const StepGeom& fg, const BliTable& tab, int stage, double dt_s,
+                         const double* vprev, const double* x, const double* y, const double* z, const double* vors,
+                         const double* area, double4* psrc, float4* psrcf, double4* proxy, bool mixed,
+                         cudaStream_t st);
+void launch_bltc_near(const TreeGeom& tg, const StepGeom& fg, int precision, const double* x, const double* y,
+                      const double* z, const double4* psrc, const float4* psrcf, double* v, cudaStream_t st);
+void launch_bltc_to_particles(const TreeGeom& tg, const StepGeom& fg, const double* tgt, double* v, cudaStream_t st);
 
 // Counts every kernel launched through the wrappers above.
 long& launch_counter();

@@ -61,6 +61,21 @@ struct sbslpm_ctx {
   GraphKey graph_key{};
   long launches_per_step = 0;
 
+  // treecode with decoupled proxy degree (proxy_degree > 0)
+  bool tree = false;
+  int Lf = 0, n = 0, qx = 0, Pf = 0, Af = 0, npl = 0;
+  long n_near = 0, n_cc = 0;
+  std::vector<sbslpm_panel> fpanels;
+  double *fpx = nullptr, *fchild = nullptr, *fcentre = nullptr, *flx = nullptr, *fly = nullptr, *fbounds = nullptr;
+  int *fface = nullptr, *near_start = nullptr, *near_src = nullptr, *cc_start = nullptr, *cc_src = nullptr;
+  double4 *fsrc = nullptr, *psrc = nullptr;
+  double* gx = nullptr;  // [3][particles]: the particle grid, for timing the near kernel alone
+  float4 *fsrcf = nullptr, *psrcf = nullptr;
+  double* ftgt = nullptr;
+  BliTable ftab{};
+  StepGeom fgeom{};
+  TreeGeom tgeom{};
+
   cudaStream_t stream() const { return user_stream_set ? user_stream : own_stream; }
 };
 
@@ -97,8 +112,16 @@ sbslpm_status validate(const sbslpm_config& c) {
     return set_last_error("velocity must be SBSLPM_VEL_FMM or SBSLPM_VEL_DIRECT"), SBSLPM_ERR_CONFIG;
   if (c.precision != SBSLPM_FP64 && c.precision != SBSLPM_MIXED)
     return set_last_error("precision must be SBSLPM_FP64 or SBSLPM_MIXED"), SBSLPM_ERR_CONFIG;
-  if (c.precision == SBSLPM_MIXED && (c.interp_degree + 1) * (c.interp_degree + 1) > 32)
-    return set_last_error("mixed precision pair kernels support interp_degree <= 4"), SBSLPM_ERR_CONFIG;
+  if (c.proxy_degree < 0 || c.proxy_degree > kMaxDegree)
+    return set_last_error("proxy_degree must be in 0..10"), SBSLPM_ERR_CONFIG;
+  if (c.proxy_degree > 0 && c.velocity == SBSLPM_VEL_FMM) {
+    const int qp = (c.interp_degree + 1) * (c.interp_degree + 1);
+    if (c.leaf_size < qp || c.leaf_size > 512 * 1024)
+      return set_last_error("leaf_size must hold at least one panel's points"), SBSLPM_ERR_CONFIG;
+    long npl = qp;
+    while (npl * 4 <= c.leaf_size) npl *= 4;
+    if (npl > 512) return set_last_error("treecode leaves hold at most 512 particles"), SBSLPM_ERR_CONFIG;
+  }
   if (!(c.kernel_eps >= 0) || !std::isfinite(c.dt) || !std::isfinite(c.omega))
     return set_last_error("kernel_eps, dt and omega must be finite (kernel_eps >= 0)"), SBSLPM_ERR_CONFIG;
   return SBSLPM_OK;
@@ -109,6 +132,12 @@ sbslpm_status precompute(sbslpm_ctx* c) {
   const int q = c->q, P = c->P, off = c->off, d = c->d;
   std::vector<double> interp;
   build_interp(d, false, interp);
+
+  for (int i = 0; i <= d; i++) {
+    c->tab.cosv[i] = d == 0 ? 0.0 : std::cos(kPi * i / d);
+    c->tab.w[i] = d == 0 ? 1.0 : (i == 0 ? 0.5 : (i == d ? 0.5 * std::pow(-1, i) : std::pow(-1, i)));
+  }
+  if (c->tree) return SBSLPM_OK;  // the treecode has its own set-up
 
   // proxy positions, exactly as the reference's interaction kernel places them
   std::vector<double> px((size_t)3 * P * q);
@@ -133,6 +162,7 @@ sbslpm_status precompute(sbslpm_ctx* c) {
     for (int k = 0; k < 3; k++) centre[4 * (size_t)p + k] = xyz[k];
   }
   SB_TRY(upload(&c->centre, centre));
+  if (c->cfg.velocity != SBSLPM_VEL_FMM) return SBSLPM_OK;
 
   // displacement interpolation at non-leaf proxies (bve_disp_interp,
   // src/bve_time_step.cpp:131-159): located leaf row and BLI basis
@@ -179,28 +209,163 @@ sbslpm_status precompute(sbslpm_ctx* c) {
   }
 
   // interaction list grouped by target panel, list order kept within a target
-  if (c->cfg.velocity == SBSLPM_VEL_FMM) {
-    std::vector<int> start(P + 1, 0), srcs(c->list.size());
-    for (const auto& e : c->list) start[e.target_panel + 1]++;
-    for (int p = 0; p < P; p++) start[p + 1] += start[p];
-    std::vector<int> fill(start.begin(), start.end() - 1);
-    for (const auto& e : c->list) srcs[fill[e.target_panel]++] = e.source_panel;
-    SB_TRY(upload(&c->tgt_start, start));
-    SB_TRY(upload(&c->src_panel, srcs));
+  std::vector<int> start(P + 1, 0), srcs(c->list.size());
+  for (const auto& e : c->list) start[e.target_panel + 1]++;
+  for (int p = 0; p < P; p++) start[p + 1] += start[p];
+  std::vector<int> fill(start.begin(), start.end() - 1);
+  for (const auto& e : c->list) srcs[fill[e.target_panel]++] = e.source_panel;
+  SB_TRY(upload(&c->tgt_start, start));
+  SB_TRY(upload(&c->src_panel, srcs));
+  return SBSLPM_OK;
+}
+
+// Treecode set-up: the quadtree truncated so that a leaf holds npl <=
+// leaf_size particles, degree-n proxies on every tree panel, the canonical
+// leaf-box basis of the particle grid, and the near / well-separated lists.
+sbslpm_status precompute_tree(sbslpm_ctx* c) {
+  const int qp = c->q, n = c->cfg.proxy_degree, n1 = n + 1;
+  int m = 0;
+  long npl = qp;
+  while (npl * 4 <= c->cfg.leaf_size && m < c->L - 1) {
+    npl *= 4;
+    m++;
+  }
+  c->tree = true;
+  c->n = n;
+  c->qx = n1 * n1;
+  c->npl = (int)npl;
+  c->Lf = c->L - m;
+  c->Pf = sbslpm_panel_count(c->Lf);
+  c->Af = sbslpm_leaf_count(c->Lf);
+  build_panels(c->Lf, c->fpanels);
+  const int Pf = c->Pf, Af = c->Af, offf = Pf - Af, qx = c->qx;
+  std::vector<double> interp_n;
+  build_interp(n, false, interp_n);
+
+  std::vector<double> fpx((size_t)3 * Pf * qx), centre((size_t)4 * Pf, 0.0), bounds((size_t)4 * Pf);
+  std::vector<int> face(Pf);
+  const size_t pn = (size_t)Pf * qx;
+  for (int p = 0; p < Pf; p++) {
+    const sbslpm_panel& pp = c->fpanels[p];
+    for (int j = 0; j < qx; j++) {
+      double xyz[3];
+      proxy_point(pp, interp_n.data(), j, xyz);
+      for (int k = 0; k < 3; k++) fpx[k * pn + (size_t)p * qx + j] = xyz[k];
+    }
+    double xyz[3];
+    xyz_from_xieta(kPi / 4.0 * 0.5 * (pp.min_xi + pp.max_xi), kPi / 4.0 * 0.5 * (pp.min_eta + pp.max_eta), pp.face,
+                   xyz);
+    for (int k = 0; k < 3; k++) centre[4 * (size_t)p + k] = xyz[k];
+    bounds[4 * p + 0] = kPi / 4.0 * pp.min_xi;
+    bounds[4 * p + 1] = kPi / 4.0 * pp.max_xi;
+    bounds[4 * p + 2] = kPi / 4.0 * pp.min_eta;
+    bounds[4 * p + 3] = kPi / 4.0 * pp.max_eta;
+    face[p] = pp.face;
+  }
+  SB_TRY(upload(&c->fpx, fpx));
+  SB_TRY(upload(&c->fcentre, centre));
+  SB_TRY(upload(&c->fbounds, bounds));
+  SB_TRY(upload(&c->fface, face));
+
+  for (int i = 0; i <= n; i++) {
+    c->ftab.cosv[i] = n == 0 ? 0.0 : std::cos(kPi * i / n);
+    c->ftab.w[i] = n == 0 ? 1.0 : (i == 0 ? 0.5 : (i == n ? 0.5 * std::pow(-1, i) : std::pow(-1, i)));
+  }
+  unsigned err = 0;
+  if (c->Lf > 1) {
+    std::vector<double> mat((size_t)4 * qx * qx);
+    const sbslpm_panel& par = c->fpanels[0];
+    for (int ch = 0; ch < 4; ch++) {
+      const sbslpm_panel& k = c->fpanels[child_of(par, ch)];
+      double xo = kPi / 4.0 * 0.5 * (k.min_xi + k.max_xi), xs = kPi / 4.0 * 0.5 * (k.max_xi - k.min_xi);
+      double eo = kPi / 4.0 * 0.5 * (k.min_eta + k.max_eta), es = kPi / 4.0 * 0.5 * (k.max_eta - k.min_eta);
+      for (int i = 0; i < qx; i++)
+        host_bli(&mat[((size_t)ch * qx + i) * qx], interp_n[4 * i] * xs + xo, interp_n[4 * i + 1] * es + eo,
+                 par.min_xi * kPi / 4.0, par.max_xi * kPi / 4.0, par.min_eta * kPi / 4.0, par.max_eta * kPi / 4.0, n,
+                 err);
+    }
+    SB_TRY(upload(&c->fchild, mat));
   }
 
-  for (int i = 0; i <= d; i++) {
-    c->tab.cosv[i] = d == 0 ? 0.0 : std::cos(kPi * i / d);
-    c->tab.w[i] = d == 0 ? 1.0 : (i == 0 ? 0.5 : (i == d ? 0.5 * std::pow(-1, i) : std::pow(-1, i)));
+  // leaf-box basis of the particles of the first tree leaf (the same for every leaf)
+  {
+    std::vector<double> interp_p;
+    build_interp(c->d, false, interp_p);
+    std::vector<double> lx((size_t)npl * n1), ly((size_t)npl * n1);
+    const sbslpm_panel& leaf = c->fpanels[offf];
+    const double lo_x = kPi / 4.0 * leaf.min_xi, hi_x = kPi / 4.0 * leaf.max_xi;
+    const double lo_e = kPi / 4.0 * leaf.min_eta, hi_e = kPi / 4.0 * leaf.max_eta;
+    const int first_dp = level_start(c->L - 1);  // the first leaf's descendants come first
+    for (long k = 0; k < npl; k++) {
+      const sbslpm_panel& dp = c->panels[first_dp + k / qp];
+      const int j = (int)(k % qp);
+      double max_xi = kPi / 4.0 * dp.max_xi, min_xi = kPi / 4.0 * dp.min_xi;
+      double max_eta = kPi / 4.0 * dp.max_eta, min_eta = kPi / 4.0 * dp.min_eta;
+      double xi = 0.5 * (max_xi + min_xi) + 0.5 * (max_xi - min_xi) * interp_p[4 * j];
+      double eta = 0.5 * (max_eta + min_eta) + 0.5 * (max_eta - min_eta) * interp_p[4 * j + 1];
+      bli_1d(xi, lo_x, hi_x, n, c->ftab.cosv, c->ftab.w, &lx[k * n1], err);
+      bli_1d(eta, lo_e, hi_e, n, c->ftab.cosv, c->ftab.w, &ly[k * n1], err);
+    }
+    SB_TRY(upload(&c->flx, lx));
+    SB_TRY(upload(&c->fly, ly));
+  }
+  if (err) {
+    set_last_error("treecode set-up: a particle fell outside its leaf");
+    return SBSLPM_ERR_OUT_OF_PANEL;
+  }
+
+  // near leaf pairs (particle x particle) and well-separated pairs (proxy x proxy)
+  std::vector<sbslpm_interact_pair> list;
+  std::vector<char> near;
+  build_interactions_flagged(c->Lf, c->fpanels, c->cfg.fmm_theta, list, near);
+  std::vector<int> ns(Af + 1, 0), cs(Pf + 1, 0);
+  for (size_t e = 0; e < list.size(); e++) {
+    if (near[e]) ns[list[e].target_panel - offf + 1]++;
+    else cs[list[e].target_panel + 1]++;
+  }
+  for (int i = 0; i < Af; i++) ns[i + 1] += ns[i];
+  for (int i = 0; i < Pf; i++) cs[i + 1] += cs[i];
+  std::vector<int> nsrc(ns[Af]), csrc(cs[Pf]), nf(ns.begin(), ns.end() - 1), cf(cs.begin(), cs.end() - 1);
+  for (size_t e = 0; e < list.size(); e++) {
+    if (near[e]) nsrc[nf[list[e].target_panel - offf]++] = list[e].source_panel - offf;
+    else csrc[cf[list[e].target_panel]++] = list[e].source_panel;
+  }
+  c->n_near = ns[Af];
+  c->n_cc = cs[Pf];
+  c->list = list;
+  SB_TRY(upload(&c->near_start, ns));
+  SB_TRY(upload(&c->near_src, nsrc));
+  SB_TRY(upload(&c->cc_start, cs));
+  SB_TRY(upload(&c->cc_src, csrc));
+
+  // workspace; proxy positions are fixed, strengths are written every stage
+  const size_t N = (size_t)c->A * qp;
+  {
+    std::vector<double> interp_p, g(3 * N), area(N);
+    build_interp(c->d, false, interp_p);
+    build_points(c->L, c->d, c->panels, interp_p.data(), g.data(), g.data() + N, g.data() + 2 * N, area.data());
+    SB_TRY(upload(&c->gx, g));
+  }
+  SB_TRY(dalloc(&c->fsrc, pn));
+  std::vector<double4> init(pn);
+  for (size_t i = 0; i < pn; i++) init[i] = make_double4(fpx[i], fpx[pn + i], fpx[2 * pn + i], 0.0);
+  SB_CUDA(cudaMemcpy(c->fsrc, init.data(), sizeof(double4) * pn, cudaMemcpyHostToDevice));
+  SB_TRY(dalloc(&c->ftgt, 3 * pn));
+  SB_TRY(dalloc(&c->psrc, N));
+  if (c->cfg.precision == SBSLPM_MIXED) {
+    SB_TRY(dalloc(&c->fsrcf, pn));
+    SB_TRY(dalloc(&c->psrcf, N));
   }
   return SBSLPM_OK;
 }
 
 sbslpm_status allocate_workspace(sbslpm_ctx* c) {
   const size_t pn = (size_t)c->P * c->q, ln = (size_t)c->A * c->q;
-  SB_TRY(dalloc(&c->src, pn));
-  if (c->cfg.precision == SBSLPM_MIXED) SB_TRY(dalloc(&c->srcf, pn));
-  SB_TRY(dalloc(&c->tgt, 3 * pn));
+  if (!c->tree) {
+    SB_TRY(dalloc(&c->src, pn));
+    if (c->cfg.precision == SBSLPM_MIXED) SB_TRY(dalloc(&c->srcf, pn));
+    SB_TRY(dalloc(&c->tgt, 3 * pn));
+  }
   SB_TRY(dalloc(&c->vbuf, 4 * 3 * ln));
   SB_TRY(dalloc(&c->dep, 3 * ln));
   SB_TRY(dalloc(&c->newvor, ln));
@@ -235,6 +400,36 @@ void fill_geom(sbslpm_ctx* c) {
   g.pd_centre = c->centre;
   g.srcf = c->srcf;
   g.err = c->err;
+  if (c->tree) {
+    StepGeom& f = c->fgeom;
+    f.levels = c->Lf;
+    f.degree = c->n;
+    f.q = c->qx;
+    f.panels = c->Pf;
+    f.leaves = c->Af;
+    f.offset = c->Pf - c->Af;
+    f.eps = c->cfg.kernel_eps;
+    f.omega = c->cfg.omega;
+    f.px = c->fpx;
+    f.tgt_start = c->cc_start;
+    f.src_panel = c->cc_src;
+    f.child_mat = c->fchild;
+    f.pd_centre = c->fcentre;
+    f.srcf = c->fsrcf;
+    f.err = c->err;
+    TreeGeom& t = c->tgeom;
+    t.n = c->n;
+    t.npl = c->npl;
+    t.N = (long)c->A * c->q;
+    t.eps = c->cfg.kernel_eps;
+    t.omega = c->cfg.omega;
+    t.lx = c->flx;
+    t.ly = c->fly;
+    t.fbounds = c->fbounds;
+    t.fface = c->fface;
+    t.near_start = c->near_start;
+    t.near_src = c->near_src;
+  }
 }
 
 // One velocity evaluation (one RK4 stage) into v (contiguous [3][leaves*q]).
@@ -242,19 +437,30 @@ void velocity_eval(sbslpm_ctx* c, int stage, double dt_s, const double* vprev, c
                    const double* z, const double* area, const double* vors, double* v) {
   cudaStream_t st = c->stream();
   const StepGeom& g = c->geom;
-  launch_leaf_sources(g, stage, dt_s, vprev, x, y, z, vors, area, c->src, st);
   if (c->cfg.velocity == SBSLPM_VEL_DIRECT) {
+    launch_leaf_sources(g, stage, dt_s, vprev, x, y, z, vors, area, c->src, st);
     launch_direct_leaves(g, c->cfg.precision, c->src, v, c->partial, c->groups, st);
     return;
   }
-  launch_nonleaf_sources(g, stage, dt_s, vprev, c->src, st);
-  for (int lev = c->L - 2; lev >= 0; lev--) launch_upward_level(g, lev, c->src, st);
-  launch_interactions(g, c->cfg.precision, c->src, c->tgt, false, st);
+  const bool mixed = c->cfg.precision == SBSLPM_MIXED;
+  if (c->tree) {
+    const StepGeom& fg = c->fgeom;
+    launch_bltc_sources(c->tgeom, fg, c->ftab, stage, dt_s, vprev, x, y, z, vors, area, c->psrc, c->psrcf, c->fsrc,
+                        mixed, st);
+    launch_upward_fused(fg, 2, 0, 0.0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, c->fsrc, mixed, st);
+    launch_interactions_only(fg, c->cfg.precision, c->fsrc, c->ftgt, st);
+    launch_downward_fused(fg, c->ftgt, nullptr, st);
+    launch_bltc_near(c->tgeom, fg, c->cfg.precision, x, y, z, c->psrc, c->psrcf, v, st);
+    launch_bltc_to_particles(c->tgeom, fg, c->ftgt, v, st);
+    return;
+  }
+  launch_upward_fused(g, 0, stage, dt_s, vprev, x, y, z, vors, area, c->src, mixed, st);
+  launch_interactions_only(g, c->cfg.precision, c->src, c->tgt, st);
   if (c->L == 1) {
     cudaMemcpyAsync(v, c->tgt, sizeof(double) * 3 * c->P * c->q, cudaMemcpyDeviceToDevice, st);
     return;
   }
-  for (int lev = 1; lev < c->L; lev++) launch_downward_level(g, lev, c->tgt, lev == c->L - 1 ? v : nullptr, st);
+  launch_downward_fused(g, c->tgt, v, st);
 }
 
 // The work of one bve_back_rk4_step (src/bve_time_step.cpp:311-419), enqueued on the stream.
@@ -419,12 +625,14 @@ sbslpm_status sbslpm_create(const sbslpm_config* cfg, sbslpm_ctx** out) {
   c->A = sbslpm_leaf_count(c->L);
   c->off = c->P - c->A;
   build_panels(c->L, c->panels);
-  if (cfg->velocity == SBSLPM_VEL_FMM) build_interactions(c->L, c->panels, cfg->fmm_theta, c->list);
-  c->I = (long)c->list.size();
+  c->tree = cfg->velocity == SBSLPM_VEL_FMM && cfg->proxy_degree > 0;
+  if (cfg->velocity == SBSLPM_VEL_FMM && !c->tree) build_interactions(c->L, c->panels, cfg->fmm_theta, c->list);
   sbslpm_status s = SBSLPM_OK;
   if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) s = SBSLPM_ERR_CUDA;
   if (s == SBSLPM_OK) s = precompute(c);
+  if (s == SBSLPM_OK && c->tree) s = precompute_tree(c);
   if (s == SBSLPM_OK) s = allocate_workspace(c);
+  c->I = (long)c->list.size();
   if (s != SBSLPM_OK) {
     sbslpm_destroy(c);
     return s;
@@ -438,7 +646,9 @@ sbslpm_status sbslpm_destroy(sbslpm_ctx* c) {
   if (!c) return SBSLPM_OK;
   if (c->graph) cudaGraphExecDestroy(c->graph);
   void* bufs[] = {c->px, c->il_basis, c->child_mat, c->centre, c->tgt_start, c->src_panel, c->il_row, c->src,
-                  c->srcf, c->tgt, c->vbuf, c->partial, c->newvor, c->newtr, c->dep, c->err};
+                  c->srcf, c->tgt, c->vbuf, c->partial, c->newvor, c->newtr, c->dep, c->err, c->fpx, c->fchild,
+                  c->fcentre, c->flx, c->fly, c->fbounds, c->fface, c->near_start, c->near_src, c->cc_start,
+                  c->cc_src, c->fsrc, c->psrc, c->fsrcf, c->psrcf, c->ftgt, c->gx};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (c->h_err) cudaFreeHost(c->h_err);
@@ -532,10 +742,11 @@ sbslpm_status sbslpm_bve_run(sbslpm_ctx* c, const double* x, const double* y, co
 
 sbslpm_status sbslpm_upward_pass(sbslpm_ctx* c, const double* area, const double* pots, double* proxy_source) {
   if (!c || bad(area) || bad(pots) || bad(proxy_source)) return SBSLPM_ERR_ARG;
+  if (c->tree || c->cfg.velocity != SBSLPM_VEL_FMM)
+    return set_last_error("the reference's spectral FMM passes need proxy_degree 0 and FMM velocity"), SBSLPM_ERR_CONFIG;
   cudaStream_t st = c->stream();
   SB_CUDA(cudaMemsetAsync(c->src, 0, sizeof(double4) * c->P * c->q, st));
-  launch_leaf_strength(c->geom, area, pots, c->src, st);
-  for (int lev = c->L - 2; lev >= 0; lev--) launch_upward_level(c->geom, lev, c->src, st);
+  launch_upward_fused(c->geom, 1, 0, 0.0, nullptr, nullptr, nullptr, nullptr, pots, area, c->src, false, st);
   launch_copy_strength(c->geom, c->src, proxy_source, st);
   return finish(c);
 }
@@ -554,7 +765,8 @@ __global__ void k_add3(const double* __restrict__ t, long n, double* a, double* 
 sbslpm_status sbslpm_bve_vel_interactions(sbslpm_ctx* c, const double* dx, const double* dy, const double* dz,
                                           const double* source, double* t1, double* t2, double* t3) {
   if (!c || bad(dx) || bad(dy) || bad(dz) || bad(source) || bad(t1) || bad(t2) || bad(t3)) return SBSLPM_ERR_ARG;
-  if (c->cfg.velocity != SBSLPM_VEL_FMM) return set_last_error("context has no interaction list"), SBSLPM_ERR_CONFIG;
+  if (c->cfg.velocity != SBSLPM_VEL_FMM || c->tree)
+    return set_last_error("the reference's interaction list needs proxy_degree 0 and FMM velocity"), SBSLPM_ERR_CONFIG;
   cudaStream_t st = c->stream();
   launch_sources_from_disp(c->geom, dx, dy, dz, source, c->src, st);
   launch_interactions(c->geom, c->cfg.precision, c->src, c->tgt, false, st);
@@ -567,13 +779,15 @@ sbslpm_status sbslpm_bve_vel_interactions(sbslpm_ctx* c, const double* dx, const
 sbslpm_status sbslpm_downward_pass_3(sbslpm_ctx* c, double* t1, double* t2, double* t3, double* s1, double* s2,
                                      double* s3) {
   if (!c || bad(t1) || bad(t2) || bad(t3) || bad(s1) || bad(s2) || bad(s3)) return SBSLPM_ERR_ARG;
+  if (c->tree || c->cfg.velocity != SBSLPM_VEL_FMM)
+    return set_last_error("the reference's spectral FMM passes need proxy_degree 0 and FMM velocity"), SBSLPM_ERR_CONFIG;
   cudaStream_t st = c->stream();
   size_t pn = (size_t)c->P * c->q, ln = (size_t)c->A * c->q, off = (size_t)c->off * c->q;
   double* tin[3] = {t1, t2, t3};
   double* sout[3] = {s1, s2, s3};
   for (int k = 0; k < 3; k++)
     SB_CUDA(cudaMemcpyAsync(c->tgt + k * pn, tin[k], sizeof(double) * pn, cudaMemcpyDeviceToDevice, st));
-  for (int lev = 1; lev < c->L; lev++) launch_downward_level(c->geom, lev, c->tgt, nullptr, st);
+  launch_downward_fused(c->geom, c->tgt, nullptr, st);
   for (int k = 0; k < 3; k++) {
     SB_CUDA(cudaMemcpyAsync(tin[k], c->tgt + k * pn, sizeof(double) * pn, cudaMemcpyDeviceToDevice, st));
     SB_CUDA(cudaMemcpyAsync(sout[k], c->tgt + k * pn + off, sizeof(double) * ln, cudaMemcpyDeviceToDevice, st));
@@ -653,6 +867,25 @@ sbslpm_status sbslpm_time_interactions(sbslpm_ctx* c, int reps, double* ms_per_l
   if (!c || reps < 1 || !ms_per_launch) return SBSLPM_ERR_ARG;
   if (c->cfg.velocity != SBSLPM_VEL_FMM) return set_last_error("context has no interaction list"), SBSLPM_ERR_CONFIG;
   cudaStream_t st = c->stream();
+  if (c->tree) {  // the dominant kernel is the near-field particle kernel
+    double* v = c->vbuf;
+    cudaEvent_t a, b;
+    SB_CUDA(cudaEventCreate(&a));
+    SB_CUDA(cudaEventCreate(&b));
+    SB_CUDA(cudaEventRecord(a, st));
+    for (int r = 0; r < reps; r++)
+      launch_bltc_near(c->tgeom, c->fgeom, c->cfg.precision, c->gx, c->gx + c->tgeom.N, c->gx + 2 * c->tgeom.N,
+                       c->psrc, c->psrcf, v, st);
+    SB_CUDA(cudaEventRecord(b, st));
+    SB_CUDA(cudaEventSynchronize(b));
+    float tms = 0;
+    SB_CUDA(cudaEventElapsedTime(&tms, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    *ms_per_launch = tms / reps;
+    if (pairs) *pairs = (double)c->n_near * c->npl * c->npl;
+    return finish(c);
+  }
   if (c->cfg.precision == SBSLPM_MIXED) launch_pack_mixed(c->geom, c->src, st);
   cudaEvent_t e0, e1;
   SB_CUDA(cudaEventCreate(&e0));

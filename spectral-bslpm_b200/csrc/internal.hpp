@@ -16,6 +16,8 @@ void build_panels(int levels, std::vector<sbslpm_panel>& panels);
 void build_interp(int degree, bool exact_cc, std::vector<double>& info);
 void build_interactions(int levels, const std::vector<sbslpm_panel>& panels, double theta,
                         std::vector<sbslpm_interact_pair>& out);
+void build_interactions_flagged(int levels, const std::vector<sbslpm_panel>& panels, double theta,
+                                std::vector<sbslpm_interact_pair>& out, std::vector<char>& near);
 void build_points(int levels, int degree, const std::vector<sbslpm_panel>& panels, const double* interp, double* x,
                   double* y, double* z, double* area);
 void proxy_point(const sbslpm_panel& p, const double* interp, int j, double* xyz);

@@ -175,7 +175,17 @@ void build_interp(int d, bool exact_cc, std::vector<double>& info) {
 // is the reference's.
 void build_interactions(int levels, const std::vector<sbslpm_panel>& P, double theta,
                         std::vector<sbslpm_interact_pair>& out) {
+  std::vector<char> near;
+  build_interactions_flagged(levels, P, theta, out, near);
+}
+
+// The same traversal, also recording which pairs failed the MAC (near leaf
+// pairs); the reference's type codes do not separate them from
+// well-separated leaf pairs, both are type 0.
+void build_interactions_flagged(int levels, const std::vector<sbslpm_panel>& P, double theta,
+                                std::vector<sbslpm_interact_pair>& out, std::vector<char>& near) {
   out.clear();
+  near.clear();
   std::deque<std::pair<int, int>> work;
   for (int t = 0; t < 6; t++)
     for (int s = 0; s < 6; s++) work.emplace_back(t, s);
@@ -194,8 +204,10 @@ void build_interactions(int levels, const std::vector<sbslpm_panel>& P, double t
     if (sep < theta) {
       int type = (pt.level < levels - 1 ? 2 : 0) + (ps.level < levels - 1 ? 1 : 0);
       out.push_back({t, s, type});
+      near.push_back(0);
     } else if (pt.is_leaf && ps.is_leaf) {
       out.push_back({t, s, 0});
+      near.push_back(1);
     } else {
       bool split_target = !pt.is_leaf && (ps.is_leaf || pt.level <= ps.level);
       for (int c = 0; c < 4; c++)
@@ -277,6 +289,8 @@ bool read_namelist(const char* path, sbslpm_config* cfg, std::string& msg) {
       } else if (key == "velocity") cfg->velocity = (val == "direct") ? SBSLPM_VEL_DIRECT : SBSLPM_VEL_FMM;
       else if (key == "precision") cfg->precision = (val == "mixed") ? SBSLPM_MIXED : SBSLPM_FP64;
       else if (key == "exact_cc") cfg->exact_cc = std::stoi(val) != 0;
+      else if (key == "proxy_degree") cfg->proxy_degree = std::stoi(val);
+      else if (key == "leaf_size") cfg->leaf_size = std::stoi(val);
       else if (key == "out_path" || key == "write_precision" || key == "write_output" || key == "grid_spacing" ||
                key == "end_time" || key == "output_vel" || key == "output_freq" || key == "initial_condition" ||
                key == "balance_ic" || key == "interp_output" || key == "forcing" || key == "forcing_type" ||

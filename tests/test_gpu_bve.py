@@ -268,3 +268,63 @@ def test_solid_body_rotation_levels7(sb):
         u = torch.stack(f["vel"]).cpu().numpy()
         assert np.abs(u[0] + a * g.y).max() / a < 1e-2
         assert np.abs(u[1] - a * g.x).max() / a < 1e-2
+
+
+def tree_ctx(sb, levels, n, precision=0, theta=0.7, leaf=256):
+    cfg = sb.config_default(levels=levels, interp_degree=3, fmm_theta=theta, kernel_eps=1e-4, omega=2 * np.pi,
+                            dt=0.005, proxy_degree=n, leaf_size=leaf, precision=precision)
+    return sb.Context(cfg)
+
+
+def one_step(ctx, g, vor):
+    f = unit_fields(g, vor)
+    step(ctx, f)
+    return f
+
+
+@pytest.fixture(scope="module")
+def direct_l5(sb):
+    g = sb.build_grid(5, 3, exact_cc=True)
+    vor = unit_sphere_rh4(g)
+    return g, vor, one_step(unit_ctx(sb, 5, velocity=sb.VEL_DIRECT), g, vor)
+
+
+def test_treecode_matches_direct_sum_levels5(sb, direct_l5):
+    """24,576 particles, degree-8 proxies on 256-particle leaves, theta 0.7:
+    within 1e-6 (vorticity) of the float64 direct sum after one step."""
+    g, vor, fd = direct_l5
+    ft = one_step(tree_ctx(sb, 5, 8), g, vor)
+    ev = rel(torch.stack(ft["vel"]), torch.stack(fd["vel"]))
+    ew = rel(ft["vors"], fd["vors"])
+    print(f"treecode n=8: rel vel err {ev:.3e}, rel vort err {ew:.3e}")
+    assert ew <= 1e-6
+    assert ev <= 1e-4
+
+
+def test_treecode_error_falls_with_degree(sb, direct_l5):
+    g, vor, fd = direct_l5
+    errs = []
+    for n in (2, 4, 6, 8):
+        ft = one_step(tree_ctx(sb, 5, n), g, vor)
+        errs.append(rel(torch.stack(ft["vel"]), torch.stack(fd["vel"])))
+    print("treecode velocity error by degree 2,4,6,8:", errs)
+    assert errs[0] > errs[1] > errs[2] > errs[3]
+
+
+def test_treecode_mixed_matches_fp64_levels6(sb):
+    g = sb.build_grid(6, 3, exact_cc=True)
+    vor = unit_sphere_rh4(g)
+    f64 = one_step(tree_ctx(sb, 6, 8), g, vor)
+    f32 = one_step(tree_ctx(sb, 6, 8, precision=sb.MIXED), g, vor)
+    assert rel(torch.stack(f32["vel"]), torch.stack(f64["vel"])) <= MIXED_TOL
+    assert rel(f32["vors"], f64["vors"]) <= MIXED_TOL
+
+
+def test_treecode_graph_replay_and_determinism(sb):
+    g = sb.build_grid(5, 3, exact_cc=True)
+    vor = unit_sphere_rh4(g)
+    ctx = tree_ctx(sb, 5, 6, precision=sb.MIXED)
+    a, b = unit_fields(g, vor), unit_fields(g, vor)
+    step(ctx, a, 2)
+    step(ctx, b, 2, graph=True)
+    assert torch.equal(a["vors"], b["vors"])
