@@ -108,7 +108,9 @@ __global__ void __launch_bounds__(kThreads)
     }
     if (stage == 0) project_to_sphere(xx, yy, zz);
     psrc[i] = make_double4(xx, yy, zz, w);
-    if (mixed) psrcf[i] = make_float4((float)(xx - cc[0]), (float)(yy - cc[1]), (float)(zz - cc[2]), (float)w);
+    if (mixed)
+      psrcf[i] = make_float4((float)((xx - cc[0]) * kPackScale), (float)((yy - cc[1]) * kPackScale),
+                             (float)((zz - cc[2]) * kPackScale), (float)w);
     double xi, eta;
     xieta_from_xyz_face(xx, yy, zz, face, xi, eta);
     bli_1d_free(xi, bd[0], bd[1], tg.n, tab.cosv, tab.w, lx + k * n1);
@@ -125,18 +127,23 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
-// Near leaf pairs: one CTA per target leaf, TPT targets per thread, the
-// source leaf's particles staged in shared memory.
-template <int TPT, bool GUARD>
-__global__ void __launch_bounds__(kThreads)
+// Near leaf pairs: one CTA of NT threads per (target leaf, source split),
+// TPT targets per thread (NT * TPT >= particles per leaf), the source leaf's
+// particles staged in shared memory and read back as broadcasts.  Split y of
+// gridDim.y takes every gridDim.y-th source leaf and writes its partial sums
+// to out + y * 3N (the splits even out the work across SMs);
+// k_bltc_to_particles adds them in split order.
+template <int NT, int TPT, bool GUARD>
+__global__ void __launch_bounds__(NT)
     k_bltc_near64(TreeGeom tg, const double* __restrict__ x, const double* __restrict__ y,
-                  const double* __restrict__ z, const double4* __restrict__ psrc, double* __restrict__ v) {
+                  const double* __restrict__ z, const double4* __restrict__ psrc, double* __restrict__ out) {
+  double* v = out + (long)blockIdx.y * 3 * tg.N;  // partial sums of this source split
   extern __shared__ double4 tile[];
   const int npl = tg.npl, f = blockIdx.x;
   double tx[TPT], ty[TPT], tz[TPT], ax[TPT], ay[TPT], az[TPT];
 #pragma unroll
   for (int r = 0; r < TPT; r++) {
-    int k = threadIdx.x + r * kThreads;
+    int k = threadIdx.x + r * NT;
     long i = (long)f * npl + (k < npl ? k : 0);
     tx[r] = x[i];
     ty[r] = y[i];
@@ -144,11 +151,12 @@ __global__ void __launch_bounds__(kThreads)
     ax[r] = ay[r] = az[r] = 0;
   }
   const double eps = tg.eps;
-  for (int e = tg.near_start[f]; e < tg.near_start[f + 1]; e++) {
+  for (int e = tg.near_start[f] + blockIdx.y; e < tg.near_start[f + 1]; e += gridDim.y) {
     const long sb = (long)tg.near_src[e] * npl;
     __syncthreads();
-    for (int k = threadIdx.x; k < npl; k += kThreads) tile[k] = psrc[sb + k];
+    for (int k = threadIdx.x; k < npl; k += NT) tile[k] = psrc[sb + k];
     __syncthreads();
+#pragma unroll 8
     for (int k = 0; k < npl; k++) {
       const double4 s = tile[k];
 #pragma unroll
@@ -165,7 +173,7 @@ __global__ void __launch_bounds__(kThreads)
   }
 #pragma unroll
   for (int r = 0; r < TPT; r++) {
-    int k = threadIdx.x + r * kThreads;
+    int k = threadIdx.x + r * NT;
     if (k >= npl) continue;
     long i = (long)f * npl + k;
     v[i] = kBiotSavart * (ty[r] * az[r] - tz[r] * ay[r]);
@@ -175,81 +183,108 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 // Mixed precision: target and source particles relative to their leaves'
-// centres, float32 pairs, per-source-leaf float32 sums added into float64.
-template <int TPT, bool GUARD>
-__global__ void __launch_bounds__(kThreads)
+// centres (scaled by kPackScale), float32 pairs, per-source-leaf float32
+// sums added into float64.  Sources are staged two at a time, transposed as
+// (x0,x1,y0,y1),(z0,z1,w0,w1), so that every operand of the pair arithmetic
+// is a register pair and the paired FP32 instructions of sm_100
+// (FADD2 / FFMA2 / FMUL2) evaluate two pairs per instruction; a missing
+// partner of an odd source count has zero strength.
+template <bool GUARD>
+__device__ __forceinline__ void pair32x2(const float2 bx, const float2 by, const float2 bz, const float2 sx,
+                                         const float2 sy, const float2 sz, const float2 sw, const float2 eps2,
+                                         float2& ax, float2& ay, float2& az) {
+  const float2 dx = __fadd2_rn(bx, sx), dy = __fadd2_rn(by, sy), dz = __fadd2_rn(bz, sz);
+  const float2 den = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, eps2)));
+  float2 g = __fmul2_rn(sw, make_float2(recip_f32(den.x), recip_f32(den.y)));
+  if (GUARD) {
+    g.x = den.x > 0.0f ? g.x : 0.0f;
+    g.y = den.y > 0.0f ? g.y : 0.0f;
+  }
+  ax = __ffma2_rn(g, dx, ax);
+  ay = __ffma2_rn(g, dy, ay);
+  az = __ffma2_rn(g, dz, az);
+}
+
+template <int NT, int TPT, bool GUARD>
+__global__ void __launch_bounds__(NT)
     k_bltc_near32(TreeGeom tg, StepGeom fg, const double* __restrict__ x, const double* __restrict__ y,
-                  const double* __restrict__ z, const float4* __restrict__ psrcf, double* __restrict__ v) {
-  extern __shared__ float4 tilef[];
-  const int npl = tg.npl, f = blockIdx.x;
+                  const double* __restrict__ z, const float4* __restrict__ psrcf, double* __restrict__ out) {
+  double* v = out + (long)blockIdx.y * 3 * tg.N;  // partial sums of this source split
+  extern __shared__ float4 tilef[];  // [(npl+1)/2][2]
+  const int npl = tg.npl, npl2 = (npl + 1) >> 1, f = blockIdx.x;
   const double* ct = fg.pd_centre + 4 * (long)(fg.offset + f);
   const double cx = ct[0], cy = ct[1], cz = ct[2];
-  double tx[TPT], ty[TPT], tz[TPT], ax[TPT], ay[TPT], az[TPT];
+  // target positions are re-read for the final cross product, so only their
+  // packed offsets stay in registers
+  double ax[TPT], ay[TPT], az[TPT];
   float dtx[TPT], dty[TPT], dtz[TPT];
 #pragma unroll
   for (int r = 0; r < TPT; r++) {
-    int k = threadIdx.x + r * kThreads;
+    int k = threadIdx.x + r * NT;
     long i = (long)f * npl + (k < npl ? k : 0);
-    tx[r] = x[i];
-    ty[r] = y[i];
-    tz[r] = z[i];
-    dtx[r] = (float)(tx[r] - cx);
-    dty[r] = (float)(ty[r] - cy);
-    dtz[r] = (float)(tz[r] - cz);
+    dtx[r] = (float)((x[i] - cx) * kPackScale);
+    dty[r] = (float)((y[i] - cy) * kPackScale);
+    dtz[r] = (float)((z[i] - cz) * kPackScale);
     ax[r] = ay[r] = az[r] = 0;
   }
-  const float eps = (float)tg.eps;
-  for (int e = tg.near_start[f]; e < tg.near_start[f + 1]; e++) {
+  const float feps = (float)tg.eps;
+  const float2 eps2 = make_float2(feps, feps);
+  for (int e = tg.near_start[f] + blockIdx.y; e < tg.near_start[f + 1]; e += gridDim.y) {
     const int sl = tg.near_src[e];
     const long sb = (long)sl * npl;
     const double* cs = fg.pd_centre + 4 * (long)(fg.offset + sl);
-    const float bx0 = (float)(cs[0] - cx), by0 = (float)(cs[1] - cy), bz0 = (float)(cs[2] - cz);
+    const float bx0 = (float)((cs[0] - cx) * kPackScale), by0 = (float)((cs[1] - cy) * kPackScale),
+                bz0 = (float)((cs[2] - cz) * kPackScale);
     __syncthreads();
-    for (int k = threadIdx.x; k < npl; k += kThreads) tilef[k] = psrcf[sb + k];
+    for (int k2 = threadIdx.x; k2 < npl2; k2 += NT) {
+      const float4 s0 = psrcf[sb + 2 * k2];
+      const float4 s1 = (2 * k2 + 1 < npl) ? psrcf[sb + 2 * k2 + 1] : make_float4(0.f, 0.f, 0.f, 0.f);
+      tilef[2 * k2] = make_float4(s0.x, s1.x, s0.y, s1.y);
+      tilef[2 * k2 + 1] = make_float4(s0.z, s1.z, s0.w, s1.w);
+    }
     __syncthreads();
-    float fx[TPT], fy[TPT], fz[TPT], bx[TPT], by[TPT], bz[TPT];
+    float2 fx[TPT], fy[TPT], fz[TPT], bx[TPT], by[TPT], bz[TPT];
 #pragma unroll
     for (int r = 0; r < TPT; r++) {
-      fx[r] = fy[r] = fz[r] = 0.f;
-      bx[r] = bx0 - dtx[r];
-      by[r] = by0 - dty[r];
-      bz[r] = bz0 - dtz[r];
+      fx[r] = fy[r] = fz[r] = make_float2(0.f, 0.f);
+      const float b0 = bx0 - dtx[r], b1 = by0 - dty[r], b2 = bz0 - dtz[r];
+      bx[r] = make_float2(b0, b0);
+      by[r] = make_float2(b1, b1);
+      bz[r] = make_float2(b2, b2);
     }
-    for (int k = 0; k < npl; k++) {
-      const float4 s = tilef[k];
+#pragma unroll 4
+    for (int k2 = 0; k2 < npl2; k2++) {
+      const float4 A = tilef[2 * k2], B = tilef[2 * k2 + 1];
+      const float2 sx = make_float2(A.x, A.y), sy = make_float2(A.z, A.w), sz = make_float2(B.x, B.y),
+                   sw = make_float2(B.z, B.w);
 #pragma unroll
-      for (int r = 0; r < TPT; r++) {
-        float dx = bx[r] + s.x, dy = by[r] + s.y, dz = bz[r] + s.z;
-        float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-        float g = s.w * recip_f32(fmaf(0.5f, r2, eps));
-        if (GUARD) g = r2 > 0.0f ? g : 0.0f;
-        fx[r] = fmaf(g, dx, fx[r]);
-        fy[r] = fmaf(g, dy, fy[r]);
-        fz[r] = fmaf(g, dz, fz[r]);
-      }
+      for (int r = 0; r < TPT; r++) pair32x2<GUARD>(bx[r], by[r], bz[r], sx, sy, sz, sw, eps2, fx[r], fy[r], fz[r]);
     }
 #pragma unroll
     for (int r = 0; r < TPT; r++) {
-      ax[r] += fx[r];
-      ay[r] += fy[r];
-      az[r] += fz[r];
+      ax[r] += (double)fx[r].x + (double)fx[r].y;
+      ay[r] += (double)fy[r].x + (double)fy[r].y;
+      az[r] += (double)fz[r].x + (double)fz[r].y;
     }
   }
 #pragma unroll
   for (int r = 0; r < TPT; r++) {
-    int k = threadIdx.x + r * kThreads;
+    int k = threadIdx.x + r * NT;
     if (k >= npl) continue;
     long i = (long)f * npl + k;
-    v[i] = kBiotSavart * (ty[r] * az[r] - tz[r] * ay[r]);
-    v[tg.N + i] = kBiotSavart * (tz[r] * ax[r] - tx[r] * az[r]);
-    v[2 * tg.N + i] = kBiotSavart * (tx[r] * ay[r] - ty[r] * ax[r]);
+    const double tx = x[i], ty = y[i], tz = z[i];
+    v[i] = kBiotSavartPacked * (ty * az[r] - tz * ay[r]);
+    v[tg.N + i] = kBiotSavartPacked * (tz * ax[r] - tx * az[r]);
+    v[2 * tg.N + i] = kBiotSavartPacked * (tx * ay[r] - ty * ax[r]);
   }
 }
 
-// Leaf proxy targets -> particles: v_i += sum_a lx[k][a] sum_b ly[k][b] T[a][b]
-// with the leaf-box basis of particle k of the (uniform) leaf.
+// Leaf proxy targets -> particles: v_i = (near-field splits summed in order)
+// + sum_a lx[k][a] sum_b ly[k][b] T[a][b], with the leaf-box basis of
+// particle k of the (uniform) leaf.
 __global__ void __launch_bounds__(kThreads)
-    k_bltc_to_particles(TreeGeom tg, StepGeom fg, const double* __restrict__ tgt, double* __restrict__ v) {
+    k_bltc_to_particles(TreeGeom tg, StepGeom fg, const double* __restrict__ tgt, const double* __restrict__ near,
+                        int splits, double* __restrict__ v) {
   extern __shared__ double tsh[];  // 3 x qx
   const int n1 = tg.n + 1, qx = n1 * n1, npl = tg.npl, f = blockIdx.x;
   const long pn = (long)fg.panels * qx;
@@ -278,9 +313,16 @@ __global__ void __launch_bounds__(kThreads)
       u2 = fma(la, s2, u2);
     }
     const long i = (long)f * npl + k;
-    v[i] += u0;
-    v[tg.N + i] += u1;
-    v[2 * tg.N + i] += u2;
+    double n0 = 0, n1s = 0, n2 = 0;
+    for (int y = 0; y < splits; y++) {
+      const double* p = near + (long)y * 3 * tg.N;
+      n0 += p[i];
+      n1s += p[tg.N + i];
+      n2 += p[2 * tg.N + i];
+    }
+    v[i] = n0 + u0;
+    v[tg.N + i] = n1s + u1;
+    v[2 * tg.N + i] = n2 + u2;
   }
 }
 
@@ -309,34 +351,36 @@ void launch_bltc_sources(const TreeGeom& tg, const StepGeom& fg, const BliTable&
 }
 
 void launch_bltc_near(const TreeGeom& tg, const StepGeom& fg, int precision, const double* x, const double* y,
-                      const double* z, const double4* psrc, const float4* psrcf, double* v, cudaStream_t st) {
+                      const double* z, const double4* psrc, const float4* psrcf, double* v, int splits,
+                      cudaStream_t st) {
   const bool guard = !(tg.eps > 0);
-  const unsigned grid = (unsigned)fg.leaves;
-  if (precision == SBSLPM_MIXED) {
-    size_t smem = sizeof(float4) * tg.npl;
-    if (tg.npl <= kThreads) {
-      if (guard) SB_LAUNCH((k_bltc_near32<1, true>), grid, kThreads, smem, st, tg, fg, x, y, z, psrcf, v);
-      else SB_LAUNCH((k_bltc_near32<1, false>), grid, kThreads, smem, st, tg, fg, x, y, z, psrcf, v);
-    } else {
-      if (guard) SB_LAUNCH((k_bltc_near32<2, true>), grid, kThreads, smem, st, tg, fg, x, y, z, psrcf, v);
-      else SB_LAUNCH((k_bltc_near32<2, false>), grid, kThreads, smem, st, tg, fg, x, y, z, psrcf, v);
-    }
-  } else {
-    size_t smem = sizeof(double4) * tg.npl;
-    if (tg.npl <= kThreads) {
-      if (guard) SB_LAUNCH((k_bltc_near64<1, true>), grid, kThreads, smem, st, tg, x, y, z, psrc, v);
-      else SB_LAUNCH((k_bltc_near64<1, false>), grid, kThreads, smem, st, tg, x, y, z, psrc, v);
-    } else {
-      if (guard) SB_LAUNCH((k_bltc_near64<2, true>), grid, kThreads, smem, st, tg, x, y, z, psrc, v);
-      else SB_LAUNCH((k_bltc_near64<2, false>), grid, kThreads, smem, st, tg, x, y, z, psrc, v);
-    }
-  }
+  const dim3 grid((unsigned)fg.leaves, (unsigned)splits);
+  // two targets per thread: each staged source feeds two pair evaluations
+#define SB_NEAR(NT, TPT)                                                                                      \
+  do {                                                                                                        \
+    if (precision == SBSLPM_MIXED) {                                                                          \
+      const size_t sm32 = sizeof(float4) * 2 * ((tg.npl + 1) / 2);                                           \
+      if (guard) SB_LAUNCH((k_bltc_near32<NT, TPT, true>), grid, NT, sm32, st, tg, fg, x, y, z, psrcf, v);     \
+      else SB_LAUNCH((k_bltc_near32<NT, TPT, false>), grid, NT, sm32, st, tg, fg, x, y, z, psrcf, v);          \
+    } else {                                                                                                  \
+      if (guard) SB_LAUNCH((k_bltc_near64<NT, TPT, true>), grid, NT, sizeof(double4) * tg.npl, st, tg, x, y, z, \
+                           psrc, v);                                                                          \
+      else SB_LAUNCH((k_bltc_near64<NT, TPT, false>), grid, NT, sizeof(double4) * tg.npl, st, tg, x, y, z,      \
+                     psrc, v);                                                                                \
+    }                                                                                                         \
+  } while (0)
+  if (tg.npl <= 64) SB_NEAR(64, 1);
+  else if (tg.npl <= 128) SB_NEAR(64, 2);
+  else if (tg.npl <= 256) SB_NEAR(128, 2);
+  else SB_NEAR(256, 2);
+#undef SB_NEAR
 }
 
-void launch_bltc_to_particles(const TreeGeom& tg, const StepGeom& fg, const double* tgt, double* v,
-                              cudaStream_t st) {
+void launch_bltc_to_particles(const TreeGeom& tg, const StepGeom& fg, const double* tgt, const double* near,
+                              int splits, double* v, cudaStream_t st) {
   int qx = (tg.n + 1) * (tg.n + 1);
-  SB_LAUNCH(k_bltc_to_particles, (unsigned)fg.leaves, kThreads, sizeof(double) * 3 * qx, st, tg, fg, tgt, v);
+  SB_LAUNCH(k_bltc_to_particles, (unsigned)fg.leaves, kThreads, sizeof(double) * 3 * qx, st, tg, fg, tgt, near, splits,
+            v);
 }
 
 }  // namespace sbslpm

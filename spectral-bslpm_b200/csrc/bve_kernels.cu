@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
+#include <type_traits>
 
 #include "../../include/sbslpm.h"
 #include "bve_kernels.cuh"
@@ -64,18 +65,38 @@ __device__ __forceinline__ void pair64(double tx, double ty, double tz, const do
   az = fma(g, dz, az);
 }
 
-// The same pair in float32 on panel-relative coordinates: d = base + s.xyz
-// with base = (c_S - c_T) - delta_t.
+// The same pair in float32 on panel-relative coordinates scaled by 1/sqrt(2)
+// (kPackScale): d' = base + s.xyz with base = (c_S - c_T)/sqrt(2) - delta_t,
+// and |d'|^2 + eps = |d|^2/2 + eps in one FMA chain.
 template <bool GUARD>
 __device__ __forceinline__ void pair32(float bx, float by, float bz, const float4 s, float eps, float& ax, float& ay,
                                        float& az) {
   float dx = bx + s.x, dy = by + s.y, dz = bz + s.z;
-  float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-  float g = s.w * recip_f32(fmaf(0.5f, r2, eps));
-  if (GUARD) g = r2 > 0.0f ? g : 0.0f;
+  float den = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps)));
+  float g = s.w * recip_f32(den);
+  if (GUARD) g = den > 0.0f ? g : 0.0f;
   ax = fmaf(g, dx, ax);
   ay = fmaf(g, dy, ay);
   az = fmaf(g, dz, az);
+}
+
+// Two pairs at once with the paired FP32 instructions of sm_100 (FADD2 /
+// FFMA2 / FMUL2): one target (b broadcast in both halves) against two
+// sources given as register pairs (x0,x1), (y0,y1), (z0,z1), (w0,w1).
+template <bool GUARD>
+__device__ __forceinline__ void pair32x2(const float2 bx, const float2 by, const float2 bz, const float2 sx,
+                                         const float2 sy, const float2 sz, const float2 sw, const float2 eps2,
+                                         float2& ax, float2& ay, float2& az) {
+  const float2 dx = __fadd2_rn(bx, sx), dy = __fadd2_rn(by, sy), dz = __fadd2_rn(bz, sz);
+  const float2 den = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, eps2)));
+  float2 g = __fmul2_rn(sw, make_float2(recip_f32(den.x), recip_f32(den.y)));
+  if (GUARD) {
+    g.x = den.x > 0.0f ? g.x : 0.0f;
+    g.y = den.y > 0.0f ? g.y : 0.0f;
+  }
+  ax = __ffma2_rn(g, dx, ax);
+  ay = __ffma2_rn(g, dy, ay);
+  az = __ffma2_rn(g, dz, az);
 }
 
 // ---------------------------------------------------------------------------
@@ -136,10 +157,13 @@ __global__ void k_copy_strength(StepGeom g, const double4* __restrict__ src, dou
 // ---------------------------------------------------------------------------
 // Tree passes (upward_pass / downward_pass_3, src/fmm_funcs.cpp:341-392;
 // child_to_parent / parent_to_child_3, src/fmm_funcs_impl.hpp:36-172).
-// child_mat[c][k][l] is the BLI basis of parent node l at child c's node k;
-// the uniform quadtree makes it the same matrix for every parent:
-//   upward:   parent node j  = sum_c sum_k child_mat[c][k][j] * child_c node k
-//   downward: child_c node k += sum_l child_mat[c][k][l] * parent node l
+// The BLI basis of parent node (a,b) at child c's node (i,j) is the product
+// Lx_c[i][a] Ly_c[j][b] of one-dimensional bases, and the uniform quadtree has
+// only two of them: child_1d[h][i][a] for the child in the upper (h = 0) or
+// lower (h = 1) half of its parent.  The passes contract one direction at a
+// time:
+//   upward:   T[c][i][b] = sum_j Ly_c[j][b] S_c[i][j];  S[a][b] = sum_c sum_i Lx_c[i][a] T[c][i][b]
+//   downward: U[c][a][j] = sum_b Ly_c[j][b] T[a][b];    T_c[i][j] += sum_a Lx_c[i][a] U[c][a][j]
 //
 // One CTA owns the subtree of depth D below one panel of level r and keeps
 // the strengths (upward) or target values (downward) of all its levels in
@@ -189,8 +213,8 @@ __global__ void k_upward_subtree(StepGeom g, int r, int D, int mode, int stage, 
                                  const double* __restrict__ y, const double* __restrict__ z,
                                  const double* __restrict__ vors, const double* __restrict__ area,
                                  double4* __restrict__ src, int mixed) {
-  extern __shared__ double sh[];  // strengths of levels r..r+D, level k at offset q*(4^k-1)/3
-  const int q = g.q, root_rel = blockIdx.x;
+  extern __shared__ double sh[];  // strengths of levels r..r+D (level k at q*(4^k-1)/3), then scratch
+  const int q = g.q, root_rel = blockIdx.x, n1 = g.degree + 1;
   const bool leaves_here = (r + D == g.levels - 1);
   const long ln = (long)g.leaves * g.q, pn = (long)g.panels * g.q;
   auto lvl = [&](int k) { return sh + q * (((1 << (2 * k)) - 1) / 3); };
@@ -243,18 +267,28 @@ __global__ void k_upward_subtree(StepGeom g, int r, int D, int mode, int stage, 
     }
   }
   __syncthreads();
-  // anterpolation, deepest parents first
+  // anterpolation, deepest parents first, one direction at a time
+  double* scratch = sh + q * (((1 << (2 * (D + 1))) - 1) / 3);
   for (int k = D - 1; k >= 0; k--) {
     const double* ch = lvl(k + 1);
     double* pa = lvl(k);
-    const int npts = (1 << (2 * k)) * q, first = subtree_first(r, root_rel, k);
-    for (int t = threadIdx.x; t < npts; t += blockDim.x) {
-      const int p = t / q, j = t % q;
+    const int np = 1 << (2 * k), first = subtree_first(r, root_rel, k);
+    for (int t = threadIdx.x; t < 4 * np * q; t += blockDim.x) {  // T[cc][i][b]
+      const int cc = t / q, rem = t % q, i = rem / n1, b = rem % n1;
+      const double* ly = g.child_1d + ((cc & 3) >= 2 ? n1 * n1 : 0);
+      const double* sc = ch + cc * q + i * n1;
+      double acc = 0;
+      for (int j = 0; j < n1; j++) acc = fma(__ldg(ly + j * n1 + b), sc[j], acc);
+      scratch[t] = acc;
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < np * q; t += blockDim.x) {  // S[p][a][b]
+      const int p = t / q, rem = t % q, a = rem / n1, b = rem % n1;
       double acc = 0;
       for (int c = 0; c < 4; c++) {
-        const double* cs = ch + (4 * p + c) * q;
-        const double* m = g.child_mat + (long)c * q * q + j;
-        for (int kk = 0; kk < q; kk++) acc = fma(__ldg(m + (long)kk * q), cs[kk], acc);
+        const double* lx = g.child_1d + ((c == 1 || c == 2) ? n1 * n1 : 0);
+        const double* tc = scratch + (4 * p + c) * q + b;
+        for (int i = 0; i < n1; i++) acc = fma(__ldg(lx + i * n1 + a), tc[i * n1], acc);
       }
       pa[t] = acc;
       src[(long)first * q + t].w = acc;
@@ -270,7 +304,8 @@ __global__ void k_upward_subtree(StepGeom g, int r, int D, int mode, int stage, 
         const long i = (long)first * q + t;
         const double* cc = g.pd_centre + 4 * (i / q);
         double4 sv = src[i];
-        g.srcf[i] = make_float4((float)(sv.x - cc[0]), (float)(sv.y - cc[1]), (float)(sv.z - cc[2]), (float)sv.w);
+        g.srcf[i] = make_float4((float)((sv.x - cc[0]) * kPackScale), (float)((sv.y - cc[1]) * kPackScale),
+                                (float)((sv.z - cc[2]) * kPackScale), (float)sv.w);
       }
     }
   }
@@ -282,11 +317,13 @@ __global__ void k_upward_subtree(StepGeom g, int r, int D, int mode, int stage, 
 // deepest non-leaf level is written back for the next launch.
 __global__ void k_downward_subtree(StepGeom g, int r, int D, double* __restrict__ tgt,
                                    double* __restrict__ leaf_out) {
-  extern __shared__ double sh[];  // 3 fields x levels r..r+D
-  const int q = g.q, root_rel = blockIdx.x;
+  extern __shared__ double sh[];  // 3 fields x levels r..r+D, then 3 x 4^D q scratch
+  const int q = g.q, root_rel = blockIdx.x, n1 = g.degree + 1;
   const long pn = (long)g.panels * g.q, ln = (long)g.leaves * g.q;
   const int per_field = q * (((1 << (2 * (D + 1))) - 1) / 3);
   auto lvl = [&](int f, int k) { return sh + f * per_field + q * (((1 << (2 * k)) - 1) / 3); };
+  double* scratch = sh + 3 * per_field;
+  const int sstride = (1 << (2 * D)) * q;
   {
     const int first = subtree_first(r, root_rel, 0);
     for (int t = threadIdx.x; t < q; t += blockDim.x)
@@ -296,16 +333,34 @@ __global__ void k_downward_subtree(StepGeom g, int r, int D, double* __restrict_
   for (int k = 1; k <= D; k++) {
     const int level = r + k, npts = (1 << (2 * k)) * q, first = subtree_first(r, root_rel, k);
     const bool is_leaf = (level == g.levels - 1);
-    for (int t = threadIdx.x; t < npts; t += blockDim.x) {
-      const int pc = t / q, kk = t % q, c = pc & 3, pp = pc >> 2;
-      const double* m = g.child_mat + ((long)c * q + kk) * q;
-      const double *t0 = lvl(0, k - 1) + pp * q, *t1 = lvl(1, k - 1) + pp * q, *t2 = lvl(2, k - 1) + pp * q;
+    for (int t = threadIdx.x; t < npts; t += blockDim.x) {  // U[cc][a][j]
+      const int cc = t / q, rem = t % q, a = rem / n1, j = rem % n1;
+      const double* ly = g.child_1d + ((cc & 3) >= 2 ? n1 * n1 : 0) + j * n1;
+      const int pp = cc >> 2;
+      const double *p0 = lvl(0, k - 1) + pp * q + a * n1, *p1 = lvl(1, k - 1) + pp * q + a * n1,
+                   *p2 = lvl(2, k - 1) + pp * q + a * n1;
+      double u0 = 0, u1 = 0, u2 = 0;
+      for (int b = 0; b < n1; b++) {
+        const double l = __ldg(ly + b);
+        u0 = fma(l, p0[b], u0);
+        u1 = fma(l, p1[b], u1);
+        u2 = fma(l, p2[b], u2);
+      }
+      scratch[t] = u0;
+      scratch[sstride + t] = u1;
+      scratch[2 * sstride + t] = u2;
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < npts; t += blockDim.x) {  // T_c[i][j] += sum_a Lx[i][a] U[a][j]
+      const int cc = t / q, rem = t % q, i = rem / n1, j = rem % n1, c = cc & 3;
+      const double* lx = g.child_1d + ((c == 1 || c == 2) ? n1 * n1 : 0) + i * n1;
+      const double* u = scratch + cc * q + j;
       double a0 = 0, a1 = 0, a2 = 0;
-      for (int l = 0; l < q; l++) {
-        double ml = __ldg(m + l);
-        a0 = fma(ml, t0[l], a0);
-        a1 = fma(ml, t1[l], a1);
-        a2 = fma(ml, t2[l], a2);
+      for (int a = 0; a < n1; a++) {
+        const double l = __ldg(lx + a);
+        a0 = fma(l, u[a * n1], a0);
+        a1 = fma(l, u[sstride + a * n1], a1);
+        a2 = fma(l, u[2 * sstride + a * n1], a2);
       }
       const long o = (long)first * q + t;
       a0 += tgt[o];
@@ -348,6 +403,8 @@ struct WarpShape {
   static constexpr int S = Q <= 16 ? 32 / Q : 1;          // source splits per warp
   static constexpr int TPL = Q <= 32 ? 1 : (Q + 31) / 32;  // target nodes per lane
   static constexpr int STAGE = (S * Q > Q ? S * Q : Q);    // staged points per warp
+  static constexpr int Q2 = (Q + 1) / 2;                    // source pairs per panel
+  static constexpr int STAGE2 = (S > 1 ? S : 1) * 2 * Q2;   // float4 slots per warp, paired layout
 };
 
 template <int Q, bool ALL_LEAVES, bool GUARD>
@@ -467,14 +524,15 @@ __global__ void k_pack_mixed(StepGeom g, const double4* __restrict__ src, float4
   if (i >= pn) return;
   const double* c = g.pd_centre + 4 * (i / g.q);
   double4 s = src[i];
-  srcf[i] = make_float4((float)(s.x - c[0]), (float)(s.y - c[1]), (float)(s.z - c[2]), (float)s.w);
+  srcf[i] = make_float4((float)((s.x - c[0]) * kPackScale), (float)((s.y - c[1]) * kPackScale),
+                        (float)((s.z - c[2]) * kPackScale), (float)s.w);
 }
 
 template <int Q, bool ALL_LEAVES, bool GUARD>
 __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_interact32(StepGeom g, const float4* __restrict__ srcf,
                                                                     double* __restrict__ out, long out_stride) {
   using W = WarpShape<Q>;
-  __shared__ float4 stage[kWarpsPerBlock][W::STAGE];
+  __shared__ float4 stage[kWarpsPerBlock][W::STAGE2];
   __shared__ double red[kWarpsPerBlock][3][32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int tp_first = ALL_LEAVES ? g.offset : 0;
@@ -505,28 +563,49 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_interact32(StepGeom g, 
       tx = g.px[o];
       ty = g.px[pn + o];
       tz = g.px[2 * pn + o];
-      dtx = (float)(tx - ctx);
-      dty = (float)(ty - cty);
-      dtz = (float)(tz - ctz);
+      dtx = (float)((tx - ctx) * kPackScale);
+      dty = (float)((ty - cty) * kPackScale);
+      dtz = (float)((tz - ctz) * kPackScale);
     }
     double ax = 0, ay = 0, az = 0;
+    const float2 eps2 = make_float2(eps, eps);
+    // each split's panel staged two sources per pair slot, transposed as
+    // (x0,x1,y0,y1),(z0,z1,w0,w1); a missing partner (odd q) has zero strength
+    float* sl = reinterpret_cast<float*>(&stage[warp][0]) + h * 8 * W::Q2;
     for (int e = e0; e < e1; e += W::S) {
       int sp = 0;
       if (active && e + h < e1) {
         sp = ALL_LEAVES ? g.offset + e + h : __ldg(g.src_panel + e + h);
-        stage[warp][h * Q + j] = srcf[(long)sp * Q + j];
+        const float4 sv = srcf[(long)sp * Q + j];
+        const int k2 = j >> 1, o = j & 1;
+        sl[8 * k2 + o] = sv.x;
+        sl[8 * k2 + 2 + o] = sv.y;
+        sl[8 * k2 + 4 + o] = sv.z;
+        sl[8 * k2 + 6 + o] = sv.w;
+        if ((Q & 1) && j == Q - 1) {
+          sl[8 * k2 + 1] = 0.f;
+          sl[8 * k2 + 3] = 0.f;
+          sl[8 * k2 + 5] = 0.f;
+          sl[8 * k2 + 7] = 0.f;
+        }
       }
       __syncwarp();
       if (active && e + h < e1) {
         const double* cs = g.pd_centre + 4 * (long)sp;
-        float bx = (float)(cs[0] - ctx) - dtx, by = (float)(cs[1] - cty) - dty, bz = (float)(cs[2] - ctz) - dtz;
-        float fx = 0.f, fy = 0.f, fz = 0.f;
-        const float4* sb = &stage[warp][h * Q];
+        const float b0 = (float)((cs[0] - ctx) * kPackScale) - dtx, b1 = (float)((cs[1] - cty) * kPackScale) - dty,
+                    b2 = (float)((cs[2] - ctz) * kPackScale) - dtz;
+        const float2 bx = make_float2(b0, b0), by = make_float2(b1, b1), bz = make_float2(b2, b2);
+        float2 fx = make_float2(0.f, 0.f), fy = fx, fz = fx;
+        const float4* sb = reinterpret_cast<const float4*>(sl);
 #pragma unroll
-        for (int k = 0; k < Q; k++) pair32<GUARD>(bx, by, bz, sb[k], eps, fx, fy, fz);
-        ax += fx;
-        ay += fy;
-        az += fz;
+        for (int k2 = 0; k2 < W::Q2; k2++) {
+          const float4 A = sb[2 * k2], B = sb[2 * k2 + 1];
+          pair32x2<GUARD>(bx, by, bz, make_float2(A.x, A.y), make_float2(A.z, A.w), make_float2(B.x, B.y),
+                          make_float2(B.z, B.w), eps2, fx, fy, fz);
+        }
+        ax += (double)fx.x + (double)fx.y;
+        ay += (double)fy.x + (double)fy.y;
+        az += (double)fz.x + (double)fz.y;
       }
       __syncwarp();
     }
@@ -545,9 +624,9 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_interact32(StepGeom g, 
     if (h == 0) {
       long o = ALL_LEAVES ? (long)blockIdx.y * 3 * out_stride + (long)tix * Q + j : (long)t * Q + j;
       long s = ALL_LEAVES ? out_stride : pn;
-      out[o] = kBiotSavart * (ty * az - tz * ay);
-      out[s + o] = kBiotSavart * (tz * ax - tx * az);
-      out[2 * s + o] = kBiotSavart * (tx * ay - ty * ax);
+      out[o] = kBiotSavartPacked * (ty * az - tz * ay);
+      out[s + o] = kBiotSavartPacked * (tz * ax - tx * az);
+      out[2 * s + o] = kBiotSavartPacked * (tx * ay - ty * ax);
     }
   } else {
     constexpr int TPL = W::TPL;
@@ -560,9 +639,9 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_interact32(StepGeom g, 
       tx[r] = g.px[o];
       ty[r] = g.px[pn + o];
       tz[r] = g.px[2 * pn + o];
-      dtx[r] = (float)(tx[r] - ctx);
-      dty[r] = (float)(ty[r] - cty);
-      dtz[r] = (float)(tz[r] - ctz);
+      dtx[r] = (float)((tx[r] - ctx) * kPackScale);
+      dty[r] = (float)((ty[r] - cty) * kPackScale);
+      dtz[r] = (float)((tz[r] - ctz) * kPackScale);
       ax[r] = ay[r] = az[r] = 0;
     }
     for (int e = e0; e < e1; e++) {
@@ -570,7 +649,8 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_interact32(StepGeom g, 
       const long sb = (long)sp * Q;
       for (int k = lane; k < Q; k += 32) stage[warp][k] = srcf[sb + k];
       const double* cs = g.pd_centre + 4 * (long)sp;
-      const float bx0 = (float)(cs[0] - ctx), by0 = (float)(cs[1] - cty), bz0 = (float)(cs[2] - ctz);
+      const float bx0 = (float)((cs[0] - ctx) * kPackScale), by0 = (float)((cs[1] - cty) * kPackScale),
+                  bz0 = (float)((cs[2] - ctz) * kPackScale);
       float fx[TPL], fy[TPL], fz[TPL], bx[TPL], by[TPL], bz[TPL];
 #pragma unroll
       for (int r = 0; r < TPL; r++) {
@@ -599,10 +679,135 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_interact32(StepGeom g, 
       if (j >= Q) continue;
       long o = ALL_LEAVES ? (long)blockIdx.y * 3 * out_stride + (long)tix * Q + j : (long)t * Q + j;
       long s = ALL_LEAVES ? out_stride : pn;
-      out[o] = kBiotSavart * (ty[r] * az[r] - tz[r] * ay[r]);
-      out[s + o] = kBiotSavart * (tz[r] * ax[r] - tx[r] * az[r]);
-      out[2 * s + o] = kBiotSavart * (tx[r] * ay[r] - ty[r] * ax[r]);
+      out[o] = kBiotSavartPacked * (ty[r] * az[r] - tz[r] * ay[r]);
+      out[s + o] = kBiotSavartPacked * (tz[r] * ax[r] - tx[r] * az[r]);
+      out[2 * s + o] = kBiotSavartPacked * (tx[r] * ay[r] - ty[r] * ax[r]);
     }
+  }
+}
+
+// Wide panels (q > 32, e.g. 81 treecode proxies): one CTA of four warps per
+// target panel; the warps take every fourth source panel, each lane owns
+// ceil(q/32) target nodes, and the four partial sums are added in warp order
+// (deterministic).  MIXED: float32 pairs on packed sources (kPackScale),
+// per-source-panel float32 sums added into float64.
+template <int Q, bool ALL_LEAVES, bool GUARD, bool MIXED>
+__global__ void __launch_bounds__(128) k_interact_wide(StepGeom g, const double4* __restrict__ src,
+                                                       const float4* __restrict__ srcf, double* __restrict__ out,
+                                                       long out_stride) {
+  constexpr int TPL = (Q + 31) / 32, NW = 4, Q2 = (Q + 1) / 2;
+  using Src = typename std::conditional<MIXED, float4, double4>::type;
+  // MIXED: sources staged two at a time, transposed, (x0,x1,y0,y1),(z0,z1,w0,w1)
+  __shared__ Src stage[NW][MIXED ? 2 * Q2 : Q];
+  __shared__ double red[NW][3][Q];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int tix = blockIdx.x;
+  const int t = (ALL_LEAVES ? g.offset : 0) + tix;
+  const long pn = (long)g.panels * g.q;
+  int e0, e1;
+  if (ALL_LEAVES) {
+    int per = (g.leaves + gridDim.y - 1) / gridDim.y;
+    e0 = blockIdx.y * per;
+    e1 = min(g.leaves, e0 + per);
+  } else {
+    e0 = g.tgt_start[t];
+    e1 = g.tgt_start[t + 1];
+  }
+  const double* ct = g.pd_centre + 4 * (long)t;
+  const double ctx = ct[0], cty = ct[1], ctz = ct[2];
+  double tx[TPL], ty[TPL], tz[TPL], ax[TPL], ay[TPL], az[TPL];
+  float dtx[TPL], dty[TPL], dtz[TPL];
+#pragma unroll
+  for (int r = 0; r < TPL; r++) {
+    int j = lane + 32 * r;
+    long o = (long)t * Q + (j < Q ? j : 0);
+    tx[r] = g.px[o];
+    ty[r] = g.px[pn + o];
+    tz[r] = g.px[2 * pn + o];
+    dtx[r] = (float)((tx[r] - ctx) * kPackScale);
+    dty[r] = (float)((ty[r] - cty) * kPackScale);
+    dtz[r] = (float)((tz[r] - ctz) * kPackScale);
+    ax[r] = ay[r] = az[r] = 0;
+  }
+  const float feps = (float)g.eps;
+  for (int e = e0 + warp; e < e1; e += NW) {
+    const int sp = ALL_LEAVES ? g.offset + e : __ldg(g.src_panel + e);
+    const long sb = (long)sp * Q;
+    if constexpr (MIXED) {
+      for (int k2 = lane; k2 < Q2; k2 += 32) {
+        const float4 s0 = srcf[sb + 2 * k2];
+        const float4 s1 = (2 * k2 + 1 < Q) ? srcf[sb + 2 * k2 + 1] : make_float4(0.f, 0.f, 0.f, 0.f);
+        stage[warp][2 * k2] = make_float4(s0.x, s1.x, s0.y, s1.y);
+        stage[warp][2 * k2 + 1] = make_float4(s0.z, s1.z, s0.w, s1.w);
+      }
+    } else {
+      for (int k = lane; k < Q; k += 32) stage[warp][k] = src[sb + k];
+    }
+    __syncwarp();
+    if constexpr (MIXED) {
+      const double* cs = g.pd_centre + 4 * (long)sp;
+      const float bx0 = (float)((cs[0] - ctx) * kPackScale), by0 = (float)((cs[1] - cty) * kPackScale),
+                  bz0 = (float)((cs[2] - ctz) * kPackScale);
+      const float2 eps2 = make_float2(feps, feps);
+      float2 fx[TPL], fy[TPL], fz[TPL], bx[TPL], by[TPL], bz[TPL];
+#pragma unroll
+      for (int r = 0; r < TPL; r++) {
+        fx[r] = fy[r] = fz[r] = make_float2(0.f, 0.f);
+        const float b0 = bx0 - dtx[r], b1 = by0 - dty[r], b2 = bz0 - dtz[r];
+        bx[r] = make_float2(b0, b0);
+        by[r] = make_float2(b1, b1);
+        bz[r] = make_float2(b2, b2);
+      }
+#pragma unroll 3
+      for (int k2 = 0; k2 < Q2; k2++) {
+        const float4 A = stage[warp][2 * k2], B = stage[warp][2 * k2 + 1];
+        const float2 sx = make_float2(A.x, A.y), sy = make_float2(A.z, A.w), sz = make_float2(B.x, B.y),
+                     sw = make_float2(B.z, B.w);
+#pragma unroll
+        for (int r = 0; r < TPL; r++)
+          pair32x2<GUARD>(bx[r], by[r], bz[r], sx, sy, sz, sw, eps2, fx[r], fy[r], fz[r]);
+      }
+#pragma unroll
+      for (int r = 0; r < TPL; r++) {
+        ax[r] += (double)fx[r].x + (double)fx[r].y;
+        ay[r] += (double)fy[r].x + (double)fy[r].y;
+        az[r] += (double)fz[r].x + (double)fz[r].y;
+      }
+    } else {
+#pragma unroll 3
+      for (int k = 0; k < Q; k++) {
+        const double4 s = stage[warp][k];
+#pragma unroll
+        for (int r = 0; r < TPL; r++) pair64<GUARD>(tx[r], ty[r], tz[r], s, g.eps, ax[r], ay[r], az[r]);
+      }
+    }
+    __syncwarp();
+  }
+#pragma unroll
+  for (int r = 0; r < TPL; r++) {
+    int j = lane + 32 * r;
+    if (j < Q) {
+      red[warp][0][j] = ax[r];
+      red[warp][1][j] = ay[r];
+      red[warp][2][j] = az[r];
+    }
+  }
+  __syncthreads();
+  const double cb = MIXED ? kBiotSavartPacked : kBiotSavart;
+  for (int j = threadIdx.x; j < Q; j += blockDim.x) {
+    double sx = red[0][0][j], sy = red[0][1][j], sz = red[0][2][j];
+    for (int w = 1; w < NW; w++) {
+      sx += red[w][0][j];
+      sy += red[w][1][j];
+      sz += red[w][2][j];
+    }
+    long o = (long)t * Q + j;
+    const double px = g.px[o], py = g.px[pn + o], pz = g.px[2 * pn + o];
+    long oo = ALL_LEAVES ? (long)blockIdx.y * 3 * out_stride + (long)tix * Q + j : o;
+    long st = ALL_LEAVES ? out_stride : pn;
+    out[oo] = cb * (py * sz - pz * sy);
+    out[st + oo] = cb * (pz * sx - px * sz);
+    out[2 * st + oo] = cb * (px * sy - py * sx);
   }
 }
 
@@ -793,7 +998,8 @@ __global__ void __launch_bounds__(kDirectThreads)
     y = ty[i];
     z = tz[i];
   }
-  const float dtx = (float)(x - tcx), dty = (float)(y - tcy), dtz = (float)(z - tcz);
+  const float dtx = (float)((x - tcx) * kPackScale), dty = (float)((y - tcy) * kPackScale),
+              dtz = (float)((z - tcz) * kPackScale);
   long per = (ns + gridDim.y - 1) / gridDim.y;
   long s0 = blockIdx.y * per, s1 = min(ns, s0 + per);
   double ax = 0, ay = 0, az = 0;
@@ -801,11 +1007,12 @@ __global__ void __launch_bounds__(kDirectThreads)
   for (long b = s0; b < s1; b += kDirectThreads) {
     const double scx = sx[b], scy = sy[b], scz = sz[b];
     long k = b + threadIdx.x;
-    tile[threadIdx.x] = k < s1 ? make_float4((float)(sx[k] - scx), (float)(sy[k] - scy), (float)(sz[k] - scz),
-                                             (float)sw[k])
+    tile[threadIdx.x] = k < s1 ? make_float4((float)((sx[k] - scx) * kPackScale), (float)((sy[k] - scy) * kPackScale),
+                                             (float)((sz[k] - scz) * kPackScale), (float)sw[k])
                                : make_float4(0, 0, 0, 0);
     __syncthreads();
-    float bx = (float)(scx - tcx) - dtx, by = (float)(scy - tcy) - dty, bz = (float)(scz - tcz) - dtz;
+    float bx = (float)((scx - tcx) * kPackScale) - dtx, by = (float)((scy - tcy) * kPackScale) - dty,
+          bz = (float)((scz - tcz) * kPackScale) - dtz;
     float fx = 0, fy = 0, fz = 0;
     int cnt = (int)min((long)kDirectThreads, s1 - b);
     for (int m = 0; m < cnt; m++) pair32<true>(bx, by, bz, tile[m], feps, fx, fy, fz);
@@ -816,9 +1023,9 @@ __global__ void __launch_bounds__(kDirectThreads)
   }
   if (i < nt) {
     long o = (long)blockIdx.y * 3 * nt + i;
-    partial[o] = kBiotSavart * (y * az - z * ay);
-    partial[nt + o] = kBiotSavart * (z * ax - x * az);
-    partial[2 * nt + o] = kBiotSavart * (x * ay - y * ax);
+    partial[o] = kBiotSavartPacked * (y * az - z * ay);
+    partial[nt + o] = kBiotSavartPacked * (z * ax - x * az);
+    partial[2 * nt + o] = kBiotSavartPacked * (x * ay - y * ax);
   }
 }
 
@@ -883,16 +1090,13 @@ void launch_copy_strength(const StepGeom& g, const double4* src, double* out, cu
   SB_LAUNCH(k_copy_strength, blocks_for(n, 256), 256, 0, st, g, src, out);
 }
 
-// Subtree depth per launch: 3 levels (85 panels) when the shared memory
-// allows, fewer for large q.
-static int subtree_depth(int q, int fields) {
-  for (int D = 3; D >= 1; D--)
-    if ((long)q * fields * 8 * (((1L << (2 * (D + 1))) - 1) / 3) <= 160 * 1024) return D;
-  return 1;
-}
+// Subtree depth per launch: three levels (85 panels) for small q, one level
+// for large q so that a pass has enough CTAs; shared memory holds the levels
+// plus one scratch level.
+static int subtree_depth(int q) { return q <= 25 ? 3 : 1; }
 
 static size_t subtree_smem(int q, int fields, int D) {
-  return (size_t)q * fields * 8 * (((1L << (2 * (D + 1))) - 1) / 3);
+  return (size_t)q * fields * 8 * ((((1L << (2 * (D + 1))) - 1) / 3) + (1L << (2 * D)));
 }
 
 void launch_upward_fused(const StepGeom& g, int mode, int stage, double dt_s, const double* vprev, const double* x,
@@ -903,7 +1107,7 @@ void launch_upward_fused(const StepGeom& g, int mode, int stage, double dt_s, co
     cudaFuncSetAttribute(k_upward_subtree, cudaFuncAttributeMaxDynamicSharedMemorySize, 164 * 1024);
     attr = true;
   }
-  const int Dmax = subtree_depth(g.q, 1);
+  const int Dmax = subtree_depth(g.q);
   int r = g.levels - 1;  // the bottom of the next subtree
   bool first = true;
   while (first || r > 0) {
@@ -922,7 +1126,7 @@ void launch_downward_fused(const StepGeom& g, double* tgt, double* leaf_out, cud
     cudaFuncSetAttribute(k_downward_subtree, cudaFuncAttributeMaxDynamicSharedMemorySize, 164 * 1024);
     attr = true;
   }
-  const int Dmax = subtree_depth(g.q, 3);
+  const int Dmax = subtree_depth(g.q);
   int r = 0;
   while (r < g.levels - 1) {
     int D = (g.levels - 1 - r) < Dmax ? (g.levels - 1 - r) : Dmax;
@@ -937,6 +1141,22 @@ template <int Q, bool GUARD>
 void interact_qg(const StepGeom& g, int precision, const double4* src, double* out, bool all_leaves, int groups,
                  long out_stride, cudaStream_t st, bool pack) {
   int tp = all_leaves ? g.leaves : g.panels;
+  if constexpr (Q > 32) {
+    dim3 wgrid((unsigned)tp, all_leaves ? groups : 1);
+    const bool mixed = precision == SBSLPM_MIXED;
+    if (mixed && pack) {
+      long pn = (long)g.panels * g.q;
+      SB_LAUNCH(k_pack_mixed, blocks_for(pn, 256), 256, 0, st, g, src, g.srcf);
+    }
+    if (mixed) {
+      if (all_leaves) SB_LAUNCH((k_interact_wide<Q, true, GUARD, true>), wgrid, 128, 0, st, g, src, g.srcf, out, out_stride);
+      else SB_LAUNCH((k_interact_wide<Q, false, GUARD, true>), wgrid, 128, 0, st, g, src, g.srcf, out, out_stride);
+    } else {
+      if (all_leaves) SB_LAUNCH((k_interact_wide<Q, true, GUARD, false>), wgrid, 128, 0, st, g, src, g.srcf, out, out_stride);
+      else SB_LAUNCH((k_interact_wide<Q, false, GUARD, false>), wgrid, 128, 0, st, g, src, g.srcf, out, out_stride);
+    }
+    return;
+  }
   dim3 grid(blocks_for(tp, kWarpsPerBlock), all_leaves ? groups : 1);
   if (precision == SBSLPM_MIXED) {
     long pn = (long)g.panels * g.q;

@@ -8,6 +8,12 @@
 
 namespace sbslpm {
 
+// Mixed precision stores source coordinates scaled by 1/sqrt(2), so that
+// |d'|^2 + eps = |d|^2 / 2 + eps is one chain of fused multiply-adds; the
+// accumulated sum is scaled back by sqrt(2) with the Biot-Savart constant.
+constexpr double kPackScale = 0.70710678118654752440;
+constexpr double kBiotSavartPacked = kBiotSavart * 1.41421356237309504880;
+
 // Static per-problem constants used by the BLI code on the device.
 struct BliTable {
   double cosv[kMaxDegree + 1];  // cos(pi*i/d), computed on the host with libm
@@ -23,7 +29,7 @@ struct StepGeom {
   const int* src_panel;       // [interactions] source panel, list order within a target
   const int* il_row;          // [(panels-leaves)*q] leaf row interpolating a non-leaf proxy
   const double* il_basis;     // [(panels-leaves)*q*q] BLI basis at that leaf
-  const double* child_mat;    // [4][q][q]: basis of parent node l at child c's node k
+  const double* child_1d;     // [2][d+1][d+1]: 1-D basis of parent node a at the node i of a child in the upper (0) / lower (1) half
   const double* pd_centre;    // mixed: panel centres [panels][4] (double)
   float4* srcf;               // mixed: packed sources [panels*q] (workspace)
   unsigned* err;              // device error word
@@ -88,9 +94,13 @@ void launch_bltc_sources(const TreeGeom& tg, const StepGeom& fg, const BliTable&
                          const double* vprev, const double* x, const double* y, const double* z, const double* vors,
                          const double* area, double4* psrc, float4* psrcf, double4* proxy, bool mixed,
                          cudaStream_t st);
+// near: splits x 3 x particles partial sums (splits = source-list splits per target leaf)
 void launch_bltc_near(const TreeGeom& tg, const StepGeom& fg, int precision, const double* x, const double* y,
-                      const double* z, const double4* psrc, const float4* psrcf, double* v, cudaStream_t st);
-void launch_bltc_to_particles(const TreeGeom& tg, const StepGeom& fg, const double* tgt, double* v, cudaStream_t st);
+                      const double* z, const double4* psrc, const float4* psrcf, double* near, int splits,
+                      cudaStream_t st);
+// v = near splits summed + far field interpolated from the leaf proxies
+void launch_bltc_to_particles(const TreeGeom& tg, const StepGeom& fg, const double* tgt, const double* near,
+                              int splits, double* v, cudaStream_t st);
 
 // Counts every kernel launched through the wrappers above.
 long& launch_counter();

@@ -70,6 +70,8 @@ struct sbslpm_ctx {
   int *fface = nullptr, *near_start = nullptr, *near_src = nullptr, *cc_start = nullptr, *cc_src = nullptr;
   double4 *fsrc = nullptr, *psrc = nullptr;
   double* gx = nullptr;  // [3][particles]: the particle grid, for timing the near kernel alone
+  double* near = nullptr;  // [near_splits][3][particles] near-field partial sums
+  int near_splits = 2;
   float4 *fsrcf = nullptr, *psrcf = nullptr;
   double* ftgt = nullptr;
   BliTable ftab{};
@@ -125,6 +127,27 @@ sbslpm_status validate(const sbslpm_config& c) {
   if (!(c.kernel_eps >= 0) || !std::isfinite(c.dt) || !std::isfinite(c.omega))
     return set_last_error("kernel_eps, dt and omega must be finite (kernel_eps >= 0)"), SBSLPM_ERR_CONFIG;
   return SBSLPM_OK;
+}
+
+// One-dimensional BLI basis of the parent's degree-d nodes at the nodes of a
+// child in the upper (h = 0) or lower (h = 1) half of the parent, computed on
+// face 0 as child_to_parent places the child nodes
+// (src/fmm_funcs_impl.hpp:53-64).  out: [2][d+1][d+1].
+void child_basis_1d(const std::vector<sbslpm_panel>& P, const BliTable& tab, int d, std::vector<double>& out,
+                    unsigned& err) {
+  const int n1 = d + 1;
+  out.assign((size_t)2 * n1 * n1, 0.0);
+  const sbslpm_panel& par = P[0];
+  const double lo = par.min_xi * kPi / 4.0, hi = par.max_xi * kPi / 4.0;
+  for (int h = 0; h < 2; h++) {
+    const sbslpm_panel& ch = P[child_of(par, h == 0 ? 0 : 2)];  // child 0: upper half; child 2: lower half
+    const double xo = kPi / 4.0 * 0.5 * (ch.min_xi + ch.max_xi), xs = kPi / 4.0 * 0.5 * (ch.max_xi - ch.min_xi);
+    for (int i = 0; i < n1; i++) {
+      double node = d == 0 ? 0.0 : std::cos(kPi / d * i);
+      if (std::fabs(node) < 1e-16) node = 0;
+      bli_1d(node * xs + xo, lo, hi, d, tab.cosv, tab.w, &out[((size_t)h * n1 + i) * n1], err);
+    }
+  }
 }
 
 // Host precomputation of everything that does not change during a run.
@@ -190,22 +213,13 @@ sbslpm_status precompute(sbslpm_ctx* c) {
   SB_TRY(upload(&c->il_row, il_row));
   SB_TRY(upload(&c->il_basis, il_basis));
 
-  // child-in-parent BLI matrices (child_to_parent / parent_to_child_3,
-  // src/fmm_funcs_impl.hpp:47-70, 138-171), identical for every parent of
-  // the uniform quadtree; built from face 0 and its four children.
+  // child-in-parent BLI bases (child_to_parent / parent_to_child_3,
+  // src/fmm_funcs_impl.hpp:47-70, 138-171), the same for every parent of the
+  // uniform quadtree
   if (c->L > 1) {
-    std::vector<double> mat((size_t)4 * q * q);
-    const sbslpm_panel& par = c->panels[0];
-    for (int ch = 0; ch < 4; ch++) {
-      const sbslpm_panel& k = c->panels[child_of(par, ch)];
-      double xo = kPi / 4.0 * 0.5 * (k.min_xi + k.max_xi), xs = kPi / 4.0 * 0.5 * (k.max_xi - k.min_xi);
-      double eo = kPi / 4.0 * 0.5 * (k.min_eta + k.max_eta), es = kPi / 4.0 * 0.5 * (k.max_eta - k.min_eta);
-      for (int i = 0; i < q; i++)
-        host_bli(&mat[((size_t)ch * q + i) * q], interp[4 * i] * xs + xo, interp[4 * i + 1] * es + eo,
-                 par.min_xi * kPi / 4.0, par.max_xi * kPi / 4.0, par.min_eta * kPi / 4.0, par.max_eta * kPi / 4.0, d,
-                 err);
-    }
-    SB_TRY(upload(&c->child_mat, mat));
+    std::vector<double> c1d;
+    child_basis_1d(c->panels, c->tab, d, c1d, err);
+    SB_TRY(upload(&c->child_mat, c1d));
   }
 
   // interaction list grouped by target panel, list order kept within a target
@@ -273,18 +287,9 @@ sbslpm_status precompute_tree(sbslpm_ctx* c) {
   }
   unsigned err = 0;
   if (c->Lf > 1) {
-    std::vector<double> mat((size_t)4 * qx * qx);
-    const sbslpm_panel& par = c->fpanels[0];
-    for (int ch = 0; ch < 4; ch++) {
-      const sbslpm_panel& k = c->fpanels[child_of(par, ch)];
-      double xo = kPi / 4.0 * 0.5 * (k.min_xi + k.max_xi), xs = kPi / 4.0 * 0.5 * (k.max_xi - k.min_xi);
-      double eo = kPi / 4.0 * 0.5 * (k.min_eta + k.max_eta), es = kPi / 4.0 * 0.5 * (k.max_eta - k.min_eta);
-      for (int i = 0; i < qx; i++)
-        host_bli(&mat[((size_t)ch * qx + i) * qx], interp_n[4 * i] * xs + xo, interp_n[4 * i + 1] * es + eo,
-                 par.min_xi * kPi / 4.0, par.max_xi * kPi / 4.0, par.min_eta * kPi / 4.0, par.max_eta * kPi / 4.0, n,
-                 err);
-    }
-    SB_TRY(upload(&c->fchild, mat));
+    std::vector<double> c1d;
+    child_basis_1d(c->fpanels, c->ftab, n, c1d, err);
+    SB_TRY(upload(&c->fchild, c1d));
   }
 
   // leaf-box basis of the particles of the first tree leaf (the same for every leaf)
@@ -352,6 +357,7 @@ sbslpm_status precompute_tree(sbslpm_ctx* c) {
   SB_CUDA(cudaMemcpy(c->fsrc, init.data(), sizeof(double4) * pn, cudaMemcpyHostToDevice));
   SB_TRY(dalloc(&c->ftgt, 3 * pn));
   SB_TRY(dalloc(&c->psrc, N));
+  SB_TRY(dalloc(&c->near, (size_t)c->near_splits * 3 * N));
   if (c->cfg.precision == SBSLPM_MIXED) {
     SB_TRY(dalloc(&c->fsrcf, pn));
     SB_TRY(dalloc(&c->psrcf, N));
@@ -396,7 +402,7 @@ void fill_geom(sbslpm_ctx* c) {
   g.src_panel = c->src_panel;
   g.il_row = c->il_row;
   g.il_basis = c->il_basis;
-  g.child_mat = c->child_mat;
+  g.child_1d = c->child_mat;
   g.pd_centre = c->centre;
   g.srcf = c->srcf;
   g.err = c->err;
@@ -413,7 +419,7 @@ void fill_geom(sbslpm_ctx* c) {
     f.px = c->fpx;
     f.tgt_start = c->cc_start;
     f.src_panel = c->cc_src;
-    f.child_mat = c->fchild;
+    f.child_1d = c->fchild;
     f.pd_centre = c->fcentre;
     f.srcf = c->fsrcf;
     f.err = c->err;
@@ -450,8 +456,8 @@ void velocity_eval(sbslpm_ctx* c, int stage, double dt_s, const double* vprev, c
     launch_upward_fused(fg, 2, 0, 0.0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, c->fsrc, mixed, st);
     launch_interactions_only(fg, c->cfg.precision, c->fsrc, c->ftgt, st);
     launch_downward_fused(fg, c->ftgt, nullptr, st);
-    launch_bltc_near(c->tgeom, fg, c->cfg.precision, x, y, z, c->psrc, c->psrcf, v, st);
-    launch_bltc_to_particles(c->tgeom, fg, c->ftgt, v, st);
+    launch_bltc_near(c->tgeom, fg, c->cfg.precision, x, y, z, c->psrc, c->psrcf, c->near, c->near_splits, st);
+    launch_bltc_to_particles(c->tgeom, fg, c->ftgt, c->near, c->near_splits, v, st);
     return;
   }
   launch_upward_fused(g, 0, stage, dt_s, vprev, x, y, z, vors, area, c->src, mixed, st);
@@ -648,7 +654,7 @@ sbslpm_status sbslpm_destroy(sbslpm_ctx* c) {
   void* bufs[] = {c->px, c->il_basis, c->child_mat, c->centre, c->tgt_start, c->src_panel, c->il_row, c->src,
                   c->srcf, c->tgt, c->vbuf, c->partial, c->newvor, c->newtr, c->dep, c->err, c->fpx, c->fchild,
                   c->fcentre, c->flx, c->fly, c->fbounds, c->fface, c->near_start, c->near_src, c->cc_start,
-                  c->cc_src, c->fsrc, c->psrc, c->fsrcf, c->psrcf, c->ftgt, c->gx};
+                  c->cc_src, c->fsrc, c->psrc, c->fsrcf, c->psrcf, c->ftgt, c->gx, c->near};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (c->h_err) cudaFreeHost(c->h_err);
@@ -868,14 +874,13 @@ sbslpm_status sbslpm_time_interactions(sbslpm_ctx* c, int reps, double* ms_per_l
   if (c->cfg.velocity != SBSLPM_VEL_FMM) return set_last_error("context has no interaction list"), SBSLPM_ERR_CONFIG;
   cudaStream_t st = c->stream();
   if (c->tree) {  // the dominant kernel is the near-field particle kernel
-    double* v = c->vbuf;
     cudaEvent_t a, b;
     SB_CUDA(cudaEventCreate(&a));
     SB_CUDA(cudaEventCreate(&b));
     SB_CUDA(cudaEventRecord(a, st));
     for (int r = 0; r < reps; r++)
       launch_bltc_near(c->tgeom, c->fgeom, c->cfg.precision, c->gx, c->gx + c->tgeom.N, c->gx + 2 * c->tgeom.N,
-                       c->psrc, c->psrcf, v, st);
+                       c->psrc, c->psrcf, c->near, c->near_splits, st);
     SB_CUDA(cudaEventRecord(b, st));
     SB_CUDA(cudaEventSynchronize(b));
     float tms = 0;
