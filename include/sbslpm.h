@@ -70,6 +70,11 @@ typedef struct {
    * irregular-point tree, src/fmm_interactions/swe_vel_impl.hpp:149-288). */
   int proxy_degree;
   int leaf_size; /* RunConfig::leaf_size: particles per treecode leaf (proxy_degree > 0) */
+  /* Shallow water: the factor of the height Laplacian in the divergence
+   * tendency, g/a.  The reference hard-codes 9.81/6371000.0 (Earth, height in
+   * units of the radius; src/swe_time_step_2_impl.hpp:103); 1 on the unit
+   * sphere with the height field holding g*h. */
+  double g_over_a;
 } sbslpm_config;
 
 /* Same fields and order as the reference's CubedSpherePanel
@@ -188,6 +193,70 @@ sbslpm_status sbslpm_bve_departure(sbslpm_ctx* ctx, const double* xcos, const do
 sbslpm_status sbslpm_bve_remap(sbslpm_ctx* ctx, const double* zcos, const double* dep_x, const double* dep_y,
                                const double* dep_z, const double* vors, const double* tracers, double* new_vors,
                                double* new_tracers);
+
+/* ---------------- shallow water, SWE v2 (device pointers) ---------------- */
+
+/* The shallow-water entry points need interp_degree >= 2 (the one-sided
+ * finite-difference stencils of src/deriv_funcs_impl.hpp:94-185 read three
+ * nodes) and the spectral FMM (proxy_degree 0) or the direct velocity.
+ * Fields are [leaf][q]; vel_* hold the velocity, base_* the base tendencies
+ * the driver computes once (sbslpm_swe_init).  The reference's
+ * one_d_no_of_points / two_d_to_1d arguments are not taken: the context keeps
+ * the same map (sbslpm_cubed_sphere_2d_to_1d), built once from its grid. */
+
+/* Replaces swe_back_rk4_step_2 (src/swe_time_step_2.cpp:785-1035, declared in
+ * src/swe_time_step_2.hpp:7-14): four velocity evaluations of the vorticity
+ * (displaced sources) and divergence (fixed sources) fields, finite-difference
+ * tendencies, forward-Euler arrival values, backward RK4 departure points and
+ * the remap of vorticity and tracers.  vors, divs, height and tracers are
+ * advanced in place; vel_x/y/z receive the first-stage velocity (unified
+ * across panel edges as the reference leaves it).  time is unused. */
+sbslpm_status sbslpm_swe_step(sbslpm_ctx* ctx, const double* xcos, const double* ycos, const double* zcos,
+                              const double* area, double* vors, double* divs, double* height, double* vel_x,
+                              double* vel_y, double* vel_z, double* tracers, const double* base_vor_tend,
+                              const double* base_div_tend, const double* base_h_tend, double time);
+/* nsteps steps of the reference driver's loop (executables/swe_time_evo.cpp:413-418):
+ * each step followed by unify_boundary_vals of vors, divs and height;
+ * captured once as a CUDA graph and replayed. */
+sbslpm_status sbslpm_swe_run(sbslpm_ctx* ctx, const double* xcos, const double* ycos, const double* zcos,
+                             const double* area, double* vors, double* divs, double* height, double* vel_x,
+                             double* vel_y, double* vel_z, double* tracers, const double* base_vor_tend,
+                             const double* base_div_tend, const double* base_h_tend, double time, int nsteps);
+/* The driver's set-up before its time loop (executables/swe_time_evo.cpp:352-410):
+ * velocity of the undisplaced vorticity and divergence (unified), and the
+ * base tendencies computed from it (unified).  vel_* and base_* are written. */
+sbslpm_status sbslpm_swe_init(sbslpm_ctx* ctx, const double* xcos, const double* ycos, const double* zcos,
+                              const double* area, const double* vors, const double* divs, const double* height,
+                              double* vel_x, double* vel_y, double* vel_z, double* base_vor_tend,
+                              double* base_div_tend, double* base_h_tend);
+/* Replaces swe_tendency_computation_2 (src/swe_time_step_2_impl.hpp:10-128)
+ * over every leaf panel: vorticity, divergence and height tendencies from the
+ * velocity, vorticity, divergence, height and surface (the height with
+ * topography) fields. */
+sbslpm_status sbslpm_swe_tendencies(sbslpm_ctx* ctx, const double* xcos, const double* ycos, const double* zcos,
+                                    const double* vel_x, const double* vel_y, const double* vel_z,
+                                    const double* vors, const double* divs, const double* height,
+                                    const double* surface, double* vor_tend, double* div_tend, double* h_tend);
+/* Replaces unify_boundary_vals (src/initialize_cubed_sphere.cpp:364-370):
+ * every copy of a grid point shared by several panels gets the mean of the
+ * copies (summed in [leaf][q] order). */
+sbslpm_status sbslpm_unify_boundary_vals(sbslpm_ctx* ctx, double* vals);
+/* Replaces swe_vel_interactions_2 (src/fmm_interactions/swe_vel.cpp:39-67):
+ * proxy-target velocities of vorticity sources at proj(proxy + disp) and
+ * divergence sources at the fixed proxies; [panel][q] inputs; target_1..3
+ * are accumulated into, as in the reference. */
+sbslpm_status sbslpm_swe_vel_interactions(sbslpm_ctx* ctx, const double* disp_x, const double* disp_y,
+                                          const double* disp_z, const double* source_vor, const double* source_div,
+                                          double* target_1, double* target_2, double* target_3);
+/* Host.  Replaces cubed_sphere_2d_to_1d (src/initialize_cubed_sphere.cpp:290-326)
+ * with a hashed search (the reference compares every point with every
+ * distinct point found so far): two_d_to_1d [leaf][q] receives the index of
+ * each grid point's distinct position (numbered in order of first appearance,
+ * coordinates equal within 1e-15), counts [unique] how many grid points share
+ * it.  counts must hold leaf_count*interp_degree^2 + 2 entries; *unique
+ * receives the number found. */
+sbslpm_status sbslpm_cubed_sphere_2d_to_1d(long n_leaves, int degree, const double* xcos, const double* ycos,
+                                           const double* zcos, int* two_d_to_1d, int* counts, long* unique);
 
 /* ---------------- direct sums (device pointers, no context) ---------------- */
 

@@ -84,6 +84,37 @@ void bve_back_rk4_step(const RunConfig& run_config, V2& xcos, V2& ycos, V2& zcos
         "sbslpm_bve_step");
 }
 
+// swe_back_rk4_step_2 (src/swe_time_step_2.cpp:785-1035; declared in
+// src/swe_time_step_2.hpp:7-14, called from executables/swe_time_evo.cpp:415).
+// The grid-point map the reference passes (one_d_no_of_points, two_d_to_1d)
+// is rebuilt inside the library from the same grid; only its size is checked.
+// The library's g/a is the reference's hard-coded 9.81/6371000.
+template <class RunConfig, class V2, class VPanels, class VList, class V3, class VI1, class VI2>
+void swe_back_rk4_step_2(const RunConfig& run_config, V2& xcos, V2& ycos, V2& zcos, V2& area, V2& vors, V2& divs,
+                         V2& height, V2& interp_vals, VPanels& cubed_sphere_panels, VList& /*interaction_list*/,
+                         V2& vel_x, V2& vel_y, V2& vel_z, V3& passive_tracers, V2& base_vor_tend, V2& base_div_tend,
+                         V2& base_h_tend, VI1& one_d_no_of_points, VI2& two_d_to_1d, double time) {
+  sbslpm_ctx* c = context_for(run_config, static_cast<double>(run_config.delta_t));
+  long sizes[4];
+  check(sbslpm_get_sizes(c, sizes), "sbslpm_get_sizes");
+  if ((long)cubed_sphere_panels.extent(0) != sizes[0] || (long)xcos.extent(0) != sizes[1] ||
+      (long)xcos.extent(1) != sizes[2] || (long)interp_vals.extent(0) != sizes[2] ||
+      (long)two_d_to_1d.extent(0) != sizes[1] || (long)one_d_no_of_points.extent(0) < 1)
+    throw std::runtime_error("swe_back_rk4_step_2: view sizes do not match run_config");
+  double* tr = run_config.tracer_count > 0 ? passive_tracers.data() : nullptr;
+  check(sbslpm_swe_step(c, xcos.data(), ycos.data(), zcos.data(), area.data(), vors.data(), divs.data(),
+                        height.data(), vel_x.data(), vel_y.data(), vel_z.data(), tr, base_vor_tend.data(),
+                        base_div_tend.data(), base_h_tend.data(), time),
+        "sbslpm_swe_step");
+}
+
+// unify_boundary_vals (src/initialize_cubed_sphere.cpp:364-370).
+template <class RunConfig, class VI1, class VI2, class V2>
+void unify_boundary_vals(const RunConfig& run_config, VI1& /*one_d_no_of_points*/, VI2& /*two_d_to_1d*/, V2& vals) {
+  sbslpm_ctx* c = context_for(run_config, static_cast<double>(run_config.delta_t));
+  check(sbslpm_unify_boundary_vals(c, vals.data()), "sbslpm_unify_boundary_vals");
+}
+
 // direct_sum_inv_lap (src/direct_sum.cpp:8-15) over the caller's row block
 // [oned_lb, oned_ub) as the reference does; with one GPU the block is usually
 // all points.  The reference then all-reduces soln across ranks.

@@ -203,6 +203,11 @@ class Ref:
         L.ref_point_locate_panel.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_double]
         L.ref_interp_vals_bli.argtypes = [_D] + [ctypes.c_double] * 6 + [ctypes.c_int]
         L.ref_num_threads.restype = ctypes.c_int
+        L.ref_swe_map.restype = ctypes.c_int
+        for name in ("ref_unify", "ref_swe_vel_interactions", "ref_swe_tendency", "ref_swe_init", "ref_swe_step"):
+            getattr(L, name).restype = None
+        L.ref_swe_step.argtypes = [ctypes.c_void_p] + [_D] * 10 + [_I, _I, ctypes.c_double, ctypes.c_int,
+                                                                   ctypes.c_int]
 
     def create(self, levels, degree, theta, eps, omega, delta_t, tracer_count):
         h = ctypes.c_void_p(self.lib.ref_create(levels, degree, theta, eps, omega, delta_t, tracer_count))
@@ -288,3 +293,51 @@ class Ref:
         out = np.zeros(n)
         self.lib.ref_direct_sum_inv_lap(n, _dp(x), _dp(y), _dp(z), _dp(area), _dp(pots), _dp(out))
         return out
+
+    # ---- shallow water (SWE v2) -------------------------------------------
+
+    def swe_map(self, c):
+        """cubed_sphere_2d_to_1d: (two_d_to_1d A x q int32, counts U int32)."""
+        U = c["A"] * c["degree"] ** 2 + 2
+        m = np.zeros((c["A"], c["q"]), np.int32)
+        n = np.zeros(U, np.int32)
+        u = self.lib.ref_swe_map(c["h"], _ip(m), _ip(n))
+        assert u == U
+        return m, n
+
+    def unify(self, c, vals, smap):
+        v = np.array(vals, dtype=np.float64, order="C")
+        self.lib.ref_unify(c["h"], _dp(v), _ip(smap[0]), _ip(smap[1]))
+        return v
+
+    def swe_vel_interactions(self, c, dx, dy, dz, src_vor, src_div):
+        t = [np.zeros((c["P"], c["q"])) for _ in range(3)]
+        a = [np.ascontiguousarray(v, dtype=np.float64) for v in (dx, dy, dz, src_vor, src_div)]
+        self.lib.ref_swe_vel_interactions(c["h"], *[_dp(v) for v in a], *[_dp(v) for v in t])
+        return t
+
+    def swe_tendency(self, c, vel, vors, divs, height, surface):
+        a = [np.ascontiguousarray(v, dtype=np.float64) for v in (*vel, vors, divs, height, surface)]
+        out = [np.zeros((c["A"], c["q"])) for _ in range(3)]
+        self.lib.ref_swe_tendency(c["h"], *[_dp(v) for v in a], *[_dp(v) for v in out])
+        return out
+
+    def swe_init(self, c, vors, divs, height, smap):
+        a = [np.ascontiguousarray(v, dtype=np.float64) for v in (vors, divs, height)]
+        vel = [np.zeros((c["A"], c["q"])) for _ in range(3)]
+        base = [np.zeros((c["A"], c["q"])) for _ in range(3)]
+        self.lib.ref_swe_init(c["h"], *[_dp(v) for v in a], *[_dp(v) for v in vel], *[_dp(v) for v in base],
+                              _ip(smap[0]), _ip(smap[1]))
+        return vel, base
+
+    def swe_step(self, c, vors, divs, height, base, smap, vel=None, tracers=None, time=0.0, nsteps=1,
+                 driver_unify=False):
+        A, q, T = c["A"], c["q"], c["T"]
+        v, d, h = (np.array(a, dtype=np.float64, order="C") for a in (vors, divs, height))
+        vel = [np.zeros((A, q)) for _ in range(3)] if vel is None else [np.array(a, dtype=np.float64, order="C")
+                                                                        for a in vel]
+        tr = np.zeros((A, q, max(T, 1))) if tracers is None else np.array(tracers, dtype=np.float64, order="C")
+        b = [np.ascontiguousarray(a, dtype=np.float64) for a in base]
+        self.lib.ref_swe_step(c["h"], _dp(v), _dp(d), _dp(h), *[_dp(a) for a in vel], _dp(tr),
+                              *[_dp(a) for a in b], _ip(smap[0]), _ip(smap[1]), time, nsteps, int(driver_unify))
+        return v, d, h, vel, (tr if T else None)

@@ -30,33 +30,9 @@
 #include "initial_conditions.hpp"
 #include "direct_sum.hpp"
 #include "bve_time_step.cpp"
+#include "ref_ctx.hpp"
 
-namespace {
-using V2 = Kokkos::View<double**, Kokkos::LayoutRight>;
-using V2H = Kokkos::View<double**, Kokkos::LayoutRight, Kokkos::HostSpace>;
-using V3 = Kokkos::View<double***, Kokkos::LayoutRight>;
-
-struct RefCtx {
-  RunConfig rc;
-  Kokkos::View<CubedSpherePanel*, Kokkos::HostSpace> panels_h;
-  Kokkos::View<CubedSpherePanel*> panels;
-  V2H interp_h;
-  V2 interp;
-  V2H xcos_h, ycos_h, zcos_h, area_h;
-  V2 xcos, ycos, zcos, area;
-  Kokkos::View<interact_pair*, Kokkos::HostSpace> list_h;
-  Kokkos::View<interact_pair*> list;
-  V2 proxy_source;
-  int q;
-};
-
-void copy_in(const V2& v, const double* src) {
-  std::memcpy(v.data(), src, sizeof(double) * v.size());
-}
-void copy_out(const V2& v, double* dst) {
-  std::memcpy(dst, v.data(), sizeof(double) * v.size());
-}
-}  // namespace
+using namespace refh;
 
 extern "C" {
 

@@ -18,6 +18,13 @@
 
 #include <algorithm>
 #include <cmath>
+// The C++ <math.h> / <stdlib.h> wrappers declare the floating-point ::abs
+// overloads in the global namespace, as the real Kokkos headers' includes do;
+// the reference calls unqualified abs() on doubles
+// (src/initialize_cubed_sphere.cpp:305), which would otherwise bind to the
+// C library's int abs(int).
+#include <math.h>
+#include <stdlib.h>
 #include <cstddef>
 #include <cstdio>
 #include <cstdlib>

@@ -30,6 +30,7 @@ FP64, MIXED = 0, 1
 VEL_FMM, VEL_DIRECT = 0, 1
 
 _D = ctypes.POINTER(ctypes.c_double)
+_I = ctypes.POINTER(ctypes.c_int)
 _VP = ctypes.c_void_p
 
 
@@ -55,6 +56,7 @@ class Config(ctypes.Structure):
         ("exact_cc", ctypes.c_int),
         ("proxy_degree", ctypes.c_int),
         ("leaf_size", ctypes.c_int),
+        ("g_over_a", ctypes.c_double),
     ]
 
 
@@ -112,6 +114,14 @@ def lib() -> ctypes.CDLL:
                                         ctypes.c_double, ctypes.c_int, _VP, _VP, _VP, _VP]
     L.sbslpm_direct_sum_bve_noalloc.argtypes = L.sbslpm_direct_sum_bve.argtypes
     L.sbslpm_direct_sum_inv_lap.argtypes = [ctypes.c_long] + [_VP] * 7
+    L.sbslpm_swe_step.argtypes = [_VP] + [_VP] * 14 + [ctypes.c_double]
+    L.sbslpm_swe_run.argtypes = [_VP] + [_VP] * 14 + [ctypes.c_double, ctypes.c_int]
+    L.sbslpm_swe_init.argtypes = [_VP] * 14
+    L.sbslpm_swe_tendencies.argtypes = [_VP] * 14
+    L.sbslpm_unify_boundary_vals.argtypes = [_VP] * 2
+    L.sbslpm_swe_vel_interactions.argtypes = [_VP] * 9
+    L.sbslpm_cubed_sphere_2d_to_1d.argtypes = [ctypes.c_long, ctypes.c_int, _D, _D, _D, _I, _I,
+                                               ctypes.POINTER(ctypes.c_long)]
     L.sbslpm_time_interactions.argtypes = [_VP, ctypes.c_int, _D, _D]
     L.sbslpm_measure_fma_peak.argtypes = [ctypes.c_int, ctypes.c_double, _D]
     _lib = L
@@ -194,6 +204,20 @@ def interp_vals_bli(xi, eta, min_xi, max_xi, min_eta, max_eta, degree) -> np.nda
     _check(lib().sbslpm_interp_vals_bli(out.ctypes.data_as(_D), xi, eta, min_xi, max_xi, min_eta, max_eta, degree),
            "sbslpm_interp_vals_bli")
     return out
+
+
+def cubed_sphere_2d_to_1d(x: np.ndarray, y: np.ndarray, z: np.ndarray, degree: int):
+    """cubed_sphere_2d_to_1d (src/initialize_cubed_sphere.cpp:290-326) on host
+    arrays [leaf][q]: (two_d_to_1d int32 [leaf][q], counts int32 [unique])."""
+    x, y, z = (np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z))
+    A = x.shape[0]
+    m = np.zeros(x.shape, np.int32)
+    counts = np.zeros(A * degree * degree + 2, np.int32)
+    u = ctypes.c_long(0)
+    _check(lib().sbslpm_cubed_sphere_2d_to_1d(A, degree, *[a.ctypes.data_as(_D) for a in (x, y, z)],
+                                              m.ctypes.data_as(_I), counts.ctypes.data_as(_I), ctypes.byref(u)),
+           "sbslpm_cubed_sphere_2d_to_1d")
+    return m, counts[: u.value].copy()
 
 
 def point_locate_panel(panels, x, y, z) -> int:
@@ -297,6 +321,60 @@ class Context:
             (xcos, "xcos"), (ycos, "ycos"), (zcos, "zcos"), (area, "area"), (vors, "vors"), (vel_x, "vel_x"),
             (vel_y, "vel_y"), (vel_z, "vel_z"))], _dev(tracers, "tracers"), float(time), int(nsteps)),
             "sbslpm_bve_run")
+
+    # -- shallow water (SWE v2) ------------------------------------------
+    def swe_back_rk4_step_2(self, xcos, ycos, zcos, area, vors, divs, height, vel_x, vel_y, vel_z, tracers,
+                            base_vor_tend, base_div_tend, base_h_tend, time=0.0):
+        """swe_back_rk4_step_2 (src/swe_time_step_2.cpp:785-1035): vors, divs, height,
+        vel_*, tracers in place."""
+        lq = (self.leaf_count, self.q)
+        self._sync_stream()
+        _check(lib().sbslpm_swe_step(self._h, *[_dev(t, n, lq) for t, n in (
+            (xcos, "xcos"), (ycos, "ycos"), (zcos, "zcos"), (area, "area"), (vors, "vors"), (divs, "divs"),
+            (height, "height"), (vel_x, "vel_x"), (vel_y, "vel_y"), (vel_z, "vel_z"))], _dev(tracers, "tracers"),
+            *[_dev(t, n, lq) for t, n in ((base_vor_tend, "base_vor_tend"), (base_div_tend, "base_div_tend"),
+                                          (base_h_tend, "base_h_tend"))], float(time)), "sbslpm_swe_step")
+
+    def swe_run(self, xcos, ycos, zcos, area, vors, divs, height, vel_x, vel_y, vel_z, tracers, base_vor_tend,
+                base_div_tend, base_h_tend, time=0.0, nsteps=1):
+        """nsteps of the driver loop (step + unify of vors, divs, height) from one CUDA graph."""
+        lq = (self.leaf_count, self.q)
+        self._sync_stream()
+        _check(lib().sbslpm_swe_run(self._h, *[_dev(t, n, lq) for t, n in (
+            (xcos, "xcos"), (ycos, "ycos"), (zcos, "zcos"), (area, "area"), (vors, "vors"), (divs, "divs"),
+            (height, "height"), (vel_x, "vel_x"), (vel_y, "vel_y"), (vel_z, "vel_z"))], _dev(tracers, "tracers"),
+            *[_dev(t, n, lq) for t, n in ((base_vor_tend, "base_vor_tend"), (base_div_tend, "base_div_tend"),
+                                          (base_h_tend, "base_h_tend"))], float(time), int(nsteps)),
+            "sbslpm_swe_run")
+
+    def swe_init(self, xcos, ycos, zcos, area, vors, divs, height, vel_x, vel_y, vel_z, base_vor_tend,
+                 base_div_tend, base_h_tend):
+        """The driver's set-up: unified initial velocity and base tendencies (written)."""
+        lq = (self.leaf_count, self.q)
+        self._sync_stream()
+        _check(lib().sbslpm_swe_init(self._h, *[_dev(t, "field", lq) for t in (
+            xcos, ycos, zcos, area, vors, divs, height, vel_x, vel_y, vel_z, base_vor_tend, base_div_tend,
+            base_h_tend)]), "sbslpm_swe_init")
+
+    def swe_tendencies(self, xcos, ycos, zcos, vel_x, vel_y, vel_z, vors, divs, height, surface, vor_tend,
+                       div_tend, h_tend):
+        """swe_tendency_computation_2 over every leaf panel."""
+        lq = (self.leaf_count, self.q)
+        self._sync_stream()
+        _check(lib().sbslpm_swe_tendencies(self._h, *[_dev(t, "field", lq) for t in (
+            xcos, ycos, zcos, vel_x, vel_y, vel_z, vors, divs, height, surface, vor_tend, div_tend, h_tend)]),
+            "sbslpm_swe_tendencies")
+
+    def unify_boundary_vals(self, vals):
+        """unify_boundary_vals (src/initialize_cubed_sphere.cpp:364-370), in place."""
+        self._sync_stream()
+        _check(lib().sbslpm_unify_boundary_vals(self._h, _dev(vals, "vals", (self.leaf_count, self.q))),
+               "sbslpm_unify_boundary_vals")
+
+    def swe_vel_interactions(self, disp_x, disp_y, disp_z, source_vor, source_div, t1, t2, t3):
+        self._sync_stream()
+        _check(lib().sbslpm_swe_vel_interactions(self._h, *[_dev(t, "field") for t in (
+            disp_x, disp_y, disp_z, source_vor, source_div, t1, t2, t3)]), "sbslpm_swe_vel_interactions")
 
     def time_interactions(self, reps: int = 5):
         """(ms per launch, pair evaluations per launch) of the interaction kernel alone."""

@@ -27,29 +27,15 @@
 
 #include "../../include/sbslpm.h"
 #include "bve_kernels.cuh"
+#include "device_common.cuh"
 
 namespace sbslpm {
 
-long& launch_counter();
-
 namespace {
 
+using namespace dev;
+
 constexpr int kThreads = 256;
-
-__device__ __forceinline__ double recip_nr(double d) {
-  double r;
-  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(d));
-  double e = fma(-d, r, 1.0);
-  r = fma(r, e, r);
-  e = fma(-d, r, 1.0);
-  return fma(r, e, r);
-}
-
-__device__ __forceinline__ float recip_f32(float d) {
-  float r;
-  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(d));
-  return r;
-}
 
 // Barycentric Lagrange basis of degree n on Chebyshev extrema of [lo, hi]
 // without the reference's range check: displaced sources may sit slightly
@@ -188,23 +174,7 @@ __global__ void __launch_bounds__(NT)
 // (x0,x1,y0,y1),(z0,z1,w0,w1), so that every operand of the pair arithmetic
 // is a register pair and the paired FP32 instructions of sm_100
 // (FADD2 / FFMA2 / FMUL2) evaluate two pairs per instruction; a missing
-// partner of an odd source count has zero strength.
-template <bool GUARD>
-__device__ __forceinline__ void pair32x2(const float2 bx, const float2 by, const float2 bz, const float2 sx,
-                                         const float2 sy, const float2 sz, const float2 sw, const float2 eps2,
-                                         float2& ax, float2& ay, float2& az) {
-  const float2 dx = __fadd2_rn(bx, sx), dy = __fadd2_rn(by, sy), dz = __fadd2_rn(bz, sz);
-  const float2 den = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, eps2)));
-  float2 g = __fmul2_rn(sw, make_float2(recip_f32(den.x), recip_f32(den.y)));
-  if (GUARD) {
-    g.x = den.x > 0.0f ? g.x : 0.0f;
-    g.y = den.y > 0.0f ? g.y : 0.0f;
-  }
-  ax = __ffma2_rn(g, dx, ax);
-  ay = __ffma2_rn(g, dy, ay);
-  az = __ffma2_rn(g, dz, az);
-}
-
+// partner of an odd source count has zero strength (pair32x2).
 template <int NT, int TPT, bool GUARD>
 __global__ void __launch_bounds__(NT)
     k_bltc_near32(TreeGeom tg, StepGeom fg, const double* __restrict__ x, const double* __restrict__ y,
@@ -326,15 +296,9 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
-inline unsigned blocks_for(long n, int t) { return (unsigned)((n + t - 1) / t); }
-
 }  // namespace
 
-#define SB_LAUNCH(kernel, grid, block, shmem, st, ...)      \
-  do {                                                     \
-    kernel<<<grid, block, shmem, st>>>(__VA_ARGS__);       \
-    launch_counter()++;                                    \
-  } while (0)
+using dev::blocks_for;
 
 void launch_bltc_sources(const TreeGeom& tg, const StepGeom& fg, const BliTable& tab, int stage, double dt_s,
                          const double* vprev, const double* x, const double* y, const double* z, const double* vors,

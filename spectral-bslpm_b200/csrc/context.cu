@@ -10,9 +10,8 @@
 #include <string>
 #include <vector>
 
-#include "bve_kernels.cuh"
+#include "context_internal.hpp"
 #include "geometry.cuh"
-#include "internal.hpp"
 
 using namespace sbslpm;
 
@@ -23,87 +22,7 @@ thread_local std::string g_last_error;
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 }  // namespace sbslpm
 
-#define SB_CUDA(call)                                                                      \
-  do {                                                                                     \
-    cudaError_t e_ = (call);                                                               \
-    if (e_ != cudaSuccess) {                                                               \
-      set_last_error(std::string(#call) + ": " + cudaGetErrorString(e_));                 \
-      return SBSLPM_ERR_CUDA;                                                              \
-    }                                                                                      \
-  } while (0)
-
-struct GraphKey {
-  const void* p[9];
-  bool operator==(const GraphKey& o) const { return std::memcmp(p, o.p, sizeof p) == 0; }
-};
-
-struct sbslpm_ctx {
-  sbslpm_config cfg{};
-  int L = 0, d = 0, q = 0, P = 0, A = 0, off = 0;
-  long I = 0;
-  std::vector<sbslpm_panel> panels;
-  std::vector<sbslpm_interact_pair> list;
-  cudaStream_t user_stream = nullptr, own_stream = nullptr;
-  bool user_stream_set = false;  // set_stream(NULL) selects the legacy default stream
-  // static device data
-  double *px = nullptr, *il_basis = nullptr, *child_mat = nullptr, *centre = nullptr;
-  int *tgt_start = nullptr, *src_panel = nullptr, *il_row = nullptr;
-  // workspace
-  double4* src = nullptr;
-  float4* srcf = nullptr;
-  double *tgt = nullptr, *vbuf = nullptr, *partial = nullptr, *newvor = nullptr, *newtr = nullptr, *dep = nullptr;
-  int groups = 1;
-  unsigned* err = nullptr;
-  unsigned* h_err = nullptr;
-  BliTable tab{};
-  StepGeom geom{};
-  cudaGraphExec_t graph = nullptr;
-  GraphKey graph_key{};
-  long launches_per_step = 0;
-
-  // treecode with decoupled proxy degree (proxy_degree > 0)
-  bool tree = false;
-  int Lf = 0, n = 0, qx = 0, Pf = 0, Af = 0, npl = 0;
-  long n_near = 0, n_cc = 0;
-  std::vector<sbslpm_panel> fpanels;
-  double *fpx = nullptr, *fchild = nullptr, *fcentre = nullptr, *flx = nullptr, *fly = nullptr, *fbounds = nullptr;
-  int *fface = nullptr, *near_start = nullptr, *near_src = nullptr, *cc_start = nullptr, *cc_src = nullptr;
-  double4 *fsrc = nullptr, *psrc = nullptr;
-  double* gx = nullptr;  // [3][particles]: the particle grid, for timing the near kernel alone
-  double* near = nullptr;  // [near_splits][3][particles] near-field partial sums
-  int near_splits = 2;
-  float4 *fsrcf = nullptr, *psrcf = nullptr;
-  double* ftgt = nullptr;
-  BliTable ftab{};
-  StepGeom fgeom{};
-  TreeGeom tgeom{};
-
-  cudaStream_t stream() const { return user_stream_set ? user_stream : own_stream; }
-};
-
 namespace {
-
-template <class T>
-sbslpm_status dalloc(T** p, size_t count) {
-  *p = nullptr;
-  if (count == 0) return SBSLPM_OK;
-  SB_CUDA(cudaMalloc(reinterpret_cast<void**>(p), sizeof(T) * count));
-  return SBSLPM_OK;
-}
-
-template <class T>
-sbslpm_status upload(T** p, const std::vector<T>& h) {
-  sbslpm_status s = dalloc(p, h.size());
-  if (s != SBSLPM_OK) return s;
-  if (!h.empty()) SB_CUDA(cudaMemcpy(*p, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
-  return SBSLPM_OK;
-}
-
-#define SB_TRY(expr)                           \
-  do {                                         \
-    sbslpm_status s_ = (expr);                 \
-    if (s_ != SBSLPM_OK) return s_;            \
-  } while (0)
 
 sbslpm_status validate(const sbslpm_config& c) {
   if (c.levels < 1 || c.levels > 12) return set_last_error("levels must be in 1..12"), SBSLPM_ERR_CONFIG;
@@ -124,7 +43,7 @@ sbslpm_status validate(const sbslpm_config& c) {
     while (npl * 4 <= c.leaf_size) npl *= 4;
     if (npl > 512) return set_last_error("treecode leaves hold at most 512 particles"), SBSLPM_ERR_CONFIG;
   }
-  if (!(c.kernel_eps >= 0) || !std::isfinite(c.dt) || !std::isfinite(c.omega))
+  if (!(c.kernel_eps >= 0) || !std::isfinite(c.dt) || !std::isfinite(c.omega) || !std::isfinite(c.g_over_a))
     return set_last_error("kernel_eps, dt and omega must be finite (kernel_eps >= 0)"), SBSLPM_ERR_CONFIG;
   return SBSLPM_OK;
 }
@@ -438,6 +357,10 @@ void fill_geom(sbslpm_ctx* c) {
   }
 }
 
+}  // namespace
+
+namespace sbslpm {
+
 // One velocity evaluation (one RK4 stage) into v (contiguous [3][leaves*q]).
 void velocity_eval(sbslpm_ctx* c, int stage, double dt_s, const double* vprev, const double* x, const double* y,
                    const double* z, const double* area, const double* vors, double* v) {
@@ -506,6 +429,43 @@ sbslpm_status finish(sbslpm_ctx* c) {
   return SBSLPM_OK;
 }
 
+// Captures body() once on the context's own stream (the legacy default stream
+// cannot be captured), after the current stream's earlier work, into *graph.
+// Kernels enqueued by body() are not counted as launched; the count per
+// replay is returned through c->launches_per_step.
+sbslpm_status capture_graph(sbslpm_ctx* c, cudaGraphExec_t* graph, const std::function<void()>& body) {
+  if (*graph) {
+    cudaGraphExecDestroy(*graph);
+    *graph = nullptr;
+  }
+  cudaStream_t st = c->stream(), cap = c->own_stream;
+  if (st != cap) {
+    cudaEvent_t ev;
+    SB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    SB_CUDA(cudaEventRecord(ev, st));
+    SB_CUDA(cudaStreamWaitEvent(cap, ev, 0));
+    cudaEventDestroy(ev);
+  }
+  const bool saved_set = c->user_stream_set;
+  c->user_stream_set = false;  // enqueue on the capturing stream
+  const long before = launch_counter();
+  cudaGraph_t g;
+  SB_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+  body();
+  cudaError_t ce = cudaStreamEndCapture(cap, &g);
+  c->user_stream_set = saved_set;
+  c->launches_per_step = launch_counter() - before;
+  launch_counter() = before;
+  SB_CUDA(ce);
+  SB_CUDA(cudaGraphInstantiate(graph, g, 0));
+  cudaGraphDestroy(g);
+  return SBSLPM_OK;
+}
+
+}  // namespace sbslpm
+
+namespace {
+
 bool bad(const void* p) { return p == nullptr; }
 
 }  // namespace
@@ -527,6 +487,7 @@ sbslpm_status sbslpm_config_default(sbslpm_config* cfg) {
   cfg->velocity = SBSLPM_VEL_FMM;
   cfg->precision = SBSLPM_FP64;
   cfg->exact_cc = 0;
+  cfg->g_over_a = 9.81 / 6371000.0;  // src/swe_time_step_2_impl.hpp:103
   return SBSLPM_OK;
 }
 
@@ -651,10 +612,13 @@ sbslpm_status sbslpm_create(const sbslpm_config* cfg, sbslpm_ctx** out) {
 sbslpm_status sbslpm_destroy(sbslpm_ctx* c) {
   if (!c) return SBSLPM_OK;
   if (c->graph) cudaGraphExecDestroy(c->graph);
+  if (c->swe_graph) cudaGraphExecDestroy(c->swe_graph);
   void* bufs[] = {c->px, c->il_basis, c->child_mat, c->centre, c->tgt_start, c->src_panel, c->il_row, c->src,
                   c->srcf, c->tgt, c->vbuf, c->partial, c->newvor, c->newtr, c->dep, c->err, c->fpx, c->fchild,
                   c->fcentre, c->flx, c->fly, c->fbounds, c->fface, c->near_start, c->near_src, c->cc_start,
-                  c->cc_src, c->fsrc, c->psrc, c->fsrcf, c->psrcf, c->ftgt, c->gx, c->near};
+                  c->cc_src, c->fsrc, c->psrc, c->fsrcf, c->psrcf, c->ftgt, c->gx, c->near, c->s_fd,
+                  c->s_ntan, c->s_pow15, c->s_filt, c->s_ptan, c->s_pface, c->s_ustart, c->s_umem, c->src2,
+                  c->srcf2, c->tend, c->avor};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (c->h_err) cudaFreeHost(c->h_err);
@@ -711,32 +675,7 @@ sbslpm_status sbslpm_bve_run(sbslpm_ctx* c, const double* x, const double* y, co
   GraphKey key{{x, y, z, area, vors, vel_x, vel_y, vel_z, tracers}};
   cudaStream_t st = c->stream();
   if (!c->graph || !(key == c->graph_key)) {
-    if (c->graph) {
-      cudaGraphExecDestroy(c->graph);
-      c->graph = nullptr;
-    }
-    // capture on the context's own stream (the legacy default stream cannot be captured)
-    cudaStream_t cap = c->own_stream;
-    if (st != cap) {
-      cudaEvent_t ev;
-      SB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-      SB_CUDA(cudaEventRecord(ev, st));
-      SB_CUDA(cudaStreamWaitEvent(cap, ev, 0));
-      cudaEventDestroy(ev);
-    }
-    const bool saved_set = c->user_stream_set;
-    c->user_stream_set = false;  // enqueue on the capturing stream
-    long before = launch_counter();
-    cudaGraph_t graph;
-    SB_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
-    enqueue_step(c, x, y, z, area, vors, vel_x, vel_y, vel_z, tracers);
-    cudaError_t ce = cudaStreamEndCapture(cap, &graph);
-    c->user_stream_set = saved_set;
-    c->launches_per_step = launch_counter() - before;
-    launch_counter() = before;
-    SB_CUDA(ce);
-    SB_CUDA(cudaGraphInstantiate(&c->graph, graph, 0));
-    cudaGraphDestroy(graph);
+    SB_TRY(capture_graph(c, &c->graph, [&] { enqueue_step(c, x, y, z, area, vors, vel_x, vel_y, vel_z, tracers); }));
     c->graph_key = key;
   }
   for (int s = 0; s < nsteps; s++) {
@@ -757,6 +696,7 @@ sbslpm_status sbslpm_upward_pass(sbslpm_ctx* c, const double* area, const double
   return finish(c);
 }
 
+extern "C++" {
 namespace sbslpm {
 // t_c[i] += tgt[c][i] for the three components (accumulating API of bve_vel_interactions).
 __global__ void k_add3(const double* __restrict__ t, long n, double* a, double* b, double* cc) {
@@ -766,7 +706,12 @@ __global__ void k_add3(const double* __restrict__ t, long n, double* a, double* 
   b[i] += t[n + i];
   cc[i] += t[2 * n + i];
 }
+void launch_add3(const double* t, long n, double* a, double* b, double* cc, cudaStream_t st) {
+  k_add3<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(t, n, a, b, cc);
+  launch_counter()++;
+}
 }  // namespace sbslpm
+}  // extern "C++"
 
 sbslpm_status sbslpm_bve_vel_interactions(sbslpm_ctx* c, const double* dx, const double* dy, const double* dz,
                                           const double* source, double* t1, double* t2, double* t3) {
@@ -776,9 +721,7 @@ sbslpm_status sbslpm_bve_vel_interactions(sbslpm_ctx* c, const double* dx, const
   cudaStream_t st = c->stream();
   launch_sources_from_disp(c->geom, dx, dy, dz, source, c->src, st);
   launch_interactions(c->geom, c->cfg.precision, c->src, c->tgt, false, st);
-  long n = (long)c->P * c->q;
-  k_add3<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(c->tgt, n, t1, t2, t3);
-  launch_counter()++;
+  launch_add3(c->tgt, (long)c->P * c->q, t1, t2, t3, st);
   return finish(c);
 }
 

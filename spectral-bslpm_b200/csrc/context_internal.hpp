@@ -1,0 +1,120 @@
+// Internal: the context object shared by the step orchestration files
+// (context.cu: set-up, BVE step, C ABI; swe_context.cu: the shallow-water
+// step) and their small host helpers.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <functional>
+#include <string>
+#include <vector>
+
+#include "bve_kernels.cuh"
+#include "internal.hpp"
+#include "swe_kernels.cuh"
+
+#define SB_CUDA(call)                                                                      \
+  do {                                                                                     \
+    cudaError_t e_ = (call);                                                               \
+    if (e_ != cudaSuccess) {                                                               \
+      set_last_error(std::string(#call) + ": " + cudaGetErrorString(e_));                 \
+      return SBSLPM_ERR_CUDA;                                                              \
+    }                                                                                      \
+  } while (0)
+
+struct GraphKey {
+  const void* p[16];
+  bool operator==(const GraphKey& o) const { return std::memcmp(p, o.p, sizeof p) == 0; }
+};
+
+struct sbslpm_ctx {
+  sbslpm_config cfg{};
+  int L = 0, d = 0, q = 0, P = 0, A = 0, off = 0;
+  long I = 0;
+  std::vector<sbslpm_panel> panels;
+  std::vector<sbslpm_interact_pair> list;
+  cudaStream_t user_stream = nullptr, own_stream = nullptr;
+  bool user_stream_set = false;  // set_stream(NULL) selects the legacy default stream
+  // static device data
+  double *px = nullptr, *il_basis = nullptr, *child_mat = nullptr, *centre = nullptr;
+  int *tgt_start = nullptr, *src_panel = nullptr, *il_row = nullptr;
+  // workspace
+  double4* src = nullptr;
+  float4* srcf = nullptr;
+  double *tgt = nullptr, *vbuf = nullptr, *partial = nullptr, *newvor = nullptr, *newtr = nullptr, *dep = nullptr;
+  int groups = 1;
+  unsigned* err = nullptr;
+  unsigned* h_err = nullptr;
+  sbslpm::BliTable tab{};
+  sbslpm::StepGeom geom{};
+  cudaGraphExec_t graph = nullptr;
+  GraphKey graph_key{};
+  long launches_per_step = 0;
+
+  // treecode with decoupled proxy degree (proxy_degree > 0)
+  bool tree = false;
+  int Lf = 0, n = 0, qx = 0, Pf = 0, Af = 0, npl = 0;
+  long n_near = 0, n_cc = 0;
+  std::vector<sbslpm_panel> fpanels;
+  double *fpx = nullptr, *fchild = nullptr, *fcentre = nullptr, *flx = nullptr, *fly = nullptr, *fbounds = nullptr;
+  int *fface = nullptr, *near_start = nullptr, *near_src = nullptr, *cc_start = nullptr, *cc_src = nullptr;
+  double4 *fsrc = nullptr, *psrc = nullptr;
+  double* gx = nullptr;  // [3][particles]: the particle grid, for timing the near kernel alone
+  double* near = nullptr;  // [near_splits][3][particles] near-field partial sums
+  int near_splits = 2;
+  float4 *fsrcf = nullptr, *psrcf = nullptr;
+  double* ftgt = nullptr;
+  sbslpm::BliTable ftab{};
+  sbslpm::StepGeom fgeom{};
+  sbslpm::TreeGeom tgeom{};
+
+  // shallow water (SWE v2): static tables and workspace, set up on first use
+  bool swe_ready = false;
+  double *s_fd = nullptr, *s_ntan = nullptr, *s_pow15 = nullptr, *s_filt = nullptr, *s_ptan = nullptr;
+  int *s_pface = nullptr, *s_ustart = nullptr, *s_umem = nullptr;
+  std::vector<int> two_d_to_1d, unique_counts;
+  double4* src2 = nullptr;
+  float4* srcf2 = nullptr;
+  double* tend = nullptr;  // [3 stages][3 fields][leaves*q]: vorticity, divergence, height tendencies
+  double* avor = nullptr;  // arrival vorticity
+  sbslpm::SweGeom sgeom{};
+  cudaGraphExec_t swe_graph = nullptr;
+  GraphKey swe_graph_key{};
+  long swe_launches_per_step = 0;
+
+  cudaStream_t stream() const { return user_stream_set ? user_stream : own_stream; }
+};
+
+namespace sbslpm {
+
+template <class T>
+sbslpm_status dalloc(T** p, size_t count) {
+  *p = nullptr;
+  if (count == 0) return SBSLPM_OK;
+  SB_CUDA(cudaMalloc(reinterpret_cast<void**>(p), sizeof(T) * count));
+  return SBSLPM_OK;
+}
+
+template <class T>
+sbslpm_status upload(T** p, const std::vector<T>& h) {
+  sbslpm_status s = dalloc(p, h.size());
+  if (s != SBSLPM_OK) return s;
+  if (!h.empty()) SB_CUDA(cudaMemcpy(*p, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
+  return SBSLPM_OK;
+}
+
+#define SB_TRY(expr)                           \
+  do {                                         \
+    sbslpm_status s_ = (expr);                 \
+    if (s_ != SBSLPM_OK) return s_;            \
+  } while (0)
+
+
+sbslpm_status finish(sbslpm_ctx* c);
+void velocity_eval(sbslpm_ctx* c, int stage, double dt_s, const double* vprev, const double* x, const double* y,
+                   const double* z, const double* area, const double* vors, double* v);
+void launch_add3(const double* t, long n, double* a, double* b, double* cc, cudaStream_t st);
+sbslpm_status capture_graph(sbslpm_ctx* c, cudaGraphExec_t* graph, const std::function<void()>& body);
+
+}  // namespace sbslpm

@@ -1,0 +1,126 @@
+// Device helpers shared by the kernel files: the reciprocal used by every
+// pair kernel, the Biot-Savart pair in float64 / float32 / paired float32,
+// the device error word, and the launch macro that counts launches.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "bve_kernels.cuh"
+
+namespace sbslpm {
+namespace dev {
+
+__device__ __forceinline__ void flag(unsigned* err, unsigned bits) {
+  if (bits) atomicOr(err, bits);
+}
+
+// 1/d from the hardware approximation refined by two Newton-Raphson steps
+// r <- r + r (1 - d r); each step squares the relative error.  d > 0.
+__device__ __forceinline__ double recip_nr(double d) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(d));
+  double e = fma(-d, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-d, r, 1.0);
+  return fma(r, e, r);
+}
+
+__device__ __forceinline__ float recip_f32(float d) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(d));
+  return r;
+}
+
+// One Biot-Savart pair in float64.  With d = y - x and |x| = |y| = 1,
+// 1 - x.y = |d|^2 / 2, and x cross y = x cross d, so the accumulated
+// a = sum g d gives u = -1/(4 pi) x cross a.  Coincident points add nothing:
+// with eps > 0 because d = 0; with eps = 0 (GUARD) because g is zeroed.
+template <bool GUARD>
+__device__ __forceinline__ void pair64(double tx, double ty, double tz, const double4 s, double eps, double& ax,
+                                       double& ay, double& az) {
+  double dx = s.x - tx, dy = s.y - ty, dz = s.z - tz;
+  double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+  double g = s.w * recip_nr(fma(0.5, r2, eps));
+  if (GUARD) g = r2 > 0.0 ? g : 0.0;
+  ax = fma(g, dx, ax);
+  ay = fma(g, dy, ay);
+  az = fma(g, dz, az);
+}
+
+// The same pair in float32 on panel-relative coordinates scaled by 1/sqrt(2)
+// (kPackScale): d' = base + s.xyz with base = (c_S - c_T)/sqrt(2) - delta_t,
+// and |d'|^2 + eps = |d|^2/2 + eps in one FMA chain.
+template <bool GUARD>
+__device__ __forceinline__ void pair32(float bx, float by, float bz, const float4 s, float eps, float& ax, float& ay,
+                                       float& az) {
+  float dx = bx + s.x, dy = by + s.y, dz = bz + s.z;
+  float den = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps)));
+  float g = s.w * recip_f32(den);
+  if (GUARD) g = den > 0.0f ? g : 0.0f;
+  ax = fmaf(g, dx, ax);
+  ay = fmaf(g, dy, ay);
+  az = fmaf(g, dz, az);
+}
+
+// Two pairs at once with the paired FP32 instructions of sm_100 (FADD2 /
+// FFMA2 / FMUL2): one target (b broadcast in both halves) against two
+// sources given as register pairs (x0,x1), (y0,y1), (z0,z1), (w0,w1).
+template <bool GUARD>
+__device__ __forceinline__ void pair32x2(const float2 bx, const float2 by, const float2 bz, const float2 sx,
+                                         const float2 sy, const float2 sz, const float2 sw, const float2 eps2,
+                                         float2& ax, float2& ay, float2& az) {
+  const float2 dx = __fadd2_rn(bx, sx), dy = __fadd2_rn(by, sy), dz = __fadd2_rn(bz, sz);
+  const float2 den = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, eps2)));
+  float2 g = __fmul2_rn(sw, make_float2(recip_f32(den.x), recip_f32(den.y)));
+  if (GUARD) {
+    g.x = den.x > 0.0f ? g.x : 0.0f;
+    g.y = den.y > 0.0f ? g.y : 0.0f;
+  }
+  ax = __ffma2_rn(g, dx, ax);
+  ay = __ffma2_rn(g, dy, ay);
+  az = __ffma2_rn(g, dz, az);
+}
+
+// First panel id of the k-th level below the subtree root (level, root_rel).
+__device__ __forceinline__ int subtree_first(int level, int root_rel, int k) {
+  return level_start(level + k) + (root_rel << (2 * k));
+}
+
+__device__ __forceinline__ void nonleaf_position(const StepGeom& g, long i, int stage, double dt_s,
+                                                 const double* __restrict__ vprev, double& px, double& py,
+                                                 double& pz) {
+  const long pn = (long)g.panels * g.q, ln = (long)g.leaves * g.q;
+  px = g.px[i];
+  py = g.px[pn + i];
+  pz = g.px[2 * pn + i];
+  if (stage > 0) {
+    const double* b = g.il_basis + i * g.q;
+    const long row = (long)g.il_row[i] * g.q;
+    double ax = 0, ay = 0, az = 0;
+    for (int m = 0; m < g.q; m++) {
+      double bm = b[m];
+      ax += (dt_s * vprev[row + m]) * bm;
+      ay += (dt_s * vprev[ln + row + m]) * bm;
+      az += (dt_s * vprev[2 * ln + row + m]) * bm;
+    }
+    px += ax;
+    py += ay;
+    pz += az;
+  }
+  project_to_sphere(px, py, pz);
+}
+
+
+inline unsigned blocks_for(long n, int t) { return (unsigned)((n + t - 1) / t); }
+
+}  // namespace dev
+
+long& launch_counter();
+
+}  // namespace sbslpm
+
+#define SB_LAUNCH(kernel, grid, block, shmem, st, ...)      \
+  do {                                                     \
+    kernel<<<grid, block, shmem, st>>>(__VA_ARGS__);       \
+    ::sbslpm::launch_counter()++;                          \
+  } while (0)

@@ -25,6 +25,14 @@ void host_bli(double* basis, double xi, double eta, double min_xi, double max_xi
               int degree, unsigned& err);
 bool read_namelist(const char* path, sbslpm_config* cfg, std::string& msg);
 
+// swe_setup.cpp
+long unique_points(long n_leaves, int q, const double* x, const double* y, const double* z, int* two_d_to_1d,
+                   std::vector<int>& counts);
+void build_swe_tables(int degree, const std::vector<sbslpm_panel>& panels, int offset, long n_leaves,
+                      const double* x, const double* y, const double* z, std::vector<double>& fd,
+                      std::vector<double>& ntan, std::vector<double>& pow15, std::vector<double>& filt,
+                      std::vector<double>& ptan, std::vector<int>& pface);
+
 void set_last_error(const std::string& msg);
 
 }  // namespace sbslpm

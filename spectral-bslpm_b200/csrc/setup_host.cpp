@@ -291,6 +291,7 @@ bool read_namelist(const char* path, sbslpm_config* cfg, std::string& msg) {
       else if (key == "exact_cc") cfg->exact_cc = std::stoi(val) != 0;
       else if (key == "proxy_degree") cfg->proxy_degree = std::stoi(val);
       else if (key == "leaf_size") cfg->leaf_size = std::stoi(val);
+      else if (key == "g_over_a") cfg->g_over_a = std::stod(val);
       else if (key == "out_path" || key == "write_precision" || key == "write_output" || key == "grid_spacing" ||
                key == "end_time" || key == "output_vel" || key == "output_freq" || key == "initial_condition" ||
                key == "balance_ic" || key == "interp_output" || key == "forcing" || key == "forcing_type" ||

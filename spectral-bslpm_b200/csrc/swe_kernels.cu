@@ -1,0 +1,478 @@
+// Shallow-water (SWE v2) velocity kernels, sm_100a: the two-field sources and
+// upward pass, and the proxy interactions of swe_vel_panel_interaction_2
+// (src/fmm_interactions/swe_vel_impl.hpp:80-147):
+//
+//   u(x) += 1/(4 pi) [ -S_vor (x cross y')/(1 - x.y' + eps)
+//                      + S_div (y - x (x.y))/(1 - x.y + eps) ]
+//
+// with y' the displaced, re-projected source proxy and y the fixed one.  Both
+// denominators are computed as |y - x|^2/2 + eps (|x| = |y| = 1), the
+// rotational part as x cross sum g (y' - x), and the divergent part as the
+// tangential projection (I - x x^T) of sum g2 (y - x), which equals
+// sum g2 (y - x (x.y)) for |x| = 1.  Sources (double4, 32 B per proxy):
+//   src  = (y'_x, y'_y, y'_z, S_vor),   src2 = (y_x, y_y, y_z, S_div).
+// Every kernel is owner-computes (no atomics) and deterministic.
+#include <cuda_runtime.h>
+
+#include <type_traits>
+
+#include "../../include/sbslpm.h"
+#include "device_common.cuh"
+#include "swe_kernels.cuh"
+
+namespace sbslpm {
+namespace {
+
+using namespace dev;
+
+constexpr int kWarps = 4;
+
+// ---------------------------------------------------------------------------
+// Sources.
+
+// Strengths of leaf point i (relative index) at a stage: swe_apply_tendencies_2
+// (src/swe_time_step_2.cpp:390-414) folded into base_pots
+// (src/fmm_funcs_impl.hpp:17-34): w_vor = area (1 + dts div) (vor + dts tv),
+// w_div = area (div + dts td).
+__device__ __forceinline__ void leaf_strengths(long i, long ln, int stage, double dts, const double* tprev,
+                                               const double* vors, const double* divs, const double* area,
+                                               double& wv, double& wd) {
+  const double a = area[i], vor = vors[i], div = divs[i];
+  if (stage == 0) {
+    wv = a * vor;
+    wd = a * div;
+  } else {
+    const double dvor = vor + dts * tprev[i];
+    const double ddiv = div + dts * tprev[ln + i];
+    wv = (a * (1.0 + dts * div)) * dvor;
+    wd = a * ddiv;
+  }
+}
+
+__device__ __forceinline__ float4 pack(const double* c, double x, double y, double z, double w) {
+  return make_float4((float)((x - c[0]) * kPackScale), (float)((y - c[1]) * kPackScale),
+                     (float)((z - c[2]) * kPackScale), (float)w);
+}
+
+// Fused upward pass over one subtree (the SWE form of k_upward_subtree): leaf
+// sources of both fields when the subtree reaches the leaves, displaced
+// positions of its non-leaf proxies (swe_disp_interp_2,
+// src/swe_time_step_2.cpp:436-476, identical to the BVE form), both strengths
+// anterpolated level by level (upward_pass, src/fmm_funcs.cpp:341-355), and
+// the packed float sources in mixed precision.
+__global__ void k_swe_upward_subtree(StepGeom g, SweGeom sw, int r, int D, int stage, double dtd, double dts,
+                                     const double* __restrict__ vprev, const double* __restrict__ tprev,
+                                     const double* __restrict__ vors, const double* __restrict__ divs,
+                                     const double* __restrict__ area, double4* __restrict__ src,
+                                     double4* __restrict__ src2, int mixed) {
+  extern __shared__ double sh[];  // 2 fields x levels r..r+D, then 2 x 4^D q scratch
+  const int q = g.q, root_rel = blockIdx.x, n1 = g.degree + 1;
+  const bool leaves_here = (r + D == g.levels - 1);
+  const long ln = (long)g.leaves * g.q, pn = (long)g.panels * g.q;
+  const int per_field = q * (((1 << (2 * (D + 1))) - 1) / 3);
+  auto lvl = [&](int f, int k) { return sh + f * per_field + q * (((1 << (2 * k)) - 1) / 3); };
+  double* scratch = sh + 2 * per_field;
+  const int sstride = (1 << (2 * D)) * q;
+
+  {
+    const int first = subtree_first(r, root_rel, D), npts = (1 << (2 * D)) * q;
+    for (int t = threadIdx.x; t < npts; t += blockDim.x) {
+      const long o = (long)first * q + t;
+      double wv, wd;
+      if (leaves_here) {
+        const long i = o - (long)g.offset * q;
+        leaf_strengths(i, ln, stage, dts, tprev, vors, divs, area, wv, wd);
+        double px = g.px[o], py = g.px[pn + o], pz = g.px[2 * pn + o];
+        src2[o] = make_double4(px, py, pz, wd);
+        if (stage > 0) {
+          px += dtd * vprev[i];
+          py += dtd * vprev[ln + i];
+          pz += dtd * vprev[2 * ln + i];
+        }
+        project_to_sphere(px, py, pz);
+        src[o] = make_double4(px, py, pz, wv);
+      } else {
+        wv = src[o].w;
+        wd = src2[o].w;
+      }
+      lvl(0, D)[t] = wv;
+      lvl(1, D)[t] = wd;
+    }
+  }
+  for (int k = 0; k < D; k++) {
+    const int first = subtree_first(r, root_rel, k), npts = (1 << (2 * k)) * q;
+    for (int t = threadIdx.x; t < npts; t += blockDim.x) {
+      const long i = (long)first * q + t;
+      double px, py, pz;
+      nonleaf_position(g, i, stage, dtd, vprev, px, py, pz);
+      src[i] = make_double4(px, py, pz, 0.0);
+      src2[i] = make_double4(g.px[i], g.px[pn + i], g.px[2 * pn + i], 0.0);
+    }
+  }
+  __syncthreads();
+  for (int k = D - 1; k >= 0; k--) {
+    const int np = 1 << (2 * k), first = subtree_first(r, root_rel, k);
+    for (int t = threadIdx.x; t < 2 * 4 * np * q; t += blockDim.x) {  // T[f][cc][i][b]
+      const int f = t / (4 * np * q), tt = t % (4 * np * q);
+      const int cc = tt / q, rem = tt % q, i = rem / n1, b = rem % n1;
+      const double* ly = g.child_1d + ((cc & 3) >= 2 ? n1 * n1 : 0);
+      const double* sc = lvl(f, k + 1) + cc * q + i * n1;
+      double acc = 0;
+      for (int j = 0; j < n1; j++) acc = fma(__ldg(ly + j * n1 + b), sc[j], acc);
+      scratch[f * sstride + tt] = acc;
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < 2 * np * q; t += blockDim.x) {  // S[f][p][a][b]
+      const int f = t / (np * q), tt = t % (np * q);
+      const int p = tt / q, rem = tt % q, a = rem / n1, b = rem % n1;
+      double acc = 0;
+      for (int c = 0; c < 4; c++) {
+        const double* lx = g.child_1d + ((c == 1 || c == 2) ? n1 * n1 : 0);
+        const double* tc = scratch + f * sstride + (4 * p + c) * q + b;
+        for (int i = 0; i < n1; i++) acc = fma(__ldg(lx + i * n1 + a), tc[i * n1], acc);
+      }
+      lvl(f, k)[tt] = acc;
+      if (f == 0) src[(long)first * q + tt].w = acc;
+      else src2[(long)first * q + tt].w = acc;
+    }
+    __syncthreads();
+  }
+  if (mixed) {
+    const int kmax = leaves_here ? D : D - 1;
+    for (int k = 0; k <= kmax; k++) {
+      const int first = subtree_first(r, root_rel, k), npts = (1 << (2 * k)) * q;
+      for (int t = threadIdx.x; t < npts; t += blockDim.x) {
+        const long i = (long)first * q + t;
+        const double* cc = g.pd_centre + 4 * (i / q);
+        const double4 a = src[i], b = src2[i];
+        g.srcf[i] = pack(cc, a.x, a.y, a.z, a.w);
+        sw.srcf2[i] = pack(cc, b.x, b.y, b.z, b.w);
+      }
+    }
+  }
+}
+
+// Direct velocity: leaf sources of both fields (no tree).
+__global__ void k_swe_leaf_sources(StepGeom g, SweGeom sw, int stage, double dtd, double dts,
+                                   const double* __restrict__ vprev, const double* __restrict__ tprev,
+                                   const double* __restrict__ vors, const double* __restrict__ divs,
+                                   const double* __restrict__ area, double4* __restrict__ src,
+                                   double4* __restrict__ src2, int mixed) {
+  const long ln = (long)g.leaves * g.q, pn = (long)g.panels * g.q;
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= ln) return;
+  const long o = (long)g.offset * g.q + i;
+  double wv, wd;
+  leaf_strengths(i, ln, stage, dts, tprev, vors, divs, area, wv, wd);
+  double px = g.px[o], py = g.px[pn + o], pz = g.px[2 * pn + o];
+  src2[o] = make_double4(px, py, pz, wd);
+  if (mixed) sw.srcf2[o] = pack(g.pd_centre + 4 * (o / g.q), px, py, pz, wd);
+  if (stage > 0) {
+    px += dtd * vprev[i];
+    py += dtd * vprev[ln + i];
+    pz += dtd * vprev[2 * ln + i];
+  }
+  project_to_sphere(px, py, pz);
+  src[o] = make_double4(px, py, pz, wv);
+  if (mixed) g.srcf[o] = pack(g.pd_centre + 4 * (o / g.q), px, py, pz, wv);
+}
+
+// Piecewise API: sources from explicit displacements (swe_vel_panel_interaction_2
+// displaces every proxy, src/fmm_interactions/swe_vel_impl.hpp:124-128) and strengths.
+__global__ void k_swe_sources_from_disp(StepGeom g, SweGeom sw, const double* __restrict__ dx,
+                                        const double* __restrict__ dy, const double* __restrict__ dz,
+                                        const double* __restrict__ sv, const double* __restrict__ sd,
+                                        double4* __restrict__ src, double4* __restrict__ src2, int mixed) {
+  const long pn = (long)g.panels * g.q;
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= pn) return;
+  const double x0 = g.px[i], y0 = g.px[pn + i], z0 = g.px[2 * pn + i];
+  double px = x0 + dx[i], py = y0 + dy[i], pz = z0 + dz[i];
+  project_to_sphere(px, py, pz);
+  src[i] = make_double4(px, py, pz, sv[i]);
+  src2[i] = make_double4(x0, y0, z0, sd[i]);
+  if (mixed) {
+    const double* c = g.pd_centre + 4 * (i / g.q);
+    g.srcf[i] = pack(c, px, py, pz, sv[i]);
+    sw.srcf2[i] = pack(c, x0, y0, z0, sd[i]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Interactions.  One warp per target panel; for q <= 16 the warp's lanes are
+// (32/q source splits) x (q target nodes), for larger q each lane owns
+// ceil(q/32) target nodes.  A source panel's q proxies of both fields are
+// staged in shared memory and every lane sweeps them.  ALL_LEAVES: every
+// leaf against every leaf, source leaves split into gridDim.y groups whose
+// partials are reduced in order afterwards.
+
+template <int Q>
+struct Shape {
+  static constexpr int S = Q <= 16 ? 32 / Q : 1;
+  static constexpr int TPL = Q <= 32 ? 1 : (Q + 31) / 32;
+  static constexpr int STAGE = S * Q > Q ? S * Q : Q;
+};
+
+// u = K x cross A - K (B - x (x.B)); K = -1/(4 pi), or scaled by sqrt(2)
+// for the packed float sums.
+__device__ __forceinline__ void swe_epilogue(double K, double tx, double ty, double tz, double ax, double ay,
+                                             double az, double bx, double by, double bz, double& ux, double& uy,
+                                             double& uz) {
+  const double tb = tx * bx + ty * by + tz * bz;
+  ux = K * (ty * az - tz * ay) - K * (bx - tx * tb);
+  uy = K * (tz * ax - tx * az) - K * (by - ty * tb);
+  uz = K * (tx * ay - ty * ax) - K * (bz - tz * tb);
+}
+
+template <int Q, bool ALL_LEAVES, bool GUARD, bool MIXED>
+__global__ void __launch_bounds__(32 * kWarps)
+    k_swe_interact(StepGeom g, SweGeom sw, const double4* __restrict__ src, const double4* __restrict__ src2,
+                   double* __restrict__ out, long out_stride) {
+  using W = Shape<Q>;
+  using Src = typename std::conditional<MIXED, float4, double4>::type;
+  __shared__ Src stage[kWarps][2][W::STAGE];
+  __shared__ double red[kWarps][6][32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int tp_first = ALL_LEAVES ? g.offset : 0;
+  const int tp_count = ALL_LEAVES ? g.leaves : g.panels;
+  const int tix = blockIdx.x * kWarps + warp;
+  if (tix >= tp_count) return;
+  const int t = tp_first + tix;
+  const long pn = (long)g.panels * g.q;
+  int e0, e1;
+  if (ALL_LEAVES) {
+    const int per = (g.leaves + gridDim.y - 1) / gridDim.y;
+    e0 = blockIdx.y * per;
+    e1 = min(g.leaves, e0 + per);
+  } else {
+    e0 = g.tgt_start[t];
+    e1 = g.tgt_start[t + 1];
+  }
+  auto source_of = [&](int e) { return ALL_LEAVES ? g.offset + e : __ldg(g.src_panel + e); };
+  const Src* s1 = nullptr;
+  const Src* s2 = nullptr;
+  if constexpr (MIXED) {
+    s1 = g.srcf;
+    s2 = sw.srcf2;
+  } else {
+    s1 = src;
+    s2 = src2;
+  }
+  const double* ct = g.pd_centre + 4 * (long)t;
+  const float eps32 = (float)g.eps;
+  constexpr double K = MIXED ? kBiotSavartPacked : kBiotSavart;
+  constexpr int TPL = W::TPL;
+  const int h = Q <= 32 ? lane / Q : 0;
+  const bool active = Q <= 32 ? h < W::S : true;
+
+  double tx[TPL], ty[TPL], tz[TPL], ax[TPL], ay[TPL], az[TPL], bx[TPL], by[TPL], bz[TPL];
+  float dtx[TPL], dty[TPL], dtz[TPL];
+#pragma unroll
+  for (int r = 0; r < TPL; r++) {
+    const int j = Q <= 32 ? lane % Q : lane + 32 * r;
+    const long o = (long)t * Q + (j < Q ? j : 0);
+    tx[r] = g.px[o];
+    ty[r] = g.px[pn + o];
+    tz[r] = g.px[2 * pn + o];
+    if (MIXED) {
+      dtx[r] = (float)((tx[r] - ct[0]) * kPackScale);
+      dty[r] = (float)((ty[r] - ct[1]) * kPackScale);
+      dtz[r] = (float)((tz[r] - ct[2]) * kPackScale);
+    }
+    ax[r] = ay[r] = az[r] = bx[r] = by[r] = bz[r] = 0;
+  }
+  constexpr int STEP = Q <= 32 ? W::S : 1;
+  for (int e = e0; e < e1; e += STEP) {
+    int sp = 0;
+    if (Q <= 32) {
+      if (active && e + h < e1) {
+        sp = source_of(e + h);
+        const int j = lane % Q;
+        stage[warp][0][h * Q + j] = s1[(long)sp * Q + j];
+        stage[warp][1][h * Q + j] = s2[(long)sp * Q + j];
+      }
+    } else {
+      sp = source_of(e);
+      for (int k = lane; k < Q; k += 32) {
+        stage[warp][0][k] = s1[(long)sp * Q + k];
+        stage[warp][1][k] = s2[(long)sp * Q + k];
+      }
+    }
+    __syncwarp();
+    if (active && e + h < e1) {
+      const Src* st1 = &stage[warp][0][h * Q];
+      const Src* st2 = &stage[warp][1][h * Q];
+      if constexpr (MIXED) {
+        const double* cs = g.pd_centre + 4 * (long)sp;
+        const float c0 = (float)((cs[0] - ct[0]) * kPackScale), c1 = (float)((cs[1] - ct[1]) * kPackScale),
+                    c2 = (float)((cs[2] - ct[2]) * kPackScale);
+        float fa[TPL][3], fb[TPL][3], b0[TPL], b1[TPL], b2[TPL];
+#pragma unroll
+        for (int r = 0; r < TPL; r++) {
+          b0[r] = c0 - dtx[r];
+          b1[r] = c1 - dty[r];
+          b2[r] = c2 - dtz[r];
+          fa[r][0] = fa[r][1] = fa[r][2] = fb[r][0] = fb[r][1] = fb[r][2] = 0.f;
+        }
+#pragma unroll 4
+        for (int k = 0; k < Q; k++) {
+          const float4 v1 = st1[k], v2 = st2[k];
+#pragma unroll
+          for (int r = 0; r < TPL; r++) {
+            pair32<GUARD>(b0[r], b1[r], b2[r], v1, eps32, fa[r][0], fa[r][1], fa[r][2]);
+            pair32<GUARD>(b0[r], b1[r], b2[r], v2, eps32, fb[r][0], fb[r][1], fb[r][2]);
+          }
+        }
+#pragma unroll
+        for (int r = 0; r < TPL; r++) {
+          ax[r] += fa[r][0];
+          ay[r] += fa[r][1];
+          az[r] += fa[r][2];
+          bx[r] += fb[r][0];
+          by[r] += fb[r][1];
+          bz[r] += fb[r][2];
+        }
+      } else {
+#pragma unroll 4
+        for (int k = 0; k < Q; k++) {
+          const double4 v1 = st1[k], v2 = st2[k];
+#pragma unroll
+          for (int r = 0; r < TPL; r++) {
+            pair64<GUARD>(tx[r], ty[r], tz[r], v1, g.eps, ax[r], ay[r], az[r]);
+            pair64<GUARD>(tx[r], ty[r], tz[r], v2, g.eps, bx[r], by[r], bz[r]);
+          }
+        }
+      }
+    }
+    __syncwarp();
+  }
+  if (Q <= 32 && W::S > 1) {
+    red[warp][0][lane] = ax[0];
+    red[warp][1][lane] = ay[0];
+    red[warp][2][lane] = az[0];
+    red[warp][3][lane] = bx[0];
+    red[warp][4][lane] = by[0];
+    red[warp][5][lane] = bz[0];
+    __syncwarp();
+    if (h == 0)
+      for (int hh = 1; hh < W::S; hh++) {
+        const int l = hh * Q + lane % Q;
+        ax[0] += red[warp][0][l];
+        ay[0] += red[warp][1][l];
+        az[0] += red[warp][2][l];
+        bx[0] += red[warp][3][l];
+        by[0] += red[warp][4][l];
+        bz[0] += red[warp][5][l];
+      }
+  }
+  if (h != 0) return;
+#pragma unroll
+  for (int r = 0; r < TPL; r++) {
+    const int j = Q <= 32 ? lane % Q : lane + 32 * r;
+    if (j >= Q) continue;
+    double ux, uy, uz;
+    swe_epilogue(K, tx[r], ty[r], tz[r], ax[r], ay[r], az[r], bx[r], by[r], bz[r], ux, uy, uz);
+    const long o = ALL_LEAVES ? (long)blockIdx.y * 3 * out_stride + (long)tix * Q + j : (long)t * Q + j;
+    const long s = ALL_LEAVES ? out_stride : pn;
+    out[o] = ux;
+    out[s + o] = uy;
+    out[2 * s + o] = uz;
+  }
+}
+
+__global__ void k_swe_reduce(const double* __restrict__ partial, int groups, long n, long gstride,
+                             double* __restrict__ out) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double s = 0;
+  for (int k = 0; k < groups; k++) s += partial[k * gstride + i];
+  out[i] = s;
+}
+
+template <int Q, bool GUARD>
+void swe_interact_qg(const StepGeom& g, const SweGeom& s, int precision, const double4* src, const double4* src2,
+                     double* out, bool all_leaves, int groups, long out_stride, cudaStream_t st) {
+  const int tp = all_leaves ? g.leaves : g.panels;
+  dim3 grid(blocks_for(tp, kWarps), all_leaves ? groups : 1);
+  const bool mixed = precision == SBSLPM_MIXED;
+#define SB_SWE_K(AL, MX) \
+  SB_LAUNCH((k_swe_interact<Q, AL, GUARD, MX>), grid, 32 * kWarps, 0, st, g, s, src, src2, out, out_stride)
+  if (all_leaves) {
+    if (mixed) SB_SWE_K(true, true);
+    else SB_SWE_K(true, false);
+  } else {
+    if (mixed) SB_SWE_K(false, true);
+    else SB_SWE_K(false, false);
+  }
+#undef SB_SWE_K
+}
+
+void swe_interact_dispatch(const StepGeom& g, const SweGeom& s, int precision, const double4* src,
+                           const double4* src2, double* out, bool all_leaves, int groups, long out_stride,
+                           cudaStream_t st) {
+#define SB_SQ(Q)                                                                                   \
+  case Q:                                                                                          \
+    if (g.eps > 0) swe_interact_qg<Q, false>(g, s, precision, src, src2, out, all_leaves, groups, out_stride, st); \
+    else swe_interact_qg<Q, true>(g, s, precision, src, src2, out, all_leaves, groups, out_stride, st);            \
+    break;
+  switch (g.q) {
+    SB_SQ(1) SB_SQ(4) SB_SQ(9) SB_SQ(16) SB_SQ(25) SB_SQ(36) SB_SQ(49) SB_SQ(64) SB_SQ(81) SB_SQ(100) SB_SQ(121)
+  }
+#undef SB_SQ
+}
+
+size_t swe_subtree_smem(int q, int D) {
+  return (size_t)q * 2 * 8 * ((((1L << (2 * (D + 1))) - 1) / 3) + (1L << (2 * D)));
+}
+
+}  // namespace
+
+void launch_swe_upward(const StepGeom& g, const SweGeom& s, int stage, double dtd, double dts, const double* vprev,
+                       const double* tprev, const double*, const double*, const double*, const double* vors,
+                       const double* divs, const double* area, double4* src, double4* src2, bool mixed,
+                       cudaStream_t st) {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_swe_upward_subtree, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr = true;
+  }
+  const int Dmax = g.q <= 25 ? 3 : 1;
+  int r = g.levels - 1;
+  do {
+    const int D = r < Dmax ? r : Dmax;
+    const int root = r - D;
+    SB_LAUNCH(k_swe_upward_subtree, (unsigned)(6 << (2 * root)), 256, swe_subtree_smem(g.q, D), st, g, s, root, D,
+              stage, dtd, dts, vprev, tprev, vors, divs, area, src, src2, mixed ? 1 : 0);
+    r = root;
+  } while (r > 0);
+}
+
+void launch_swe_leaf_sources(const StepGeom& g, const SweGeom& s, int stage, double dtd, double dts,
+                             const double* vprev, const double* tprev, const double* vors, const double* divs,
+                             const double* area, double4* src, double4* src2, bool mixed, cudaStream_t st) {
+  const long ln = (long)g.leaves * g.q;
+  SB_LAUNCH(k_swe_leaf_sources, blocks_for(ln, 256), 256, 0, st, g, s, stage, dtd, dts, vprev, tprev, vors, divs,
+            area, src, src2, mixed ? 1 : 0);
+}
+
+void launch_swe_interactions(const StepGeom& g, const SweGeom& s, int precision, const double4* src,
+                             const double4* src2, double* tgt, cudaStream_t st) {
+  swe_interact_dispatch(g, s, precision, src, src2, tgt, false, 1, 0, st);
+}
+
+void launch_swe_direct(const StepGeom& g, const SweGeom& s, int precision, const double4* src, const double4* src2,
+                       double* vout, double* partial, int groups, cudaStream_t st) {
+  const long n = (long)g.leaves * g.q;
+  swe_interact_dispatch(g, s, precision, src, src2, partial, true, groups, n, st);
+  SB_LAUNCH(k_swe_reduce, blocks_for(3 * n, 256), 256, 0, st, partial, groups, 3 * n, 3 * n, vout);
+}
+
+void launch_swe_sources_from_disp(const StepGeom& g, const SweGeom& s, const double* dx, const double* dy,
+                                  const double* dz, const double* s_vor, const double* s_div, double4* src,
+                                  double4* src2, bool mixed, cudaStream_t st) {
+  const long pn = (long)g.panels * g.q;
+  SB_LAUNCH(k_swe_sources_from_disp, blocks_for(pn, 256), 256, 0, st, g, s, dx, dy, dz, s_vor, s_div, src, src2,
+            mixed ? 1 : 0);
+}
+
+}  // namespace sbslpm

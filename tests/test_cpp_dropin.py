@@ -40,6 +40,17 @@ PROGRAM = textwrap.dedent(r"""
       } catch (const std::exception& e) {
         std::printf("exception: %s\n", e.what());
       }
+      // swe_back_rk4_step_2 with the reference's argument list
+      V2 divs("d", 96, 16), height("h", 96, 16), bv("bv", 96, 16), bd("bd", 96, 16), bh("bh", 96, 16);
+      Kokkos::View<int*> counts("counts", 96 * 9 + 2);
+      Kokkos::View<int**, Kokkos::LayoutRight> map("map", 96, 16);
+      try {
+        sbslpm_kokkos::swe_back_rk4_step_2(rc, x, y, z, area, vors, divs, height, interp, panels, list, vx, vy, vz,
+                                           tracers, bv, bd, bh, counts, map, 0.0);
+        std::printf("swe stepped\n");
+      } catch (const std::exception& e) {
+        std::printf("swe exception: %s\n", e.what());
+      }
       return 0;
     }
 """)
@@ -60,3 +71,4 @@ def test_cpp_dropin_header_compiles_and_reaches_the_abi(sb, tmp_path):
     if torch.cuda.is_available():
         pytest.skip("a GPU is present; this test checks the CPU-side path only")
     assert "exception: sbslpm_create" in out.stdout and "no CUDA device" in out.stdout, out.stdout
+    assert "swe exception: sbslpm_create" in out.stdout, out.stdout
