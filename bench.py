@@ -161,6 +161,90 @@ def run_reference(args, rank):
     }))
 
 
+SWE_DT, SWE_STEPS = 0.002, 100
+
+
+def swe_bench(sb, torch, dev, flush, steps):
+    """The shallow-water configuration: 393,216 particles, steady geostrophic
+    solid-body flow on the unit sphere (Omega = 2 pi, u0 = 2 pi/12, g h =
+    2.94 - (Omega u0 + u0^2/2) sin^2 lat, the height field holding g h so g/a
+    = 1), divergence zero, seeded N(0, 1e-4^2) noise on the height, dt =
+    0.002, the reference's spectral FMM (theta 0.7) for both the stream
+    function and the velocity potential.  Reports steps/s of the float64 and
+    mixed paths (L2 flushed between timed steps) and, after 100 steps, the
+    L2 height difference mixed vs float64 and the float64 run's steady-state
+    height drift."""
+    g = sb.build_grid(LEVELS, DEGREE, exact_cc=True)
+    om, u0 = 2 * np.pi, 2 * np.pi / 12
+    lat = np.arcsin(np.clip(g.z, -1, 1))
+    vors = 2 * u0 * np.sin(lat)
+    h0 = 2.94 - (om * u0 + 0.5 * u0 * u0) * np.sin(lat) ** 2
+    h0 = h0 + 1e-4 * np.random.default_rng(4).standard_normal(h0.shape)
+
+    def T(a):
+        return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
+    out, runs = {}, {}
+    for name, prec in (("fp64", sb.FP64), ("mixed", sb.MIXED)):
+        ctx = sb.Context(sb.config_default(levels=LEVELS, interp_degree=DEGREE, fmm_theta=THETA, kernel_eps=EPS,
+                                           omega=om, dt=SWE_DT, precision=prec, g_over_a=1.0))
+        f = [T(g.x), T(g.y), T(g.z), T(g.area), T(vors), torch.zeros_like(T(vors)), T(h0)]
+        vel = [torch.zeros_like(f[0]) for _ in range(3)]
+        base = [torch.zeros_like(f[0]) for _ in range(3)]
+        ctx.swe_init(*f, *vel, *base)
+        args = (*f, *vel, None, *base)
+        ctx.swe_run(*args, nsteps=3)  # warm-up (and the graph capture)
+        torch.cuda.synchronize()
+        st = torch.cuda.current_stream()
+        ts = []
+        for _ in range(steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            ctx.swe_run(*args, nsteps=1)
+            e1.record(st)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        # the drift run: 100 steps from the initial state, in chunks of 10
+        f[4].copy_(T(vors))
+        f[5].zero_()
+        f[6].copy_(T(h0))
+        hist, done = [], 0
+        while done < SWE_STEPS:
+            try:
+                ctx.swe_run(*args, nsteps=10)
+            except sb.SbslpmError as e:
+                hist.append((done + 10, None, str(e).split("(")[-1].rstrip(")")))
+                break
+            done += 10
+            hist.append((done, f[6].clone(), None))
+        torch.cuda.synchronize()
+        runs[name] = hist
+        out[name] = {"steps_per_s": 1e3 / (sum(ts) / len(ts)), "ms_per_step": sum(ts) / len(ts)}
+        del ctx
+    w = T(g.area) / float(g.area.sum())
+    hi = T(h0)
+    l2 = lambda a: float(torch.sqrt((w * a * a).sum()))
+    drift = []
+    for (n64, h64, e64), (n32, h32, e32) in zip(runs["fp64"], runs["mixed"]):
+        row = {"step": n64}
+        if h64 is not None:
+            row["height_l2_drift_fp64"] = l2(h64 - hi) / l2(hi)
+        if h32 is not None:
+            row["height_l2_drift_mixed"] = l2(h32 - hi) / l2(hi)
+        if h64 is not None and h32 is not None:
+            row["height_l2_mixed_vs_fp64"] = l2(h32 - h64) / l2(h64)
+        if e64 or e32:
+            row["stopped"] = e64 or e32
+        drift.append(row)
+    out["drift"] = drift
+    out["speedup_mixed_vs_fp64"] = out["mixed"]["steps_per_s"] / out["fp64"]["steps_per_s"]
+    out["config"] = {"workload": "SWE v2 RK4, 393,216 particles, steady geostrophic flow + N(0,1e-4^2) height "
+                                 "noise, spectral FMM theta 0.7 (proxy degree 3)", "dt": SWE_DT,
+                     "drift_steps": SWE_STEPS, "g_over_a": 1.0, "omega": om, "u0": u0, "gh0": 2.94}
+    return out
+
+
 def timed_steps(torch, ctx, f, steps, flush):
     """Per-step device times (ms) of bve_run(nsteps=1) with an L2 flush between."""
     st = torch.cuda.current_stream()
@@ -183,6 +267,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-swe", action="store_true", help="skip the shallow-water measurement")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 
@@ -286,6 +371,9 @@ def main():
     peak64 = sb.measure_fma_peak(1, 50.0) / 1e12
     share = 4 * ms_int / ms_per_step
 
+    # ---- shallow water (SWE v2) ---------------------------------------------
+    swe = None if args.no_swe else swe_bench(sb, torch, dev, flush, min(args.steps, 20))
+
     # ---- end to end through the C ABI with host buffers ---------------------
     host = [torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in (g.x, g.y, g.z, g.area, vor0)]
     out_host = [torch.empty(g.x.shape, dtype=torch.float64).pin_memory() for _ in range(4)]
@@ -347,7 +435,7 @@ def main():
             "reference_spectral_fmm": {"mixed_steps_per_s": r32_sps, "fp64_steps_per_s": r64_sps,
                                        "note": "the reference's own algorithm (proxy degree = particle degree 3)"},
             "accuracy_step1_vs_fp64_direct": dict(acc, direct_step_s=direct_s),
-            "cpu_baseline": cpu, "clocks": clk.summary(),
+            "swe": swe, "cpu_baseline": cpu, "clocks": clk.summary(),
         }
         print(json.dumps(line))
     if dist:

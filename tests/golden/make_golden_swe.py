@@ -14,6 +14,11 @@ so that its atomics accumulate in a fixed order, and stores small cases as .npz:
                     the driver loop (step + unify of vors/divs/height).
   swe_L4_d2.npz     levels=4, degree=2, theta=0.5: set-up and one step.
   swe_L3_direct.npz levels=3, theta=1e-6 (every pair leaf-leaf): one step.
+  swe_L4_unit.npz   levels=4, theta=0.7: the unit-sphere steady geostrophic
+                    flow with N(0, 1e-4^2) height noise (the 393,216-particle
+                    benchmark configuration at 6,144 particles), time scaled
+                    by 500 so that dt = 0.002 is one integer second; 20 steps
+                    of the driver loop.
 
 Units are the reference's: the unit sphere with time in integer seconds,
 Omega = 2 pi / 86400, and the height Laplacian scaled by the reference's
@@ -100,12 +105,39 @@ def case(ref: Ref, levels, degree, theta, tracer_count, full, rng):
     return out
 
 
+def unit_sphere_case(ref: Ref, levels, nsteps):
+    """Omega = 2 pi, u0 = 2 pi/12, g h = 2.94 - (Omega u0 + u0^2/2) sin^2 lat
+    (+ noise), dt = 0.002 on the unit sphere, expressed in the reference's
+    units: time t' = 500 t (dt' = 1 s), so Omega' = Omega/500, vorticity and
+    divergence / 500, and the height h' = (g h)/500^2/(9.81/6371000), which
+    makes the reference's (9.81/6371000) lap(h') the unit-sphere lap(g h)."""
+    S = 500.0
+    om, u0 = 2 * np.pi, 2 * np.pi / 12
+    c = ref.create(levels, 3, 0.7, EPS, om / S, 1, 0)
+    x, y, z, area, interp = ref.points(c)
+    smap = ref.swe_map(c)
+    lat = np.arcsin(np.clip(z, -1, 1))
+    vors = 2 * u0 * np.sin(lat) / S
+    divs = np.zeros_like(vors)
+    gh = 2.94 - (om * u0 + 0.5 * u0 * u0) * np.sin(lat) ** 2 + 1e-4 * np.random.default_rng(4).standard_normal(vors.shape)
+    height = gh / S ** 2 / G_OVER_A
+    out = dict(levels=levels, degree=3, theta=0.7, eps=EPS, omega=om / S, dt=1.0, g_over_a=G_OVER_A, x=x, y=y, z=z,
+               area=area, vors=vors, divs=divs, height=height, time_scale=S, nsteps=nsteps)
+    vel, base = ref.swe_init(c, vors, divs, height, smap)
+    out["init_base"] = np.stack(base)
+    v, d, h, vel2, _ = ref.swe_step(c, vors, divs, height, base, smap, vel=vel, nsteps=nsteps, driver_unify=True)
+    out["run_vors"], out["run_divs"], out["run_height"], out["run_vel"] = v, d, h, np.stack(vel2)
+    ref.destroy(c)
+    return out
+
+
 def main():
     ref = Ref()
     rng = np.random.default_rng(20261204)
     np.savez_compressed(os.path.join(HERE, "swe_L3.npz"), **case(ref, 3, 3, 0.7, 2, True, rng))
     np.savez_compressed(os.path.join(HERE, "swe_L4_d2.npz"), **case(ref, 4, 2, 0.5, 1, False, rng))
     np.savez_compressed(os.path.join(HERE, "swe_L3_direct.npz"), **case(ref, 3, 3, 1e-6, 0, False, rng))
+    np.savez_compressed(os.path.join(HERE, "swe_L4_unit.npz"), **unit_sphere_case(ref, 4, 20))
     print("SWE golden vectors written to", HERE)
 
 
