@@ -258,6 +258,46 @@ sbslpm_status sbslpm_swe_vel_interactions(sbslpm_ctx* ctx, const double* disp_x,
 sbslpm_status sbslpm_cubed_sphere_2d_to_1d(long n_leaves, int degree, const double* xcos, const double* ycos,
                                            const double* zcos, int* two_d_to_1d, int* counts, long* unique);
 
+/* ---------------- batched ensemble (device pointers) ---------------- */
+
+/* No counterpart in the reference (its drivers run one problem per process).
+ * An ensemble of `members` BVE problems on one particle grid (base->levels,
+ * base->interp_degree, kernel_eps, omega, dt, precision, leaf_size shared),
+ * each with its own vorticity, MAC parameter theta[m] and treecode proxy
+ * degree proxy_degree[m] (5..10), so the members' trees and interaction lists
+ * differ.  A step is one launch per phase over all members (the
+ * well-separated proxy interactions once per proxy degree in use); member m's
+ * result is the one a single context with (theta[m], proxy_degree[m]) gives
+ * on the same input.  The near-field launch shape is chosen by timing the
+ * candidates on the first step. */
+typedef struct sbslpm_batch sbslpm_batch;
+sbslpm_status sbslpm_batch_create(const sbslpm_config* base, int members, const double* theta,
+                                  const int* proxy_degree, sbslpm_batch** out);
+sbslpm_status sbslpm_batch_destroy(sbslpm_batch* batch);
+sbslpm_status sbslpm_batch_set_stream(sbslpm_batch* batch, void* cuda_stream);
+/* sizes[0..3] = members, leaf_count, q, particles per member */
+sbslpm_status sbslpm_batch_get_sizes(const sbslpm_batch* batch, long* sizes);
+/* One bve_back_rk4_step of every member.  xcos..area: [leaf][q] (shared);
+ * vors: [members][leaf][q], advanced in place; vel: [members][3][leaf][q]
+ * receives the stage-0 velocities. */
+sbslpm_status sbslpm_batch_step(sbslpm_batch* batch, const double* xcos, const double* ycos, const double* zcos,
+                                const double* area, double* vors, double* vel, double time);
+/* nsteps steps, captured once as a CUDA graph and replayed. */
+sbslpm_status sbslpm_batch_run(sbslpm_batch* batch, const double* xcos, const double* ycos, const double* zcos,
+                               const double* area, double* vors, double* vel, double time, int nsteps);
+/* The autotuner's choice: shape[0..3] = threads per block, targets per thread,
+ * source-list splits, candidates timed; *ms_per_launch of the chosen shape. */
+sbslpm_status sbslpm_batch_tuning(const sbslpm_batch* batch, int* shape, double* ms_per_launch);
+/* Fixes the near-field launch shape instead of the autotuner's choice:
+ * threads per block 64 | 128 | 256, targets per thread 1 | 2 | 4 (threads x
+ * targets >= particles per treecode leaf), source-list splits 1..4.  The
+ * split count sets the order in which a target's near-field partial sums are
+ * added (a single context uses 2). */
+sbslpm_status sbslpm_batch_set_tuning(sbslpm_batch* batch, int threads, int targets_per_thread, int splits);
+/* Pair evaluations of one velocity evaluation over all members: near field
+ * (particle x particle) and well-separated (proxy x proxy). */
+sbslpm_status sbslpm_batch_pairs(const sbslpm_batch* batch, double* near_pairs, double* far_pairs);
+
 /* ---------------- direct sums (device pointers, no context) ---------------- */
 
 /* Biot-Savart direct sum on the sphere (the reference's BVE kernel,

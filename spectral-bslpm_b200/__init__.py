@@ -122,6 +122,15 @@ def lib() -> ctypes.CDLL:
     L.sbslpm_swe_vel_interactions.argtypes = [_VP] * 9
     L.sbslpm_cubed_sphere_2d_to_1d.argtypes = [ctypes.c_long, ctypes.c_int, _D, _D, _D, _I, _I,
                                                ctypes.POINTER(ctypes.c_long)]
+    L.sbslpm_batch_create.argtypes = [ctypes.POINTER(Config), ctypes.c_int, _D, _I, ctypes.POINTER(_VP)]
+    L.sbslpm_batch_destroy.argtypes = [_VP]
+    L.sbslpm_batch_set_stream.argtypes = [_VP, _VP]
+    L.sbslpm_batch_get_sizes.argtypes = [_VP, ctypes.POINTER(ctypes.c_long)]
+    L.sbslpm_batch_step.argtypes = [_VP] + [_VP] * 6 + [ctypes.c_double]
+    L.sbslpm_batch_run.argtypes = [_VP] + [_VP] * 6 + [ctypes.c_double, ctypes.c_int]
+    L.sbslpm_batch_tuning.argtypes = [_VP, _I, _D]
+    L.sbslpm_batch_pairs.argtypes = [_VP, _D, _D]
+    L.sbslpm_batch_set_tuning.argtypes = [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     L.sbslpm_time_interactions.argtypes = [_VP, ctypes.c_int, _D, _D]
     L.sbslpm_measure_fma_peak.argtypes = [ctypes.c_int, ctypes.c_double, _D]
     _lib = L
@@ -411,6 +420,74 @@ class Context:
         _check(lib().sbslpm_bve_remap(self._h, *[_dev(t, "field") for t in (zcos, dep_x, dep_y, dep_z, vors)],
                                       _dev(tracers, "tracers"), _dev(new_vors, "new_vors"),
                                       _dev(new_tracers, "new_tracers")), "sbslpm_bve_remap")
+
+
+class Batch:
+    """sbslpm_batch: an ensemble of BVE problems on one particle grid, each
+    member with its own vorticity, theta and treecode proxy degree."""
+
+    def __init__(self, base: Config, theta, proxy_degree):
+        theta = np.ascontiguousarray(theta, dtype=np.float64)
+        deg = np.ascontiguousarray(proxy_degree, dtype=np.int32)
+        if theta.shape != deg.shape or theta.ndim != 1:
+            raise ValueError("theta and proxy_degree must be 1-D of equal length")
+        self.cfg = base
+        h = _VP()
+        _check(lib().sbslpm_batch_create(ctypes.byref(base), len(theta), theta.ctypes.data_as(_D),
+                                         deg.ctypes.data_as(_I), ctypes.byref(h)), "sbslpm_batch_create")
+        self._h = h
+        sizes = (ctypes.c_long * 4)()
+        _check(lib().sbslpm_batch_get_sizes(self._h, sizes), "sbslpm_batch_get_sizes")
+        self.members, self.leaf_count, self.q, self.particles = (int(v) for v in sizes)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().sbslpm_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _sync_stream(self):
+        _check(lib().sbslpm_batch_set_stream(self._h, _VP(_stream())), "sbslpm_batch_set_stream")
+
+    def _ptrs(self, xcos, ycos, zcos, area, vors, vel):
+        lq = (self.leaf_count, self.q)
+        return ([_dev(t, n, lq) for t, n in ((xcos, "xcos"), (ycos, "ycos"), (zcos, "zcos"), (area, "area"))] +
+                [_dev(vors, "vors", (self.members,) + lq), _dev(vel, "vel", (self.members, 3) + lq)])
+
+    def step(self, xcos, ycos, zcos, area, vors, vel, time=0.0):
+        """One step of every member: vors [members][leaf][q] in place,
+        vel [members][3][leaf][q] receives the stage-0 velocities."""
+        self._sync_stream()
+        _check(lib().sbslpm_batch_step(self._h, *self._ptrs(xcos, ycos, zcos, area, vors, vel), float(time)),
+               "sbslpm_batch_step")
+
+    def run(self, xcos, ycos, zcos, area, vors, vel, time=0.0, nsteps=1):
+        """nsteps steps of every member replayed from one captured CUDA graph."""
+        self._sync_stream()
+        _check(lib().sbslpm_batch_run(self._h, *self._ptrs(xcos, ycos, zcos, area, vors, vel), float(time),
+                                      int(nsteps)), "sbslpm_batch_run")
+
+    def tuning(self):
+        """(threads per block, targets per thread, splits, candidates timed, ms per near launch)."""
+        shape = (ctypes.c_int * 4)()
+        ms = ctypes.c_double()
+        _check(lib().sbslpm_batch_tuning(self._h, shape, ctypes.byref(ms)), "sbslpm_batch_tuning")
+        return (*[int(v) for v in shape], ms.value)
+
+    def set_tuning(self, threads: int, targets_per_thread: int, splits: int):
+        _check(lib().sbslpm_batch_set_tuning(self._h, int(threads), int(targets_per_thread), int(splits)),
+               "sbslpm_batch_set_tuning")
+
+    def pairs(self):
+        """(near-field, well-separated) pair evaluations of one velocity evaluation, all members."""
+        a, b = ctypes.c_double(), ctypes.c_double()
+        _check(lib().sbslpm_batch_pairs(self._h, ctypes.byref(a), ctypes.byref(b)), "sbslpm_batch_pairs")
+        return a.value, b.value
 
 
 def measure_fma_peak(kind: int = 0, ms: float = 50.0) -> float:

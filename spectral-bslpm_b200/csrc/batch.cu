@@ -1,0 +1,470 @@
+// Batched ensemble of BVE problems on one particle grid: M members, each with
+// its own vorticity, MAC parameter theta and treecode proxy degree (uneven
+// trees and lists).  One velocity evaluation is one launch per phase over all
+// members (the well-separated proxy interactions once per proxy degree), the
+// departure search and remap one launch over all members' particles, and a
+// whole step one CUDA graph.  The near-field tile shape and source-list split
+// are chosen by a timing autotuner on the first step.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "context_internal.hpp"
+#include "geometry.cuh"
+
+using namespace sbslpm;
+
+struct sbslpm_batch {
+  sbslpm_config cfg{};
+  int M = 0, L = 0, d = 0, q = 0, P = 0, A = 0, off = 0;
+  long N = 0;
+  std::vector<double> theta;
+  std::vector<int> degree;
+  std::vector<sbslpm_panel> panels;
+  cudaStream_t user_stream = nullptr, own_stream = nullptr;
+  bool user_stream_set = false;
+  BliTable tab{};
+  StepGeom g{};  // the particle grid (departure search and remap)
+  int Lf = 0, Pf = 0, Af = 0, npl = 0, nmax = 0, qmax = 0;
+
+  struct Degree {
+    int n = -1, qx = 0;
+    TreeTables t;
+    double *fpx = nullptr, *fcentre = nullptr, *fbounds = nullptr, *fchild = nullptr, *flx = nullptr, *fly = nullptr;
+    int* fface = nullptr;
+    std::vector<int> members;
+    int* d_idx = nullptr;
+  };
+  std::vector<Degree> degs;
+  std::vector<void*> bufs;  // every device buffer of the batch, freed on destroy
+  std::vector<BatchMember> h_mem;
+  BatchMember* d_mem = nullptr;
+  std::vector<long> near_pairs, cc_pairs;  // leaf pairs / well-separated pairs per member
+
+  double4* psrc = nullptr;
+  float4* psrcf = nullptr;
+  double *near = nullptr, *vbuf = nullptr, *newvor = nullptr;
+  unsigned* err = nullptr;
+  unsigned* h_err = nullptr;
+
+  // autotuned near-field launch shape
+  bool tuned = false;
+  int nt = 128, tpt = 2, splits = 2, candidates = 0;
+  double tuned_ms = 0;
+  static constexpr int kMaxSplits = 4;
+
+  cudaGraphExec_t graph = nullptr;
+  const void* key[7] = {};
+  long launches_per_step = 0;
+
+  cudaStream_t stream() const { return user_stream_set ? user_stream : own_stream; }
+};
+
+namespace {
+
+template <class T>
+sbslpm_status balloc(sbslpm_batch* b, T** p, size_t count) {
+  SB_TRY(dalloc(p, count));
+  if (*p) b->bufs.push_back(*p);
+  return SBSLPM_OK;
+}
+
+template <class T>
+sbslpm_status bupload(sbslpm_batch* b, T** p, const std::vector<T>& h) {
+  SB_TRY(upload(p, h));
+  if (*p) b->bufs.push_back(*p);
+  return SBSLPM_OK;
+}
+
+sbslpm_status batch_finish(sbslpm_batch* b) {
+  cudaStream_t st = b->stream();
+  SB_CUDA(cudaGetLastError());
+  SB_CUDA(cudaMemcpyAsync(b->h_err, b->err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+  SB_CUDA(cudaStreamSynchronize(st));
+  const unsigned e = *b->h_err;
+  if (e) {
+    SB_CUDA(cudaMemsetAsync(b->err, 0, sizeof(unsigned), st));
+    SB_CUDA(cudaStreamSynchronize(st));
+    if (e & kErrNonFinite) return set_last_error("non-finite point in a location step"), SBSLPM_ERR_NONFINITE;
+    return set_last_error("interpolation point outside its panel"), SBSLPM_ERR_OUT_OF_PANEL;
+  }
+  return SBSLPM_OK;
+}
+
+sbslpm_status batch_setup(sbslpm_batch* b) {
+  const sbslpm_config& c = b->cfg;
+  b->L = c.levels;
+  b->d = c.interp_degree;
+  b->q = (b->d + 1) * (b->d + 1);
+  b->P = sbslpm_panel_count(b->L);
+  b->A = sbslpm_leaf_count(b->L);
+  b->off = b->P - b->A;
+  b->N = (long)b->A * b->q;
+  build_panels(b->L, b->panels);
+  bli_table(b->d, b->tab);
+  SB_TRY(balloc(b, &b->err, 1));
+  SB_CUDA(cudaMemset(b->err, 0, sizeof(unsigned)));
+  SB_CUDA(cudaMallocHost(reinterpret_cast<void**>(&b->h_err), sizeof(unsigned)));
+
+  StepGeom& g = b->g;
+  g.levels = b->L;
+  g.degree = b->d;
+  g.q = b->q;
+  g.panels = b->P;
+  g.leaves = b->A;
+  g.offset = b->off;
+  g.eps = c.kernel_eps;
+  g.omega = c.omega;
+  g.err = b->err;
+
+  // one set of tree tables per proxy degree in use
+  std::vector<int> uniq(b->degree.begin(), b->degree.end());
+  std::sort(uniq.begin(), uniq.end());
+  uniq.erase(std::unique(uniq.begin(), uniq.end()), uniq.end());
+  b->degs.resize(uniq.size());
+  for (size_t k = 0; k < uniq.size(); k++) {
+    sbslpm_batch::Degree& D = b->degs[k];
+    D.n = uniq[k];
+    D.qx = (D.n + 1) * (D.n + 1);
+    SB_TRY(build_tree_tables(b->L, b->d, b->panels, c.leaf_size, D.n, D.t));
+    SB_TRY(bupload(b, &D.fpx, D.t.fpx));
+    SB_TRY(bupload(b, &D.fcentre, D.t.centre));
+    SB_TRY(bupload(b, &D.fbounds, D.t.bounds));
+    SB_TRY(bupload(b, &D.fface, D.t.face));
+    if (!D.t.c1d.empty()) SB_TRY(bupload(b, &D.fchild, D.t.c1d));
+    SB_TRY(bupload(b, &D.flx, D.t.lx));
+    SB_TRY(bupload(b, &D.fly, D.t.ly));
+  }
+  b->Lf = b->degs[0].t.Lf;
+  b->Pf = b->degs[0].t.Pf;
+  b->Af = b->degs[0].t.Af;
+  b->npl = b->degs[0].t.npl;
+  b->nmax = uniq.back();
+  b->qmax = (b->nmax + 1) * (b->nmax + 1);
+
+  const bool mixed = c.precision == SBSLPM_MIXED;
+  b->h_mem.resize(b->M);
+  b->near_pairs.assign(b->M, 0);
+  b->cc_pairs.assign(b->M, 0);
+  for (int m = 0; m < b->M; m++) {
+    const size_t k = std::lower_bound(uniq.begin(), uniq.end(), b->degree[m]) - uniq.begin();
+    sbslpm_batch::Degree& D = b->degs[k];
+    D.members.push_back(m);
+    TreeLists l;
+    build_tree_lists(D.t, b->theta[m], l);
+    b->near_pairs[m] = l.ns.back();
+    b->cc_pairs[m] = l.cs.back();
+    int *ns = nullptr, *nsrc = nullptr, *cs = nullptr, *csrc = nullptr;
+    SB_TRY(bupload(b, &ns, l.ns));
+    SB_TRY(bupload(b, &nsrc, l.nsrc));
+    SB_TRY(bupload(b, &cs, l.cs));
+    SB_TRY(bupload(b, &csrc, l.csrc));
+    const size_t pn = (size_t)b->Pf * D.qx;
+    double4* fsrc = nullptr;
+    float4* fsrcf = nullptr;
+    double* ftgt = nullptr;
+    SB_TRY(balloc(b, &fsrc, pn));
+    std::vector<double4> init(pn);
+    for (size_t i = 0; i < pn; i++) init[i] = make_double4(D.t.fpx[i], D.t.fpx[pn + i], D.t.fpx[2 * pn + i], 0.0);
+    SB_CUDA(cudaMemcpy(fsrc, init.data(), sizeof(double4) * pn, cudaMemcpyHostToDevice));
+    if (mixed) SB_TRY(balloc(b, &fsrcf, pn));
+    SB_TRY(balloc(b, &ftgt, 3 * pn));
+
+    BatchMember& bm = b->h_mem[m];
+    StepGeom& fg = bm.fg;
+    fg = StepGeom{};
+    fg.levels = D.t.Lf;
+    fg.degree = D.n;
+    fg.q = D.qx;
+    fg.panels = D.t.Pf;
+    fg.leaves = D.t.Af;
+    fg.offset = D.t.Pf - D.t.Af;
+    fg.eps = c.kernel_eps;
+    fg.omega = c.omega;
+    fg.px = D.fpx;
+    fg.tgt_start = cs;
+    fg.src_panel = csrc;
+    fg.child_1d = D.fchild;
+    fg.pd_centre = D.fcentre;
+    fg.srcf = fsrcf;
+    fg.err = b->err;
+    TreeGeom& tg = bm.tg;
+    tg.n = D.n;
+    tg.npl = D.t.npl;
+    tg.N = b->N;
+    tg.eps = c.kernel_eps;
+    tg.omega = c.omega;
+    tg.lx = D.flx;
+    tg.ly = D.fly;
+    tg.fbounds = D.fbounds;
+    tg.fface = D.fface;
+    tg.near_start = ns;
+    tg.near_src = nsrc;
+    bm.tab = D.t.ftab;
+    bm.fsrc = fsrc;
+    bm.ftgt = ftgt;
+  }
+  for (auto& D : b->degs) SB_TRY(bupload(b, &D.d_idx, D.members));
+  SB_TRY(bupload(b, &b->d_mem, b->h_mem));
+
+  const size_t MN = (size_t)b->M * b->N;
+  SB_TRY(balloc(b, &b->psrc, MN));
+  if (mixed) SB_TRY(balloc(b, &b->psrcf, MN));
+  SB_TRY(balloc(b, &b->near, (size_t)sbslpm_batch::kMaxSplits * 3 * MN));
+  SB_TRY(balloc(b, &b->vbuf, 4 * 3 * MN));
+  SB_TRY(balloc(b, &b->newvor, MN));
+  return SBSLPM_OK;
+}
+
+// One velocity evaluation of every member (bve_back_rk4_step's stage, with the
+// treecode of section "decoupled proxy degree"), stage velocities into v.
+void batch_velocity(sbslpm_batch* b, int stage, double dt_s, const double* vprev, const double* x, const double* y,
+                    const double* z, const double* area, const double* vors, double* v) {
+  cudaStream_t st = b->stream();
+  const int prec = b->cfg.precision;
+  const bool mixed = prec == SBSLPM_MIXED;
+  launch_bltc_sources_batch(b->d_mem, b->M, b->Af, b->npl, b->nmax, stage, dt_s, vprev, x, y, z, vors, area, b->psrc,
+                            b->psrcf, mixed, st);
+  launch_upward_batch(b->d_mem, b->M, b->Lf, b->qmax, mixed, st);
+  for (const auto& D : b->degs)
+    launch_cc_batch(b->d_mem, D.d_idx, (int)D.members.size(), D.qx, b->Pf, b->cfg.kernel_eps, prec, st);
+  launch_downward_batch(b->d_mem, b->M, b->Lf, b->qmax, st);
+  launch_bltc_near_batch(b->d_mem, b->M, b->Af, b->npl, b->cfg.kernel_eps, prec, x, y, z, b->psrc, b->psrcf, b->near,
+                         b->splits, b->nt, b->tpt, st);
+  launch_bltc_to_particles_batch(b->d_mem, b->M, b->Af, b->nmax, b->near, b->splits, v, st);
+}
+
+void batch_enqueue_step(sbslpm_batch* b, const double* x, const double* y, const double* z, const double* area,
+                        double* vors, double* vel) {
+  cudaStream_t st = b->stream();
+  const size_t MN = (size_t)b->M * b->N;
+  const double dt = b->cfg.dt;
+  double* v[4];
+  for (int k = 0; k < 4; k++) v[k] = b->vbuf + (size_t)k * 3 * MN;
+  const double stage_dt[4] = {0.0, 0.5 * dt, 0.5 * dt, dt};
+  for (int s = 0; s < 4; s++) batch_velocity(b, s, stage_dt[s], s ? v[s - 1] : nullptr, x, y, z, area, vors, v[s]);
+  launch_depart_remap_batch(b->g, &b->tab, b->M, x, y, z, v[0], v[1], v[2], v[3], dt, vors, b->newvor, st);
+  cudaMemcpyAsync(vors, b->newvor, sizeof(double) * MN, cudaMemcpyDeviceToDevice, st);
+  cudaMemcpyAsync(vel, v[0], sizeof(double) * 3 * MN, cudaMemcpyDeviceToDevice, st);
+}
+
+// Times every near-field launch shape (threads x targets per thread covering a
+// leaf, and 1..4 source-list splits) on the members' stage-0 sources and
+// keeps the fastest.  Runs once, before the first step, outside any capture.
+sbslpm_status batch_autotune(sbslpm_batch* b, const double* x, const double* y, const double* z, const double* area,
+                             const double* vors) {
+  if (b->tuned) return SBSLPM_OK;
+  cudaStream_t st = b->stream();
+  const int prec = b->cfg.precision;
+  launch_bltc_sources_batch(b->d_mem, b->M, b->Af, b->npl, b->nmax, 0, 0.0, nullptr, x, y, z, vors, area, b->psrc,
+                            b->psrcf, prec == SBSLPM_MIXED, st);
+  const int shapes[][2] = {{64, 4}, {128, 2}, {256, 1}, {256, 2}, {64, 2}, {64, 1}, {128, 1}};
+  cudaEvent_t e0, e1;
+  SB_CUDA(cudaEventCreate(&e0));
+  SB_CUDA(cudaEventCreate(&e1));
+  double best = 1e30;
+  int cand = 0;
+  for (const auto& sh : shapes) {
+    if (sh[0] * sh[1] < b->npl || sh[0] * sh[1] >= 4 * b->npl) continue;
+    for (int sp = 1; sp <= sbslpm_batch::kMaxSplits; sp++) {
+      launch_bltc_near_batch(b->d_mem, b->M, b->Af, b->npl, b->cfg.kernel_eps, prec, x, y, z, b->psrc, b->psrcf,
+                             b->near, sp, sh[0], sh[1], st);  // warm-up
+      SB_CUDA(cudaEventRecord(e0, st));
+      for (int r = 0; r < 3; r++)
+        launch_bltc_near_batch(b->d_mem, b->M, b->Af, b->npl, b->cfg.kernel_eps, prec, x, y, z, b->psrc, b->psrcf,
+                               b->near, sp, sh[0], sh[1], st);
+      SB_CUDA(cudaEventRecord(e1, st));
+      SB_CUDA(cudaEventSynchronize(e1));
+      float ms = 0;
+      SB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      cand++;
+      if (ms / 3 < best) {
+        best = ms / 3;
+        b->nt = sh[0];
+        b->tpt = sh[1];
+        b->splits = sp;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  b->candidates = cand;
+  b->tuned_ms = best;
+  b->tuned = true;
+  return batch_finish(b);
+}
+
+bool bad(const void* p) { return p == nullptr; }
+
+}  // namespace
+
+extern "C" {
+
+sbslpm_status sbslpm_batch_destroy(sbslpm_batch* b) {
+  if (!b) return SBSLPM_OK;
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  for (void* p : b->bufs) cudaFree(p);
+  if (b->h_err) cudaFreeHost(b->h_err);
+  if (b->own_stream) cudaStreamDestroy(b->own_stream);
+  delete b;
+  return SBSLPM_OK;
+}
+
+sbslpm_status sbslpm_batch_create(const sbslpm_config* base, int members, const double* theta,
+                                  const int* proxy_degree, sbslpm_batch** out) {
+  if (!base || !theta || !proxy_degree || !out || members < 1 || members > 65535) return SBSLPM_ERR_ARG;
+  *out = nullptr;
+  sbslpm_config c = *base;
+  c.velocity = SBSLPM_VEL_FMM;
+  c.tracer_count = 0;
+  for (int m = 0; m < members; m++) {
+    if (proxy_degree[m] < 5 || proxy_degree[m] > kMaxDegree)
+      return set_last_error("batched members need proxy_degree in 5..10"), SBSLPM_ERR_CONFIG;
+    if (!(theta[m] > 0) || !std::isfinite(theta[m]))
+      return set_last_error("batched members need a positive finite theta"), SBSLPM_ERR_CONFIG;
+  }
+  c.proxy_degree = proxy_degree[0];
+  c.fmm_theta = theta[0];
+  if (c.levels < 1 || c.levels > 12 || c.interp_degree < 0 || c.interp_degree > kMaxDegree ||
+      (c.precision != SBSLPM_FP64 && c.precision != SBSLPM_MIXED) || !(c.kernel_eps >= 0) || !std::isfinite(c.dt) ||
+      !std::isfinite(c.omega))
+    return set_last_error("invalid base configuration"), SBSLPM_ERR_CONFIG;
+  const int qp = (c.interp_degree + 1) * (c.interp_degree + 1);
+  long npl = qp;
+  while (npl * 4 <= c.leaf_size) npl *= 4;
+  if (c.leaf_size < qp || npl > 512)
+    return set_last_error("leaf_size must hold at least one panel's points and at most 512"), SBSLPM_ERR_CONFIG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    set_last_error("no CUDA device available");
+    return SBSLPM_ERR_NO_DEVICE;
+  }
+  sbslpm_batch* b = new sbslpm_batch();
+  b->cfg = c;
+  b->M = members;
+  b->theta.assign(theta, theta + members);
+  b->degree.assign(proxy_degree, proxy_degree + members);
+  sbslpm_status s = SBSLPM_OK;
+  if (cudaStreamCreateWithFlags(&b->own_stream, cudaStreamNonBlocking) != cudaSuccess) s = SBSLPM_ERR_CUDA;
+  if (s == SBSLPM_OK) s = batch_setup(b);
+  if (s != SBSLPM_OK) {
+    sbslpm_batch_destroy(b);
+    return s;
+  }
+  *out = b;
+  return SBSLPM_OK;
+}
+
+sbslpm_status sbslpm_batch_set_stream(sbslpm_batch* b, void* stream) {
+  if (!b) return SBSLPM_ERR_ARG;
+  b->user_stream = static_cast<cudaStream_t>(stream);
+  b->user_stream_set = true;
+  return SBSLPM_OK;
+}
+
+sbslpm_status sbslpm_batch_get_sizes(const sbslpm_batch* b, long* sizes) {
+  if (!b || !sizes) return SBSLPM_ERR_ARG;
+  sizes[0] = b->M;
+  sizes[1] = b->A;
+  sizes[2] = b->q;
+  sizes[3] = b->N;
+  return SBSLPM_OK;
+}
+
+sbslpm_status sbslpm_batch_step(sbslpm_batch* b, const double* x, const double* y, const double* z,
+                                const double* area, double* vors, double* vel, double) {
+  if (!b || bad(x) || bad(y) || bad(z) || bad(area) || bad(vors) || bad(vel)) return SBSLPM_ERR_ARG;
+  SB_TRY(batch_autotune(b, x, y, z, area, vors));
+  batch_enqueue_step(b, x, y, z, area, vors, vel);
+  return batch_finish(b);
+}
+
+sbslpm_status sbslpm_batch_run(sbslpm_batch* b, const double* x, const double* y, const double* z,
+                               const double* area, double* vors, double* vel, double, int nsteps) {
+  if (!b || bad(x) || bad(y) || bad(z) || bad(area) || bad(vors) || bad(vel) || nsteps < 0) return SBSLPM_ERR_ARG;
+  SB_TRY(batch_autotune(b, x, y, z, area, vors));
+  const void* key[7] = {x, y, z, area, vors, vel, nullptr};
+  cudaStream_t st = b->stream();
+  if (!b->graph || std::memcmp(key, b->key, sizeof key) != 0) {
+    if (b->graph) {
+      cudaGraphExecDestroy(b->graph);
+      b->graph = nullptr;
+    }
+    cudaStream_t cap = b->own_stream;
+    if (st != cap) {
+      cudaEvent_t ev;
+      SB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+      SB_CUDA(cudaEventRecord(ev, st));
+      SB_CUDA(cudaStreamWaitEvent(cap, ev, 0));
+      cudaEventDestroy(ev);
+    }
+    const bool saved = b->user_stream_set;
+    b->user_stream_set = false;
+    const long before = launch_counter();
+    cudaGraph_t gr;
+    SB_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+    batch_enqueue_step(b, x, y, z, area, vors, vel);
+    cudaError_t ce = cudaStreamEndCapture(cap, &gr);
+    b->user_stream_set = saved;
+    b->launches_per_step = launch_counter() - before;
+    launch_counter() = before;
+    SB_CUDA(ce);
+    SB_CUDA(cudaGraphInstantiate(&b->graph, gr, 0));
+    cudaGraphDestroy(gr);
+    std::memcpy(b->key, key, sizeof key);
+  }
+  for (int s = 0; s < nsteps; s++) {
+    SB_CUDA(cudaGraphLaunch(b->graph, st));
+    launch_counter() += b->launches_per_step;
+  }
+  return batch_finish(b);
+}
+
+sbslpm_status sbslpm_batch_tuning(const sbslpm_batch* b, int* shape, double* ms_per_launch) {
+  if (!b || !shape || !ms_per_launch) return SBSLPM_ERR_ARG;
+  shape[0] = b->nt;
+  shape[1] = b->tpt;
+  shape[2] = b->splits;
+  shape[3] = b->candidates;
+  *ms_per_launch = b->tuned_ms;
+  return SBSLPM_OK;
+}
+
+sbslpm_status sbslpm_batch_set_tuning(sbslpm_batch* b, int threads, int targets_per_thread, int splits) {
+  if (!b) return SBSLPM_ERR_ARG;
+  const bool ok = ((threads == 64 && (targets_per_thread == 1 || targets_per_thread == 2 || targets_per_thread == 4)) ||
+                   (threads == 128 && (targets_per_thread == 1 || targets_per_thread == 2)) ||
+                   (threads == 256 && (targets_per_thread == 1 || targets_per_thread == 2))) &&
+                  threads * targets_per_thread >= b->npl && splits >= 1 && splits <= sbslpm_batch::kMaxSplits;
+  if (!ok) return set_last_error("unsupported near-field launch shape"), SBSLPM_ERR_ARG;
+  b->nt = threads;
+  b->tpt = targets_per_thread;
+  b->splits = splits;
+  b->candidates = 0;
+  b->tuned_ms = 0;
+  b->tuned = true;
+  if (b->graph) {
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  return SBSLPM_OK;
+}
+
+sbslpm_status sbslpm_batch_pairs(const sbslpm_batch* b, double* near_pairs, double* far_pairs) {
+  if (!b || !near_pairs || !far_pairs) return SBSLPM_ERR_ARG;
+  double np = 0, fp = 0;
+  for (int m = 0; m < b->M; m++) {
+    const double qx = (b->degree[m] + 1.0) * (b->degree[m] + 1.0);
+    np += (double)b->near_pairs[m] * b->npl * b->npl;
+    fp += (double)b->cc_pairs[m] * qx * qx;
+  }
+  *near_pairs = np;
+  *far_pairs = fp;
+  return SBSLPM_OK;
+}
+
+}  // extern "C"

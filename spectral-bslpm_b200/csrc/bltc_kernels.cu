@@ -64,13 +64,15 @@ __device__ __forceinline__ void bli_1d_free(double t, double lo, double hi, int 
   for (int i = 0; i <= n; i++) f[i] *= inv;
 }
 
-__global__ void __launch_bounds__(kThreads)
-    k_bltc_sources(TreeGeom tg, StepGeom fg, BliTable tab, int stage, double dt_s, const double* __restrict__ vprev,
-                   const double* __restrict__ x, const double* __restrict__ y, const double* __restrict__ z,
-                   const double* __restrict__ vors, const double* __restrict__ area, double4* __restrict__ psrc,
-                   float4* __restrict__ psrcf, double4* __restrict__ proxy, int mixed) {
+__device__ __forceinline__ void bltc_sources_body(const TreeGeom& tg, const StepGeom& fg, const BliTable& tab, int f,
+                                                  int stage, double dt_s, const double* __restrict__ vprev,
+                                                  const double* __restrict__ x, const double* __restrict__ y,
+                                                  const double* __restrict__ z, const double* __restrict__ vors,
+                                                  const double* __restrict__ area, double4* __restrict__ psrc,
+                                                  float4* __restrict__ psrcf, double4* __restrict__ proxy,
+                                                  int mixed) {
   extern __shared__ double sh[];
-  const int n1 = tg.n + 1, npl = tg.npl, f = blockIdx.x;
+  const int n1 = tg.n + 1, npl = tg.npl;
   double* lx = sh;              // [npl][n1]
   double* ly = lx + npl * n1;   // [npl][n1]
   double* sw = ly + npl * n1;   // [npl]
@@ -113,6 +115,28 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+__global__ void __launch_bounds__(kThreads)
+    k_bltc_sources(TreeGeom tg, StepGeom fg, BliTable tab, int stage, double dt_s, const double* __restrict__ vprev,
+                   const double* __restrict__ x, const double* __restrict__ y, const double* __restrict__ z,
+                   const double* __restrict__ vors, const double* __restrict__ area, double4* __restrict__ psrc,
+                   float4* __restrict__ psrcf, double4* __restrict__ proxy, int mixed) {
+  bltc_sources_body(tg, fg, tab, blockIdx.x, stage, dt_s, vprev, x, y, z, vors, area, psrc, psrcf, proxy, mixed);
+}
+
+// Batched members (member blockIdx.y) on one particle grid.
+__global__ void __launch_bounds__(kThreads)
+    k_bltc_sources_batch(const BatchMember* __restrict__ mem, int stage, double dt_s, const double* __restrict__ vprev,
+                         const double* __restrict__ x, const double* __restrict__ y, const double* __restrict__ z,
+                         const double* __restrict__ vors, const double* __restrict__ area,
+                         double4* __restrict__ psrc, float4* __restrict__ psrcf, int mixed) {
+  const BatchMember& m = mem[blockIdx.y];
+  const TreeGeom tg = m.tg;
+  const StepGeom fg = m.fg;
+  const long N = tg.N, mo = (long)blockIdx.y;
+  bltc_sources_body(tg, fg, m.tab, blockIdx.x, stage, dt_s, vprev ? vprev + mo * 3 * N : nullptr, x, y, z,
+                    vors + mo * N, area, psrc + mo * N, psrcf ? psrcf + mo * N : nullptr, m.fsrc, mixed);
+}
+
 // Near leaf pairs: one CTA of NT threads per (target leaf, source split),
 // TPT targets per thread (NT * TPT >= particles per leaf), the source leaf's
 // particles staged in shared memory and read back as broadcasts.  Split y of
@@ -120,12 +144,13 @@ __global__ void __launch_bounds__(kThreads)
 // to out + y * 3N (the splits even out the work across SMs);
 // k_bltc_to_particles adds them in split order.
 template <int NT, int TPT, bool GUARD>
-__global__ void __launch_bounds__(NT)
-    k_bltc_near64(TreeGeom tg, const double* __restrict__ x, const double* __restrict__ y,
-                  const double* __restrict__ z, const double4* __restrict__ psrc, double* __restrict__ out) {
-  double* v = out + (long)blockIdx.y * 3 * tg.N;  // partial sums of this source split
+__device__ __forceinline__ void bltc_near64_body(const TreeGeom& tg, int f, int split, int nsplit,
+                                                 const double* __restrict__ x, const double* __restrict__ y,
+                                                 const double* __restrict__ z, const double4* __restrict__ psrc,
+                                                 double* __restrict__ out) {
+  double* v = out + (long)split * 3 * tg.N;  // partial sums of this source split
   extern __shared__ double4 tile[];
-  const int npl = tg.npl, f = blockIdx.x;
+  const int npl = tg.npl;
   double tx[TPT], ty[TPT], tz[TPT], ax[TPT], ay[TPT], az[TPT];
 #pragma unroll
   for (int r = 0; r < TPT; r++) {
@@ -137,7 +162,7 @@ __global__ void __launch_bounds__(NT)
     ax[r] = ay[r] = az[r] = 0;
   }
   const double eps = tg.eps;
-  for (int e = tg.near_start[f] + blockIdx.y; e < tg.near_start[f + 1]; e += gridDim.y) {
+  for (int e = tg.near_start[f] + split; e < tg.near_start[f + 1]; e += nsplit) {
     const long sb = (long)tg.near_src[e] * npl;
     __syncthreads();
     for (int k = threadIdx.x; k < npl; k += NT) tile[k] = psrc[sb + k];
@@ -168,6 +193,25 @@ __global__ void __launch_bounds__(NT)
   }
 }
 
+template <int NT, int TPT, bool GUARD>
+__global__ void __launch_bounds__(NT)
+    k_bltc_near64(TreeGeom tg, const double* __restrict__ x, const double* __restrict__ y,
+                  const double* __restrict__ z, const double4* __restrict__ psrc, double* __restrict__ out) {
+  bltc_near64_body<NT, TPT, GUARD>(tg, blockIdx.x, blockIdx.y, gridDim.y, x, y, z, psrc, out);
+}
+
+// Batched members (member blockIdx.z): sources psrc + m N, partials out + m splits 3N.
+template <int NT, int TPT, bool GUARD>
+__global__ void __launch_bounds__(NT)
+    k_bltc_near64_batch(const BatchMember* __restrict__ mem, const double* __restrict__ x,
+                        const double* __restrict__ y, const double* __restrict__ z,
+                        const double4* __restrict__ psrc, double* __restrict__ out) {
+  const TreeGeom tg = mem[blockIdx.z].tg;
+  const long mo = blockIdx.z;
+  bltc_near64_body<NT, TPT, GUARD>(tg, blockIdx.x, blockIdx.y, gridDim.y, x, y, z, psrc + mo * tg.N,
+                                   out + mo * gridDim.y * 3 * tg.N);
+}
+
 // Mixed precision: target and source particles relative to their leaves'
 // centres (scaled by kPackScale), float32 pairs, per-source-leaf float32
 // sums added into float64.  Sources are staged two at a time, transposed as
@@ -176,12 +220,13 @@ __global__ void __launch_bounds__(NT)
 // (FADD2 / FFMA2 / FMUL2) evaluate two pairs per instruction; a missing
 // partner of an odd source count has zero strength (pair32x2).
 template <int NT, int TPT, bool GUARD>
-__global__ void __launch_bounds__(NT)
-    k_bltc_near32(TreeGeom tg, StepGeom fg, const double* __restrict__ x, const double* __restrict__ y,
-                  const double* __restrict__ z, const float4* __restrict__ psrcf, double* __restrict__ out) {
-  double* v = out + (long)blockIdx.y * 3 * tg.N;  // partial sums of this source split
+__device__ __forceinline__ void bltc_near32_body(const TreeGeom& tg, const StepGeom& fg, int f, int split,
+                                                 int nsplit, const double* __restrict__ x,
+                                                 const double* __restrict__ y, const double* __restrict__ z,
+                                                 const float4* __restrict__ psrcf, double* __restrict__ out) {
+  double* v = out + (long)split * 3 * tg.N;  // partial sums of this source split
   extern __shared__ float4 tilef[];  // [(npl+1)/2][2]
-  const int npl = tg.npl, npl2 = (npl + 1) >> 1, f = blockIdx.x;
+  const int npl = tg.npl, npl2 = (npl + 1) >> 1;
   const double* ct = fg.pd_centre + 4 * (long)(fg.offset + f);
   const double cx = ct[0], cy = ct[1], cz = ct[2];
   // target positions are re-read for the final cross product, so only their
@@ -199,7 +244,7 @@ __global__ void __launch_bounds__(NT)
   }
   const float feps = (float)tg.eps;
   const float2 eps2 = make_float2(feps, feps);
-  for (int e = tg.near_start[f] + blockIdx.y; e < tg.near_start[f + 1]; e += gridDim.y) {
+  for (int e = tg.near_start[f] + split; e < tg.near_start[f + 1]; e += nsplit) {
     const int sl = tg.near_src[e];
     const long sb = (long)sl * npl;
     const double* cs = fg.pd_centre + 4 * (long)(fg.offset + sl);
@@ -249,14 +294,34 @@ __global__ void __launch_bounds__(NT)
   }
 }
 
+template <int NT, int TPT, bool GUARD>
+__global__ void __launch_bounds__(NT)
+    k_bltc_near32(TreeGeom tg, StepGeom fg, const double* __restrict__ x, const double* __restrict__ y,
+                  const double* __restrict__ z, const float4* __restrict__ psrcf, double* __restrict__ out) {
+  bltc_near32_body<NT, TPT, GUARD>(tg, fg, blockIdx.x, blockIdx.y, gridDim.y, x, y, z, psrcf, out);
+}
+
+template <int NT, int TPT, bool GUARD>
+__global__ void __launch_bounds__(NT)
+    k_bltc_near32_batch(const BatchMember* __restrict__ mem, const double* __restrict__ x,
+                        const double* __restrict__ y, const double* __restrict__ z,
+                        const float4* __restrict__ psrcf, double* __restrict__ out) {
+  const TreeGeom tg = mem[blockIdx.z].tg;
+  const StepGeom fg = mem[blockIdx.z].fg;
+  const long mo = blockIdx.z;
+  bltc_near32_body<NT, TPT, GUARD>(tg, fg, blockIdx.x, blockIdx.y, gridDim.y, x, y, z, psrcf + mo * tg.N,
+                                   out + mo * gridDim.y * 3 * tg.N);
+}
+
 // Leaf proxy targets -> particles: v_i = (near-field splits summed in order)
 // + sum_a lx[k][a] sum_b ly[k][b] T[a][b], with the leaf-box basis of
 // particle k of the (uniform) leaf.
-__global__ void __launch_bounds__(kThreads)
-    k_bltc_to_particles(TreeGeom tg, StepGeom fg, const double* __restrict__ tgt, const double* __restrict__ near,
-                        int splits, double* __restrict__ v) {
+__device__ __forceinline__ void bltc_to_particles_body(const TreeGeom& tg, const StepGeom& fg, int f,
+                                                       const double* __restrict__ tgt,
+                                                       const double* __restrict__ near, int splits,
+                                                       double* __restrict__ v) {
   extern __shared__ double tsh[];  // 3 x qx
-  const int n1 = tg.n + 1, qx = n1 * n1, npl = tg.npl, f = blockIdx.x;
+  const int n1 = tg.n + 1, qx = n1 * n1, npl = tg.npl;
   const long pn = (long)fg.panels * qx;
   const long base = (long)(fg.offset + f) * qx;
   for (int m = threadIdx.x; m < qx; m += blockDim.x) {
@@ -294,6 +359,22 @@ __global__ void __launch_bounds__(kThreads)
     v[tg.N + i] = n1s + u1;
     v[2 * tg.N + i] = n2 + u2;
   }
+}
+
+__global__ void __launch_bounds__(kThreads)
+    k_bltc_to_particles(TreeGeom tg, StepGeom fg, const double* __restrict__ tgt, const double* __restrict__ near,
+                        int splits, double* __restrict__ v) {
+  bltc_to_particles_body(tg, fg, blockIdx.x, tgt, near, splits, v);
+}
+
+__global__ void __launch_bounds__(kThreads)
+    k_bltc_to_particles_batch(const BatchMember* __restrict__ mem, const double* __restrict__ near, int splits,
+                              double* __restrict__ v) {
+  const BatchMember& m = mem[blockIdx.y];
+  const TreeGeom tg = m.tg;
+  const StepGeom fg = m.fg;
+  const long mo = blockIdx.y;
+  bltc_to_particles_body(tg, fg, blockIdx.x, m.ftgt, near + mo * splits * 3 * tg.N, splits, v + mo * 3 * tg.N);
 }
 
 }  // namespace
@@ -338,6 +419,55 @@ void launch_bltc_near(const TreeGeom& tg, const StepGeom& fg, int precision, con
   else if (tg.npl <= 256) SB_NEAR(128, 2);
   else SB_NEAR(256, 2);
 #undef SB_NEAR
+}
+
+void launch_bltc_sources_batch(const BatchMember* mem, int members, int leaves, int npl, int nmax, int stage,
+                               double dt_s, const double* vprev, const double* x, const double* y, const double* z,
+                               const double* vors, const double* area, double4* psrc, float4* psrcf, bool mixed,
+                               cudaStream_t st) {
+  size_t smem = sizeof(double) * ((size_t)npl * (nmax + 1) * 2 + npl);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_bltc_sources_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr = true;
+  }
+  SB_LAUNCH(k_bltc_sources_batch, dim3((unsigned)leaves, (unsigned)members), kThreads, smem, st, mem, stage, dt_s,
+            vprev, x, y, z, vors, area, psrc, mixed ? psrcf : nullptr, mixed ? 1 : 0);
+}
+
+void launch_bltc_near_batch(const BatchMember* mem, int members, int leaves, int npl, double eps, int precision,
+                            const double* x, const double* y, const double* z, const double4* psrc,
+                            const float4* psrcf, double* near, int splits, int nt, int tpt, cudaStream_t st) {
+  const bool guard = !(eps > 0);
+  const dim3 grid((unsigned)leaves, (unsigned)splits, (unsigned)members);
+#define SB_NEARB(NT, TPT)                                                                                         \
+  do {                                                                                                            \
+    if (precision == SBSLPM_MIXED) {                                                                              \
+      const size_t sm32 = sizeof(float4) * 2 * ((npl + 1) / 2);                                                  \
+      if (guard) SB_LAUNCH((k_bltc_near32_batch<NT, TPT, true>), grid, NT, sm32, st, mem, x, y, z, psrcf, near);  \
+      else SB_LAUNCH((k_bltc_near32_batch<NT, TPT, false>), grid, NT, sm32, st, mem, x, y, z, psrcf, near);       \
+    } else {                                                                                                      \
+      const size_t sm64 = sizeof(double4) * npl;                                                                 \
+      if (guard) SB_LAUNCH((k_bltc_near64_batch<NT, TPT, true>), grid, NT, sm64, st, mem, x, y, z, psrc, near);   \
+      else SB_LAUNCH((k_bltc_near64_batch<NT, TPT, false>), grid, NT, sm64, st, mem, x, y, z, psrc, near);        \
+    }                                                                                                             \
+  } while (0)
+  // tile shapes the autotuner chooses from (NT threads x TPT targets per thread >= npl)
+  if (nt == 64 && tpt == 4) SB_NEARB(64, 4);
+  else if (nt == 128 && tpt == 2) SB_NEARB(128, 2);
+  else if (nt == 256 && tpt == 1) SB_NEARB(256, 1);
+  else if (nt == 64 && tpt == 2) SB_NEARB(64, 2);
+  else if (nt == 64 && tpt == 1) SB_NEARB(64, 1);
+  else if (nt == 256 && tpt == 2) SB_NEARB(256, 2);
+  else if (nt == 128 && tpt == 1) SB_NEARB(128, 1);
+#undef SB_NEARB
+}
+
+void launch_bltc_to_particles_batch(const BatchMember* mem, int members, int leaves, int nmax, const double* near,
+                                    int splits, double* v, cudaStream_t st) {
+  const int qx = (nmax + 1) * (nmax + 1);
+  SB_LAUNCH(k_bltc_to_particles_batch, dim3((unsigned)leaves, (unsigned)members), kThreads,
+            sizeof(double) * 3 * qx, st, mem, near, splits, v);
 }
 
 void launch_bltc_to_particles(const TreeGeom& tg, const StepGeom& fg, const double* tgt, const double* near,

@@ -112,13 +112,14 @@ __global__ void k_copy_strength(StepGeom g, const double4* __restrict__ src, dou
 // Mode 2 (treecode): leaf strengths already anterpolated into src, fixed
 // proxy positions untouched, mixed packing as in mode 0.
 
-__global__ void k_upward_subtree(StepGeom g, int r, int D, int mode, int stage, double dt_s,
-                                 const double* __restrict__ vprev, const double* __restrict__ x,
-                                 const double* __restrict__ y, const double* __restrict__ z,
-                                 const double* __restrict__ vors, const double* __restrict__ area,
-                                 double4* __restrict__ src, int mixed) {
+__device__ __forceinline__ void upward_subtree_body(const StepGeom& g, int root_rel, int r, int D, int mode,
+                                                    int stage, double dt_s, const double* __restrict__ vprev,
+                                                    const double* __restrict__ x, const double* __restrict__ y,
+                                                    const double* __restrict__ z, const double* __restrict__ vors,
+                                                    const double* __restrict__ area, double4* __restrict__ src,
+                                                    int mixed) {
   extern __shared__ double sh[];  // strengths of levels r..r+D (level k at q*(4^k-1)/3), then scratch
-  const int q = g.q, root_rel = blockIdx.x, n1 = g.degree + 1;
+  const int q = g.q, n1 = g.degree + 1;
   const bool leaves_here = (r + D == g.levels - 1);
   const long ln = (long)g.leaves * g.q, pn = (long)g.panels * g.q;
   auto lvl = [&](int k) { return sh + q * (((1 << (2 * k)) - 1) / 3); };
@@ -215,14 +216,29 @@ __global__ void k_upward_subtree(StepGeom g, int r, int D, int mode, int stage, 
   }
 }
 
+__global__ void k_upward_subtree(StepGeom g, int r, int D, int mode, int stage, double dt_s,
+                                 const double* __restrict__ vprev, const double* __restrict__ x,
+                                 const double* __restrict__ y, const double* __restrict__ z,
+                                 const double* __restrict__ vors, const double* __restrict__ area,
+                                 double4* __restrict__ src, int mixed) {
+  upward_subtree_body(g, blockIdx.x, r, D, mode, stage, dt_s, vprev, x, y, z, vors, area, src, mixed);
+}
+
+// Batched treecode members (mode 2): member blockIdx.z.
+__global__ void k_upward_subtree_batch(const BatchMember* __restrict__ mem, int r, int D, int mixed) {
+  const StepGeom g = mem[blockIdx.z].fg;
+  upward_subtree_body(g, blockIdx.x, r, D, 2, 0, 0.0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                      mem[blockIdx.z].fsrc, mixed);
+}
+
 // Downward: the root's targets are final; children of levels r+1..r+D get
 // own + interpolated parent values.  Leaves go to leaf_out when given (the
 // stage velocity), intermediate levels stay in shared memory, and the
 // deepest non-leaf level is written back for the next launch.
-__global__ void k_downward_subtree(StepGeom g, int r, int D, double* __restrict__ tgt,
-                                   double* __restrict__ leaf_out) {
+__device__ __forceinline__ void downward_subtree_body(const StepGeom& g, int root_rel, int r, int D,
+                                                      double* __restrict__ tgt, double* __restrict__ leaf_out) {
   extern __shared__ double sh[];  // 3 fields x levels r..r+D, then 3 x 4^D q scratch
-  const int q = g.q, root_rel = blockIdx.x, n1 = g.degree + 1;
+  const int q = g.q, n1 = g.degree + 1;
   const long pn = (long)g.panels * g.q, ln = (long)g.leaves * g.q;
   const int per_field = q * (((1 << (2 * (D + 1))) - 1) / 3);
   auto lvl = [&](int f, int k) { return sh + f * per_field + q * (((1 << (2 * k)) - 1) / 3); };
@@ -286,6 +302,16 @@ __global__ void k_downward_subtree(StepGeom g, int r, int D, double* __restrict_
     }
     __syncthreads();
   }
+}
+
+__global__ void k_downward_subtree(StepGeom g, int r, int D, double* __restrict__ tgt,
+                                   double* __restrict__ leaf_out) {
+  downward_subtree_body(g, blockIdx.x, r, D, tgt, leaf_out);
+}
+
+__global__ void k_downward_subtree_batch(const BatchMember* __restrict__ mem, int r, int D) {
+  const StepGeom g = mem[blockIdx.z].fg;
+  downward_subtree_body(g, blockIdx.x, r, D, mem[blockIdx.z].ftgt, nullptr);
 }
 
 // ---------------------------------------------------------------------------
@@ -596,22 +622,21 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_interact32(StepGeom g, 
 // (deterministic).  MIXED: float32 pairs on packed sources (kPackScale),
 // per-source-panel float32 sums added into float64.
 template <int Q, bool ALL_LEAVES, bool GUARD, bool MIXED>
-__global__ void __launch_bounds__(128) k_interact_wide(StepGeom g, const double4* __restrict__ src,
-                                                       const float4* __restrict__ srcf, double* __restrict__ out,
-                                                       long out_stride) {
+__device__ __forceinline__ void interact_wide_body(const StepGeom& g, int tix, int gy, int ngy,
+                                                   const double4* __restrict__ src, const float4* __restrict__ srcf,
+                                                   double* __restrict__ out, long out_stride) {
   constexpr int TPL = (Q + 31) / 32, NW = 4, Q2 = (Q + 1) / 2;
   using Src = typename std::conditional<MIXED, float4, double4>::type;
   // MIXED: sources staged two at a time, transposed, (x0,x1,y0,y1),(z0,z1,w0,w1)
   __shared__ Src stage[NW][MIXED ? 2 * Q2 : Q];
   __shared__ double red[NW][3][Q];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int tix = blockIdx.x;
-  const int t = (ALL_LEAVES ? g.offset : 0) + tix;
+    const int t = (ALL_LEAVES ? g.offset : 0) + tix;
   const long pn = (long)g.panels * g.q;
   int e0, e1;
   if (ALL_LEAVES) {
-    int per = (g.leaves + gridDim.y - 1) / gridDim.y;
-    e0 = blockIdx.y * per;
+    int per = (g.leaves + ngy - 1) / ngy;
+    e0 = gy * per;
     e1 = min(g.leaves, e0 + per);
   } else {
     e0 = g.tgt_start[t];
@@ -707,12 +732,28 @@ __global__ void __launch_bounds__(128) k_interact_wide(StepGeom g, const double4
     }
     long o = (long)t * Q + j;
     const double px = g.px[o], py = g.px[pn + o], pz = g.px[2 * pn + o];
-    long oo = ALL_LEAVES ? (long)blockIdx.y * 3 * out_stride + (long)tix * Q + j : o;
+    long oo = ALL_LEAVES ? (long)gy * 3 * out_stride + (long)tix * Q + j : o;
     long st = ALL_LEAVES ? out_stride : pn;
     out[oo] = cb * (py * sz - pz * sy);
     out[st + oo] = cb * (pz * sx - px * sz);
     out[2 * st + oo] = cb * (px * sy - py * sx);
   }
+}
+
+template <int Q, bool ALL_LEAVES, bool GUARD, bool MIXED>
+__global__ void __launch_bounds__(128) k_interact_wide(StepGeom g, const double4* __restrict__ src,
+                                                       const float4* __restrict__ srcf, double* __restrict__ out,
+                                                       long out_stride) {
+  interact_wide_body<Q, ALL_LEAVES, GUARD, MIXED>(g, blockIdx.x, blockIdx.y, gridDim.y, src, srcf, out, out_stride);
+}
+
+// Batched treecode members with q = Q: member idx[blockIdx.z], well-separated pairs.
+template <int Q, bool GUARD, bool MIXED>
+__global__ void __launch_bounds__(128) k_interact_wide_batch(const BatchMember* __restrict__ mem,
+                                                             const int* __restrict__ idx) {
+  const BatchMember& m = mem[idx[blockIdx.z]];
+  const StepGeom g = m.fg;
+  interact_wide_body<Q, false, GUARD, MIXED>(g, blockIdx.x, 0, 1, m.fsrc, g.srcf, m.ftgt, 0);
 }
 
 // Sum of per-group partials (group gi at partial + gi * gstride) in group order.
@@ -785,15 +826,15 @@ __device__ __forceinline__ void gather3(const Basis<D>& b, const double* __restr
 }
 
 template <int D>
-__global__ void k_depart_remap(StepGeom g, BliTable tab, const double* __restrict__ x, const double* __restrict__ y,
-                               const double* __restrict__ z, const double* __restrict__ v0,
-                               const double* __restrict__ v1, const double* __restrict__ v2,
-                               const double* __restrict__ v3, double dt, double* __restrict__ dep,
-                               const double* __restrict__ vors, const double* __restrict__ tracers, int T,
-                               double* __restrict__ new_vors, double* __restrict__ new_tracers, int mode) {
+__device__ __forceinline__ void depart_remap_body(const StepGeom& g, const BliTable& tab, long o,
+                                                  const double* __restrict__ x, const double* __restrict__ y,
+                                                  const double* __restrict__ z, const double* __restrict__ v0,
+                                                  const double* __restrict__ v1, const double* __restrict__ v2,
+                                                  const double* __restrict__ v3, double dt, double* __restrict__ dep,
+                                                  const double* __restrict__ vors, const double* __restrict__ tracers,
+                                                  int T, double* __restrict__ new_vors,
+                                                  double* __restrict__ new_tracers, int mode) {
   const long n = (long)g.leaves * g.q;
-  const long o = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (o >= n) return;
   unsigned err = 0;
   Basis<D> b;
   double dx, dy, dz;
@@ -844,6 +885,34 @@ __global__ void k_depart_remap(StepGeom g, BliTable tab, const double* __restric
     new_vors[o] = vor - 2 * g.omega * z[o];
   }
   flag(g.err, err);
+}
+
+template <int D>
+__global__ void k_depart_remap(StepGeom g, BliTable tab, const double* __restrict__ x, const double* __restrict__ y,
+                               const double* __restrict__ z, const double* __restrict__ v0,
+                               const double* __restrict__ v1, const double* __restrict__ v2,
+                               const double* __restrict__ v3, double dt, double* __restrict__ dep,
+                               const double* __restrict__ vors, const double* __restrict__ tracers, int T,
+                               double* __restrict__ new_vors, double* __restrict__ new_tracers, int mode) {
+  const long o = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (o >= (long)g.leaves * g.q) return;
+  depart_remap_body<D>(g, tab, o, x, y, z, v0, v1, v2, v3, dt, dep, vors, tracers, T, new_vors, new_tracers, mode);
+}
+
+// Batched members on one particle grid (member blockIdx.y): departure and
+// remap in one pass (mode 3), stage velocities v_k + m * 3n, vorticity + m * n.
+template <int D>
+__global__ void k_depart_remap_batch(StepGeom g, BliTable tab, const double* __restrict__ x,
+                                     const double* __restrict__ y, const double* __restrict__ z,
+                                     const double* __restrict__ v0, const double* __restrict__ v1,
+                                     const double* __restrict__ v2, const double* __restrict__ v3, double dt,
+                                     const double* __restrict__ vors, double* __restrict__ new_vors) {
+  const long n = (long)g.leaves * g.q;
+  const long o = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (o >= n) return;
+  const long m = blockIdx.y, vo = m * 3 * n, so = m * n;
+  depart_remap_body<D>(g, tab, o, x, y, z, v0 + vo, v1 + vo, v2 + vo, v3 + vo, dt, nullptr, vors + so, nullptr, 0,
+                       new_vors + so, nullptr, 3);
 }
 
 // ---------------------------------------------------------------------------
@@ -1018,6 +1087,60 @@ void launch_upward_fused(const StepGeom& g, int mode, int stage, double dt_s, co
   }
 }
 
+void launch_upward_batch(const BatchMember* mem, int members, int levels, int qmax, bool mixed, cudaStream_t st) {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_upward_subtree_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, 164 * 1024);
+    attr = true;
+  }
+  const int Dmax = subtree_depth(qmax);
+  int r = levels - 1;
+  do {
+    const int D = r < Dmax ? r : Dmax;
+    const int root = r - D;
+    SB_LAUNCH(k_upward_subtree_batch, dim3((unsigned)(6 << (2 * root)), 1, (unsigned)members), 256,
+              subtree_smem(qmax, 1, D), st, mem, root, D, mixed ? 1 : 0);
+    r = root;
+  } while (r > 0);
+}
+
+void launch_downward_batch(const BatchMember* mem, int members, int levels, int qmax, cudaStream_t st) {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_downward_subtree_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, 164 * 1024);
+    attr = true;
+  }
+  const int Dmax = subtree_depth(qmax);
+  int r = 0;
+  while (r < levels - 1) {
+    const int D = (levels - 1 - r) < Dmax ? (levels - 1 - r) : Dmax;
+    SB_LAUNCH(k_downward_subtree_batch, dim3((unsigned)(6 << (2 * r)), 1, (unsigned)members), 256,
+              subtree_smem(qmax, 3, D), st, mem, r, D);
+    r += D;
+  }
+}
+
+void launch_cc_batch(const BatchMember* mem, const int* idx, int count, int q, int tree_panels, double eps,
+                     int precision, cudaStream_t st) {
+  if (count <= 0) return;
+  const dim3 grid((unsigned)tree_panels, 1, (unsigned)count);
+  const bool mixed = precision == SBSLPM_MIXED, guard = !(eps > 0);
+#define SB_CCB(Q)                                                                                              \
+  case Q:                                                                                                      \
+    if (mixed) {                                                                                               \
+      if (guard) SB_LAUNCH((k_interact_wide_batch<Q, true, true>), grid, 128, 0, st, mem, idx);                \
+      else SB_LAUNCH((k_interact_wide_batch<Q, false, true>), grid, 128, 0, st, mem, idx);                     \
+    } else {                                                                                                   \
+      if (guard) SB_LAUNCH((k_interact_wide_batch<Q, true, false>), grid, 128, 0, st, mem, idx);               \
+      else SB_LAUNCH((k_interact_wide_batch<Q, false, false>), grid, 128, 0, st, mem, idx);                    \
+    }                                                                                                          \
+    break;
+  switch (q) {
+    SB_CCB(36) SB_CCB(49) SB_CCB(64) SB_CCB(81) SB_CCB(100) SB_CCB(121)
+  }
+#undef SB_CCB
+}
+
 void launch_downward_fused(const StepGeom& g, double* tgt, double* leaf_out, cudaStream_t st) {
   static bool attr = false;
   if (!attr) {
@@ -1160,6 +1283,22 @@ void launch_depart_remap(const StepGeom& g, const BliTable* tab, const double* x
     SB_DR(0) SB_DR(1) SB_DR(2) SB_DR(3) SB_DR(4) SB_DR(5) SB_DR(6) SB_DR(7) SB_DR(8) SB_DR(9) SB_DR(10)
   }
 #undef SB_DR
+}
+
+void launch_depart_remap_batch(const StepGeom& g, const BliTable* tab, int members, const double* x,
+                               const double* y, const double* z, const double* v0, const double* v1,
+                               const double* v2, const double* v3, double dt, const double* vors, double* new_vors,
+                               cudaStream_t st) {
+  const long n = (long)g.leaves * g.q;
+  const dim3 grid(blocks_for(n, 128), (unsigned)members);
+#define SB_DRB(D)                                                                                               \
+  case D:                                                                                                       \
+    SB_LAUNCH(k_depart_remap_batch<D>, grid, 128, 0, st, g, *tab, x, y, z, v0, v1, v2, v3, dt, vors, new_vors); \
+    break;
+  switch (g.degree) {
+    SB_DRB(0) SB_DRB(1) SB_DRB(2) SB_DRB(3) SB_DRB(4) SB_DRB(5) SB_DRB(6) SB_DRB(7) SB_DRB(8) SB_DRB(9) SB_DRB(10)
+  }
+#undef SB_DRB
 }
 
 int direct_groups(long nt, long ns) {

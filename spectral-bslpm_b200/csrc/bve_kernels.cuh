@@ -50,6 +50,19 @@ struct TreeGeom {
   const int* near_src;    // source leaf (relative to the first leaf)
 };
 
+// One member of a batched ensemble (treecode velocity, shared particle grid):
+// its tree and well-separated list (fg, with fg.srcf its packed proxy
+// sources), its near lists and leaf bases (tg), its degree's BLI table, and
+// its proxy source / target buffers.  Per-particle buffers of the batch are
+// [member][...] with a uniform stride.
+struct BatchMember {
+  StepGeom fg;
+  TreeGeom tg;
+  BliTable tab;
+  double4* fsrc;  // [tree panels * q] proxy sources
+  double* ftgt;   // [3][tree panels * q] proxy targets
+};
+
 // Launch wrappers (stream-ordered).
 void launch_leaf_sources(const StepGeom& g, int stage, double dt_s, const double* vprev, const double* x,
                          const double* y, const double* z, const double* vors, const double* area, double4* src,
@@ -101,6 +114,28 @@ void launch_bltc_near(const TreeGeom& tg, const StepGeom& fg, int precision, con
 // v = near splits summed + far field interpolated from the leaf proxies
 void launch_bltc_to_particles(const TreeGeom& tg, const StepGeom& fg, const double* tgt, const double* near,
                               int splits, double* v, cudaStream_t st);
+
+// Batched treecode (members on one particle grid; one launch per phase over
+// all members, the cc launch once per proxy degree).  mem: device array of
+// members; per-particle arrays are [member][...]; nmax = largest proxy degree.
+void launch_bltc_sources_batch(const BatchMember* mem, int members, int leaves, int npl, int nmax, int stage,
+                               double dt_s, const double* vprev, const double* x, const double* y, const double* z,
+                               const double* vors, const double* area, double4* psrc, float4* psrcf, bool mixed,
+                               cudaStream_t st);
+void launch_upward_batch(const BatchMember* mem, int members, int levels, int qmax, bool mixed, cudaStream_t st);
+// idx: device array of the member indices whose proxies number q
+void launch_cc_batch(const BatchMember* mem, const int* idx, int count, int q, int tree_panels, double eps,
+                     int precision, cudaStream_t st);
+void launch_downward_batch(const BatchMember* mem, int members, int levels, int qmax, cudaStream_t st);
+void launch_bltc_near_batch(const BatchMember* mem, int members, int leaves, int npl, double eps, int precision,
+                            const double* x, const double* y, const double* z, const double4* psrc,
+                            const float4* psrcf, double* near, int splits, int nt, int tpt, cudaStream_t st);
+void launch_bltc_to_particles_batch(const BatchMember* mem, int members, int leaves, int nmax, const double* near,
+                                    int splits, double* v, cudaStream_t st);
+void launch_depart_remap_batch(const StepGeom& g, const BliTable* tab, int members, const double* x,
+                               const double* y, const double* z, const double* v0, const double* v1,
+                               const double* v2, const double* v3, double dt, const double* vors, double* new_vors,
+                               cudaStream_t st);
 
 // Counts every kernel launched through the wrappers above.
 long& launch_counter();

@@ -48,37 +48,13 @@ sbslpm_status validate(const sbslpm_config& c) {
   return SBSLPM_OK;
 }
 
-// One-dimensional BLI basis of the parent's degree-d nodes at the nodes of a
-// child in the upper (h = 0) or lower (h = 1) half of the parent, computed on
-// face 0 as child_to_parent places the child nodes
-// (src/fmm_funcs_impl.hpp:53-64).  out: [2][d+1][d+1].
-void child_basis_1d(const std::vector<sbslpm_panel>& P, const BliTable& tab, int d, std::vector<double>& out,
-                    unsigned& err) {
-  const int n1 = d + 1;
-  out.assign((size_t)2 * n1 * n1, 0.0);
-  const sbslpm_panel& par = P[0];
-  const double lo = par.min_xi * kPi / 4.0, hi = par.max_xi * kPi / 4.0;
-  for (int h = 0; h < 2; h++) {
-    const sbslpm_panel& ch = P[child_of(par, h == 0 ? 0 : 2)];  // child 0: upper half; child 2: lower half
-    const double xo = kPi / 4.0 * 0.5 * (ch.min_xi + ch.max_xi), xs = kPi / 4.0 * 0.5 * (ch.max_xi - ch.min_xi);
-    for (int i = 0; i < n1; i++) {
-      double node = d == 0 ? 0.0 : std::cos(kPi / d * i);
-      if (std::fabs(node) < 1e-16) node = 0;
-      bli_1d(node * xs + xo, lo, hi, d, tab.cosv, tab.w, &out[((size_t)h * n1 + i) * n1], err);
-    }
-  }
-}
-
 // Host precomputation of everything that does not change during a run.
 sbslpm_status precompute(sbslpm_ctx* c) {
   const int q = c->q, P = c->P, off = c->off, d = c->d;
   std::vector<double> interp;
   build_interp(d, false, interp);
 
-  for (int i = 0; i <= d; i++) {
-    c->tab.cosv[i] = d == 0 ? 0.0 : std::cos(kPi * i / d);
-    c->tab.w[i] = d == 0 ? 1.0 : (i == 0 ? 0.5 : (i == d ? 0.5 * std::pow(-1, i) : std::pow(-1, i)));
-  }
+  bli_table(d, c->tab);
   if (c->tree) return SBSLPM_OK;  // the treecode has its own set-up
 
   // proxy positions, exactly as the reference's interaction kernel places them
@@ -156,111 +132,37 @@ sbslpm_status precompute(sbslpm_ctx* c) {
 // leaf_size particles, degree-n proxies on every tree panel, the canonical
 // leaf-box basis of the particle grid, and the near / well-separated lists.
 sbslpm_status precompute_tree(sbslpm_ctx* c) {
-  const int qp = c->q, n = c->cfg.proxy_degree, n1 = n + 1;
-  int m = 0;
-  long npl = qp;
-  while (npl * 4 <= c->cfg.leaf_size && m < c->L - 1) {
-    npl *= 4;
-    m++;
-  }
+  const int qp = c->q;
+  TreeTables t;
+  SB_TRY(build_tree_tables(c->L, c->d, c->panels, c->cfg.leaf_size, c->cfg.proxy_degree, t));
   c->tree = true;
-  c->n = n;
-  c->qx = n1 * n1;
-  c->npl = (int)npl;
-  c->Lf = c->L - m;
-  c->Pf = sbslpm_panel_count(c->Lf);
-  c->Af = sbslpm_leaf_count(c->Lf);
-  build_panels(c->Lf, c->fpanels);
-  const int Pf = c->Pf, Af = c->Af, offf = Pf - Af, qx = c->qx;
-  std::vector<double> interp_n;
-  build_interp(n, false, interp_n);
+  c->n = t.n;
+  c->qx = t.qx;
+  c->npl = t.npl;
+  c->Lf = t.Lf;
+  c->Pf = t.Pf;
+  c->Af = t.Af;
+  c->fpanels = t.fpanels;
+  c->ftab = t.ftab;
+  const size_t pn = (size_t)t.Pf * t.qx;
+  const std::vector<double>& fpx = t.fpx;
+  SB_TRY(upload(&c->fpx, t.fpx));
+  SB_TRY(upload(&c->fcentre, t.centre));
+  SB_TRY(upload(&c->fbounds, t.bounds));
+  SB_TRY(upload(&c->fface, t.face));
+  if (!t.c1d.empty()) SB_TRY(upload(&c->fchild, t.c1d));
+  SB_TRY(upload(&c->flx, t.lx));
+  SB_TRY(upload(&c->fly, t.ly));
 
-  std::vector<double> fpx((size_t)3 * Pf * qx), centre((size_t)4 * Pf, 0.0), bounds((size_t)4 * Pf);
-  std::vector<int> face(Pf);
-  const size_t pn = (size_t)Pf * qx;
-  for (int p = 0; p < Pf; p++) {
-    const sbslpm_panel& pp = c->fpanels[p];
-    for (int j = 0; j < qx; j++) {
-      double xyz[3];
-      proxy_point(pp, interp_n.data(), j, xyz);
-      for (int k = 0; k < 3; k++) fpx[k * pn + (size_t)p * qx + j] = xyz[k];
-    }
-    double xyz[3];
-    xyz_from_xieta(kPi / 4.0 * 0.5 * (pp.min_xi + pp.max_xi), kPi / 4.0 * 0.5 * (pp.min_eta + pp.max_eta), pp.face,
-                   xyz);
-    for (int k = 0; k < 3; k++) centre[4 * (size_t)p + k] = xyz[k];
-    bounds[4 * p + 0] = kPi / 4.0 * pp.min_xi;
-    bounds[4 * p + 1] = kPi / 4.0 * pp.max_xi;
-    bounds[4 * p + 2] = kPi / 4.0 * pp.min_eta;
-    bounds[4 * p + 3] = kPi / 4.0 * pp.max_eta;
-    face[p] = pp.face;
-  }
-  SB_TRY(upload(&c->fpx, fpx));
-  SB_TRY(upload(&c->fcentre, centre));
-  SB_TRY(upload(&c->fbounds, bounds));
-  SB_TRY(upload(&c->fface, face));
-
-  for (int i = 0; i <= n; i++) {
-    c->ftab.cosv[i] = n == 0 ? 0.0 : std::cos(kPi * i / n);
-    c->ftab.w[i] = n == 0 ? 1.0 : (i == 0 ? 0.5 : (i == n ? 0.5 * std::pow(-1, i) : std::pow(-1, i)));
-  }
-  unsigned err = 0;
-  if (c->Lf > 1) {
-    std::vector<double> c1d;
-    child_basis_1d(c->fpanels, c->ftab, n, c1d, err);
-    SB_TRY(upload(&c->fchild, c1d));
-  }
-
-  // leaf-box basis of the particles of the first tree leaf (the same for every leaf)
-  {
-    std::vector<double> interp_p;
-    build_interp(c->d, false, interp_p);
-    std::vector<double> lx((size_t)npl * n1), ly((size_t)npl * n1);
-    const sbslpm_panel& leaf = c->fpanels[offf];
-    const double lo_x = kPi / 4.0 * leaf.min_xi, hi_x = kPi / 4.0 * leaf.max_xi;
-    const double lo_e = kPi / 4.0 * leaf.min_eta, hi_e = kPi / 4.0 * leaf.max_eta;
-    const int first_dp = level_start(c->L - 1);  // the first leaf's descendants come first
-    for (long k = 0; k < npl; k++) {
-      const sbslpm_panel& dp = c->panels[first_dp + k / qp];
-      const int j = (int)(k % qp);
-      double max_xi = kPi / 4.0 * dp.max_xi, min_xi = kPi / 4.0 * dp.min_xi;
-      double max_eta = kPi / 4.0 * dp.max_eta, min_eta = kPi / 4.0 * dp.min_eta;
-      double xi = 0.5 * (max_xi + min_xi) + 0.5 * (max_xi - min_xi) * interp_p[4 * j];
-      double eta = 0.5 * (max_eta + min_eta) + 0.5 * (max_eta - min_eta) * interp_p[4 * j + 1];
-      bli_1d(xi, lo_x, hi_x, n, c->ftab.cosv, c->ftab.w, &lx[k * n1], err);
-      bli_1d(eta, lo_e, hi_e, n, c->ftab.cosv, c->ftab.w, &ly[k * n1], err);
-    }
-    SB_TRY(upload(&c->flx, lx));
-    SB_TRY(upload(&c->fly, ly));
-  }
-  if (err) {
-    set_last_error("treecode set-up: a particle fell outside its leaf");
-    return SBSLPM_ERR_OUT_OF_PANEL;
-  }
-
-  // near leaf pairs (particle x particle) and well-separated pairs (proxy x proxy)
-  std::vector<sbslpm_interact_pair> list;
-  std::vector<char> near;
-  build_interactions_flagged(c->Lf, c->fpanels, c->cfg.fmm_theta, list, near);
-  std::vector<int> ns(Af + 1, 0), cs(Pf + 1, 0);
-  for (size_t e = 0; e < list.size(); e++) {
-    if (near[e]) ns[list[e].target_panel - offf + 1]++;
-    else cs[list[e].target_panel + 1]++;
-  }
-  for (int i = 0; i < Af; i++) ns[i + 1] += ns[i];
-  for (int i = 0; i < Pf; i++) cs[i + 1] += cs[i];
-  std::vector<int> nsrc(ns[Af]), csrc(cs[Pf]), nf(ns.begin(), ns.end() - 1), cf(cs.begin(), cs.end() - 1);
-  for (size_t e = 0; e < list.size(); e++) {
-    if (near[e]) nsrc[nf[list[e].target_panel - offf]++] = list[e].source_panel - offf;
-    else csrc[cf[list[e].target_panel]++] = list[e].source_panel;
-  }
-  c->n_near = ns[Af];
-  c->n_cc = cs[Pf];
-  c->list = list;
-  SB_TRY(upload(&c->near_start, ns));
-  SB_TRY(upload(&c->near_src, nsrc));
-  SB_TRY(upload(&c->cc_start, cs));
-  SB_TRY(upload(&c->cc_src, csrc));
+  TreeLists l;
+  build_tree_lists(t, c->cfg.fmm_theta, l);
+  c->n_near = l.ns.back();
+  c->n_cc = l.cs.back();
+  c->list = l.list;
+  SB_TRY(upload(&c->near_start, l.ns));
+  SB_TRY(upload(&c->near_src, l.nsrc));
+  SB_TRY(upload(&c->cc_start, l.cs));
+  SB_TRY(upload(&c->cc_src, l.csrc));
 
   // workspace; proxy positions are fixed, strengths are written every stage
   const size_t N = (size_t)c->A * qp;

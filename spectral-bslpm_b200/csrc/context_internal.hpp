@@ -115,6 +115,25 @@ sbslpm_status finish(sbslpm_ctx* c);
 void velocity_eval(sbslpm_ctx* c, int stage, double dt_s, const double* vprev, const double* x, const double* y,
                    const double* z, const double* area, const double* vors, double* v);
 void launch_add3(const double* t, long n, double* a, double* b, double* cc, cudaStream_t st);
+
+// tree_setup.cu: host tables of the decoupled-degree treecode.
+struct TreeTables {
+  int Lf = 0, Pf = 0, Af = 0, npl = 0, n = 0, qx = 0;
+  std::vector<sbslpm_panel> fpanels;
+  std::vector<double> fpx, centre, bounds, c1d, lx, ly;
+  std::vector<int> face;
+  BliTable ftab{};
+};
+struct TreeLists {
+  std::vector<int> ns, nsrc, cs, csrc;
+  std::vector<sbslpm_interact_pair> list;
+};
+void child_basis_1d(const std::vector<sbslpm_panel>& P, const BliTable& tab, int d, std::vector<double>& out,
+                    unsigned& err);
+void bli_table(int n, BliTable& t);
+sbslpm_status build_tree_tables(int L, int d, const std::vector<sbslpm_panel>& grid, int leaf_size, int n,
+                                TreeTables& t);
+void build_tree_lists(const TreeTables& t, double theta, TreeLists& l);
 sbslpm_status capture_graph(sbslpm_ctx* c, cudaGraphExec_t* graph, const std::function<void()>& body);
 
 }  // namespace sbslpm

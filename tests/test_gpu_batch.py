@@ -1,0 +1,117 @@
+"""GPU tests of the batched ensemble (sbslpm_batch): members with uneven trees
+(different theta and proxy degree) stepped in one launch per phase must give
+exactly what single contexts give member by member, and stay within the
+accuracy bar against the float64 direct sum.
+
+Tolerances: bit-exact against single contexts with the same near-field split
+count (the arithmetic per target is the same; only the split count changes
+the order of the near-field partial sums), <= 1e-12 with the autotuned
+split, mixed precision <= 1e-6 relative L-infinity vorticity against the
+float64 direct sum after one step.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+LEVELS, DEGREE, EPS, OMEGA, DT = 5, 3, 1e-4, 2 * np.pi, 0.005
+THETA = [0.5, 0.8, 0.65, 0.7]
+PDEG = [6, 8, 10, 8]
+
+
+def rel(a, b):
+    s = b.abs().max().item()
+    return (a - b).abs().max().item() / (s if s > 0 else 1.0)
+
+
+def grid_and_vors(sb, members):
+    g = sb.build_grid(LEVELS, DEGREE, exact_cc=True)
+    lat, lon = np.arcsin(np.clip(g.z, -1, 1)), np.arctan2(g.y, g.x)
+    base = 2 * 0.5 * np.sin(lat) - 0.5 * np.sin(lat) * np.cos(lat) ** 4 * 30 * np.cos(4 * lon)
+    vors = []
+    for m in range(members):
+        pert = 1e-3 * np.random.default_rng(m).standard_normal(3) @ np.stack([g.x, g.y, g.z]).reshape(3, -1)
+        vors.append(base + pert.reshape(base.shape))
+    vors = np.stack(vors)
+    vors -= (vors * g.area).sum(axis=(1, 2), keepdims=True) / (4 * np.pi)
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    return g, [T(g.x), T(g.y), T(g.z), T(g.area)], T(vors)
+
+
+def base_cfg(sb, precision, **kw):
+    return sb.config_default(levels=LEVELS, interp_degree=DEGREE, kernel_eps=EPS, omega=OMEGA, dt=DT,
+                             precision=precision, leaf_size=256, **kw)
+
+
+def single_step(sb, precision, theta, pdeg, xyza, vor):
+    ctx = sb.Context(base_cfg(sb, precision, fmm_theta=theta, proxy_degree=pdeg))
+    v = vor.clone()
+    vel = [torch.zeros_like(v) for _ in range(3)]
+    ctx.bve_back_rk4_step(*xyza, v, *vel)
+    return v, torch.stack(vel)
+
+
+@pytest.mark.parametrize("precision", ["FP64", "MIXED"])
+def test_batch_equals_single_contexts(sb, precision):
+    prec = getattr(sb, precision)
+    g, xyza, vors = grid_and_vors(sb, len(THETA))
+    batch = sb.Batch(base_cfg(sb, prec), THETA, PDEG)
+    batch.set_tuning(128, 2, 2)  # the single context's near-field shape and split count
+    v = vors.clone()
+    vel = torch.zeros((len(THETA), 3) + v.shape[1:], dtype=torch.float64, device="cuda")
+    batch.step(*xyza, v, vel)
+    for m in range(len(THETA)):
+        sv, svel = single_step(sb, prec, THETA[m], PDEG[m], xyza, vors[m].contiguous())
+        assert torch.equal(v[m], sv), m
+        assert torch.equal(vel[m], svel), m
+
+
+def test_batch_autotuned_close_to_single(sb):
+    g, xyza, vors = grid_and_vors(sb, len(THETA))
+    batch = sb.Batch(base_cfg(sb, sb.FP64), THETA, PDEG)
+    v = vors.clone()
+    vel = torch.zeros((len(THETA), 3) + v.shape[1:], dtype=torch.float64, device="cuda")
+    batch.step(*xyza, v, vel)
+    nt, tpt, splits, cand, ms = batch.tuning()
+    assert cand >= 4 and nt * tpt >= 256 and 1 <= splits <= 4 and ms > 0
+    for m in range(len(THETA)):
+        sv, svel = single_step(sb, sb.FP64, THETA[m], PDEG[m], xyza, vors[m].contiguous())
+        assert rel(v[m], sv) <= 1e-12, m
+        assert rel(vel[m], svel) <= 1e-12, m
+
+
+def test_batch_graph_replay_equals_steps(sb):
+    g, xyza, vors = grid_and_vors(sb, len(THETA))
+    a = sb.Batch(base_cfg(sb, sb.MIXED), THETA, PDEG)
+    b = sb.Batch(base_cfg(sb, sb.MIXED), THETA, PDEG)
+    for x in (a, b):
+        x.set_tuning(128, 2, 2)
+    va, vb = vors.clone(), vors.clone()
+    vela = torch.zeros((len(THETA), 3) + va.shape[1:], dtype=torch.float64, device="cuda")
+    velb = torch.zeros_like(vela)
+    a.run(*xyza, va, vela, nsteps=3)
+    for _ in range(3):
+        b.step(*xyza, vb, velb)
+    assert torch.equal(va, vb) and torch.equal(vela, velb)
+
+
+def test_batch_mixed_accuracy_vs_direct_sum(sb):
+    g, xyza, vors = grid_and_vors(sb, len(THETA))
+    batch = sb.Batch(base_cfg(sb, sb.MIXED), THETA, PDEG)
+    v = vors.clone()
+    vel = torch.zeros((len(THETA), 3) + v.shape[1:], dtype=torch.float64, device="cuda")
+    batch.step(*xyza, v, vel)
+    for m in range(len(THETA)):
+        ctx = sb.Context(base_cfg(sb, sb.FP64, velocity=sb.VEL_DIRECT))
+        d = vors[m].clone()
+        dvel = [torch.zeros_like(d) for _ in range(3)]
+        ctx.bve_back_rk4_step(*xyza, d, *dvel)
+        assert rel(v[m], d) <= 1e-6, (m, rel(v[m], d))
+
+
+def test_batch_rejects_bad_members(sb):
+    with pytest.raises(sb.SbslpmError):
+        sb.Batch(base_cfg(sb, sb.FP64), [0.7, 0.7], [8, 4])
+    with pytest.raises(sb.SbslpmError):
+        sb.Batch(base_cfg(sb, sb.FP64), [0.7, -1.0], [8, 8])
