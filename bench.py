@@ -245,6 +245,164 @@ def swe_bench(sb, torch, dev, flush, steps):
     return out
 
 
+ENS_MEMBERS, ENS_LEVELS, ENS_SH_DEGREE = 128, 6, 20
+
+
+def sh_basis(g, lmax):
+    """Real orthonormal spherical harmonics of degrees 1..lmax at the grid points
+    ([functions][leaf*q]); degree 0 is left out because relative vorticity
+    integrates to zero over the sphere."""
+    import scipy.special as sp
+
+    colat = np.arccos(np.clip(g.z.ravel(), -1, 1))
+    lon = np.arctan2(g.y.ravel(), g.x.ravel())
+    cols = []
+    for l in range(1, lmax + 1):
+        for m in range(0, l + 1):
+            Y = sp.sph_harm_y(l, m, colat, lon)
+            if m == 0:
+                cols.append(Y.real)
+            else:
+                cols.append(np.sqrt(2) * Y.real)
+                cols.append(np.sqrt(2) * Y.imag)
+    return np.stack(cols)
+
+
+def ensemble_bench(sb, torch, dev, flush, steps):
+    """The batched ensemble: 128 members on 6 x 32 x 32 panels x 4 x 4 points
+    (98,304 particles each, levels 6), each the Rossby-Haurwitz state plus a
+    seeded real spherical-harmonic perturbation of degrees 1..20 with
+    N(0, 1e-3^2) coefficients (seed = member id), theta ~ U[0.5, 0.8] and proxy
+    degree in {6, 8, 10} from a seeded generator, leaves <= 256 particles,
+    dt = 0.005, mixed precision, one CUDA graph per step.  Reports ensemble
+    steps/s, member-steps/s, pair rates, the autotuner's choice, the float64
+    plain single-member path at the same size, and the vorticity error of
+    four members after one step against the float64 direct sum."""
+    g = sb.build_grid(ENS_LEVELS, DEGREE, exact_cc=True)
+    base = rh4(g)
+    B = sh_basis(g, ENS_SH_DEGREE)
+    coef = np.stack([np.random.default_rng(m).normal(0.0, 1e-3, B.shape[0]) for m in range(ENS_MEMBERS)])
+    vors = base[None] + (coef @ B).reshape((ENS_MEMBERS,) + base.shape)
+    rng = np.random.default_rng(2026)
+    theta = rng.uniform(0.5, 0.8, ENS_MEMBERS)
+    pdeg = rng.choice([6, 8, 10], ENS_MEMBERS)
+
+    def T(a):
+        return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
+    xyza = [T(g.x), T(g.y), T(g.z), T(g.area)]
+    cfg = sb.config_default(levels=ENS_LEVELS, interp_degree=DEGREE, kernel_eps=EPS, omega=OMEGA, dt=DT,
+                            precision=sb.MIXED, leaf_size=LEAF_SIZE)
+    batch = sb.Batch(cfg, theta, pdeg)
+    v = T(vors)
+    vel = torch.zeros((ENS_MEMBERS, 3) + base.shape, dtype=torch.float64, device=dev)
+    batch.run(*xyza, v, vel, nsteps=3)  # autotune on the first step, graph capture, warm-up
+    torch.cuda.synchronize()
+    st = torch.cuda.current_stream()
+    launches0 = sb.kernel_launches()
+    ts = []
+    for _ in range(steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        batch.run(*xyza, v, vel, nsteps=1)
+        e1.record(st)
+        e1.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    launches = sb.kernel_launches() - launches0
+    ms = sum(ts) / len(ts)
+    near_pairs, far_pairs = batch.pairs()
+    nt, tpt, splits, cand, near_ms = batch.tuning()
+
+    # accuracy of four members after one step against the float64 direct sum
+    acc = []
+    for m in (0, 1, 2, 3):
+        one = sb.Batch(cfg, theta[m:m + 1], pdeg[m:m + 1])
+        vm = T(vors[m:m + 1])
+        velm = torch.zeros((1, 3) + base.shape, dtype=torch.float64, device=dev)
+        one.step(*xyza, vm, velm)
+        ctxd = sb.Context(sb.config_default(levels=ENS_LEVELS, interp_degree=DEGREE, kernel_eps=EPS, omega=OMEGA,
+                                            dt=DT, velocity=sb.VEL_DIRECT))
+        d = T(vors[m])
+        dv = [torch.zeros_like(d) for _ in range(3)]
+        ctxd.bve_back_rk4_step(*xyza, d, *dv)
+        acc.append({"member": m, "theta": float(theta[m]), "proxy_degree": int(pdeg[m]),
+                    "rel_linf_vort": (vm[0] - d).abs().max().item() / d.abs().max().item()})
+        del one, ctxd
+
+    # the float64 plain path on one member of the same size (theta 0.7, degree 8)
+    ctx64 = sb.Context(sb.config_default(levels=ENS_LEVELS, interp_degree=DEGREE, fmm_theta=THETA, kernel_eps=EPS,
+                                         omega=OMEGA, dt=DT, precision=sb.FP64, proxy_degree=PROXY_DEGREE,
+                                         leaf_size=LEAF_SIZE))
+    f64 = [*xyza, T(vors[0]), *[torch.zeros_like(xyza[0]) for _ in range(3)], None]
+    for _ in range(3):
+        ctx64.bve_run(*f64, nsteps=1)
+    t64 = timed_steps(torch, ctx64, f64, steps, flush)
+    fp64_sps = 1e3 / (sum(t64) / len(t64))
+    member_sps = ENS_MEMBERS * 1e3 / ms
+    return {
+        "ensemble_steps_per_s": 1e3 / ms, "member_steps_per_s": member_sps, "ms_per_step": ms,
+        "members": ENS_MEMBERS, "particles_per_member": int(g.x.size), "gpu_launches_per_step": launches / steps,
+        "pairs_per_s": 4 * (near_pairs + far_pairs) / (ms * 1e-3),
+        "near_pairs_per_eval": near_pairs, "far_pairs_per_eval": far_pairs,
+        "near_tflops": PAIR_FLOP * near_pairs / (near_ms * 1e-3) / 1e12,
+        "autotune": {"threads": nt, "targets_per_thread": tpt, "splits": splits, "candidates": cand,
+                     "near_ms": near_ms},
+        "fp64_plain_single_member_steps_per_s": fp64_sps,
+        "speedup_member_steps_vs_fp64_plain": member_sps / fp64_sps,
+        "accuracy_step1_vs_fp64_direct": acc,
+        "config": {"workload": "batched BVE ensemble: 128 members x 98,304 particles (levels 6), RH4 + seeded "
+                               "real SH perturbation (degrees 1..20, N(0,1e-3^2)), theta ~ U[0.5,0.8], proxy "
+                               "degree in {6,8,10}, leaf <= 256, dt 0.005, mixed", "theta_seed": 2026,
+                   "proxy_degree_counts": {str(k): int((pdeg == k).sum()) for k in (6, 8, 10)}},
+    }
+
+
+def profile_run(sb, torch, dev, args):
+    """One path of the benchmark, stepped warmup + steps times, for profiler
+    captures of its launches (nothing is timed or printed)."""
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    n = args.warmup + args.steps
+    if args.profile == "ensemble":
+        g = sb.build_grid(ENS_LEVELS, DEGREE, exact_cc=True)
+        rng = np.random.default_rng(2026)
+        M = args.members
+        theta, pdeg = rng.uniform(0.5, 0.8, M), rng.choice([6, 8, 10], M)
+        cfg = sb.config_default(levels=ENS_LEVELS, interp_degree=DEGREE, kernel_eps=EPS, omega=OMEGA, dt=DT,
+                                precision=sb.MIXED, leaf_size=LEAF_SIZE)
+        batch = sb.Batch(cfg, theta, pdeg)
+        batch.set_tuning(64, 4, 2)
+        v = T(np.broadcast_to(rh4(g), (M,) + g.x.shape))
+        vel = torch.zeros((M, 3) + g.x.shape, dtype=torch.float64, device=dev)
+        for _ in range(n):
+            batch.step(T(g.x), T(g.y), T(g.z), T(g.area), v, vel)
+    elif args.profile in ("swe", "swe64"):
+        g = sb.build_grid(LEVELS, DEGREE, exact_cc=True)
+        om, u0 = 2 * np.pi, 2 * np.pi / 12
+        lat = np.arcsin(np.clip(g.z, -1, 1))
+        h0 = 2.94 - (om * u0 + 0.5 * u0 * u0) * np.sin(lat) ** 2
+        prec = sb.MIXED if args.profile == "swe" else sb.FP64
+        ctx = sb.Context(sb.config_default(levels=LEVELS, interp_degree=DEGREE, fmm_theta=THETA, kernel_eps=EPS,
+                                           omega=om, dt=SWE_DT, precision=prec, g_over_a=1.0))
+        f = [T(g.x), T(g.y), T(g.z), T(g.area), T(2 * u0 * np.sin(lat)), torch.zeros_like(T(g.x)), T(h0)]
+        vel = [torch.zeros_like(f[0]) for _ in range(3)]
+        base = [torch.zeros_like(f[0]) for _ in range(3)]
+        ctx.swe_init(*f, *vel, *base)
+        for _ in range(n):
+            ctx.swe_back_rk4_step_2(*f, *vel, None, *base)
+    else:
+        g = sb.build_grid(LEVELS, DEGREE, exact_cc=True)
+        prec = sb.FP64 if args.profile == "treecode64" else sb.MIXED
+        proxy = 0 if args.profile == "spectral" else PROXY_DEGREE
+        ctx = sb.Context(sb.config_default(levels=LEVELS, interp_degree=DEGREE, fmm_theta=THETA, kernel_eps=EPS,
+                                           omega=OMEGA, dt=DT, precision=prec, proxy_degree=proxy,
+                                           leaf_size=LEAF_SIZE))
+        f = [T(g.x), T(g.y), T(g.z), T(g.area), T(rh4(g)), *[torch.zeros_like(T(g.x)) for _ in range(3)], None]
+        for _ in range(n):
+            ctx.bve_back_rk4_step(*f)
+    torch.cuda.synchronize()
+
+
 def timed_steps(torch, ctx, f, steps, flush):
     """Per-step device times (ms) of bve_run(nsteps=1) with an L2 flush between."""
     st = torch.cuda.current_stream()
@@ -268,6 +426,10 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-swe", action="store_true", help="skip the shallow-water measurement")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble measurement")
+    ap.add_argument("--profile", choices=["treecode", "treecode64", "spectral", "swe", "swe64", "ensemble"],
+                    help="run --warmup + --steps steps of one path and exit (for profiler captures; no timing)")
+    ap.add_argument("--members", type=int, default=ENS_MEMBERS, help="ensemble members in --profile ensemble")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 
@@ -291,6 +453,9 @@ def main():
                                 device_id=torch.device("cuda", local_rank))
     sb = import_package()
     dev = torch.device("cuda", local_rank)
+    if args.profile:
+        profile_run(sb, torch, dev, args)
+        return
 
     g = sb.build_grid(LEVELS, DEGREE, exact_cc=True)
     vor0 = rh4(g)
@@ -371,6 +536,9 @@ def main():
     peak64 = sb.measure_fma_peak(1, 50.0) / 1e12
     share = 4 * ms_int / ms_per_step
 
+    # ---- batched ensemble ----------------------------------------------------
+    ens = None if args.no_ensemble else ensemble_bench(sb, torch, dev, flush, min(args.steps, 20))
+
     # ---- shallow water (SWE v2) ---------------------------------------------
     swe = None if args.no_swe else swe_bench(sb, torch, dev, flush, min(args.steps, 20))
 
@@ -435,7 +603,7 @@ def main():
             "reference_spectral_fmm": {"mixed_steps_per_s": r32_sps, "fp64_steps_per_s": r64_sps,
                                        "note": "the reference's own algorithm (proxy degree = particle degree 3)"},
             "accuracy_step1_vs_fp64_direct": dict(acc, direct_step_s=direct_s),
-            "swe": swe, "cpu_baseline": cpu, "clocks": clk.summary(),
+            "ensemble": ens, "swe": swe, "cpu_baseline": cpu, "clocks": clk.summary(),
         }
         print(json.dumps(line))
     if dist:
