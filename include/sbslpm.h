@@ -258,6 +258,30 @@ sbslpm_status sbslpm_swe_vel_interactions(sbslpm_ctx* ctx, const double* disp_x,
 sbslpm_status sbslpm_cubed_sphere_2d_to_1d(long n_leaves, int degree, const double* xcos, const double* ycos,
                                            const double* zcos, int* two_d_to_1d, int* counts, long* unique);
 
+/* ---------------- adjoint (device pointers) ---------------- */
+
+/* No counterpart in the reference (it has no derivatives).  One reverse step
+ * of bve_back_rk4_step: given the step's input vorticity vors (the per-step
+ * checkpoint) and the adjoint of its output vorticity vors_bar_next, writes
+ * the adjoint of the input vorticity, vors_bar = (d vors_next / d vors)^T
+ * vors_bar_next, through the four velocity evaluations (source positions and
+ * strengths), the departure search and the remap.  The forward step is
+ * recomputed from the checkpoint inside the call.  Needs a float64 context
+ * with direct-sum velocity and no tracers.  Locating points in panels is
+ * piecewise constant and is not differentiated. */
+sbslpm_status sbslpm_bve_adjoint_step(sbslpm_ctx* ctx, const double* xcos, const double* ycos, const double* zcos,
+                                      const double* area, const double* vors, const double* vors_bar_next,
+                                      double* vors_bar);
+/* Vector-Jacobian product of sbslpm_direct_sum_bve (float64) with respect to
+ * the sources: given ubar at the targets, strength_bar_j = sum_i ubar_i .
+ * du_i/dq_j and s*_bar = the same with respect to the source positions
+ * (written, not accumulated).  stream: cudaStream_t or NULL. */
+sbslpm_status sbslpm_direct_sum_bve_vjp(long n_targets, const double* tx, const double* ty, const double* tz,
+                                        const double* ubar_x, const double* ubar_y, const double* ubar_z,
+                                        long n_sources, const double* sx, const double* sy, const double* sz,
+                                        const double* strength, double eps, double* strength_bar, double* sx_bar,
+                                        double* sy_bar, double* sz_bar, void* stream);
+
 /* ---------------- batched ensemble (device pointers) ---------------- */
 
 /* No counterpart in the reference (its drivers run one problem per process).

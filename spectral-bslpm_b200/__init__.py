@@ -122,6 +122,9 @@ def lib() -> ctypes.CDLL:
     L.sbslpm_swe_vel_interactions.argtypes = [_VP] * 9
     L.sbslpm_cubed_sphere_2d_to_1d.argtypes = [ctypes.c_long, ctypes.c_int, _D, _D, _D, _I, _I,
                                                ctypes.POINTER(ctypes.c_long)]
+    L.sbslpm_bve_adjoint_step.argtypes = [_VP] * 8
+    L.sbslpm_direct_sum_bve_vjp.argtypes = [ctypes.c_long] + [_VP] * 6 + [ctypes.c_long] + [_VP] * 4 + [
+        ctypes.c_double] + [_VP] * 5
     L.sbslpm_batch_create.argtypes = [ctypes.POINTER(Config), ctypes.c_int, _D, _I, ctypes.POINTER(_VP)]
     L.sbslpm_batch_destroy.argtypes = [_VP]
     L.sbslpm_batch_set_stream.argtypes = [_VP, _VP]
@@ -385,6 +388,15 @@ class Context:
         _check(lib().sbslpm_swe_vel_interactions(self._h, *[_dev(t, "field") for t in (
             disp_x, disp_y, disp_z, source_vor, source_div, t1, t2, t3)]), "sbslpm_swe_vel_interactions")
 
+    # -- adjoint -----------------------------------------------------------
+    def bve_adjoint_step(self, xcos, ycos, zcos, area, vors, vors_bar_next, vors_bar):
+        """One reverse step: vors_bar = (d step(vors) / d vors)^T vors_bar_next."""
+        lq = (self.leaf_count, self.q)
+        self._sync_stream()
+        _check(lib().sbslpm_bve_adjoint_step(self._h, *[_dev(t, n, lq) for t, n in (
+            (xcos, "xcos"), (ycos, "ycos"), (zcos, "zcos"), (area, "area"), (vors, "vors"),
+            (vors_bar_next, "vors_bar_next"), (vors_bar, "vors_bar"))]), "sbslpm_bve_adjoint_step")
+
     def time_interactions(self, reps: int = 5):
         """(ms per launch, pair evaluations per launch) of the interaction kernel alone."""
         ms, pairs = ctypes.c_double(), ctypes.c_double()
@@ -524,6 +536,83 @@ def direct_sum_bve_noalloc(tx, ty, tz, sx, sy, sz, strength, eps, precision=FP64
                                                int(precision), *[_dev(t, "out") for t in out], _VP(_stream())),
            "sbslpm_direct_sum_bve_noalloc")
     return out
+
+
+def direct_sum_bve_vjp(tx, ty, tz, ubar, sx, sy, sz, strength, eps):
+    """VJP of direct_sum_bve with respect to the sources: (strength_bar, (sx_bar, sy_bar, sz_bar))."""
+    import torch
+
+    nt, ns = tx.numel(), sx.numel()
+    qb = torch.empty(ns, dtype=torch.float64, device=sx.device)
+    yb = tuple(torch.empty(ns, dtype=torch.float64, device=sx.device) for _ in range(3))
+    _check(lib().sbslpm_direct_sum_bve_vjp(nt, *[_dev(t, "target") for t in (tx, ty, tz)],
+                                           *[_dev(t.contiguous(), "ubar") for t in ubar], ns,
+                                           *[_dev(t, "source") for t in (sx, sy, sz, strength)], float(eps),
+                                           _dev(qb, "out"), *[_dev(t, "out") for t in yb], _VP(_stream())),
+           "sbslpm_direct_sum_bve_vjp")
+    return qb, yb
+
+
+def _autograd():
+    """torch.autograd.Function wrappers (built on first use: torch is optional at import)."""
+    import torch
+
+    class DirectSumBVE(torch.autograd.Function):
+        """u = direct_sum_bve(targets, sources, strength); gradients for the
+        source positions and strengths (targets are treated as constants)."""
+
+        @staticmethod
+        def forward(ctx, tx, ty, tz, sx, sy, sz, strength, eps):
+            ctx.save_for_backward(tx, ty, tz, sx, sy, sz, strength)
+            ctx.eps = eps
+            ux, uy, uz = direct_sum_bve(tx, ty, tz, sx, sy, sz, strength, eps)
+            return torch.stack([ux, uy, uz])
+
+        @staticmethod
+        def backward(ctx, ubar):
+            tx, ty, tz, sx, sy, sz, q = ctx.saved_tensors
+            qb, (xb, yb, zb) = direct_sum_bve_vjp(tx, ty, tz, [ubar[0], ubar[1], ubar[2]], sx, sy, sz, q, ctx.eps)
+            return None, None, None, xb, yb, zb, qb, None
+
+    class BVERollout(torch.autograd.Function):
+        """nsteps of bve_back_rk4_step from vors0 with per-step checkpoints of
+        the vorticity; the backward pass runs the hand-written adjoint step
+        in reverse order from the checkpoints."""
+
+        @staticmethod
+        def forward(ctx, vors0, context, xcos, ycos, zcos, area, nsteps):
+            v = vors0.detach().clone().contiguous()
+            vel = [torch.zeros_like(v) for _ in range(3)]
+            ckpt = []
+            for _ in range(int(nsteps)):
+                ckpt.append(v.clone())
+                context.bve_back_rk4_step(xcos, ycos, zcos, area, v, *vel)
+            ctx.context = context
+            ctx.fields = (xcos, ycos, zcos, area)
+            ctx.ckpt = ckpt
+            return v
+
+        @staticmethod
+        def backward(ctx, vbar):
+            wbar = vbar.detach().clone().contiguous()
+            out = torch.empty_like(wbar)
+            for v in reversed(ctx.ckpt):
+                ctx.context.bve_adjoint_step(*ctx.fields, v, wbar, out)
+                wbar, out = out, wbar
+            return wbar, None, None, None, None, None, None
+
+    return DirectSumBVE, BVERollout
+
+
+def direct_sum_bve_autograd(tx, ty, tz, sx, sy, sz, strength, eps):
+    """direct_sum_bve as a differentiable torch function (gradients for the sources)."""
+    return _autograd()[0].apply(tx, ty, tz, sx, sy, sz, strength, eps)
+
+
+def bve_rollout(context, xcos, ycos, zcos, area, vors0, nsteps):
+    """nsteps BVE steps as a differentiable torch function of the initial
+    vorticity (float64 direct-sum context), adjoint with per-step checkpoints."""
+    return _autograd()[1].apply(vors0, context, xcos, ycos, zcos, area, int(nsteps))
 
 
 def direct_sum_inv_lap(x, y, z, area, pots, soln):

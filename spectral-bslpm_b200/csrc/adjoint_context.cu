@@ -1,0 +1,106 @@
+// C ABI of the adjoint: one reverse step of bve_back_rk4_step
+// (src/bve_time_step.cpp:311-419) and the stand-alone vector-Jacobian product
+// of the Biot-Savart direct sum.
+//
+// The reverse step recomputes the forward step from its input vorticity (the
+// per-step checkpoint): stage velocities v0..v3 and stage sources, then runs
+// the departure/remap adjoint and the four velocity evaluations' adjoints in
+// reverse stage order (stage s's sources depend on v_{s-1}).
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "adjoint.cuh"
+#include "context_internal.hpp"
+
+using namespace sbslpm;
+
+namespace {
+
+sbslpm_status adjoint_setup(sbslpm_ctx* c) {
+  if (c->adj_src) return SBSLPM_OK;
+  const size_t pn = (size_t)c->P * c->q, ln = (size_t)c->A * c->q;
+  c->adj_groups = adjoint_groups((long)ln, (long)ln);
+  SB_TRY(dalloc(&c->adj_src, 4 * pn));
+  SB_TRY(dalloc(&c->adj_vbar, 4 * 3 * ln));
+  SB_TRY(dalloc(&c->adj_q, ln));
+  SB_TRY(dalloc(&c->adj_y, 3 * ln));
+  SB_TRY(dalloc(&c->adj_part, (size_t)c->adj_groups * 4 * ln));
+  SB_TRY(dalloc(&c->adj_w, ln));
+  SB_TRY(dalloc(&c->adj_vel, 3 * ln));
+  return SBSLPM_OK;
+}
+
+bool bad(const void* p) { return p == nullptr; }
+
+}  // namespace
+
+extern "C" {
+
+sbslpm_status sbslpm_bve_adjoint_step(sbslpm_ctx* c, const double* x, const double* y, const double* z,
+                                      const double* area, const double* vors, const double* vors_bar_next,
+                                      double* vors_bar) {
+  if (!c || bad(x) || bad(y) || bad(z) || bad(area) || bad(vors) || bad(vors_bar_next) || bad(vors_bar))
+    return SBSLPM_ERR_ARG;
+  if (c->cfg.velocity != SBSLPM_VEL_DIRECT || c->cfg.precision != SBSLPM_FP64)
+    return set_last_error("the adjoint step runs on the float64 direct-sum velocity"), SBSLPM_ERR_CONFIG;
+  if (c->cfg.tracer_count != 0)
+    return set_last_error("the adjoint step needs a context without tracers"), SBSLPM_ERR_CONFIG;
+  SB_TRY(adjoint_setup(c));
+  cudaStream_t st = c->stream();
+  const size_t ln = (size_t)c->A * c->q, pn = (size_t)c->P * c->q, off = (size_t)c->off * c->q;
+  const double dt = c->cfg.dt;
+  // forward recompute from the checkpoint: stage velocities into vbuf
+  SB_CUDA(cudaMemcpyAsync(c->adj_w, vors, sizeof(double) * ln, cudaMemcpyDeviceToDevice, st));
+  enqueue_step(c, x, y, z, area, c->adj_w, c->adj_vel, c->adj_vel + ln, c->adj_vel + 2 * ln, nullptr);
+  const double* v[4];
+  for (int k = 0; k < 4; k++) v[k] = c->vbuf + (size_t)k * 3 * ln;
+  const double h[4] = {0.0, 0.5 * dt, 0.5 * dt, dt};
+  for (int s = 0; s < 4; s++)
+    launch_leaf_sources(c->geom, s, h[s], s ? v[s - 1] : nullptr, x, y, z, vors, area, c->adj_src + s * pn, st);
+  // reverse: departure search and remap, then the stages from the last
+  double* vb[4];
+  for (int k = 0; k < 4; k++) vb[k] = c->adj_vbar + (size_t)k * 3 * ln;
+  SB_CUDA(cudaMemsetAsync(vors_bar, 0, sizeof(double) * ln, st));
+  SB_CUDA(cudaMemsetAsync(c->adj_vbar, 0, sizeof(double) * 4 * 3 * ln, st));
+  launch_depart_remap_adjoint(c->geom, c->tab, x, y, z, v[0], v[1], v[2], v[3], dt, vors, vors_bar_next, vors_bar,
+                              vb[0], vb[1], vb[2], vb[3], st);
+  for (int s = 3; s >= 0; s--) {
+    launch_bs_vjp((long)ln, x, y, z, vb[s], vb[s] + ln, vb[s] + 2 * ln, (long)ln, c->adj_src + s * pn + off,
+                  c->cfg.kernel_eps, c->adj_part, c->adj_groups, c->adj_q, c->adj_y, st);
+    launch_src_adjoint((long)ln, s, h[s], c->cfg.omega, s ? v[s - 1] : nullptr, x, y, z, area, c->adj_q, c->adj_y,
+                       vors_bar, s ? vb[s - 1] : nullptr, st);
+  }
+  return finish(c);
+}
+
+sbslpm_status sbslpm_direct_sum_bve_vjp(long nt, const double* tx, const double* ty, const double* tz,
+                                        const double* ubar_x, const double* ubar_y, const double* ubar_z, long ns,
+                                        const double* sx, const double* sy, const double* sz, const double* strength,
+                                        double eps, double* strength_bar, double* sx_bar, double* sy_bar,
+                                        double* sz_bar, void* stream) {
+  if (nt <= 0 || ns <= 0 || bad(tx) || bad(ty) || bad(tz) || bad(ubar_x) || bad(ubar_y) || bad(ubar_z) ||
+      bad(sx) || bad(sy) || bad(sz) || bad(strength) || bad(strength_bar) || bad(sx_bar) || bad(sy_bar) ||
+      bad(sz_bar) || !(eps >= 0))
+    return SBSLPM_ERR_ARG;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int groups = adjoint_groups(nt, ns);
+  double4* src = nullptr;
+  double *part = nullptr, *ybar = nullptr;
+  SB_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&src), sizeof(double4) * ns, st));
+  SB_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&part), sizeof(double) * groups * 4 * ns, st));
+  SB_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&ybar), sizeof(double) * 3 * ns, st));
+  launch_pack_sources(ns, sx, sy, sz, strength, src, st);
+  launch_bs_vjp(nt, tx, ty, tz, ubar_x, ubar_y, ubar_z, ns, src, eps, part, groups, strength_bar, ybar, st);
+  SB_CUDA(cudaMemcpyAsync(sx_bar, ybar, sizeof(double) * ns, cudaMemcpyDeviceToDevice, st));
+  SB_CUDA(cudaMemcpyAsync(sy_bar, ybar + ns, sizeof(double) * ns, cudaMemcpyDeviceToDevice, st));
+  SB_CUDA(cudaMemcpyAsync(sz_bar, ybar + 2 * ns, sizeof(double) * ns, cudaMemcpyDeviceToDevice, st));
+  cudaFreeAsync(src, st);
+  cudaFreeAsync(part, st);
+  cudaFreeAsync(ybar, st);
+  SB_CUDA(cudaGetLastError());
+  SB_CUDA(cudaStreamSynchronize(st));
+  return SBSLPM_OK;
+}
+
+}  // extern "C"

@@ -778,54 +778,6 @@ __global__ void k_reduce_groups(const double* __restrict__ partial, int groups, 
 // write dep).
 
 template <int D>
-struct Basis {
-  double fx[D + 1], fe[D + 1];
-  long row;  // (leaf - offset) * q
-};
-
-template <int D>
-__device__ __forceinline__ void locate_basis(const StepGeom& g, const BliTable& tab, double x, double y, double z,
-                                             Basis<D>& b, unsigned& err) {
-  double xi, eta;
-  Bounds bd;
-  int leaf = locate_leaf(x, y, z, g.levels, xi, eta, bd, err);
-  bli_1d(xi, kPi / 4.0 * bd.min_xi, kPi / 4.0 * bd.max_xi, D, tab.cosv, tab.w, b.fx, err);
-  bli_1d(eta, kPi / 4.0 * bd.min_eta, kPi / 4.0 * bd.max_eta, D, tab.cosv, tab.w, b.fe, err);
-  b.row = (long)(leaf - g.offset) * g.q;
-}
-
-// sum_m field[row + m] * fx[i] fe[j] with m = i (D+1) + j, in m order.
-template <int D>
-__device__ __forceinline__ double gather(const Basis<D>& b, const double* __restrict__ f, long stride = 1,
-                                         long base = 0) {
-  double acc = 0;
-  int m = 0;
-#pragma unroll
-  for (int i = 0; i <= D; i++)
-#pragma unroll
-    for (int j = 0; j <= D; j++, m++) acc += f[(b.row + m) * stride + base] * (b.fx[i] * b.fe[j]);
-  return acc;
-}
-
-template <int D>
-__device__ __forceinline__ void gather3(const Basis<D>& b, const double* __restrict__ v, long n, double& a,
-                                        double& c, double& e) {
-  a = 0;
-  c = 0;
-  e = 0;
-  int m = 0;
-#pragma unroll
-  for (int i = 0; i <= D; i++)
-#pragma unroll
-    for (int j = 0; j <= D; j++, m++) {
-      double bm = b.fx[i] * b.fe[j];
-      a += v[b.row + m] * bm;
-      c += v[n + b.row + m] * bm;
-      e += v[2 * n + b.row + m] * bm;
-    }
-}
-
-template <int D>
 __device__ __forceinline__ void depart_remap_body(const StepGeom& g, const BliTable& tab, long o,
                                                   const double* __restrict__ x, const double* __restrict__ y,
                                                   const double* __restrict__ z, const double* __restrict__ v0,
