@@ -44,6 +44,7 @@ METRIC = "BVE RK4 steps/s at ≤1e-6 rel vort err: mixed+batched vs FP64 plain, 
 LEVELS, DEGREE, THETA, EPS, OMEGA, DT = 7, 3, 0.7, 1e-4, 2 * np.pi, 0.005
 PROXY_DEGREE, LEAF_SIZE = 8, 256
 PAIR_FLOP = 17  # FLOP per Biot-Savart pair (division counted as 1)
+NEAR_TRAFFIC = 15.888640e6 + 3.84e3  # DRAM bytes of one near-field launch, from the committed ncu capture
 
 
 def workload_config():
@@ -403,6 +404,64 @@ def profile_run(sb, torch, dev, args):
     torch.cuda.synchronize()
 
 
+ADJ_LEVELS, ADJ_STEPS, ADJ_DT = 5, 20, 0.01
+
+
+def adjoint_bench(sb, torch, dev, directions=8):
+    """The adjoint configuration: 24,576 particles (levels 5), Gaussian vortex
+    exp(-|x - x0|^2/(2 0.15^2)) at 30N 0E plus seeded N(0, 1e-2^2) noise,
+    J = 1/2 sum w (w(T) - w*(T))^2 (w = quadrature weights, w* from the
+    noiseless state), 20 steps of dt = 0.01 on the float64 direct-sum
+    velocity, gradient through the hand-written adjoint with per-step
+    checkpoints.  Reports forward and backward times and the gradient against
+    central differences (h = 1e-6) in seeded directions (the test suite
+    checks 64)."""
+    g = sb.build_grid(ADJ_LEVELS, DEGREE, exact_cc=True)
+    lat0 = np.deg2rad(30.0)
+    c = np.array([np.cos(lat0), 0.0, np.sin(lat0)])
+    w0 = np.exp(-((g.x - c[0]) ** 2 + (g.y - c[1]) ** 2 + (g.z - c[2]) ** 2) / (2 * 0.15 ** 2))
+    wn = w0 + 1e-2 * np.random.default_rng(3).standard_normal(w0.shape)
+    ctx = sb.Context(sb.config_default(levels=ADJ_LEVELS, interp_degree=DEGREE, kernel_eps=EPS, omega=OMEGA,
+                                       dt=ADJ_DT, velocity=sb.VEL_DIRECT, precision=sb.FP64))
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    f = [T(g.x), T(g.y), T(g.z), T(g.area)]
+    area = f[3]
+
+    def run(w):
+        v = w.clone()
+        vel = [torch.zeros_like(v) for _ in range(3)]
+        ctx.bve_run(*f, v, *vel, nsteps=ADJ_STEPS)
+        return v
+
+    wstar = run(T(w0))
+    J = lambda w: 0.5 * float((area * (run(w) - wstar) ** 2).sum())
+    st = torch.cuda.current_stream()
+    x = T(wn).requires_grad_()
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    e0.record(st)
+    out = sb.bve_rollout(ctx, *f, x, ADJ_STEPS)
+    loss = 0.5 * (area * (out - wstar) ** 2).sum()
+    e1.record(st)
+    loss.backward()
+    e2.record(st)
+    e2.synchronize()
+    grad = x.grad
+    fds, ads = [], []
+    for k in range(directions):
+        d = T(np.random.default_rng(1000 + k).standard_normal(wn.shape))
+        fds.append((J(T(wn) + 1e-6 * d) - J(T(wn) - 1e-6 * d)) / 2e-6)
+        ads.append(float((grad * d).sum()))
+    fds, ads = np.array(fds), np.array(ads)
+    rms = float(np.sqrt((ads ** 2).mean()))
+    return {"forward_ms": e0.elapsed_time(e1), "backward_ms": e1.elapsed_time(e2), "steps": ADJ_STEPS,
+            "particles": int(g.x.size), "J": float(loss.detach()), "grad_norm": float(grad.norm()),
+            "fd_directions": directions, "fd_max_err_over_rms": float(np.abs(fds - ads).max() / rms),
+            "fd_max_rel_err": float((np.abs(fds - ads) / np.abs(ads)).max()),
+            "config": {"workload": "BVE adjoint: 24,576 particles, Gaussian vortex (30N, 0E, sigma 0.15) + "
+                                   "N(0,1e-2^2) noise, 20 steps dt 0.01, float64 direct sum, per-step "
+                                   "checkpoints", "h": 1e-6}}
+
+
 def timed_steps(torch, ctx, f, steps, flush):
     """Per-step device times (ms) of bve_run(nsteps=1) with an L2 flush between."""
     st = torch.cuda.current_stream()
@@ -427,6 +486,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-swe", action="store_true", help="skip the shallow-water measurement")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble measurement")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint measurement")
     ap.add_argument("--profile", choices=["treecode", "treecode64", "spectral", "swe", "swe64", "ensemble"],
                     help="run --warmup + --steps steps of one path and exit (for profiler captures; no timing)")
     ap.add_argument("--members", type=int, default=ENS_MEMBERS, help="ensemble members in --profile ensemble")
@@ -511,9 +571,13 @@ def main():
     # ---- accuracy after one step vs the float64 direct sum ------------------
     ctxd = ctx_for(sb.FP64, sb.VEL_DIRECT, proxy=0)
     fd = fields()
-    t0 = time.perf_counter()
+    st0 = torch.cuda.current_stream()
+    ed0, ed1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ed0.record(st0)
     ctxd.bve_back_rk4_step(*fd)
-    direct_s = time.perf_counter() - t0
+    ed1.record(st0)
+    ed1.synchronize()
+    direct_s = ed0.elapsed_time(ed1) * 1e-3
     ref = fd[4]
     scale = ref.abs().max().item()
     vel_ref = torch.stack(fd[5:8])
@@ -538,6 +602,9 @@ def main():
 
     # ---- batched ensemble ----------------------------------------------------
     ens = None if args.no_ensemble else ensemble_bench(sb, torch, dev, flush, min(args.steps, 20))
+
+    # ---- adjoint -------------------------------------------------------------
+    adj = None if args.no_adjoint else adjoint_bench(sb, torch, dev)
 
     # ---- shallow water (SWE v2) ---------------------------------------------
     swe = None if args.no_swe else swe_bench(sb, torch, dev, flush, min(args.steps, 20))
@@ -593,17 +660,23 @@ def main():
             "gpu_launches": launches,
             "roofline": {"bound": "fp32", "kernel": "k_bltc_near32 (near-field particle pairs, 256 x 256 tiles)",
                          "achieved": achieved, "peak": peak_meas, "unit": "TFLOP/s", "frac": achieved / peak_meas,
-                         "traffic": None, "flop_per_pair": PAIR_FLOP, "pairs_per_launch": pairs,
+                         "traffic": NEAR_TRAFFIC, "traffic_source": "profiles/k_bltc_near32_levels7.md "
+                         "(dram__bytes_read.sum + dram__bytes_write.sum of one launch)",
+                         "flop_per_pair": PAIR_FLOP, "pairs_per_launch": pairs,
                          "ms_per_launch": ms_int, "step_share": share,
                          "peak_source": "measured f32 FMA-chain throughput on this GPU (sbslpm_measure_fma_peak); "
                                         "MEASURED_PEAKS.json has no CUDA-core peak"},
             "fp64_plain": {"steps_per_s": fp64_sps, "ms_per_step": 1e3 / fp64_sps, "near_kernel_tflops": ach64,
                            "fp64_fma_peak_tflops": peak64, "frac": ach64 / peak64},
             "speedup_mixed_vs_fp64_plain": value / world / fp64_sps,
+            "fp64_direct_sum": {"steps_per_s": 1.0 / direct_s,
+                                "note": "the float64 Biot-Savart direct sum (the reference's algorithm at theta -> 0, "
+                                        "the float64 path that meets the 1e-6 bar with the reference's method)",
+                                "speedup_mixed_treecode_vs_fp64_direct": value / world * direct_s},
             "reference_spectral_fmm": {"mixed_steps_per_s": r32_sps, "fp64_steps_per_s": r64_sps,
                                        "note": "the reference's own algorithm (proxy degree = particle degree 3)"},
             "accuracy_step1_vs_fp64_direct": dict(acc, direct_step_s=direct_s),
-            "ensemble": ens, "swe": swe, "cpu_baseline": cpu, "clocks": clk.summary(),
+            "ensemble": ens, "adjoint": adj, "swe": swe, "cpu_baseline": cpu, "clocks": clk.summary(),
         }
         print(json.dumps(line))
     if dist:
