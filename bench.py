@@ -453,7 +453,23 @@ def adjoint_bench(sb, torch, dev, directions=8):
         ads.append(float((grad * d).sum()))
     fds, ads = np.array(fds), np.array(ads)
     rms = float(np.sqrt((ads ** 2).mean()))
+    # the same gradient through the treecode's adjoint (float64, degree-8 proxies, 256-particle leaves)
+    ctxt = sb.Context(sb.config_default(levels=ADJ_LEVELS, interp_degree=DEGREE, kernel_eps=EPS, omega=OMEGA,
+                                        dt=ADJ_DT, precision=sb.FP64, fmm_theta=THETA, proxy_degree=PROXY_DEGREE,
+                                        leaf_size=LEAF_SIZE))
+    xt = T(wn).requires_grad_()
+    t0, t1, t2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    t0.record(st)
+    outt = sb.bve_rollout(ctxt, *f, xt, ADJ_STEPS)
+    losst = 0.5 * (area * (outt - wstar) ** 2).sum()
+    t1.record(st)
+    losst.backward()
+    t2.record(st)
+    t2.synchronize()
+    tree = {"forward_ms": t0.elapsed_time(t1), "backward_ms": t1.elapsed_time(t2),
+            "grad_rel_l2_vs_direct_sum_adjoint": float((xt.grad - grad).norm() / grad.norm())}
     return {"forward_ms": e0.elapsed_time(e1), "backward_ms": e1.elapsed_time(e2), "steps": ADJ_STEPS,
+            "treecode": tree,
             "particles": int(g.x.size), "J": float(loss.detach()), "grad_norm": float(grad.norm()),
             "fd_directions": directions, "fd_max_err_over_rms": float(np.abs(fds - ads).max() / rms),
             "fd_max_rel_err": float((np.abs(fds - ads) / np.abs(ads)).max()),

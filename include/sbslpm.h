@@ -267,8 +267,8 @@ sbslpm_status sbslpm_cubed_sphere_2d_to_1d(long n_leaves, int degree, const doub
  * vors_bar_next, through the four velocity evaluations (source positions and
  * strengths), the departure search and the remap.  The forward step is
  * recomputed from the checkpoint inside the call.  Needs a float64 context
- * with direct-sum velocity and no tracers.  Locating points in panels is
- * piecewise constant and is not differentiated. */
+ * with direct-sum or treecode (proxy_degree > 0) velocity and no tracers.
+ * Locating points in panels is piecewise constant and is not differentiated. */
 sbslpm_status sbslpm_bve_adjoint_step(sbslpm_ctx* ctx, const double* xcos, const double* ycos, const double* zcos,
                                       const double* area, const double* vors, const double* vors_bar_next,
                                       double* vors_bar);

@@ -10,7 +10,10 @@
 
 #include <string>
 
+#include <vector>
+
 #include "adjoint.cuh"
+#include "adjoint_tree.cuh"
 #include "context_internal.hpp"
 
 using namespace sbslpm;
@@ -18,16 +21,43 @@ using namespace sbslpm;
 namespace {
 
 sbslpm_status adjoint_setup(sbslpm_ctx* c) {
-  if (c->adj_src) return SBSLPM_OK;
+  if (c->adj_vbar) return SBSLPM_OK;
   const size_t pn = (size_t)c->P * c->q, ln = (size_t)c->A * c->q;
   c->adj_groups = adjoint_groups((long)ln, (long)ln);
-  SB_TRY(dalloc(&c->adj_src, 4 * pn));
+  if (!c->tree) SB_TRY(dalloc(&c->adj_src, 4 * pn));
   SB_TRY(dalloc(&c->adj_vbar, 4 * 3 * ln));
   SB_TRY(dalloc(&c->adj_q, ln));
   SB_TRY(dalloc(&c->adj_y, 3 * ln));
   SB_TRY(dalloc(&c->adj_part, (size_t)c->adj_groups * 4 * ln));
   SB_TRY(dalloc(&c->adj_w, ln));
   SB_TRY(dalloc(&c->adj_vel, 3 * ln));
+  if (c->tree) {
+    // transposed near and well-separated lists of the treecode
+    TreeTables t;
+    SB_TRY(build_tree_tables(c->L, c->d, c->panels, c->cfg.leaf_size, c->cfg.proxy_degree, t));
+    TreeLists l;
+    build_tree_lists(t, c->cfg.fmm_theta, l);
+    auto transpose = [](const std::vector<int>& start, const std::vector<int>& src, int nsrc, int base,
+                        std::vector<int>& tstart, std::vector<int>& ttgt) {
+      const int nt = (int)start.size() - 1;
+      tstart.assign(nsrc + 1, 0);
+      for (int e = 0; e < start[nt]; e++) tstart[src[e] - base + 1]++;
+      for (int i = 0; i < nsrc; i++) tstart[i + 1] += tstart[i];
+      ttgt.assign(start[nt], 0);
+      std::vector<int> fill(tstart.begin(), tstart.end() - 1);
+      for (int tg = 0; tg < nt; tg++)
+        for (int e = start[tg]; e < start[tg + 1]; e++) ttgt[fill[src[e] - base]++] = tg;
+    };
+    std::vector<int> nts, ntt, cts, ctt;
+    transpose(l.ns, l.nsrc, t.Af, 0, nts, ntt);
+    transpose(l.cs, l.csrc, t.Pf, 0, cts, ctt);
+    SB_TRY(upload(&c->adj_near_ts, nts));
+    SB_TRY(upload(&c->adj_near_tt, ntt));
+    SB_TRY(upload(&c->adj_cc_ts, cts));
+    SB_TRY(upload(&c->adj_cc_tt, ctt));
+    SB_TRY(dalloc(&c->adj_tbar, (size_t)3 * t.Pf * t.qx));
+    SB_TRY(dalloc(&c->adj_qbl, (size_t)t.Pf * t.qx));
+  }
   return SBSLPM_OK;
 }
 
@@ -42,8 +72,9 @@ sbslpm_status sbslpm_bve_adjoint_step(sbslpm_ctx* c, const double* x, const doub
                                       double* vors_bar) {
   if (!c || bad(x) || bad(y) || bad(z) || bad(area) || bad(vors) || bad(vors_bar_next) || bad(vors_bar))
     return SBSLPM_ERR_ARG;
-  if (c->cfg.velocity != SBSLPM_VEL_DIRECT || c->cfg.precision != SBSLPM_FP64)
-    return set_last_error("the adjoint step runs on the float64 direct-sum velocity"), SBSLPM_ERR_CONFIG;
+  if (c->cfg.precision != SBSLPM_FP64 || !(c->cfg.velocity == SBSLPM_VEL_DIRECT || c->tree))
+    return set_last_error("the adjoint step runs on the float64 direct-sum or treecode velocity"),
+           SBSLPM_ERR_CONFIG;
   if (c->cfg.tracer_count != 0)
     return set_last_error("the adjoint step needs a context without tracers"), SBSLPM_ERR_CONFIG;
   SB_TRY(adjoint_setup(c));
@@ -56,8 +87,9 @@ sbslpm_status sbslpm_bve_adjoint_step(sbslpm_ctx* c, const double* x, const doub
   const double* v[4];
   for (int k = 0; k < 4; k++) v[k] = c->vbuf + (size_t)k * 3 * ln;
   const double h[4] = {0.0, 0.5 * dt, 0.5 * dt, dt};
-  for (int s = 0; s < 4; s++)
-    launch_leaf_sources(c->geom, s, h[s], s ? v[s - 1] : nullptr, x, y, z, vors, area, c->adj_src + s * pn, st);
+  if (!c->tree)
+    for (int s = 0; s < 4; s++)
+      launch_leaf_sources(c->geom, s, h[s], s ? v[s - 1] : nullptr, x, y, z, vors, area, c->adj_src + s * pn, st);
   // reverse: departure search and remap, then the stages from the last
   double* vb[4];
   for (int k = 0; k < 4; k++) vb[k] = c->adj_vbar + (size_t)k * 3 * ln;
@@ -65,9 +97,18 @@ sbslpm_status sbslpm_bve_adjoint_step(sbslpm_ctx* c, const double* x, const doub
   SB_CUDA(cudaMemsetAsync(c->adj_vbar, 0, sizeof(double) * 4 * 3 * ln, st));
   launch_depart_remap_adjoint(c->geom, c->tab, x, y, z, v[0], v[1], v[2], v[3], dt, vors, vors_bar_next, vors_bar,
                               vb[0], vb[1], vb[2], vb[3], st);
+  const TreeAdjointLists tl{c->adj_near_ts, c->adj_near_tt, c->adj_cc_ts, c->adj_cc_tt};
   for (int s = 3; s >= 0; s--) {
-    launch_bs_vjp((long)ln, x, y, z, vb[s], vb[s] + ln, vb[s] + 2 * ln, (long)ln, c->adj_src + s * pn + off,
-                  c->cfg.kernel_eps, c->adj_part, c->adj_groups, c->adj_q, c->adj_y, st);
+    if (c->tree) {
+      // this stage's particle sources, then the treecode's adjoint
+      launch_bltc_sources(c->tgeom, c->fgeom, c->ftab, s, h[s], s ? v[s - 1] : nullptr, x, y, z, vors, area, c->psrc,
+                          nullptr, c->fsrc, false, st);
+      launch_tree_velocity_adjoint(c->tgeom, c->fgeom, c->ftab, tl, x, y, z, vb[s], c->psrc, c->adj_tbar, c->adj_qbl,
+                                   c->adj_q, c->adj_y, st);
+    } else {
+      launch_bs_vjp((long)ln, x, y, z, vb[s], vb[s] + ln, vb[s] + 2 * ln, (long)ln, c->adj_src + s * pn + off,
+                    c->cfg.kernel_eps, c->adj_part, c->adj_groups, c->adj_q, c->adj_y, st);
+    }
     launch_src_adjoint((long)ln, s, h[s], c->cfg.omega, s ? v[s - 1] : nullptr, x, y, z, area, c->adj_q, c->adj_y,
                        vors_bar, s ? vb[s - 1] : nullptr, st);
   }

@@ -1,0 +1,330 @@
+// Adjoint of the decoupled-degree treecode velocity (float64): the reverse
+// of k_bltc_sources -> upward pass -> well-separated proxy interactions ->
+// downward pass -> leaf interpolation + near field.  Every forward piece is
+// linear in the strengths; the source positions enter the near field and the
+// anterpolation onto the leaf proxies (the proxies themselves are fixed):
+//
+//   v_i      = near_i + sum_k B_k(x_i) T_leaf(i),k          B: leaf-box BLI basis (fixed)
+//   T        = D (cc(Q))                                    D: downward pass
+//   cc(Q)_t  = K x_t x sum_s sum_k g (y_k - x_t) Q_s,k       fixed proxies x_t, y_k
+//   Q        = U (A(y) q)                                   U: upward pass, A: anterpolation
+//   near_i   = K x_i x sum_j g (y_j - x_i) q_j              near leaf pairs
+//
+// Reverse: Tbar_leaf = B^T vbar; Tbar = D^T Tbar (an upward accumulation of
+// three fields); Qbar_s = cc^T(Tbar) (a source-owned sum over the transposed
+// well-separated list); Qbar = U^T Qbar (a downward accumulation); then per
+// particle qbar_j = [A^T Qbar]_j + near^T, ybar_j = q_j grad_y(A^T Qbar) +
+// near^T, with near^T the source-owned sum over the transposed near list.
+#include <cuda_runtime.h>
+
+#include "adjoint_tree.cuh"
+#include "device_common.cuh"
+
+namespace sbslpm {
+namespace {
+
+using namespace dev;
+
+constexpr int kT = 128;
+
+// Tbar_leaf[c][k] = sum_i B_k(x_i) vbar_c,i over the leaf's particles.
+__global__ void k_tree_to_particles_T(TreeGeom tg, StepGeom fg, const double* __restrict__ vbar,
+                                      double* __restrict__ tbar) {
+  extern __shared__ double sv[];  // 3 x npl
+  const int f = blockIdx.x, npl = tg.npl, n1 = tg.n + 1, qx = n1 * n1;
+  const long N = tg.N, pn = (long)fg.panels * qx;
+  for (int i = threadIdx.x; i < npl; i += blockDim.x)
+    for (int c = 0; c < 3; c++) sv[c * npl + i] = vbar[c * N + (long)f * npl + i];
+  __syncthreads();
+  const long base = (long)(fg.offset + f) * qx;
+  for (int m = threadIdx.x; m < 3 * qx; m += blockDim.x) {
+    const int c = m / qx, k = m % qx, a = k / n1, b = k % n1;
+    double acc = 0;
+    for (int i = 0; i < npl; i++) acc = fma(__ldg(tg.lx + i * n1 + a) * __ldg(tg.ly + i * n1 + b), sv[c * npl + i], acc);
+    tbar[c * pn + base + k] = acc;
+  }
+}
+
+// One level of the transpose of the downward pass: parents at `level` add
+// the anterpolation of their children's three fields (child_to_parent form).
+__global__ void k_tree_up3(StepGeom fg, int level, double* __restrict__ t) {
+  const int n1 = fg.degree + 1, q = fg.q;
+  const long pn = (long)fg.panels * q;
+  const long np = 6L << (2 * level);
+  const long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (idx >= np * q * 3) return;
+  const int c3 = (int)(idx / (np * q));
+  const long r = idx % (np * q);
+  const long p = level_start(level) + r / q;
+  const int k = (int)(r % q), a = k / n1, b = k % n1;
+  double acc = 0;
+  for (int c = 0; c < 4; c++) {
+    const long ch = level_start(level + 1) + 4 * (p - level_start(level)) + c;
+    const double* lx = fg.child_1d + ((c == 1 || c == 2) ? n1 * n1 : 0);
+    const double* ly = fg.child_1d + (c >= 2 ? n1 * n1 : 0);
+    const double* tc = t + c3 * pn + ch * q;
+    for (int i = 0; i < n1; i++) {
+      double s = 0;
+      for (int j = 0; j < n1; j++) s = fma(__ldg(ly + j * n1 + b), tc[i * n1 + j], s);
+      acc = fma(__ldg(lx + i * n1 + a), s, acc);
+    }
+  }
+  t[c3 * pn + p * q + k] += acc;
+}
+
+// One level of the transpose of the upward pass: children of `level` add the
+// interpolation of their parent's (final) adjoint strengths.
+__global__ void k_tree_down1(StepGeom fg, int level, double* __restrict__ qb) {
+  const int n1 = fg.degree + 1, q = fg.q;
+  const long nc = 6L << (2 * (level + 1));
+  const long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (idx >= nc * q) return;
+  const long ch = level_start(level + 1) + idx / q;
+  const int k = (int)(idx % q), i = k / n1, j = k % n1;
+  const long rel = ch - level_start(level + 1);
+  const long p = level_start(level) + rel / 4;
+  const int c = (int)(rel % 4);
+  const double* lx = fg.child_1d + ((c == 1 || c == 2) ? n1 * n1 : 0) + i * n1;
+  const double* ly = fg.child_1d + (c >= 2 ? n1 * n1 : 0) + j * n1;
+  double acc = 0;
+  for (int a = 0; a < n1; a++) {
+    double s = 0;
+    for (int b = 0; b < n1; b++) s = fma(__ldg(ly + b), qb[p * q + a * n1 + b], s);
+    acc = fma(__ldg(lx + a), s, acc);
+  }
+  qb[ch * q + k] += acc;
+}
+
+// Transposed well-separated interactions: source panel s (blockIdx.x) sums
+// over the target panels t whose list holds s: Qbar_s,k = K sum_t sum_i g c.d,
+// c = Tbar_t,i x x_i, d = y_k - x_i.
+template <bool GUARD>
+__global__ void __launch_bounds__(kT) k_tree_cc_T(StepGeom fg, const int* __restrict__ tstart,
+                                                 const int* __restrict__ ttgt, const double* __restrict__ tbar,
+                                                 double* __restrict__ qbar) {
+  __shared__ double sx[kT], sy[kT], sz[kT], cx[kT], cy[kT], cz[kT];
+  const int s = blockIdx.x, q = fg.q;
+  const long pn = (long)fg.panels * q;
+  const int k = threadIdx.x;
+  double yx = 0, yy = 0, yz = 0;
+  if (k < q) {
+    yx = fg.px[(long)s * q + k];
+    yy = fg.px[pn + (long)s * q + k];
+    yz = fg.px[2 * pn + (long)s * q + k];
+  }
+  double acc = 0;
+  for (int e = tstart[s]; e < tstart[s + 1]; e++) {
+    const long tb = (long)ttgt[e] * q;
+    __syncthreads();
+    if (k < q) {
+      const double x = fg.px[tb + k], y = fg.px[pn + tb + k], z = fg.px[2 * pn + tb + k];
+      const double a = tbar[tb + k], b = tbar[pn + tb + k], c = tbar[2 * pn + tb + k];
+      sx[k] = x;
+      sy[k] = y;
+      sz[k] = z;
+      cx[k] = b * z - c * y;
+      cy[k] = c * x - a * z;
+      cz[k] = a * y - b * x;
+    }
+    __syncthreads();
+    if (k < q)
+      for (int i = 0; i < q; i++) {
+        const double dx = yx - sx[i], dy = yy - sy[i], dz = yz - sz[i];
+        const double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+        double g = recip_nr(fma(0.5, r2, fg.eps));
+        if (GUARD) g = r2 > 0.0 ? g : 0.0;
+        acc = fma(g, fma(cx[i], dx, fma(cy[i], dy, cz[i] * dz)), acc);
+      }
+  }
+  if (k < q) qbar[(long)s * q + k] = kBiotSavart * acc;
+}
+
+// Transposed near field: source leaf sl (blockIdx.x), one thread per source
+// particle, over the target leaves whose near list holds sl.  Writes qbar_j
+// and ybar_j (3 components) of the leaf's particles.
+template <bool GUARD>
+__global__ void __launch_bounds__(512) k_tree_near_T(TreeGeom tg, const int* __restrict__ tstart,
+                                                   const int* __restrict__ ttgt, const double* __restrict__ x,
+                                                   const double* __restrict__ y, const double* __restrict__ z,
+                                                   const double* __restrict__ vbar, const double4* __restrict__ psrc,
+                                                   double* __restrict__ qbar, double* __restrict__ ybar) {
+  extern __shared__ double tile[];  // 6 x npl: target positions, c = vbar x x
+  const int sl = blockIdx.x, npl = tg.npl;
+  const long N = tg.N;
+  double* tx = tile;
+  double* ty = tx + npl;
+  double* tz = ty + npl;
+  double* cx = tz + npl;
+  double* cy = cx + npl;
+  double* cz = cy + npl;
+  const int j = threadIdx.x;
+  const long oj = (long)sl * npl + j;
+  const double4 s = j < npl ? psrc[oj] : make_double4(0, 0, 0, 0);
+  double qb = 0, bx = 0, by = 0, bz = 0;
+  for (int e = tstart[sl]; e < tstart[sl + 1]; e++) {
+    const long tb = (long)ttgt[e] * npl;
+    __syncthreads();
+    for (int i = threadIdx.x; i < npl; i += blockDim.x) {
+      const double a = vbar[tb + i], b = vbar[N + tb + i], c = vbar[2 * N + tb + i];
+      const double px = x[tb + i], py = y[tb + i], pz = z[tb + i];
+      tx[i] = px;
+      ty[i] = py;
+      tz[i] = pz;
+      cx[i] = b * pz - c * py;
+      cy[i] = c * px - a * pz;
+      cz[i] = a * py - b * px;
+    }
+    __syncthreads();
+    if (j < npl)
+      for (int i = 0; i < npl; i++) {
+        const double dx = s.x - tx[i], dy = s.y - ty[i], dz = s.z - tz[i];
+        const double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+        double g = recip_nr(fma(0.5, r2, tg.eps));
+        if (GUARD) g = r2 > 0.0 ? g : 0.0;
+        const double sd = fma(cx[i], dx, fma(cy[i], dy, cz[i] * dz));
+        qb = fma(g, sd, qb);
+        const double t = g * g * sd;
+        bx = fma(g, cx[i], fma(-t, dx, bx));
+        by = fma(g, cy[i], fma(-t, dy, by));
+        bz = fma(g, cz[i], fma(-t, dz, bz));
+      }
+  }
+  if (j < npl) {
+    qbar[oj] = kBiotSavart * qb;
+    ybar[oj] = kBiotSavart * s.w * bx;
+    ybar[N + oj] = kBiotSavart * s.w * by;
+    ybar[2 * N + oj] = kBiotSavart * s.w * bz;
+  }
+}
+
+// 1-D barycentric basis on the leaf's Chebyshev proxies and its derivative,
+// without a range check (displaced particles may leave their leaf).
+__device__ __forceinline__ void bli_free_deriv(double t, double lo, double hi, int n, const BliTable& tab, double* f,
+                                               double* df) {
+  const double range = 0.5 * (hi - lo), offset = 0.5 * (hi + lo);
+  int hit = -1;
+  for (int i = 0; i <= n; i++)
+    if (hit < 0 && fabs(t - (tab.cosv[i] * range + offset)) < 1e-15) hit = i;
+  if (hit >= 0) {
+    const double th = tab.cosv[hit] * range + offset;
+    double sum = 0;
+    for (int a = 0; a <= n; a++) {
+      f[a] = a == hit ? 1.0 : 0.0;
+      df[a] = a == hit ? 0.0 : (tab.w[a] / tab.w[hit]) / (th - (tab.cosv[a] * range + offset));
+      sum += df[a];
+    }
+    df[hit] = -sum;
+    return;
+  }
+  double S = 0, T = 0;
+  for (int k = 0; k <= n; k++) {
+    const double dk = t - (tab.cosv[k] * range + offset);
+    const double r = tab.w[k] / dk;
+    f[k] = r;
+    S += r;
+    T += r / dk;
+  }
+  const double iS = 1.0 / S, TS = T * iS;
+  for (int a = 0; a <= n; a++) {
+    f[a] *= iS;
+    df[a] = f[a] * (TS - 1.0 / (t - (tab.cosv[a] * range + offset)));
+  }
+}
+
+__device__ __forceinline__ void atan_grad2(double u, int iu, double su, double w, int iw, double sw, double* gr) {
+  const double den = 1.0 / (u * u + w * w);
+  gr[0] = gr[1] = gr[2] = 0;
+  gr[iu] += w * su * den;
+  gr[iw] -= u * sw * den;
+}
+
+// Anterpolation adjoint: particle j of tree leaf f (blockIdx.x) adds
+// sum_k B_k(y_j) Qbar_k to qbar_j and q_j sum_k grad B_k(y_j) Qbar_k to ybar_j,
+// B_k = Lx_a(xi(y)) Ly_b(eta(y)) on the leaf's face.
+__global__ void k_tree_sources_T(TreeGeom tg, StepGeom fg, BliTable tab, const double4* __restrict__ psrc,
+                                 const double* __restrict__ qbl, double* __restrict__ qbar,
+                                 double* __restrict__ ybar) {
+  extern __shared__ double sq[];  // the leaf's adjoint proxy strengths, qx
+  const int f = blockIdx.x, npl = tg.npl, n = tg.n, n1 = n + 1, qx = n1 * n1;
+  const long N = tg.N;
+  const int panel = fg.offset + f;
+  for (int k = threadIdx.x; k < qx; k += blockDim.x) sq[k] = qbl[(long)panel * qx + k];
+  __syncthreads();
+  const double* bd = tg.fbounds + 4 * panel;
+  const int face = tg.fface[panel];
+  for (int jj = threadIdx.x; jj < npl; jj += blockDim.x) {
+    const long o = (long)f * npl + jj;
+    const double4 s = psrc[o];
+    double xi, eta;
+    xieta_from_xyz_face(s.x, s.y, s.z, face, xi, eta);
+    double fx[kMaxDegree + 1], dfx[kMaxDegree + 1], fe[kMaxDegree + 1], dfe[kMaxDegree + 1];
+    bli_free_deriv(xi, bd[0], bd[1], n, tab, fx, dfx);
+    bli_free_deriv(eta, bd[2], bd[3], n, tab, fe, dfe);
+    double val = 0, dxi = 0, deta = 0;
+    for (int a = 0; a <= n; a++)
+      for (int b = 0; b <= n; b++) {
+        const double qk = sq[a * n1 + b];
+        val = fma(fx[a] * fe[b], qk, val);
+        dxi = fma(dfx[a] * fe[b], qk, dxi);
+        deta = fma(fx[a] * dfe[b], qk, deta);
+      }
+    double gxi[3], geta[3];
+    const double X = s.x, Y = s.y, Z = s.z;
+    switch (face) {
+      case 0: atan_grad2(Y, 1, 1, X, 0, 1, gxi); atan_grad2(Z, 2, 1, X, 0, 1, geta); break;
+      case 1: atan_grad2(-X, 0, -1, Y, 1, 1, gxi); atan_grad2(Z, 2, 1, Y, 1, 1, geta); break;
+      case 2: atan_grad2(Y, 1, 1, X, 0, 1, gxi); atan_grad2(-Z, 2, -1, X, 0, 1, geta); break;
+      case 3: atan_grad2(-X, 0, -1, Y, 1, 1, gxi); atan_grad2(-Z, 2, -1, Y, 1, 1, geta); break;
+      case 4: atan_grad2(Y, 1, 1, Z, 2, 1, gxi); atan_grad2(-X, 0, -1, Z, 2, 1, geta); break;
+      default: atan_grad2(-Y, 1, -1, Z, 2, 1, gxi); atan_grad2(-X, 0, -1, Z, 2, 1, geta); break;
+    }
+    qbar[o] += val;
+    for (int c = 0; c < 3; c++) ybar[c * N + o] += s.w * (dxi * gxi[c] + deta * geta[c]);
+  }
+}
+
+}  // namespace
+
+void launch_tree_velocity_adjoint(const TreeGeom& tg, const StepGeom& fg, const BliTable& ftab,
+                                  const TreeAdjointLists& tl, const double* x, const double* y, const double* z,
+                                  const double* vbar, const double4* psrc, double* tbar, double* qbl, double* qbar,
+                                  double* ybar, cudaStream_t st) {
+  const int qx = fg.q, Pf = fg.panels;
+  const long pn = (long)Pf * qx;
+  // leaf interpolation, transposed; non-leaf rows start at zero
+  cudaMemsetAsync(tbar, 0, sizeof(double) * 3 * pn, st);
+  SB_LAUNCH(k_tree_to_particles_T, (unsigned)fg.leaves, kT, sizeof(double) * 3 * tg.npl, st, tg, fg, vbar, tbar);
+  // downward pass, transposed: accumulate up the tree
+  for (int lev = fg.levels - 2; lev >= 0; lev--) {
+    const long work = (6L << (2 * lev)) * qx * 3;
+    SB_LAUNCH(k_tree_up3, blocks_for(work, 256), 256, 0, st, fg, lev, tbar);
+  }
+  // well-separated interactions, transposed
+  if (fg.eps > 0)
+    SB_LAUNCH(k_tree_cc_T<false>, (unsigned)Pf, kT, 0, st, fg, tl.cc_tstart, tl.cc_ttgt, tbar, qbl);
+  else
+    SB_LAUNCH(k_tree_cc_T<true>, (unsigned)Pf, kT, 0, st, fg, tl.cc_tstart, tl.cc_ttgt, tbar, qbl);
+  // upward pass, transposed: interpolate down the tree
+  for (int lev = 0; lev < fg.levels - 1; lev++) {
+    const long work = (6L << (2 * (lev + 1))) * qx;
+    SB_LAUNCH(k_tree_down1, blocks_for(work, 256), 256, 0, st, fg, lev, qbl);
+  }
+  // near field, transposed (writes qbar, ybar), then the anterpolation adjoint (adds)
+  const size_t sm = sizeof(double) * 6 * tg.npl;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_tree_near_T<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+    cudaFuncSetAttribute(k_tree_near_T<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+    attr = true;
+  }
+  const int nth = tg.npl <= 256 ? 256 : 512;
+  if (tg.eps > 0)
+    SB_LAUNCH(k_tree_near_T<false>, (unsigned)fg.leaves, nth, sm, st, tg, tl.near_tstart, tl.near_ttgt, x, y, z, vbar,
+              psrc, qbar, ybar);
+  else
+    SB_LAUNCH(k_tree_near_T<true>, (unsigned)fg.leaves, nth, sm, st, tg, tl.near_tstart, tl.near_ttgt, x, y, z, vbar,
+              psrc, qbar, ybar);
+  SB_LAUNCH(k_tree_sources_T, (unsigned)fg.leaves, kT, sizeof(double) * qx, st, tg, fg, ftab, psrc, qbl, qbar, ybar);
+}
+
+}  // namespace sbslpm

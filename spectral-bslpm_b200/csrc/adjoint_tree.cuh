@@ -1,0 +1,29 @@
+// Adjoint of the decoupled-degree treecode velocity; adjoint_tree.cu.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "bve_kernels.cuh"
+
+namespace sbslpm {
+
+// Transposed interaction lists (device CSR): for each source leaf the target
+// leaves whose near list holds it (relative leaf indices), for each source
+// panel the target panels whose well-separated list holds it.
+struct TreeAdjointLists {
+  const int* near_tstart;
+  const int* near_ttgt;
+  const int* cc_tstart;
+  const int* cc_ttgt;
+};
+
+// Given vbar [3][N] (adjoint of one stage velocity) and that stage's particle
+// sources psrc (positions, strengths), writes qbar [N] and ybar [3][N], the
+// adjoints of the particle source strengths and positions.  Scratch: tbar
+// [3][tree panels * q], qbl [tree panels * q].
+void launch_tree_velocity_adjoint(const TreeGeom& tg, const StepGeom& fg, const BliTable& ftab,
+                                  const TreeAdjointLists& tl, const double* x, const double* y, const double* z,
+                                  const double* vbar, const double4* psrc, double* tbar, double* qbl, double* qbar,
+                                  double* ybar, cudaStream_t st);
+
+}  // namespace sbslpm

@@ -521,7 +521,8 @@ sbslpm_status sbslpm_destroy(sbslpm_ctx* c) {
                   c->cc_src, c->fsrc, c->psrc, c->fsrcf, c->psrcf, c->ftgt, c->gx, c->near, c->s_fd,
                   c->s_ntan, c->s_pow15, c->s_filt, c->s_ptan, c->s_pface, c->s_ustart, c->s_umem, c->src2,
                   c->srcf2, c->tend, c->avor, c->adj_src, c->adj_vbar, c->adj_q, c->adj_y, c->adj_part,
-                  c->adj_w, c->adj_vel};
+                  c->adj_w, c->adj_vel, c->adj_near_ts, c->adj_near_tt, c->adj_cc_ts, c->adj_cc_tt, c->adj_tbar,
+                  c->adj_qbl};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (c->h_err) cudaFreeHost(c->h_err);

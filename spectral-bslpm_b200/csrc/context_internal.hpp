@@ -88,6 +88,8 @@ struct sbslpm_ctx {
   double *adj_vbar = nullptr, *adj_q = nullptr, *adj_y = nullptr, *adj_part = nullptr, *adj_w = nullptr,
          *adj_vel = nullptr;
   int adj_groups = 1;
+  int *adj_near_ts = nullptr, *adj_near_tt = nullptr, *adj_cc_ts = nullptr, *adj_cc_tt = nullptr;
+  double *adj_tbar = nullptr, *adj_qbl = nullptr;
 
   cudaStream_t stream() const { return user_stream_set ? user_stream : own_stream; }
 };

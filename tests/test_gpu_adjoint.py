@@ -130,3 +130,53 @@ def test_twenty_step_gradient_matches_finite_differences(sb):
     # and relative to its own derivative wherever that is not near zero
     big = np.abs(ads) >= 0.1 * rms
     assert big.sum() >= 56 and (np.abs(fds - ads)[big] / np.abs(ads[big])).max() <= 1e-5
+
+
+def tree_ctx(sb, levels, dt, theta=0.7, degree=8):
+    cfg = sb.config_default(levels=levels, interp_degree=3, kernel_eps=1e-4, omega=2 * np.pi, dt=dt,
+                            precision=sb.FP64, fmm_theta=theta, proxy_degree=degree, leaf_size=256)
+    return sb.Context(cfg)
+
+
+def test_treecode_adjoint_step_dot_product(sb):
+    _, f, w0, wn = gaussian_vortex_state(sb, 5, 0.01, 1e-2)
+    ctx = tree_ctx(sb, 5, 0.01)
+    rng = np.random.default_rng(9)
+    wbar_next = torch.from_numpy(rng.standard_normal(tuple(wn.shape))).cuda()
+    wbar = torch.empty_like(wn)
+    ctx.bve_adjoint_step(*f, wn, wbar_next, wbar)
+
+    def step(w):
+        v = w.clone()
+        vel = [torch.zeros_like(v) for _ in range(3)]
+        ctx.bve_back_rk4_step(*f, v, *vel)
+        return v
+
+    for seed in range(3):
+        d = torch.from_numpy(np.random.default_rng(70 + seed).standard_normal(tuple(wn.shape))).cuda()
+        h = 1e-6
+        fd = float((wbar_next * (step(wn + h * d) - step(wn - h * d))).sum()) / (2 * h)
+        ad = float((wbar * d).sum())
+        assert abs(fd - ad) <= 1e-6 * abs(ad), (seed, fd, ad)
+
+
+def test_treecode_gradient_matches_direct_sum_adjoint(sb):
+    """The 20-step loss gradient through the treecode's adjoint against the
+    float64 direct-sum adjoint's (the reference gradient): they differ by the
+    treecode's approximation error."""
+    ctxd, f, w0, wn = gaussian_vortex_state(sb, 5, 0.01, 1e-2)
+    ctxt = tree_ctx(sb, 5, 0.01)
+    area = f[3]
+    grads = []
+    for ctx in (ctxd, ctxt):
+        v = w0.clone()
+        vel = [torch.zeros_like(v) for _ in range(3)]
+        ctx.bve_run(*f, v, *vel, nsteps=20)
+        x = wn.clone().requires_grad_()
+        out = sb.bve_rollout(ctx, *f, x, 20)
+        (0.5 * (area * (out - v) ** 2).sum()).backward()
+        grads.append(x.grad.clone())
+    gd, gt = grads
+    rel = float((gt - gd).norm() / gd.norm())
+    print("treecode vs direct-sum adjoint gradient: relative L2 %.2e" % rel)
+    assert rel <= 1e-5, rel
