@@ -615,6 +615,7 @@ def main():
     ach64 = PAIR_FLOP * pairs64 / (ms_int64 * 1e-3) / 1e12
     peak64 = sb.measure_fma_peak(1, 50.0) / 1e12
     share = 4 * ms_int / ms_per_step
+    tune32, tune64 = ctx32.near_tuning(), ctx64.near_tuning()
 
     # ---- batched ensemble ----------------------------------------------------
     ens = None if args.no_ensemble else ensemble_bench(sb, torch, dev, flush, min(args.steps, 20))
@@ -674,7 +675,10 @@ def main():
             "config": dict(workload_config(), parallelism=f"replicas x{world}" if world > 1 else "1 GPU"),
             "e2e": {"value": e2e, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
-            "roofline": {"bound": "fp32", "kernel": "k_bltc_near32 (near-field particle pairs, 256 x 256 tiles)",
+            "roofline": {"bound": "fp32", "kernel": "k_bltc_near32_batch (near-field particle pairs, 256 x 256 "
+                         "leaf tiles, one-member table)",
+                         "launch_shape": {"threads": tune32[0], "targets_per_thread": tune32[1],
+                                          "splits": tune32[2], "candidates_timed": tune32[3]},
                          "achieved": achieved, "peak": peak_meas, "unit": "TFLOP/s", "frac": achieved / peak_meas,
                          "traffic": NEAR_TRAFFIC, "traffic_source": "profiles/k_bltc_near32_levels7.md "
                          "(dram__bytes_read.sum + dram__bytes_write.sum of one launch)",
@@ -683,6 +687,7 @@ def main():
                          "peak_source": "measured f32 FMA-chain throughput on this GPU (sbslpm_measure_fma_peak); "
                                         "MEASURED_PEAKS.json has no CUDA-core peak"},
             "fp64_plain": {"steps_per_s": fp64_sps, "ms_per_step": 1e3 / fp64_sps, "near_kernel_tflops": ach64,
+                           "near_launch_shape": list(tune64[:3]),
                            "fp64_fma_peak_tflops": peak64, "frac": ach64 / peak64},
             "speedup_mixed_vs_fp64_plain": value / world / fp64_sps,
             "fp64_direct_sum": {"steps_per_s": 1.0 / direct_s,

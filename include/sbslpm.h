@@ -368,6 +368,15 @@ sbslpm_status sbslpm_direct_sum_bve_noalloc(long n_targets, const double* tx, co
  * the context (those of the last stage run), timed with CUDA events on the
  * context's stream.  *pairs receives the pair evaluations per launch. */
 sbslpm_status sbslpm_time_interactions(sbslpm_ctx* ctx, int reps, double* ms_per_launch, double* pairs);
+/* Treecode contexts (proxy_degree > 0): the near-field launch shape.  The
+ * first step of a context times every shape (threads per block 64 | 128 |
+ * 256 x targets per thread covering a treecode leaf, 1..4 source-list
+ * splits) and keeps the fastest; sbslpm_set_near_tuning fixes one instead
+ * (the split count sets the order in which a target's near-field partial
+ * sums are added).  shape[0..3] = threads, targets per thread, splits,
+ * candidates timed. */
+sbslpm_status sbslpm_set_near_tuning(sbslpm_ctx* ctx, int threads, int targets_per_thread, int splits);
+sbslpm_status sbslpm_near_tuning(const sbslpm_ctx* ctx, int* shape, double* ms_per_launch);
 /* CUDA-core fused multiply-add throughput of this GPU, measured with
  * independent FMA chains on every SM for about ms milliseconds: kind 0 =
  * float32, 1 = float64.  Returns FLOP/s (2 per FMA) in *flops. */

@@ -135,6 +135,8 @@ def lib() -> ctypes.CDLL:
     L.sbslpm_batch_pairs.argtypes = [_VP, _D, _D]
     L.sbslpm_batch_set_tuning.argtypes = [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     L.sbslpm_time_interactions.argtypes = [_VP, ctypes.c_int, _D, _D]
+    L.sbslpm_set_near_tuning.argtypes = [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    L.sbslpm_near_tuning.argtypes = [_VP, _I, _D]
     L.sbslpm_measure_fma_peak.argtypes = [ctypes.c_int, ctypes.c_double, _D]
     _lib = L
     return L
@@ -396,6 +398,18 @@ class Context:
         _check(lib().sbslpm_bve_adjoint_step(self._h, *[_dev(t, n, lq) for t, n in (
             (xcos, "xcos"), (ycos, "ycos"), (zcos, "zcos"), (area, "area"), (vors, "vors"),
             (vors_bar_next, "vors_bar_next"), (vors_bar, "vors_bar"))]), "sbslpm_bve_adjoint_step")
+
+    def set_near_tuning(self, threads: int, targets_per_thread: int, splits: int):
+        """Fix the treecode's near-field launch shape instead of autotuning it."""
+        _check(lib().sbslpm_set_near_tuning(self._h, int(threads), int(targets_per_thread), int(splits)),
+               "sbslpm_set_near_tuning")
+
+    def near_tuning(self):
+        """(threads, targets per thread, splits, candidates timed, ms per near launch)."""
+        shape = (ctypes.c_int * 4)()
+        ms = ctypes.c_double()
+        _check(lib().sbslpm_near_tuning(self._h, shape, ctypes.byref(ms)), "sbslpm_near_tuning")
+        return (*[int(v) for v in shape], ms.value)
 
     def time_interactions(self, reps: int = 5):
         """(ms per launch, pair evaluations per launch) of the interaction kernel alone."""

@@ -78,6 +78,7 @@ sbslpm_status sbslpm_bve_adjoint_step(sbslpm_ctx* c, const double* x, const doub
   if (c->cfg.tracer_count != 0)
     return set_last_error("the adjoint step needs a context without tracers"), SBSLPM_ERR_CONFIG;
   SB_TRY(adjoint_setup(c));
+  SB_TRY(near_autotune(c, x, y, z, area, vors));
   cudaStream_t st = c->stream();
   const size_t ln = (size_t)c->A * c->q, pn = (size_t)c->P * c->q, off = (size_t)c->off * c->q;
   const double dt = c->cfg.dt;

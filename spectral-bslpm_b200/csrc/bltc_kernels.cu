@@ -193,13 +193,6 @@ __device__ __forceinline__ void bltc_near64_body(const TreeGeom& tg, int f, int 
   }
 }
 
-template <int NT, int TPT, bool GUARD>
-__global__ void __launch_bounds__(NT)
-    k_bltc_near64(TreeGeom tg, const double* __restrict__ x, const double* __restrict__ y,
-                  const double* __restrict__ z, const double4* __restrict__ psrc, double* __restrict__ out) {
-  bltc_near64_body<NT, TPT, GUARD>(tg, blockIdx.x, blockIdx.y, gridDim.y, x, y, z, psrc, out);
-}
-
 // Batched members (member blockIdx.z): sources psrc + m N, partials out + m splits 3N.
 template <int NT, int TPT, bool GUARD>
 __global__ void __launch_bounds__(NT)
@@ -296,13 +289,6 @@ __device__ __forceinline__ void bltc_near32_body(const TreeGeom& tg, const StepG
 
 template <int NT, int TPT, bool GUARD>
 __global__ void __launch_bounds__(NT)
-    k_bltc_near32(TreeGeom tg, StepGeom fg, const double* __restrict__ x, const double* __restrict__ y,
-                  const double* __restrict__ z, const float4* __restrict__ psrcf, double* __restrict__ out) {
-  bltc_near32_body<NT, TPT, GUARD>(tg, fg, blockIdx.x, blockIdx.y, gridDim.y, x, y, z, psrcf, out);
-}
-
-template <int NT, int TPT, bool GUARD>
-__global__ void __launch_bounds__(NT)
     k_bltc_near32_batch(const BatchMember* __restrict__ mem, const double* __restrict__ x,
                         const double* __restrict__ y, const double* __restrict__ z,
                         const float4* __restrict__ psrcf, double* __restrict__ out) {
@@ -393,32 +379,6 @@ void launch_bltc_sources(const TreeGeom& tg, const StepGeom& fg, const BliTable&
   }
   SB_LAUNCH(k_bltc_sources, (unsigned)fg.leaves, kThreads, smem, st, tg, fg, tab, stage, dt_s, vprev, x, y, z, vors,
             area, psrc, psrcf, proxy, mixed ? 1 : 0);
-}
-
-void launch_bltc_near(const TreeGeom& tg, const StepGeom& fg, int precision, const double* x, const double* y,
-                      const double* z, const double4* psrc, const float4* psrcf, double* v, int splits,
-                      cudaStream_t st) {
-  const bool guard = !(tg.eps > 0);
-  const dim3 grid((unsigned)fg.leaves, (unsigned)splits);
-  // two targets per thread: each staged source feeds two pair evaluations
-#define SB_NEAR(NT, TPT)                                                                                      \
-  do {                                                                                                        \
-    if (precision == SBSLPM_MIXED) {                                                                          \
-      const size_t sm32 = sizeof(float4) * 2 * ((tg.npl + 1) / 2);                                           \
-      if (guard) SB_LAUNCH((k_bltc_near32<NT, TPT, true>), grid, NT, sm32, st, tg, fg, x, y, z, psrcf, v);     \
-      else SB_LAUNCH((k_bltc_near32<NT, TPT, false>), grid, NT, sm32, st, tg, fg, x, y, z, psrcf, v);          \
-    } else {                                                                                                  \
-      if (guard) SB_LAUNCH((k_bltc_near64<NT, TPT, true>), grid, NT, sizeof(double4) * tg.npl, st, tg, x, y, z, \
-                           psrc, v);                                                                          \
-      else SB_LAUNCH((k_bltc_near64<NT, TPT, false>), grid, NT, sizeof(double4) * tg.npl, st, tg, x, y, z,      \
-                     psrc, v);                                                                                \
-    }                                                                                                         \
-  } while (0)
-  if (tg.npl <= 64) SB_NEAR(64, 1);
-  else if (tg.npl <= 128) SB_NEAR(64, 2);
-  else if (tg.npl <= 256) SB_NEAR(128, 2);
-  else SB_NEAR(256, 2);
-#undef SB_NEAR
 }
 
 void launch_bltc_sources_batch(const BatchMember* mem, int members, int leaves, int npl, int nmax, int stage,

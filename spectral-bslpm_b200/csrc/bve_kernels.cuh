@@ -108,9 +108,6 @@ void launch_bltc_sources(const TreeGeom& tg, const StepGeom& fg, const BliTable&
                          const double* area, double4* psrc, float4* psrcf, double4* proxy, bool mixed,
                          cudaStream_t st);
 // near: splits x 3 x particles partial sums (splits = source-list splits per target leaf)
-void launch_bltc_near(const TreeGeom& tg, const StepGeom& fg, int precision, const double* x, const double* y,
-                      const double* z, const double4* psrc, const float4* psrcf, double* near, int splits,
-                      cudaStream_t st);
 // v = near splits summed + far field interpolated from the leaf proxies
 void launch_bltc_to_particles(const TreeGeom& tg, const StepGeom& fg, const double* tgt, const double* near,
                               int splits, double* v, cudaStream_t st);

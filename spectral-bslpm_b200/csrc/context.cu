@@ -178,7 +178,7 @@ sbslpm_status precompute_tree(sbslpm_ctx* c) {
   SB_CUDA(cudaMemcpy(c->fsrc, init.data(), sizeof(double4) * pn, cudaMemcpyHostToDevice));
   SB_TRY(dalloc(&c->ftgt, 3 * pn));
   SB_TRY(dalloc(&c->psrc, N));
-  SB_TRY(dalloc(&c->near, (size_t)c->near_splits * 3 * N));
+  SB_TRY(dalloc(&c->near, (size_t)4 * 3 * N));
   if (c->cfg.precision == SBSLPM_MIXED) {
     SB_TRY(dalloc(&c->fsrcf, pn));
     SB_TRY(dalloc(&c->psrcf, N));
@@ -281,7 +281,8 @@ void velocity_eval(sbslpm_ctx* c, int stage, double dt_s, const double* vprev, c
     launch_upward_fused(fg, 2, 0, 0.0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, c->fsrc, mixed, st);
     launch_interactions_only(fg, c->cfg.precision, c->fsrc, c->ftgt, st);
     launch_downward_fused(fg, c->ftgt, nullptr, st);
-    launch_bltc_near(c->tgeom, fg, c->cfg.precision, x, y, z, c->psrc, c->psrcf, c->near, c->near_splits, st);
+    launch_bltc_near_batch(c->self, 1, fg.leaves, c->npl, c->cfg.kernel_eps, c->cfg.precision, x, y, z, c->psrc,
+                           c->psrcf, c->near, c->near_splits, c->near_nt, c->near_tpt, st);
     launch_bltc_to_particles(c->tgeom, fg, c->ftgt, c->near, c->near_splits, v, st);
     return;
   }
@@ -362,6 +363,53 @@ sbslpm_status capture_graph(sbslpm_ctx* c, cudaGraphExec_t* graph, const std::fu
   SB_CUDA(cudaGraphInstantiate(graph, g, 0));
   cudaGraphDestroy(g);
   return SBSLPM_OK;
+}
+
+// Times every near-field launch shape (threads x targets per thread covering a
+// treecode leaf, 1..4 source-list splits) on the stage-0 sources and keeps the
+// fastest.  Runs once per context, before the first step, outside any capture.
+sbslpm_status near_autotune(sbslpm_ctx* c, const double* x, const double* y, const double* z, const double* area,
+                            const double* vors) {
+  if (!c->tree || c->near_tuned) return SBSLPM_OK;
+  cudaStream_t st = c->stream();
+  const int prec = c->cfg.precision;
+  launch_bltc_sources(c->tgeom, c->fgeom, c->ftab, 0, 0.0, nullptr, x, y, z, vors, area, c->psrc, c->psrcf, c->fsrc,
+                      prec == SBSLPM_MIXED, st);
+  const int shapes[][2] = {{64, 4}, {128, 2}, {256, 1}, {256, 2}, {64, 2}, {64, 1}, {128, 1}};
+  cudaEvent_t e0, e1;
+  SB_CUDA(cudaEventCreate(&e0));
+  SB_CUDA(cudaEventCreate(&e1));
+  double best = 1e30;
+  int cand = 0;
+  for (const auto& sh : shapes) {
+    if (sh[0] * sh[1] < c->npl || sh[0] * sh[1] >= 4 * c->npl) continue;
+    for (int sp = 1; sp <= 4; sp++) {
+      auto run = [&] {
+        launch_bltc_near_batch(c->self, 1, c->fgeom.leaves, c->npl, c->cfg.kernel_eps, prec, x, y, z, c->psrc,
+                               c->psrcf, c->near, sp, sh[0], sh[1], st);
+      };
+      run();
+      SB_CUDA(cudaEventRecord(e0, st));
+      for (int r = 0; r < 5; r++) run();
+      SB_CUDA(cudaEventRecord(e1, st));
+      SB_CUDA(cudaEventSynchronize(e1));
+      float ms = 0;
+      SB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      cand++;
+      if (ms / 5 < best) {
+        best = ms / 5;
+        c->near_nt = sh[0];
+        c->near_tpt = sh[1];
+        c->near_splits = sp;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c->near_candidates = cand;
+  c->near_tuned_ms = best;
+  c->near_tuned = true;
+  return finish(c);
 }
 
 }  // namespace sbslpm
@@ -507,6 +555,20 @@ sbslpm_status sbslpm_create(const sbslpm_config* cfg, sbslpm_ctx** out) {
     return s;
   }
   fill_geom(c);
+  if (c->tree) {
+    BatchMember m{};
+    m.fg = c->fgeom;
+    m.tg = c->tgeom;
+    m.tab = c->ftab;
+    m.fsrc = c->fsrc;
+    m.ftgt = c->ftgt;
+    std::vector<BatchMember> one(1, m);
+    s = upload(&c->self, one);
+    if (s != SBSLPM_OK) {
+      sbslpm_destroy(c);
+      return s;
+    }
+  }
   *out = c;
   return SBSLPM_OK;
 }
@@ -522,7 +584,7 @@ sbslpm_status sbslpm_destroy(sbslpm_ctx* c) {
                   c->s_ntan, c->s_pow15, c->s_filt, c->s_ptan, c->s_pface, c->s_ustart, c->s_umem, c->src2,
                   c->srcf2, c->tend, c->avor, c->adj_src, c->adj_vbar, c->adj_q, c->adj_y, c->adj_part,
                   c->adj_w, c->adj_vel, c->adj_near_ts, c->adj_near_tt, c->adj_cc_ts, c->adj_cc_tt, c->adj_tbar,
-                  c->adj_qbl};
+                  c->adj_qbl, c->self};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (c->h_err) cudaFreeHost(c->h_err);
@@ -566,6 +628,7 @@ sbslpm_status sbslpm_bve_step(sbslpm_ctx* c, const double* x, const double* y, c
   if (!c || bad(x) || bad(y) || bad(z) || bad(area) || bad(vors) || bad(vel_x) || bad(vel_y) || bad(vel_z) ||
       (c->cfg.tracer_count > 0 && bad(tracers)))
     return SBSLPM_ERR_ARG;
+  SB_TRY(near_autotune(c, x, y, z, area, vors));
   enqueue_step(c, x, y, z, area, vors, vel_x, vel_y, vel_z, tracers);
   return finish(c);
 }
@@ -576,6 +639,7 @@ sbslpm_status sbslpm_bve_run(sbslpm_ctx* c, const double* x, const double* y, co
   if (!c || bad(x) || bad(y) || bad(z) || bad(area) || bad(vors) || bad(vel_x) || bad(vel_y) || bad(vel_z) ||
       (c->cfg.tracer_count > 0 && bad(tracers)) || nsteps < 0)
     return SBSLPM_ERR_ARG;
+  SB_TRY(near_autotune(c, x, y, z, area, vors));
   GraphKey key{{x, y, z, area, vors, vel_x, vel_y, vel_z, tracers}};
   cudaStream_t st = c->stream();
   if (!c->graph || !(key == c->graph_key)) {
@@ -726,8 +790,9 @@ sbslpm_status sbslpm_time_interactions(sbslpm_ctx* c, int reps, double* ms_per_l
     SB_CUDA(cudaEventCreate(&b));
     SB_CUDA(cudaEventRecord(a, st));
     for (int r = 0; r < reps; r++)
-      launch_bltc_near(c->tgeom, c->fgeom, c->cfg.precision, c->gx, c->gx + c->tgeom.N, c->gx + 2 * c->tgeom.N,
-                       c->psrc, c->psrcf, c->near, c->near_splits, st);
+      launch_bltc_near_batch(c->self, 1, c->fgeom.leaves, c->npl, c->cfg.kernel_eps, c->cfg.precision, c->gx,
+                             c->gx + c->tgeom.N, c->gx + 2 * c->tgeom.N, c->psrc, c->psrcf, c->near, c->near_splits,
+                             c->near_nt, c->near_tpt, st);
     SB_CUDA(cudaEventRecord(b, st));
     SB_CUDA(cudaEventSynchronize(b));
     float tms = 0;
@@ -753,6 +818,36 @@ sbslpm_status sbslpm_time_interactions(sbslpm_ctx* c, int reps, double* ms_per_l
   *ms_per_launch = ms / reps;
   if (pairs) *pairs = (double)c->I * c->q * c->q;
   return finish(c);
+}
+
+sbslpm_status sbslpm_set_near_tuning(sbslpm_ctx* c, int threads, int targets_per_thread, int splits) {
+  if (!c || !c->tree) return SBSLPM_ERR_ARG;
+  const bool ok = ((threads == 64 && (targets_per_thread == 1 || targets_per_thread == 2 || targets_per_thread == 4)) ||
+                   (threads == 128 && (targets_per_thread == 1 || targets_per_thread == 2)) ||
+                   (threads == 256 && (targets_per_thread == 1 || targets_per_thread == 2))) &&
+                  threads * targets_per_thread >= c->npl && splits >= 1 && splits <= 4;
+  if (!ok) return set_last_error("unsupported near-field launch shape"), SBSLPM_ERR_ARG;
+  c->near_nt = threads;
+  c->near_tpt = targets_per_thread;
+  c->near_splits = splits;
+  c->near_candidates = 0;
+  c->near_tuned_ms = 0;
+  c->near_tuned = true;
+  if (c->graph) {
+    cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+  }
+  return SBSLPM_OK;
+}
+
+sbslpm_status sbslpm_near_tuning(const sbslpm_ctx* c, int* shape, double* ms_per_launch) {
+  if (!c || !c->tree || !shape || !ms_per_launch) return SBSLPM_ERR_ARG;
+  shape[0] = c->near_nt;
+  shape[1] = c->near_tpt;
+  shape[2] = c->near_splits;
+  shape[3] = c->near_candidates;
+  *ms_per_launch = c->near_tuned_ms;
+  return SBSLPM_OK;
 }
 
 sbslpm_status sbslpm_measure_fma_peak(int kind, double ms_target, double* flops) {

@@ -61,8 +61,12 @@ struct sbslpm_ctx {
   int *fface = nullptr, *near_start = nullptr, *near_src = nullptr, *cc_start = nullptr, *cc_src = nullptr;
   double4 *fsrc = nullptr, *psrc = nullptr;
   double* gx = nullptr;  // [3][particles]: the particle grid, for timing the near kernel alone
-  double* near = nullptr;  // [near_splits][3][particles] near-field partial sums
-  int near_splits = 2;
+  double* near = nullptr;  // [4][3][particles] near-field partial sums (near_splits in use)
+  int near_splits = 2, near_nt = 128, near_tpt = 2;  // near-field launch shape (autotuned on the first step)
+  bool near_tuned = false;
+  int near_candidates = 0;
+  double near_tuned_ms = 0;
+  sbslpm::BatchMember* self = nullptr;  // this context's treecode as a one-member table (shaped near-field launches)
   float4 *fsrcf = nullptr, *psrcf = nullptr;
   double* ftgt = nullptr;
   sbslpm::BliTable ftab{};
@@ -144,6 +148,8 @@ void bli_table(int n, BliTable& t);
 sbslpm_status build_tree_tables(int L, int d, const std::vector<sbslpm_panel>& grid, int leaf_size, int n,
                                 TreeTables& t);
 void build_tree_lists(const TreeTables& t, double theta, TreeLists& l);
+sbslpm_status near_autotune(sbslpm_ctx* c, const double* x, const double* y, const double* z, const double* area,
+                            const double* vors);
 sbslpm_status capture_graph(sbslpm_ctx* c, cudaGraphExec_t* graph, const std::function<void()>& body);
 
 }  // namespace sbslpm

@@ -44,8 +44,10 @@ def base_cfg(sb, precision, **kw):
                              precision=precision, leaf_size=256, **kw)
 
 
-def single_step(sb, precision, theta, pdeg, xyza, vor):
+def single_step(sb, precision, theta, pdeg, xyza, vor, tuning=(128, 2, 2)):
     ctx = sb.Context(base_cfg(sb, precision, fmm_theta=theta, proxy_degree=pdeg))
+    if tuning:
+        ctx.set_near_tuning(*tuning)
     v = vor.clone()
     vel = [torch.zeros_like(v) for _ in range(3)]
     ctx.bve_back_rk4_step(*xyza, v, *vel)
