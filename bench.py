@@ -297,21 +297,32 @@ def ensemble_bench(sb, torch, dev, flush, steps):
     batch = sb.Batch(cfg, theta, pdeg)
     v = T(vors)
     vel = torch.zeros((ENS_MEMBERS, 3) + base.shape, dtype=torch.float64, device=dev)
-    batch.run(*xyza, v, vel, nsteps=3)  # autotune on the first step, graph capture, warm-up
-    torch.cuda.synchronize()
     st = torch.cuda.current_stream()
+
+    def time_mode(mode, nsteps):
+        batch.set_cc_mode(mode)
+        batch.run(*xyza, v, vel, nsteps=3)  # (autotune on the first step,) graph capture, warm-up
+        torch.cuda.synchronize()
+        out = []
+        for _ in range(nsteps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            batch.run(*xyza, v, vel, nsteps=1)
+            e1.record(st)
+            e1.synchronize()
+            out.append(e0.elapsed_time(e1))
+        return sum(out) / len(out)
+
+    # the well-separated interactions in each fixed mode, for comparison
+    ms_cuda_cores = time_mode(batch.CC_CUDA_CORES, max(3, steps // 4))
+    ms_tc3 = time_mode(batch.CC_TC_3XTF32, max(3, steps // 4))
+    _, union_pairs, mma_flops = batch.cc_info()
+    ms_tf32 = time_mode(batch.CC_TC_TF32, max(3, steps // 4))
+    # the headline: the mode the autotuner chose for each proxy-degree group
     launches0 = sb.kernel_launches()
-    ts = []
-    for _ in range(steps):
-        flush.zero_()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(st)
-        batch.run(*xyza, v, vel, nsteps=1)
-        e1.record(st)
-        e1.synchronize()
-        ts.append(e0.elapsed_time(e1))
-    launches = sb.kernel_launches() - launches0
-    ms = sum(ts) / len(ts)
+    ms = time_mode(batch.CC_AUTO, steps)
+    launches_per_step = (sb.kernel_launches() - launches0) / (steps + 3)  # three warm-up steps and the timed ones
     near_pairs, far_pairs = batch.pairs()
     nt, tpt, splits, cand, near_ms = batch.tuning()
 
@@ -343,12 +354,18 @@ def ensemble_bench(sb, torch, dev, flush, steps):
     member_sps = ENS_MEMBERS * 1e3 / ms
     return {
         "ensemble_steps_per_s": 1e3 / ms, "member_steps_per_s": member_sps, "ms_per_step": ms,
-        "members": ENS_MEMBERS, "particles_per_member": int(g.x.size), "gpu_launches_per_step": launches / steps,
+        "members": ENS_MEMBERS, "particles_per_member": int(g.x.size), "gpu_launches_per_step": launches_per_step,
         "pairs_per_s": 4 * (near_pairs + far_pairs) / (ms * 1e-3),
         "near_pairs_per_eval": near_pairs, "far_pairs_per_eval": far_pairs,
         "near_tflops": PAIR_FLOP * near_pairs / (near_ms * 1e-3) / 1e12,
         "autotune": {"threads": nt, "targets_per_thread": tpt, "splits": splits, "candidates": cand,
                      "near_ms": near_ms},
+        "well_separated": {"headline_mode": "autotuned per proxy-degree group (CUDA-core float32 pairs or the "
+                                            "tensor-core 3xTF32 GEMM over the group's members)",
+                           "groups": batch.cc_groups(), "union_cluster_pairs_per_eval": union_pairs,
+                           "useful_proxy_pairs_per_eval": far_pairs, "mma_flops_per_eval_3xtf32": mma_flops,
+                           "ms_per_step_cuda_core_pairs": ms_cuda_cores, "ms_per_step_tensor_core_3xtf32": ms_tc3,
+                           "ms_per_step_tensor_core_tf32_single_pass": ms_tf32},
         "fp64_plain_single_member_steps_per_s": fp64_sps,
         "speedup_member_steps_vs_fp64_plain": member_sps / fp64_sps,
         "accuracy_step1_vs_fp64_direct": acc,
@@ -369,10 +386,13 @@ def profile_run(sb, torch, dev, args):
         rng = np.random.default_rng(2026)
         M = args.members
         theta, pdeg = rng.uniform(0.5, 0.8, M), rng.choice([6, 8, 10], M)
+        if args.degree:
+            pdeg[:] = args.degree
         cfg = sb.config_default(levels=ENS_LEVELS, interp_degree=DEGREE, kernel_eps=EPS, omega=OMEGA, dt=DT,
                                 precision=sb.MIXED, leaf_size=LEAF_SIZE)
         batch = sb.Batch(cfg, theta, pdeg)
         batch.set_tuning(64, 4, 2)
+        batch.set_cc_mode(args.cc_mode)
         v = T(np.broadcast_to(rh4(g), (M,) + g.x.shape))
         vel = torch.zeros((M, 3) + g.x.shape, dtype=torch.float64, device=dev)
         for _ in range(n):
@@ -506,6 +526,11 @@ def main():
     ap.add_argument("--profile", choices=["treecode", "treecode64", "spectral", "swe", "swe64", "ensemble"],
                     help="run --warmup + --steps steps of one path and exit (for profiler captures; no timing)")
     ap.add_argument("--members", type=int, default=ENS_MEMBERS, help="ensemble members in --profile ensemble")
+    ap.add_argument("--cc-mode", type=int, default=1, choices=[0, 1, 2],
+                    help="--profile ensemble: well-separated interactions, 0 CUDA-core pairs, 1 tensor-core "
+                         "3xTF32, 2 tensor-core TF32")
+    ap.add_argument("--degree", type=int, default=0,
+                    help="--profile ensemble: one proxy degree for every member (0: drawn from {6, 8, 10})")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 

@@ -36,7 +36,8 @@ typedef enum {
   SBSLPM_ERR_OUT_OF_PANEL = 3, /* BLI point outside its panel (reference aborts) */
   SBSLPM_ERR_NONFINITE = 4,    /* NaN/Inf met in a location step */
   SBSLPM_ERR_ARG = 5,          /* bad argument (null pointer, size) */
-  SBSLPM_ERR_NO_DEVICE = 6     /* no CUDA device / library built without it */
+  SBSLPM_ERR_NO_DEVICE = 6,    /* no CUDA device / library built without it */
+  SBSLPM_ERR_TIMEOUT = 7       /* a bounded device-side wait ran out (the kernel returned) */
 } sbslpm_status;
 
 /* Velocity evaluation used by the step. */
@@ -321,6 +322,21 @@ sbslpm_status sbslpm_batch_set_tuning(sbslpm_batch* batch, int threads, int targ
 /* Pair evaluations of one velocity evaluation over all members: near field
  * (particle x particle) and well-separated (proxy x proxy). */
 sbslpm_status sbslpm_batch_pairs(const sbslpm_batch* batch, double* near_pairs, double* far_pairs);
+/* Well-separated (cluster-cluster) interactions of a mixed-precision batch:
+ * mode -1 = chosen per proxy-degree group by the autotuner of the first
+ * step (the default), 0 = CUDA-core float32 pairs per member (bit-exact with
+ * single contexts), 1 = tensor-core GEMM over the members sharing a proxy
+ * degree in 3xTF32, 2 = the same GEMM in one TF32 pass.  Float64 batches
+ * accept mode 0 only.  sbslpm_batch_cc_info reports the mode, the union of
+ * the members' well-separated pairs over the degree groups (cluster pairs),
+ * and the MMA flops one velocity evaluation issues.  sbslpm_batch_cc_groups
+ * reports per group (at most n): proxy degree, members, the mode in use and
+ * the autotuner's timings of one launch in modes 0 and 1 (0 before the
+ * first step). */
+sbslpm_status sbslpm_batch_set_cc_mode(sbslpm_batch* batch, int mode);
+sbslpm_status sbslpm_batch_cc_info(const sbslpm_batch* batch, int* mode, double* union_pairs, double* mma_flops);
+sbslpm_status sbslpm_batch_cc_groups(const sbslpm_batch* batch, int n, int* degree, int* members, int* mode,
+                                     double* ms_cuda_cores, double* ms_tensor_cores);
 
 /* ---------------- direct sums (device pointers, no context) ---------------- */
 

@@ -133,6 +133,9 @@ def lib() -> ctypes.CDLL:
     L.sbslpm_batch_run.argtypes = [_VP] + [_VP] * 6 + [ctypes.c_double, ctypes.c_int]
     L.sbslpm_batch_tuning.argtypes = [_VP, _I, _D]
     L.sbslpm_batch_pairs.argtypes = [_VP, _D, _D]
+    L.sbslpm_batch_set_cc_mode.argtypes = [_VP, ctypes.c_int]
+    L.sbslpm_batch_cc_info.argtypes = [_VP, _I, _D, _D]
+    L.sbslpm_batch_cc_groups.argtypes = [_VP, ctypes.c_int, _I, _I, _I, _D, _D]
     L.sbslpm_batch_set_tuning.argtypes = [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     L.sbslpm_time_interactions.argtypes = [_VP, ctypes.c_int, _D, _D]
     L.sbslpm_set_near_tuning.argtypes = [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_int]
@@ -514,6 +517,31 @@ class Batch:
         a, b = ctypes.c_double(), ctypes.c_double()
         _check(lib().sbslpm_batch_pairs(self._h, ctypes.byref(a), ctypes.byref(b)), "sbslpm_batch_pairs")
         return a.value, b.value
+
+    CC_AUTO, CC_CUDA_CORES, CC_TC_3XTF32, CC_TC_TF32 = -1, 0, 1, 2
+
+    def set_cc_mode(self, mode: int):
+        """Well-separated interactions: -1 autotuned per proxy-degree group (default for mixed
+        precision), 0 CUDA-core pairs, 1 tensor-core 3xTF32 GEMM, 2 tensor-core single-pass TF32 GEMM."""
+        _check(lib().sbslpm_batch_set_cc_mode(self._h, int(mode)), "sbslpm_batch_set_cc_mode")
+
+    def cc_info(self):
+        """(mode, union cluster pairs over the degree groups, MMA flops per velocity evaluation)."""
+        mode = ctypes.c_int()
+        up, fl = ctypes.c_double(), ctypes.c_double()
+        _check(lib().sbslpm_batch_cc_info(self._h, ctypes.byref(mode), ctypes.byref(up), ctypes.byref(fl)),
+               "sbslpm_batch_cc_info")
+        return mode.value, up.value, fl.value
+
+    def cc_groups(self):
+        """Per proxy-degree group: dicts of degree, members, mode in use and the autotuner's
+        timings (ms per launch) of the CUDA-core and tensor-core modes."""
+        n = 16
+        deg, mem, mode = (ctypes.c_int * n)(), (ctypes.c_int * n)(), (ctypes.c_int * n)()
+        t0, t1 = (ctypes.c_double * n)(), (ctypes.c_double * n)()
+        _check(lib().sbslpm_batch_cc_groups(self._h, n, deg, mem, mode, t0, t1), "sbslpm_batch_cc_groups")
+        return [{"degree": deg[k], "members": mem[k], "mode": mode[k], "ms_cuda_cores": t0[k],
+                 "ms_tensor_cores": t1[k]} for k in range(n) if mem[k] > 0]
 
 
 def measure_fma_peak(kind: int = 0, ms: float = 50.0) -> float:

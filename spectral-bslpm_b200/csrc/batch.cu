@@ -13,6 +13,7 @@
 #include <string>
 #include <vector>
 
+#include "cc_tcgen05.cuh"
 #include "context_internal.hpp"
 #include "geometry.cuh"
 
@@ -38,6 +39,11 @@ struct sbslpm_batch {
     int* fface = nullptr;
     std::vector<int> members;
     int* d_idx = nullptr;
+    // tensor-core well-separated interactions: union of the members' lists
+    CcTcGroup tc{};
+    long upairs = 0;
+    int cc_auto = 0;           // the autotuner's choice for this group (0 CUDA cores, 1 tensor cores 3xTF32)
+    double cc_ms[2] = {0, 0};  // its timings of one launch in each mode
   };
   std::vector<Degree> degs;
   std::vector<void*> bufs;  // every device buffer of the batch, freed on destroy
@@ -50,6 +56,11 @@ struct sbslpm_batch {
   double *near = nullptr, *vbuf = nullptr, *newvor = nullptr;
   unsigned* err = nullptr;
   unsigned* h_err = nullptr;
+
+  // well-separated interactions: -1 autotuned per proxy-degree group (mixed
+  // precision default), 0 CUDA-core pairs, 1 tensor cores 3xTF32, 2 tensor
+  // cores TF32 (mixed precision only)
+  int cc_mode = 0;
 
   // autotuned near-field launch shape
   bool tuned = false;
@@ -89,6 +100,8 @@ sbslpm_status batch_finish(sbslpm_batch* b) {
   if (e) {
     SB_CUDA(cudaMemsetAsync(b->err, 0, sizeof(unsigned), st));
     SB_CUDA(cudaStreamSynchronize(st));
+    if (e & kErrTimeout)
+      return set_last_error("a tensor-core interaction kernel's bounded wait ran out"), SBSLPM_ERR_TIMEOUT;
     if (e & kErrNonFinite) return set_last_error("non-finite point in a location step"), SBSLPM_ERR_NONFINITE;
     return set_last_error("interpolation point outside its panel"), SBSLPM_ERR_OUT_OF_PANEL;
   }
@@ -147,6 +160,28 @@ sbslpm_status batch_setup(sbslpm_batch* b) {
   b->qmax = (b->nmax + 1) * (b->nmax + 1);
 
   const bool mixed = c.precision == SBSLPM_MIXED;
+  b->cc_mode = mixed ? -1 : 0;
+  // tensor-core member tiling of each degree group, and the union of the
+  // group's well-separated lists with one member bit per pair
+  std::vector<int> gsize(uniq.size(), 0);
+  for (int m = 0; m < b->M; m++) gsize[std::lower_bound(uniq.begin(), uniq.end(), b->degree[m]) - uniq.begin()]++;
+  std::vector<std::vector<int>> uidx(uniq.size());
+  std::vector<std::vector<std::pair<int, int>>> upair(uniq.size());
+  std::vector<std::vector<unsigned>> umask(uniq.size());
+  for (size_t k = 0; k < uniq.size(); k++) {
+    CcTcGroup& G = b->degs[k].tc;
+    G.Q = b->degs[k].qx;
+    G.Pf = b->degs[k].t.Pf;
+    G.nmem = gsize[k];
+    const int maxtile = cc_tc_max_tile(G.Q), r16 = (G.nmem + 15) / 16 * 16;
+    const int ntiles = (r16 + maxtile - 1) / maxtile;
+    G.ntile = ((G.nmem + ntiles - 1) / ntiles + 15) / 16 * 16;
+    G.npad = G.ntile * ntiles;
+    G.kch = ((G.Q + 7) / 8 * 8 + cc_tc_kc(G.Q) - 1) / cc_tc_kc(G.Q);
+    G.mw = (G.npad + 31) / 32;
+    G.eps = c.kernel_eps;
+    if (mixed) uidx[k].assign((size_t)G.Pf * G.Pf, -1);
+  }
   b->h_mem.resize(b->M);
   b->near_pairs.assign(b->M, 0);
   b->cc_pairs.assign(b->M, 0);
@@ -158,6 +193,19 @@ sbslpm_status batch_setup(sbslpm_batch* b) {
     build_tree_lists(D.t, b->theta[m], l);
     b->near_pairs[m] = l.ns.back();
     b->cc_pairs[m] = l.cs.back();
+    if (mixed) {
+      const int j = (int)D.members.size() - 1, mw = D.tc.mw, Pf = D.t.Pf;
+      for (int t = 0; t < Pf; t++)
+        for (int e = l.cs[t]; e < l.cs[t + 1]; e++) {
+          int& u = uidx[k][(size_t)t * Pf + l.csrc[e]];
+          if (u < 0) {
+            u = (int)upair[k].size();
+            upair[k].push_back({t, l.csrc[e]});
+            umask[k].resize(umask[k].size() + mw, 0u);
+          }
+          umask[k][(size_t)u * mw + (j >> 5)] |= 1u << (j & 31);
+        }
+    }
     int *ns = nullptr, *nsrc = nullptr, *cs = nullptr, *csrc = nullptr;
     SB_TRY(bupload(b, &ns, l.ns));
     SB_TRY(bupload(b, &nsrc, l.nsrc));
@@ -210,6 +258,60 @@ sbslpm_status batch_setup(sbslpm_batch* b) {
   }
   for (auto& D : b->degs) SB_TRY(bupload(b, &D.d_idx, D.members));
   SB_TRY(bupload(b, &b->d_mem, b->h_mem));
+  if (mixed) {
+    for (size_t k = 0; k < b->degs.size(); k++) {
+      sbslpm_batch::Degree& D = b->degs[k];
+      CcTcGroup& G = D.tc;
+      // CSR by target cluster, sources ascending (the accumulation order)
+      std::vector<int> order(upair[k].size());
+      for (size_t e = 0; e < order.size(); e++) order[e] = (int)e;
+      std::sort(order.begin(), order.end(), [&](int x, int y) { return upair[k][x] < upair[k][y]; });
+      std::vector<int> us(G.Pf + 1, 0), usrc(order.size());
+      std::vector<unsigned> um(order.size() * G.mw);
+      for (size_t e = 0; e < order.size(); e++) {
+        const auto& pr = upair[k][order[e]];
+        us[pr.first + 1]++;
+        usrc[e] = pr.second;
+        for (int w = 0; w < G.mw; w++) um[e * G.mw + w] = umask[k][(size_t)order[e] * G.mw + w];
+      }
+      G.maxlist = 0;
+      for (int t = 0; t < G.Pf; t++) G.maxlist = std::max(G.maxlist, us[t + 1]);
+      for (int t = 0; t < G.Pf; t++) us[t + 1] += us[t];
+      D.upairs = (long)order.size();
+      int *dus = nullptr, *dusrc = nullptr;
+      unsigned* dum = nullptr;
+      SB_TRY(bupload(b, &dus, us));
+      if (!usrc.empty()) {
+        SB_TRY(bupload(b, &dusrc, usrc));
+        SB_TRY(bupload(b, &dum, um));
+      }
+      const size_t pn = (size_t)G.Pf * G.Q;
+      std::vector<float4> pxf(pn);
+      for (size_t i = 0; i < pn; i++) {
+        const double* cc = &D.t.centre[4 * (i / G.Q)];
+        pxf[i] = make_float4((float)((D.t.fpx[i] - cc[0]) * kPackScale), (float)((D.t.fpx[pn + i] - cc[1]) * kPackScale),
+                             (float)((D.t.fpx[2 * pn + i] - cc[2]) * kPackScale), 0.f);
+      }
+      float4* dpxf = nullptr;
+      SB_TRY(bupload(b, &dpxf, pxf));
+      float *whi = nullptr, *wlo = nullptr;
+      const size_t wn = (size_t)G.Pf * G.kch * G.npad * cc_tc_kc(G.Q);
+      SB_TRY(balloc(b, &whi, wn));
+      SB_TRY(balloc(b, &wlo, wn));
+      G.ustart = dus;
+      G.usrc = dusrc;
+      G.umask = dum;
+      G.pxf = dpxf;
+      G.centre = D.fcentre;
+      G.px = D.fpx;
+      G.whi = whi;
+      G.wlo = wlo;
+      G.idx = D.d_idx;
+      G.mem = b->d_mem;
+      G.err = b->err;
+      SB_CUDA(cc_tc_prepare(G));
+    }
+  }
 
   const size_t MN = (size_t)b->M * b->N;
   SB_TRY(balloc(b, &b->psrc, MN));
@@ -230,8 +332,15 @@ void batch_velocity(sbslpm_batch* b, int stage, double dt_s, const double* vprev
   launch_bltc_sources_batch(b->d_mem, b->M, b->Af, b->npl, b->nmax, stage, dt_s, vprev, x, y, z, vors, area, b->psrc,
                             b->psrcf, mixed, st);
   launch_upward_batch(b->d_mem, b->M, b->Lf, b->qmax, mixed, st);
-  for (const auto& D : b->degs)
-    launch_cc_batch(b->d_mem, D.d_idx, (int)D.members.size(), D.qx, b->Pf, b->cfg.kernel_eps, prec, st);
+  for (const auto& D : b->degs) {
+    const int mode = mixed ? (b->cc_mode < 0 ? D.cc_auto : b->cc_mode) : 0;
+    if (mode != 0) {
+      launch_cc_tc_pack(D.tc, st);
+      launch_cc_tc(D.tc, mode == 1 ? 3 : 1, st);
+    } else {
+      launch_cc_batch(b->d_mem, D.d_idx, (int)D.members.size(), D.qx, b->Pf, b->cfg.kernel_eps, prec, st);
+    }
+  }
   launch_downward_batch(b->d_mem, b->M, b->Lf, b->qmax, st);
   launch_bltc_near_batch(b->d_mem, b->M, b->Af, b->npl, b->cfg.kernel_eps, prec, x, y, z, b->psrc, b->psrcf, b->near,
                          b->splits, b->nt, b->tpt, st);
@@ -288,6 +397,33 @@ sbslpm_status batch_autotune(sbslpm_batch* b, const double* x, const double* y, 
         b->tpt = sh[1];
         b->splits = sp;
       }
+    }
+  }
+  // well-separated interactions of each proxy-degree group: CUDA-core pairs
+  // or the tensor-core 3xTF32 GEMM, whichever is faster here (needs the
+  // proxy sources of the stage-0 upward pass)
+  if (prec == SBSLPM_MIXED) {
+    launch_upward_batch(b->d_mem, b->M, b->Lf, b->qmax, true, st);
+    for (auto& D : b->degs) {
+      for (int mode = 0; mode < 2; mode++) {
+        auto run = [&] {
+          if (mode == 0)
+            launch_cc_batch(b->d_mem, D.d_idx, (int)D.members.size(), D.qx, b->Pf, b->cfg.kernel_eps, prec, st);
+          else {
+            launch_cc_tc_pack(D.tc, st);
+            launch_cc_tc(D.tc, 3, st);
+          }
+        };
+        run();  // warm-up
+        SB_CUDA(cudaEventRecord(e0, st));
+        for (int r = 0; r < 3; r++) run();
+        SB_CUDA(cudaEventRecord(e1, st));
+        SB_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        SB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        D.cc_ms[mode] = ms / 3;
+      }
+      D.cc_auto = D.cc_ms[1] < D.cc_ms[0] ? 1 : 0;
     }
   }
   cudaEventDestroy(e0);
@@ -452,6 +588,50 @@ sbslpm_status sbslpm_batch_set_tuning(sbslpm_batch* b, int threads, int targets_
     b->graph = nullptr;
   }
   return SBSLPM_OK;
+}
+
+sbslpm_status sbslpm_batch_set_cc_mode(sbslpm_batch* b, int mode) {
+  if (!b || mode < -1 || mode > 2) return SBSLPM_ERR_ARG;
+  if (mode != 0 && b->cfg.precision != SBSLPM_MIXED)
+    return set_last_error("tensor-core well-separated interactions need mixed precision"), SBSLPM_ERR_CONFIG;
+  if (mode != b->cc_mode && b->graph) {
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  b->cc_mode = mode;
+  return SBSLPM_OK;
+}
+
+sbslpm_status sbslpm_batch_cc_info(const sbslpm_batch* b, int* mode, double* union_pairs, double* mma_flops) {
+  if (!b || !mode || !union_pairs || !mma_flops) return SBSLPM_ERR_ARG;
+  *mode = b->cc_mode;
+  double up = 0, fl = 0;
+  for (const auto& D : b->degs) {
+    const CcTcGroup& G = D.tc;
+    const int mode = b->cc_mode < 0 ? D.cc_auto : b->cc_mode;
+    up += (double)D.upairs;
+    if (mode != 0) {
+      const double tiles = ((3 * G.Q + 127) / 128), ksteps = (G.Q + 7) / 8;
+      fl += (double)D.upairs * tiles * ksteps * 2.0 * 128 * 8 * G.npad * (mode == 1 ? 3 : 1);
+    }
+  }
+  *union_pairs = up;
+  *mma_flops = fl;
+  return SBSLPM_OK;
+}
+
+sbslpm_status sbslpm_batch_cc_groups(const sbslpm_batch* b, int n, int* degree, int* members, int* mode,
+                                     double* ms_cuda_cores, double* ms_tensor_cores) {
+  if (!b || n < 0 || !degree || !members || !mode || !ms_cuda_cores || !ms_tensor_cores) return SBSLPM_ERR_ARG;
+  for (int k = 0; k < n && k < (int)b->degs.size(); k++) {
+    const auto& D = b->degs[k];
+    degree[k] = D.n;
+    members[k] = (int)D.members.size();
+    mode[k] = b->cfg.precision != SBSLPM_MIXED ? 0 : (b->cc_mode < 0 ? D.cc_auto : b->cc_mode);
+    ms_cuda_cores[k] = D.cc_ms[0];
+    ms_tensor_cores[k] = D.cc_ms[1];
+  }
+  return (int)b->degs.size() > n ? SBSLPM_ERR_ARG : SBSLPM_OK;
 }
 
 sbslpm_status sbslpm_batch_pairs(const sbslpm_batch* b, double* near_pairs, double* far_pairs) {

@@ -460,6 +460,7 @@ const char* sbslpm_status_string(sbslpm_status s) {
     case SBSLPM_ERR_NONFINITE: return "non-finite value";
     case SBSLPM_ERR_ARG: return "invalid argument";
     case SBSLPM_ERR_NO_DEVICE: return "no CUDA device";
+    case SBSLPM_ERR_TIMEOUT: return "device wait timed out";
   }
   return "unknown status";
 }

@@ -23,7 +23,7 @@ constexpr int kMaxQ = (kMaxDegree + 1) * (kMaxDegree + 1);
 constexpr double kBiotSavart = -0.07957747154594767;
 
 // Error bits reported by device code through the context's error word.
-enum : unsigned { kErrOutOfPanel = 1u, kErrNonFinite = 2u, kErrBadFace = 4u };
+enum : unsigned { kErrOutOfPanel = 1u, kErrNonFinite = 2u, kErrBadFace = 4u, kErrTimeout = 8u };
 
 SB_HD int level_start(int level) { return 2 * ((1 << (2 * level)) - 1); }
 

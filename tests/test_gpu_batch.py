@@ -4,10 +4,13 @@ exactly what single contexts give member by member, and stay within the
 accuracy bar against the float64 direct sum.
 
 Tolerances: bit-exact against single contexts with the same near-field split
-count (the arithmetic per target is the same; only the split count changes
-the order of the near-field partial sums), <= 1e-12 with the autotuned
-split, mixed precision <= 1e-6 relative L-infinity vorticity against the
-float64 direct sum after one step.
+count and the CUDA-core well-separated interactions (the arithmetic per
+target is the same; only the split count changes the order of the
+near-field partial sums), <= 1e-12 with the autotuned split, mixed precision
+<= 1e-6 relative L-infinity vorticity against the float64 direct sum after
+one step.  The tensor-core well-separated interactions (3xTF32 GEMM over the
+members) agree with the CUDA-core float32 pairs to <= 1e-6 relative
+L-infinity in velocity, the single-pass TF32 GEMM to <= 1e-4.
 """
 import numpy as np
 import pytest
@@ -60,6 +63,8 @@ def test_batch_equals_single_contexts(sb, precision):
     g, xyza, vors = grid_and_vors(sb, len(THETA))
     batch = sb.Batch(base_cfg(sb, prec), THETA, PDEG)
     batch.set_tuning(128, 2, 2)  # the single context's near-field shape and split count
+    if prec == sb.MIXED:
+        batch.set_cc_mode(batch.CC_CUDA_CORES)  # the single context's float32 pair arithmetic
     v = vors.clone()
     vel = torch.zeros((len(THETA), 3) + v.shape[1:], dtype=torch.float64, device="cuda")
     batch.step(*xyza, v, vel)
@@ -98,9 +103,11 @@ def test_batch_graph_replay_equals_steps(sb):
     assert torch.equal(va, vb) and torch.equal(vela, velb)
 
 
-def test_batch_mixed_accuracy_vs_direct_sum(sb):
+@pytest.mark.parametrize("mode", [-1, 0, 1, 2])
+def test_batch_mixed_accuracy_vs_direct_sum(sb, mode):
     g, xyza, vors = grid_and_vors(sb, len(THETA))
     batch = sb.Batch(base_cfg(sb, sb.MIXED), THETA, PDEG)
+    batch.set_cc_mode(mode)
     v = vors.clone()
     vel = torch.zeros((len(THETA), 3) + v.shape[1:], dtype=torch.float64, device="cuda")
     batch.step(*xyza, v, vel)
@@ -109,7 +116,56 @@ def test_batch_mixed_accuracy_vs_direct_sum(sb):
         d = vors[m].clone()
         dvel = [torch.zeros_like(d) for _ in range(3)]
         ctx.bve_back_rk4_step(*xyza, d, *dvel)
+        print("cc mode %d member %d: vorticity vs float64 direct sum %.2e" % (mode, m, rel(v[m], d)))
         assert rel(v[m], d) <= 1e-6, (m, rel(v[m], d))
+
+
+def batch_step(sb, batch, xyza, vors):
+    v = vors.clone()
+    vel = torch.zeros((vors.shape[0], 3) + v.shape[1:], dtype=torch.float64, device="cuda")
+    batch.step(*xyza, v, vel)
+    return v, vel
+
+
+@pytest.mark.parametrize("mode,tol", [(1, 1e-6), (2, 1e-4)])
+def test_tensor_core_cc_matches_cuda_core_pairs(sb, mode, tol):
+    g, xyza, vors = grid_and_vors(sb, len(THETA))
+    ref = sb.Batch(base_cfg(sb, sb.MIXED), THETA, PDEG)
+    ref.set_tuning(128, 2, 2)
+    ref.set_cc_mode(ref.CC_CUDA_CORES)
+    tc = sb.Batch(base_cfg(sb, sb.MIXED), THETA, PDEG)
+    tc.set_tuning(128, 2, 2)
+    tc.set_cc_mode(mode)
+    m, up, flops = tc.cc_info()
+    near, far = tc.pairs()
+    assert m == mode and flops > 0 and up * 81 * 81 >= far / len(THETA)
+    vr, velr = batch_step(sb, ref, xyza, vors)
+    vt, velt = batch_step(sb, tc, xyza, vors)
+    for k in range(len(THETA)):
+        e = rel(velt[k], velr[k])
+        print("member %d: tensor-core vs CUDA-core velocity %.2e" % (k, e))
+        assert e <= tol, (k, e)
+        assert rel(vt[k], vr[k]) <= tol, k
+
+
+def test_cc_autotuner_times_both_modes(sb):
+    g, xyza, vors = grid_and_vors(sb, len(THETA))
+    batch = sb.Batch(base_cfg(sb, sb.MIXED), THETA, PDEG)
+    assert batch.cc_info()[0] == batch.CC_AUTO
+    batch_step(sb, batch, xyza, vors)
+    groups = batch.cc_groups()
+    assert sorted(gr["degree"] for gr in groups) == sorted(set(PDEG))
+    assert sum(gr["members"] for gr in groups) == len(THETA)
+    for gr in groups:
+        assert gr["ms_cuda_cores"] > 0 and gr["ms_tensor_cores"] > 0
+        assert gr["mode"] == (1 if gr["ms_tensor_cores"] < gr["ms_cuda_cores"] else 0)
+
+
+def test_tensor_core_cc_rejects_float64(sb):
+    batch = sb.Batch(base_cfg(sb, sb.FP64), THETA, PDEG)
+    assert batch.cc_info()[0] == 0
+    with pytest.raises(sb.SbslpmError):
+        batch.set_cc_mode(1)
 
 
 def test_batch_rejects_bad_members(sb):
