@@ -338,6 +338,45 @@ sbslpm_status sbslpm_batch_cc_info(const sbslpm_batch* batch, int* mode, double*
 sbslpm_status sbslpm_batch_cc_groups(const sbslpm_batch* batch, int n, int* degree, int* members, int* mode,
                                      double* ms_cuda_cores, double* ms_tensor_cores);
 
+/* ---------------- output path (the drivers' per-step output) ---------------- */
+
+/* Replaces interp_to_latlon_host (src/interp_funcs.hpp:22-77, host, OpenMP):
+ * a [leaf][q] field interpolated to the nlat x nlon grid of latitudes lats
+ * and longitudes lons (degrees), out[nlat][nlon]; all device pointers, on the
+ * context's stream. */
+sbslpm_status sbslpm_interp_to_latlon(sbslpm_ctx* ctx, const double* data, int nlat, const double* lats, int nlon,
+                                      const double* lons, double* out);
+/* Replaces xyz_vel_to_uv_vel (src/general_utils_impl.hpp:195-229): zonal and
+ * meridional velocity of the [leaf][q] grid (device pointers). */
+sbslpm_status sbslpm_xyz_vel_to_uv_vel(sbslpm_ctx* ctx, const double* x, const double* y, const double* z,
+                                       const double* vel_x, const double* vel_y, const double* vel_z, double* vel_u,
+                                       double* vel_v);
+/* The drivers' output grid (executables/bve_time_evo.cpp:93-95, 206-211):
+ * spacing 2^floor(log2(sqrt(4 pi / point_count) 180 / pi)) degrees,
+ * nlat = 180 / spacing + 1 latitudes from -90, nlon = 360 / spacing
+ * longitudes from 0; lats / lons (host, may be NULL) receive the values. */
+sbslpm_status sbslpm_output_grid(long point_count, double* spacing, int* nlat, int* nlon, double* lats,
+                                 double* lons);
+
+/* netCDF classic (64-bit offset) writer for the drivers' output files; the
+ * calls mirror the netCDF library's nc_create, nc_def_dim, nc_def_var,
+ * nc_put_att_text / _int / _double, nc_enddef, nc_put_vara_double / _int and
+ * nc_close as executables/bve_time_evo.cpp:125-358 uses them.  Types: 4 =
+ * int, 6 = double.  varid -1 names the global attributes.  start / count
+ * NULL = the whole variable.  Host memory. */
+typedef struct sbslpm_nc sbslpm_nc;
+sbslpm_status sbslpm_nc_create(const char* path, sbslpm_nc** out);
+sbslpm_status sbslpm_nc_def_dim(sbslpm_nc* nc, const char* name, long len, int* dimid);
+sbslpm_status sbslpm_nc_def_var(sbslpm_nc* nc, const char* name, int type, int ndims, const int* dimids, int* varid);
+sbslpm_status sbslpm_nc_put_att_text(sbslpm_nc* nc, int varid, const char* name, const char* text);
+sbslpm_status sbslpm_nc_put_att_int(sbslpm_nc* nc, int varid, const char* name, long n, const int* vals);
+sbslpm_status sbslpm_nc_put_att_double(sbslpm_nc* nc, int varid, const char* name, long n, const double* vals);
+sbslpm_status sbslpm_nc_enddef(sbslpm_nc* nc);
+sbslpm_status sbslpm_nc_put_vara_double(sbslpm_nc* nc, int varid, const long* start, const long* count,
+                                        const double* data);
+sbslpm_status sbslpm_nc_put_vara_int(sbslpm_nc* nc, int varid, const long* start, const long* count, const int* data);
+sbslpm_status sbslpm_nc_close(sbslpm_nc* nc);
+
 /* ---------------- direct sums (device pointers, no context) ---------------- */
 
 /* Biot-Savart direct sum on the sphere (the reference's BVE kernel,

@@ -779,3 +779,49 @@ void orc_direct_sum_inv_lap(int n, const double* x, const double* y, const doubl
     soln[i] = acc;
   }
 }
+
+/* ---------------- output path: src/interp_funcs.hpp, src/general_utils_impl.hpp ---------------- */
+
+/* latlon_interp_host::operator() (src/interp_funcs.hpp:38-70) over the whole
+ * (lat, lon) grid, as interp_to_latlon_host (src/interp_funcs.hpp:72-77) runs
+ * it: the point of latitude lats[i] / longitude lons[j] (degrees), its leaf
+ * by point_locate_panel_2 (src/interp_funcs.cpp:175-203, the same descent as
+ * point_locate_panel), the face-free xieta_from_xyz, interp_vals_bli at the
+ * leaf and the sum over m, n in order.  data is [leaf][q]; out is [nlat][nlon]. */
+void orc_interp_to_latlon(int levels, int degree, const orc_panel* p, const double* data, int nlat,
+                          const double* lats, int nlon, const double* lons, double* out) {
+  int q = (degree + 1) * (degree + 1), off = orc_panel_count(levels) - orc_leaf_count(levels);
+  double basis[MAXQ], xe[2];
+  for (int i = 0; i < nlat; i++)
+    for (int j = 0; j < nlon; j++) {
+      double lat = lats[i] * ORC_PI / 180.0, lon = lons[j] * ORC_PI / 180.0;
+      double x = cos(lat) * cos(lon), y = cos(lat) * sin(lon), z = sin(lat);
+      int panel = orc_point_locate_panel(p, x, y, z);
+      xieta_from_xyz(x, y, z, xe);
+      orc_interp_vals_bli(basis, xe[0], xe[1], ORC_PI / 4.0 * p[panel].min_xi, ORC_PI / 4.0 * p[panel].max_xi,
+                          ORC_PI / 4.0 * p[panel].min_eta, ORC_PI / 4.0 * p[panel].max_eta, degree);
+      double acc = 0;
+      for (int m = 0; m < degree + 1; m++)
+        for (int n = 0; n < degree + 1; n++) {
+          int k = m * (degree + 1) + n;
+          acc += basis[k] * data[(long)(panel - off) * q + k];
+        }
+      out[(long)i * nlon + j] = acc;
+    }
+}
+
+/* xyz_vel_to_uv_vel (src/general_utils_impl.hpp:195-229): zonal and
+ * meridional components of a tangent velocity, zero within 1e-16 of a pole. */
+void orc_xyz_vel_to_uv_vel(long n, const double* x, const double* y, const double* z, const double* vx,
+                           const double* vy, const double* vz, double* u, double* v) {
+  for (long i = 0; i < n; i++) {
+    double xx = x[i], yy = y[i], zz = z[i], xc = vx[i], yc = vy[i], zc = vz[i];
+    if (fabs(zz) < 1 - 1e-16) {
+      u[i] = (-yy * xc + xx * yc) / sqrt(xx * xx + yy * yy);
+      v[i] = -((xx * xc + yy * yc) * zz - (xx * xx + yy * yy) * zc) / sqrt(xx * xx + yy * yy);
+    } else {
+      u[i] = 0;
+      v[i] = 0;
+    }
+  }
+}

@@ -78,6 +78,14 @@ void orc_bve_step(const orc_bve_problem* pb, double* vors, double* vel_x, double
 void orc_direct_sum_inv_lap(int n, const double* x, const double* y, const double* z, const double* area,
                             const double* pots, double* soln);
 
+/* Output path: interp_to_latlon_host (src/interp_funcs.hpp:22-77) of one
+ * [leaf][q] field to an nlat x nlon grid in degrees, and xyz_vel_to_uv_vel
+ * (src/general_utils_impl.hpp:195-229). */
+void orc_interp_to_latlon(int levels, int degree, const orc_panel* p, const double* data, int nlat,
+                          const double* lats, int nlon, const double* lons, double* out);
+void orc_xyz_vel_to_uv_vel(long n, const double* x, const double* y, const double* z, const double* vx,
+                           const double* vy, const double* vz, double* u, double* v);
+
 #ifdef __cplusplus
 }
 #endif

@@ -85,6 +85,8 @@ class Port:
         L.orc_point_locate_panel.argtypes = [ctypes.POINTER(OrcPanel), ctypes.c_double, ctypes.c_double, ctypes.c_double]
         L.orc_interp_vals_bli.argtypes = [_D] + [ctypes.c_double] * 6 + [ctypes.c_int]
         L.orc_bve_step.argtypes = [ctypes.POINTER(OrcProblem), _D, _D, _D, _D, _D]
+        L.orc_interp_to_latlon.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(OrcPanel), _D, ctypes.c_int,
+                                           _D, ctypes.c_int, _D, _D]
 
     # ---- setup -------------------------------------------------------------
     def build(self, levels: int, degree: int, theta: float | None, exact_cc: bool = False):
@@ -177,6 +179,21 @@ class Port:
             self.lib.orc_bve_step(ctypes.byref(pb), _dp(v), _dp(vx), _dp(vy), _dp(vz), _dp(tr))
         return v, (vx, vy, vz), (tr if T else None)
 
+    def interp_to_latlon(self, g, data, lats, lons):
+        """interp_to_latlon_host (src/interp_funcs.hpp:22-77): [nlat][nlon]."""
+        lats, lons = np.ascontiguousarray(lats, float), np.ascontiguousarray(lons, float)
+        out = np.zeros((len(lats), len(lons)))
+        self.lib.orc_interp_to_latlon(g["levels"], g["degree"], g["panels"], _dp(np.ascontiguousarray(data)),
+                                      len(lats), _dp(lats), len(lons), _dp(lons), _dp(out))
+        return out
+
+    def xyz_vel_to_uv_vel(self, x, y, z, vx, vy, vz):
+        """xyz_vel_to_uv_vel (src/general_utils_impl.hpp:195-229): (u, v)."""
+        a = [np.ascontiguousarray(t, float).ravel() for t in (x, y, z, vx, vy, vz)]
+        u, v = np.zeros(a[0].size), np.zeros(a[0].size)
+        self.lib.orc_xyz_vel_to_uv_vel(ctypes.c_long(a[0].size), *[_dp(t) for t in a], _dp(u), _dp(v))
+        return u.reshape(np.shape(x)), v.reshape(np.shape(x))
+
     def direct_sum_inv_lap(self, x, y, z, area, pots):
         n = len(x)
         out = np.zeros(n)
@@ -204,6 +221,9 @@ class Ref:
         L.ref_interp_vals_bli.argtypes = [_D] + [ctypes.c_double] * 6 + [ctypes.c_int]
         L.ref_num_threads.restype = ctypes.c_int
         L.ref_swe_map.restype = ctypes.c_int
+        L.ref_interp_to_latlon.restype = None
+        L.ref_interp_to_latlon.argtypes = [ctypes.c_void_p, _D, ctypes.c_int, _D, ctypes.c_int, _D, _D]
+        L.ref_xyz_vel_to_uv_vel.restype = None
         for name in ("ref_unify", "ref_swe_vel_interactions", "ref_swe_tendency", "ref_swe_init", "ref_swe_step"):
             getattr(L, name).restype = None
         L.ref_swe_step.argtypes = [ctypes.c_void_p] + [_D] * 10 + [_I, _I, ctypes.c_double, ctypes.c_int,
@@ -287,6 +307,18 @@ class Ref:
 
     def locate(self, c, x, y, z) -> int:
         return self.lib.ref_point_locate_panel(c["h"], x, y, z)
+
+    def interp_to_latlon(self, c, data, lats, lons):
+        lats, lons = np.ascontiguousarray(lats, float), np.ascontiguousarray(lons, float)
+        out = np.zeros((len(lats), len(lons)))
+        self.lib.ref_interp_to_latlon(c["h"], _dp(np.ascontiguousarray(data)), len(lats), _dp(lats), len(lons),
+                                      _dp(lons), _dp(out))
+        return out
+
+    def xyz_vel_to_uv_vel(self, c, vx, vy, vz):
+        u, v = np.zeros(np.shape(vx)), np.zeros(np.shape(vx))
+        self.lib.ref_xyz_vel_to_uv_vel(c["h"], *[_dp(np.ascontiguousarray(t)) for t in (vx, vy, vz)], _dp(u), _dp(v))
+        return u, v
 
     def direct_sum_inv_lap(self, x, y, z, area, pots):
         n = len(x)

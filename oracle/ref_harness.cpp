@@ -16,6 +16,8 @@
 //   interp_vals_bli / point_locate_panel (src/interp_funcs_impl.hpp:11-142)
 //   bve_initialize                 (src/initial_conditions.cpp:358-385)
 //   direct_sum_inv_lap             (src/direct_sum.cpp:8-15)
+//   interp_to_latlon_host          (src/interp_funcs.hpp:22-77)
+//   xyz_vel_to_uv_vel              (src/general_utils_impl.hpp:195-229)
 // The reference's bve_time_step.cpp is included textually (unmodified) so that
 // its file-local departure / remap functors can be called one at a time.
 #include <Kokkos_Core.hpp>
@@ -284,6 +286,33 @@ void ref_direct_sum_inv_lap(int n, const double* x, const double* y, const doubl
   std::memcpy(vp.data(), pots, sizeof(double) * n);
   direct_sum_inv_lap(rc, vx, vy, vz, va, vp, vs);
   std::memcpy(soln, vs.data(), sizeof(double) * n);
+}
+
+// interp_to_latlon_host (src/interp_funcs.hpp:22-77) of one [leaf][q] field.
+void ref_interp_to_latlon(void* h, const double* data, int nlat, const double* lats, int nlon, const double* lons,
+                          double* out) {
+  RefCtx* c = static_cast<RefCtx*>(h);
+  const int A = c->rc.active_panel_count;
+  V2H d("data", A, c->q), o("out", nlat, nlon);
+  Kokkos::View<double*, Kokkos::HostSpace> la("lats", nlat), lo("lons", nlon);
+  std::memcpy(d.data(), data, sizeof(double) * A * c->q);
+  std::memcpy(la.data(), lats, sizeof(double) * nlat);
+  std::memcpy(lo.data(), lons, sizeof(double) * nlon);
+  interp_to_latlon_host(c->rc, d, c->panels_h, o, la, lo);
+  std::memcpy(out, o.data(), sizeof(double) * nlat * nlon);
+}
+
+// xyz_vel_to_uv_vel (src/general_utils_impl.hpp:195-229) over the grid points.
+void ref_xyz_vel_to_uv_vel(void* h, const double* vx, const double* vy, const double* vz, double* u, double* v) {
+  RefCtx* c = static_cast<RefCtx*>(h);
+  const int A = c->rc.active_panel_count;
+  V2 X("vx", A, c->q), Y("vy", A, c->q), Z("vz", A, c->q), U("u", A, c->q), W("v", A, c->q);
+  copy_in(X, vx);
+  copy_in(Y, vy);
+  copy_in(Z, vz);
+  Kokkos::parallel_for(A, xyz_vel_to_uv_vel(c->xcos, c->ycos, c->zcos, X, Y, Z, U, W));
+  copy_out(U, u);
+  copy_out(W, v);
 }
 
 int ref_num_threads(void) { return Kokkos::num_threads(); }

@@ -22,7 +22,8 @@ __all__ = [
     "SbslpmError", "Config", "Panel", "InteractPair", "FP64", "MIXED", "VEL_FMM", "VEL_DIRECT", "library_path",
     "lib", "config_default", "read_run_config", "panel_count", "leaf_count", "cubed_sphere_panels_init",
     "interp_init", "cube_sphere_spec_points", "dual_tree_traversal", "interp_vals_bli", "point_locate_panel",
-    "Context", "direct_sum_bve", "direct_sum_inv_lap", "kernel_launches", "Grid", "build_grid",
+    "Context", "direct_sum_bve", "direct_sum_inv_lap", "output_grid", "NcFile", "kernel_launches", "Grid",
+    "build_grid",
 ]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -114,6 +115,20 @@ def lib() -> ctypes.CDLL:
                                         ctypes.c_double, ctypes.c_int, _VP, _VP, _VP, _VP]
     L.sbslpm_direct_sum_bve_noalloc.argtypes = L.sbslpm_direct_sum_bve.argtypes
     L.sbslpm_direct_sum_inv_lap.argtypes = [ctypes.c_long] + [_VP] * 7
+    L.sbslpm_interp_to_latlon.argtypes = [_VP, _VP, ctypes.c_int, _VP, ctypes.c_int, _VP, _VP]
+    L.sbslpm_xyz_vel_to_uv_vel.argtypes = [_VP] * 9
+    L.sbslpm_output_grid.argtypes = [ctypes.c_long, _D, _I, _I, _D, _D]
+    _L = ctypes.POINTER(ctypes.c_long)
+    L.sbslpm_nc_create.argtypes = [ctypes.c_char_p, ctypes.POINTER(_VP)]
+    L.sbslpm_nc_def_dim.argtypes = [_VP, ctypes.c_char_p, ctypes.c_long, _I]
+    L.sbslpm_nc_def_var.argtypes = [_VP, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, _I, _I]
+    L.sbslpm_nc_put_att_text.argtypes = [_VP, ctypes.c_int, ctypes.c_char_p, ctypes.c_char_p]
+    L.sbslpm_nc_put_att_int.argtypes = [_VP, ctypes.c_int, ctypes.c_char_p, ctypes.c_long, _I]
+    L.sbslpm_nc_put_att_double.argtypes = [_VP, ctypes.c_int, ctypes.c_char_p, ctypes.c_long, _D]
+    L.sbslpm_nc_enddef.argtypes = [_VP]
+    L.sbslpm_nc_put_vara_double.argtypes = [_VP, ctypes.c_int, _L, _L, _D]
+    L.sbslpm_nc_put_vara_int.argtypes = [_VP, ctypes.c_int, _L, _L, _I]
+    L.sbslpm_nc_close.argtypes = [_VP]
     L.sbslpm_swe_step.argtypes = [_VP] + [_VP] * 14 + [ctypes.c_double]
     L.sbslpm_swe_run.argtypes = [_VP] + [_VP] * 14 + [ctypes.c_double, ctypes.c_int]
     L.sbslpm_swe_init.argtypes = [_VP] * 14
@@ -320,6 +335,35 @@ class Context:
         _check(lib().sbslpm_get_interactions(self._h, out), "sbslpm_get_interactions")
         arr = np.ctypeslib.as_array(ctypes.cast(out, ctypes.POINTER(ctypes.c_int)), (n, 3))
         return arr[: self.interaction_count].copy()
+
+    # -- output path ----------------------------------------------------
+    def interp_to_latlon(self, data, lats, lons, out=None):
+        """interp_to_latlon_host (src/interp_funcs.hpp:22-77) on the device: the [leaf][q]
+        field data at latitudes lats x longitudes lons (degrees, float64 CUDA tensors);
+        returns out [len(lats)][len(lons)]."""
+        import torch
+
+        nlat, nlon = int(lats.numel()), int(lons.numel())
+        if out is None:
+            out = torch.empty((nlat, nlon), dtype=torch.float64, device=data.device)
+        self._sync_stream()
+        _check(lib().sbslpm_interp_to_latlon(self._h, _dev(data, "data", (self.leaf_count, self.q)), nlat,
+                                             _dev(lats, "lats"), nlon, _dev(lons, "lons"),
+                                             _dev(out, "out", (nlat, nlon))), "sbslpm_interp_to_latlon")
+        return out
+
+    def xyz_vel_to_uv_vel(self, xcos, ycos, zcos, vel_x, vel_y, vel_z, vel_u=None, vel_v=None):
+        """xyz_vel_to_uv_vel (src/general_utils_impl.hpp:195-229): (vel_u, vel_v) of the grid."""
+        import torch
+
+        vel_u = torch.empty_like(vel_x) if vel_u is None else vel_u
+        vel_v = torch.empty_like(vel_x) if vel_v is None else vel_v
+        lq = (self.leaf_count, self.q)
+        self._sync_stream()
+        _check(lib().sbslpm_xyz_vel_to_uv_vel(self._h, *[_dev(t, n, lq) for t, n in (
+            (xcos, "xcos"), (ycos, "ycos"), (zcos, "zcos"), (vel_x, "vel_x"), (vel_y, "vel_y"), (vel_z, "vel_z"),
+            (vel_u, "vel_u"), (vel_v, "vel_v"))]), "sbslpm_xyz_vel_to_uv_vel")
+        return vel_u, vel_v
 
     # -- the step -------------------------------------------------------
     def bve_back_rk4_step(self, xcos, ycos, zcos, area, vors, vel_x, vel_y, vel_z, tracers=None, time=0.0):
@@ -655,6 +699,87 @@ def bve_rollout(context, xcos, ycos, zcos, area, vors0, nsteps):
     """nsteps BVE steps as a differentiable torch function of the initial
     vorticity (float64 direct-sum context), adjoint with per-step checkpoints."""
     return _autograd()[1].apply(vors0, context, xcos, ycos, zcos, area, int(nsteps))
+
+
+def output_grid(point_count: int):
+    """The drivers' output grid (executables/bve_time_evo.cpp:93-95, 206-211):
+    (spacing in degrees, latitudes, longitudes) as float64 numpy arrays."""
+    sp, nlat, nlon = ctypes.c_double(), ctypes.c_int(), ctypes.c_int()
+    _check(lib().sbslpm_output_grid(int(point_count), ctypes.byref(sp), ctypes.byref(nlat), ctypes.byref(nlon),
+                                    None, None), "sbslpm_output_grid")
+    lats, lons = np.zeros(nlat.value), np.zeros(nlon.value)
+    _check(lib().sbslpm_output_grid(int(point_count), ctypes.byref(sp), ctypes.byref(nlat), ctypes.byref(nlon),
+                                    _dp(lats), _dp(lons)), "sbslpm_output_grid")
+    return sp.value, lats, lons
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class NcFile:
+    """netCDF classic (64-bit offset) writer with the netCDF library's call
+    pattern (nc_def_dim, nc_def_var, nc_put_att_*, nc_enddef, nc_put_vara_*,
+    nc_close) as the reference drivers use it.  Host arrays."""
+
+    INT, DOUBLE, GLOBAL = 4, 6, -1
+
+    def __init__(self, path: str):
+        h = _VP()
+        _check(lib().sbslpm_nc_create(str(path).encode(), ctypes.byref(h)), "sbslpm_nc_create")
+        self._h = h
+
+    def def_dim(self, name: str, length: int) -> int:
+        d = ctypes.c_int()
+        _check(lib().sbslpm_nc_def_dim(self._h, name.encode(), int(length), ctypes.byref(d)), "sbslpm_nc_def_dim")
+        return d.value
+
+    def def_var(self, name: str, nctype: int, dims) -> int:
+        dims = (ctypes.c_int * max(len(dims), 1))(*dims)
+        v = ctypes.c_int()
+        _check(lib().sbslpm_nc_def_var(self._h, name.encode(), int(nctype), len(dims) if dims else 0, dims,
+                                       ctypes.byref(v)), "sbslpm_nc_def_var")
+        return v.value
+
+    def put_att(self, varid: int, name: str, value):
+        if isinstance(value, str):
+            _check(lib().sbslpm_nc_put_att_text(self._h, varid, name.encode(), value.encode()), "sbslpm_nc_put_att")
+            return
+        arr = np.atleast_1d(value)
+        if np.issubdtype(arr.dtype, np.integer):
+            a = np.ascontiguousarray(arr, np.int32)
+            _check(lib().sbslpm_nc_put_att_int(self._h, varid, name.encode(), a.size,
+                                               a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))), "sbslpm_nc_put_att")
+        else:
+            a = np.ascontiguousarray(arr, np.float64)
+            _check(lib().sbslpm_nc_put_att_double(self._h, varid, name.encode(), a.size, _dp(a)), "sbslpm_nc_put_att")
+
+    def enddef(self):
+        _check(lib().sbslpm_nc_enddef(self._h), "sbslpm_nc_enddef")
+
+    def put_vara(self, varid: int, data, start=None):
+        data = np.asarray(data)
+        cl = ctypes.c_long * max(data.ndim, 1)
+        st = cl(*(start if start is not None else [0] * data.ndim))
+        cnt = cl(*data.shape)
+        if np.issubdtype(data.dtype, np.integer):
+            a = np.ascontiguousarray(data, np.int32)
+            _check(lib().sbslpm_nc_put_vara_int(self._h, varid, st, cnt, a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))),
+                   "sbslpm_nc_put_vara")
+        else:
+            a = np.ascontiguousarray(data, np.float64)
+            _check(lib().sbslpm_nc_put_vara_double(self._h, varid, st, cnt, _dp(a)), "sbslpm_nc_put_vara")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _check(lib().sbslpm_nc_close(self._h), "sbslpm_nc_close")
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 def direct_sum_inv_lap(x, y, z, area, pots, soln):
