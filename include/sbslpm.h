@@ -338,6 +338,20 @@ sbslpm_status sbslpm_batch_cc_info(const sbslpm_batch* batch, int* mode, double*
 sbslpm_status sbslpm_batch_cc_groups(const sbslpm_batch* batch, int n, int* degree, int* members, int* mode,
                                      double* ms_cuda_cores, double* ms_tensor_cores);
 
+/* ---------------- Poisson (inverse Laplacian) FMM ---------------- */
+
+/* The solve of executables/poisson_eq_fmm.cpp:128-160 on a spectral-FMM
+ * context (proxy_degree 0, velocity SBSLPM_VEL_FMM): upward_pass, then
+ * poisson_fmm_interactions (src/fmm_interactions/inverse_poisson.cpp:9-34,
+ * kernel -1/(4 pi) log(1 - x.y), pairs with x.y >= 1 - 1e-15 skipped), then
+ * downward_pass (src/fmm_funcs.cpp:357-372); soln[leaf][q] is written.
+ * sbslpm_poisson_fmm_interactions adds into target[panel][q] from
+ * source[panel][q] like the reference; sbslpm_downward_pass updates
+ * proxy_target[panel][q] in place and writes soln[leaf][q].  Device pointers. */
+sbslpm_status sbslpm_poisson_fmm(sbslpm_ctx* ctx, const double* area, const double* pots, double* soln);
+sbslpm_status sbslpm_poisson_fmm_interactions(sbslpm_ctx* ctx, const double* source, double* target);
+sbslpm_status sbslpm_downward_pass(sbslpm_ctx* ctx, double* proxy_target, double* soln);
+
 /* ---------------- output path (the drivers' per-step output) ---------------- */
 
 /* Replaces interp_to_latlon_host (src/interp_funcs.hpp:22-77, host, OpenMP):

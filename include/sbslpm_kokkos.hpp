@@ -128,4 +128,34 @@ void direct_sum_inv_lap(const RunConfig& run_config, V1 xcos, V1 ycos, V1 zcos, 
         "sbslpm_direct_sum_inv_lap");
 }
 
+// poisson_fmm_interactions (src/fmm_interactions/inverse_poisson.cpp:9-34,
+// called from executables/poisson_eq_fmm.cpp:148): target_pots += the log
+// kernel over the interaction list, which the library rebuilds from run_config.
+template <class RunConfig, class V2, class VList, class VPanels>
+void poisson_fmm_interactions(const RunConfig& run_config, V2& target_pots, V2& source_vals,
+                              VList& /*interaction_list*/, VPanels cubed_sphere_panels, V2& interp_vals) {
+  sbslpm_ctx* c = context_for(run_config, 1.0);
+  long sizes[4];
+  check(sbslpm_get_sizes(c, sizes), "sbslpm_get_sizes");
+  if ((long)cubed_sphere_panels.extent(0) != sizes[0] || (long)target_pots.extent(0) != sizes[0] ||
+      (long)interp_vals.extent(0) != sizes[2])
+    throw std::runtime_error("poisson_fmm_interactions: view sizes do not match run_config");
+  check(sbslpm_poisson_fmm_interactions(c, source_vals.data(), target_pots.data()),
+        "sbslpm_poisson_fmm_interactions");
+}
+
+// downward_pass (src/fmm_funcs.cpp:357-372, called from
+// executables/poisson_eq_fmm.cpp:156).
+template <class RunConfig, class V2, class VPanels>
+void downward_pass(const RunConfig& run_config, V2& interp_vals, VPanels cubed_sphere_panels, V2& proxy_target_pots,
+                   V2& sols) {
+  sbslpm_ctx* c = context_for(run_config, 1.0);
+  long sizes[4];
+  check(sbslpm_get_sizes(c, sizes), "sbslpm_get_sizes");
+  if ((long)cubed_sphere_panels.extent(0) != sizes[0] || (long)sols.extent(0) != sizes[1] ||
+      (long)interp_vals.extent(0) != sizes[2])
+    throw std::runtime_error("downward_pass: view sizes do not match run_config");
+  check(sbslpm_downward_pass(c, proxy_target_pots.data(), sols.data()), "sbslpm_downward_pass");
+}
+
 }  // namespace sbslpm_kokkos

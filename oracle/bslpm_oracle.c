@@ -825,3 +825,54 @@ void orc_xyz_vel_to_uv_vel(long n, const double* x, const double* y, const doubl
     }
   }
 }
+
+/* ---------------- Poisson FMM: src/fmm_interactions/inverse_poisson*.{hpp,cpp} ---------------- */
+
+/* poisson_fmm_interactions (src/fmm_interactions/inverse_poisson.cpp:9-34)
+ * with one rank: for each list entry, poisson_panel_interaction
+ * (src/fmm_interactions/inverse_poisson_impl.hpp:22-52) adds
+ * -1/(4 pi) log(1 - x_t.x_s) w_s over the two panels' proxy points, skipping
+ * pairs with x_t.x_s >= 1 - 1e-15.  Entries grouped by target panel (stable),
+ * sources in list order, source points k in order. */
+void orc_poisson_fmm_interactions(int levels, int degree, const orc_panel* p, const double* interp, long n_list,
+                                  const int* list, const double* source, double* target) {
+  int q = (degree + 1) * (degree + 1), P = orc_panel_count(levels);
+  long* start = (long*)calloc((size_t)P + 1, sizeof(long));
+  long* order = (long*)malloc(sizeof(long) * (size_t)(n_list > 0 ? n_list : 1));
+  for (long i = 0; i < n_list; i++) start[list[3 * i] + 1]++;
+  for (int i = 0; i < P; i++) start[i + 1] += start[i];
+  long* fill = (long*)malloc(sizeof(long) * (size_t)P);
+  for (int i = 0; i < P; i++) fill[i] = start[i];
+  for (long i = 0; i < n_list; i++) order[fill[list[3 * i]]++] = i;
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int t = 0; t < P; t++) {
+    double xt[3], xs[3];
+    for (long e = start[t]; e < start[t + 1]; e++) {
+      int s = list[3 * order[e] + 1];
+      for (int j = 0; j < q; j++) {
+        proxy_point(p, t, interp, j, xt);
+        double a = target[(size_t)t * q + j];
+        for (int k = 0; k < q; k++) {
+          proxy_point(p, s, interp, k, xs);
+          double dp = xt[0] * xs[0] + xt[1] * xs[1] + xt[2] * xs[2];
+          if (dp < 1.0 - 1e-15) a += -0.07957747154594767 * log(1 - dp) * source[(size_t)s * q + k];
+        }
+        target[(size_t)t * q + j] = a;
+      }
+    }
+  }
+  free(start);
+  free(order);
+  free(fill);
+}
+
+/* downward_pass (src/fmm_funcs.cpp:357-372): parent_to_child per level, then
+ * child_panel_copy of the leaves; the one-field form of downward_pass_3. */
+void orc_downward_pass(int levels, int degree, const orc_panel* p, const double* interp, double* t, double* s) {
+  int q = (degree + 1) * (degree + 1), P = orc_panel_count(levels);
+  double* z = (double*)calloc((size_t)2 * P * q, sizeof(double));
+  double* zs = (double*)calloc((size_t)2 * orc_leaf_count(levels) * q, sizeof(double));
+  orc_downward_pass_3(levels, degree, p, interp, t, z, z + (size_t)P * q, s, zs, zs + (size_t)orc_leaf_count(levels) * q);
+  free(z);
+  free(zs);
+}

@@ -78,6 +78,12 @@ void orc_bve_step(const orc_bve_problem* pb, double* vors, double* vel_x, double
 void orc_direct_sum_inv_lap(int n, const double* x, const double* y, const double* z, const double* area,
                             const double* pots, double* soln);
 
+/* Poisson FMM: poisson_fmm_interactions (src/fmm_interactions/inverse_poisson.cpp:9-34,
+ * target += ...) and downward_pass (src/fmm_funcs.cpp:357-372). */
+void orc_poisson_fmm_interactions(int levels, int degree, const orc_panel* p, const double* interp, long n_list,
+                                  const int* list, const double* source, double* target);
+void orc_downward_pass(int levels, int degree, const orc_panel* p, const double* interp, double* t, double* s);
+
 /* Output path: interp_to_latlon_host (src/interp_funcs.hpp:22-77) of one
  * [leaf][q] field to an nlat x nlon grid in degrees, and xyz_vel_to_uv_vel
  * (src/general_utils_impl.hpp:195-229). */

@@ -179,6 +179,22 @@ class Port:
             self.lib.orc_bve_step(ctypes.byref(pb), _dp(v), _dp(vx), _dp(vy), _dp(vz), _dp(tr))
         return v, (vx, vy, vz), (tr if T else None)
 
+    def poisson_fmm_interactions(self, g, source, target):
+        """poisson_fmm_interactions (src/fmm_interactions/inverse_poisson.cpp:9-34): target += ..."""
+        t = np.ascontiguousarray(target, float).copy()
+        lst = np.ascontiguousarray(g["list"], np.int32)
+        self.lib.orc_poisson_fmm_interactions(g["levels"], g["degree"], g["panels"], _dp(g["interp"]),
+                                              ctypes.c_long(len(lst)), _ip(lst),
+                                              _dp(np.ascontiguousarray(source, float)), _dp(t))
+        return t
+
+    def downward_pass(self, g, target):
+        """downward_pass (src/fmm_funcs.cpp:357-372): (updated proxy targets, leaf values)."""
+        t = np.ascontiguousarray(target, float).copy()
+        s = np.zeros_like(g["x"])
+        self.lib.orc_downward_pass(g["levels"], g["degree"], g["panels"], _dp(g["interp"]), _dp(t), _dp(s))
+        return t, s
+
     def interp_to_latlon(self, g, data, lats, lons):
         """interp_to_latlon_host (src/interp_funcs.hpp:22-77): [nlat][nlon]."""
         lats, lons = np.ascontiguousarray(lats, float), np.ascontiguousarray(lons, float)
@@ -224,6 +240,8 @@ class Ref:
         L.ref_interp_to_latlon.restype = None
         L.ref_interp_to_latlon.argtypes = [ctypes.c_void_p, _D, ctypes.c_int, _D, ctypes.c_int, _D, _D]
         L.ref_xyz_vel_to_uv_vel.restype = None
+        L.ref_poisson_fmm.restype = None
+        L.ref_poisson_fmm_interactions.restype = None
         for name in ("ref_unify", "ref_swe_vel_interactions", "ref_swe_tendency", "ref_swe_init", "ref_swe_step"):
             getattr(L, name).restype = None
         L.ref_swe_step.argtypes = [ctypes.c_void_p] + [_D] * 10 + [_I, _I, ctypes.c_double, ctypes.c_int,
@@ -307,6 +325,18 @@ class Ref:
 
     def locate(self, c, x, y, z) -> int:
         return self.lib.ref_point_locate_panel(c["h"], x, y, z)
+
+    def poisson_fmm(self, c, pots):
+        """The Poisson FMM driver's solve: (proxy source, proxy target, soln)."""
+        P, A, q = c["P"], c["A"], c["q"]
+        src, tgt, soln = np.zeros((P, q)), np.zeros((P, q)), np.zeros((A, q))
+        self.lib.ref_poisson_fmm(c["h"], _dp(np.ascontiguousarray(pots, float)), _dp(src), _dp(tgt), _dp(soln))
+        return src, tgt, soln
+
+    def poisson_fmm_interactions(self, c, source, target):
+        t = np.ascontiguousarray(target, float).copy()
+        self.lib.ref_poisson_fmm_interactions(c["h"], _dp(np.ascontiguousarray(source, float)), _dp(t))
+        return t
 
     def interp_to_latlon(self, c, data, lats, lons):
         lats, lons = np.ascontiguousarray(lats, float), np.ascontiguousarray(lons, float)

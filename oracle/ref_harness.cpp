@@ -16,6 +16,8 @@
 //   interp_vals_bli / point_locate_panel (src/interp_funcs_impl.hpp:11-142)
 //   bve_initialize                 (src/initial_conditions.cpp:358-385)
 //   direct_sum_inv_lap             (src/direct_sum.cpp:8-15)
+//   poisson_fmm_interactions, downward_pass
+//                                  (src/fmm_interactions/inverse_poisson.cpp:9-34, src/fmm_funcs.cpp:357-372)
 //   interp_to_latlon_host          (src/interp_funcs.hpp:22-77)
 //   xyz_vel_to_uv_vel              (src/general_utils_impl.hpp:195-229)
 // The reference's bve_time_step.cpp is included textually (unmodified) so that
@@ -31,6 +33,7 @@
 #include "fmm_interactions/bve_vel.hpp"
 #include "initial_conditions.hpp"
 #include "direct_sum.hpp"
+#include "fmm_interactions/inverse_poisson.hpp"
 #include "bve_time_step.cpp"
 #include "ref_ctx.hpp"
 
@@ -313,6 +316,32 @@ void ref_xyz_vel_to_uv_vel(void* h, const double* vx, const double* vy, const do
   Kokkos::parallel_for(A, xyz_vel_to_uv_vel(c->xcos, c->ycos, c->zcos, X, Y, Z, U, W));
   copy_out(U, u);
   copy_out(W, v);
+}
+
+// The Poisson FMM driver's solve (executables/poisson_eq_fmm.cpp:128-160):
+// upward_pass, poisson_fmm_interactions, downward_pass on the context's list.
+void ref_poisson_fmm(void* h, const double* pots, double* proxy_source, double* proxy_target, double* soln) {
+  RefCtx* c = static_cast<RefCtx*>(h);
+  const int A = c->rc.active_panel_count, P = c->rc.panel_count;
+  V2 p("pots", A, c->q), s("soln", A, c->q), src("proxy source", P, c->q), tgt("proxy target", P, c->q);
+  copy_in(p, pots);
+  upward_pass(c->rc, c->interp, c->panels, c->area, p, src);
+  copy_out(src, proxy_source);
+  poisson_fmm_interactions(c->rc, tgt, src, c->list, c->panels, c->interp);
+  downward_pass(c->rc, c->interp, c->panels, tgt, s);
+  copy_out(tgt, proxy_target);
+  copy_out(s, soln);
+}
+
+// poisson_fmm_interactions alone (target += ...).
+void ref_poisson_fmm_interactions(void* h, const double* source, double* target) {
+  RefCtx* c = static_cast<RefCtx*>(h);
+  const int P = c->rc.panel_count;
+  V2 src("proxy source", P, c->q), tgt("proxy target", P, c->q);
+  copy_in(src, source);
+  copy_in(tgt, target);
+  poisson_fmm_interactions(c->rc, tgt, src, c->list, c->panels, c->interp);
+  copy_out(tgt, target);
 }
 
 int ref_num_threads(void) { return Kokkos::num_threads(); }

@@ -116,6 +116,9 @@ def lib() -> ctypes.CDLL:
     L.sbslpm_direct_sum_bve_noalloc.argtypes = L.sbslpm_direct_sum_bve.argtypes
     L.sbslpm_direct_sum_inv_lap.argtypes = [ctypes.c_long] + [_VP] * 7
     L.sbslpm_interp_to_latlon.argtypes = [_VP, _VP, ctypes.c_int, _VP, ctypes.c_int, _VP, _VP]
+    L.sbslpm_poisson_fmm.argtypes = [_VP] * 4
+    L.sbslpm_poisson_fmm_interactions.argtypes = [_VP] * 3
+    L.sbslpm_downward_pass.argtypes = [_VP] * 3
     L.sbslpm_xyz_vel_to_uv_vel.argtypes = [_VP] * 9
     L.sbslpm_output_grid.argtypes = [ctypes.c_long, _D, _I, _I, _D, _D]
     _L = ctypes.POINTER(ctypes.c_long)
@@ -335,6 +338,27 @@ class Context:
         _check(lib().sbslpm_get_interactions(self._h, out), "sbslpm_get_interactions")
         arr = np.ctypeslib.as_array(ctypes.cast(out, ctypes.POINTER(ctypes.c_int)), (n, 3))
         return arr[: self.interaction_count].copy()
+
+    # -- Poisson FMM ----------------------------------------------------
+    def poisson_fmm(self, area, pots, soln):
+        """The Poisson FMM driver's solve (executables/poisson_eq_fmm.cpp:128-160): soln written."""
+        lq = (self.leaf_count, self.q)
+        self._sync_stream()
+        _check(lib().sbslpm_poisson_fmm(self._h, _dev(area, "area", lq), _dev(pots, "pots", lq),
+                                        _dev(soln, "soln", lq)), "sbslpm_poisson_fmm")
+
+    def poisson_fmm_interactions(self, source, target):
+        """poisson_fmm_interactions (src/fmm_interactions/inverse_poisson.cpp:9-34): target += ..."""
+        pq = (self.panel_count, self.q)
+        self._sync_stream()
+        _check(lib().sbslpm_poisson_fmm_interactions(self._h, _dev(source, "source", pq), _dev(target, "target", pq)),
+               "sbslpm_poisson_fmm_interactions")
+
+    def downward_pass(self, proxy_target, soln):
+        """downward_pass (src/fmm_funcs.cpp:357-372): proxy_target updated, soln written."""
+        self._sync_stream()
+        _check(lib().sbslpm_downward_pass(self._h, _dev(proxy_target, "proxy_target", (self.panel_count, self.q)),
+                                          _dev(soln, "soln", (self.leaf_count, self.q))), "sbslpm_downward_pass")
 
     # -- output path ----------------------------------------------------
     def interp_to_latlon(self, data, lats, lons, out=None):

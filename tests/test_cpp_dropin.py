@@ -51,6 +51,15 @@ PROGRAM = textwrap.dedent(r"""
       } catch (const std::exception& e) {
         std::printf("swe exception: %s\n", e.what());
       }
+      // the Poisson FMM driver's calls (executables/poisson_eq_fmm.cpp:148-156)
+      V2 ptgt("pt", 126, 16), psrc("ps", 126, 16), soln("s", 96, 16);
+      try {
+        sbslpm_kokkos::poisson_fmm_interactions(rc, ptgt, psrc, list, panels, interp);
+        sbslpm_kokkos::downward_pass(rc, interp, panels, ptgt, soln);
+        std::printf("poisson solved\n");
+      } catch (const std::exception& e) {
+        std::printf("poisson exception: %s\n", e.what());
+      }
       return 0;
     }
 """)
@@ -72,3 +81,4 @@ def test_cpp_dropin_header_compiles_and_reaches_the_abi(sb, tmp_path):
         pytest.skip("a GPU is present; this test checks the CPU-side path only")
     assert "exception: sbslpm_create" in out.stdout and "no CUDA device" in out.stdout, out.stdout
     assert "swe exception: sbslpm_create" in out.stdout, out.stdout
+    assert "poisson exception: sbslpm_create" in out.stdout, out.stdout
