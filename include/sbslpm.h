@@ -76,7 +76,15 @@ typedef struct {
    * units of the radius; src/swe_time_step_2_impl.hpp:103); 1 on the unit
    * sphere with the height field holding g*h. */
   double g_over_a;
+  /* BVE forcing (src/forcing_funcs.cpp:82-96; namelist keys forcing=1 and
+   * forcing_type): SBSLPM_FORCING_NONE, _SSW (bve_ssw_forcing, wavenumber 1)
+   * or _SSW2 (bve_ssw_forcing_2, wavenumber 2) added to the vorticity that
+   * sets the source strengths of every velocity evaluation, at the step's
+   * time (seconds; the ramps are in days). */
+  int forcing;
 } sbslpm_config;
+
+enum { SBSLPM_FORCING_NONE = 0, SBSLPM_FORCING_SSW = 1, SBSLPM_FORCING_SSW2 = 2 };
 
 /* Same fields and order as the reference's CubedSpherePanel
  * (src/initialize_cubed_sphere.hpp:8-29); is_leaf is an int here. */

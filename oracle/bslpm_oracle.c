@@ -722,9 +722,41 @@ static void velocity_eval(const orc_bve_problem* pb, const double* eff_vor, cons
   orc_downward_pass_3(pb->levels, pb->degree, pb->panels, pb->interp, t1, t2, t3, vel, vel + n, vel + 2 * n);
 }
 
-/* bve_back_rk4_step: src/bve_time_step.cpp:311-419 (forcing off, so the
- * effective vorticity is the (displaced) relative vorticity:
- * src/forcing_funcs.cpp:82-96). */
+/* bve_forcing (src/forcing_funcs.cpp:82-96): eff = vor without forcing;
+ * with it, bve_ssw_forcing (type 1, :6-43) or bve_ssw_forcing_2 (type 2,
+ * :45-80) per leaf panel, points in order, bcomp kept from the panel's
+ * previous point where lat <= 0 as the reference's loop keeps it. */
+static void bve_forcing(const orc_bve_problem* pb, const double* vor, double* eff) {
+  int A = orc_leaf_count(pb->levels), q = (pb->degree + 1) * (pb->degree + 1);
+  if (pb->forcing == 0) {
+    memcpy(eff, vor, sizeof(double) * (size_t)A * q);
+    return;
+  }
+  double Tp = 4.0, Tf = 4.0 + 11.0, theta1 = ORC_PI / 3.0, time = pb->time;
+  for (int i = 0; i < A; i++) {
+    double lat, lon, acomp, bcomp = 0, ccomp;
+    for (int j = 0; j < q; j++) {
+      size_t o = (size_t)i * q + j;
+      double x = pb->x[o], y = pb->y[o], z = pb->z[o];
+      lat = ORC_PI / 2.0 - atan2(sqrt(x * x + y * y), z); /* xyz_to_latlon, src/general_utils_impl.hpp:230-235 */
+      lon = atan2(y, x);
+      if (time / 86400.0 < Tp) acomp = 0.5 * (1.0 - cos(ORC_PI * (time / 86400.0) / Tp));
+      else if (time / 86400.0 < Tf - Tp) acomp = 1.0;
+      else if (time / 86400.0 < Tf) acomp = 0.5 * (1.0 - cos(ORC_PI + ORC_PI * ((time / 86400.0) - Tf + Tp) / Tp));
+      else acomp = 0.0;
+      if (lat > 0) {
+        ccomp = pow(tan(theta1), 2) / pow(tan(lat), 2);
+        bcomp = ccomp * exp(1.0 - ccomp);
+      }
+      if (pb->forcing == 1) eff[o] = vor[o] + 0.6 * pb->omega * acomp * bcomp * cos(lon);
+      else eff[o] = vor[o] + 1.2 * pb->omega * acomp * bcomp * cos(2.0 * lon);
+    }
+  }
+}
+
+/* bve_back_rk4_step: src/bve_time_step.cpp:311-419; the effective vorticity
+ * of every stage is bve_forcing of the (displaced) relative vorticity at the
+ * step's time. */
 void orc_bve_step(const orc_bve_problem* pb, double* vors, double* vel_x, double* vel_y, double* vel_z,
                   double* tracers) {
   int d = pb->degree, q = (d + 1) * (d + 1), P = orc_panel_count(pb->levels), A = orc_leaf_count(pb->levels);
@@ -743,13 +775,16 @@ void orc_bve_step(const orc_bve_problem* pb, double* vors, double* vel_x, double
   double* dep = (double*)calloc(3 * n, sizeof(double));
   double* nv = (double*)calloc(n, sizeof(double));
   double* ntr = (double*)calloc(n * (T > 0 ? T : 1), sizeof(double));
+  double* eff = (double*)calloc(n, sizeof(double));
 
-  velocity_eval(pb, vors, dx, dy, dz, proxy, t1, t2, t3, v[0]);
+  bve_forcing(pb, vors, eff);
+  velocity_eval(pb, eff, dx, dy, dz, proxy, t1, t2, t3, v[0]);
   const double fr[3] = {0.5, 0.5, 1.0};
   for (int s = 1; s < 4; s++) {
     disp_update(A, q, off, pb->x, pb->y, pb->z, v[s - 1], vors, dvor, dx, dy, dz, fr[s - 1] * pb->dt, pb->omega);
     disp_interp(pb->panels, off, d, pb->interp, dx, dy, dz);
-    velocity_eval(pb, dvor, dx, dy, dz, proxy, t1, t2, t3, v[s]);
+    bve_forcing(pb, dvor, eff);
+    velocity_eval(pb, eff, dx, dy, dz, proxy, t1, t2, t3, v[s]);
   }
   orc_bve_departure(pb->levels, d, pb->panels, pb->x, pb->y, pb->z, v[0], v[1], v[2], v[3], pb->dt, dep, dep + n,
                     dep + 2 * n);
@@ -761,7 +796,7 @@ void orc_bve_step(const orc_bve_problem* pb, double* vors, double* vel_x, double
   memcpy(vel_z, v[0] + 2 * n, sizeof(double) * n);
   free(dx); free(dy); free(dz); free(proxy); free(t1); free(t2); free(t3);
   for (int k = 0; k < 4; k++) free(v[k]);
-  free(dvor); free(dep); free(nv); free(ntr);
+  free(dvor); free(dep); free(nv); free(ntr); free(eff);
 }
 
 /* inv_lap: src/direct_sum_impl.hpp:20-27 (row i sums over j in order). */

@@ -70,6 +70,8 @@ typedef struct {
   const double *x, *y, *z, *area;
   long n_list;
   const int* list;
+  int forcing;  /* 0 none, 1 ssw, 2 ssw2 (src/forcing_funcs.cpp:82-96) */
+  double time;  /* the step's time (seconds), for the forcing */
 } orc_bve_problem;
 void orc_bve_step(const orc_bve_problem* pb, double* vors, double* vel_x, double* vel_y, double* vel_z,
                   double* tracers);

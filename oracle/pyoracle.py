@@ -59,6 +59,8 @@ class OrcProblem(ctypes.Structure):
         ("area", _D),
         ("n_list", ctypes.c_long),
         ("list", _I),
+        ("forcing", ctypes.c_int),
+        ("time", ctypes.c_double),
     ]
 
 
@@ -165,17 +167,20 @@ class Port:
                                _dp(np.ascontiguousarray(vors)), T, _dp(tr), ctypes.c_double(omega), _dp(nv), _dp(ntr))
         return nv, (ntr if T else None)
 
-    def bve_step(self, g, vors, tracers=None, *, dt, omega, eps, mode=0, nsteps=1):
-        """nsteps of bve_back_rk4_step; returns (vors, (vx, vy, vz), tracers)."""
+    def bve_step(self, g, vors, tracers=None, *, dt, omega, eps, mode=0, nsteps=1, forcing=0, time=0.0):
+        """nsteps of bve_back_rk4_step from time (forcing 0 none, 1 ssw, 2 ssw2);
+        returns (vors, (vx, vy, vz), tracers)."""
         A, q = g["x"].shape
         T = 0 if tracers is None else tracers.shape[2]
         lst = np.ascontiguousarray(g["list"], dtype=np.int32)
         pb = OrcProblem(g["levels"], g["degree"], T, mode, eps, omega, dt, g["panels"], _dp(g["interp"]), _dp(g["x"]),
-                        _dp(g["y"]), _dp(g["z"]), _dp(g["area"]), len(lst), _ip(lst) if len(lst) else None)
+                        _dp(g["y"]), _dp(g["z"]), _dp(g["area"]), len(lst), _ip(lst) if len(lst) else None,
+                        int(forcing), float(time))
         v = np.array(vors, dtype=np.float64, order="C")
         tr = np.zeros(1) if tracers is None else np.array(tracers, dtype=np.float64, order="C")
         vx, vy, vz = (np.zeros((A, q)) for _ in range(3))
-        for _ in range(nsteps):
+        for k in range(nsteps):
+            pb.time = float(time) + k * dt
             self.lib.orc_bve_step(ctypes.byref(pb), _dp(v), _dp(vx), _dp(vy), _dp(vz), _dp(tr))
         return v, (vx, vy, vz), (tr if T else None)
 
@@ -241,6 +246,7 @@ class Ref:
         L.ref_interp_to_latlon.argtypes = [ctypes.c_void_p, _D, ctypes.c_int, _D, ctypes.c_int, _D, _D]
         L.ref_xyz_vel_to_uv_vel.restype = None
         L.ref_poisson_fmm.restype = None
+        L.ref_set_forcing.restype = None
         L.ref_poisson_fmm_interactions.restype = None
         for name in ("ref_unify", "ref_swe_vel_interactions", "ref_swe_tendency", "ref_swe_init", "ref_swe_step"):
             getattr(L, name).restype = None
@@ -325,6 +331,10 @@ class Ref:
 
     def locate(self, c, x, y, z) -> int:
         return self.lib.ref_point_locate_panel(c["h"], x, y, z)
+
+    def set_forcing(self, c, forcing: int):
+        """forcing 0 none, 1 ssw, 2 ssw2 (RunConfig::forcing / forcing_type)."""
+        self.lib.ref_set_forcing(c["h"], int(forcing))
 
     def poisson_fmm(self, c, pots):
         """The Poisson FMM driver's solve: (proxy source, proxy target, soln)."""

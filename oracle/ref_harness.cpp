@@ -150,6 +150,13 @@ void ref_bve_initialize(void* h, const char* ic, int balance, double* vors_out) 
   copy_out(v, vors_out);
 }
 
+// RunConfig::forcing / forcing_type (src/run_config.hpp:35-36): 0 none, 1 "ssw", 2 "ssw2".
+void ref_set_forcing(void* h, int forcing) {
+  RefCtx* c = static_cast<RefCtx*>(h);
+  c->rc.forcing = forcing != 0;
+  c->rc.forcing_type = forcing == 2 ? "ssw2" : "ssw";
+}
+
 // nsteps calls of bve_back_rk4_step; vors / vel / tracers are in-out (A x q [x T]).
 void ref_bve_step(void* h, double* vors, double* vel_x, double* vel_y, double* vel_z, double* tracers,
                   double time, int nsteps) {

@@ -20,6 +20,7 @@ import numpy as np
 
 __all__ = [
     "SbslpmError", "Config", "Panel", "InteractPair", "FP64", "MIXED", "VEL_FMM", "VEL_DIRECT", "library_path",
+    "FORCING_NONE", "FORCING_SSW", "FORCING_SSW2",
     "lib", "config_default", "read_run_config", "panel_count", "leaf_count", "cubed_sphere_panels_init",
     "interp_init", "cube_sphere_spec_points", "dual_tree_traversal", "interp_vals_bli", "point_locate_panel",
     "Context", "direct_sum_bve", "direct_sum_inv_lap", "output_grid", "NcFile", "kernel_launches", "Grid",
@@ -28,6 +29,7 @@ __all__ = [
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 FP64, MIXED = 0, 1
+FORCING_NONE, FORCING_SSW, FORCING_SSW2 = 0, 1, 2
 VEL_FMM, VEL_DIRECT = 0, 1
 
 _D = ctypes.POINTER(ctypes.c_double)
@@ -58,6 +60,7 @@ class Config(ctypes.Structure):
         ("proxy_degree", ctypes.c_int),
         ("leaf_size", ctypes.c_int),
         ("g_over_a", ctypes.c_double),
+        ("forcing", ctypes.c_int),
     ]
 
 

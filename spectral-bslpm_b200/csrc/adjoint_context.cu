@@ -75,8 +75,8 @@ sbslpm_status sbslpm_bve_adjoint_step(sbslpm_ctx* c, const double* x, const doub
   if (c->cfg.precision != SBSLPM_FP64 || !(c->cfg.velocity == SBSLPM_VEL_DIRECT || c->tree))
     return set_last_error("the adjoint step runs on the float64 direct-sum or treecode velocity"),
            SBSLPM_ERR_CONFIG;
-  if (c->cfg.tracer_count != 0)
-    return set_last_error("the adjoint step needs a context without tracers"), SBSLPM_ERR_CONFIG;
+  if (c->cfg.tracer_count != 0 || c->cfg.forcing != SBSLPM_FORCING_NONE)
+    return set_last_error("the adjoint step needs a context without tracers or forcing"), SBSLPM_ERR_CONFIG;
   SB_TRY(adjoint_setup(c));
   SB_TRY(near_autotune(c, x, y, z, area, vors));
   cudaStream_t st = c->stream();

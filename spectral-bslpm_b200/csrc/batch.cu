@@ -463,6 +463,8 @@ sbslpm_status sbslpm_batch_create(const sbslpm_config* base, int members, const 
     if (!(theta[m] > 0) || !std::isfinite(theta[m]))
       return set_last_error("batched members need a positive finite theta"), SBSLPM_ERR_CONFIG;
   }
+  if (c.forcing != SBSLPM_FORCING_NONE)
+    return set_last_error("batched members run without forcing"), SBSLPM_ERR_CONFIG;
   c.proxy_degree = proxy_degree[0];
   c.fmm_theta = theta[0];
   if (c.levels < 1 || c.levels > 12 || c.interp_degree < 0 || c.interp_degree > kMaxDegree ||

@@ -85,14 +85,15 @@ __device__ __forceinline__ void bltc_sources_body(const TreeGeom& tg, const Step
     const long i = (long)f * npl + k;
     double xx = x[i], yy = y[i], zz = z[i], w;
     if (stage == 0) {
-      w = area[i] * vors[i];
+      w = area[i] * (fg.force ? vors[i] + fg.force[i] : vors[i]);
     } else {
       const double vx = vprev[i], vy = vprev[N + i], vz = vprev[2 * N + i];
       xx += vx * dt_s;
       yy += vy * dt_s;
       zz += vz * dt_s;
       project_to_sphere(xx, yy, zz);
-      w = area[i] * (vors[i] + 2 * tg.omega * z[i] - 2 * tg.omega * zz);
+      const double dvor = vors[i] + 2 * tg.omega * z[i] - 2 * tg.omega * zz;
+      w = area[i] * (fg.force ? dvor + fg.force[i] : dvor);
     }
     if (stage == 0) project_to_sphere(xx, yy, zz);
     psrc[i] = make_double4(xx, yy, zz, w);

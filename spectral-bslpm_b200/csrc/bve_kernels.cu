@@ -51,13 +51,13 @@ __global__ void k_leaf_sources(StepGeom g, int stage, double dt_s, const double*
   double px = g.px[o], py = g.px[pn + o], pz = g.px[2 * pn + o];
   double w;
   if (stage == 0) {
-    w = area[i] * vors[i];
+    w = area[i] * (g.force ? vors[i] + g.force[i] : vors[i]);
   } else {
     double vx = vprev[i], vy = vprev[n + i], vz = vprev[2 * n + i];
     double xx = x[i] + vx * dt_s, yy = y[i] + vy * dt_s, zz = z[i] + vz * dt_s;
     project_to_sphere(xx, yy, zz);
     double dvor = vors[i] + 2 * g.omega * z[i] - 2 * g.omega * zz;
-    w = area[i] * dvor;
+    w = area[i] * (g.force ? dvor + g.force[i] : dvor);
     px += dt_s * vx;
     py += dt_s * vy;
     pz += dt_s * vz;
@@ -139,13 +139,13 @@ __device__ __forceinline__ void upward_subtree_body(const StepGeom& g, int root_
         } else {
           double px = g.px[o], py = g.px[pn + o], pz = g.px[2 * pn + o];
           if (stage == 0) {
-            w = area[i] * vors[i];
+            w = area[i] * (g.force ? vors[i] + g.force[i] : vors[i]);
           } else {
             double vx = vprev[i], vy = vprev[ln + i], vz = vprev[2 * ln + i];
             double xx = x[i] + vx * dt_s, yy = y[i] + vy * dt_s, zz = z[i] + vz * dt_s;
             project_to_sphere(xx, yy, zz);
             double dvor = vors[i] + 2 * g.omega * z[i] - 2 * g.omega * zz;
-            w = area[i] * dvor;
+            w = area[i] * (g.force ? dvor + g.force[i] : dvor);
             px += dt_s * vx;
             py += dt_s * vy;
             pz += dt_s * vz;
@@ -984,6 +984,41 @@ __global__ void __launch_bounds__(kDirectThreads)
   if (i < n) soln[i] += acc;
 }
 
+// The forcing of bve_ssw_forcing (type 1) / bve_ssw_forcing_2 (type 2),
+// src/forcing_funcs.cpp:6-80: one thread per leaf panel walking its points
+// in order as the reference's functor does, so that bcomp carries over from
+// the panel's previous point where lat <= 0 (the reference sets it only for
+// lat > 0).  force = 0.6 omega a b cos(lon) (type 1) or 1.2 omega a b
+// cos(2 lon) (type 2), added to the vorticity by the source kernels.
+__global__ void k_ssw_forcing(int leaves, int q, int type, double omega, const double* __restrict__ time,
+                              const double* __restrict__ x, const double* __restrict__ y,
+                              const double* __restrict__ z, double* __restrict__ force) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= leaves) return;
+  const double t = *time, Tp = 4.0, Tf = 4.0 + 11.0, theta1 = kPi / 3.0;
+  double acomp, bcomp = 0;
+  if (t / 86400.0 < Tp) acomp = 0.5 * (1.0 - cos(kPi * (t / 86400.0) / Tp));
+  else if (t / 86400.0 < Tf - Tp) acomp = 1.0;
+  else if (t / 86400.0 < Tf) acomp = 0.5 * (1.0 - cos(kPi + kPi * ((t / 86400.0) - Tf + Tp) / Tp));
+  else acomp = 0.0;
+  for (int j = 0; j < q; j++) {
+    const long o = (long)i * q + j;
+    const double xx = x[o], yy = y[o], zz = z[o];
+    // xyz_to_latlon, src/general_utils_impl.hpp:230-235
+    const double lat = kPi / 2.0 - atan2(sqrt(xx * xx + yy * yy), zz), lon = atan2(yy, xx);
+    if (lat > 0) {
+      const double tt = tan(theta1), tl = tan(lat);
+      const double ccomp = (tt * tt) / (tl * tl);
+      bcomp = ccomp * exp(1.0 - ccomp);
+    }
+    force[o] = type == 1 ? 0.6 * omega * acomp * bcomp * cos(lon) : 1.2 * omega * acomp * bcomp * cos(2.0 * lon);
+  }
+}
+
+__global__ void k_time_advance(double* time, double dt) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *time += dt;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -1274,6 +1309,15 @@ void launch_direct_bve(long nt, const double* tx, const double* ty, const double
   double* outs[3] = {ux, uy, uz};
   for (int c = 0; c < 3; c++)
     SB_LAUNCH(k_reduce_groups, blocks_for(nt, 256), 256, 0, st, partial + (long)c * nt, groups, nt, 3 * nt, outs[c]);
+}
+
+void launch_ssw_forcing(int leaves, int q, int type, double omega, const double* time, const double* x,
+                        const double* y, const double* z, double* force, cudaStream_t st) {
+  SB_LAUNCH(k_ssw_forcing, blocks_for(leaves, 128), 128, 0, st, leaves, q, type, omega, time, x, y, z, force);
+}
+
+void launch_time_advance(double* time, double dt, cudaStream_t st) {
+  SB_LAUNCH(k_time_advance, 1, 32, 0, st, time, dt);
 }
 
 void launch_inv_lap(long n, const double* x, const double* y, const double* z, const double* area,

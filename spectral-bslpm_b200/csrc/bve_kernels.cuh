@@ -33,6 +33,7 @@ struct StepGeom {
   const double* pd_centre;    // mixed: panel centres [panels][4] (double)
   float4* srcf;               // mixed: packed sources [panels*q] (workspace)
   unsigned* err;              // device error word
+  const double* force;        // forcing added to the leaf vorticity [leaves*q], or null
 };
 
 // Treecode with decoupled proxy degree (bltc_kernels.cu).  The treecode tree
@@ -94,6 +95,11 @@ int direct_groups(long n_targets, long n_sources);
 void launch_direct_bve(long nt, const double* tx, const double* ty, const double* tz, long ns, const double* sx,
                        const double* sy, const double* sz, const double* s, double eps, int precision, double* partial,
                        int groups, double* ux, double* uy, double* uz, cudaStream_t st);
+// bve_ssw_forcing / bve_ssw_forcing_2 (src/forcing_funcs.cpp:6-80) at the
+// device-held time: force[leaf][q]; then time += dt (launch_time_advance).
+void launch_ssw_forcing(int leaves, int q, int type, double omega, const double* time, const double* x,
+                        const double* y, const double* z, double* force, cudaStream_t st);
+void launch_time_advance(double* time, double dt, cudaStream_t st);
 void launch_inv_lap(long n, const double* x, const double* y, const double* z, const double* area,
                     const double* pots, double* soln, cudaStream_t st);
 

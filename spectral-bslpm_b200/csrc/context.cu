@@ -45,6 +45,8 @@ sbslpm_status validate(const sbslpm_config& c) {
   }
   if (!(c.kernel_eps >= 0) || !std::isfinite(c.dt) || !std::isfinite(c.omega) || !std::isfinite(c.g_over_a))
     return set_last_error("kernel_eps, dt and omega must be finite (kernel_eps >= 0)"), SBSLPM_ERR_CONFIG;
+  if (c.forcing != SBSLPM_FORCING_NONE && c.forcing != SBSLPM_FORCING_SSW && c.forcing != SBSLPM_FORCING_SSW2)
+    return set_last_error("forcing must be SBSLPM_FORCING_NONE, _SSW or _SSW2"), SBSLPM_ERR_CONFIG;
   return SBSLPM_OK;
 }
 
@@ -304,7 +306,10 @@ void enqueue_step(sbslpm_ctx* c, const double* x, const double* y, const double*
   double* v[4];
   for (int k = 0; k < 4; k++) v[k] = c->vbuf + (size_t)k * 3 * ln;
   const double stage_dt[4] = {0.0, 0.5 * dt, 0.5 * dt, dt};
+  // bve_forcing at the step's time, the same for all four stages (src/bve_time_step.cpp:323-395)
+  if (c->force) launch_ssw_forcing(c->A, c->q, c->cfg.forcing, c->cfg.omega, c->d_time, x, y, z, c->force, st);
   for (int s = 0; s < 4; s++) velocity_eval(c, s, stage_dt[s], s ? v[s - 1] : nullptr, x, y, z, area, vors, v[s]);
+  if (c->force) launch_time_advance(c->d_time, dt, st);
   const int T = c->cfg.tracer_count;
   launch_depart_remap(c->geom, &c->tab, x, y, z, v[0], v[1], v[2], v[3], dt, c->dep, vors, tracers, T, c->newvor,
                       c->newtr, 3, st);
@@ -550,12 +555,19 @@ sbslpm_status sbslpm_create(const sbslpm_config* cfg, sbslpm_ctx** out) {
   if (s == SBSLPM_OK) s = precompute(c);
   if (s == SBSLPM_OK && c->tree) s = precompute_tree(c);
   if (s == SBSLPM_OK) s = allocate_workspace(c);
+  if (s == SBSLPM_OK && cfg->forcing != SBSLPM_FORCING_NONE) {
+    s = dalloc(&c->force, (size_t)c->A * c->q);
+    if (s == SBSLPM_OK) s = dalloc(&c->d_time, 1);
+    if (s == SBSLPM_OK && cudaMemset(c->force, 0, sizeof(double) * c->A * c->q) != cudaSuccess) s = SBSLPM_ERR_CUDA;
+  }
   c->I = (long)c->list.size();
   if (s != SBSLPM_OK) {
     sbslpm_destroy(c);
     return s;
   }
   fill_geom(c);
+  c->geom.force = c->force;
+  c->fgeom.force = c->force;
   if (c->tree) {
     BatchMember m{};
     m.fg = c->fgeom;
@@ -585,7 +597,7 @@ sbslpm_status sbslpm_destroy(sbslpm_ctx* c) {
                   c->s_ntan, c->s_pow15, c->s_filt, c->s_ptan, c->s_pface, c->s_ustart, c->s_umem, c->src2,
                   c->srcf2, c->tend, c->avor, c->adj_src, c->adj_vbar, c->adj_q, c->adj_y, c->adj_part,
                   c->adj_w, c->adj_vel, c->adj_near_ts, c->adj_near_tt, c->adj_cc_ts, c->adj_cc_tt, c->adj_tbar,
-                  c->adj_qbl, c->self};
+                  c->adj_qbl, c->self, c->force, c->d_time};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (c->h_err) cudaFreeHost(c->h_err);
@@ -625,24 +637,27 @@ sbslpm_status sbslpm_get_interactions(const sbslpm_ctx* c, sbslpm_interact_pair*
 long sbslpm_kernel_launches(void) { return launch_counter(); }
 
 sbslpm_status sbslpm_bve_step(sbslpm_ctx* c, const double* x, const double* y, const double* z, const double* area,
-                              double* vors, double* vel_x, double* vel_y, double* vel_z, double* tracers, double) {
+                              double* vors, double* vel_x, double* vel_y, double* vel_z, double* tracers, double time) {
   if (!c || bad(x) || bad(y) || bad(z) || bad(area) || bad(vors) || bad(vel_x) || bad(vel_y) || bad(vel_z) ||
-      (c->cfg.tracer_count > 0 && bad(tracers)))
+      (c->cfg.tracer_count > 0 && bad(tracers)) || !std::isfinite(time))
     return SBSLPM_ERR_ARG;
   SB_TRY(near_autotune(c, x, y, z, area, vors));
+  if (c->force) SB_CUDA(cudaMemcpyAsync(c->d_time, &time, sizeof(double), cudaMemcpyHostToDevice, c->stream()));
   enqueue_step(c, x, y, z, area, vors, vel_x, vel_y, vel_z, tracers);
   return finish(c);
 }
 
 sbslpm_status sbslpm_bve_run(sbslpm_ctx* c, const double* x, const double* y, const double* z, const double* area,
-                             double* vors, double* vel_x, double* vel_y, double* vel_z, double* tracers, double,
+                             double* vors, double* vel_x, double* vel_y, double* vel_z, double* tracers, double time,
                              int nsteps) {
   if (!c || bad(x) || bad(y) || bad(z) || bad(area) || bad(vors) || bad(vel_x) || bad(vel_y) || bad(vel_z) ||
-      (c->cfg.tracer_count > 0 && bad(tracers)) || nsteps < 0)
+      (c->cfg.tracer_count > 0 && bad(tracers)) || nsteps < 0 || !std::isfinite(time))
     return SBSLPM_ERR_ARG;
   SB_TRY(near_autotune(c, x, y, z, area, vors));
   GraphKey key{{x, y, z, area, vors, vel_x, vel_y, vel_z, tracers}};
   cudaStream_t st = c->stream();
+  // step n of the replays runs at time + n dt (each step advances the device time)
+  if (c->force) SB_CUDA(cudaMemcpyAsync(c->d_time, &time, sizeof(double), cudaMemcpyHostToDevice, st));
   if (!c->graph || !(key == c->graph_key)) {
     SB_TRY(capture_graph(c, &c->graph, [&] { enqueue_step(c, x, y, z, area, vors, vel_x, vel_y, vel_z, tracers); }));
     c->graph_key = key;

@@ -66,7 +66,9 @@ struct sbslpm_ctx {
   bool near_tuned = false;
   int near_candidates = 0;
   double near_tuned_ms = 0;
-  sbslpm::BatchMember* self = nullptr;  // this context's treecode as a one-member table (shaped near-field launches)
+  sbslpm::BatchMember* self = nullptr;
+  double* force = nullptr;   // [leaves*q] forcing of the current step (forcing configured)
+  double* d_time = nullptr;  // the step's time on the device, advanced by dt inside each step  // this context's treecode as a one-member table (shaped near-field launches)
   float4 *fsrcf = nullptr, *psrcf = nullptr;
   double* ftgt = nullptr;
   sbslpm::BliTable ftab{};

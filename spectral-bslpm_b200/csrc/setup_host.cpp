@@ -268,7 +268,9 @@ bool read_namelist(const char* path, sbslpm_config* cfg, std::string& msg) {
     return false;
   }
   std::string line;
-  while (std::getline(f, line)) {
+  bool forcing_on = cfg->forcing != SBSLPM_FORCING_NONE, stop = false;
+  std::string forcing_type = cfg->forcing == SBSLPM_FORCING_SSW2 ? "ssw2" : "ssw";
+  while (!stop && std::getline(f, line)) {
     std::stringstream ss(line);
     std::string key, val;
     std::getline(ss, key, '=');
@@ -292,18 +294,27 @@ bool read_namelist(const char* path, sbslpm_config* cfg, std::string& msg) {
       else if (key == "proxy_degree") cfg->proxy_degree = std::stoi(val);
       else if (key == "leaf_size") cfg->leaf_size = std::stoi(val);
       else if (key == "g_over_a") cfg->g_over_a = std::stod(val);
+      else if (key == "forcing") forcing_on = std::stoi(val) == 1;  // src/io_utils.cpp:69-72
+      else if (key == "forcing_type") forcing_type = val;
       else if (key == "out_path" || key == "write_precision" || key == "write_output" || key == "grid_spacing" ||
                key == "end_time" || key == "output_vel" || key == "output_freq" || key == "initial_condition" ||
-               key == "balance_ic" || key == "interp_output" || key == "forcing" || key == "forcing_type" ||
-               key == "topo_type") {
+               key == "balance_ic" || key == "interp_output" || key == "topo_type") {
         // keys of the reference's drivers, not used on this path
       } else {
-        return true;  // the reference stops at the first unknown key ("end")
+        stop = true;  // the reference stops at the first unknown key ("end")
       }
     } catch (const std::exception&) {
       msg = "bad value for namelist key '" + key + "': " + val;
       return false;
     }
+  }
+  // bve_forcing (src/forcing_funcs.cpp:82-96) knows the types "ssw" and "ssw2"
+  if (!forcing_on) cfg->forcing = SBSLPM_FORCING_NONE;
+  else if (forcing_type == "ssw") cfg->forcing = SBSLPM_FORCING_SSW;
+  else if (forcing_type == "ssw2") cfg->forcing = SBSLPM_FORCING_SSW2;
+  else {
+    msg = "forcing_type must be ssw or ssw2, got '" + forcing_type + "'";
+    return false;
   }
   return true;
 }

@@ -328,3 +328,57 @@ def test_treecode_graph_replay_and_determinism(sb):
     step(ctx, a, 2)
     step(ctx, b, 2, graph=True)
     assert torch.equal(a["vors"], b["vors"])
+
+
+@pytest.mark.parametrize("case", ["ssw_ramp", "ssw2_plateau", "ssw_down"])
+def test_forced_step_matches_reference(sb, case):
+    """The SSW forcing (src/forcing_funcs.cpp:6-96) in the step, eager steps
+    from the case's time and one graph-replayed run, against the reference.
+    Tolerance 1e-11: the forcing term's tan / exp / atan2 / cos run in the
+    device's libm (last-bit differences from the host's), and the forced
+    flow is strong (the forcing moves the vorticity by 2.5 in one step)."""
+    gd = load("bve_forcing_L3.npz")
+    cfg = sb.config_default(levels=3, interp_degree=3, fmm_theta=0.7, kernel_eps=float(gd["eps"]),
+                            omega=float(gd["omega"]), dt=1.0, forcing=int(gd[case + "_forcing"]))
+    ctx = sb.Context(cfg)
+    n, t0 = int(gd[case + "_n"]), float(gd[case + "_t0"])
+    xyza = [cuda(gd[k]) for k in ("x", "y", "z", "area")]
+    v = cuda(gd["ic"])
+    vel = [torch.zeros_like(v) for _ in range(3)]
+    for k in range(n):
+        ctx.bve_back_rk4_step(*xyza, v, *vel, time=t0 + k)
+    assert rel(v, gd[case + "_vors"]) <= 1e-11, rel(v, gd[case + "_vors"])
+    assert rel(torch.stack(vel), gd[case + "_vel"]) <= 1e-11
+    w = cuda(gd["ic"])
+    wel = [torch.zeros_like(w) for _ in range(3)]
+    ctx.bve_run(*xyza, w, *wel, nsteps=n, time=t0)
+    assert torch.equal(w, v) and all(torch.equal(a, b) for a, b in zip(wel, vel))
+
+
+def test_forcing_on_treecode_and_mixed(sb):
+    """The forcing through the other velocity paths, at the benchmark's time
+    step (dt 0.005; the golden case's dt = 1 turns the flow too far per step
+    for the mixed-precision bar): mixed spectral FMM against the float64 one
+    <= 1e-6, treecode and spectral FMM against the forced float64 direct sum."""
+    g = sb.build_grid(4, 3, exact_cc=True)
+    xyza = [cuda(a) for a in (g.x, g.y, g.z, g.area)]
+    lat = np.arcsin(np.clip(g.z, -1, 1))
+    vor0 = 2 * 0.5 * np.sin(lat) - 0.5 * np.sin(lat) * np.cos(lat) ** 4 * 30 * np.cos(4 * np.arctan2(g.y, g.x))
+    out = {}
+    for name, kw in (("direct", dict(velocity=sb.VEL_DIRECT)), ("fp64", {}), ("mixed", dict(precision=sb.MIXED)),
+                     ("tree", dict(proxy_degree=8, leaf_size=64))):
+        cfg = sb.config_default(levels=4, interp_degree=3, fmm_theta=0.7, kernel_eps=1e-4, omega=2 * np.pi,
+                                dt=0.005, forcing=sb.FORCING_SSW2, **kw)
+        ctx = sb.Context(cfg)
+        v = cuda(vor0)
+        vel = [torch.zeros_like(v) for _ in range(3)]
+        ctx.bve_back_rk4_step(*xyza, v, *vel, time=6 * 86400.0)
+        out[name] = v
+    unforced = sb.Context(sb.config_default(levels=4, interp_degree=3, kernel_eps=1e-4, omega=2 * np.pi, dt=0.005,
+                                            velocity=sb.VEL_DIRECT))
+    u = cuda(vor0)
+    unforced.bve_back_rk4_step(*xyza, u, *[torch.zeros_like(u) for _ in range(3)])
+    assert rel(u, out["direct"].cpu().numpy()) > 1e-3  # the forcing acts
+    assert rel(out["mixed"], out["fp64"].cpu().numpy()) <= MIXED_TOL
+    assert rel(out["tree"], out["direct"].cpu().numpy()) <= 1e-7
+    assert rel(out["fp64"], out["direct"].cpu().numpy()) <= 1e-4  # the spectral FMM's own error at theta 0.7

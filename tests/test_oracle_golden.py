@@ -157,3 +157,15 @@ def test_solid_body_rotation_is_steady(port):
     # the velocity is the rigid rotation a * (z_hat x x)
     assert np.abs(vel[0] + a * g["y"]).max() / a < 2e-2
     assert np.abs(vel[1] - a * g["x"]).max() / a < 2e-2
+
+
+@pytest.mark.parametrize("case", ["ssw_ramp", "ssw2_plateau", "ssw_down"])
+def test_forced_step_matches_reference(port, case):
+    """bve_back_rk4_step with the SSW forcing on (src/forcing_funcs.cpp:6-96)."""
+    gd = load("bve_forcing_L3.npz")
+    g = port.build(3, 3, 0.7)
+    v, vel, _ = port.bve_step(g, gd["ic"], None, dt=1.0, omega=float(gd["omega"]), eps=float(gd["eps"]), mode=0,
+                              nsteps=int(gd[case + "_n"]), forcing=int(gd[case + "_forcing"]),
+                              time=float(gd[case + "_t0"]))
+    assert rel(v, gd[case + "_vors"]) <= TOL
+    assert rel(np.stack(vel), gd[case + "_vel"]) <= TOL

@@ -4,6 +4,7 @@ the configuration key for the height-Laplacian factor."""
 import os
 
 import numpy as np
+import pytest
 
 from conftest import GOLDEN
 
@@ -36,3 +37,16 @@ def test_g_over_a_default_and_namelist(sb, tmp_path):
     p.write_text("levels=4\ng_over_a=1.0\nend\n")
     cfg = sb.read_run_config(str(p))
     assert cfg.levels == 4 and cfg.g_over_a == 1.0
+
+
+def test_forcing_namelist_keys(sb, tmp_path):
+    """forcing=1 with forcing_type ssw / ssw2 (src/io_utils.cpp:69-74)."""
+    p = tmp_path / "namelist.txt"
+    for text, want in (("forcing=1\nforcing_type=ssw2\nend\n", sb.FORCING_SSW2),
+                       ("forcing_type=ssw\nforcing=1\nend\n", sb.FORCING_SSW),
+                       ("forcing=0\nforcing_type=ssw\nend\n", sb.FORCING_NONE)):
+        p.write_text(text)
+        assert sb.read_run_config(str(p)).forcing == want
+    p.write_text("forcing=1\nforcing_type=other\nend\n")
+    with pytest.raises(sb.SbslpmError):
+        sb.read_run_config(str(p))
