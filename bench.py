@@ -498,6 +498,23 @@ def adjoint_bench(sb, torch, dev, directions=8):
                                    "checkpoints", "h": 1e-6}}
 
 
+def replica_vorticity(vor0, z, rank, world):
+    """The replica of rank `rank`: with one rank the benchmark state itself,
+    with several an independent ensemble member (seeded perturbation)."""
+    if world <= 1:
+        return vor0
+    return vor0 + np.random.default_rng(rank).standard_normal(np.shape(vor0)) * 1e-3 * z
+
+
+def job_time(dist, torch, t_ms, device):
+    """Max over ranks of a rank's device-timed total (ms); the whole job's time."""
+    if dist is None:
+        return t_ms
+    tt = torch.tensor([t_ms], dtype=torch.float64, device=device)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return float(tt.item())
+
+
 def timed_steps(torch, ctx, f, steps, flush):
     """Per-step device times (ms) of bve_run(nsteps=1) with an L2 flush between."""
     st = torch.cuda.current_stream()
@@ -559,9 +576,7 @@ def main():
         return
 
     g = sb.build_grid(LEVELS, DEGREE, exact_cc=True)
-    vor0 = rh4(g)
-    if world > 1:  # independent ensemble members: seeded perturbation per rank
-        vor0 = vor0 + np.random.default_rng(rank).standard_normal(vor0.shape) * 1e-3 * g.z
+    vor0 = replica_vorticity(rh4(g), g.z, rank, world)
 
     def T(a):
         return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
@@ -593,11 +608,8 @@ def main():
         ts32 = timed_steps(torch, ctx32, f32, args.steps, flush)
     launches = sb.kernel_launches() - launches0
     torch.cuda.synchronize()
-    t_total = sum(ts32)
+    t_total = job_time(dist, torch, sum(ts32), dev)
     if dist:
-        tt = torch.tensor([t_total], dtype=torch.float64, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_total = float(tt.item())
         dist.barrier()
     ms_per_step = t_total / args.steps
     value = world * args.steps / (t_total * 1e-3)
@@ -671,11 +683,7 @@ def main():
         e1.record(st)
         e1.synchronize()
         te.append(e0.elapsed_time(e1))
-    e2e_total = sum(te)
-    if dist:
-        tt = torch.tensor([e2e_total], dtype=torch.float64, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_total = float(tt.item())
+    e2e_total = job_time(dist, torch, sum(te), dev)
     e2e = world * args.steps / (e2e_total * 1e-3)
 
     # ---- CPU baseline: the reference's own step on the host cores ----------

@@ -1,0 +1,82 @@
+"""The multi-rank path of bench.py on the CPU with the gloo backend
+(world size 2): every rank steps an independent replica (no data-path
+collective), the job's time is the maximum over ranks and the rate counts
+every rank's steps; the reference arm runs on rank 0 alone."""
+import importlib.util
+import os
+import socket
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+torch = pytest.importorskip("torch")
+
+
+def load_bench():
+    spec = importlib.util.spec_from_file_location("bench_under_test", os.path.join(ROOT, "bench.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank(rank, world, port, out):
+    import datetime
+
+    import torch.distributed as dist
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=30))
+    try:
+        bench = load_bench()
+        # rank-specific device times; the job's time is their maximum
+        t = bench.job_time(dist, torch, [30.0, 45.0][rank], "cpu")
+        z = np.linspace(-1, 1, 16)
+        v = bench.replica_vorticity(np.ones(16), z, rank, world)
+        vs = [torch.zeros(16, dtype=torch.float64) for _ in range(world)]
+        dist.all_gather(vs, torch.from_numpy(v))
+        out.put((rank, t, [x.numpy().tolist() for x in vs]))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_ranks_gloo():
+    ctx = torch.multiprocessing.get_context("spawn")
+    q = ctx.Queue()
+    port = free_port()
+    procs = [ctx.Process(target=_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    (r0, t0, v0), (r1, t1, v1) = res
+    assert t0 == t1 == 45.0  # max over ranks, the same on every rank
+    assert v0 == v1 and v0[0] != v0[1]  # the two replicas differ (independent members)
+    bench = load_bench()
+    steps, world = 10, 2
+    assert world * steps / (t0 * 1e-3) == pytest.approx(444.444, rel=1e-5)
+
+
+def test_single_rank_is_the_benchmark_state():
+    bench = load_bench()
+    v = np.arange(5.0)
+    assert bench.replica_vorticity(v, np.ones(5), 0, 1) is v
+
+
+def test_reference_arm_other_ranks_do_nothing(capsys):
+    bench = load_bench()
+
+    class Args:
+        steps, warmup, gpus = 1, 0, 2
+
+    bench.run_reference(Args(), 1)  # rank 1 returns without work or output
+    assert capsys.readouterr().out == ""
