@@ -132,6 +132,11 @@ sbslpm_status sbslpm_cube_sphere_spec_points(int levels, int degree, const sbslp
  * pairs to out (may be NULL) and returns the full count in *count. */
 sbslpm_status sbslpm_dual_tree_traversal(int levels, const sbslpm_panel* panels, double theta,
                                          sbslpm_interact_pair* out, long cap, long* count);
+/* The same traversal on the GPU (generation by generation: classification,
+ * prefix sums, emission): the same list in the same order.  Host arrays in
+ * and out; device workspace is allocated and freed inside the call. */
+sbslpm_status sbslpm_dual_tree_traversal_device(int levels, const sbslpm_panel* panels, double theta,
+                                                sbslpm_interact_pair* out, long cap, long* count);
 /* Host versions of interp_vals_bli / point_locate_panel
  * (src/interp_funcs_impl.hpp:11-142). */
 sbslpm_status sbslpm_interp_vals_bli(double* basis, double xi, double eta, double min_xi, double max_xi,

@@ -103,6 +103,7 @@ def lib() -> ctypes.CDLL:
     L.sbslpm_dual_tree_traversal.argtypes = [ctypes.c_int, ctypes.POINTER(Panel), ctypes.c_double,
                                              ctypes.POINTER(InteractPair), ctypes.c_long,
                                              ctypes.POINTER(ctypes.c_long)]
+    L.sbslpm_dual_tree_traversal_device.argtypes = L.sbslpm_dual_tree_traversal.argtypes
     L.sbslpm_create.argtypes = [ctypes.POINTER(Config), ctypes.POINTER(_VP)]
     for name in ("sbslpm_destroy", "sbslpm_set_stream", "sbslpm_get_sizes", "sbslpm_get_panels",
                  "sbslpm_get_interactions"):
@@ -228,12 +229,14 @@ def cube_sphere_spec_points(levels: int, degree: int, panels, interp: np.ndarray
     return x, y, z, area
 
 
-def dual_tree_traversal(levels: int, panels, theta: float) -> np.ndarray:
-    """Interaction list (I x 3 int32: target, source, type) in the reference's order."""
+def dual_tree_traversal(levels: int, panels, theta: float, device: bool = False) -> np.ndarray:
+    """Interaction list (I x 3 int32: target, source, type) in the reference's order,
+    built on the host or (device=True) on the GPU."""
+    fn = lib().sbslpm_dual_tree_traversal_device if device else lib().sbslpm_dual_tree_traversal
     n = ctypes.c_long(0)
-    _check(lib().sbslpm_dual_tree_traversal(levels, panels, theta, None, 0, ctypes.byref(n)), "traversal")
+    _check(fn(levels, panels, theta, None, 0, ctypes.byref(n)), "traversal")
     out = (InteractPair * max(n.value, 1))()
-    _check(lib().sbslpm_dual_tree_traversal(levels, panels, theta, out, n.value, ctypes.byref(n)), "traversal")
+    _check(fn(levels, panels, theta, out, n.value, ctypes.byref(n)), "traversal")
     return np.ctypeslib.as_array(ctypes.cast(out, ctypes.POINTER(ctypes.c_int)), (max(n.value, 1), 3))[: n.value].copy()
 
 

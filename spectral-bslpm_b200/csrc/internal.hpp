@@ -2,6 +2,8 @@
 // C ABI implementation.
 #pragma once
 
+#include <cuda_runtime.h>
+
 #include <array>
 #include <string>
 #include <vector>
@@ -34,5 +36,9 @@ void build_swe_tables(int degree, const std::vector<sbslpm_panel>& panels, int o
                       std::vector<double>& ptan, std::vector<int>& pface);
 
 void set_last_error(const std::string& msg);
+
+// traversal.cu: dual_tree_traversal on the device (same list, same order as build_interactions)
+sbslpm_status device_dual_tree_traversal(int levels, const std::vector<sbslpm_panel>& P, double theta,
+                                         std::vector<sbslpm_interact_pair>& out, cudaStream_t st);
 
 }  // namespace sbslpm
