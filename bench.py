@@ -44,7 +44,7 @@ METRIC = "BVE RK4 steps/s at ≤1e-6 rel vort err: mixed+batched vs FP64 plain, 
 LEVELS, DEGREE, THETA, EPS, OMEGA, DT = 7, 3, 0.7, 1e-4, 2 * np.pi, 0.005
 PROXY_DEGREE, LEAF_SIZE = 8, 256
 PAIR_FLOP = 17  # FLOP per Biot-Savart pair (division counted as 1)
-NEAR_TRAFFIC = 15.888640e6 + 3.84e3  # DRAM bytes of one near-field launch, from the committed ncu capture
+NEAR_TRAFFIC = 15.889664e6 + 0.385792e6  # DRAM bytes of one near-field launch, from the committed ncu capture
 
 
 def workload_config():
@@ -418,6 +418,8 @@ def profile_run(sb, torch, dev, args):
         ctx = sb.Context(sb.config_default(levels=LEVELS, interp_degree=DEGREE, fmm_theta=THETA, kernel_eps=EPS,
                                            omega=OMEGA, dt=DT, precision=prec, proxy_degree=proxy,
                                            leaf_size=LEAF_SIZE))
+        if proxy:  # the first-step autotuner's choice on this workload, fixed so that the capture sees steps only
+            ctx.set_near_tuning(*[int(v) for v in args.near_shape.split(",")])
         f = [T(g.x), T(g.y), T(g.z), T(g.area), T(rh4(g)), *[torch.zeros_like(T(g.x)) for _ in range(3)], None]
         for _ in range(n):
             ctx.bve_back_rk4_step(*f)
@@ -546,6 +548,8 @@ def main():
     ap.add_argument("--cc-mode", type=int, default=1, choices=[0, 1, 2],
                     help="--profile ensemble: well-separated interactions, 0 CUDA-core pairs, 1 tensor-core "
                          "3xTF32, 2 tensor-core TF32")
+    ap.add_argument("--near-shape", default="128,2,4",
+                    help="--profile treecode/treecode64: near-field threads,targets per thread,splits")
     ap.add_argument("--degree", type=int, default=0,
                     help="--profile ensemble: one proxy degree for every member (0: drawn from {6, 8, 10})")
     args = ap.parse_args()
@@ -713,7 +717,7 @@ def main():
                          "launch_shape": {"threads": tune32[0], "targets_per_thread": tune32[1],
                                           "splits": tune32[2], "candidates_timed": tune32[3]},
                          "achieved": achieved, "peak": peak_meas, "unit": "TFLOP/s", "frac": achieved / peak_meas,
-                         "traffic": NEAR_TRAFFIC, "traffic_source": "profiles/k_bltc_near32_levels7.md "
+                         "traffic": NEAR_TRAFFIC, "traffic_source": "profiles/k_bltc_near32_batch_levels7.md "
                          "(dram__bytes_read.sum + dram__bytes_write.sum of one launch)",
                          "flop_per_pair": PAIR_FLOP, "pairs_per_launch": pairs,
                          "ms_per_launch": ms_int, "step_share": share,
