@@ -420,6 +420,7 @@ def profile_run(sb, torch, dev, args):
                                            leaf_size=LEAF_SIZE))
         if proxy:  # the first-step autotuner's choice on this workload, fixed so that the capture sees steps only
             ctx.set_near_tuning(*[int(v) for v in args.near_shape.split(",")])
+            ctx.set_cc_tuning(*[int(v) for v in args.cc_shape.split(",")])
         f = [T(g.x), T(g.y), T(g.z), T(g.area), T(rh4(g)), *[torch.zeros_like(T(g.x)) for _ in range(3)], None]
         for _ in range(n):
             ctx.bve_back_rk4_step(*f)
@@ -550,6 +551,9 @@ def main():
                          "3xTF32, 2 tensor-core TF32")
     ap.add_argument("--near-shape", default="128,2,4",
                     help="--profile treecode/treecode64: near-field threads,targets per thread,splits")
+    ap.add_argument("--cc-shape", default="3,3",
+                    help="--profile treecode/treecode64: well-separated chunk slots per block,chunk length (0,0: "
+                         "one block per target panel)")
     ap.add_argument("--degree", type=int, default=0,
                     help="--profile ensemble: one proxy degree for every member (0: drawn from {6, 8, 10})")
     args = ap.parse_args()
@@ -673,6 +677,8 @@ def main():
     peak64 = sb.measure_fma_peak(1, 50.0) / 1e12
     share = 4 * ms_int / ms_per_step
     tune32, tune64 = ctx32.near_tuning(), ctx64.near_tuning()
+    cc32, cc64 = ctx32.cc_tuning(), ctx64.cc_tuning()
+    well_sep_pairs = 4 * 52566 * 81 * 81  # per step: well-separated tree-panel pairs x 81 x 81 proxies
 
     # ---- batched ensemble ----------------------------------------------------
     ens = None if args.no_ensemble else ensemble_bench(sb, torch, dev, flush, min(args.steps, 20))
@@ -739,6 +745,14 @@ def main():
                          "ms_per_launch": ms_int, "step_share": share,
                          "peak_source": "measured f32 FMA-chain throughput on this GPU (sbslpm_measure_fma_peak); "
                                         "MEASURED_PEAKS.json has no CUDA-core peak"},
+            "well_separated_kernel": {"slots": cc32[0], "chunk_len": cc32[1], "threads": cc32[2],
+                                      "candidates_timed": cc32[3], "ms_per_launch": cc32[4],
+                                      "pairs_per_launch": well_sep_pairs / 4,
+                                      "pairs_per_s": well_sep_pairs / 4 / (cc32[4] * 1e-3) if cc32[4] else None,
+                                      "fp64": {"slots": cc64[0], "chunk_len": cc64[1], "ms_per_launch": cc64[4]},
+                                      "note": "slots 0: one block per target panel; else blocks of `slots` chunks "
+                                              "of chunk_len list entries (autotuned on the first step; the time "
+                                              "includes the chunk reduction)"},
             "fp64_plain": {"steps_per_s": fp64_sps, "ms_per_step": 1e3 / fp64_sps, "near_kernel_tflops": ach64,
                            "near_launch_shape": list(tune64[:3]),
                            "fp64_fma_peak_tflops": peak64, "frac": ach64 / peak64},

@@ -338,7 +338,8 @@ sbslpm_status sbslpm_batch_pairs(const sbslpm_batch* batch, double* near_pairs, 
 /* Well-separated (cluster-cluster) interactions of a mixed-precision batch:
  * mode -1 = chosen per proxy-degree group by the autotuner of the first
  * step (the default), 0 = CUDA-core float32 pairs per member (bit-exact with
- * single contexts), 1 = tensor-core GEMM over the members sharing a proxy
+ * single contexts on the whole-panel well-separated kernel,
+ * sbslpm_set_cc_tuning(ctx, 0, 0)), 1 = tensor-core GEMM over the members sharing a proxy
  * degree in 3xTF32, 2 = the same GEMM in one TF32 pass.  Float64 batches
  * accept mode 0 only.  sbslpm_batch_cc_info reports the mode, the union of
  * the members' well-separated pairs over the degree groups (cluster pairs),
@@ -459,6 +460,21 @@ sbslpm_status sbslpm_time_interactions(sbslpm_ctx* ctx, int reps, double* ms_per
  * candidates timed. */
 sbslpm_status sbslpm_set_near_tuning(sbslpm_ctx* ctx, int threads, int targets_per_thread, int splits);
 sbslpm_status sbslpm_near_tuning(const sbslpm_ctx* ctx, int* shape, double* ms_per_launch);
+/* Treecode contexts with 36..121 proxies (proxy_degree 5..10): the launch
+ * shape of the well-separated (cluster-cluster) interactions, either one
+ * block of four warps per target panel (slots 0, chunk length 0, the kernel
+ * of the batched CUDA-core path) or blocks of 1 | 2 | 3 | 4 | 6 | 8 chunk
+ * slots of q threads each (rounded up to whole warps: at most 512 threads,
+ * at most a fifth of them idle), a chunk being 1..4 consecutive list entries
+ * of one target panel.  The first step times every shape with the near field
+ * and keeps the fastest; sbslpm_set_cc_tuning fixes one instead (the chunk
+ * length sets the order in which a target's sums are added, the slot count
+ * does not; SBSLPM_ERR_CONFIG for other proxy counts).  shape[0..3] = slots,
+ * chunk length, threads per block, candidates timed.  Both replace nothing
+ * in the reference (its interactions run one list entry per Kokkos
+ * iteration, src/fmm_interactions/bve_vel.cpp:35-150). */
+sbslpm_status sbslpm_set_cc_tuning(sbslpm_ctx* ctx, int slots, int chunk_len);
+sbslpm_status sbslpm_cc_tuning(const sbslpm_ctx* ctx, int* shape, double* ms_per_launch);
 /* CUDA-core fused multiply-add throughput of this GPU, measured with
  * independent FMA chains on every SM for about ms milliseconds: kind 0 =
  * float32, 1 = float64.  Returns FLOP/s (2 per FMA) in *flops. */

@@ -162,6 +162,8 @@ def lib() -> ctypes.CDLL:
     L.sbslpm_time_interactions.argtypes = [_VP, ctypes.c_int, _D, _D]
     L.sbslpm_set_near_tuning.argtypes = [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     L.sbslpm_near_tuning.argtypes = [_VP, _I, _D]
+    L.sbslpm_set_cc_tuning.argtypes = [_VP, ctypes.c_int, ctypes.c_int]
+    L.sbslpm_cc_tuning.argtypes = [_VP, _I, _D]
     L.sbslpm_measure_fma_peak.argtypes = [ctypes.c_int, ctypes.c_double, _D]
     _lib = L
     return L
@@ -486,6 +488,20 @@ class Context:
         shape = (ctypes.c_int * 4)()
         ms = ctypes.c_double()
         _check(lib().sbslpm_near_tuning(self._h, shape, ctypes.byref(ms)), "sbslpm_near_tuning")
+        return (*[int(v) for v in shape], ms.value)
+
+    def set_cc_tuning(self, slots: int, chunk_len: int):
+        """Fix the treecode's well-separated launch shape (chunk slots per block,
+        list entries per chunk; 0, 0: one block per target panel) instead of
+        autotuning it."""
+        _check(lib().sbslpm_set_cc_tuning(self._h, int(slots), int(chunk_len)), "sbslpm_set_cc_tuning")
+
+    def cc_tuning(self):
+        """(slots, chunk length, threads per block, candidates timed, ms per
+        well-separated launch)."""
+        shape = (ctypes.c_int * 4)()
+        ms = ctypes.c_double()
+        _check(lib().sbslpm_cc_tuning(self._h, shape, ctypes.byref(ms)), "sbslpm_cc_tuning")
         return (*[int(v) for v in shape], ms.value)
 
     def time_interactions(self, reps: int = 5):

@@ -4,6 +4,8 @@
 
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "geometry.cuh"
 
 namespace sbslpm {
@@ -102,6 +104,22 @@ void launch_ssw_forcing(int leaves, int q, int type, double omega, const double*
 void launch_time_advance(double* time, double dt, cudaStream_t st);
 void launch_inv_lap(long n, const double* x, const double* y, const double* z, const double* area,
                     const double* pots, double* soln, cudaStream_t st);
+
+// Treecode well-separated interactions over chunks of consecutive list
+// entries of one target panel (cc_chunks.cu), for q in {36, 49, 64, 81, 100,
+// 121}: blocks of `slots` chunks (slots in {1, 2, 3, 4, 6, 8}, at most 512
+// threads with at most a fifth of them idle: cc_chunk_shape_ok) write each
+// chunk's raw sums to partial[chunk][3][q], then a reduction adds each
+// target's chunks in list order into tgt ([3][panels*q]).  chunks[c] =
+// (target, first entry, end entry, 0); cstart[panels+1] is the CSR of chunks
+// by target.
+bool cc_chunk_supported(int q);
+bool cc_chunk_shape_ok(int q, int slots);
+int cc_chunk_threads(int q, int slots);
+void launch_cc_chunks(const StepGeom& g, int precision, int slots, const int4* chunks, int nchunks, const int* cstart,
+                      const double4* src, double* partial, double* tgt, cudaStream_t st);
+void build_cc_chunks(const std::vector<int>& start, int chunk_len, std::vector<int4>& chunks,
+                     std::vector<int>& cstart);
 
 // The interaction kernel alone (no mixed-precision packing), for timing.
 void launch_interactions_only(const StepGeom& g, int precision, const double4* src, double* tgt, cudaStream_t st);

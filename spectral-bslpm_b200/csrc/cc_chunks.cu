@@ -1,0 +1,282 @@
+// Well-separated proxy interactions of the decoupled-degree treecode
+// (q = (n+1)^2 proxies, n = 5..10) over chunks of the interaction list.
+//
+// The reference evaluates each (target panel, source panel) pair of its
+// interaction list with a loop over the proxies
+// (src/fmm_interactions/bve_vel.cpp:35-150).  Here the treecode's
+// well-separated list (CSR by target panel) is cut into chunks of at most C
+// consecutive entries of one target panel (near-equal lengths), and a block
+// evaluates S chunks side by side.  One block of four warps per target panel
+// (k_interact_wide) runs a target's whole list in one block and leaves
+// (32 - q mod 32) lanes of its last warp idle; chunks spread long lists over
+// the GPU, and the slots fill the warps (81 proxies: 3 slots in 256
+// threads).  Each slot writes the raw sums a = sum g d of its chunk (float64)
+// to its own row; k_cc_reduce adds a target's chunks in list order and
+// applies the cross product.  The result depends on C (the order of the
+// float64 additions), not on S.
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "../../include/sbslpm.h"
+#include "bve_kernels.cuh"
+#include "device_common.cuh"
+
+namespace sbslpm {
+namespace {
+
+using dev::blocks_for;
+using dev::pair32x2;
+using dev::pair64;
+
+// A block holds S chunk slots of Q target proxies each: thread k works on
+// target node k % Q of slot k / Q (threads past S*Q idle), so that a block
+// of a multiple of 32 threads leaves few lanes idle for any Q.  Every slot
+// walks its own chunk, staging one source panel at a time in its own part of
+// the shared tile.  (Loading the next panel into registers during the
+// current one, with a double-buffered tile, measured slower: the extra
+// registers cost more occupancy than the barrier it saves.)
+template <int Q, int S>
+struct CcShape {
+  static constexpr int NT = (S * Q + 31) / 32 * 32;
+  static constexpr int Q2 = (Q + 1) / 2;
+  static constexpr bool ok = NT <= 512 && 5 * S * Q >= 4 * NT;  // at most a fifth of the lanes idle
+};
+
+__device__ __forceinline__ int chunk_entries_max(const int4* __restrict__ chunks, int nchunks, int first, int S) {
+  int m = 0;
+  for (int h = 0; h < S && first + h < nchunks; h++) {
+    const int4 c = chunks[first + h];
+    m = max(m, c.z - c.y);
+  }
+  return m;
+}
+
+// Mixed precision: proxies relative to panel centres (kPackScale), float32
+// pairs two at a time (FADD2 / FFMA2 / FMUL2), per-source-panel float32 sums
+// added into float64.
+template <int Q, int S, bool GUARD>
+__global__ void __launch_bounds__(CcShape<Q, S>::NT)
+    k_cc32(StepGeom g, const int4* __restrict__ chunks, int nchunks, double* __restrict__ partial) {
+  constexpr int Q2 = CcShape<Q, S>::Q2;
+  __shared__ float4 tile[S][2 * Q2];  // (x0,x1,y0,y1),(z0,z1,w0,w1); odd q: zero-strength partner
+  const int h = threadIdx.x / Q, j = threadIdx.x - h * Q;
+  const int c = blockIdx.x * S + h;
+  const bool live = h < S && c < nchunks;
+  const int nmax = chunk_entries_max(chunks, nchunks, blockIdx.x * S, S);
+  int4 ch = make_int4(0, 0, 0, 0);
+  if (live) ch = chunks[c];
+  const int n = ch.z - ch.y;
+  const long pn = (long)g.panels * Q;
+  double cx = 0, cy = 0, cz = 0;
+  float dtx = 0, dty = 0, dtz = 0;
+  if (live) {
+    const double* ct = g.pd_centre + 4 * (long)ch.x;
+    cx = ct[0];
+    cy = ct[1];
+    cz = ct[2];
+    const long o = (long)ch.x * Q + j;
+    dtx = (float)((g.px[o] - cx) * kPackScale);
+    dty = (float)((g.px[pn + o] - cy) * kPackScale);
+    dtz = (float)((g.px[2 * pn + o] - cz) * kPackScale);
+  }
+  const float feps = (float)g.eps;
+  const float2 eps2 = make_float2(feps, feps);
+  double ax = 0, ay = 0, az = 0;
+  for (int e = 0; e < nmax; e++) {
+    const bool act = live && e < n;
+    int sp = 0;
+    if (act) sp = __ldg(g.src_panel + ch.y + e);
+    __syncthreads();
+    if (act && j < Q2) {
+      const long sb = (long)sp * Q + 2 * j;
+      const float4 s0 = g.srcf[sb];
+      const float4 s1 = (2 * j + 1 < Q) ? g.srcf[sb + 1] : make_float4(0.f, 0.f, 0.f, 0.f);
+      tile[h][2 * j] = make_float4(s0.x, s1.x, s0.y, s1.y);
+      tile[h][2 * j + 1] = make_float4(s0.z, s1.z, s0.w, s1.w);
+    }
+    __syncthreads();
+    if (act) {
+      const double* cs = g.pd_centre + 4 * (long)sp;
+      const float b0 = (float)((cs[0] - cx) * kPackScale) - dtx, b1 = (float)((cs[1] - cy) * kPackScale) - dty,
+                  b2 = (float)((cs[2] - cz) * kPackScale) - dtz;
+      const float2 bx = make_float2(b0, b0), by = make_float2(b1, b1), bz = make_float2(b2, b2);
+      float2 fx = make_float2(0.f, 0.f), fy = fx, fz = fx;
+      const float4* tb = tile[h];
+#pragma unroll 4
+      for (int k2 = 0; k2 < Q2; k2++) {
+        const float4 A = tb[2 * k2], B = tb[2 * k2 + 1];
+        pair32x2<GUARD>(bx, by, bz, make_float2(A.x, A.y), make_float2(A.z, A.w), make_float2(B.x, B.y),
+                        make_float2(B.z, B.w), eps2, fx, fy, fz);
+      }
+      ax += (double)fx.x + (double)fx.y;
+      ay += (double)fy.x + (double)fy.y;
+      az += (double)fz.x + (double)fz.y;
+    }
+  }
+  if (live) {
+    double* p = partial + (long)c * 3 * Q;
+    p[j] = ax;
+    p[Q + j] = ay;
+    p[2 * Q + j] = az;
+  }
+}
+
+// Float64: the same slots and chunks with absolute proxy positions (pair64).
+template <int Q, int S, bool GUARD>
+__global__ void __launch_bounds__(CcShape<Q, S>::NT)
+    k_cc64(StepGeom g, const int4* __restrict__ chunks, int nchunks, const double4* __restrict__ src,
+           double* __restrict__ partial) {
+  __shared__ double4 tile[S][Q];
+  const int h = threadIdx.x / Q, j = threadIdx.x - h * Q;
+  const int c = blockIdx.x * S + h;
+  const bool live = h < S && c < nchunks;
+  const int nmax = chunk_entries_max(chunks, nchunks, blockIdx.x * S, S);
+  int4 ch = make_int4(0, 0, 0, 0);
+  if (live) ch = chunks[c];
+  const int n = ch.z - ch.y;
+  const long pn = (long)g.panels * Q;
+  double tx = 0, ty = 0, tz = 0;
+  if (live) {
+    const long o = (long)ch.x * Q + j;
+    tx = g.px[o];
+    ty = g.px[pn + o];
+    tz = g.px[2 * pn + o];
+  }
+  double ax = 0, ay = 0, az = 0;
+  for (int e = 0; e < nmax; e++) {
+    const bool act = live && e < n;
+    __syncthreads();
+    if (act) tile[h][j] = src[(long)__ldg(g.src_panel + ch.y + e) * Q + j];
+    __syncthreads();
+    if (act) {
+      const double4* tb = tile[h];
+#pragma unroll 3
+      for (int k = 0; k < Q; k++) pair64<GUARD>(tx, ty, tz, tb[k], g.eps, ax, ay, az);
+    }
+  }
+  if (live) {
+    double* p = partial + (long)c * 3 * Q;
+    p[j] = ax;
+    p[Q + j] = ay;
+    p[2 * Q + j] = az;
+  }
+}
+
+// Target proxy velocities: a target's chunk sums added in list order, then
+// u = cb * x cross a.  Panels with no entries get zeros.
+__global__ void k_cc_reduce(StepGeom g, const int* __restrict__ cstart, const double* __restrict__ partial, double cb,
+                            double* __restrict__ out) {
+  const int q = g.q;
+  const long pn = (long)g.panels * q;
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= pn) return;
+  const int t = (int)(i / q), j = (int)(i - (long)t * q);
+  double sx = 0, sy = 0, sz = 0;
+  for (int c = cstart[t]; c < cstart[t + 1]; c++) {
+    const double* p = partial + (long)c * 3 * q;
+    sx += p[j];
+    sy += p[q + j];
+    sz += p[2 * q + j];
+  }
+  const double px = g.px[i], py = g.px[pn + i], pz = g.px[2 * pn + i];
+  out[i] = cb * (py * sz - pz * sy);
+  out[pn + i] = cb * (pz * sx - px * sz);
+  out[2 * pn + i] = cb * (px * sy - py * sx);
+}
+
+template <int Q, int S>
+void launch_q_s(const StepGeom& g, bool mixed, const int4* chunks, int nchunks, const double4* src, double* partial,
+                cudaStream_t st) {
+  if constexpr (CcShape<Q, S>::ok) {
+    constexpr int NT = CcShape<Q, S>::NT;
+    const unsigned grid = (unsigned)((nchunks + S - 1) / S);
+    const bool guard = !(g.eps > 0);
+    if (mixed) {
+      if (guard) SB_LAUNCH((k_cc32<Q, S, true>), grid, NT, 0, st, g, chunks, nchunks, partial);
+      else SB_LAUNCH((k_cc32<Q, S, false>), grid, NT, 0, st, g, chunks, nchunks, partial);
+    } else {
+      if (guard) SB_LAUNCH((k_cc64<Q, S, true>), grid, NT, 0, st, g, chunks, nchunks, src, partial);
+      else SB_LAUNCH((k_cc64<Q, S, false>), grid, NT, 0, st, g, chunks, nchunks, src, partial);
+    }
+  }
+}
+
+template <int Q>
+void launch_q(const StepGeom& g, bool mixed, int slots, const int4* chunks, int nchunks, const double4* src,
+              double* partial, cudaStream_t st) {
+  switch (slots) {
+    case 1: launch_q_s<Q, 1>(g, mixed, chunks, nchunks, src, partial, st); break;
+    case 2: launch_q_s<Q, 2>(g, mixed, chunks, nchunks, src, partial, st); break;
+    case 3: launch_q_s<Q, 3>(g, mixed, chunks, nchunks, src, partial, st); break;
+    case 4: launch_q_s<Q, 4>(g, mixed, chunks, nchunks, src, partial, st); break;
+    case 6: launch_q_s<Q, 6>(g, mixed, chunks, nchunks, src, partial, st); break;
+    default: launch_q_s<Q, 8>(g, mixed, chunks, nchunks, src, partial, st); break;
+  }
+}
+
+template <int Q>
+bool shape_ok_q(int slots) {
+  switch (slots) {
+    case 1: return CcShape<Q, 1>::ok;
+    case 2: return CcShape<Q, 2>::ok;
+    case 3: return CcShape<Q, 3>::ok;
+    case 4: return CcShape<Q, 4>::ok;
+    case 6: return CcShape<Q, 6>::ok;
+    case 8: return CcShape<Q, 8>::ok;
+    default: return false;
+  }
+}
+
+}  // namespace
+
+bool cc_chunk_supported(int q) { return q == 36 || q == 49 || q == 64 || q == 81 || q == 100 || q == 121; }
+
+bool cc_chunk_shape_ok(int q, int slots) {
+  switch (q) {
+    case 36: return shape_ok_q<36>(slots);
+    case 49: return shape_ok_q<49>(slots);
+    case 64: return shape_ok_q<64>(slots);
+    case 81: return shape_ok_q<81>(slots);
+    case 100: return shape_ok_q<100>(slots);
+    case 121: return shape_ok_q<121>(slots);
+    default: return false;
+  }
+}
+
+int cc_chunk_threads(int q, int slots) { return (slots * q + 31) / 32 * 32; }
+
+void launch_cc_chunks(const StepGeom& g, int precision, int slots, const int4* chunks, int nchunks, const int* cstart,
+                      const double4* src, double* partial, double* out, cudaStream_t st) {
+  const bool mixed = precision == SBSLPM_MIXED;
+  if (nchunks > 0) {
+    switch (g.q) {
+      case 36: launch_q<36>(g, mixed, slots, chunks, nchunks, src, partial, st); break;
+      case 49: launch_q<49>(g, mixed, slots, chunks, nchunks, src, partial, st); break;
+      case 64: launch_q<64>(g, mixed, slots, chunks, nchunks, src, partial, st); break;
+      case 81: launch_q<81>(g, mixed, slots, chunks, nchunks, src, partial, st); break;
+      case 100: launch_q<100>(g, mixed, slots, chunks, nchunks, src, partial, st); break;
+      default: launch_q<121>(g, mixed, slots, chunks, nchunks, src, partial, st); break;
+    }
+  }
+  const long pn = (long)g.panels * g.q;
+  SB_LAUNCH(k_cc_reduce, blocks_for(pn, 256), 256, 0, st, g, cstart, partial,
+            mixed ? kBiotSavartPacked : kBiotSavart, out);
+}
+
+void build_cc_chunks(const std::vector<int>& start, int chunk_len, std::vector<int4>& chunks,
+                     std::vector<int>& cstart) {
+  const int panels = (int)start.size() - 1;
+  chunks.clear();
+  cstart.assign(panels + 1, 0);
+  for (int t = 0; t < panels; t++) {
+    cstart[t] = (int)chunks.size();
+    const int len = start[t + 1] - start[t];
+    const int nc = (len + chunk_len - 1) / chunk_len;
+    for (int k = 0; k < nc; k++)  // near-equal chunks: entries [len k / nc, len (k+1) / nc)
+      chunks.push_back(make_int4(t, start[t] + (int)((long)len * k / nc), start[t] + (int)((long)len * (k + 1) / nc), 0));
+  }
+  cstart[panels] = (int)chunks.size();
+}
+
+}  // namespace sbslpm

@@ -165,6 +165,19 @@ sbslpm_status precompute_tree(sbslpm_ctx* c) {
   SB_TRY(upload(&c->near_src, l.nsrc));
   SB_TRY(upload(&c->cc_start, l.cs));
   SB_TRY(upload(&c->cc_src, l.csrc));
+  if (c->n_cc > 0 && cc_chunk_supported(t.qx)) {
+    for (int k = 0; k < 4; k++) {
+      std::vector<int4> chunks;
+      std::vector<int> cstart;
+      build_cc_chunks(l.cs, k + 1, chunks, cstart);
+      c->cc_nchunks[k] = (int)chunks.size();
+      SB_TRY(upload(&c->cc_chunks[k], chunks));
+      SB_TRY(upload(&c->cc_cstart[k], cstart));
+    }
+    SB_TRY(dalloc(&c->cc_partial, (size_t)c->n_cc * 3 * t.qx));
+  } else {
+    c->cc_tuned = true;  // k_interact_wide / k_interact32 over whole target panels
+  }
 
   // workspace; proxy positions are fixed, strengths are written every stage
   const size_t N = (size_t)c->A * qp;
@@ -265,6 +278,16 @@ void fill_geom(sbslpm_ctx* c) {
 
 namespace sbslpm {
 
+void launch_tree_cc(sbslpm_ctx* c, cudaStream_t st) {
+  if (c->cc_partial && c->cc_slots > 0) {
+    const int k = c->cc_len - 1;
+    launch_cc_chunks(c->fgeom, c->cfg.precision, c->cc_slots, c->cc_chunks[k], c->cc_nchunks[k], c->cc_cstart[k],
+                     c->fsrc, c->cc_partial, c->ftgt, st);
+  } else {
+    launch_interactions_only(c->fgeom, c->cfg.precision, c->fsrc, c->ftgt, st);
+  }
+}
+
 // One velocity evaluation (one RK4 stage) into v (contiguous [3][leaves*q]).
 void velocity_eval(sbslpm_ctx* c, int stage, double dt_s, const double* vprev, const double* x, const double* y,
                    const double* z, const double* area, const double* vors, double* v) {
@@ -281,7 +304,7 @@ void velocity_eval(sbslpm_ctx* c, int stage, double dt_s, const double* vprev, c
     launch_bltc_sources(c->tgeom, fg, c->ftab, stage, dt_s, vprev, x, y, z, vors, area, c->psrc, c->psrcf, c->fsrc,
                         mixed, st);
     launch_upward_fused(fg, 2, 0, 0.0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, c->fsrc, mixed, st);
-    launch_interactions_only(fg, c->cfg.precision, c->fsrc, c->ftgt, st);
+    launch_tree_cc(c, st);
     launch_downward_fused(fg, c->ftgt, nullptr, st);
     launch_bltc_near_batch(c->self, 1, fg.leaves, c->npl, c->cfg.kernel_eps, c->cfg.precision, x, y, z, c->psrc,
                            c->psrcf, c->near, c->near_splits, c->near_nt, c->near_tpt, st);
@@ -370,16 +393,64 @@ sbslpm_status capture_graph(sbslpm_ctx* c, cudaGraphExec_t* graph, const std::fu
   return SBSLPM_OK;
 }
 
+// Times every well-separated launch shape (the whole-panel kernel, and blocks
+// of 1..8 chunk slots over chunks of 1..4 list entries) on the current proxy
+// sources and keeps the fastest.
+sbslpm_status cc_autotune(sbslpm_ctx* c) {
+  cudaStream_t st = c->stream();
+  cudaEvent_t e0, e1;
+  SB_CUDA(cudaEventCreate(&e0));
+  SB_CUDA(cudaEventCreate(&e1));
+  double best = 1e30;
+  int cand = 0;
+  const int keep_slots = c->cc_slots, keep_len = c->cc_len;
+  int best_slots = keep_slots, best_len = keep_len;
+  for (int sl = 0; sl <= 8; sl++) {  // chunk slots per block; 0: one block per target panel
+    if (sl > 0 && !cc_chunk_shape_ok(c->qx, sl)) continue;
+    for (int len = sl > 0 ? 1 : 0; len <= (sl > 0 ? 4 : 0); len++) {
+      c->cc_slots = sl;
+      c->cc_len = len;
+      launch_tree_cc(c, st);
+      SB_CUDA(cudaEventRecord(e0, st));
+      for (int r = 0; r < 5; r++) launch_tree_cc(c, st);
+      SB_CUDA(cudaEventRecord(e1, st));
+      SB_CUDA(cudaEventSynchronize(e1));
+      float ms = 0;
+      SB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      cand++;
+      if (ms / 5 < best) {
+        best = ms / 5;
+        best_slots = sl;
+        best_len = len;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c->cc_slots = best_slots;
+  c->cc_len = best_len;
+  c->cc_candidates = cand;
+  c->cc_tuned_ms = best;
+  c->cc_tuned = true;
+  return SBSLPM_OK;
+}
+
 // Times every near-field launch shape (threads x targets per thread covering a
 // treecode leaf, 1..4 source-list splits) on the stage-0 sources and keeps the
 // fastest.  Runs once per context, before the first step, outside any capture.
 sbslpm_status near_autotune(sbslpm_ctx* c, const double* x, const double* y, const double* z, const double* area,
                             const double* vors) {
-  if (!c->tree || c->near_tuned) return SBSLPM_OK;
+  if (!c->tree || (c->near_tuned && c->cc_tuned)) return SBSLPM_OK;
   cudaStream_t st = c->stream();
   const int prec = c->cfg.precision;
   launch_bltc_sources(c->tgeom, c->fgeom, c->ftab, 0, 0.0, nullptr, x, y, z, vors, area, c->psrc, c->psrcf, c->fsrc,
                       prec == SBSLPM_MIXED, st);
+  if (!c->cc_tuned) {
+    launch_upward_fused(c->fgeom, 2, 0, 0.0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, c->fsrc,
+                        prec == SBSLPM_MIXED, st);
+    SB_TRY(cc_autotune(c));
+  }
+  if (c->near_tuned) return finish(c);
   const int shapes[][2] = {{64, 4}, {128, 2}, {256, 1}, {256, 2}, {64, 2}, {64, 1}, {128, 1}};
   cudaEvent_t e0, e1;
   SB_CUDA(cudaEventCreate(&e0));
@@ -597,9 +668,13 @@ sbslpm_status sbslpm_destroy(sbslpm_ctx* c) {
                   c->s_ntan, c->s_pow15, c->s_filt, c->s_ptan, c->s_pface, c->s_ustart, c->s_umem, c->src2,
                   c->srcf2, c->tend, c->avor, c->adj_src, c->adj_vbar, c->adj_q, c->adj_y, c->adj_part,
                   c->adj_w, c->adj_vel, c->adj_near_ts, c->adj_near_tt, c->adj_cc_ts, c->adj_cc_tt, c->adj_tbar,
-                  c->adj_qbl, c->self, c->force, c->d_time};
+                  c->adj_qbl, c->self, c->force, c->d_time, c->cc_partial};
   for (void* b : bufs)
     if (b) cudaFree(b);
+  for (int k = 0; k < 4; k++) {
+    if (c->cc_chunks[k]) cudaFree(c->cc_chunks[k]);
+    if (c->cc_cstart[k]) cudaFree(c->cc_cstart[k]);
+  }
   if (c->h_err) cudaFreeHost(c->h_err);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
@@ -853,6 +928,34 @@ sbslpm_status sbslpm_set_near_tuning(sbslpm_ctx* c, int threads, int targets_per
     cudaGraphExecDestroy(c->graph);
     c->graph = nullptr;
   }
+  return SBSLPM_OK;
+}
+
+sbslpm_status sbslpm_set_cc_tuning(sbslpm_ctx* c, int slots, int chunk_len) {
+  if (!c || !c->tree) return SBSLPM_ERR_ARG;
+  if (!c->cc_partial) return set_last_error("the treecode's proxy count has no chunked well-separated kernel"), SBSLPM_ERR_CONFIG;
+  const bool whole = slots == 0 && chunk_len == 0;
+  if (!whole && (!cc_chunk_shape_ok(c->qx, slots) || chunk_len < 1 || chunk_len > 4))
+    return set_last_error("unsupported well-separated launch shape"), SBSLPM_ERR_ARG;
+  c->cc_slots = slots;
+  c->cc_len = chunk_len;
+  c->cc_candidates = 0;
+  c->cc_tuned_ms = 0;
+  c->cc_tuned = true;
+  if (c->graph) {
+    cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+  }
+  return SBSLPM_OK;
+}
+
+sbslpm_status sbslpm_cc_tuning(const sbslpm_ctx* c, int* shape, double* ms_per_launch) {
+  if (!c || !c->tree || !shape || !ms_per_launch) return SBSLPM_ERR_ARG;
+  shape[0] = c->cc_partial && c->cc_slots > 0 ? c->cc_slots : 0;
+  shape[1] = c->cc_partial && c->cc_slots > 0 ? c->cc_len : 0;
+  shape[2] = c->cc_partial && c->cc_slots > 0 ? cc_chunk_threads(c->qx, c->cc_slots) : 128;
+  shape[3] = c->cc_candidates;
+  *ms_per_launch = c->cc_tuned_ms;
   return SBSLPM_OK;
 }
 

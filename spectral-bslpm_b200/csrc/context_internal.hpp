@@ -66,6 +66,17 @@ struct sbslpm_ctx {
   bool near_tuned = false;
   int near_candidates = 0;
   double near_tuned_ms = 0;
+  // the well-separated list cut into chunks of 1..4 entries per target panel
+  // (k = chunk length - 1), used for q >= 36; threads and chunk length are
+  // autotuned with the near field
+  int4* cc_chunks[4] = {};
+  int* cc_cstart[4] = {};
+  int cc_nchunks[4] = {};
+  double* cc_partial = nullptr;  // [n_cc][3][qx] chunk sums
+  int cc_slots = 1, cc_len = 2;  // chunk slots per block (0: one block per target panel), entries per chunk
+  bool cc_tuned = false;
+  int cc_candidates = 0;
+  double cc_tuned_ms = 0;
   sbslpm::BatchMember* self = nullptr;
   double* force = nullptr;   // [leaves*q] forcing of the current step (forcing configured)
   double* d_time = nullptr;  // the step's time on the device, advanced by dt inside each step  // this context's treecode as a one-member table (shaped near-field launches)
@@ -152,6 +163,8 @@ sbslpm_status build_tree_tables(int L, int d, const std::vector<sbslpm_panel>& g
 void build_tree_lists(const TreeTables& t, double theta, TreeLists& l);
 sbslpm_status near_autotune(sbslpm_ctx* c, const double* x, const double* y, const double* z, const double* area,
                             const double* vors);
+// The treecode's well-separated interactions into ftgt (chunked kernels where q allows).
+void launch_tree_cc(sbslpm_ctx* c, cudaStream_t st);
 sbslpm_status capture_graph(sbslpm_ctx* c, cudaGraphExec_t* graph, const std::function<void()>& body);
 
 }  // namespace sbslpm

@@ -51,6 +51,7 @@ def single_step(sb, precision, theta, pdeg, xyza, vor, tuning=(128, 2, 2)):
     ctx = sb.Context(base_cfg(sb, precision, fmm_theta=theta, proxy_degree=pdeg))
     if tuning:
         ctx.set_near_tuning(*tuning)
+        ctx.set_cc_tuning(0, 0)  # one block per target panel, the batch's CUDA-core kernel
     v = vor.clone()
     vel = [torch.zeros_like(v) for _ in range(3)]
     ctx.bve_back_rk4_step(*xyza, v, *vel)

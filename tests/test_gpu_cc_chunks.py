@@ -1,0 +1,106 @@
+"""GPU tests of the treecode's well-separated (cluster-cluster) launch shapes:
+every chunked shape (1..8 chunk slots per block, 1..4 list entries per
+chunk) against the whole-panel kernel, for every proxy count with a chunked
+kernel, in both precisions, through the C ABI (sbslpm_set_cc_tuning).
+
+The shapes evaluate the same pairs with the same per-source-panel arithmetic
+and differ only in the order in which a target's float64 sums are added, so
+the step agrees to <= 1e-13 relative L-infinity; shapes with the same chunk
+length agree bit for bit.  The treecode itself is checked against the
+float64 direct sum in test_gpu_bve.py.
+"""
+import numpy as np
+import pytest
+
+from test_gpu_bve import rel, step, unit_fields, unit_sphere_rh4
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+ORDER_TOL = 1e-13
+
+
+def tree_ctx(sb, n, precision, leaf=64):
+    cfg = sb.config_default(levels=5, interp_degree=3, fmm_theta=0.7, kernel_eps=1e-4, omega=2 * np.pi, dt=0.005,
+                            proxy_degree=n, leaf_size=leaf, precision=precision)
+    return sb.Context(cfg)
+
+
+def shapes(q):
+    """(slots, chunk length) of every chunked shape: slots in {1, 2, 3, 4, 6,
+    8} whose blocks (slots x q threads rounded up to whole warps) hold at most
+    512 threads with at most a fifth of them idle."""
+    out = []
+    for s in (1, 2, 3, 4, 6, 8):
+        nt = -(-s * q // 32) * 32
+        if nt <= 512 and 5 * s * q >= 4 * nt:
+            out += [(s, k) for k in (1, 2, 3, 4)]
+    return out
+
+
+@pytest.fixture(scope="module")
+def grid(sb):
+    g = sb.build_grid(5, 3, exact_cc=True)
+    return g, unit_sphere_rh4(g)
+
+
+@pytest.mark.parametrize("n", [5, 6, 7, 8, 9, 10])
+@pytest.mark.parametrize("precision", ["FP64", "MIXED"])
+def test_chunked_shapes_match_whole_panel_kernel(sb, grid, n, precision):
+    g, vor = grid
+    ctx = tree_ctx(sb, n, getattr(sb, precision))
+    ctx.set_near_tuning(128, 2, 2)
+    ctx.set_cc_tuning(0, 0)
+    ref = unit_fields(g, vor)
+    step(ctx, ref)
+    q = (n + 1) ** 2
+    by_len = {}
+    for sl, k in shapes(q):
+        ctx.set_cc_tuning(sl, k)
+        assert ctx.cc_tuning()[:3] == (sl, k, -(-sl * q // 32) * 32)
+        f = unit_fields(g, vor)
+        step(ctx, f)
+        assert rel(torch.stack(f["vel"]), torch.stack(ref["vel"])) <= ORDER_TOL, (sl, k)
+        assert rel(f["vors"], ref["vors"]) <= ORDER_TOL, (sl, k)
+        if k in by_len:  # the slot count does not change the arithmetic
+            assert torch.equal(f["vors"], by_len[k]["vors"]), (sl, k)
+            assert all(torch.equal(a, b) for a, b in zip(f["vel"], by_len[k]["vel"])), (sl, k)
+        by_len.setdefault(k, f)
+
+
+def test_autotuner_times_every_shape(sb, grid):
+    g, vor = grid
+    ctx = tree_ctx(sb, 8, sb.MIXED)
+    f = unit_fields(g, vor)
+    step(ctx, f)
+    sl, k, threads, cand, ms = ctx.cc_tuning()
+    assert cand == 1 + len(shapes(81)) and ms > 0
+    assert (sl, k, threads) == (0, 0, 128) or ((sl, k) in shapes(81) and threads == -(-sl * 81 // 32) * 32)
+    again = unit_fields(g, vor)
+    step(ctx, again)
+    assert torch.equal(again["vors"], f["vors"])  # a fixed shape is deterministic
+
+
+def test_graph_replay_with_chunked_shape(sb, grid):
+    g, vor = grid
+    ctx = tree_ctx(sb, 6, sb.MIXED)
+    ctx.set_near_tuning(128, 2, 2)
+    ctx.set_cc_tuning(3, 3)
+    a, b = unit_fields(g, vor), unit_fields(g, vor)
+    step(ctx, a, 2)
+    step(ctx, b, 2, graph=True)
+    assert torch.equal(a["vors"], b["vors"])
+
+
+def test_rejects_unsupported_shapes(sb):
+    ctx = tree_ctx(sb, 6, sb.MIXED)  # 49 proxies: slots 3, 4, 6, 8
+    for sl, k in ((1, 1), (2, 2), (5, 1), (3, 0), (3, 5), (9, 1), (0, 1), (-1, 1)):
+        with pytest.raises(sb.SbslpmError):
+            ctx.set_cc_tuning(sl, k)
+    small = tree_ctx(sb, 3, sb.MIXED)  # 16 proxies: whole-panel kernel only
+    with pytest.raises(sb.SbslpmError):
+        small.set_cc_tuning(1, 1)
+    assert small.cc_tuning()[:3] == (0, 0, 128)
+    spectral = sb.Context(sb.config_default(levels=4, interp_degree=3, fmm_theta=0.7, kernel_eps=1e-4))
+    with pytest.raises(sb.SbslpmError):
+        spectral.set_cc_tuning(0, 0)
