@@ -373,15 +373,47 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_interact64(StepGeom g, 
       tz = g.px[2 * pn + o];
     }
     double ax = 0, ay = 0, az = 0;
-    for (int e = e0; e < e1; e += W::S) {
-      if (active && e + h < e1) stage[warp][h * Q + j] = src[(long)source_of(e + h) * Q + j];
-      __syncwarp();
-      if (active && e + h < e1) {
-        const double4* sp = &stage[warp][h * Q];
+    if constexpr (ALL_LEAVES) {
+      for (int e = e0; e < e1; e += W::S) {
+        if (active && e + h < e1) stage[warp][h * Q + j] = src[(long)source_of(e + h) * Q + j];
+        __syncwarp();
+        if (active && e + h < e1) {
+          const double4* sp = &stage[warp][h * Q];
 #pragma unroll
-        for (int k = 0; k < Q; k++) pair64<GUARD>(tx, ty, tz, sp[k], g.eps, ax, ay, az);
+          for (int k = 0; k < Q; k++) pair64<GUARD>(tx, ty, tz, sp[k], g.eps, ax, ay, az);
+        }
+        __syncwarp();
       }
-      __syncwarp();
+    } else {
+      // the list in batches of 32 entries, one source index per lane, handed
+      // to the splits by shuffles; the next entry's sources are loaded while
+      // the current ones are evaluated
+      for (int eb = e0; eb < e1; eb += 32) {
+        const int nb = min(32, e1 - eb);
+        const int idx = lane < nb ? __ldg(g.src_panel + eb + lane) : 0;
+        const int iters = (nb + W::S - 1) / W::S;
+        double4 sv = make_double4(0, 0, 0, 0);
+        {
+          const int sp = __shfl_sync(0xffffffffu, idx, h & 31);
+          if (active && h < nb) sv = src[(long)sp * Q + j];
+        }
+        for (int it = 0; it < iters; it++) {
+          const bool on = active && it * W::S + h < nb;
+          const int ns = (it + 1) * W::S + h;
+          const int sp_n = __shfl_sync(0xffffffffu, idx, ns & 31);
+          double4 sv_n = make_double4(0, 0, 0, 0);
+          if (active && ns < nb) sv_n = src[(long)sp_n * Q + j];
+          if (on) stage[warp][h * Q + j] = sv;
+          __syncwarp();
+          if (on) {
+            const double4* sp = &stage[warp][h * Q];
+#pragma unroll
+            for (int k = 0; k < Q; k++) pair64<GUARD>(tx, ty, tz, sp[k], g.eps, ax, ay, az);
+          }
+          __syncwarp();
+          sv = sv_n;
+        }
+      }
     }
     if (W::S > 1) {
       red[warp][0][lane] = ax;
@@ -447,7 +479,10 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_interact64(StepGeom g, 
 
 // Mixed precision: positions relative to panel centres in float, pair
 // arithmetic in float32, per-source-panel partial sums in float32 added into
-// float64 accumulators.
+// float64 accumulators.  For q <= 32 the two float32 halves of a panel's sum
+// are added in float32 before the conversion: with 16 sources per panel the
+// float64 conversions would otherwise load the MUFU/conversion pipe more than
+// the reciprocals do.
 __global__ void k_pack_mixed(StepGeom g, const double4* __restrict__ src, float4* __restrict__ srcf) {
   long pn = (long)g.panels * g.q;
   long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
@@ -502,42 +537,112 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_interact32(StepGeom g, 
     // each split's panel staged two sources per pair slot, transposed as
     // (x0,x1,y0,y1),(z0,z1,w0,w1); a missing partner (odd q) has zero strength
     float* sl = reinterpret_cast<float*>(&stage[warp][0]) + h * 8 * W::Q2;
-    for (int e = e0; e < e1; e += W::S) {
-      int sp = 0;
-      if (active && e + h < e1) {
-        sp = ALL_LEAVES ? g.offset + e + h : __ldg(g.src_panel + e + h);
-        const float4 sv = srcf[(long)sp * Q + j];
-        const int k2 = j >> 1, o = j & 1;
-        sl[8 * k2 + o] = sv.x;
-        sl[8 * k2 + 2 + o] = sv.y;
-        sl[8 * k2 + 4 + o] = sv.z;
-        sl[8 * k2 + 6 + o] = sv.w;
-        if ((Q & 1) && j == Q - 1) {
-          sl[8 * k2 + 1] = 0.f;
-          sl[8 * k2 + 3] = 0.f;
-          sl[8 * k2 + 5] = 0.f;
-          sl[8 * k2 + 7] = 0.f;
+    if constexpr (ALL_LEAVES) {
+      for (int e = e0; e < e1; e += W::S) {
+        int sp = 0;
+        if (active && e + h < e1) {
+          sp = g.offset + e + h;
+          const float4 sv = srcf[(long)sp * Q + j];
+          const int k2 = j >> 1, o = j & 1;
+          sl[8 * k2 + o] = sv.x;
+          sl[8 * k2 + 2 + o] = sv.y;
+          sl[8 * k2 + 4 + o] = sv.z;
+          sl[8 * k2 + 6 + o] = sv.w;
+          if ((Q & 1) && j == Q - 1) {
+            sl[8 * k2 + 1] = 0.f;
+            sl[8 * k2 + 3] = 0.f;
+            sl[8 * k2 + 5] = 0.f;
+            sl[8 * k2 + 7] = 0.f;
+          }
         }
-      }
-      __syncwarp();
-      if (active && e + h < e1) {
-        const double* cs = g.pd_centre + 4 * (long)sp;
-        const float b0 = (float)((cs[0] - ctx) * kPackScale) - dtx, b1 = (float)((cs[1] - cty) * kPackScale) - dty,
-                    b2 = (float)((cs[2] - ctz) * kPackScale) - dtz;
-        const float2 bx = make_float2(b0, b0), by = make_float2(b1, b1), bz = make_float2(b2, b2);
-        float2 fx = make_float2(0.f, 0.f), fy = fx, fz = fx;
-        const float4* sb = reinterpret_cast<const float4*>(sl);
+        __syncwarp();
+        if (active && e + h < e1) {
+          const double* cs = g.pd_centre + 4 * (long)sp;
+          const float b0 = (float)((cs[0] - ctx) * kPackScale) - dtx, b1 = (float)((cs[1] - cty) * kPackScale) - dty,
+                      b2 = (float)((cs[2] - ctz) * kPackScale) - dtz;
+          const float2 bx = make_float2(b0, b0), by = make_float2(b1, b1), bz = make_float2(b2, b2);
+          float2 fx = make_float2(0.f, 0.f), fy = fx, fz = fx;
+          const float4* sb = reinterpret_cast<const float4*>(sl);
 #pragma unroll
-        for (int k2 = 0; k2 < W::Q2; k2++) {
-          const float4 A = sb[2 * k2], B = sb[2 * k2 + 1];
-          pair32x2<GUARD>(bx, by, bz, make_float2(A.x, A.y), make_float2(A.z, A.w), make_float2(B.x, B.y),
-                          make_float2(B.z, B.w), eps2, fx, fy, fz);
+          for (int k2 = 0; k2 < W::Q2; k2++) {
+            const float4 A = sb[2 * k2], B = sb[2 * k2 + 1];
+            pair32x2<GUARD>(bx, by, bz, make_float2(A.x, A.y), make_float2(A.z, A.w), make_float2(B.x, B.y),
+                            make_float2(B.z, B.w), eps2, fx, fy, fz);
+          }
+          ax += (double)(fx.x + fx.y);
+          ay += (double)(fy.x + fy.y);
+          az += (double)(fz.x + fz.y);
         }
-        ax += (double)fx.x + (double)fx.y;
-        ay += (double)fy.x + (double)fy.y;
-        az += (double)fz.x + (double)fz.y;
+        __syncwarp();
       }
-      __syncwarp();
+    } else {
+      // The list in batches of 32 entries (g.entry: source panel and its
+      // centre's offset from the target's, one entry per lane), handed to the
+      // splits by shuffles; the next entry's sources are loaded while the
+      // current ones are evaluated.  A source pair is staged by one store per
+      // lane: the even node of a pair writes (x0,x1,y0,y1), the odd one
+      // (z0,z1,w0,w1), each taking its partner's half by a shuffle.
+      const unsigned full = 0xffffffffu;
+      float4* st4 = reinterpret_cast<float4*>(sl);
+      const bool odd = j & 1, last_odd = (Q & 1) && j == Q - 1;
+      const int partner = (odd ? lane - 1 : lane + 1) & 31;
+      for (int eb = e0; eb < e1; eb += 32) {
+        const int nb = min(32, e1 - eb);
+        int4 en = make_int4(0, 0, 0, 0);
+        if (lane < nb) en = __ldg(g.entry + eb + lane);
+        const int iters = (nb + W::S - 1) / W::S;
+        float cbx = __int_as_float(__shfl_sync(full, en.y, h & 31));
+        float cby = __int_as_float(__shfl_sync(full, en.z, h & 31));
+        float cbz = __int_as_float(__shfl_sync(full, en.w, h & 31));
+        float4 sv = make_float4(0.f, 0.f, 0.f, 0.f);
+        {
+          const int sp = __shfl_sync(full, en.x, h & 31);
+          if (active && h < nb) sv = srcf[(long)sp * Q + j];
+        }
+        for (int it = 0; it < iters; it++) {
+          const bool on = active && it * W::S + h < nb;
+          const int ns = (it + 1) * W::S + h;
+          const int sp_n = __shfl_sync(full, en.x, ns & 31);
+          const float nbx = __int_as_float(__shfl_sync(full, en.y, ns & 31));
+          const float nby = __int_as_float(__shfl_sync(full, en.z, ns & 31));
+          const float nbz = __int_as_float(__shfl_sync(full, en.w, ns & 31));
+          float4 sv_n = make_float4(0.f, 0.f, 0.f, 0.f);
+          if (active && ns < nb) sv_n = srcf[(long)sp_n * Q + j];
+          const float r0 = __shfl_sync(full, odd ? sv.x : sv.z, partner);
+          const float r1 = __shfl_sync(full, odd ? sv.y : sv.w, partner);
+          if (on) {
+            const int k2 = j >> 1;
+            if (last_odd) {
+              st4[2 * k2] = make_float4(sv.x, 0.f, sv.y, 0.f);
+              st4[2 * k2 + 1] = make_float4(sv.z, 0.f, sv.w, 0.f);
+            } else if (!odd) {
+              st4[2 * k2] = make_float4(sv.x, r0, sv.y, r1);
+            } else {
+              st4[2 * k2 + 1] = make_float4(r0, sv.z, r1, sv.w);
+            }
+          }
+          __syncwarp();
+          if (on) {
+            const float b0 = cbx - dtx, b1 = cby - dty, b2 = cbz - dtz;
+            const float2 bx = make_float2(b0, b0), by = make_float2(b1, b1), bz = make_float2(b2, b2);
+            float2 fx = make_float2(0.f, 0.f), fy = fx, fz = fx;
+#pragma unroll
+            for (int k2 = 0; k2 < W::Q2; k2++) {
+              const float4 A = st4[2 * k2], B = st4[2 * k2 + 1];
+              pair32x2<GUARD>(bx, by, bz, make_float2(A.x, A.y), make_float2(A.z, A.w), make_float2(B.x, B.y),
+                              make_float2(B.z, B.w), eps2, fx, fy, fz);
+            }
+            ax += (double)(fx.x + fx.y);
+            ay += (double)(fy.x + fy.y);
+            az += (double)(fz.x + fz.y);
+          }
+          __syncwarp();
+          sv = sv_n;
+          cbx = nbx;
+          cby = nby;
+          cbz = nbz;
+        }
+      }
     }
     if (W::S > 1) {
       red[warp][0][lane] = ax;
@@ -612,6 +717,132 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_interact32(StepGeom g, 
       out[o] = kBiotSavartPacked * (ty[r] * az[r] - tz[r] * ay[r]);
       out[s + o] = kBiotSavartPacked * (tz[r] * ax[r] - tx[r] * az[r]);
       out[2 * s + o] = kBiotSavartPacked * (tx[r] * ay[r] - ty[r] * ax[r]);
+    }
+  }
+}
+
+// The list kernel of the reference's default degree 3 (q = 16) in mixed
+// precision, two targets per lane: a warp holds one target panel as 4
+// source splits x 8 lanes, lane jj of a split owns target nodes jj and
+// jj + 8, stages the source pair (2 jj, 2 jj + 1) of its split's panel
+// ((x0,x1,y0,y1),(z0,z1,w0,w1), one pair slot per lane) and evaluates the
+// split's 16 sources against both targets, so every shared-memory read feeds
+// two targets' pairs.  Entries come in batches of 32 (g.entry) handed out by
+// shuffles, the next entry's sources are loaded while the current ones are
+// evaluated, and the four splits' float64 sums are added in split order.
+template <bool GUARD>
+__global__ void __launch_bounds__(32 * kWarpsPerBlock) k_interact32_q16(StepGeom g, const float4* __restrict__ srcf,
+                                                                        double* __restrict__ out) {
+  constexpr int Q = 16, S = 4;
+  __shared__ float4 stage[kWarpsPerBlock][S][Q];
+  __shared__ double red[kWarpsPerBlock][6][32];
+  const unsigned full = 0xffffffffu;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int t = blockIdx.x * kWarpsPerBlock + warp;
+  if (t >= g.panels) return;
+  const long pn = (long)g.panels * Q;
+  const int e0 = g.tgt_start[t], e1 = g.tgt_start[t + 1];
+  const int h = lane >> 3, jj = lane & 7;
+  const double* ct = g.pd_centre + 4 * (long)t;
+  float dtx[2], dty[2], dtz[2];
+#pragma unroll
+  for (int r = 0; r < 2; r++) {
+    const long o = (long)t * Q + jj + 8 * r;
+    dtx[r] = (float)((g.px[o] - ct[0]) * kPackScale);
+    dty[r] = (float)((g.px[pn + o] - ct[1]) * kPackScale);
+    dtz[r] = (float)((g.px[2 * pn + o] - ct[2]) * kPackScale);
+  }
+  double ax[2] = {0, 0}, ay[2] = {0, 0}, az[2] = {0, 0};
+  const float feps = (float)g.eps;
+  const float2 eps2 = make_float2(feps, feps);
+  float4* tile = stage[warp][h];
+  for (int eb = e0; eb < e1; eb += 32) {
+    const int nb = min(32, e1 - eb);
+    int4 en = make_int4(0, 0, 0, 0);
+    if (lane < nb) en = __ldg(g.entry + eb + lane);
+    const int iters = (nb + S - 1) / S;
+    float cbx = __int_as_float(__shfl_sync(full, en.y, h));
+    float cby = __int_as_float(__shfl_sync(full, en.z, h));
+    float cbz = __int_as_float(__shfl_sync(full, en.w, h));
+    float4 s0 = make_float4(0.f, 0.f, 0.f, 0.f), s1 = s0;
+    {
+      const int sp = __shfl_sync(full, en.x, h);
+      if (h < nb) {
+        s0 = srcf[(long)sp * Q + 2 * jj];
+        s1 = srcf[(long)sp * Q + 2 * jj + 1];
+      }
+    }
+    for (int it = 0; it < iters; it++) {
+      const bool on = it * S + h < nb;
+      const int ns = (it + 1) * S + h;
+      const int sp_n = __shfl_sync(full, en.x, ns & 31);
+      const float nbx = __int_as_float(__shfl_sync(full, en.y, ns & 31));
+      const float nby = __int_as_float(__shfl_sync(full, en.z, ns & 31));
+      const float nbz = __int_as_float(__shfl_sync(full, en.w, ns & 31));
+      float4 n0 = make_float4(0.f, 0.f, 0.f, 0.f), n1 = n0;
+      if (ns < nb) {
+        n0 = srcf[(long)sp_n * Q + 2 * jj];
+        n1 = srcf[(long)sp_n * Q + 2 * jj + 1];
+      }
+      if (on) {
+        tile[2 * jj] = make_float4(s0.x, s1.x, s0.y, s1.y);
+        tile[2 * jj + 1] = make_float4(s0.z, s1.z, s0.w, s1.w);
+      }
+      __syncwarp();
+      if (on) {
+        float2 bx[2], by[2], bz[2], fx[2], fy[2], fz[2];
+#pragma unroll
+        for (int r = 0; r < 2; r++) {
+          const float b0 = cbx - dtx[r], b1 = cby - dty[r], b2 = cbz - dtz[r];
+          bx[r] = make_float2(b0, b0);
+          by[r] = make_float2(b1, b1);
+          bz[r] = make_float2(b2, b2);
+          fx[r] = fy[r] = fz[r] = make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (int k2 = 0; k2 < Q / 2; k2++) {
+          const float4 A = tile[2 * k2], B = tile[2 * k2 + 1];
+          const float2 sx = make_float2(A.x, A.y), sy = make_float2(A.z, A.w), sz = make_float2(B.x, B.y),
+                       sw = make_float2(B.z, B.w);
+#pragma unroll
+          for (int r = 0; r < 2; r++) pair32x2<GUARD>(bx[r], by[r], bz[r], sx, sy, sz, sw, eps2, fx[r], fy[r], fz[r]);
+        }
+#pragma unroll
+        for (int r = 0; r < 2; r++) {
+          ax[r] += (double)(fx[r].x + fx[r].y);
+          ay[r] += (double)(fy[r].x + fy[r].y);
+          az[r] += (double)(fz[r].x + fz[r].y);
+        }
+      }
+      __syncwarp();
+      s0 = n0;
+      s1 = n1;
+      cbx = nbx;
+      cby = nby;
+      cbz = nbz;
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < 2; r++) {
+    red[warp][3 * r][lane] = ax[r];
+    red[warp][3 * r + 1][lane] = ay[r];
+    red[warp][3 * r + 2][lane] = az[r];
+  }
+  __syncwarp();
+  if (h == 0) {
+#pragma unroll
+    for (int r = 0; r < 2; r++) {
+      double sx = ax[r], sy = ay[r], sz = az[r];
+      for (int hh = 1; hh < S; hh++) {
+        sx += red[warp][3 * r][hh * 8 + jj];
+        sy += red[warp][3 * r + 1][hh * 8 + jj];
+        sz += red[warp][3 * r + 2][hh * 8 + jj];
+      }
+      const long o = (long)t * Q + jj + 8 * r;
+      const double tx = g.px[o], ty = g.px[pn + o], tz = g.px[2 * pn + o];
+      out[o] = kBiotSavartPacked * (ty * sz - tz * sy);
+      out[pn + o] = kBiotSavartPacked * (tz * sx - tx * sz);
+      out[2 * pn + o] = kBiotSavartPacked * (tx * sy - ty * sx);
     }
   }
 }
@@ -1171,6 +1402,8 @@ void interact_qg(const StepGeom& g, int precision, const double4* src, double* o
     if (pack) SB_LAUNCH(k_pack_mixed, blocks_for(pn, 256), 256, 0, st, g, src, g.srcf);
     if (all_leaves)
       SB_LAUNCH((k_interact32<Q, true, GUARD>), grid, 32 * kWarpsPerBlock, 0, st, g, g.srcf, out, out_stride);
+    else if constexpr (Q == 16)
+      SB_LAUNCH((k_interact32_q16<GUARD>), grid, 32 * kWarpsPerBlock, 0, st, g, g.srcf, out);
     else
       SB_LAUNCH((k_interact32<Q, false, GUARD>), grid, 32 * kWarpsPerBlock, 0, st, g, g.srcf, out, out_stride);
     return;

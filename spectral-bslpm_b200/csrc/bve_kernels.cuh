@@ -34,6 +34,10 @@ struct StepGeom {
   const double* child_1d;     // [2][d+1][d+1]: 1-D basis of parent node a at the node i of a child in the upper (0) / lower (1) half
   const double* pd_centre;    // mixed: panel centres [panels][4] (double)
   float4* srcf;               // mixed: packed sources [panels*q] (workspace)
+  // mixed, q <= 32: per list entry (CSR order) the source panel and the offset
+  // of its centre from the target panel's, (float)((c_S - c_T) kPackScale) as
+  // float bits
+  const int4* entry;
   unsigned* err;              // device error word
   const double* force;        // forcing added to the leaf vorticity [leaves*q], or null
 };

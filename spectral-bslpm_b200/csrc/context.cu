@@ -51,6 +51,27 @@ sbslpm_status validate(const sbslpm_config& c) {
 }
 
 // Host precomputation of everything that does not change during a run.
+
+// The entry table of the mixed-precision kernels for q <= 32: per entry of a
+// CSR list (start by target, src) the source panel and the offset of its
+// centre from the target's centre, (float)((c_S - c_T) kPackScale), as float
+// bits; the same double arithmetic and rounding as the direct-sum kernels
+// apply per source leaf on the device.
+std::vector<int4> entry_table(const std::vector<int>& start, const std::vector<int>& src,
+                              const std::vector<double>& centre) {
+  std::vector<int4> out(src.size());
+  for (size_t t = 0; t + 1 < start.size(); t++)
+    for (int e = start[t]; e < start[t + 1]; e++) {
+      const size_t sp = (size_t)src[e];
+      float b[3];
+      for (int k = 0; k < 3; k++) b[k] = (float)((centre[4 * sp + k] - centre[4 * t + k]) * kPackScale);
+      int bits[3];
+      std::memcpy(bits, b, sizeof b);
+      out[e] = make_int4(src[e], bits[0], bits[1], bits[2]);
+    }
+  return out;
+}
+
 sbslpm_status precompute(sbslpm_ctx* c) {
   const int q = c->q, P = c->P, off = c->off, d = c->d;
   std::vector<double> interp;
@@ -127,6 +148,7 @@ sbslpm_status precompute(sbslpm_ctx* c) {
   for (const auto& e : c->list) srcs[fill[e.target_panel]++] = e.source_panel;
   SB_TRY(upload(&c->tgt_start, start));
   SB_TRY(upload(&c->src_panel, srcs));
+  if (c->cfg.precision == SBSLPM_MIXED && q <= 32) SB_TRY(upload(&c->entry32, entry_table(start, srcs, centre)));
   return SBSLPM_OK;
 }
 
@@ -165,6 +187,7 @@ sbslpm_status precompute_tree(sbslpm_ctx* c) {
   SB_TRY(upload(&c->near_src, l.nsrc));
   SB_TRY(upload(&c->cc_start, l.cs));
   SB_TRY(upload(&c->cc_src, l.csrc));
+  if (c->cfg.precision == SBSLPM_MIXED && t.qx <= 32) SB_TRY(upload(&c->fentry32, entry_table(l.cs, l.csrc, t.centre)));
   if (c->n_cc > 0 && cc_chunk_supported(t.qx)) {
     for (int k = 0; k < 4; k++) {
       std::vector<int4> chunks;
@@ -241,6 +264,7 @@ void fill_geom(sbslpm_ctx* c) {
   g.child_1d = c->child_mat;
   g.pd_centre = c->centre;
   g.srcf = c->srcf;
+  g.entry = c->entry32;
   g.err = c->err;
   if (c->tree) {
     StepGeom& f = c->fgeom;
@@ -258,6 +282,7 @@ void fill_geom(sbslpm_ctx* c) {
     f.child_1d = c->fchild;
     f.pd_centre = c->fcentre;
     f.srcf = c->fsrcf;
+    f.entry = c->fentry32;
     f.err = c->err;
     TreeGeom& t = c->tgeom;
     t.n = c->n;
@@ -668,7 +693,7 @@ sbslpm_status sbslpm_destroy(sbslpm_ctx* c) {
                   c->s_ntan, c->s_pow15, c->s_filt, c->s_ptan, c->s_pface, c->s_ustart, c->s_umem, c->src2,
                   c->srcf2, c->tend, c->avor, c->adj_src, c->adj_vbar, c->adj_q, c->adj_y, c->adj_part,
                   c->adj_w, c->adj_vel, c->adj_near_ts, c->adj_near_tt, c->adj_cc_ts, c->adj_cc_tt, c->adj_tbar,
-                  c->adj_qbl, c->self, c->force, c->d_time, c->cc_partial};
+                  c->adj_qbl, c->self, c->force, c->d_time, c->cc_partial, c->entry32, c->fentry32};
   for (void* b : bufs)
     if (b) cudaFree(b);
   for (int k = 0; k < 4; k++) {

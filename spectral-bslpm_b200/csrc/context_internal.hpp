@@ -39,6 +39,7 @@ struct sbslpm_ctx {
   // static device data
   double *px = nullptr, *il_basis = nullptr, *child_mat = nullptr, *centre = nullptr;
   int *tgt_start = nullptr, *src_panel = nullptr, *il_row = nullptr;
+  int4* entry32 = nullptr;  // mixed, q <= 32: per list entry source panel + centre offset (StepGeom::entry)
   // workspace
   double4* src = nullptr;
   float4* srcf = nullptr;
@@ -59,6 +60,7 @@ struct sbslpm_ctx {
   std::vector<sbslpm_panel> fpanels;
   double *fpx = nullptr, *fchild = nullptr, *fcentre = nullptr, *flx = nullptr, *fly = nullptr, *fbounds = nullptr;
   int *fface = nullptr, *near_start = nullptr, *near_src = nullptr, *cc_start = nullptr, *cc_src = nullptr;
+  int4* fentry32 = nullptr;  // the same entry table over the well-separated list (mixed, q <= 32)
   double4 *fsrc = nullptr, *psrc = nullptr;
   double* gx = nullptr;  // [3][particles]: the particle grid, for timing the near kernel alone
   double* near = nullptr;  // [4][3][particles] near-field partial sums (near_splits in use)
