@@ -113,7 +113,8 @@ __global__ void k_copy_strength(StepGeom g, const double4* __restrict__ src, dou
 // proxy positions untouched, mixed packing as in mode 0.
 
 __device__ __forceinline__ void upward_subtree_body(const StepGeom& g, int root_rel, int r, int D, int mode,
-                                                    int stage, double dt_s, const double* __restrict__ vprev,
+                                                    int positions, int stage, double dt_s,
+                                                    const double* __restrict__ vprev,
                                                     const double* __restrict__ x, const double* __restrict__ y,
                                                     const double* __restrict__ z, const double* __restrict__ vors,
                                                     const double* __restrict__ area, double4* __restrict__ src,
@@ -159,8 +160,9 @@ __device__ __forceinline__ void upward_subtree_body(const StepGeom& g, int root_
       }
     }
   }
-  // displaced positions of the subtree's non-leaf proxies (levels r..r+D-1)
-  if (mode == 0) {
+  // displaced positions of the subtree's non-leaf proxies (levels r..r+D-1),
+  // unless k_nonleaf_positions wrote them before the pass
+  if (mode == 0 && positions) {
     for (int k = 0; k < D; k++) {
       const int first = subtree_first(r, root_rel, k), npts = (1 << (2 * k)) * q;
       for (int t = threadIdx.x; t < npts; t += blockDim.x) {
@@ -216,18 +218,50 @@ __device__ __forceinline__ void upward_subtree_body(const StepGeom& g, int root_
   }
 }
 
-__global__ void k_upward_subtree(StepGeom g, int r, int D, int mode, int stage, double dt_s,
+__global__ void k_upward_subtree(StepGeom g, int r, int D, int mode, int positions, int stage, double dt_s,
                                  const double* __restrict__ vprev, const double* __restrict__ x,
                                  const double* __restrict__ y, const double* __restrict__ z,
                                  const double* __restrict__ vors, const double* __restrict__ area,
                                  double4* __restrict__ src, int mixed) {
-  upward_subtree_body(g, blockIdx.x, r, D, mode, stage, dt_s, vprev, x, y, z, vors, area, src, mixed);
+  upward_subtree_body(g, blockIdx.x, r, D, mode, positions, stage, dt_s, vprev, x, y, z, vors, area, src, mixed);
+}
+
+// The displaced positions of every non-leaf proxy (bve_disp_interp,
+// src/bve_time_step.cpp:107-160) in one flat launch, a thread per point, ahead
+// of the subtree passes of mode 0: the same arithmetic as nonleaf_position,
+// with the q-term interpolation unrolled for q = 16, so that the passes
+// themselves no longer wait on these gathers level by level.
+template <int Q>
+__global__ void k_nonleaf_positions(StepGeom g, int stage, double dt_s, const double* __restrict__ vprev,
+                                    double4* __restrict__ src) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const int q = Q > 0 ? Q : g.q;
+  if (i >= (long)g.offset * q) return;
+  const long pn = (long)g.panels * q, ln = (long)g.leaves * q;
+  double px = g.px[i], py = g.px[pn + i], pz = g.px[2 * pn + i];
+  if (stage > 0) {
+    const double* b = g.il_basis + i * q;
+    const long row = (long)g.il_row[i] * q;
+    double ax = 0, ay = 0, az = 0;
+#pragma unroll
+    for (int m = 0; m < (Q > 0 ? Q : q); m++) {
+      const double bm = b[m];
+      ax += (dt_s * vprev[row + m]) * bm;
+      ay += (dt_s * vprev[ln + row + m]) * bm;
+      az += (dt_s * vprev[2 * ln + row + m]) * bm;
+    }
+    px += ax;
+    py += ay;
+    pz += az;
+  }
+  project_to_sphere(px, py, pz);
+  src[i] = make_double4(px, py, pz, 0.0);
 }
 
 // Batched treecode members (mode 2): member blockIdx.z.
 __global__ void k_upward_subtree_batch(const BatchMember* __restrict__ mem, int r, int D, int mixed) {
   const StepGeom g = mem[blockIdx.z].fg;
-  upward_subtree_body(g, blockIdx.x, r, D, 2, 0, 0.0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+  upward_subtree_body(g, blockIdx.x, r, D, 2, 0, 0, 0.0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
                       mem[blockIdx.z].fsrc, mixed);
 }
 
@@ -1294,12 +1328,18 @@ void launch_upward_fused(const StepGeom& g, int mode, int stage, double dt_s, co
   }
   const int Dmax = subtree_depth(g.q);
   int r = g.levels - 1;  // the bottom of the next subtree
+  const long nl = (long)g.offset * g.q;  // non-leaf proxy points
+  const bool flat = mode == 0 && nl > 0;
+  if (flat) {
+    if (g.q == 16) SB_LAUNCH(k_nonleaf_positions<16>, blocks_for(nl, 256), 256, 0, st, g, stage, dt_s, vprev, src);
+    else SB_LAUNCH(k_nonleaf_positions<0>, blocks_for(nl, 256), 256, 0, st, g, stage, dt_s, vprev, src);
+  }
   bool first = true;
   while (first || r > 0) {
     int D = first ? (r < Dmax ? r : Dmax) : (r < Dmax ? r : Dmax);
     int root = r - D;
     SB_LAUNCH(k_upward_subtree, (unsigned)(6 << (2 * root)), 256, subtree_smem(g.q, 1, D), st, g, root, D, mode,
-              stage, dt_s, vprev, x, y, z, vors, area, src, mixed ? 1 : 0);
+              flat ? 0 : 1, stage, dt_s, vprev, x, y, z, vors, area, src, mixed ? 1 : 0);
     r = root;
     first = false;
   }
