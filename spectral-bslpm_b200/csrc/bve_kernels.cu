@@ -240,12 +240,12 @@ __global__ void k_nonleaf_positions(StepGeom g, int stage, double dt_s, const do
   const long pn = (long)g.panels * q, ln = (long)g.leaves * q;
   double px = g.px[i], py = g.px[pn + i], pz = g.px[2 * pn + i];
   if (stage > 0) {
-    const double* b = g.il_basis + i * q;
+    const long np = (long)g.offset * q;
     const long row = (long)g.il_row[i] * q;
     double ax = 0, ay = 0, az = 0;
 #pragma unroll
     for (int m = 0; m < (Q > 0 ? Q : q); m++) {
-      const double bm = b[m];
+      const double bm = g.il_basis[m * np + i];
       ax += (dt_s * vprev[row + m]) * bm;
       ay += (dt_s * vprev[ln + row + m]) * bm;
       az += (dt_s * vprev[2 * ln + row + m]) * bm;

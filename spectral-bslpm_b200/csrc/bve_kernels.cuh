@@ -30,7 +30,7 @@ struct StepGeom {
   const int* tgt_start;       // [panels+1] CSR of the interaction list by target
   const int* src_panel;       // [interactions] source panel, list order within a target
   const int* il_row;          // [(panels-leaves)*q] leaf row interpolating a non-leaf proxy
-  const double* il_basis;     // [(panels-leaves)*q*q] BLI basis at that leaf
+  const double* il_basis;     // [q][(panels-leaves)*q] BLI basis at that leaf, term-major (coalesced per point)
   const double* child_1d;     // [2][d+1][d+1]: 1-D basis of parent node a at the node i of a child in the upper (0) / lower (1) half
   const double* pd_centre;    // mixed: panel centres [panels][4] (double)
   float4* srcf;               // mixed: packed sources [panels*q] (workspace)

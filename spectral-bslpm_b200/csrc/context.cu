@@ -120,8 +120,10 @@ sbslpm_status precompute(sbslpm_ctx* c) {
       Bounds b;
       int leaf = locate_leaf(xyz[0], xyz[1], xyz[2], c->L, lxi, leta, b, err);
       il_row[(size_t)i * q + j] = leaf - off;
-      host_bli(&il_basis[((size_t)i * q + j) * q], xi, eta, kPi / 4.0 * b.min_xi, kPi / 4.0 * b.max_xi,
-               kPi / 4.0 * b.min_eta, kPi / 4.0 * b.max_eta, d, err);
+      double basis[(kMaxDegree + 1) * (kMaxDegree + 1)];
+      host_bli(basis, xi, eta, kPi / 4.0 * b.min_xi, kPi / 4.0 * b.max_xi, kPi / 4.0 * b.min_eta,
+               kPi / 4.0 * b.max_eta, d, err);
+      for (int m = 0; m < q; m++) il_basis[(size_t)m * off * q + (size_t)i * q + j] = basis[m];
     }
   }
   if (err) {

@@ -94,11 +94,11 @@ __device__ __forceinline__ void nonleaf_position(const StepGeom& g, long i, int 
   py = g.px[pn + i];
   pz = g.px[2 * pn + i];
   if (stage > 0) {
-    const double* b = g.il_basis + i * g.q;
+    const long np = (long)g.offset * g.q;
     const long row = (long)g.il_row[i] * g.q;
     double ax = 0, ay = 0, az = 0;
     for (int m = 0; m < g.q; m++) {
-      double bm = b[m];
+      double bm = g.il_basis[m * np + i];
       ax += (dt_s * vprev[row + m]) * bm;
       ay += (dt_s * vprev[ln + row + m]) * bm;
       az += (dt_s * vprev[2 * ln + row + m]) * bm;
