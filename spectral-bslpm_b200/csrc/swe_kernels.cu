@@ -380,6 +380,152 @@ __global__ void __launch_bounds__(32 * kWarps)
   }
 }
 
+// Mixed precision, q <= 32, list mode: the BVE list kernel's organisation
+// (k_interact32) with both source fields.  List entries come 32 at a time
+// from the static entry table (source panel, centre offset as float) and are
+// handed to the splits by shuffles; the next entry's sources of both fields
+// are loaded while the current ones are evaluated; each field's source pair
+// is staged (x0,x1,y0,y1),(z0,z1,w0,w1) by one store per lane, and both
+// fields' pairs run on the paired float32 instructions (pair32x2), two
+// sources per instruction.  A panel's float32 halves are added before the
+// float64 conversion.
+template <int Q, bool GUARD>
+__global__ void __launch_bounds__(32 * kWarps) k_swe_interact32_list(StepGeom g, SweGeom sw,
+                                                                     double* __restrict__ out) {
+  using W = Shape<Q>;
+  constexpr int Q2 = (Q + 1) / 2;
+  __shared__ float4 stage[kWarps][2][W::S * 2 * Q2];
+  __shared__ double red[kWarps][6][32];
+  const unsigned full = 0xffffffffu;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int t = blockIdx.x * kWarps + warp;
+  if (t >= g.panels) return;
+  const long pn = (long)g.panels * Q;
+  const int e0 = g.tgt_start[t], e1 = g.tgt_start[t + 1];
+  const int h = lane / Q, j = lane % Q;
+  const bool active = h < W::S;
+  const double* ct = g.pd_centre + 4 * (long)t;
+  double tx = 0, ty = 0, tz = 0;
+  float dtx = 0, dty = 0, dtz = 0;
+  if (active) {
+    const long o = (long)t * Q + j;
+    tx = g.px[o];
+    ty = g.px[pn + o];
+    tz = g.px[2 * pn + o];
+    dtx = (float)((tx - ct[0]) * kPackScale);
+    dty = (float)((ty - ct[1]) * kPackScale);
+    dtz = (float)((tz - ct[2]) * kPackScale);
+  }
+  double ax = 0, ay = 0, az = 0, bx = 0, by = 0, bz = 0;
+  const float feps = (float)g.eps;
+  const float2 eps2 = make_float2(feps, feps);
+  float4* t1 = &stage[warp][0][(active ? h : 0) * 2 * Q2];
+  float4* t2 = &stage[warp][1][(active ? h : 0) * 2 * Q2];
+  const bool odd = j & 1, last_odd = (Q & 1) && j == Q - 1;
+  const int partner = (odd ? lane - 1 : lane + 1) & 31;
+  auto put = [&](float4* tl, const float4& v, float r0, float r1) {
+    const int k2 = j >> 1;
+    if (last_odd) {
+      tl[2 * k2] = make_float4(v.x, 0.f, v.y, 0.f);
+      tl[2 * k2 + 1] = make_float4(v.z, 0.f, v.w, 0.f);
+    } else if (!odd) {
+      tl[2 * k2] = make_float4(v.x, r0, v.y, r1);
+    } else {
+      tl[2 * k2 + 1] = make_float4(r0, v.z, r1, v.w);
+    }
+  };
+  for (int eb = e0; eb < e1; eb += 32) {
+    const int nb = min(32, e1 - eb);
+    int4 en = make_int4(0, 0, 0, 0);
+    if (lane < nb) en = __ldg(g.entry + eb + lane);
+    const int iters = (nb + W::S - 1) / W::S;
+    float cbx = __int_as_float(__shfl_sync(full, en.y, h & 31));
+    float cby = __int_as_float(__shfl_sync(full, en.z, h & 31));
+    float cbz = __int_as_float(__shfl_sync(full, en.w, h & 31));
+    float4 v1 = make_float4(0.f, 0.f, 0.f, 0.f), v2 = v1;
+    {
+      const int sp = __shfl_sync(full, en.x, h & 31);
+      if (active && h < nb) {
+        v1 = g.srcf[(long)sp * Q + j];
+        v2 = sw.srcf2[(long)sp * Q + j];
+      }
+    }
+    for (int it = 0; it < iters; it++) {
+      const bool on = active && it * W::S + h < nb;
+      const int ns = (it + 1) * W::S + h;
+      const int sp_n = __shfl_sync(full, en.x, ns & 31);
+      const float nbx = __int_as_float(__shfl_sync(full, en.y, ns & 31));
+      const float nby = __int_as_float(__shfl_sync(full, en.z, ns & 31));
+      const float nbz = __int_as_float(__shfl_sync(full, en.w, ns & 31));
+      float4 n1 = make_float4(0.f, 0.f, 0.f, 0.f), n2 = n1;
+      if (active && ns < nb) {
+        n1 = g.srcf[(long)sp_n * Q + j];
+        n2 = sw.srcf2[(long)sp_n * Q + j];
+      }
+      const float p0 = __shfl_sync(full, odd ? v1.x : v1.z, partner);
+      const float p1 = __shfl_sync(full, odd ? v1.y : v1.w, partner);
+      const float q0 = __shfl_sync(full, odd ? v2.x : v2.z, partner);
+      const float q1 = __shfl_sync(full, odd ? v2.y : v2.w, partner);
+      if (on) {
+        put(t1, v1, p0, p1);
+        put(t2, v2, q0, q1);
+      }
+      __syncwarp();
+      if (on) {
+        const float b0 = cbx - dtx, b1 = cby - dty, b2 = cbz - dtz;
+        const float2 px2 = make_float2(b0, b0), py2 = make_float2(b1, b1), pz2 = make_float2(b2, b2);
+        float2 fax = make_float2(0.f, 0.f), fay = fax, faz = fax, fbx = fax, fby = fax, fbz = fax;
+#pragma unroll
+        for (int k2 = 0; k2 < Q2; k2++) {
+          const float4 A = t1[2 * k2], B = t1[2 * k2 + 1], C = t2[2 * k2], D = t2[2 * k2 + 1];
+          pair32x2<GUARD>(px2, py2, pz2, make_float2(A.x, A.y), make_float2(A.z, A.w), make_float2(B.x, B.y),
+                          make_float2(B.z, B.w), eps2, fax, fay, faz);
+          pair32x2<GUARD>(px2, py2, pz2, make_float2(C.x, C.y), make_float2(C.z, C.w), make_float2(D.x, D.y),
+                          make_float2(D.z, D.w), eps2, fbx, fby, fbz);
+        }
+        ax += (double)(fax.x + fax.y);
+        ay += (double)(fay.x + fay.y);
+        az += (double)(faz.x + faz.y);
+        bx += (double)(fbx.x + fbx.y);
+        by += (double)(fby.x + fby.y);
+        bz += (double)(fbz.x + fbz.y);
+      }
+      __syncwarp();
+      v1 = n1;
+      v2 = n2;
+      cbx = nbx;
+      cby = nby;
+      cbz = nbz;
+    }
+  }
+  if (W::S > 1) {
+    red[warp][0][lane] = ax;
+    red[warp][1][lane] = ay;
+    red[warp][2][lane] = az;
+    red[warp][3][lane] = bx;
+    red[warp][4][lane] = by;
+    red[warp][5][lane] = bz;
+    __syncwarp();
+    if (h == 0)
+      for (int hh = 1; hh < W::S; hh++) {
+        const int l = hh * Q + j;
+        ax += red[warp][0][l];
+        ay += red[warp][1][l];
+        az += red[warp][2][l];
+        bx += red[warp][3][l];
+        by += red[warp][4][l];
+        bz += red[warp][5][l];
+      }
+  }
+  if (h != 0) return;
+  double ux, uy, uz;
+  swe_epilogue(kBiotSavartPacked, tx, ty, tz, ax, ay, az, bx, by, bz, ux, uy, uz);
+  const long o = (long)t * Q + j;
+  out[o] = ux;
+  out[pn + o] = uy;
+  out[2 * pn + o] = uz;
+}
+
 __global__ void k_swe_reduce(const double* __restrict__ partial, int groups, long n, long gstride,
                              double* __restrict__ out) {
   const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
@@ -401,6 +547,12 @@ void swe_interact_qg(const StepGeom& g, const SweGeom& s, int precision, const d
     if (mixed) SB_SWE_K(true, true);
     else SB_SWE_K(true, false);
   } else {
+    if constexpr (Q <= 32) {
+      if (mixed && g.entry) {
+        SB_LAUNCH((k_swe_interact32_list<Q, GUARD>), grid, 32 * kWarps, 0, st, g, s, out);
+        return;
+      }
+    }
     if (mixed) SB_SWE_K(false, true);
     else SB_SWE_K(false, false);
   }
