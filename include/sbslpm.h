@@ -169,11 +169,25 @@ long sbslpm_kernel_launches(void);
  * src/bve_time_step.hpp:7-13).  Device pointers: xcos, ycos, zcos, area are
  * [leaf][q]; vors is advanced in place; vel_x/y/z receive the stage-0
  * velocity (the reference's vel_x/y/z); tracers [leaf][q][tracer_count] are
- * remapped in place (may be NULL when tracer_count is 0).  time is accepted
- * for interface parity (forcing is off, so it is unused). */
+ * remapped in place (may be NULL when tracer_count is 0).  time is the
+ * step's time in seconds (read by the forcing, unused without it). */
 sbslpm_status sbslpm_bve_step(sbslpm_ctx* ctx, const double* xcos, const double* ycos, const double* zcos,
                               const double* area, double* vors, double* vel_x, double* vel_y, double* vel_z,
                               double* tracers, double time);
+/* The same step on HOST arrays (the layout and meaning of sbslpm_bve_step's
+ * arguments; pinned host memory gives the fastest copies, pageable memory
+ * works).  The inputs are copied to device buffers the context allocates on
+ * first use; the stage-0 velocity is copied back on a second stream while
+ * stages 1-3 run, and vors / tracers after the remap.  Returns when every
+ * output is in host memory.  The reference's bve_back_rk4_step on Kokkos
+ * HostSpace Views (its OpenMP build) maps onto this call. */
+sbslpm_status sbslpm_bve_step_host(sbslpm_ctx* ctx, const double* xcos, const double* ycos, const double* zcos,
+                                   const double* area, double* vors, double* vel_x, double* vel_y, double* vel_z,
+                                   double* tracers, double time);
+/* 1 when p is memory the device can address as a device pointer
+ * (cudaMalloc'd, managed, or a CUDA tensor's storage), 0 for host memory
+ * (pageable or pinned), -1 when the query fails. */
+int sbslpm_pointer_on_device(const void* p);
 /* nsteps consecutive steps, captured once as a CUDA graph and replayed. */
 sbslpm_status sbslpm_bve_run(sbslpm_ctx* ctx, const double* xcos, const double* ycos, const double* zcos,
                              const double* area, double* vors, double* vel_x, double* vel_y, double* vel_z,

@@ -10,8 +10,10 @@
 //                     passive_tracers, time);
 // (reference: src/bve_time_step.hpp:7-13, called from
 // executables/bve_time_evo.cpp:305) switches by including this header and
-// `using sbslpm_kokkos::bve_back_rk4_step;`.  The Views must live in device
-// memory (CudaSpace / CudaUVMSpace) with LayoutRight.
+// `using sbslpm_kokkos::bve_back_rk4_step;`.  The Views are LayoutRight, in
+// device memory (CudaSpace / CudaUVMSpace) or, for bve_back_rk4_step, in host
+// memory (HostSpace: the reference's OpenMP build), where the step copies
+// through sbslpm_bve_step_host; all Views of one call in the same space.
 //
 // The panel table, interaction list and interpolation table the reference
 // passes are rebuilt inside the library from run_config (they are functions
@@ -79,9 +81,14 @@ void bve_back_rk4_step(const RunConfig& run_config, V2& xcos, V2& ycos, V2& zcos
       (long)xcos.extent(1) != sizes[2] || (long)interp_vals.extent(0) != sizes[2])
     throw std::runtime_error("bve_back_rk4_step: view sizes do not match run_config");
   double* tr = run_config.tracer_count > 0 ? passive_tracers.data() : nullptr;
-  check(sbslpm_bve_step(c, xcos.data(), ycos.data(), zcos.data(), area.data(), vors.data(), vel_x.data(),
-                        vel_y.data(), vel_z.data(), tr, time),
-        "sbslpm_bve_step");
+  if (sbslpm_pointer_on_device(vors.data()) == 0)
+    check(sbslpm_bve_step_host(c, xcos.data(), ycos.data(), zcos.data(), area.data(), vors.data(), vel_x.data(),
+                               vel_y.data(), vel_z.data(), tr, time),
+          "sbslpm_bve_step_host");
+  else
+    check(sbslpm_bve_step(c, xcos.data(), ycos.data(), zcos.data(), area.data(), vors.data(), vel_x.data(),
+                          vel_y.data(), vel_z.data(), tr, time),
+          "sbslpm_bve_step");
 }
 
 // swe_back_rk4_step_2 (src/swe_time_step_2.cpp:785-1035; declared in

@@ -109,6 +109,9 @@ def lib() -> ctypes.CDLL:
                  "sbslpm_get_interactions"):
         getattr(L, name).argtypes = None
     L.sbslpm_bve_step.argtypes = [_VP] + [_VP] * 9 + [ctypes.c_double]
+    L.sbslpm_bve_step_host.argtypes = [_VP] + [_VP] * 9 + [ctypes.c_double]
+    L.sbslpm_pointer_on_device.argtypes = [_VP]
+    L.sbslpm_pointer_on_device.restype = ctypes.c_int
     L.sbslpm_bve_run.argtypes = [_VP] + [_VP] * 9 + [ctypes.c_double, ctypes.c_int]
     L.sbslpm_upward_pass.argtypes = [_VP] * 4
     L.sbslpm_bve_vel_interactions.argtypes = [_VP] * 8
@@ -303,6 +306,33 @@ def _dev(t, name, shape=None):
     return t.data_ptr()
 
 
+def _host(a, name, shape=None, write=False):
+    """Host pointer of a C-contiguous float64 numpy array or CPU torch tensor
+    (pinned or pageable; None -> NULL)."""
+    if a is None:
+        return None
+    if hasattr(a, "is_cuda"):
+        import torch
+
+        if a.is_cuda or a.dtype != torch.float64 or not a.is_contiguous():
+            raise TypeError(f"{name} must be a contiguous float64 host tensor")
+        n, ptr = a.numel(), a.data_ptr()
+    else:
+        if not isinstance(a, np.ndarray) or a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"]:
+            raise TypeError(f"{name} must be a C-contiguous float64 numpy array")
+        if write and not a.flags["WRITEABLE"]:
+            raise ValueError(f"{name} is read-only")
+        n, ptr = a.size, a.ctypes.data
+    if shape is not None and n != int(np.prod(shape)):
+        raise ValueError(f"{name} has {n} elements, expected {shape}")
+    return ptr
+
+
+def pointer_on_device(p) -> int:
+    """sbslpm_pointer_on_device: 1 device memory, 0 host memory, -1 unknown."""
+    return int(lib().sbslpm_pointer_on_device(ctypes.c_void_p(p)))
+
+
 def _stream():
     import torch
 
@@ -405,6 +435,17 @@ class Context:
         _check(lib().sbslpm_bve_step(self._h, *[_dev(t, n, lq) for t, n in (
             (xcos, "xcos"), (ycos, "ycos"), (zcos, "zcos"), (area, "area"), (vors, "vors"), (vel_x, "vel_x"),
             (vel_y, "vel_y"), (vel_z, "vel_z"))], _dev(tracers, "tracers"), float(time)), "sbslpm_bve_step")
+
+    def bve_back_rk4_step_host(self, xcos, ycos, zcos, area, vors, vel_x, vel_y, vel_z, tracers=None, time=0.0):
+        """The step on host arrays (numpy or CPU torch, float64, C order):
+        vors, vel_*, tracers in place (sbslpm_bve_step_host)."""
+        lq = (self.leaf_count, self.q)
+        self._sync_stream()
+        ptrs = [_host(a, n, lq, w) for a, n, w in (
+            (xcos, "xcos", False), (ycos, "ycos", False), (zcos, "zcos", False), (area, "area", False),
+            (vors, "vors", True), (vel_x, "vel_x", True), (vel_y, "vel_y", True), (vel_z, "vel_z", True))]
+        tr = _host(tracers, "tracers", lq + (self.cfg.tracer_count,), True) if tracers is not None else None
+        _check(lib().sbslpm_bve_step_host(self._h, *ptrs, tr, float(time)), "sbslpm_bve_step_host")
 
     def bve_run(self, xcos, ycos, zcos, area, vors, vel_x, vel_y, vel_z, tracers=None, time=0.0, nsteps=1):
         """nsteps steps replayed from one captured CUDA graph."""

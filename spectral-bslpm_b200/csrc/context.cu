@@ -348,8 +348,10 @@ void velocity_eval(sbslpm_ctx* c, int stage, double dt_s, const double* vprev, c
 }
 
 // The work of one bve_back_rk4_step (src/bve_time_step.cpp:311-419), enqueued on the stream.
+// vel_x == nullptr: the stage-0 velocity stays in vbuf (its first 3 x
+// leaves*q values); stage0, when given, is recorded once it is complete.
 void enqueue_step(sbslpm_ctx* c, const double* x, const double* y, const double* z, const double* area, double* vors,
-                  double* vel_x, double* vel_y, double* vel_z, double* tracers) {
+                  double* vel_x, double* vel_y, double* vel_z, double* tracers, cudaEvent_t stage0) {
   cudaStream_t st = c->stream();
   const size_t ln = (size_t)c->A * c->q;
   const double dt = c->cfg.dt;
@@ -358,16 +360,21 @@ void enqueue_step(sbslpm_ctx* c, const double* x, const double* y, const double*
   const double stage_dt[4] = {0.0, 0.5 * dt, 0.5 * dt, dt};
   // bve_forcing at the step's time, the same for all four stages (src/bve_time_step.cpp:323-395)
   if (c->force) launch_ssw_forcing(c->A, c->q, c->cfg.forcing, c->cfg.omega, c->d_time, x, y, z, c->force, st);
-  for (int s = 0; s < 4; s++) velocity_eval(c, s, stage_dt[s], s ? v[s - 1] : nullptr, x, y, z, area, vors, v[s]);
+  for (int s = 0; s < 4; s++) {
+    velocity_eval(c, s, stage_dt[s], s ? v[s - 1] : nullptr, x, y, z, area, vors, v[s]);
+    if (s == 0 && stage0) cudaEventRecord(stage0, st);
+  }
   if (c->force) launch_time_advance(c->d_time, dt, st);
   const int T = c->cfg.tracer_count;
   launch_depart_remap(c->geom, &c->tab, x, y, z, v[0], v[1], v[2], v[3], dt, c->dep, vors, tracers, T, c->newvor,
                       c->newtr, 3, st);
   cudaMemcpyAsync(vors, c->newvor, sizeof(double) * ln, cudaMemcpyDeviceToDevice, st);
   if (T > 0) cudaMemcpyAsync(tracers, c->newtr, sizeof(double) * ln * T, cudaMemcpyDeviceToDevice, st);
-  cudaMemcpyAsync(vel_x, v[0], sizeof(double) * ln, cudaMemcpyDeviceToDevice, st);
-  cudaMemcpyAsync(vel_y, v[0] + ln, sizeof(double) * ln, cudaMemcpyDeviceToDevice, st);
-  cudaMemcpyAsync(vel_z, v[0] + 2 * ln, sizeof(double) * ln, cudaMemcpyDeviceToDevice, st);
+  if (vel_x) {
+    cudaMemcpyAsync(vel_x, v[0], sizeof(double) * ln, cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(vel_y, v[0] + ln, sizeof(double) * ln, cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(vel_z, v[0] + 2 * ln, sizeof(double) * ln, cudaMemcpyDeviceToDevice, st);
+  }
 }
 
 // Waits for the stream, then turns launch errors and the device error word
@@ -704,6 +711,10 @@ sbslpm_status sbslpm_destroy(sbslpm_ctx* c) {
   }
   if (c->h_err) cudaFreeHost(c->h_err);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
+  if (c->hio) cudaFree(c->hio);
+  if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+  if (c->ev_stage0) cudaEventDestroy(c->ev_stage0);
+  if (c->ev_copied) cudaEventDestroy(c->ev_copied);
   delete c;
   return SBSLPM_OK;
 }
@@ -747,6 +758,52 @@ sbslpm_status sbslpm_bve_step(sbslpm_ctx* c, const double* x, const double* y, c
   if (c->force) SB_CUDA(cudaMemcpyAsync(c->d_time, &time, sizeof(double), cudaMemcpyHostToDevice, c->stream()));
   enqueue_step(c, x, y, z, area, vors, vel_x, vel_y, vel_z, tracers);
   return finish(c);
+}
+
+sbslpm_status sbslpm_bve_step_host(sbslpm_ctx* c, const double* x, const double* y, const double* z,
+                                   const double* area, double* vors, double* vel_x, double* vel_y, double* vel_z,
+                                   double* tracers, double time) {
+  if (!c || bad(x) || bad(y) || bad(z) || bad(area) || bad(vors) || bad(vel_x) || bad(vel_y) || bad(vel_z) ||
+      (c->cfg.tracer_count > 0 && bad(tracers)) || !std::isfinite(time))
+    return SBSLPM_ERR_ARG;
+  const int T = c->cfg.tracer_count;
+  const size_t ln = (size_t)c->A * c->q, bytes = sizeof(double) * ln;
+  if (!c->hio) {
+    SB_TRY(dalloc(&c->hio, (size_t)(5 + T) * ln));
+    SB_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+    SB_CUDA(cudaEventCreateWithFlags(&c->ev_stage0, cudaEventDisableTiming));
+    SB_CUDA(cudaEventCreateWithFlags(&c->ev_copied, cudaEventDisableTiming));
+  }
+  cudaStream_t st = c->stream();
+  double* d[5];
+  for (int k = 0; k < 5; k++) d[k] = c->hio + (size_t)k * ln;
+  double* dtr = T > 0 ? c->hio + 5 * ln : nullptr;
+  const double* in[5] = {x, y, z, area, vors};
+  for (int k = 0; k < 5; k++) SB_CUDA(cudaMemcpyAsync(d[k], in[k], bytes, cudaMemcpyHostToDevice, st));
+  if (T > 0) SB_CUDA(cudaMemcpyAsync(dtr, tracers, bytes * T, cudaMemcpyHostToDevice, st));
+  SB_TRY(near_autotune(c, d[0], d[1], d[2], d[3], d[4]));
+  if (c->force) SB_CUDA(cudaMemcpyAsync(c->d_time, &time, sizeof(double), cudaMemcpyHostToDevice, st));
+  enqueue_step(c, d[0], d[1], d[2], d[3], d[4], nullptr, nullptr, nullptr, dtr, c->ev_stage0);
+  // the stage-0 velocity (vbuf's first 3 x leaves*q) leaves while stages 1-3 run
+  SB_CUDA(cudaStreamWaitEvent(c->copy_stream, c->ev_stage0, 0));
+  double* vel[3] = {vel_x, vel_y, vel_z};
+  for (int k = 0; k < 3; k++)
+    SB_CUDA(cudaMemcpyAsync(vel[k], c->vbuf + (size_t)k * ln, bytes, cudaMemcpyDeviceToHost, c->copy_stream));
+  SB_CUDA(cudaEventRecord(c->ev_copied, c->copy_stream));
+  SB_CUDA(cudaMemcpyAsync(vors, d[4], bytes, cudaMemcpyDeviceToHost, st));
+  if (T > 0) SB_CUDA(cudaMemcpyAsync(tracers, dtr, bytes * T, cudaMemcpyDeviceToHost, st));
+  SB_CUDA(cudaStreamWaitEvent(st, c->ev_copied, 0));
+  return finish(c);
+}
+
+int sbslpm_pointer_on_device(const void* p) {
+  if (!p) return -1;
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return -1;
+  }
+  return (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) ? 1 : 0;
 }
 
 sbslpm_status sbslpm_bve_run(sbslpm_ctx* c, const double* x, const double* y, const double* z, const double* area,

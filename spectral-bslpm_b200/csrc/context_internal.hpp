@@ -102,6 +102,12 @@ struct sbslpm_ctx {
   GraphKey swe_graph_key{};
   long swe_launches_per_step = 0;
 
+  // host-array step (sbslpm_bve_step_host): device copies of the inputs and
+  // outputs, a second stream for the velocity copy, allocated on first use
+  double* hio = nullptr;  // [5 + T][leaves*q]: x, y, z, area, vors, tracers
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_stage0 = nullptr, ev_copied = nullptr;
+
   // adjoint workspace, allocated on first use
   double4* adj_src = nullptr;  // [4 stages][panels*q] stage sources (positions, strengths)
   double *adj_vbar = nullptr, *adj_q = nullptr, *adj_y = nullptr, *adj_part = nullptr, *adj_w = nullptr,
@@ -140,7 +146,8 @@ sbslpm_status upload(T** p, const std::vector<T>& h) {
 
 sbslpm_status finish(sbslpm_ctx* c);
 void enqueue_step(sbslpm_ctx* c, const double* x, const double* y, const double* z, const double* area, double* vors,
-                  double* vel_x, double* vel_y, double* vel_z, double* tracers);
+                  double* vel_x, double* vel_y, double* vel_z, double* tracers,
+                  cudaEvent_t stage0 = nullptr);
 void velocity_eval(sbslpm_ctx* c, int stage, double dt_s, const double* vprev, const double* x, const double* y,
                    const double* z, const double* area, const double* vors, double* v);
 void launch_add3(const double* t, long n, double* a, double* b, double* cc, cudaStream_t st);
