@@ -330,11 +330,21 @@ void velocity_eval(sbslpm_ctx* c, int stage, double dt_s, const double* vprev, c
     const StepGeom& fg = c->fgeom;
     launch_bltc_sources(c->tgeom, fg, c->ftab, stage, dt_s, vprev, x, y, z, vors, area, c->psrc, c->psrcf, c->fsrc,
                         mixed, st);
-    launch_upward_fused(fg, 2, 0, 0.0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, c->fsrc, mixed, st);
-    launch_tree_cc(c, st);
-    launch_downward_fused(fg, c->ftgt, nullptr, st);
+    // the tree passes (proxy sources up, well-separated pairs, proxy targets
+    // down) depend only on the leaf proxies, the near field only on the
+    // particle sources: the tree runs on the auxiliary stream beside it
+    cudaStream_t tree_st = c->aux_stream ? c->aux_stream : st;
+    if (c->aux_stream) {
+      cudaEventRecord(c->ev_fork, st);
+      cudaStreamWaitEvent(tree_st, c->ev_fork, 0);
+    }
+    launch_upward_fused(fg, 2, 0, 0.0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, c->fsrc, mixed, tree_st);
+    launch_tree_cc(c, tree_st);
+    launch_downward_fused(fg, c->ftgt, nullptr, tree_st);
+    if (c->aux_stream) cudaEventRecord(c->ev_join, tree_st);
     launch_bltc_near_batch(c->self, 1, fg.leaves, c->npl, c->cfg.kernel_eps, c->cfg.precision, x, y, z, c->psrc,
                            c->psrcf, c->near, c->near_splits, c->near_nt, c->near_tpt, st);
+    if (c->aux_stream) cudaStreamWaitEvent(st, c->ev_join, 0);
     launch_bltc_to_particles(c->tgeom, fg, c->ftgt, c->near, c->near_splits, v, st);
     return;
   }
@@ -659,6 +669,14 @@ sbslpm_status sbslpm_create(const sbslpm_config* cfg, sbslpm_ctx** out) {
   if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) s = SBSLPM_ERR_CUDA;
   if (s == SBSLPM_OK) s = precompute(c);
   if (s == SBSLPM_OK && c->tree) s = precompute_tree(c);
+  if (s == SBSLPM_OK && c->tree) {
+    int least = 0, greatest = 0;
+    if (cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&c->aux_stream, cudaStreamNonBlocking, greatest) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess)
+      s = SBSLPM_ERR_CUDA;
+  }
   if (s == SBSLPM_OK) s = allocate_workspace(c);
   if (s == SBSLPM_OK && cfg->forcing != SBSLPM_FORCING_NONE) {
     s = dalloc(&c->force, (size_t)c->A * c->q);
@@ -712,6 +730,9 @@ sbslpm_status sbslpm_destroy(sbslpm_ctx* c) {
   if (c->h_err) cudaFreeHost(c->h_err);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   if (c->hio) cudaFree(c->hio);
+  if (c->aux_stream) cudaStreamDestroy(c->aux_stream);
+  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+  if (c->ev_join) cudaEventDestroy(c->ev_join);
   if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
   if (c->ev_stage0) cudaEventDestroy(c->ev_stage0);
   if (c->ev_copied) cudaEventDestroy(c->ev_copied);

@@ -79,6 +79,10 @@ struct sbslpm_ctx {
   bool cc_tuned = false;
   int cc_candidates = 0;
   double cc_tuned_ms = 0;
+  // treecode stages: the tree passes run on aux_stream (higher priority)
+  // beside the near field on the context's stream, forked and joined by events
+  cudaStream_t aux_stream = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   sbslpm::BatchMember* self = nullptr;
   double* force = nullptr;   // [leaves*q] forcing of the current step (forcing configured)
   double* d_time = nullptr;  // the step's time on the device, advanced by dt inside each step  // this context's treecode as a one-member table (shaped near-field launches)
