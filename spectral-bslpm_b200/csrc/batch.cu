@@ -27,6 +27,10 @@ struct sbslpm_batch {
   std::vector<int> degree;
   std::vector<sbslpm_panel> panels;
   cudaStream_t user_stream = nullptr, own_stream = nullptr;
+  // the members' tree passes run on aux_stream (higher priority) beside the
+  // near field, forked and joined by events
+  cudaStream_t aux_stream = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   bool user_stream_set = false;
   BliTable tab{};
   StepGeom g{};  // the particle grid (departure search and remap)
@@ -331,19 +335,28 @@ void batch_velocity(sbslpm_batch* b, int stage, double dt_s, const double* vprev
   const bool mixed = prec == SBSLPM_MIXED;
   launch_bltc_sources_batch(b->d_mem, b->M, b->Af, b->npl, b->nmax, stage, dt_s, vprev, x, y, z, vors, area, b->psrc,
                             b->psrcf, mixed, st);
-  launch_upward_batch(b->d_mem, b->M, b->Lf, b->qmax, mixed, st);
+  // the tree passes need only the leaf proxies, the near field only the
+  // particle sources: the tree runs on the auxiliary stream beside it
+  cudaStream_t tree_st = b->aux_stream ? b->aux_stream : st;
+  if (b->aux_stream) {
+    cudaEventRecord(b->ev_fork, st);
+    cudaStreamWaitEvent(tree_st, b->ev_fork, 0);
+  }
+  launch_upward_batch(b->d_mem, b->M, b->Lf, b->qmax, mixed, tree_st);
   for (const auto& D : b->degs) {
     const int mode = mixed ? (b->cc_mode < 0 ? D.cc_auto : b->cc_mode) : 0;
     if (mode != 0) {
-      launch_cc_tc_pack(D.tc, st);
-      launch_cc_tc(D.tc, mode == 1 ? 3 : 1, st);
+      launch_cc_tc_pack(D.tc, tree_st);
+      launch_cc_tc(D.tc, mode == 1 ? 3 : 1, tree_st);
     } else {
-      launch_cc_batch(b->d_mem, D.d_idx, (int)D.members.size(), D.qx, b->Pf, b->cfg.kernel_eps, prec, st);
+      launch_cc_batch(b->d_mem, D.d_idx, (int)D.members.size(), D.qx, b->Pf, b->cfg.kernel_eps, prec, tree_st);
     }
   }
-  launch_downward_batch(b->d_mem, b->M, b->Lf, b->qmax, st);
+  launch_downward_batch(b->d_mem, b->M, b->Lf, b->qmax, tree_st);
+  if (b->aux_stream) cudaEventRecord(b->ev_join, tree_st);
   launch_bltc_near_batch(b->d_mem, b->M, b->Af, b->npl, b->cfg.kernel_eps, prec, x, y, z, b->psrc, b->psrcf, b->near,
                          b->splits, b->nt, b->tpt, st);
+  if (b->aux_stream) cudaStreamWaitEvent(st, b->ev_join, 0);
   launch_bltc_to_particles_batch(b->d_mem, b->M, b->Af, b->nmax, b->near, b->splits, v, st);
 }
 
@@ -446,6 +459,9 @@ sbslpm_status sbslpm_batch_destroy(sbslpm_batch* b) {
   for (void* p : b->bufs) cudaFree(p);
   if (b->h_err) cudaFreeHost(b->h_err);
   if (b->own_stream) cudaStreamDestroy(b->own_stream);
+  if (b->aux_stream) cudaStreamDestroy(b->aux_stream);
+  if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+  if (b->ev_join) cudaEventDestroy(b->ev_join);
   delete b;
   return SBSLPM_OK;
 }
@@ -488,6 +504,15 @@ sbslpm_status sbslpm_batch_create(const sbslpm_config* base, int members, const 
   b->degree.assign(proxy_degree, proxy_degree + members);
   sbslpm_status s = SBSLPM_OK;
   if (cudaStreamCreateWithFlags(&b->own_stream, cudaStreamNonBlocking) != cudaSuccess) s = SBSLPM_ERR_CUDA;
+  {
+    int least = 0, greatest = 0;
+    if (s == SBSLPM_OK &&
+        (cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess ||
+         cudaStreamCreateWithPriority(&b->aux_stream, cudaStreamNonBlocking, greatest) != cudaSuccess ||
+         cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+         cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming) != cudaSuccess))
+      s = SBSLPM_ERR_CUDA;
+  }
   if (s == SBSLPM_OK) s = batch_setup(b);
   if (s != SBSLPM_OK) {
     sbslpm_batch_destroy(b);
