@@ -151,7 +151,11 @@ int sbslpm_point_locate_panel(const sbslpm_panel* panels, double x, double y, do
 sbslpm_status sbslpm_create(const sbslpm_config* cfg, sbslpm_ctx** out);
 sbslpm_status sbslpm_destroy(sbslpm_ctx* ctx);
 /* Orders all later work of ctx on this cudaStream_t (NULL = the legacy
- * default stream).  Until it is called, ctx uses a stream of its own. */
+ * default stream).  Until it is called, ctx uses a stream of its own.
+ * Treecode contexts also run each stage's tree passes on a second stream of
+ * their own, forked from and joined back to this one by events, so every
+ * call's work still starts after, and ends before, the work this stream
+ * holds around it. */
 sbslpm_status sbslpm_set_stream(sbslpm_ctx* ctx, void* cuda_stream);
 /* sizes[0..3] = panel_count, leaf_count, q, interaction_count */
 sbslpm_status sbslpm_get_sizes(const sbslpm_ctx* ctx, long* sizes);
