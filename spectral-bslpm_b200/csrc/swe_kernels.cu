@@ -60,7 +60,8 @@ __device__ __forceinline__ float4 pack(const double* c, double x, double y, doub
 // src/swe_time_step_2.cpp:436-476, identical to the BVE form), both strengths
 // anterpolated level by level (upward_pass, src/fmm_funcs.cpp:341-355), and
 // the packed float sources in mixed precision.
-__global__ void k_swe_upward_subtree(StepGeom g, SweGeom sw, int r, int D, int stage, double dtd, double dts,
+__global__ void k_swe_upward_subtree(StepGeom g, SweGeom sw, int r, int D, int positions, int stage, double dtd,
+                                     double dts,
                                      const double* __restrict__ vprev, const double* __restrict__ tprev,
                                      const double* __restrict__ vors, const double* __restrict__ divs,
                                      const double* __restrict__ area, double4* __restrict__ src,
@@ -99,7 +100,7 @@ __global__ void k_swe_upward_subtree(StepGeom g, SweGeom sw, int r, int D, int s
       lvl(1, D)[t] = wd;
     }
   }
-  for (int k = 0; k < D; k++) {
+  for (int k = 0; positions && k < D; k++) {  // else k_swe_nonleaf_positions wrote them
     const int first = subtree_first(r, root_rel, k), npts = (1 << (2 * k)) * q;
     for (int t = threadIdx.x; t < npts; t += blockDim.x) {
       const long i = (long)first * q + t;
@@ -150,6 +151,39 @@ __global__ void k_swe_upward_subtree(StepGeom g, SweGeom sw, int r, int D, int s
       }
     }
   }
+}
+
+// Positions of every non-leaf proxy of both fields in one flat launch ahead
+// of the subtree passes, a thread per point: the vorticity sources displaced
+// by the interpolated leaf velocity (nonleaf_position's arithmetic, q = 16
+// unrolled), the divergence sources at the fixed proxies.
+template <int Q>
+__global__ void k_swe_nonleaf_positions(StepGeom g, int stage, double dtd, const double* __restrict__ vprev,
+                                        double4* __restrict__ src, double4* __restrict__ src2) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const int q = Q > 0 ? Q : g.q;
+  if (i >= (long)g.offset * q) return;
+  const long pn = (long)g.panels * q, ln = (long)g.leaves * q;
+  const double x0 = g.px[i], y0 = g.px[pn + i], z0 = g.px[2 * pn + i];
+  double px = x0, py = y0, pz = z0;
+  if (stage > 0) {
+    const long np = (long)g.offset * q;
+    const long row = (long)g.il_row[i] * q;
+    double ax = 0, ay = 0, az = 0;
+#pragma unroll
+    for (int m = 0; m < (Q > 0 ? Q : q); m++) {
+      const double bm = g.il_basis[m * np + i];
+      ax += (dtd * vprev[row + m]) * bm;
+      ay += (dtd * vprev[ln + row + m]) * bm;
+      az += (dtd * vprev[2 * ln + row + m]) * bm;
+    }
+    px += ax;
+    py += ay;
+    pz += az;
+  }
+  project_to_sphere(px, py, pz);
+  src[i] = make_double4(px, py, pz, 0.0);
+  src2[i] = make_double4(x0, y0, z0, 0.0);
 }
 
 // Direct velocity: leaf sources of both fields (no tree).
@@ -590,11 +624,18 @@ void launch_swe_upward(const StepGeom& g, const SweGeom& s, int stage, double dt
   }
   const int Dmax = g.q <= 25 ? 3 : 1;
   int r = g.levels - 1;
+  const long nl = (long)g.offset * g.q;  // non-leaf proxy points
+  if (nl > 0) {
+    if (g.q == 16)
+      SB_LAUNCH(k_swe_nonleaf_positions<16>, blocks_for(nl, 256), 256, 0, st, g, stage, dtd, vprev, src, src2);
+    else
+      SB_LAUNCH(k_swe_nonleaf_positions<0>, blocks_for(nl, 256), 256, 0, st, g, stage, dtd, vprev, src, src2);
+  }
   do {
     const int D = r < Dmax ? r : Dmax;
     const int root = r - D;
     SB_LAUNCH(k_swe_upward_subtree, (unsigned)(6 << (2 * root)), 256, swe_subtree_smem(g.q, D), st, g, s, root, D,
-              stage, dtd, dts, vprev, tprev, vors, divs, area, src, src2, mixed ? 1 : 0);
+              nl > 0 ? 0 : 1, stage, dtd, dts, vprev, tprev, vors, divs, area, src, src2, mixed ? 1 : 0);
     r = root;
   } while (r > 0);
 }
