@@ -107,11 +107,23 @@ __device__ __forceinline__ void bltc_sources_body(const TreeGeom& tg, const Step
     sw[k] = w;
   }
   __syncthreads();
-  const int qx = n1 * n1;
-  for (int m = threadIdx.x; m < qx; m += blockDim.x) {
-    const int a = m / n1, b = m % n1;
+  // proxy strengths S[a][b] = sum_k lx[k][a] ly[k][b] w_k: the particles are
+  // cut into G contiguous groups (G = threads / q), one thread per (group,
+  // proxy), and the G partial sums are added in group order
+  const int qx = n1 * n1, G = blockDim.x / qx > 0 ? blockDim.x / qx : 1;
+  double* part = sw + npl;  // [G][qx]
+  const int per = (npl + G - 1) / G;
+  for (int t = threadIdx.x; t < G * qx; t += blockDim.x) {
+    const int gi = t / qx, m = t - gi * qx, a = m / n1, b = m % n1;
+    const int k0 = gi * per, k1 = min(npl, k0 + per);
     double acc = 0;
-    for (int k = 0; k < npl; k++) acc = fma(lx[k * n1 + a] * ly[k * n1 + b], sw[k], acc);
+    for (int k = k0; k < k1; k++) acc = fma(lx[k * n1 + a] * ly[k * n1 + b], sw[k], acc);
+    part[t] = acc;
+  }
+  __syncthreads();
+  for (int m = threadIdx.x; m < qx; m += blockDim.x) {
+    double acc = part[m];
+    for (int gi = 1; gi < G; gi++) acc += part[gi * qx + m];
     proxy[(long)panel * qx + m].w = acc;
   }
 }
@@ -320,14 +332,20 @@ __device__ __forceinline__ void bltc_to_particles_body(const TreeGeom& tg, const
   for (int k = threadIdx.x; k < npl; k += blockDim.x) {
     const double* lxk = tg.lx + k * n1;
     const double* lyk = tg.ly + k * n1;
+    // the particle's eta basis in registers (n1 <= kMaxDegree + 1), read once
+    double lb[kMaxDegree + 1];
+#pragma unroll
+    for (int b = 0; b <= kMaxDegree; b++) lb[b] = b < n1 ? __ldg(lyk + b) : 0.0;
     double u0 = 0, u1 = 0, u2 = 0;
     for (int a = 0; a < n1; a++) {
       double s0 = 0, s1 = 0, s2 = 0;
-      for (int b = 0; b < n1; b++) {
-        double lb = __ldg(lyk + b);
-        s0 = fma(lb, tsh[a * n1 + b], s0);
-        s1 = fma(lb, tsh[qx + a * n1 + b], s1);
-        s2 = fma(lb, tsh[2 * qx + a * n1 + b], s2);
+#pragma unroll
+      for (int b = 0; b <= kMaxDegree; b++) {
+        if (b < n1) {
+          s0 = fma(lb[b], tsh[a * n1 + b], s0);
+          s1 = fma(lb[b], tsh[qx + a * n1 + b], s1);
+          s2 = fma(lb[b], tsh[2 * qx + a * n1 + b], s2);
+        }
       }
       double la = __ldg(lxk + a);
       u0 = fma(la, s0, u0);
@@ -372,7 +390,7 @@ void launch_bltc_sources(const TreeGeom& tg, const StepGeom& fg, const BliTable&
                          const double* vprev, const double* x, const double* y, const double* z, const double* vors,
                          const double* area, double4* psrc, float4* psrcf, double4* proxy, bool mixed,
                          cudaStream_t st) {
-  size_t smem = sizeof(double) * ((size_t)tg.npl * (tg.n + 1) * 2 + tg.npl);
+  size_t smem = sizeof(double) * ((size_t)tg.npl * (tg.n + 1) * 2 + tg.npl + kThreads);
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(k_bltc_sources, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
@@ -386,7 +404,7 @@ void launch_bltc_sources_batch(const BatchMember* mem, int members, int leaves, 
                                double dt_s, const double* vprev, const double* x, const double* y, const double* z,
                                const double* vors, const double* area, double4* psrc, float4* psrcf, bool mixed,
                                cudaStream_t st) {
-  size_t smem = sizeof(double) * ((size_t)npl * (nmax + 1) * 2 + npl);
+  size_t smem = sizeof(double) * ((size_t)npl * (nmax + 1) * 2 + npl + kThreads);
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(k_bltc_sources_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
