@@ -243,6 +243,39 @@ def test_mixed_matches_fp64_levels6(sb):
     assert rel(f32["vors"], f64["vors"]) <= MIXED_TOL
 
 
+@pytest.mark.parametrize("degree", [1, 2, 4])
+def test_mixed_list_kernel_other_degrees(sb, degree):
+    """The reference's FMM at interp degrees 1, 2 and 4 (4, 9 and 25 proxies:
+    the mixed list kernel's pair staging with even and odd proxy counts, the
+    odd one padded by a zero-strength partner): within 1e-6 of float64."""
+    g = sb.build_grid(5, degree, exact_cc=True)
+    vor = unit_sphere_rh4(g)
+    out = {}
+    for prec in (sb.FP64, sb.MIXED):
+        cfg = sb.config_default(levels=5, interp_degree=degree, fmm_theta=0.7, kernel_eps=1e-4, omega=2 * np.pi,
+                                dt=0.005, precision=prec)
+        f = unit_fields(g, vor)
+        step(sb.Context(cfg), f, 2)
+        out[prec] = f
+    assert rel(torch.stack(out[sb.MIXED]["vel"]), torch.stack(out[sb.FP64]["vel"])) <= MIXED_TOL
+    assert rel(out[sb.MIXED]["vors"], out[sb.FP64]["vors"]) <= MIXED_TOL
+
+
+@pytest.mark.parametrize("n", [2, 3, 4])
+def test_treecode_mixed_low_proxy_degrees(sb, n):
+    """Treecode proxies of degree 2, 3, 4 (9, 16, 25 per panel) run the
+    well-separated list through the q <= 32 mixed list kernels (entry table
+    of the tree's list): within 1e-6 of the float64 treecode of the same
+    degree."""
+    g = sb.build_grid(5, 3, exact_cc=True)
+    vor = unit_sphere_rh4(g)
+    f64, f32 = unit_fields(g, vor), unit_fields(g, vor)
+    step(tree_ctx(sb, 5, n, leaf=64), f64)
+    step(tree_ctx(sb, 5, n, precision=sb.MIXED, leaf=64), f32)
+    assert rel(torch.stack(f32["vel"]), torch.stack(f64["vel"])) <= MIXED_TOL
+    assert rel(f32["vors"], f64["vors"]) <= MIXED_TOL
+
+
 def test_direct_mode_matches_oracle_levels4(sb, port):
     g = sb.build_grid(4, 3, exact_cc=True)
     vor = unit_sphere_rh4(g)

@@ -185,18 +185,18 @@ def test_swe_graph_replay_equals_steps(sb):
         assert torch.equal(getattr(a, k), getattr(b, k)), k
 
 
-def unit_sphere_state(sb, levels, precision, dt=0.002, seed=7):
+def unit_sphere_state(sb, levels, precision, dt=0.002, seed=7, degree=3):
     """The steady geostrophic flow on the unit sphere (Omega = 2 pi, u0 = 2 pi/12,
     g h = 2.94 - (Omega u0 + u0^2/2) sin^2 lat, height holding g h, g/a = 1)
     with seeded N(0, 1e-4^2) noise on the height."""
-    g = sb.build_grid(levels, 3, exact_cc=True)
+    g = sb.build_grid(levels, degree, exact_cc=True)
     om, u0 = 2 * np.pi, 2 * np.pi / 12
     lat = np.arcsin(np.clip(g.z, -1, 1))
     vors = 2 * u0 * np.sin(lat)
     divs = np.zeros_like(vors)
     rng = np.random.default_rng(seed)
     height = 2.94 - (om * u0 + 0.5 * u0 * u0) * np.sin(lat) ** 2 + 1e-4 * rng.standard_normal(vors.shape)
-    cfg = sb.config_default(levels=levels, interp_degree=3, fmm_theta=0.7, kernel_eps=1e-4, omega=om, dt=dt,
+    cfg = sb.config_default(levels=levels, interp_degree=degree, fmm_theta=0.7, kernel_eps=1e-4, omega=om, dt=dt,
                             precision=precision, g_over_a=1.0)
     ctx = sb.Context(cfg)
     gd = dict(x=g.x, y=g.y, z=g.z, area=g.area, vors=vors, divs=divs, height=height,
@@ -211,6 +211,18 @@ def test_swe_mixed_close_to_fp64(sb):
     c32, s32 = unit_sphere_state(sb, 5, sb.MIXED)
     c64.swe_run(*s64.args(), nsteps=5)
     c32.swe_run(*s32.args(), nsteps=5)
+    assert rel(s32.vors, s64.vors) <= MIXED_TOL
+    assert rel(s32.height, s64.height) <= MIXED_TOL
+
+
+@pytest.mark.parametrize("degree", [2, 4])
+def test_swe_mixed_close_to_fp64_other_degrees(sb, degree):
+    """9 and 25 proxies per panel (odd counts) through the mixed two-field list
+    kernel: within 1e-6 of float64 after 3 steps."""
+    c64, s64 = unit_sphere_state(sb, 5, sb.FP64, degree=degree)
+    c32, s32 = unit_sphere_state(sb, 5, sb.MIXED, degree=degree)
+    c64.swe_run(*s64.args(), nsteps=3)
+    c32.swe_run(*s32.args(), nsteps=3)
     assert rel(s32.vors, s64.vors) <= MIXED_TOL
     assert rel(s32.height, s64.height) <= MIXED_TOL
 
