@@ -540,6 +540,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-step50", action="store_true",
+                    help="skip the 50-step accuracy check against the float64 direct sum (about 35 s)")
     ap.add_argument("--no-swe", action="store_true", help="skip the shallow-water measurement")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble measurement")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint measurement")
@@ -651,6 +653,45 @@ def main():
         acc[name] = {"rel_linf_vort": (fa[4] - ref).abs().max().item() / scale,
                      "rel_linf_vel": (torch.stack(fa[5:8]) - vel_ref).abs().max().item() / vscale}
     del ctxd
+
+    # ---- accuracy after 50 steps vs the float64 direct sum (every rank: replicas) ----
+    acc50 = None
+    if not args.no_step50:
+        ctxd = ctx_for(sb.FP64, sb.VEL_DIRECT, proxy=0)
+        fd = fields()
+        ctxd.bve_run(*fd, nsteps=50)
+        ref50 = fd[4]
+        scale50 = ref50.abs().max().item()
+        acc50 = {}
+        for name, c in (("treecode_mixed", ctx32), ("treecode_fp64", ctx64)):
+            fa = fields()
+            c.bve_run(*fa, nsteps=50)
+            acc50[name] = {"rel_linf_vort": (fa[4] - ref50).abs().max().item() / scale50}
+        del ctxd
+
+    # ---- the plain direct-sum configuration: 24,576 particles, 100 steps ----
+    g5 = sb.build_grid(5, DEGREE, exact_cc=True)
+    vor5 = rh4(g5)
+    direct5 = {}
+    out5 = {}
+    for name, prec in (("fp64", sb.FP64), ("mixed", sb.MIXED)):
+        c5 = sb.Context(sb.config_default(levels=5, interp_degree=DEGREE, kernel_eps=EPS, omega=OMEGA, dt=DT,
+                                          velocity=sb.VEL_DIRECT, precision=prec))
+        f5 = [T(g5.x), T(g5.y), T(g5.z), T(g5.area), T(vor5), *[torch.zeros_like(T(g5.x)) for _ in range(3)], None]
+        c5.bve_run(*f5, nsteps=1)  # graph capture and warm-up
+        f5[4].copy_(T(vor5))
+        st5 = torch.cuda.current_stream()
+        a5, b5 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a5.record(st5)
+        c5.bve_run(*f5, nsteps=100)
+        b5.record(st5)
+        b5.synchronize()
+        direct5[name] = {"steps_per_s": 100 / (a5.elapsed_time(b5) * 1e-3)}
+        out5[name] = f5[4]
+        del c5
+    direct5["rel_linf_vort_mixed_vs_fp64_step100"] = ((out5["mixed"] - out5["fp64"]).abs().max().item() /
+                                                      out5["fp64"].abs().max().item())
+    direct5["config"] = "24,576 particles (levels 5), RH4, direct sum, 100 steps of dt 0.005, graph replay, L2 not flushed"
 
     # ---- the reference's own FMM in float64 at the largest theta that meets the 1e-6 bar ----
     bar_sweep, bar_sweep32 = [], []
@@ -782,6 +823,8 @@ def main():
                 "speedup_vs_fp64_reference_fmm_at_bar": (mixed_at_bar["steps_per_s"] / plain_at_bar["steps_per_s"])
                 if mixed_at_bar and plain_at_bar else None},
             "accuracy_step1_vs_fp64_direct": dict(acc, direct_step_s=direct_s),
+            "accuracy_step50_vs_fp64_direct": acc50,
+            "direct_sum_levels5": direct5,
             "ensemble": ens, "adjoint": adj, "swe": swe, "cpu_baseline": cpu, "clocks": clk.summary(),
         }
         print(json.dumps(line))
