@@ -174,7 +174,9 @@ long sbslpm_kernel_launches(void);
  * [leaf][q]; vors is advanced in place; vel_x/y/z receive the stage-0
  * velocity (the reference's vel_x/y/z); tracers [leaf][q][tracer_count] are
  * remapped in place (may be NULL when tracer_count is 0).  time is the
- * step's time in seconds (read by the forcing, unused without it). */
+ * step's time in seconds (read by the forcing, unused without it).  Host
+ * memory among the arguments is refused with SBSLPM_ERR_ARG (the same holds
+ * for the run, SWE and batch steps); sbslpm_bve_step_host takes host arrays. */
 sbslpm_status sbslpm_bve_step(sbslpm_ctx* ctx, const double* xcos, const double* ycos, const double* zcos,
                               const double* area, double* vors, double* vel_x, double* vel_y, double* vel_z,
                               double* tracers, double time);

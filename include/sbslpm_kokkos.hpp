@@ -13,7 +13,8 @@
 // `using sbslpm_kokkos::bve_back_rk4_step;`.  The Views are LayoutRight, in
 // device memory (CudaSpace / CudaUVMSpace) or, for bve_back_rk4_step, in host
 // memory (HostSpace: the reference's OpenMP build), where the step copies
-// through sbslpm_bve_step_host; all Views of one call in the same space.
+// through sbslpm_bve_step_host; all Views of one call in the same space.  The
+// other drop-ins take device Views only and throw on host ones.
 //
 // The panel table, interaction list and interpolation table the reference
 // passes are rebuilt inside the library from run_config (they are functions

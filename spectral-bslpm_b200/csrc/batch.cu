@@ -541,6 +541,8 @@ sbslpm_status sbslpm_batch_get_sizes(const sbslpm_batch* b, long* sizes) {
 sbslpm_status sbslpm_batch_step(sbslpm_batch* b, const double* x, const double* y, const double* z,
                                 const double* area, double* vors, double* vel, double) {
   if (!b || bad(x) || bad(y) || bad(z) || bad(area) || bad(vors) || bad(vel)) return SBSLPM_ERR_ARG;
+  if (any_on_host({x, y, z, area, vors, vel}))
+    return set_last_error("device-pointer step given host memory"), SBSLPM_ERR_ARG;
   SB_TRY(batch_autotune(b, x, y, z, area, vors));
   batch_enqueue_step(b, x, y, z, area, vors, vel);
   return batch_finish(b);
@@ -549,6 +551,8 @@ sbslpm_status sbslpm_batch_step(sbslpm_batch* b, const double* x, const double* 
 sbslpm_status sbslpm_batch_run(sbslpm_batch* b, const double* x, const double* y, const double* z,
                                const double* area, double* vors, double* vel, double, int nsteps) {
   if (!b || bad(x) || bad(y) || bad(z) || bad(area) || bad(vors) || bad(vel) || nsteps < 0) return SBSLPM_ERR_ARG;
+  if (any_on_host({x, y, z, area, vors, vel}))
+    return set_last_error("device-pointer step given host memory"), SBSLPM_ERR_ARG;
   SB_TRY(batch_autotune(b, x, y, z, area, vors));
   const void* key[7] = {x, y, z, area, vors, vel, nullptr};
   cudaStream_t st = b->stream();

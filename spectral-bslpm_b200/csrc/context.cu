@@ -775,6 +775,8 @@ sbslpm_status sbslpm_bve_step(sbslpm_ctx* c, const double* x, const double* y, c
   if (!c || bad(x) || bad(y) || bad(z) || bad(area) || bad(vors) || bad(vel_x) || bad(vel_y) || bad(vel_z) ||
       (c->cfg.tracer_count > 0 && bad(tracers)) || !std::isfinite(time))
     return SBSLPM_ERR_ARG;
+  if (any_on_host({x, y, z, area, vors, vel_x, vel_y, vel_z, tracers}))
+    return set_last_error("device-pointer step given host memory (sbslpm_bve_step_host takes host arrays)"), SBSLPM_ERR_ARG;
   SB_TRY(near_autotune(c, x, y, z, area, vors));
   if (c->force) SB_CUDA(cudaMemcpyAsync(c->d_time, &time, sizeof(double), cudaMemcpyHostToDevice, c->stream()));
   enqueue_step(c, x, y, z, area, vors, vel_x, vel_y, vel_z, tracers);
@@ -833,6 +835,8 @@ sbslpm_status sbslpm_bve_run(sbslpm_ctx* c, const double* x, const double* y, co
   if (!c || bad(x) || bad(y) || bad(z) || bad(area) || bad(vors) || bad(vel_x) || bad(vel_y) || bad(vel_z) ||
       (c->cfg.tracer_count > 0 && bad(tracers)) || nsteps < 0 || !std::isfinite(time))
     return SBSLPM_ERR_ARG;
+  if (any_on_host({x, y, z, area, vors, vel_x, vel_y, vel_z, tracers}))
+    return set_last_error("device-pointer step given host memory (sbslpm_bve_step_host takes host arrays)"), SBSLPM_ERR_ARG;
   SB_TRY(near_autotune(c, x, y, z, area, vors));
   GraphKey key{{x, y, z, area, vors, vel_x, vel_y, vel_z, tracers}};
   cudaStream_t st = c->stream();

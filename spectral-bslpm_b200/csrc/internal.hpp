@@ -5,12 +5,21 @@
 #include <cuda_runtime.h>
 
 #include <array>
+#include <initializer_list>
 #include <string>
 #include <vector>
 
 #include "../../include/sbslpm.h"
 
 namespace sbslpm {
+
+// True when any non-null pointer is host memory: the entry points that take
+// device pointers reject those arguments instead of handing them to kernels.
+inline bool any_on_host(std::initializer_list<const void*> ps) {
+  for (const void* p : ps)
+    if (p && sbslpm_pointer_on_device(p) == 0) return true;
+  return false;
+}
 
 // setup_host.cpp
 int child_of(const sbslpm_panel& p, int c);

@@ -163,6 +163,8 @@ sbslpm_status sbslpm_swe_step(sbslpm_ctx* c, const double* x, const double* y, c
   if (!c || bad(x) || bad(y) || bad(z) || bad(area) || bad(vors) || bad(divs) || bad(height) || bad(vel_x) ||
       bad(vel_y) || bad(vel_z) || bad(bv) || bad(bd) || bad(bh) || (c->cfg.tracer_count > 0 && bad(tracers)))
     return SBSLPM_ERR_ARG;
+  if (any_on_host({x, y, z, area, vors, divs, height, vel_x, vel_y, vel_z, tracers, bv, bd, bh}))
+    return set_last_error("device-pointer step given host memory"), SBSLPM_ERR_ARG;
   SB_TRY(swe_setup(c));
   swe_enqueue_step(c, x, y, z, area, vors, divs, height, vel_x, vel_y, vel_z, tracers, bv, bd, bh);
   return finish(c);
@@ -176,6 +178,8 @@ sbslpm_status sbslpm_swe_run(sbslpm_ctx* c, const double* x, const double* y, co
       bad(vel_y) || bad(vel_z) || bad(bv) || bad(bd) || bad(bh) || (c->cfg.tracer_count > 0 && bad(tracers)) ||
       nsteps < 0)
     return SBSLPM_ERR_ARG;
+  if (any_on_host({x, y, z, area, vors, divs, height, vel_x, vel_y, vel_z, tracers, bv, bd, bh}))
+    return set_last_error("device-pointer step given host memory"), SBSLPM_ERR_ARG;
   SB_TRY(swe_setup(c));
   GraphKey key{{x, y, z, area, vors, divs, height, vel_x, vel_y, vel_z, tracers, bv, bd, bh}};
   if (!c->swe_graph || !(key == c->swe_graph_key)) {

@@ -18,6 +18,8 @@ from test_gpu_bve import unit_sphere_rh4
 pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
 
+ERR_ARG = 5  # SBSLPM_ERR_ARG
+
 
 def device_step(ctx, g, vor, tracers=None, time=0.0):
     T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
@@ -87,6 +89,24 @@ def test_host_step_rejects_device_and_misshaped_arrays(sb):
     bad[4] = args[4][:, :8].copy()
     with pytest.raises(ValueError):
         ctx.bve_back_rk4_step_host(*bad)
+
+
+def test_device_entry_points_refuse_host_memory(sb):
+    """sbslpm_bve_step / _run given host arrays return SBSLPM_ERR_ARG instead
+    of handing host memory to the kernels; the context stays usable."""
+    import ctypes
+
+    g = sb.build_grid(3, 3, exact_cc=True)
+    ctx = sb.Context(sb.config_default(levels=3, interp_degree=3, kernel_eps=1e-4))
+    H = lambda a: np.ascontiguousarray(a, dtype=np.float64).copy()
+    host = [H(g.x), H(g.y), H(g.z), H(g.area), H(unit_sphere_rh4(g))] + [H(np.zeros_like(g.x)) for _ in range(3)]
+    L = sb.lib()
+    st = L.sbslpm_bve_step(ctx._h, *[a.ctypes.data for a in host], None, ctypes.c_double(0.0))
+    assert st == ERR_ARG and b"host memory" in L.sbslpm_last_error()
+    st = L.sbslpm_bve_run(ctx._h, *[a.ctypes.data for a in host], None, ctypes.c_double(0.0), 1)
+    assert st == ERR_ARG
+    a = device_step(ctx, g, unit_sphere_rh4(g))  # still steps on device memory
+    assert np.isfinite(a[0]).all()
 
 
 def test_pointer_on_device(sb):
