@@ -359,7 +359,8 @@ sbslpm_status sbslpm_batch_pairs(const sbslpm_batch* batch, double* near_pairs, 
  * mode -1 = chosen per proxy-degree group by the autotuner of the first
  * step (the default), 0 = CUDA-core float32 pairs per member (bit-exact with
  * single contexts on the whole-panel well-separated kernel,
- * sbslpm_set_cc_tuning(ctx, 0, 0)), 1 = tensor-core GEMM over the members sharing a proxy
+ * sbslpm_set_cc_tuning(ctx, 0, 0), with sbslpm_batch_set_stage0_shared(batch,
+ * 0)), 1 = tensor-core GEMM over the members sharing a proxy
  * degree in 3xTF32, 2 = the same GEMM in one TF32 pass.  Float64 batches
  * accept mode 0 only.  sbslpm_batch_cc_info reports the mode, the union of
  * the members' well-separated pairs over the degree groups (cluster pairs),
@@ -368,6 +369,14 @@ sbslpm_status sbslpm_batch_pairs(const sbslpm_batch* batch, double* near_pairs, 
  * the autotuner's timings of one launch in modes 0 and 1 (0 before the
  * first step). */
 sbslpm_status sbslpm_batch_set_cc_mode(sbslpm_batch* batch, int mode);
+/* Mixed-precision batches: the near field of each step's first stage, where
+ * every member's particles sit on the shared grid, evaluated once per leaf
+ * pair for theta-sorted groups of 4 members and applied to their strengths
+ * (shared = 1, the default), or by every member's own near kernel (0: the
+ * arithmetic of single contexts, bit-exact with them).  The two differ only
+ * in the order of float32 additions.  SBSLPM_ERR_CONFIG for float64 batches.
+ * Replaces nothing in the reference (one problem per process there). */
+sbslpm_status sbslpm_batch_set_stage0_shared(sbslpm_batch* batch, int shared);
 sbslpm_status sbslpm_batch_cc_info(const sbslpm_batch* batch, int* mode, double* union_pairs, double* mma_flops);
 sbslpm_status sbslpm_batch_cc_groups(const sbslpm_batch* batch, int n, int* degree, int* members, int* mode,
                                      double* ms_cuda_cores, double* ms_tensor_cores);

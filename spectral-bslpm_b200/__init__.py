@@ -166,6 +166,7 @@ def lib() -> ctypes.CDLL:
     L.sbslpm_set_near_tuning.argtypes = [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     L.sbslpm_near_tuning.argtypes = [_VP, _I, _D]
     L.sbslpm_set_cc_tuning.argtypes = [_VP, ctypes.c_int, ctypes.c_int]
+    L.sbslpm_batch_set_stage0_shared.argtypes = [_VP, ctypes.c_int]
     L.sbslpm_cc_tuning.argtypes = [_VP, _I, _D]
     L.sbslpm_measure_fma_peak.argtypes = [ctypes.c_int, ctypes.c_double, _D]
     _lib = L
@@ -650,6 +651,12 @@ class Batch:
         return a.value, b.value
 
     CC_AUTO, CC_CUDA_CORES, CC_TC_3XTF32, CC_TC_TF32 = -1, 0, 1, 2
+
+    def set_stage0_shared(self, shared: bool):
+        """Mixed precision: the first stage's near field shared by theta-sorted
+        groups of members (True, the default) or run per member (False: bit-exact
+        with single contexts)."""
+        _check(lib().sbslpm_batch_set_stage0_shared(self._h, 1 if shared else 0), "sbslpm_batch_set_stage0_shared")
 
     def set_cc_mode(self, mode: int):
         """Well-separated interactions: -1 autotuned per proxy-degree group (default for mixed

@@ -66,6 +66,12 @@ struct sbslpm_batch {
   // cores TF32 (mixed precision only)
   int cc_mode = 0;
 
+  // stage-0 near field shared by theta-sorted groups of kNearGroup members
+  // (mixed precision; off: every member's own near kernel at every stage)
+  bool stage0_shared = false;
+  int ngroups = 0;
+  int *d_perm = nullptr, *d_gstart = nullptr, *d_gent = nullptr;
+
   // autotuned near-field launch shape
   bool tuned = false;
   int nt = 128, tpt = 2, splits = 2, candidates = 0;
@@ -187,6 +193,7 @@ sbslpm_status batch_setup(sbslpm_batch* b) {
     if (mixed) uidx[k].assign((size_t)G.Pf * G.Pf, -1);
   }
   b->h_mem.resize(b->M);
+  std::vector<std::vector<int>> hns(b->M), hnsrc(b->M);  // members' near lists (host)
   b->near_pairs.assign(b->M, 0);
   b->cc_pairs.assign(b->M, 0);
   for (int m = 0; m < b->M; m++) {
@@ -195,6 +202,8 @@ sbslpm_status batch_setup(sbslpm_batch* b) {
     D.members.push_back(m);
     TreeLists l;
     build_tree_lists(D.t, b->theta[m], l);
+    hns[m] = l.ns;
+    hnsrc[m] = l.nsrc;
     b->near_pairs[m] = l.ns.back();
     b->cc_pairs[m] = l.cs.back();
     if (mixed) {
@@ -262,6 +271,45 @@ sbslpm_status batch_setup(sbslpm_batch* b) {
   }
   for (auto& D : b->degs) SB_TRY(bupload(b, &D.d_idx, D.members));
   SB_TRY(bupload(b, &b->d_mem, b->h_mem));
+  if (mixed) {
+    // members sorted by theta (their near lists nest), in groups of
+    // kNearGroup; per group and target leaf the union of the members' near
+    // source leaves in ascending order, each with its members' bits
+    constexpr int MB = kNearGroup;
+    std::vector<int> perm(b->M);
+    for (int m = 0; m < b->M; m++) perm[m] = m;
+    std::stable_sort(perm.begin(), perm.end(), [&](int u, int v) { return b->theta[u] < b->theta[v]; });
+    b->ngroups = (b->M + MB - 1) / MB;
+    const int Af = b->Af;
+    std::vector<int> gstart((size_t)b->ngroups * (Af + 1), 0), gent;
+    std::vector<int> bits(Af, 0), seen;
+    for (int g = 0; g < b->ngroups; g++) {
+      gstart[(size_t)g * (Af + 1)] = (int)gent.size();  // offsets into gent, all groups in one array
+      for (int f = 0; f < Af; f++) {
+        seen.clear();
+        for (int j = 0; j < MB && g * MB + j < b->M; j++) {
+          const int m = perm[g * MB + j];
+          for (int e = hns[m][f]; e < hns[m][f + 1]; e++) {
+            const int sl = hnsrc[m][e];
+            if (!bits[sl]) seen.push_back(sl);
+            bits[sl] |= 1 << j;
+          }
+        }
+        std::sort(seen.begin(), seen.end());
+        for (int sl : seen) {
+          gent.push_back(sl | (bits[sl] << 24));
+          bits[sl] = 0;
+        }
+        gstart[(size_t)g * (Af + 1) + f + 1] = (int)gent.size();
+      }
+    }
+    if (Af < (1 << 24)) {
+      SB_TRY(bupload(b, &b->d_perm, perm));
+      SB_TRY(bupload(b, &b->d_gstart, gstart));
+      if (!gent.empty()) SB_TRY(bupload(b, &b->d_gent, gent));
+      b->stage0_shared = !gent.empty();
+    }
+  }
   if (mixed) {
     for (size_t k = 0; k < b->degs.size(); k++) {
       sbslpm_batch::Degree& D = b->degs[k];
@@ -354,8 +402,12 @@ void batch_velocity(sbslpm_batch* b, int stage, double dt_s, const double* vprev
   }
   launch_downward_batch(b->d_mem, b->M, b->Lf, b->qmax, tree_st);
   if (b->aux_stream) cudaEventRecord(b->ev_join, tree_st);
-  launch_bltc_near_batch(b->d_mem, b->M, b->Af, b->npl, b->cfg.kernel_eps, prec, x, y, z, b->psrc, b->psrcf, b->near,
-                         b->splits, b->nt, b->tpt, st);
+  if (stage == 0 && mixed && b->stage0_shared)
+    launch_bltc_near_multi(b->d_mem, b->d_perm, b->M, b->ngroups, b->Af, b->npl, b->cfg.kernel_eps, b->d_gstart,
+                           b->d_gent, x, y, z, b->psrcf, b->near, b->splits, st);
+  else
+    launch_bltc_near_batch(b->d_mem, b->M, b->Af, b->npl, b->cfg.kernel_eps, prec, x, y, z, b->psrc, b->psrcf,
+                           b->near, b->splits, b->nt, b->tpt, st);
   if (b->aux_stream) cudaStreamWaitEvent(st, b->ev_join, 0);
   launch_bltc_to_particles_batch(b->d_mem, b->M, b->Af, b->nmax, b->near, b->splits, v, st);
 }
@@ -618,6 +670,18 @@ sbslpm_status sbslpm_batch_set_tuning(sbslpm_batch* b, int threads, int targets_
     cudaGraphExecDestroy(b->graph);
     b->graph = nullptr;
   }
+  return SBSLPM_OK;
+}
+
+sbslpm_status sbslpm_batch_set_stage0_shared(sbslpm_batch* b, int shared) {
+  if (!b || (shared != 0 && shared != 1)) return SBSLPM_ERR_ARG;
+  if (shared && !b->d_gent)
+    return set_last_error("the shared stage-0 near field needs a mixed-precision batch"), SBSLPM_ERR_CONFIG;
+  if ((bool)shared != b->stage0_shared && b->graph) {
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  b->stage0_shared = shared != 0;
   return SBSLPM_OK;
 }
 

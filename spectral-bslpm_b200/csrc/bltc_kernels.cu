@@ -312,6 +312,117 @@ __global__ void __launch_bounds__(NT)
                                    out + mo * gridDim.y * 3 * tg.N);
 }
 
+// The near field of the first RK stage for a group of MB members at once.
+// At stage 0 every member's particles sit on the shared grid (only the
+// strengths differ), so a leaf pair's differences, distances and
+// reciprocals are member-independent: they are evaluated once and applied to
+// the MB members' strengths with the paired float32 instructions across
+// members (FMUL2 / FFMA2 over member pairs).  Members are grouped by sorted
+// theta; a group walks the union of its members' near lists (entry = source
+// leaf | member bits << 24), a member outside an entry's bits taking zero
+// strength there.  Per member, per source leaf: float32 sums added into
+// float64, partials per split as in the per-member kernel.
+template <int NT, int MB, bool GUARD>
+__global__ void __launch_bounds__(NT)
+    k_bltc_near32_multi(const BatchMember* __restrict__ mem, const int* __restrict__ perm, int members,
+                        const int* __restrict__ ustart, const int* __restrict__ uent, const double* __restrict__ x,
+                        const double* __restrict__ y, const double* __restrict__ z, const float4* __restrict__ psrcf,
+                        double* __restrict__ out) {
+  extern __shared__ float4 tq[];  // [npl/2][2] paired positions, then [npl][MB] strengths
+  const int f = blockIdx.x, split = blockIdx.y, nsplit = gridDim.y, grp = blockIdx.z;
+  const int m0 = perm[grp * MB];
+  const TreeGeom tg = mem[m0].tg;
+  const StepGeom fg = mem[m0].fg;
+  const int npl = tg.npl, npl2 = (npl + 1) >> 1, leaves = fg.leaves;
+  const long N = tg.N;
+  float* wt = reinterpret_cast<float*>(tq + 2 * npl2);
+  int mid[MB];
+#pragma unroll
+  for (int j = 0; j < MB; j++) mid[j] = grp * MB + j < members ? perm[grp * MB + j] : -1;
+  const int k = threadIdx.x;
+  const bool tgt = k < npl;
+  const double* ct = fg.pd_centre + 4 * (long)(fg.offset + f);
+  const long ti = (long)f * npl + (tgt ? k : 0);
+  const float dtx = (float)((x[ti] - ct[0]) * kPackScale), dty = (float)((y[ti] - ct[1]) * kPackScale),
+              dtz = (float)((z[ti] - ct[2]) * kPackScale);
+  double ax[MB], ay[MB], az[MB];
+#pragma unroll
+  for (int j = 0; j < MB; j++) ax[j] = ay[j] = az[j] = 0;
+  const float feps = (float)tg.eps;
+  const float2 eps2 = make_float2(feps, feps);
+  const int* us = ustart + (long)grp * (leaves + 1);
+  for (int e = us[f] + split; e < us[f + 1]; e += nsplit) {
+    const int ent = __ldg(uent + e), sl = ent & 0xffffff, bits = ent >> 24;
+    const double* cs = fg.pd_centre + 4 * (long)(fg.offset + sl);
+    const float bx0 = (float)((cs[0] - ct[0]) * kPackScale), by0 = (float)((cs[1] - ct[1]) * kPackScale),
+                bz0 = (float)((cs[2] - ct[2]) * kPackScale);
+    const long sb = (long)sl * npl;
+    __syncthreads();
+    for (int kk = threadIdx.x; kk < npl2; kk += NT) {
+      const float4 s0 = psrcf[(long)m0 * N + sb + 2 * kk];
+      const float4 s1 = 2 * kk + 1 < npl ? psrcf[(long)m0 * N + sb + 2 * kk + 1] : make_float4(0.f, 0.f, 0.f, 0.f);
+      tq[2 * kk] = make_float4(s0.x, s1.x, s0.y, s1.y);
+      tq[2 * kk + 1] = make_float4(s0.z, s1.z, 0.f, 0.f);
+    }
+    for (int kk = threadIdx.x; kk < 2 * npl2; kk += NT) {
+#pragma unroll
+      for (int j = 0; j < MB; j++)
+        wt[kk * MB + j] = (kk < npl && mid[j] >= 0 && ((bits >> j) & 1)) ? psrcf[(long)mid[j] * N + sb + kk].w : 0.f;
+    }
+    __syncthreads();
+    if (tgt) {
+      const float b0 = bx0 - dtx, b1 = by0 - dty, b2 = bz0 - dtz;
+      const float2 bx = make_float2(b0, b0), by = make_float2(b1, b1), bz = make_float2(b2, b2);
+      float2 fx[MB / 2], fy[MB / 2], fz[MB / 2];
+#pragma unroll
+      for (int p = 0; p < MB / 2; p++) fx[p] = fy[p] = fz[p] = make_float2(0.f, 0.f);
+#pragma unroll 2
+      for (int k2 = 0; k2 < npl2; k2++) {
+        const float4 A = tq[2 * k2], B = tq[2 * k2 + 1];
+        const float2 dx = __fadd2_rn(bx, make_float2(A.x, A.y)), dy = __fadd2_rn(by, make_float2(A.z, A.w)),
+                     dz = __fadd2_rn(bz, make_float2(B.x, B.y));
+        const float2 den = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, eps2)));
+        float r0 = recip_f32(den.x), r1 = recip_f32(den.y);
+        if (GUARD) {
+          r0 = den.x > 0.0f ? r0 : 0.0f;
+          r1 = den.y > 0.0f ? r1 : 0.0f;
+        }
+        const float2* w0 = reinterpret_cast<const float2*>(wt + (2 * k2) * MB);
+        const float2* w1 = reinterpret_cast<const float2*>(wt + (2 * k2 + 1) * MB);
+#pragma unroll
+        for (int p = 0; p < MB / 2; p++) {
+          const float2 g0 = __fmul2_rn(w0[p], make_float2(r0, r0)), g1 = __fmul2_rn(w1[p], make_float2(r1, r1));
+          fx[p] = __ffma2_rn(g0, make_float2(dx.x, dx.x), fx[p]);
+          fy[p] = __ffma2_rn(g0, make_float2(dy.x, dy.x), fy[p]);
+          fz[p] = __ffma2_rn(g0, make_float2(dz.x, dz.x), fz[p]);
+          fx[p] = __ffma2_rn(g1, make_float2(dx.y, dx.y), fx[p]);
+          fy[p] = __ffma2_rn(g1, make_float2(dy.y, dy.y), fy[p]);
+          fz[p] = __ffma2_rn(g1, make_float2(dz.y, dz.y), fz[p]);
+        }
+      }
+#pragma unroll
+      for (int p = 0; p < MB / 2; p++) {
+        ax[2 * p] += (double)fx[p].x;
+        ay[2 * p] += (double)fy[p].x;
+        az[2 * p] += (double)fz[p].x;
+        ax[2 * p + 1] += (double)fx[p].y;
+        ay[2 * p + 1] += (double)fy[p].y;
+        az[2 * p + 1] += (double)fz[p].y;
+      }
+    }
+  }
+  if (!tgt) return;
+  const double tx = x[ti], ty = y[ti], tz = z[ti];
+#pragma unroll
+  for (int j = 0; j < MB; j++) {
+    if (mid[j] < 0) continue;
+    double* v = out + (long)mid[j] * nsplit * 3 * N + (long)split * 3 * N;
+    v[ti] = kBiotSavartPacked * (ty * az[j] - tz * ay[j]);
+    v[N + ti] = kBiotSavartPacked * (tz * ax[j] - tx * az[j]);
+    v[2 * N + ti] = kBiotSavartPacked * (tx * ay[j] - ty * ax[j]);
+  }
+}
+
 // Leaf proxy targets -> particles: v_i = (near-field splits summed in order)
 // + sum_a lx[k][a] sum_b ly[k][b] T[a][b], with the leaf-box basis of
 // particle k of the (uniform) leaf.
@@ -440,6 +551,22 @@ void launch_bltc_near_batch(const BatchMember* mem, int members, int leaves, int
   else if (nt == 256 && tpt == 2) SB_NEARB(256, 2);
   else if (nt == 128 && tpt == 1) SB_NEARB(128, 1);
 #undef SB_NEARB
+}
+
+void launch_bltc_near_multi(const BatchMember* mem, const int* perm, int members, int groups, int leaves, int npl,
+                            double eps, const int* ustart, const int* uent, const double* x, const double* y,
+                            const double* z, const float4* psrcf, double* near, int splits, cudaStream_t st) {
+  constexpr int MB = kNearGroup;
+  const bool guard = !(eps > 0);
+  const dim3 grid((unsigned)leaves, (unsigned)splits, (unsigned)groups);
+  const size_t smem = sizeof(float4) * 2 * ((npl + 1) / 2) + sizeof(float) * MB * 2 * ((npl + 1) / 2);
+  if (npl <= 64) {
+    if (guard) SB_LAUNCH((k_bltc_near32_multi<64, MB, true>), grid, 64, smem, st, mem, perm, members, ustart, uent, x, y, z, psrcf, near);
+    else SB_LAUNCH((k_bltc_near32_multi<64, MB, false>), grid, 64, smem, st, mem, perm, members, ustart, uent, x, y, z, psrcf, near);
+  } else {
+    if (guard) SB_LAUNCH((k_bltc_near32_multi<256, MB, true>), grid, 256, smem, st, mem, perm, members, ustart, uent, x, y, z, psrcf, near);
+    else SB_LAUNCH((k_bltc_near32_multi<256, MB, false>), grid, 256, smem, st, mem, perm, members, ustart, uent, x, y, z, psrcf, near);
+  }
 }
 
 void launch_bltc_to_particles_batch(const BatchMember* mem, int members, int leaves, int nmax, const double* near,

@@ -148,6 +148,13 @@ void launch_bltc_sources_batch(const BatchMember* mem, int members, int leaves, 
                                const double* vors, const double* area, double4* psrc, float4* psrcf, bool mixed,
                                cudaStream_t st);
 void launch_upward_batch(const BatchMember* mem, int members, int levels, int qmax, bool mixed, cudaStream_t st);
+// Stage-0 near field of groups of kNearGroup members (mixed precision): perm
+// lists the members by group (theta-sorted), ustart[group][leaves+1] and uent
+// (source leaf | member bits << 24) are the groups' union near lists.
+constexpr int kNearGroup = 4;
+void launch_bltc_near_multi(const BatchMember* mem, const int* perm, int members, int groups, int leaves, int npl,
+                            double eps, const int* ustart, const int* uent, const double* x, const double* y,
+                            const double* z, const float4* psrcf, double* near, int splits, cudaStream_t st);
 // idx: device array of the member indices whose proxies number q
 void launch_cc_batch(const BatchMember* mem, const int* idx, int count, int q, int tree_panels, double eps,
                      int precision, cudaStream_t st);

@@ -66,6 +66,7 @@ def test_batch_equals_single_contexts(sb, precision):
     batch.set_tuning(128, 2, 2)  # the single context's near-field shape and split count
     if prec == sb.MIXED:
         batch.set_cc_mode(batch.CC_CUDA_CORES)  # the single context's float32 pair arithmetic
+        batch.set_stage0_shared(False)  # and its per-member stage-0 near field
     v = vors.clone()
     vel = torch.zeros((len(THETA), 3) + v.shape[1:], dtype=torch.float64, device="cuda")
     batch.step(*xyza, v, vel)
@@ -73,6 +74,51 @@ def test_batch_equals_single_contexts(sb, precision):
         sv, svel = single_step(sb, prec, THETA[m], PDEG[m], xyza, vors[m].contiguous())
         assert torch.equal(v[m], sv), m
         assert torch.equal(vel[m], svel), m
+
+
+def test_stage0_shared_near_field_matches_per_member(sb):
+    """The first stage's near field evaluated once per leaf pair for groups of
+    members (theta-sorted, union lists with member bits) against every member's
+    own near kernel: the same pairs, float32 sums in another order (one sum
+    per member and component over a source leaf instead of two interleaved
+    halves).  Both stay within the 1e-6 mixed-precision bar of the float64
+    batch and of each other (measured: vorticity 1e-9, stage-0 velocity 5e-7,
+    the float32 rounding of near-field sums whose terms largely cancel);
+    graph replay equals eager steps."""
+    g, xyza, vors = grid_and_vors(sb, 9)
+    theta = [0.5, 0.8, 0.65, 0.7, 0.55, 0.75, 0.6, 0.52, 0.78]
+    pdeg = [6, 8, 10, 8, 6, 10, 8, 6, 8]
+    ref = sb.Batch(base_cfg(sb, sb.FP64), theta, pdeg)
+    r = vors.clone()
+    rel_ = torch.zeros((len(theta), 3) + r.shape[1:], dtype=torch.float64, device="cuda")
+    ref.step(*xyza, r, rel_)
+    out = []
+    for shared in (False, True):
+        batch = sb.Batch(base_cfg(sb, sb.MIXED), theta, pdeg)
+        batch.set_tuning(128, 2, 2)
+        batch.set_cc_mode(batch.CC_CUDA_CORES)
+        batch.set_stage0_shared(shared)
+        v = vors.clone()
+        vel = torch.zeros((len(theta), 3) + v.shape[1:], dtype=torch.float64, device="cuda")
+        batch.step(*xyza, v, vel)
+        out.append((v, vel))
+        if shared:
+            w = vors.clone()
+            wel = torch.zeros_like(vel)
+            batch.run(*xyza, w, wel, nsteps=1)
+            assert torch.equal(w, v) and torch.equal(wel, vel)
+    assert rel(out[1][0], out[0][0]) <= 1e-8
+    assert rel(out[1][1], out[0][1]) <= 1e-6
+    for v, vel in out:
+        assert rel(v, r) <= 1e-6 and rel(vel, rel_) <= 1e-6
+
+
+def test_stage0_shared_refused_in_float64(sb):
+    g, xyza, vors = grid_and_vors(sb, 2)
+    batch = sb.Batch(base_cfg(sb, sb.FP64), THETA[:2], PDEG[:2])
+    with pytest.raises(sb.SbslpmError):
+        batch.set_stage0_shared(True)
+    batch.set_stage0_shared(False)
 
 
 def test_batch_autotuned_close_to_single(sb):
