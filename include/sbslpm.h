@@ -371,7 +371,7 @@ sbslpm_status sbslpm_batch_pairs(const sbslpm_batch* batch, double* near_pairs, 
 sbslpm_status sbslpm_batch_set_cc_mode(sbslpm_batch* batch, int mode);
 /* Mixed-precision batches: the near field of each step's first stage, where
  * every member's particles sit on the shared grid, evaluated once per leaf
- * pair for theta-sorted groups of 4 members and applied to their strengths
+ * pair for theta-sorted groups of 8 members and applied to their strengths
  * (shared = 1, the default), or by every member's own near kernel (0: the
  * arithmetic of single contexts, bit-exact with them).  The two differ only
  * in the order of float32 additions.  SBSLPM_ERR_CONFIG for float64 batches.

@@ -297,7 +297,7 @@ sbslpm_status batch_setup(sbslpm_batch* b) {
         }
         std::sort(seen.begin(), seen.end());
         for (int sl : seen) {
-          gent.push_back(sl | (bits[sl] << 24));
+          gent.push_back((int)((unsigned)sl | ((unsigned)bits[sl] << 24)));
           bits[sl] = 0;
         }
         gstart[(size_t)g * (Af + 1) + f + 1] = (int)gent.size();

@@ -352,7 +352,8 @@ __global__ void __launch_bounds__(NT)
   const float2 eps2 = make_float2(feps, feps);
   const int* us = ustart + (long)grp * (leaves + 1);
   for (int e = us[f] + split; e < us[f + 1]; e += nsplit) {
-    const int ent = __ldg(uent + e), sl = ent & 0xffffff, bits = ent >> 24;
+    const unsigned ent = (unsigned)__ldg(uent + e);
+    const int sl = (int)(ent & 0xffffffu), bits = (int)(ent >> 24);
     const double* cs = fg.pd_centre + 4 * (long)(fg.offset + sl);
     const float bx0 = (float)((cs[0] - ct[0]) * kPackScale), by0 = (float)((cs[1] - ct[1]) * kPackScale),
                 bz0 = (float)((cs[2] - ct[2]) * kPackScale);

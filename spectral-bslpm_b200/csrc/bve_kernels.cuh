@@ -151,7 +151,7 @@ void launch_upward_batch(const BatchMember* mem, int members, int levels, int qm
 // Stage-0 near field of groups of kNearGroup members (mixed precision): perm
 // lists the members by group (theta-sorted), ustart[group][leaves+1] and uent
 // (source leaf | member bits << 24) are the groups' union near lists.
-constexpr int kNearGroup = 4;
+constexpr int kNearGroup = 8;
 void launch_bltc_near_multi(const BatchMember* mem, const int* perm, int members, int groups, int leaves, int npl,
                             double eps, const int* ustart, const int* uent, const double* x, const double* y,
                             const double* z, const float4* psrcf, double* near, int splits, cudaStream_t st);
