@@ -319,6 +319,7 @@ def ensemble_bench(sb, torch, dev, flush, steps):
     ms_tc3 = time_mode(batch.CC_TC_3XTF32, max(3, steps // 4))
     _, union_pairs, mma_flops = batch.cc_info()
     ms_tf32 = time_mode(batch.CC_TC_TF32, max(3, steps // 4))
+    ms_shared = time_mode(batch.CC_SHARED, max(3, steps // 4))
     # the headline: the mode the autotuner chose for each proxy-degree group
     launches0 = sb.kernel_launches()
     ms = time_mode(batch.CC_AUTO, steps)
@@ -360,12 +361,14 @@ def ensemble_bench(sb, torch, dev, flush, steps):
         "near_tflops": PAIR_FLOP * near_pairs / (near_ms * 1e-3) / 1e12,
         "autotune": {"threads": nt, "targets_per_thread": tpt, "splits": splits, "candidates": cand,
                      "near_ms": near_ms},
-        "well_separated": {"headline_mode": "autotuned per proxy-degree group (CUDA-core float32 pairs or the "
-                                            "tensor-core 3xTF32 GEMM over the group's members)",
+        "well_separated": {"headline_mode": "autotuned per proxy-degree group (CUDA-core float32 pairs per member, "
+                                            "the tensor-core 3xTF32 GEMM over the group's members, or CUDA-core "
+                                            "pairs shared by groups of 8 members)",
                            "groups": batch.cc_groups(), "union_cluster_pairs_per_eval": union_pairs,
                            "useful_proxy_pairs_per_eval": far_pairs, "mma_flops_per_eval_3xtf32": mma_flops,
                            "ms_per_step_cuda_core_pairs": ms_cuda_cores, "ms_per_step_tensor_core_3xtf32": ms_tc3,
-                           "ms_per_step_tensor_core_tf32_single_pass": ms_tf32},
+                           "ms_per_step_tensor_core_tf32_single_pass": ms_tf32,
+                           "ms_per_step_cuda_core_shared_pairs": ms_shared},
         "fp64_plain_single_member_steps_per_s": fp64_sps,
         "speedup_member_steps_vs_fp64_plain": member_sps / fp64_sps,
         "accuracy_step1_vs_fp64_direct": acc,

@@ -361,12 +361,15 @@ sbslpm_status sbslpm_batch_pairs(const sbslpm_batch* batch, double* near_pairs, 
  * single contexts on the whole-panel well-separated kernel,
  * sbslpm_set_cc_tuning(ctx, 0, 0), with sbslpm_batch_set_stage0_shared(batch,
  * 0)), 1 = tensor-core GEMM over the members sharing a proxy
- * degree in 3xTF32, 2 = the same GEMM in one TF32 pass.  Float64 batches
+ * degree in 3xTF32, 2 = the same GEMM in one TF32 pass, 3 = CUDA-core
+ * float32 pairs whose distances and reciprocals are shared by groups of 8
+ * theta-consecutive members of a degree group (the proxies never move, so a
+ * cluster pair's geometry is the same for every member).  Float64 batches
  * accept mode 0 only.  sbslpm_batch_cc_info reports the mode, the union of
  * the members' well-separated pairs over the degree groups (cluster pairs),
  * and the MMA flops one velocity evaluation issues.  sbslpm_batch_cc_groups
  * reports per group (at most n): proxy degree, members, the mode in use and
- * the autotuner's timings of one launch in modes 0 and 1 (0 before the
+ * the autotuner's timings of one launch in modes 0, 1 and 3 (0 before the
  * first step). */
 sbslpm_status sbslpm_batch_set_cc_mode(sbslpm_batch* batch, int mode);
 /* Mixed-precision batches: the near field of each step's first stage, where
@@ -379,7 +382,7 @@ sbslpm_status sbslpm_batch_set_cc_mode(sbslpm_batch* batch, int mode);
 sbslpm_status sbslpm_batch_set_stage0_shared(sbslpm_batch* batch, int shared);
 sbslpm_status sbslpm_batch_cc_info(const sbslpm_batch* batch, int* mode, double* union_pairs, double* mma_flops);
 sbslpm_status sbslpm_batch_cc_groups(const sbslpm_batch* batch, int n, int* degree, int* members, int* mode,
-                                     double* ms_cuda_cores, double* ms_tensor_cores);
+                                     double* ms_cuda_cores, double* ms_tensor_cores, double* ms_shared);
 
 /* ---------------- Poisson (inverse Laplacian) FMM ---------------- */
 

@@ -160,7 +160,7 @@ def lib() -> ctypes.CDLL:
     L.sbslpm_batch_pairs.argtypes = [_VP, _D, _D]
     L.sbslpm_batch_set_cc_mode.argtypes = [_VP, ctypes.c_int]
     L.sbslpm_batch_cc_info.argtypes = [_VP, _I, _D, _D]
-    L.sbslpm_batch_cc_groups.argtypes = [_VP, ctypes.c_int, _I, _I, _I, _D, _D]
+    L.sbslpm_batch_cc_groups.argtypes = [_VP, ctypes.c_int, _I, _I, _I, _D, _D, _D]
     L.sbslpm_batch_set_tuning.argtypes = [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     L.sbslpm_time_interactions.argtypes = [_VP, ctypes.c_int, _D, _D]
     L.sbslpm_set_near_tuning.argtypes = [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_int]
@@ -650,7 +650,7 @@ class Batch:
         _check(lib().sbslpm_batch_pairs(self._h, ctypes.byref(a), ctypes.byref(b)), "sbslpm_batch_pairs")
         return a.value, b.value
 
-    CC_AUTO, CC_CUDA_CORES, CC_TC_3XTF32, CC_TC_TF32 = -1, 0, 1, 2
+    CC_AUTO, CC_CUDA_CORES, CC_TC_3XTF32, CC_TC_TF32, CC_SHARED = -1, 0, 1, 2, 3
 
     def set_stage0_shared(self, shared: bool):
         """Mixed precision: the first stage's near field shared by theta-sorted
@@ -673,13 +673,14 @@ class Batch:
 
     def cc_groups(self):
         """Per proxy-degree group: dicts of degree, members, mode in use and the autotuner's
-        timings (ms per launch) of the CUDA-core and tensor-core modes."""
+        timings (ms per launch) of the per-member CUDA-core, tensor-core 3xTF32 and
+        shared-pair CUDA-core modes."""
         n = 16
         deg, mem, mode = (ctypes.c_int * n)(), (ctypes.c_int * n)(), (ctypes.c_int * n)()
-        t0, t1 = (ctypes.c_double * n)(), (ctypes.c_double * n)()
-        _check(lib().sbslpm_batch_cc_groups(self._h, n, deg, mem, mode, t0, t1), "sbslpm_batch_cc_groups")
+        t0, t1, t3 = (ctypes.c_double * n)(), (ctypes.c_double * n)(), (ctypes.c_double * n)()
+        _check(lib().sbslpm_batch_cc_groups(self._h, n, deg, mem, mode, t0, t1, t3), "sbslpm_batch_cc_groups")
         return [{"degree": deg[k], "members": mem[k], "mode": mode[k], "ms_cuda_cores": t0[k],
-                 "ms_tensor_cores": t1[k]} for k in range(n) if mem[k] > 0]
+                 "ms_tensor_cores": t1[k], "ms_shared": t3[k]} for k in range(n) if mem[k] > 0]
 
 
 def measure_fma_peak(kind: int = 0, ms: float = 50.0) -> float:

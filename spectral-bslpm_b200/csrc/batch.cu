@@ -46,8 +46,8 @@ struct sbslpm_batch {
     // tensor-core well-separated interactions: union of the members' lists
     CcTcGroup tc{};
     long upairs = 0;
-    int cc_auto = 0;           // the autotuner's choice for this group (0 CUDA cores, 1 tensor cores 3xTF32)
-    double cc_ms[2] = {0, 0};  // its timings of one launch in each mode
+    int cc_auto = 0;              // the autotuner's choice for this group (mode 0, 1 or 3)
+    double cc_ms[3] = {0, 0, 0};  // its timings of one launch in modes 0, 1 and 3
   };
   std::vector<Degree> degs;
   std::vector<void*> bufs;  // every device buffer of the batch, freed on destroy
@@ -62,8 +62,9 @@ struct sbslpm_batch {
   unsigned* h_err = nullptr;
 
   // well-separated interactions: -1 autotuned per proxy-degree group (mixed
-  // precision default), 0 CUDA-core pairs, 1 tensor cores 3xTF32, 2 tensor
-  // cores TF32 (mixed precision only)
+  // precision default), 0 CUDA-core pairs per member, 1 tensor cores 3xTF32,
+  // 2 tensor cores TF32, 3 CUDA-core pairs shared by groups of members
+  // (1-3: mixed precision only)
   int cc_mode = 0;
 
   // stage-0 near field shared by theta-sorted groups of kNearGroup members
@@ -196,7 +197,13 @@ sbslpm_status batch_setup(sbslpm_batch* b) {
   std::vector<std::vector<int>> hns(b->M), hnsrc(b->M);  // members' near lists (host)
   b->near_pairs.assign(b->M, 0);
   b->cc_pairs.assign(b->M, 0);
-  for (int m = 0; m < b->M; m++) {
+  // members in theta order, so that a degree group's member bits (and the
+  // shared-pair groups of consecutive bits) follow theta
+  std::vector<int> by_theta(b->M);
+  for (int m = 0; m < b->M; m++) by_theta[m] = m;
+  std::stable_sort(by_theta.begin(), by_theta.end(), [&](int u, int v) { return b->theta[u] < b->theta[v]; });
+  for (int mi = 0; mi < b->M; mi++) {
+    const int m = by_theta[mi];
     const size_t k = std::lower_bound(uniq.begin(), uniq.end(), b->degree[m]) - uniq.begin();
     sbslpm_batch::Degree& D = b->degs[k];
     D.members.push_back(m);
@@ -393,7 +400,9 @@ void batch_velocity(sbslpm_batch* b, int stage, double dt_s, const double* vprev
   launch_upward_batch(b->d_mem, b->M, b->Lf, b->qmax, mixed, tree_st);
   for (const auto& D : b->degs) {
     const int mode = mixed ? (b->cc_mode < 0 ? D.cc_auto : b->cc_mode) : 0;
-    if (mode != 0) {
+    if (mode == 3) {
+      launch_cc_multi(D.tc, tree_st);
+    } else if (mode != 0) {
       launch_cc_tc_pack(D.tc, tree_st);
       launch_cc_tc(D.tc, mode == 1 ? 3 : 1, tree_st);
     } else {
@@ -470,10 +479,13 @@ sbslpm_status batch_autotune(sbslpm_batch* b, const double* x, const double* y, 
   if (prec == SBSLPM_MIXED) {
     launch_upward_batch(b->d_mem, b->M, b->Lf, b->qmax, true, st);
     for (auto& D : b->degs) {
-      for (int mode = 0; mode < 2; mode++) {
+      for (int mi = 0; mi < 3; mi++) {
+        const int mode = mi == 2 ? 3 : mi;
         auto run = [&] {
           if (mode == 0)
             launch_cc_batch(b->d_mem, D.d_idx, (int)D.members.size(), D.qx, b->Pf, b->cfg.kernel_eps, prec, st);
+          else if (mode == 3)
+            launch_cc_multi(D.tc, st);
           else {
             launch_cc_tc_pack(D.tc, st);
             launch_cc_tc(D.tc, 3, st);
@@ -486,9 +498,13 @@ sbslpm_status batch_autotune(sbslpm_batch* b, const double* x, const double* y, 
         SB_CUDA(cudaEventSynchronize(e1));
         float ms = 0;
         SB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-        D.cc_ms[mode] = ms / 3;
+        D.cc_ms[mi] = ms / 3;
       }
-      D.cc_auto = D.cc_ms[1] < D.cc_ms[0] ? 1 : 0;
+      const int modes[3] = {0, 1, 3};
+      int best = 0;
+      for (int mi = 1; mi < 3; mi++)
+        if (D.cc_ms[mi] < D.cc_ms[best]) best = mi;
+      D.cc_auto = modes[best];
     }
   }
   cudaEventDestroy(e0);
@@ -686,9 +702,10 @@ sbslpm_status sbslpm_batch_set_stage0_shared(sbslpm_batch* b, int shared) {
 }
 
 sbslpm_status sbslpm_batch_set_cc_mode(sbslpm_batch* b, int mode) {
-  if (!b || mode < -1 || mode > 2) return SBSLPM_ERR_ARG;
-  if (mode != 0 && b->cfg.precision != SBSLPM_MIXED)
-    return set_last_error("tensor-core well-separated interactions need mixed precision"), SBSLPM_ERR_CONFIG;
+  if (!b || mode < -1 || mode > 3) return SBSLPM_ERR_ARG;
+  if (mode > 0 && b->cfg.precision != SBSLPM_MIXED)
+    return set_last_error("the tensor-core and shared-pair well-separated modes need mixed precision"),
+           SBSLPM_ERR_CONFIG;
   if (mode != b->cc_mode && b->graph) {
     cudaGraphExecDestroy(b->graph);
     b->graph = nullptr;
@@ -705,7 +722,7 @@ sbslpm_status sbslpm_batch_cc_info(const sbslpm_batch* b, int* mode, double* uni
     const CcTcGroup& G = D.tc;
     const int mode = b->cc_mode < 0 ? D.cc_auto : b->cc_mode;
     up += (double)D.upairs;
-    if (mode != 0) {
+    if (mode == 1 || mode == 2) {
       const double tiles = ((3 * G.Q + 127) / 128), ksteps = (G.Q + 7) / 8;
       fl += (double)D.upairs * tiles * ksteps * 2.0 * 128 * 8 * G.npad * (mode == 1 ? 3 : 1);
     }
@@ -716,8 +733,9 @@ sbslpm_status sbslpm_batch_cc_info(const sbslpm_batch* b, int* mode, double* uni
 }
 
 sbslpm_status sbslpm_batch_cc_groups(const sbslpm_batch* b, int n, int* degree, int* members, int* mode,
-                                     double* ms_cuda_cores, double* ms_tensor_cores) {
-  if (!b || n < 0 || !degree || !members || !mode || !ms_cuda_cores || !ms_tensor_cores) return SBSLPM_ERR_ARG;
+                                     double* ms_cuda_cores, double* ms_tensor_cores, double* ms_shared) {
+  if (!b || n < 0 || !degree || !members || !mode || !ms_cuda_cores || !ms_tensor_cores || !ms_shared)
+    return SBSLPM_ERR_ARG;
   for (int k = 0; k < n && k < (int)b->degs.size(); k++) {
     const auto& D = b->degs[k];
     degree[k] = D.n;
@@ -725,6 +743,7 @@ sbslpm_status sbslpm_batch_cc_groups(const sbslpm_batch* b, int n, int* degree, 
     mode[k] = b->cfg.precision != SBSLPM_MIXED ? 0 : (b->cc_mode < 0 ? D.cc_auto : b->cc_mode);
     ms_cuda_cores[k] = D.cc_ms[0];
     ms_tensor_cores[k] = D.cc_ms[1];
+    ms_shared[k] = D.cc_ms[2];
   }
   return (int)b->degs.size() > n ? SBSLPM_ERR_ARG : SBSLPM_OK;
 }

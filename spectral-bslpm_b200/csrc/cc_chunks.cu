@@ -20,6 +20,7 @@
 
 #include "../../include/sbslpm.h"
 #include "bve_kernels.cuh"
+#include "cc_tcgen05.cuh"
 #include "device_common.cuh"
 
 namespace sbslpm {
@@ -185,6 +186,121 @@ __global__ void k_cc_reduce(StepGeom g, const int* __restrict__ cstart, const do
   out[2 * pn + i] = cb * (px * sy - py * sx);
 }
 
+// Batched ensembles: the well-separated interactions of a proxy-degree group
+// for MB members at once.  Treecode proxies never move, so a cluster pair's
+// differences, distances and reciprocals are the same for every member; they
+// are evaluated once per pair of the group's union list and applied to the MB
+// members' strengths with the paired float32 instructions across members.
+// One block per (target cluster, member group of MB consecutive group bits,
+// the members being theta-sorted), a thread per target proxy; a member
+// outside an entry's bits takes zero strength there.  Per member and source
+// cluster: float32 sums added into float64; every (target, member) of the
+// group is written (zeros without entries).
+template <int Q, int MB, bool GUARD>
+__global__ void __launch_bounds__((Q + 31) / 32 * 32) k_cc_multi(CcTcGroup g) {
+  constexpr int Q2 = (Q + 1) / 2;
+  __shared__ float4 tq[2 * Q2];   // (x0,x1,y0,y1),(z0,z1,0,0)
+  __shared__ float wt[2 * Q2][MB];
+  const int T = blockIdx.x, grp = blockIdx.y, j = threadIdx.x;
+  const bool tgt = j < Q;
+  const float4* sf[MB];
+  int valid = 0;
+#pragma unroll
+  for (int m = 0; m < MB; m++) {
+    const int jg = grp * MB + m;
+    sf[m] = jg < g.nmem ? g.mem[g.idx[jg]].fg.srcf : nullptr;
+    if (jg < g.nmem) valid |= 1 << m;
+  }
+  const double* ct = g.centre + 4 * (long)T;
+  const float4 self = tgt ? g.pxf[(long)T * Q + j] : make_float4(0.f, 0.f, 0.f, 0.f);
+  double ax[MB], ay[MB], az[MB];
+#pragma unroll
+  for (int m = 0; m < MB; m++) ax[m] = ay[m] = az[m] = 0;
+  const float feps = (float)g.eps;
+  const float2 eps2 = make_float2(feps, feps);
+  const int word = (grp * MB) >> 5, shift = (grp * MB) & 31;
+  for (int e = g.ustart[T]; e < g.ustart[T + 1]; e++) {
+    const int bits = (int)((__ldg(g.umask + (long)e * g.mw + word) >> shift) & ((1u << MB) - 1)) & valid;
+    if (!bits) continue;
+    const int S = __ldg(g.usrc + e);
+    const double* cs = g.centre + 4 * (long)S;
+    const float bx0 = (float)((cs[0] - ct[0]) * kPackScale), by0 = (float)((cs[1] - ct[1]) * kPackScale),
+                bz0 = (float)((cs[2] - ct[2]) * kPackScale);
+    __syncthreads();
+    if (j < Q2) {
+      const float4 s0 = g.pxf[(long)S * Q + 2 * j];
+      const float4 s1 = 2 * j + 1 < Q ? g.pxf[(long)S * Q + 2 * j + 1] : make_float4(0.f, 0.f, 0.f, 0.f);
+      tq[2 * j] = make_float4(s0.x, s1.x, s0.y, s1.y);
+      tq[2 * j + 1] = make_float4(s0.z, s1.z, 0.f, 0.f);
+    }
+    if (j < 2 * Q2) {
+#pragma unroll
+      for (int m = 0; m < MB; m++)
+        wt[j][m] = (j < Q && ((bits >> m) & 1)) ? sf[m][(long)S * Q + j].w : 0.f;
+    }
+    __syncthreads();
+    if (tgt) {
+      const float b0 = bx0 - self.x, b1 = by0 - self.y, b2 = bz0 - self.z;
+      const float2 bx = make_float2(b0, b0), by = make_float2(b1, b1), bz = make_float2(b2, b2);
+      float2 fx[MB / 2], fy[MB / 2], fz[MB / 2];
+#pragma unroll
+      for (int p = 0; p < MB / 2; p++) fx[p] = fy[p] = fz[p] = make_float2(0.f, 0.f);
+#pragma unroll 3
+      for (int k2 = 0; k2 < Q2; k2++) {
+        const float4 A = tq[2 * k2], B = tq[2 * k2 + 1];
+        const float2 dx = __fadd2_rn(bx, make_float2(A.x, A.y)), dy = __fadd2_rn(by, make_float2(A.z, A.w)),
+                     dz = __fadd2_rn(bz, make_float2(B.x, B.y));
+        const float2 den = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, eps2)));
+        float r0 = dev::recip_f32(den.x), r1 = dev::recip_f32(den.y);
+        if (GUARD) {
+          r0 = den.x > 0.0f ? r0 : 0.0f;
+          r1 = den.y > 0.0f ? r1 : 0.0f;
+        }
+        const float2* w0 = reinterpret_cast<const float2*>(&wt[2 * k2][0]);
+        const float2* w1 = reinterpret_cast<const float2*>(&wt[2 * k2 + 1][0]);
+#pragma unroll
+        for (int p = 0; p < MB / 2; p++) {
+          const float2 g0 = __fmul2_rn(w0[p], make_float2(r0, r0)), g1 = __fmul2_rn(w1[p], make_float2(r1, r1));
+          fx[p] = __ffma2_rn(g0, make_float2(dx.x, dx.x), fx[p]);
+          fy[p] = __ffma2_rn(g0, make_float2(dy.x, dy.x), fy[p]);
+          fz[p] = __ffma2_rn(g0, make_float2(dz.x, dz.x), fz[p]);
+          fx[p] = __ffma2_rn(g1, make_float2(dx.y, dx.y), fx[p]);
+          fy[p] = __ffma2_rn(g1, make_float2(dy.y, dy.y), fy[p]);
+          fz[p] = __ffma2_rn(g1, make_float2(dz.y, dz.y), fz[p]);
+        }
+      }
+#pragma unroll
+      for (int p = 0; p < MB / 2; p++) {
+        ax[2 * p] += (double)fx[p].x;
+        ay[2 * p] += (double)fy[p].x;
+        az[2 * p] += (double)fz[p].x;
+        ax[2 * p + 1] += (double)fx[p].y;
+        ay[2 * p + 1] += (double)fy[p].y;
+        az[2 * p + 1] += (double)fz[p].y;
+      }
+    }
+  }
+  if (!tgt) return;
+  const long pn = (long)g.Pf * Q, o = (long)T * Q + j;
+  const double px = g.px[o], py = g.px[pn + o], pz = g.px[2 * pn + o];
+#pragma unroll
+  for (int m = 0; m < MB; m++) {
+    if (!((valid >> m) & 1)) continue;
+    double* out = g.mem[g.idx[grp * MB + m]].ftgt;
+    out[o] = kBiotSavartPacked * (py * az[m] - pz * ay[m]);
+    out[pn + o] = kBiotSavartPacked * (pz * ax[m] - px * az[m]);
+    out[2 * pn + o] = kBiotSavartPacked * (px * ay[m] - py * ax[m]);
+  }
+}
+
+template <int Q>
+void launch_multi_q(const CcTcGroup& g, cudaStream_t st) {
+  constexpr int MB = kNearGroup, NT = (Q + 31) / 32 * 32;
+  const dim3 grid((unsigned)g.Pf, (unsigned)((g.nmem + MB - 1) / MB));
+  if (!(g.eps > 0)) SB_LAUNCH((k_cc_multi<Q, MB, true>), grid, NT, 0, st, g);
+  else SB_LAUNCH((k_cc_multi<Q, MB, false>), grid, NT, 0, st, g);
+}
+
 template <int Q, int S>
 void launch_q_s(const StepGeom& g, bool mixed, const int4* chunks, int nchunks, const double4* src, double* partial,
                 cudaStream_t st) {
@@ -262,6 +378,18 @@ void launch_cc_chunks(const StepGeom& g, int precision, int slots, const int4* c
   const long pn = (long)g.panels * g.q;
   SB_LAUNCH(k_cc_reduce, blocks_for(pn, 256), 256, 0, st, g, cstart, partial,
             mixed ? kBiotSavartPacked : kBiotSavart, out);
+}
+
+void launch_cc_multi(const CcTcGroup& g, cudaStream_t st) {
+  if (g.nmem <= 0 || !g.usrc) return;
+  switch (g.Q) {
+    case 36: launch_multi_q<36>(g, st); break;
+    case 49: launch_multi_q<49>(g, st); break;
+    case 64: launch_multi_q<64>(g, st); break;
+    case 81: launch_multi_q<81>(g, st); break;
+    case 100: launch_multi_q<100>(g, st); break;
+    default: launch_multi_q<121>(g, st); break;
+  }
 }
 
 void build_cc_chunks(const std::vector<int>& start, int chunk_len, std::vector<int4>& chunks,

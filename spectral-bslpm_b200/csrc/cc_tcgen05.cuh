@@ -54,6 +54,10 @@ void launch_cc_tc_pack(const CcTcGroup& g, cudaStream_t st);
 // D = A W for every target cluster and member, written as the members'
 // proxy-target velocities (fg.ftgt).  passes = 3 (3xTF32) or 1 (TF32).
 void launch_cc_tc(const CcTcGroup& g, int passes, cudaStream_t st);
+// The same interactions on the CUDA cores, the cluster pairs' distances and
+// reciprocals shared by groups of kNearGroup consecutive group members
+// (cc_chunks.cu; mixed precision; needs ustart/usrc/umask/pxf/centre/px).
+void launch_cc_multi(const CcTcGroup& g, cudaStream_t st);
 // Dynamic shared memory and tensor-memory columns of one CTA.
 size_t cc_tc_smem_bytes(int Q, int ntile, int passes, int maxlist, int mw);
 int cc_tc_tmem_cols(int Q, int ntile);
