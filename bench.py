@@ -363,7 +363,7 @@ def ensemble_bench(sb, torch, dev, flush, steps):
                      "near_ms": near_ms},
         "well_separated": {"headline_mode": "autotuned per proxy-degree group (CUDA-core float32 pairs per member, "
                                             "the tensor-core 3xTF32 GEMM over the group's members, or CUDA-core "
-                                            "pairs shared by groups of 8 members)",
+                                            "pairs shared by groups of 4 members)",
                            "groups": batch.cc_groups(), "union_cluster_pairs_per_eval": union_pairs,
                            "useful_proxy_pairs_per_eval": far_pairs, "mma_flops_per_eval_3xtf32": mma_flops,
                            "ms_per_step_cuda_core_pairs": ms_cuda_cores, "ms_per_step_tensor_core_3xtf32": ms_tc3,

@@ -362,7 +362,7 @@ sbslpm_status sbslpm_batch_pairs(const sbslpm_batch* batch, double* near_pairs, 
  * sbslpm_set_cc_tuning(ctx, 0, 0), with sbslpm_batch_set_stage0_shared(batch,
  * 0)), 1 = tensor-core GEMM over the members sharing a proxy
  * degree in 3xTF32, 2 = the same GEMM in one TF32 pass, 3 = CUDA-core
- * float32 pairs whose distances and reciprocals are shared by groups of 8
+ * float32 pairs whose distances and reciprocals are shared by groups of 4
  * theta-consecutive members of a degree group (the proxies never move, so a
  * cluster pair's geometry is the same for every member).  Float64 batches
  * accept mode 0 only.  sbslpm_batch_cc_info reports the mode, the union of

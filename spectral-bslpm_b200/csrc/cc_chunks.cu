@@ -196,6 +196,10 @@ __global__ void k_cc_reduce(StepGeom g, const int* __restrict__ cstart, const do
 // outside an entry's bits takes zero strength there.  Per member and source
 // cluster: float32 sums added into float64; every (target, member) of the
 // group is written (zeros without entries).
+// members per group of the shared well-separated kernel (4 measured faster
+// than 8 there: fewer registers, more resident blocks)
+constexpr int kCcGroup = 4;
+
 template <int Q, int MB, bool GUARD>
 __global__ void __launch_bounds__((Q + 31) / 32 * 32) k_cc_multi(CcTcGroup g) {
   constexpr int Q2 = (Q + 1) / 2;
@@ -295,7 +299,7 @@ __global__ void __launch_bounds__((Q + 31) / 32 * 32) k_cc_multi(CcTcGroup g) {
 
 template <int Q>
 void launch_multi_q(const CcTcGroup& g, cudaStream_t st) {
-  constexpr int MB = kNearGroup, NT = (Q + 31) / 32 * 32;
+  constexpr int MB = kCcGroup, NT = (Q + 31) / 32 * 32;
   const dim3 grid((unsigned)g.Pf, (unsigned)((g.nmem + MB - 1) / MB));
   if (!(g.eps > 0)) SB_LAUNCH((k_cc_multi<Q, MB, true>), grid, NT, 0, st, g);
   else SB_LAUNCH((k_cc_multi<Q, MB, false>), grid, NT, 0, st, g);

@@ -55,7 +55,7 @@ void launch_cc_tc_pack(const CcTcGroup& g, cudaStream_t st);
 // proxy-target velocities (fg.ftgt).  passes = 3 (3xTF32) or 1 (TF32).
 void launch_cc_tc(const CcTcGroup& g, int passes, cudaStream_t st);
 // The same interactions on the CUDA cores, the cluster pairs' distances and
-// reciprocals shared by groups of kNearGroup consecutive group members
+// reciprocals shared by groups of 4 consecutive group members
 // (cc_chunks.cu; mixed precision; needs ustart/usrc/umask/pxf/centre/px).
 void launch_cc_multi(const CcTcGroup& g, cudaStream_t st);
 // Dynamic shared memory and tensor-memory columns of one CTA.
