@@ -551,9 +551,9 @@ def main():
     ap.add_argument("--profile", choices=["treecode", "treecode64", "spectral", "swe", "swe64", "ensemble"],
                     help="run --warmup + --steps steps of one path and exit (for profiler captures; no timing)")
     ap.add_argument("--members", type=int, default=ENS_MEMBERS, help="ensemble members in --profile ensemble")
-    ap.add_argument("--cc-mode", type=int, default=1, choices=[0, 1, 2],
-                    help="--profile ensemble: well-separated interactions, 0 CUDA-core pairs, 1 tensor-core "
-                         "3xTF32, 2 tensor-core TF32")
+    ap.add_argument("--cc-mode", type=int, default=3, choices=[0, 1, 2, 3],
+                    help="--profile ensemble: well-separated interactions, 0 CUDA-core pairs per member, "
+                         "1 tensor-core 3xTF32, 2 tensor-core TF32, 3 CUDA-core pairs shared by member groups")
     ap.add_argument("--near-shape", default="128,2,4",
                     help="--profile treecode/treecode64: near-field threads,targets per thread,splits")
     ap.add_argument("--cc-shape", default="3,3",
