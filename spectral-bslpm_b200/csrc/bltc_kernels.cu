@@ -300,8 +300,12 @@ __device__ __forceinline__ void bltc_near32_body(const TreeGeom& tg, const StepG
   }
 }
 
+// 256-thread shapes are held to 64 registers (four blocks per SM): on the
+// 393,216-particle treecode the (256 x 1) shape then ran 535 us per launch
+// against 555 us uncapped; the smaller shapes measured slower when capped, so
+// they keep their registers.  The autotuner chooses among all of them.
 template <int NT, int TPT, bool GUARD>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, NT >= 256 ? 4 : 1)
     k_bltc_near32_batch(const BatchMember* __restrict__ mem, const double* __restrict__ x,
                         const double* __restrict__ y, const double* __restrict__ z,
                         const float4* __restrict__ psrcf, double* __restrict__ out) {
