@@ -113,6 +113,25 @@ def test_stage0_shared_near_field_matches_per_member(sb):
         assert rel(v, r) <= 1e-6 and rel(vel, rel_) <= 1e-6
 
 
+@pytest.mark.parametrize("members", [1, 5])
+def test_sharing_modes_with_partial_groups(sb, members):
+    """One member, and five (a group of 4 plus a group of 1 in the shared
+    well-separated kernel, one partial group of 8 in the stage-0 near field):
+    the member-sharing modes against the per-member ones, within 1e-6."""
+    g, xyza, vors = grid_and_vors(sb, members)
+    theta = [0.5, 0.8, 0.65, 0.7, 0.55][:members]
+    pdeg = [8] * members
+    out = []
+    for shared in (False, True):
+        batch = sb.Batch(base_cfg(sb, sb.MIXED), theta, pdeg)
+        batch.set_tuning(128, 2, 2)
+        batch.set_cc_mode(batch.CC_SHARED if shared else batch.CC_CUDA_CORES)
+        batch.set_stage0_shared(shared)
+        out.append(batch_step(sb, batch, xyza, vors))
+    assert rel(out[1][0], out[0][0]) <= 1e-6
+    assert rel(out[1][1], out[0][1]) <= 1e-6
+
+
 def test_stage0_shared_refused_in_float64(sb):
     g, xyza, vors = grid_and_vors(sb, 2)
     batch = sb.Batch(base_cfg(sb, sb.FP64), THETA[:2], PDEG[:2])
