@@ -383,7 +383,7 @@ __global__ void __launch_bounds__(NT)
       float2 fx[MB / 2], fy[MB / 2], fz[MB / 2];
 #pragma unroll
       for (int p = 0; p < MB / 2; p++) fx[p] = fy[p] = fz[p] = make_float2(0.f, 0.f);
-#pragma unroll 2
+#pragma unroll 4
       for (int k2 = 0; k2 < npl2; k2++) {
         const float4 A = tq[2 * k2], B = tq[2 * k2 + 1];
         const float2 dx = __fadd2_rn(bx, make_float2(A.x, A.y)), dy = __fadd2_rn(by, make_float2(A.z, A.w)),

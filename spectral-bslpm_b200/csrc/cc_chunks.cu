@@ -104,7 +104,7 @@ __global__ void __launch_bounds__(CcShape<Q, S>::NT)
       const float2 bx = make_float2(b0, b0), by = make_float2(b1, b1), bz = make_float2(b2, b2);
       float2 fx = make_float2(0.f, 0.f), fy = fx, fz = fx;
       const float4* tb = tile[h];
-#pragma unroll 4
+#pragma unroll 8
       for (int k2 = 0; k2 < Q2; k2++) {
         const float4 A = tb[2 * k2], B = tb[2 * k2 + 1];
         pair32x2<GUARD>(bx, by, bz, make_float2(A.x, A.y), make_float2(A.z, A.w), make_float2(B.x, B.y),
@@ -249,7 +249,7 @@ __global__ void __launch_bounds__((Q + 31) / 32 * 32) k_cc_multi(CcTcGroup g) {
       float2 fx[MB / 2], fy[MB / 2], fz[MB / 2];
 #pragma unroll
       for (int p = 0; p < MB / 2; p++) fx[p] = fy[p] = fz[p] = make_float2(0.f, 0.f);
-#pragma unroll 3
+#pragma unroll 6
       for (int k2 = 0; k2 < Q2; k2++) {
         const float4 A = tq[2 * k2], B = tq[2 * k2 + 1];
         const float2 dx = __fadd2_rn(bx, make_float2(A.x, A.y)), dy = __fadd2_rn(by, make_float2(A.z, A.w)),
