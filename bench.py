@@ -44,7 +44,7 @@ METRIC = "BVE RK4 steps/s at ≤1e-6 rel vort err: mixed+batched vs FP64 plain, 
 LEVELS, DEGREE, THETA, EPS, OMEGA, DT = 7, 3, 0.7, 1e-4, 2 * np.pi, 0.005
 PROXY_DEGREE, LEAF_SIZE = 8, 256
 PAIR_FLOP = 17  # FLOP per Biot-Savart pair (division counted as 1)
-NEAR_TRAFFIC = 15.889664e6 + 0.385792e6  # DRAM bytes of one near-field launch, from the committed ncu capture
+NEAR_TRAFFIC = 15.889920e6 + 0.548096e6  # DRAM bytes of one near-field launch, from the committed ncu capture
 
 
 def workload_config():
