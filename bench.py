@@ -44,7 +44,18 @@ METRIC = "BVE RK4 steps/s at ≤1e-6 rel vort err: mixed+batched vs FP64 plain, 
 LEVELS, DEGREE, THETA, EPS, OMEGA, DT = 7, 3, 0.7, 1e-4, 2 * np.pi, 0.005
 PROXY_DEGREE, LEAF_SIZE = 8, 256
 PAIR_FLOP = 17  # FLOP per Biot-Savart pair (division counted as 1)
-NEAR_TRAFFIC = 15.889920e6 + 0.548096e6  # DRAM bytes of one near-field launch, from the committed ncu capture
+# DRAM bytes (read + write) of one near-field launch at this workload, from an
+# ncu capture of one launch (dram__bytes_read.sum + dram__bytes_write.sum)
+NEAR_TRAFFIC = 15.889920e6 + 0.548096e6
+# The reference's own method (its spectral FMM, proxy degree = particle degree
+# 3, float64) meets the 1e-6 vorticity bar on this workload from theta 0.45
+# down (theta 0.5: 1.35e-6, 0.45: 6.3e-7 after one step against the float64
+# direct sum, measured with this library's float64 path of the same method,
+# which matches the reference's step to 1e-12); the reference arm and the CPU
+# baseline run it there.
+REF_THETA_AT_BAR, REF_ERR_AT_BAR = 0.45, 6.3e-7
+BAR = 1e-6
+AT_BAR_LEAVES, AT_BAR_DEGREES, AT_BAR_THETAS = (64, 256), (4, 5, 6, 7, 8), (0.9, 0.8, 0.7, 0.6, 0.5)
 
 
 def workload_config():
@@ -53,6 +64,19 @@ def workload_config():
             "particles": 6 * 4 ** (LEVELS - 1) * (DEGREE + 1) ** 2, "levels": LEVELS, "interp_degree": DEGREE,
             "theta": THETA, "proxy_degree": PROXY_DEGREE, "leaf_size": LEAF_SIZE, "kernel_eps": EPS, "omega": OMEGA,
             "dt": DT, "precision": "mixed (f32 pairs, f64 positions/remap)", "l2": "flushed between timed steps"}
+
+
+def reference_config():
+    """The reference arm's configuration: the same workload, run with the
+    reference's own method at the largest theta where it meets the bar."""
+    return {"workload": "BVE RK4, 393,216 particles (6x64x64 panels x 4x4 points), RH4 IC, the reference's "
+                        "spectral FMM (proxies = the 4x4 particle points, interp_degree 3), float64, theta 0.45",
+            "particles": 6 * 4 ** (LEVELS - 1) * (DEGREE + 1) ** 2, "levels": LEVELS, "interp_degree": DEGREE,
+            "theta": REF_THETA_AT_BAR, "kernel_eps": EPS, "omega": OMEGA, "dt": DT, "precision": "float64",
+            "rel_linf_vort_step1_vs_fp64_direct": REF_ERR_AT_BAR,
+            "why_theta": "the largest theta of {0.5, 0.45, 0.4} at which the reference's method meets the 1e-6 "
+                         "bar of the metric (0.5: 1.35e-6); the error is that of this library's float64 path of "
+                         "the same method, which matches the reference's step to 1e-12"}
 
 
 def import_package():
@@ -141,9 +165,10 @@ class ClockSampler:
 def run_reference(args, rank):
     if rank != 0:
         return
+    warm = min(args.warmup, 2)  # each warm-up step is a full CPU step (about 10 s on 16 threads)
     out = subprocess.run([sys.executable, "-m", "oracle.cpu_baseline", "--levels", str(LEVELS), "--theta",
-                          str(THETA), "--steps", str(args.steps), "--warmup", str(min(args.warmup, 1)),
-                          "--budget-s", "200"], cwd=ROOT, capture_output=True, text=True)
+                          str(REF_THETA_AT_BAR), "--steps", str(args.steps), "--warmup", str(warm),
+                          "--budget-s", "150"], cwd=ROOT, capture_output=True, text=True)
     if out.returncode != 0:
         print(json.dumps({"impl": "reference", "unavailable": "reference CPU step failed: " +
                           (out.stderr.strip().splitlines() or ["?"])[-1]}))
@@ -151,11 +176,12 @@ def run_reference(args, rank):
     r = json.loads(out.stdout.strip().splitlines()[-1])
     v = r["steps_per_s"]
     sample = (f"{r['steps_timed']} full bve_back_rk4_step calls of the {r['particles']}-particle problem "
-              f"(median), reference spectral FMM (interp_degree 3 proxies), float64")
+              f"(median) after {warm} warm-up steps, reference spectral FMM (interp_degree 3 proxies) at theta "
+              f"{REF_THETA_AT_BAR}, float64")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": args.gpus,
-        "steps": r["steps_timed"], "warmup": min(args.warmup, 1), "ms_per_step": 1e3 / v, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload_config(),
+        "steps": r["steps_timed"], "warmup": warm, "ms_per_step": 1e3 / v, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": reference_config(),
         "cpu_baseline": {"value": v, "unit": "steps/s", "cores": r["threads"], "kind": r["kind"], "sample": sample,
                          "cpu": r["cpu"]},
         "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -504,6 +530,58 @@ def adjoint_bench(sb, torch, dev, directions=8):
                                    "checkpoints", "h": 1e-6}}
 
 
+def at_bar_search(sb, torch, dev, g, vor0, ref1, ref50, flush, steps, headline_sps):
+    """The fastest treecode setting that meets the metric's bar on the
+    workload.  For each precision, leaf size (64, 256) and proxy degree
+    (4..8): the largest theta of (0.9 .. 0.5) whose vorticity after one step
+    and after 50 steps is within 1e-6 (relative L-infinity) of the float64
+    direct sum's; each such setting is then timed like the headline (first-step
+    autotuning, L2 flushed between timed steps).  Returns every setting tried,
+    the fastest per precision and their ratio."""
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    s1 = ref1.abs().max().item()
+    s50 = ref50.abs().max().item() if ref50 is not None else None
+    rows, best = [], {}
+    for pname, prec in (("mixed", sb.MIXED), ("fp64", sb.FP64)):
+        for leaf in AT_BAR_LEAVES:
+            for n in AT_BAR_DEGREES:
+                for th in AT_BAR_THETAS:
+                    ctx = sb.Context(sb.config_default(levels=LEVELS, interp_degree=DEGREE, fmm_theta=th,
+                                                       kernel_eps=EPS, omega=OMEGA, dt=DT, precision=prec,
+                                                       proxy_degree=n, leaf_size=leaf))
+                    f = [T(g.x), T(g.y), T(g.z), T(g.area), T(vor0), *[torch.zeros_like(T(g.x)) for _ in range(3)],
+                         None]
+                    ctx.bve_run(*f, nsteps=1)
+                    row = {"precision": pname, "leaf_size": leaf, "proxy_degree": n, "theta": th,
+                           "rel_linf_vort_step1": (f[4] - ref1).abs().max().item() / s1}
+                    ok = row["rel_linf_vort_step1"] <= BAR
+                    if ok and s50 is not None:
+                        ctx.bve_run(*f, nsteps=49)
+                        row["rel_linf_vort_step50"] = (f[4] - ref50).abs().max().item() / s50
+                        ok = row["rel_linf_vort_step50"] <= BAR
+                    row["meets_bar"] = ok
+                    if ok:
+                        f[4].copy_(T(vor0))
+                        ctx.bve_run(*f, nsteps=2)
+                        ts = timed_steps(torch, ctx, f, steps, flush)
+                        row["steps_per_s"] = 1e3 / (sum(ts) / len(ts))
+                        if pname not in best or row["steps_per_s"] > best[pname]["steps_per_s"]:
+                            best[pname] = row
+                    rows.append(row)
+                    del ctx, f
+                    if ok:
+                        break  # smaller theta only adds work at this leaf size and degree
+    m, d = best.get("mixed"), best.get("fp64")
+    return {"bar": BAR, "criterion": "vorticity within 1e-6 (relative L-infinity) of the float64 direct sum after "
+                                     "1 and after 50 steps" if s50 is not None else "after 1 step (no 50-step run)",
+            "grid": {"leaf_size": list(AT_BAR_LEAVES), "proxy_degree": list(AT_BAR_DEGREES),
+                     "theta": list(AT_BAR_THETAS)},
+            "mixed": m, "fp64": d,
+            "speedup_mixed_vs_fp64_at_bar": m["steps_per_s"] / d["steps_per_s"] if m and d else None,
+            "mixed_vs_headline_setting": m["steps_per_s"] / headline_sps if m else None,
+            "tried": rows}
+
+
 def replica_vorticity(vor0, z, rank, world):
     """The replica of rank `rank`: with one rank the benchmark state itself,
     with several an independent ensemble member (seeded perturbation)."""
@@ -548,6 +626,8 @@ def main():
     ap.add_argument("--no-swe", action="store_true", help="skip the shallow-water measurement")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble measurement")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint measurement")
+    ap.add_argument("--no-at-bar", action="store_true",
+                    help="skip the search for the fastest treecode settings that meet the 1e-6 bar")
     ap.add_argument("--profile", choices=["treecode", "treecode64", "spectral", "swe", "swe64", "ensemble"],
                     help="run --warmup + --steps steps of one path and exit (for profiler captures; no timing)")
     ap.add_argument("--members", type=int, default=ENS_MEMBERS, help="ensemble members in --profile ensemble")
@@ -658,7 +738,7 @@ def main():
     del ctxd
 
     # ---- accuracy after 50 steps vs the float64 direct sum (every rank: replicas) ----
-    acc50 = None
+    acc50, ref50 = None, None
     if not args.no_step50:
         ctxd = ctx_for(sb.FP64, sb.VEL_DIRECT, proxy=0)
         fd = fields()
@@ -671,6 +751,10 @@ def main():
             c.bve_run(*fa, nsteps=50)
             acc50[name] = {"rel_linf_vort": (fa[4] - ref50).abs().max().item() / scale50}
         del ctxd
+
+    # ---- the fastest treecode settings that meet the bar ---------------------
+    at_bar = None if args.no_at_bar else at_bar_search(sb, torch, dev, g, vor0, ref, ref50, flush, args.steps,
+                                                       value / world)
 
     # ---- the plain direct-sum configuration: 24,576 particles, 100 steps ----
     g5 = sb.build_grid(5, DEGREE, exact_cc=True)
@@ -764,13 +848,16 @@ def main():
     # ---- CPU baseline: the reference's own step on the host cores ----------
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        out = subprocess.run([sys.executable, "-m", "oracle.cpu_baseline", "--levels", str(LEVELS), "--steps", "1",
-                              "--warmup", "0", "--budget-s", "60"], cwd=ROOT, capture_output=True, text=True)
+        out = subprocess.run([sys.executable, "-m", "oracle.cpu_baseline", "--levels", str(LEVELS), "--theta",
+                              str(REF_THETA_AT_BAR), "--steps", "3", "--warmup", "1", "--budget-s", "60"],
+                             cwd=ROOT, capture_output=True, text=True)
         if out.returncode == 0:
             r = json.loads(out.stdout.strip().splitlines()[-1])
             cpu = {"value": r["steps_per_s"], "unit": "steps/s", "cores": r["threads"], "kind": r["kind"],
-                   "sample": f"1 full bve_back_rk4_step of the {r['particles']}-particle problem (reference "
-                             f"spectral FMM, float64), {r['threads']} OpenMP threads", "cpu": r["cpu"]}
+                   "sample": f"median of {r['steps_timed']} full bve_back_rk4_step calls after 1 warm-up step, "
+                             f"{r['particles']}-particle problem, reference spectral FMM at theta "
+                             f"{REF_THETA_AT_BAR} (its largest theta at the 1e-6 bar), float64, {r['threads']} "
+                             f"OpenMP threads", "cpu": r["cpu"], "config": reference_config()}
         else:
             cpu = {"value": None, "unit": "steps/s", "cores": os.cpu_count(), "kind": "reference",
                    "sample": "failed: " + (out.stderr.strip().splitlines() or ["?"])[-1]}
@@ -788,8 +875,8 @@ def main():
                          "launch_shape": {"threads": tune32[0], "targets_per_thread": tune32[1],
                                           "splits": tune32[2], "candidates_timed": tune32[3]},
                          "achieved": achieved, "peak": peak_meas, "unit": "TFLOP/s", "frac": achieved / peak_meas,
-                         "traffic": NEAR_TRAFFIC, "traffic_source": "profiles/k_bltc_near32_batch_levels7.md "
-                         "(dram__bytes_read.sum + dram__bytes_write.sum of one launch)",
+                         "traffic": NEAR_TRAFFIC, "traffic_source": "ncu capture of one launch of this kernel on "
+                         "this workload (dram__bytes_read.sum + dram__bytes_write.sum)",
                          "flop_per_pair": PAIR_FLOP, "pairs_per_launch": pairs,
                          "ms_per_launch": ms_int, "step_share": share,
                          "peak_source": "measured f32 FMA-chain throughput on this GPU (sbslpm_measure_fma_peak); "
@@ -827,6 +914,7 @@ def main():
                 if mixed_at_bar and plain_at_bar else None},
             "accuracy_step1_vs_fp64_direct": dict(acc, direct_step_s=direct_s),
             "accuracy_step50_vs_fp64_direct": acc50,
+            "at_bar": at_bar,
             "direct_sum_levels5": direct5,
             "ensemble": ens, "adjoint": adj, "swe": swe, "cpu_baseline": cpu, "clocks": clk.summary(),
         }

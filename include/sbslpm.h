@@ -464,10 +464,13 @@ sbslpm_status sbslpm_direct_sum_inv_lap(long n, const double* x, const double* y
  * nothing: its scratch is one fixed 16 MiB array compiled into the library,
  * which each GPU that loads the library holds until the process exits.
  * Limit: n_targets <= 699,050 (3 * n_targets doubles of scratch); larger
- * calls return SBSLPM_ERR_ARG with a message and do nothing.  The first call
- * on each device looks the array's device address up (cudaGetSymbolAddress,
- * with that device current), so make that first call before any stream
- * capture.  Every call on a device shares the one array and each call
+ * calls return SBSLPM_ERR_ARG with a message and do nothing.  Results equal
+ * sbslpm_direct_sum_bve's up to summation order: from about 100,000 targets
+ * the scratch holds fewer source groups than that entry point would use.
+ * The first call on each device looks the array's device address up
+ * (cudaGetSymbolAddress, with that device current) and keeps it, so make
+ * that first call before any stream capture, and do not reset the device
+ * (cudaDeviceReset) while the library is in use.  Every call on a device shares the one array and each call
  * overwrites the parts it uses, so calls whose kernels overlap on the GPU
  * (different streams or host threads) race: serialise them.  Synchronises
  * the stream before returning. */

@@ -324,12 +324,13 @@ long orc_dual_tree_traversal(int levels, const orc_panel* p, double theta, int* 
 
 /* interp_vals_bli: src/interp_funcs_impl.hpp:11-112.  Out-of-panel input sets
  * the oracle error flag (the reference aborts). */
-void orc_interp_vals_bli(double* basis, double xi, double eta, double min_xi, double max_xi, double min_eta,
-                         double max_eta, int d) {
+static void bli_core(double* basis, double xi, double eta, double min_xi, double max_xi, double min_eta,
+                     double max_eta, int d, int check) {
   double xi_range = 0.5 * (max_xi - min_xi), xi_offset = 0.5 * (max_xi + min_xi);
   double eta_range = 0.5 * (max_eta - min_eta), eta_offset = 0.5 * (max_eta + min_eta);
   double cheb_xi[11], cheb_eta[11], w[11], fx[11], fe[11], val;
-  if (xi < min_xi - 1e-15 || xi > max_xi + 1e-15 || eta < min_eta - 1e-15 || eta > max_eta + 1e-15) g_orc_error = 1;
+  if (check && (xi < min_xi - 1e-15 || xi > max_xi + 1e-15 || eta < min_eta - 1e-15 || eta > max_eta + 1e-15))
+    g_orc_error = 1;
   for (int i = 0; i < (d + 1) * (d + 1); i++) basis[i] = 0.0;
   if (d == 0) {
     cheb_xi[0] = xi_offset;
@@ -380,6 +381,11 @@ void orc_interp_vals_bli(double* basis, double xi, double eta, double min_xi, do
   }
   for (int i = 0; i < d + 1; i++)
     for (int j = 0; j < d + 1; j++) basis[i * (d + 1) + j] = fx[i] * fe[j];
+}
+
+void orc_interp_vals_bli(double* basis, double xi, double eta, double min_xi, double max_xi, double min_eta,
+                         double max_eta, int d) {
+  bli_core(basis, xi, eta, min_xi, max_xi, min_eta, max_eta, d, 1);
 }
 
 /* point_locate_panel: src/interp_funcs_impl.hpp:114-142 */
@@ -559,6 +565,325 @@ void orc_bve_direct_velocity(int levels, int degree, const orc_panel* p, const d
     for (int s = off; s < P; s++) bve_pair_block(p, interp, q, t, s, disp_x, disp_y, disp_z, source, eps, t1, t2, t3);
 }
 
+/* ---------------- treecode with decoupled proxy degree (Mode C) ----------
+ *
+ * The reference's irregular-point FMM (the "_ll" functions) applied to the
+ * particle grid: a cubed-sphere quadtree of tree_levels levels whose leaves
+ * hold npl particles each (the particles of the leaf's descendant grid panels,
+ * which are consecutive in the [leaf panel][q] arrays), (n+1)^2 Chebyshev
+ * proxies of degree n on every tree panel at fixed positions, and bounds in
+ * radians as in initialize_cube_sphere_irreg_points
+ * (src/initialize_cubed_sphere.cpp:446-592).
+ *
+ *   upward     base_pots_ll + child_to_parent_ll (src/fmm_funcs_impl.hpp:190-268,
+ *              src/fmm_funcs.cpp:394-405)
+ *   list       dual_tree_traversal_irreg (src/fmm_funcs.cpp:125-231): the
+ *              FIFO traversal of orc_dual_tree_traversal on the tree panels
+ *   pairs      swe_vel_panel_interaction_ll (src/fmm_interactions/swe_vel_impl.hpp:180-287),
+ *              rotational part (zero divergence), typed pp / pc / cp / cc
+ *   downward   parent_to_child_3_ll + child_panel_interp_3_ll
+ *              (src/fmm_funcs_impl.hpp:270-364, src/fmm_funcs.cpp:407-419)
+ *
+ * typed = 1 follows the reference's typing: a well-separated pair uses the
+ * particles of a side whose panel is at the deepest tree level and the
+ * proxies otherwise (pp, pc, cp, cc).  typed = 0 evaluates every
+ * well-separated pair proxy x proxy (the design of this library's treecode).
+ * Pairs that fail the MAC are leaf pairs, particle x particle, in both.
+ * Sources may be displaced (positions off the grid): they are anterpolated in
+ * the coordinates of their own leaf's face with the barycentric formula
+ * extended past the leaf, where the reference would stop (Kokkos::abort,
+ * src/interp_funcs_impl.hpp:22-33); for particles on the grid the two agree. */
+
+typedef struct {
+  int L, d, q, n, n1, qx, npl, Lf, Pf, Af, offf;
+  orc_panel* tp;
+  double* px; /* [Pf][qx][3] proxy positions */
+} bltc_tree;
+
+/* tree levels: panels are split while they hold more than leaf_size
+ * particles (src/initialize_cubed_sphere.cpp:473-474) */
+static void bltc_tree_init(int levels, int degree, int leaf_size, int n, bltc_tree* t) {
+  t->L = levels;
+  t->d = degree;
+  t->q = (degree + 1) * (degree + 1);
+  t->n = n;
+  t->n1 = n + 1;
+  t->qx = t->n1 * t->n1;
+  int m = 0;
+  long npl = t->q;
+  while (npl * 4 <= leaf_size && m < levels - 1) {
+    npl *= 4;
+    m++;
+  }
+  t->npl = (int)npl;
+  t->Lf = levels - m;
+  t->Pf = orc_panel_count(t->Lf);
+  t->Af = orc_leaf_count(t->Lf);
+  t->offf = t->Pf - t->Af;
+  t->tp = (orc_panel*)malloc(sizeof(orc_panel) * (size_t)t->Pf);
+  orc_panels_init(t->Lf, t->tp);
+  t->px = (double*)malloc(sizeof(double) * 3 * (size_t)t->Pf * t->qx);
+  for (int p = 0; p < t->Pf; p++) {
+    /* proxy (j, k): xi = cos(pi j/n) xi_scale + xi_off (swe_vel_impl.hpp:227-240) */
+    double mn = ORC_PI / 4.0 * t->tp[p].min_xi, mx = ORC_PI / 4.0 * t->tp[p].max_xi;
+    double me = ORC_PI / 4.0 * t->tp[p].min_eta, xe = ORC_PI / 4.0 * t->tp[p].max_eta;
+    double xi_off = 0.5 * (mn + mx), xi_scale = 0.5 * (mx - mn), eta_off = 0.5 * (me + xe),
+           eta_scale = 0.5 * (xe - me);
+    for (int j = 0; j < t->n1; j++)
+      for (int k = 0; k < t->n1; k++) {
+        double xi = cos(ORC_PI * j / n) * xi_scale + xi_off, eta = cos(ORC_PI * k / n) * eta_scale + eta_off;
+        xyz_from_xieta(xi, eta, t->tp[p].face, t->px + 3 * ((size_t)p * t->qx + j * t->n1 + k));
+      }
+  }
+}
+
+static void bltc_tree_free(bltc_tree* t) {
+  free(t->tp);
+  free(t->px);
+}
+
+static void panel_rad(const orc_panel* p, double* b) {
+  b[0] = ORC_PI / 4.0 * p->min_xi;
+  b[1] = ORC_PI / 4.0 * p->max_xi;
+  b[2] = ORC_PI / 4.0 * p->min_eta;
+  b[3] = ORC_PI / 4.0 * p->max_eta;
+}
+
+/* interp_vals_bli (src/interp_funcs_impl.hpp:11-112) without its range check
+ * when check == 0. */
+static void bli2(double* basis, double xi, double eta, const double* b, int d, int check) {
+  bli_core(basis, xi, eta, b[0], b[1], b[2], b[3], d, check);
+}
+
+void orc_bltc_shape(int levels, int degree, int leaf_size, int* tree_levels, int* npl) {
+  int m = 0;
+  long n = (degree + 1) * (degree + 1);
+  while (n * 4 <= leaf_size && m < levels - 1) {
+    n *= 4;
+    m++;
+  }
+  *tree_levels = levels - m;
+  *npl = (int)n;
+}
+
+/* base_pots_ll (src/fmm_funcs_impl.hpp:190-222) at the sources' positions
+ * (leaf face, extended basis), then child_to_parent_ll level by level
+ * (src/fmm_funcs_impl.hpp:224-268; src/fmm_funcs.cpp:394-405): each parent
+ * adds its children in id order, child nodes (j, k) in order. */
+static void bltc_upward(const bltc_tree* t, const double* sx, const double* sy, const double* sz, const double* w,
+                        double* S) {
+  int qx = t->qx, n = t->n;
+  memset(S, 0, sizeof(double) * (size_t)t->Pf * qx);
+#pragma omp parallel for schedule(static)
+  for (int f = 0; f < t->Af; f++) {
+    int pn = t->offf + f;
+    double b[4], bas[MAXQ], xe[2];
+    panel_rad(&t->tp[pn], b);
+    for (int k = 0; k < t->npl; k++) {
+      size_t i = (size_t)f * t->npl + k;
+      xieta_from_xyz_face(sx[i], sy[i], sz[i], t->tp[pn].face, xe);
+      bli2(bas, xe[0], xe[1], b, n, 0);
+      for (int m = 0; m < qx; m++) S[(size_t)pn * qx + m] += bas[m] * w[i];
+    }
+  }
+  for (int lev = t->Lf - 1; lev >= 1; lev--) {
+    int plo = level_start(lev - 1), phi = level_start(lev);
+#pragma omp parallel for schedule(static)
+    for (int par = plo; par < phi; par++) {
+      double bp[4], bc[4], bas[MAXQ];
+      panel_rad(&t->tp[par], bp);
+      for (int c = 0; c < 4; c++) {
+        int ch = t->tp[par].child[c];
+        panel_rad(&t->tp[ch], bc);
+        double xi_off = 0.5 * (bc[0] + bc[1]), xi_scale = 0.5 * (bc[1] - bc[0]);
+        double eta_off = 0.5 * (bc[2] + bc[3]), eta_scale = 0.5 * (bc[3] - bc[2]);
+        for (int j = 0; j < t->n1; j++)
+          for (int k = 0; k < t->n1; k++) {
+            double xi = cos(ORC_PI / n * j) * xi_scale + xi_off, eta = cos(ORC_PI / n * k) * eta_scale + eta_off;
+            bli2(bas, xi, eta, bp, n, 1);
+            double v = S[(size_t)ch * qx + j * t->n1 + k];
+            for (int m = 0; m < qx; m++) S[(size_t)par * qx + m] += bas[m] * v;
+          }
+      }
+    }
+  }
+}
+
+/* parent_to_child_3_ll level by level, then child_panel_interp_3_ll at the
+ * targets (src/fmm_funcs_impl.hpp:270-364): T (3 x Pf x qx) in place, u
+ * (3 x N) accumulated term by term. */
+static void bltc_downward(const bltc_tree* t, const double* tx, const double* ty, const double* tz, double* T,
+                          double* u) {
+  int qx = t->qx, n = t->n;
+  size_t pn = (size_t)t->Pf * qx, N = (size_t)t->Af * t->npl;
+  for (int lev = 0; lev < t->Lf - 1; lev++) {
+    int plo = level_start(lev), phi = level_start(lev + 1);
+#pragma omp parallel for schedule(static)
+    for (int par = plo; par < phi; par++) {
+      double bp[4], bc[4], bas[MAXQ];
+      panel_rad(&t->tp[par], bp);
+      for (int c = 0; c < 4; c++) {
+        int ch = t->tp[par].child[c];
+        panel_rad(&t->tp[ch], bc);
+        double xi_off = 0.5 * (bc[0] + bc[1]), xi_scale = 0.5 * (bc[1] - bc[0]);
+        double eta_off = 0.5 * (bc[2] + bc[3]), eta_scale = 0.5 * (bc[3] - bc[2]);
+        for (int k = 0; k < qx; k++) {
+          int k1 = k / t->n1, k2 = k % t->n1;
+          double xi = cos(ORC_PI / n * k1) * xi_scale + xi_off, eta = cos(ORC_PI / n * k2) * eta_scale + eta_off;
+          bli2(bas, xi, eta, bp, n, 1);
+          for (int f = 0; f < 3; f++) {
+            double a = T[f * pn + (size_t)ch * qx + k];
+            for (int l = 0; l < qx; l++) a += bas[l] * T[f * pn + (size_t)par * qx + l];
+            T[f * pn + (size_t)ch * qx + k] = a;
+          }
+        }
+      }
+    }
+  }
+#pragma omp parallel for schedule(static)
+  for (int f = 0; f < t->Af; f++) {
+    int pnl = t->offf + f;
+    double b[4], bas[MAXQ], xe[2];
+    panel_rad(&t->tp[pnl], b);
+    for (int j = 0; j < t->npl; j++) {
+      size_t i = (size_t)f * t->npl + j;
+      xieta_from_xyz_face(tx[i], ty[i], tz[i], t->tp[pnl].face, xe);
+      bli2(bas, xe[0], xe[1], b, n, 1);
+      for (int c = 0; c < 3; c++) {
+        double a = u[c * N + i];
+        for (int k = 0; k < qx; k++) a += bas[k] * T[c * pn + (size_t)pnl * qx + k];
+        u[c * N + i] = a;
+      }
+    }
+  }
+}
+
+/* The MAC of dual_tree_traversal_irreg (src/fmm_funcs.cpp:149-162), with the
+ * same arithmetic as orc_dual_tree_traversal. */
+static int bltc_well_separated(const orc_panel* p, int t, int s, double theta) {
+  double xi1 = ORC_PI / 4.0 * 0.5 * (p[t].min_xi + p[t].max_xi);
+  double xi2 = ORC_PI / 4.0 * 0.5 * (p[s].min_xi + p[s].max_xi);
+  double eta1 = ORC_PI / 4.0 * 0.5 * (p[t].min_eta + p[t].max_eta);
+  double eta2 = ORC_PI / 4.0 * 0.5 * (p[s].min_eta + p[s].max_eta);
+  double c1[3], c2[3];
+  xyz_from_xieta(xi1, eta1, p[t].face, c1);
+  xyz_from_xieta(xi2, eta2, p[s].face, c2);
+  double dist = gcdist(c1, c2), sep = 100;
+  if (dist > 1e-16) sep = (p[t].radius + p[s].radius) / dist;
+  return sep < theta;
+}
+
+/* One list entry of swe_vel_panel_interaction_ll, rotational part
+ * (src/fmm_interactions/swe_vel_impl.hpp:256-284): targets j in order, sources
+ * k in order; out receives 3 strided sums per target. */
+static void bltc_block(int nt, const double* txyz, size_t tstride, const double* tx, const double* ty,
+                       const double* tz, int ns, const double* sxyz, const double* sx, const double* sy,
+                       const double* sz, const double* sv, double eps, double* o1, double* o2, double* o3) {
+  for (int j = 0; j < nt; j++) {
+    double x_t = txyz ? txyz[3 * j] : tx[j], y_t = txyz ? txyz[3 * j + 1] : ty[j], z_t = txyz ? txyz[3 * j + 2] : tz[j];
+    double a1 = o1[j * tstride], a2 = o2[j * tstride], a3 = o3[j * tstride];
+    for (int k = 0; k < ns; k++) {
+      double x_s = sxyz ? sxyz[3 * k] : sx[k], y_s = sxyz ? sxyz[3 * k + 1] : sy[k],
+             z_s = sxyz ? sxyz[3 * k + 2] : sz[k];
+      double dp = x_t * x_s + y_t * y_s + z_t * z_s;
+      double gf = 0.07957747154594767 / (1.0 - dp + eps);
+      double gf1 = -gf * sv[k];
+      a1 += gf1 * (y_t * z_s - z_t * y_s);
+      a2 += gf1 * (z_t * x_s - x_t * z_s);
+      a3 += gf1 * (x_t * y_s - y_t * x_s);
+    }
+    o1[j * tstride] = a1;
+    o2[j * tstride] = a2;
+    o3[j * tstride] = a3;
+  }
+}
+
+/* The interaction list on the tree: entries grouped by target panel (stable,
+ * so each target sees its sources in list order), target panels in parallel.
+ * u (3 x N) receives particle-target sums, T (3 x Pf x qx) proxy-target sums. */
+static void bltc_interactions(const bltc_tree* t, long nl, const int* list, double theta, int typed,
+                              const double* tx, const double* ty, const double* tz, const double* sx,
+                              const double* sy, const double* sz, const double* w, const double* S, double eps,
+                              double* u, double* T) {
+  int Pf = t->Pf, qx = t->qx, npl = t->npl;
+  size_t pn = (size_t)Pf * qx, N = (size_t)t->Af * npl;
+  long* start = (long*)calloc((size_t)Pf + 1, sizeof(long));
+  long* order = (long*)malloc(sizeof(long) * (size_t)(nl > 0 ? nl : 1));
+  long* fill = (long*)malloc(sizeof(long) * (size_t)Pf);
+  for (long i = 0; i < nl; i++) start[list[3 * i] + 1]++;
+  for (int i = 0; i < Pf; i++) start[i + 1] += start[i];
+  for (int i = 0; i < Pf; i++) fill[i] = start[i];
+  for (long i = 0; i < nl; i++) order[fill[list[3 * i]]++] = i;
+  const int deepest = t->Lf - 1;
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int tp = 0; tp < Pf; tp++) {
+    for (long e = start[tp]; e < start[tp + 1]; e++) {
+      int s = list[3 * order[e] + 1];
+      int near = !bltc_well_separated(t->tp, tp, s, theta);
+      int tpart = near || (typed && t->tp[tp].level == deepest);
+      int spart = near || (typed && t->tp[s].level == deepest);
+      size_t t0 = (size_t)(tp - t->offf) * npl, s0 = (size_t)(s - t->offf) * npl;
+      double* o = tpart ? u + t0 : T + (size_t)tp * qx;
+      size_t stride = tpart ? N : pn;
+      if (spart)
+        bltc_block(tpart ? npl : qx, tpart ? NULL : t->px + 3 * (size_t)tp * qx, 1, tx + t0, ty + t0, tz + t0, npl,
+                   NULL, sx + s0, sy + s0, sz + s0, w + s0, eps, o, o + stride, o + 2 * stride);
+      else
+        bltc_block(tpart ? npl : qx, tpart ? NULL : t->px + 3 * (size_t)tp * qx, 1, tx + t0, ty + t0, tz + t0, qx,
+                   t->px + 3 * (size_t)s * qx, NULL, NULL, NULL, S + (size_t)s * qx, eps, o, o + stride,
+                   o + 2 * stride);
+    }
+  }
+  free(start);
+  free(order);
+  free(fill);
+}
+
+long orc_bltc_list(int levels, int degree, int leaf_size, int n, double theta, int* list, long cap) {
+  bltc_tree t;
+  bltc_tree_init(levels, degree, leaf_size, n, &t);
+  long nl = orc_dual_tree_traversal(t.Lf, t.tp, theta, list, cap);
+  bltc_tree_free(&t);
+  return nl;
+}
+
+void orc_bltc_upward(int levels, int degree, int leaf_size, int n, const double* sx, const double* sy,
+                     const double* sz, const double* w, double* proxy) {
+  bltc_tree t;
+  bltc_tree_init(levels, degree, leaf_size, n, &t);
+  bltc_upward(&t, sx, sy, sz, w, proxy);
+  bltc_tree_free(&t);
+}
+
+void orc_bltc_downward(int levels, int degree, int leaf_size, int n, double* T, const double* tx, const double* ty,
+                       const double* tz, double* u) {
+  bltc_tree t;
+  bltc_tree_init(levels, degree, leaf_size, n, &t);
+  bltc_downward(&t, tx, ty, tz, T, u);
+  bltc_tree_free(&t);
+}
+
+void orc_bltc_velocity(int levels, int degree, int leaf_size, int n, double theta, double eps, int typed,
+                       const double* tx, const double* ty, const double* tz, const double* sx, const double* sy,
+                       const double* sz, const double* w, double* u) {
+  bltc_tree t;
+  bltc_tree_init(levels, degree, leaf_size, n, &t);
+  size_t pn = (size_t)t.Pf * t.qx, N = (size_t)t.Af * t.npl;
+  long nl = orc_dual_tree_traversal(t.Lf, t.tp, theta, NULL, 0);
+  int* list = (int*)malloc(sizeof(int) * 3 * (size_t)(nl > 0 ? nl : 1));
+  orc_dual_tree_traversal(t.Lf, t.tp, theta, list, nl);
+  double* S = (double*)calloc(pn, sizeof(double));
+  double* T = (double*)calloc(3 * pn, sizeof(double));
+  memset(u, 0, sizeof(double) * 3 * N);
+  bltc_upward(&t, sx, sy, sz, w, S);
+  bltc_interactions(&t, nl, list, theta, typed, tx, ty, tz, sx, sy, sz, w, S, eps, u, T);
+  bltc_downward(&t, tx, ty, tz, T, u);
+  free(S);
+  free(T);
+  free(list);
+  bltc_tree_free(&t);
+}
+
 /* ---------------- stepper: src/bve_time_step.cpp ------------------------- */
 
 /* BLI of a field at (x,y,z) in its located leaf: the locate + BLI + gather
@@ -709,6 +1034,26 @@ static void velocity_eval(const orc_bve_problem* pb, const double* eff_vor, cons
                           const double* dz, double* proxy, double* t1, double* t2, double* t3, double* vel) {
   int q = (pb->degree + 1) * (pb->degree + 1), P = orc_panel_count(pb->levels), A = orc_leaf_count(pb->levels);
   size_t n = (size_t)A * q, pq = (size_t)P * q;
+  if (pb->mode == 2) {
+    /* treecode: sources at the displaced particles (the leaf rows of the
+     * displacement), strengths area * effective vorticity, targets at the grid */
+    int off = P - A;
+    double* s = (double*)malloc(sizeof(double) * 4 * n);
+    for (int i = 0; i < A; i++)
+      for (int j = 0; j < q; j++) {
+        size_t o = (size_t)i * q + j, dd = (size_t)(i + off) * q + j;
+        double xx = pb->x[o] + dx[dd], yy = pb->y[o] + dy[dd], zz = pb->z[o] + dz[dd];
+        project_to_sphere(&xx, &yy, &zz);
+        s[o] = xx;
+        s[n + o] = yy;
+        s[2 * n + o] = zz;
+        s[3 * n + o] = pb->area[o] * eff_vor[o];
+      }
+    orc_bltc_velocity(pb->levels, pb->degree, pb->leaf_size, pb->proxy_degree, pb->theta, pb->kernel_eps, pb->typed,
+                      pb->x, pb->y, pb->z, s, s + n, s + 2 * n, s + 3 * n, vel);
+    free(s);
+    return;
+  }
   orc_upward_pass(pb->levels, pb->degree, pb->panels, pb->interp, pb->area, eff_vor, proxy);
   memset(t1, 0, sizeof(double) * pq);
   memset(t2, 0, sizeof(double) * pq);
@@ -782,7 +1127,7 @@ void orc_bve_step(const orc_bve_problem* pb, double* vors, double* vel_x, double
   const double fr[3] = {0.5, 0.5, 1.0};
   for (int s = 1; s < 4; s++) {
     disp_update(A, q, off, pb->x, pb->y, pb->z, v[s - 1], vors, dvor, dx, dy, dz, fr[s - 1] * pb->dt, pb->omega);
-    disp_interp(pb->panels, off, d, pb->interp, dx, dy, dz);
+    if (pb->mode != 2) disp_interp(pb->panels, off, d, pb->interp, dx, dy, dz);
     bve_forcing(pb, dvor, eff);
     velocity_eval(pb, eff, dx, dy, dz, proxy, t1, t2, t3, v[s]);
   }

@@ -59,7 +59,8 @@ void orc_bve_remap(int levels, int degree, const orc_panel* panels, const double
                    const double* dep_y, const double* dep_z, const double* vors, int tracer_count,
                    const double* tracers, double omega, double* new_vors, double* new_tracers);
 
-/* One bve_back_rk4_step.  mode 0 = interaction list (FMM), 1 = direct.
+/* One bve_back_rk4_step.  mode 0 = interaction list (FMM), 1 = direct,
+ * 2 = treecode (orc_bltc_velocity with proxy_degree, leaf_size, theta, typed).
  * vors (A x q), vel_* (A x q, out = stage-0 velocity), tracers (A x q x T)
  * are in-out. */
 typedef struct {
@@ -72,9 +73,31 @@ typedef struct {
   const int* list;
   int forcing;  /* 0 none, 1 ssw, 2 ssw2 (src/forcing_funcs.cpp:82-96) */
   double time;  /* the step's time (seconds), for the forcing */
+  int proxy_degree, leaf_size, typed; /* mode 2 */
+  double theta;                       /* mode 2: the treecode's MAC */
 } orc_bve_problem;
 void orc_bve_step(const orc_bve_problem* pb, double* vors, double* vel_x, double* vel_y, double* vel_z,
                   double* tracers);
+
+/* Treecode with decoupled proxy degree: the reference's irregular-point FMM
+ * (base_pots_ll, child_to_parent_ll, dual_tree_traversal_irreg,
+ * swe_vel_panel_interaction_ll rotational part, parent_to_child_3_ll,
+ * child_panel_interp_3_ll) on the particle grid of (levels, degree), its
+ * quadtree truncated so that a leaf holds at most leaf_size particles, degree
+ * n proxies.  Particle arrays are N = A x q in [leaf panel][q] order.
+ * typed 1: the reference's pp / pc / cp / cc typing of well-separated pairs;
+ * 0: every well-separated pair proxy x proxy.  Targets t (grid points),
+ * sources s with strengths w; u (3 x N) is overwritten. */
+void orc_bltc_shape(int levels, int degree, int leaf_size, int* tree_levels, int* npl);
+long orc_bltc_list(int levels, int degree, int leaf_size, int n, double theta, int* list, long cap);
+void orc_bltc_upward(int levels, int degree, int leaf_size, int n, const double* sx, const double* sy,
+                     const double* sz, const double* w, double* proxy);
+/* T (3 x Pf x qx) is interpolated down in place; u (3 x N) accumulated. */
+void orc_bltc_downward(int levels, int degree, int leaf_size, int n, double* T, const double* tx, const double* ty,
+                       const double* tz, double* u);
+void orc_bltc_velocity(int levels, int degree, int leaf_size, int n, double theta, double eps, int typed,
+                       const double* tx, const double* ty, const double* tz, const double* sx, const double* sy,
+                       const double* sz, const double* w, double* u);
 
 /* direct_sum_inv_lap (src/direct_sum_impl.hpp:20-27) over n points. */
 void orc_direct_sum_inv_lap(int n, const double* x, const double* y, const double* z, const double* area,

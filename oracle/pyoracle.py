@@ -61,6 +61,10 @@ class OrcProblem(ctypes.Structure):
         ("list", _I),
         ("forcing", ctypes.c_int),
         ("time", ctypes.c_double),
+        ("proxy_degree", ctypes.c_int),
+        ("leaf_size", ctypes.c_int),
+        ("typed", ctypes.c_int),
+        ("theta", ctypes.c_double),
     ]
 
 
@@ -167,15 +171,19 @@ class Port:
                                _dp(np.ascontiguousarray(vors)), T, _dp(tr), ctypes.c_double(omega), _dp(nv), _dp(ntr))
         return nv, (ntr if T else None)
 
-    def bve_step(self, g, vors, tracers=None, *, dt, omega, eps, mode=0, nsteps=1, forcing=0, time=0.0):
+    def bve_step(self, g, vors, tracers=None, *, dt, omega, eps, mode=0, nsteps=1, forcing=0, time=0.0,
+                 tree=None):
         """nsteps of bve_back_rk4_step from time (forcing 0 none, 1 ssw, 2 ssw2);
-        returns (vors, (vx, vy, vz), tracers)."""
+        mode 0 the interaction list, 1 direct, 2 treecode with
+        tree = (proxy_degree, leaf_size, theta, typed); returns
+        (vors, (vx, vy, vz), tracers)."""
         A, q = g["x"].shape
         T = 0 if tracers is None else tracers.shape[2]
         lst = np.ascontiguousarray(g["list"], dtype=np.int32)
+        n, leaf, theta, typed = tree if tree is not None else (0, 0, 0.0, 0)
         pb = OrcProblem(g["levels"], g["degree"], T, mode, eps, omega, dt, g["panels"], _dp(g["interp"]), _dp(g["x"]),
                         _dp(g["y"]), _dp(g["z"]), _dp(g["area"]), len(lst), _ip(lst) if len(lst) else None,
-                        int(forcing), float(time))
+                        int(forcing), float(time), int(n), int(leaf), int(typed), float(theta))
         v = np.array(vors, dtype=np.float64, order="C")
         tr = np.zeros(1) if tracers is None else np.array(tracers, dtype=np.float64, order="C")
         vx, vy, vz = (np.zeros((A, q)) for _ in range(3))
@@ -183,6 +191,45 @@ class Port:
             pb.time = float(time) + k * dt
             self.lib.orc_bve_step(ctypes.byref(pb), _dp(v), _dp(vx), _dp(vy), _dp(vz), _dp(tr))
         return v, (vx, vy, vz), (tr if T else None)
+
+    # ---- treecode (decoupled proxy degree) ---------------------------------
+    def bltc_shape(self, levels, degree, leaf_size):
+        """(tree levels, particles per tree leaf)."""
+        lf, npl = ctypes.c_int(), ctypes.c_int()
+        self.lib.orc_bltc_shape(levels, degree, leaf_size, ctypes.byref(lf), ctypes.byref(npl))
+        return lf.value, npl.value
+
+    def bltc_list(self, levels, degree, leaf_size, n, theta):
+        f = self.lib.orc_bltc_list
+        f.restype = ctypes.c_long
+        cnt = f(levels, degree, leaf_size, n, ctypes.c_double(theta), None, ctypes.c_long(0))
+        out = np.zeros((cnt, 3), np.int32)
+        f(levels, degree, leaf_size, n, ctypes.c_double(theta), _ip(out), ctypes.c_long(cnt))
+        return out
+
+    def bltc_upward(self, levels, degree, leaf_size, n, sx, sy, sz, w):
+        lf, _ = self.bltc_shape(levels, degree, leaf_size)
+        P = 2 * (4**lf - 1)
+        out = np.zeros((P, (n + 1) ** 2))
+        a = [np.ascontiguousarray(v, dtype=np.float64).ravel() for v in (sx, sy, sz, w)]
+        self.lib.orc_bltc_upward(levels, degree, leaf_size, n, *[_dp(v) for v in a], _dp(out))
+        return out
+
+    def bltc_downward(self, levels, degree, leaf_size, n, T, tx, ty, tz):
+        """(proxy targets after the parent-to-child passes, 3 x N particle values)."""
+        t = np.array(T, dtype=np.float64, order="C")
+        a = [np.ascontiguousarray(v, dtype=np.float64).ravel() for v in (tx, ty, tz)]
+        u = np.zeros((3, a[0].size))
+        self.lib.orc_bltc_downward(levels, degree, leaf_size, n, _dp(t), *[_dp(v) for v in a], _dp(u))
+        return t, u
+
+    def bltc_velocity(self, levels, degree, leaf_size, n, theta, eps, typed, t, s, w):
+        """Treecode velocity (3 x N) at targets t = (x, y, z) of sources s with strengths w."""
+        a = [np.ascontiguousarray(v, dtype=np.float64).ravel() for v in (*t, *s, w)]
+        u = np.zeros((3, a[0].size))
+        self.lib.orc_bltc_velocity(levels, degree, leaf_size, n, ctypes.c_double(theta), ctypes.c_double(eps),
+                                   int(typed), *[_dp(v) for v in a], _dp(u))
+        return u
 
     def poisson_fmm_interactions(self, g, source, target):
         """poisson_fmm_interactions (src/fmm_interactions/inverse_poisson.cpp:9-34): target += ..."""
@@ -233,7 +280,7 @@ class Ref:
                                  ctypes.c_int, ctypes.c_int]
         for name in ("ref_destroy", "ref_sizes", "ref_get_panels", "ref_get_interactions", "ref_get_points",
                      "ref_bve_initialize", "ref_bve_step", "ref_bve_vel_interactions", "ref_upward_pass",
-                     "ref_downward_pass_3", "ref_bve_departure", "ref_bve_remap"):
+                     "ref_downward_pass_3", "ref_bve_departure", "ref_bve_remap", "ref_set_area"):
             getattr(L, name).restype = None
         L.ref_bve_step.argtypes = [ctypes.c_void_p, _D, _D, _D, _D, _D, ctypes.c_double, ctypes.c_int]
         L.ref_bve_departure.argtypes = [ctypes.c_void_p, _D, _D, _D, _D, ctypes.c_double, _D, _D, _D]
@@ -262,6 +309,10 @@ class Ref:
 
     def destroy(self, c):
         self.lib.ref_destroy(c["h"])
+
+    def set_area(self, c, area):
+        """Replaces the quadrature weights (A x q) the later calls read."""
+        self.lib.ref_set_area(c["h"], _dp(np.ascontiguousarray(area, dtype=np.float64)))
 
     def panels(self, c):
         ints = np.zeros((c["P"], 13), np.int32)
@@ -367,6 +418,45 @@ class Ref:
         return out
 
     # ---- shallow water (SWE v2) -------------------------------------------
+
+    # ---- the irregular-point ("_ll") FMM on the particle grid's truncated tree ----
+    def ll_create(self, levels, degree, leaf_size, proxy_degree, theta, eps):
+        L = self.lib
+        L.ref_ll_create.restype = ctypes.c_void_p
+        L.ref_ll_create.argtypes = [ctypes.c_int] * 4 + [ctypes.c_double, ctypes.c_double]
+        for name in ("ref_ll_destroy", "ref_ll_sizes", "ref_ll_list", "ref_ll_upward", "ref_ll_downward",
+                     "ref_ll_velocity"):
+            getattr(L, name).restype = None
+        h = ctypes.c_void_p(L.ref_ll_create(levels, degree, leaf_size, proxy_degree, theta, eps))
+        sz = np.zeros(5, np.int32)
+        L.ref_ll_sizes(h, _ip(sz))
+        Pf, Lf, npl, qx, I = (int(v) for v in sz)
+        A, q = 6 * 4 ** (levels - 1), (degree + 1) ** 2
+        return dict(h=h, Pf=Pf, Lf=Lf, npl=npl, qx=qx, I=I, A=A, q=q)
+
+    def ll_destroy(self, c):
+        self.lib.ref_ll_destroy(c["h"])
+
+    def ll_list(self, c):
+        out = np.zeros((c["I"], 3), np.int32)
+        self.lib.ref_ll_list(c["h"], _ip(out))
+        return out
+
+    def ll_upward(self, c, pots):
+        out = np.zeros((c["Pf"], c["qx"]))
+        self.lib.ref_ll_upward(c["h"], _dp(np.ascontiguousarray(pots, dtype=np.float64)), _dp(out))
+        return out
+
+    def ll_downward(self, c, t1, t2, t3):
+        t = [np.ascontiguousarray(v, dtype=np.float64) for v in (t1, t2, t3)]
+        s = [np.zeros((c["A"], c["q"])) for _ in range(3)]
+        self.lib.ref_ll_downward(c["h"], *[_dp(v) for v in t], *[_dp(v) for v in s])
+        return s
+
+    def ll_velocity(self, c, vors):
+        out = [np.zeros((c["A"], c["q"])) for _ in range(3)]
+        self.lib.ref_ll_velocity(c["h"], _dp(np.ascontiguousarray(vors, dtype=np.float64)), *[_dp(v) for v in out])
+        return out
 
     def swe_map(self, c):
         """cubed_sphere_2d_to_1d: (two_d_to_1d A x q int32, counts U int32)."""

@@ -139,6 +139,14 @@ void ref_get_points(void* h, double* x, double* y, double* z, double* area, doub
   copy_out(c->interp, interp);
 }
 
+// Replaces the quadrature weights (A x q) every later call reads, e.g. with
+// the exact Clenshaw-Curtis weights of a run that uses them; the reference's
+// own weights come from cube_sphere_spec_points (src/initialize_cubed_sphere.cpp:280-288).
+void ref_set_area(void* h, const double* area) {
+  RefCtx* c = static_cast<RefCtx*>(h);
+  copy_in(c->area, area);
+}
+
 // The reference's own initial conditions (rh4 / gv / pv / rot), with balance_ic.
 void ref_bve_initialize(void* h, const char* ic, int balance, double* vors_out) {
   RefCtx* c = static_cast<RefCtx*>(h);

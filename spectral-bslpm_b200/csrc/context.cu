@@ -949,7 +949,9 @@ sbslpm_status sbslpm_direct_sum_bve(long nt, const double* tx, const double* ty,
                                     int precision, double* ux, double* uy, double* uz, void* stream) {
   if (nt < 0 || ns < 0 || (nt > 0 && (bad(tx) || bad(ty) || bad(tz) || bad(ux) || bad(uy) || bad(uz))) ||
       (ns > 0 && (bad(sx) || bad(sy) || bad(sz) || bad(s))) || (precision != SBSLPM_FP64 && precision != SBSLPM_MIXED))
-    return SBSLPM_ERR_ARG;
+    return set_last_error("sbslpm_direct_sum_bve: negative size, null array or unknown precision"), SBSLPM_ERR_ARG;
+  if (any_on_host({tx, ty, tz, sx, sy, sz, s, ux, uy, uz}))
+    return set_last_error("sbslpm_direct_sum_bve: an array is host memory (device pointers expected)"), SBSLPM_ERR_ARG;
   if (nt == 0) return SBSLPM_OK;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (ns == 0) {
@@ -971,7 +973,11 @@ sbslpm_status sbslpm_direct_sum_bve(long nt, const double* tx, const double* ty,
 
 sbslpm_status sbslpm_direct_sum_inv_lap(long n, const double* x, const double* y, const double* z, const double* area,
                                         const double* pots, double* soln, void* stream) {
-  if (n < 0 || (n > 0 && (bad(x) || bad(y) || bad(z) || bad(area) || bad(pots) || bad(soln)))) return SBSLPM_ERR_ARG;
+  if (n < 0 || (n > 0 && (bad(x) || bad(y) || bad(z) || bad(area) || bad(pots) || bad(soln))))
+    return set_last_error("sbslpm_direct_sum_inv_lap: negative size or null array"), SBSLPM_ERR_ARG;
+  if (any_on_host({x, y, z, area, pots, soln}))
+    return set_last_error("sbslpm_direct_sum_inv_lap: an array is host memory (device pointers expected)"),
+           SBSLPM_ERR_ARG;
   if (n == 0) return SBSLPM_OK;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   launch_inv_lap(n, x, y, z, area, pots, soln, st);

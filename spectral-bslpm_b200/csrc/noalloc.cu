@@ -26,7 +26,9 @@ static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchDoubles
 
 // In host code g_noalloc_scratch names a host-side shadow, not device memory:
 // the device address must come from cudaGetSymbolAddress, once per device,
-// with that device current.  The result is cached per device.
+// with that device current.  The result is cached per device, so a device
+// must not be reset (cudaDeviceReset) while the library is in use: the
+// module reloads after a reset and the array may move.
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 double* g_addr[kMaxDevices] = {};
@@ -65,9 +67,15 @@ extern "C" sbslpm_status sbslpm_direct_sum_bve_noalloc(long nt, const double* tx
                                                        long ns, const double* sx, const double* sy, const double* sz,
                                                        const double* s, double eps, int precision, double* ux,
                                                        double* uy, double* uz, void* stream) {
-  if (nt < 0 || ns < 0 || (precision != SBSLPM_FP64 && precision != SBSLPM_MIXED)) return SBSLPM_ERR_ARG;
-  if (nt > 0 && (!tx || !ty || !tz || !ux || !uy || !uz)) return SBSLPM_ERR_ARG;
-  if (ns > 0 && (!sx || !sy || !sz || !s)) return SBSLPM_ERR_ARG;
+  if (nt < 0 || ns < 0) return set_last_error("sbslpm_direct_sum_bve_noalloc: negative size"), SBSLPM_ERR_ARG;
+  if (precision != SBSLPM_FP64 && precision != SBSLPM_MIXED)
+    return set_last_error("sbslpm_direct_sum_bve_noalloc: unknown precision"), SBSLPM_ERR_ARG;
+  if ((nt > 0 && (!tx || !ty || !tz || !ux || !uy || !uz)) || (ns > 0 && (!sx || !sy || !sz || !s)))
+    return set_last_error("sbslpm_direct_sum_bve_noalloc: null array"), SBSLPM_ERR_ARG;
+  // a host array handed to the kernels would fault the caller's context
+  if (any_on_host({tx, ty, tz, sx, sy, sz, s, ux, uy, uz}))
+    return set_last_error("sbslpm_direct_sum_bve_noalloc: an array is host memory (device pointers expected)"),
+           SBSLPM_ERR_ARG;
   if (3 * nt > kNoAllocScratchDoubles) {
     set_last_error("sbslpm_direct_sum_bve_noalloc: " + std::to_string(nt) + " targets exceed its fixed scratch (" +
                    std::to_string(kNoAllocScratchDoubles / 3) + " targets at most); use sbslpm_direct_sum_bve");
@@ -85,7 +93,10 @@ extern "C" sbslpm_status sbslpm_direct_sum_bve_noalloc(long nt, const double* tx
     sbslpm_status status = scratch_for_current_device(&partial);
     if (status != SBSLPM_OK) return status;
     // every (group, target) slot of the scratch is written before it is read,
-    // so nothing left by an earlier call needs clearing
+    // so nothing left by an earlier call needs clearing.  When the target
+    // count leaves room for fewer source groups than the allocating entry
+    // point would use, the sums are split into fewer groups: the same sum in
+    // another order.
     long groups = direct_groups(nt, ns);
     long fit = kNoAllocScratchDoubles / (3 * nt);
     if (groups > fit) groups = fit;

@@ -1,0 +1,114 @@
+"""The treecode (decoupled proxy degree) against the oracle, through the C ABI.
+
+Checkers (oracle/bslpm_oracle.c, pinned to the reference by
+tests/test_oracle_bltc.py and tests/test_oracle_golden.py):
+  * the oracle's treecode step (mode 2) with every well-separated pair proxy
+    x proxy -- this library's design, built from the reference's
+    irregular-point FMM functions (base_pots_ll, child_to_parent_ll,
+    dual_tree_traversal_irreg, swe_vel_panel_interaction_ll,
+    parent_to_child_3_ll, child_panel_interp_3_ll): the float64 GPU step must
+    agree to 1e-12, the mixed-precision step to 1e-6;
+  * the oracle's float64 direct-sum step (mode 1): the metric's bar, 1e-6
+    relative L-infinity vorticity error after one step;
+  * the oracle's treecode with the reference's pp / pc / cp / cc typing
+    (typed = 1, the reference's own arithmetic at equal theta, proxy degree
+    and leaf size): the GPU treecode's error against the direct sum must not
+    exceed twice that error (plus the float32 rounding for mixed).
+Plus the headline configuration itself (393,216 particles, theta 0.7,
+degree-8 proxies, 256-particle leaves): one step within 1e-6 of the float64
+direct sum, which is pinned to the oracle at 24,576 particles.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+FP64_TOL = 1e-12
+MIXED_TOL = 1e-6
+BAR = 1e-6
+DT, OMEGA, EPS = 0.005, 2 * np.pi, 1e-4
+
+
+def rel(a, b):
+    a = a.detach().cpu().numpy() if hasattr(a, "detach") else np.asarray(a)
+    b = b.detach().cpu().numpy() if hasattr(b, "detach") else np.asarray(b)
+    return float(np.abs(a - b).max() / np.abs(b).max())
+
+
+def cuda(a):
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).cuda()
+
+
+def rh4(x, y, z, area):
+    lat, lon = np.arcsin(np.clip(z, -1, 1)), np.arctan2(y, x)
+    vor = np.sin(lat) - 0.5 * np.sin(lat) * np.cos(lat) ** 4 * 30 * np.cos(4 * lon)
+    return vor - (vor * area).sum() / (4 * np.pi)
+
+
+def gpu_step(sb, g, vor, **kw):
+    cfg = sb.config_default(levels=kw.pop("levels"), interp_degree=3, kernel_eps=EPS, omega=OMEGA, dt=DT, **kw)
+    ctx = sb.Context(cfg)
+    v = cuda(vor)
+    vel = [torch.zeros_like(v) for _ in range(3)]
+    ctx.bve_back_rk4_step(cuda(g.x), cuda(g.y), cuda(g.z), cuda(g.area), v, *vel)
+    return v, torch.stack(vel)
+
+
+@pytest.fixture(scope="module")
+def grid5(sb, port):
+    g = sb.build_grid(5, 3, exact_cc=True)
+    og = port.build(5, 3, None, exact_cc=True)
+    assert np.array_equal(og["x"], g.x) and np.array_equal(og["area"], g.area)
+    vor = rh4(g.x, g.y, g.z, g.area)
+    dv, dvel, _ = port.bve_step(og, vor, None, dt=DT, omega=OMEGA, eps=EPS, mode=1)
+    return g, og, vor, dv, np.stack(dvel)
+
+
+# (levels, leaf size, proxy degree, theta): the headline geometry at 24,576
+# particles, the ensemble's (theta, degree) pairs, a deeper tree of 64-particle
+# leaves, and leaves that are single grid panels
+CASES = [(5, 256, 8, 0.7), (5, 256, 6, 0.5), (5, 256, 10, 0.8), (4, 64, 8, 0.7), (4, 16, 5, 0.6)]
+
+
+@pytest.mark.parametrize("levels,leaf,n,theta", CASES)
+def test_treecode_step_matches_oracle(sb, port, levels, leaf, n, theta):
+    g = sb.build_grid(levels, 3, exact_cc=True)
+    og = port.build(levels, 3, None, exact_cc=True)
+    vor = rh4(g.x, g.y, g.z, g.area)
+    ov, ovel, _ = port.bve_step(og, vor, None, dt=DT, omega=OMEGA, eps=EPS, mode=2, tree=(n, leaf, theta, 0))
+    ovel = np.stack(ovel)
+    for prec, tol in ((sb.FP64, FP64_TOL), (sb.MIXED, MIXED_TOL)):
+        v, vel = gpu_step(sb, g, vor, levels=levels, fmm_theta=theta, proxy_degree=n, leaf_size=leaf,
+                          precision=prec)
+        assert rel(vel, ovel) <= tol, (prec, rel(vel, ovel))
+        assert rel(v, ov) <= tol, (prec, rel(v, ov))
+
+
+@pytest.mark.parametrize("n,theta", [(8, 0.7), (6, 0.5), (10, 0.8)])
+def test_treecode_error_against_the_direct_sum(sb, port, grid5, n, theta):
+    """Vorticity after one step within the bar of the oracle's float64 direct
+    sum, and no further from it than the reference's typed treecode."""
+    g, og, vor, dv, dvel = grid5
+    rv, _, _ = port.bve_step(og, vor, None, dt=DT, omega=OMEGA, eps=EPS, mode=2, tree=(n, 256, theta, 1))
+    ref_err = rel(rv, dv)
+    for prec, slack in ((sb.FP64, 1e-12), (sb.MIXED, 1e-8)):
+        v, vel = gpu_step(sb, g, vor, levels=5, fmm_theta=theta, proxy_degree=n, leaf_size=256, precision=prec)
+        err = rel(v, dv)
+        print(f"n={n} theta={theta} prec={prec}: vorticity error {err:.3e} (reference typing {ref_err:.3e}), "
+              f"velocity error {rel(vel, dvel):.3e}")
+        assert err <= BAR
+        assert err <= 2 * ref_err + slack
+
+
+def test_headline_configuration_meets_the_bar(sb):
+    """393,216 particles, theta 0.7, degree-8 proxies, 256-particle leaves:
+    the mixed and float64 treecode steps within 1e-6 (vorticity) of the
+    float64 direct sum."""
+    g = sb.build_grid(7, 3, exact_cc=True)
+    vor = rh4(g.x, g.y, g.z, g.area)
+    dv, dvel = gpu_step(sb, g, vor, levels=7, velocity=sb.VEL_DIRECT)
+    for prec in (sb.MIXED, sb.FP64):
+        v, vel = gpu_step(sb, g, vor, levels=7, fmm_theta=0.7, proxy_degree=8, leaf_size=256, precision=prec)
+        print(f"levels 7 prec={prec}: vorticity error {rel(v, dv):.3e}, velocity error {rel(vel, dvel):.3e}")
+        assert rel(v, dv) <= BAR

@@ -7,7 +7,8 @@ Its scratch is a fixed array inside the library instead of a per-call
 allocation.  These tests call it through the C ABI and check it against the
 allocating entry point, sbslpm_direct_sum_bve, on two calls in a row with
 different inputs (so leftovers of the first call in the shared scratch would
-show), and check that a size beyond its fixed scratch is refused.
+show) and on a target count that leaves room for fewer source groups, and
+check that a size beyond its fixed scratch and host arrays are refused.
 
 This file is collected last, so a run that stops at the first failure has
 run every other test first; it also passes alone in a fresh process.
@@ -55,6 +56,32 @@ def test_noalloc_matches_allocating_entry_point(sb, precision):
         got = call_noalloc(sb, t, s, w, 1e-4, precision)
         assert torch.isfinite(got).all()
         assert rel(got, want) <= TOL
+
+
+def test_noalloc_with_fewer_groups_than_the_allocating_path(sb):
+    """200,000 targets leave room for 3 source groups in the fixed scratch
+    where the allocating entry point uses 4: the same sums in another
+    order, so the results agree to rounding."""
+    rng = np.random.default_rng(29)
+    t, s = points(rng, 200_000), points(rng, 8192)
+    w = torch.from_numpy(rng.standard_normal(8192) * 1e-3).cuda()
+    want = torch.stack(sb.direct_sum_bve(*t, *s, w, 1e-4, 0))
+    got = call_noalloc(sb, t, s, w, 1e-4, 0)
+    assert rel(got, want) <= TOL
+
+
+@pytest.mark.parametrize("name", ["sbslpm_direct_sum_bve_noalloc", "sbslpm_direct_sum_bve"])
+def test_direct_sums_refuse_host_arrays(sb, name):
+    """Host arrays are refused before any copy or launch, with a message."""
+    n = 64
+    host = [np.zeros(n) for _ in range(6)]
+    L = sb.lib()
+    ptr = [ctypes.c_void_p(a.ctypes.data) for a in host]
+    for ns in (0, 16):  # no sources: the path that only clears the outputs
+        status = getattr(L, name)(ctypes.c_long(n), *ptr[:3], ctypes.c_long(ns), *ptr[:3], ptr[3],
+                                  ctypes.c_double(1e-4), ctypes.c_int(0), *ptr[3:], ctypes.c_void_p(0))
+        assert status == 5
+        assert "host memory" in L.sbslpm_last_error().decode()
 
 
 def test_noalloc_refuses_sizes_beyond_its_scratch(sb):
