@@ -137,6 +137,18 @@ sbslpm_status sbslpm_dual_tree_traversal(int levels, const sbslpm_panel* panels,
  * and out; device workspace is allocated and freed inside the call. */
 sbslpm_status sbslpm_dual_tree_traversal_device(int levels, const sbslpm_panel* panels, double theta,
                                                 sbslpm_interact_pair* out, long cap, long* count);
+/* The traversal as the treecode uses it (dual_tree_traversal_irreg,
+ * src/fmm_funcs.cpp:125-231, has the same pairs and order on a uniform tree):
+ * near[e] = 1 for the leaf pairs that failed the MAC (particle x particle),
+ * 0 for the well-separated ones.  The _multi form runs one traversal per
+ * theta (members) on the GPU in one launch series and writes the members'
+ * lists one after the other (counts[m] pairs each, at most cap in all); the
+ * treecode contexts and the ensemble build their lists with it. */
+sbslpm_status sbslpm_dual_tree_traversal_flagged(int levels, const sbslpm_panel* panels, double theta,
+                                                 sbslpm_interact_pair* out, char* near, long cap, long* count);
+sbslpm_status sbslpm_dual_tree_traversal_device_multi(int levels, const sbslpm_panel* panels, int members,
+                                                      const double* theta, sbslpm_interact_pair* out, char* near,
+                                                      long cap, long* counts);
 /* Host versions of interp_vals_bli / point_locate_panel
  * (src/interp_funcs_impl.hpp:11-142). */
 sbslpm_status sbslpm_interp_vals_bli(double* basis, double xi, double eta, double min_xi, double max_xi,
@@ -381,6 +393,18 @@ sbslpm_status sbslpm_batch_set_cc_mode(sbslpm_batch* batch, int mode);
  * Replaces nothing in the reference (one problem per process there). */
 sbslpm_status sbslpm_batch_set_stage0_shared(sbslpm_batch* batch, int shared);
 sbslpm_status sbslpm_batch_cc_info(const sbslpm_batch* batch, int* mode, double* union_pairs, double* mma_flops);
+/* Wall time (seconds) of sbslpm_batch_create's list build: every member's
+ * tree traversal on the GPU in one launch series, with the lists' CSR
+ * assembly on the host. */
+sbslpm_status sbslpm_batch_setup_times(const sbslpm_batch* batch, double* lists_s);
+/* Test of the tensor-core kernel's failure path (no counterpart in the
+ * reference).  on = 1: every CTA of the tensor-core well-separated kernel
+ * (modes 1 and 2) withholds one producer thread's arrival on its first
+ * chunk's barrier and bounds its waits to 2 ms, so the MMA warp's wait runs
+ * out before any MMA is issued: the CTA frees its tensor memory and returns,
+ * and the step reports SBSLPM_ERR_TIMEOUT (its results are not valid).
+ * on = 0 restores the normal one-second bound. */
+sbslpm_status sbslpm_batch_set_wait_test(sbslpm_batch* batch, int on);
 sbslpm_status sbslpm_batch_cc_groups(const sbslpm_batch* batch, int n, int* degree, int* members, int* mode,
                                      double* ms_cuda_cores, double* ms_tensor_cores, double* ms_shared);
 
@@ -510,6 +534,16 @@ sbslpm_status sbslpm_near_tuning(const sbslpm_ctx* ctx, int* shape, double* ms_p
  * iteration, src/fmm_interactions/bve_vel.cpp:35-150). */
 sbslpm_status sbslpm_set_cc_tuning(sbslpm_ctx* ctx, int slots, int chunk_len);
 sbslpm_status sbslpm_cc_tuning(const sbslpm_ctx* ctx, int* shape, double* ms_per_launch);
+/* Mixed-precision treecode contexts (36..121 proxies) also have a barrier-free
+ * form of the chunked kernel: each slot reads its source proxies straight
+ * from a pair-transposed copy through the L1 cache instead of staging them in
+ * shared memory, with targets_per_thread (1 | 2) target proxies per thread.
+ * The first-step timing includes it; sbslpm_set_cc_tuning_direct fixes it
+ * (the chunk length sets the order of the float64 additions, as above);
+ * sbslpm_cc_form reports 0 for the staged form, else its targets per
+ * thread. */
+sbslpm_status sbslpm_set_cc_tuning_direct(sbslpm_ctx* ctx, int slots, int chunk_len, int targets_per_thread);
+sbslpm_status sbslpm_cc_form(const sbslpm_ctx* ctx, int* targets_per_thread);
 /* CUDA-core fused multiply-add throughput of this GPU, measured with
  * independent FMA chains on every SM for about ms milliseconds: kind 0 =
  * float32, 1 = float64.  Returns FLOP/s (2 per FMA) in *flops. */

@@ -22,7 +22,8 @@ __all__ = [
     "SbslpmError", "Config", "Panel", "InteractPair", "FP64", "MIXED", "VEL_FMM", "VEL_DIRECT", "library_path",
     "FORCING_NONE", "FORCING_SSW", "FORCING_SSW2",
     "lib", "config_default", "read_run_config", "panel_count", "leaf_count", "cubed_sphere_panels_init",
-    "interp_init", "cube_sphere_spec_points", "dual_tree_traversal", "interp_vals_bli", "point_locate_panel",
+    "interp_init", "cube_sphere_spec_points", "dual_tree_traversal", "dual_tree_traversal_flagged",
+    "dual_tree_traversal_device_multi", "interp_vals_bli", "point_locate_panel",
     "Context", "direct_sum_bve", "direct_sum_inv_lap", "output_grid", "NcFile", "kernel_launches", "Grid",
     "build_grid",
 ]
@@ -104,6 +105,13 @@ def lib() -> ctypes.CDLL:
                                              ctypes.POINTER(InteractPair), ctypes.c_long,
                                              ctypes.POINTER(ctypes.c_long)]
     L.sbslpm_dual_tree_traversal_device.argtypes = L.sbslpm_dual_tree_traversal.argtypes
+    L.sbslpm_dual_tree_traversal_flagged.argtypes = [ctypes.c_int, ctypes.POINTER(Panel), ctypes.c_double,
+                                                     ctypes.POINTER(InteractPair), ctypes.c_char_p, ctypes.c_long,
+                                                     ctypes.POINTER(ctypes.c_long)]
+    L.sbslpm_dual_tree_traversal_device_multi.argtypes = [ctypes.c_int, ctypes.POINTER(Panel), ctypes.c_int, _D,
+                                                          ctypes.POINTER(InteractPair), ctypes.c_char_p,
+                                                          ctypes.c_long, ctypes.POINTER(ctypes.c_long)]
+    L.sbslpm_batch_setup_times.argtypes = [_VP, _D]
     L.sbslpm_create.argtypes = [ctypes.POINTER(Config), ctypes.POINTER(_VP)]
     for name in ("sbslpm_destroy", "sbslpm_set_stream", "sbslpm_get_sizes", "sbslpm_get_panels",
                  "sbslpm_get_interactions"):
@@ -159,6 +167,7 @@ def lib() -> ctypes.CDLL:
     L.sbslpm_batch_tuning.argtypes = [_VP, _I, _D]
     L.sbslpm_batch_pairs.argtypes = [_VP, _D, _D]
     L.sbslpm_batch_set_cc_mode.argtypes = [_VP, ctypes.c_int]
+    L.sbslpm_batch_set_wait_test.argtypes = [_VP, ctypes.c_int]
     L.sbslpm_batch_cc_info.argtypes = [_VP, _I, _D, _D]
     L.sbslpm_batch_cc_groups.argtypes = [_VP, ctypes.c_int, _I, _I, _I, _D, _D, _D]
     L.sbslpm_batch_set_tuning.argtypes = [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_int]
@@ -168,6 +177,8 @@ def lib() -> ctypes.CDLL:
     L.sbslpm_set_cc_tuning.argtypes = [_VP, ctypes.c_int, ctypes.c_int]
     L.sbslpm_batch_set_stage0_shared.argtypes = [_VP, ctypes.c_int]
     L.sbslpm_cc_tuning.argtypes = [_VP, _I, _D]
+    L.sbslpm_set_cc_tuning_direct.argtypes = [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    L.sbslpm_cc_form.argtypes = [_VP, _I]
     L.sbslpm_measure_fma_peak.argtypes = [ctypes.c_int, ctypes.c_double, _D]
     _lib = L
     return L
@@ -244,6 +255,39 @@ def dual_tree_traversal(levels: int, panels, theta: float, device: bool = False)
     out = (InteractPair * max(n.value, 1))()
     _check(fn(levels, panels, theta, out, n.value, ctypes.byref(n)), "traversal")
     return np.ctypeslib.as_array(ctypes.cast(out, ctypes.POINTER(ctypes.c_int)), (max(n.value, 1), 3))[: n.value].copy()
+
+
+def dual_tree_traversal_flagged(levels: int, panels, theta: float):
+    """(list I x 3 int32, near I uint8): the treecode's traversal on the host,
+    near = 1 for the leaf pairs that failed the MAC."""
+    fn = lib().sbslpm_dual_tree_traversal_flagged
+    n = ctypes.c_long(0)
+    _check(fn(levels, panels, theta, None, None, 0, ctypes.byref(n)), "traversal")
+    out = (InteractPair * max(n.value, 1))()
+    near = ctypes.create_string_buffer(max(n.value, 1))
+    _check(fn(levels, panels, theta, out, near, n.value, ctypes.byref(n)), "traversal")
+    lst = np.ctypeslib.as_array(ctypes.cast(out, ctypes.POINTER(ctypes.c_int)), (max(n.value, 1), 3))[: n.value]
+    return lst.copy(), np.frombuffer(near.raw, np.uint8)[: n.value].copy()
+
+
+def dual_tree_traversal_device_multi(levels: int, panels, thetas):
+    """One traversal per theta on the GPU in one launch series: a list of
+    (list I x 3 int32, near I uint8) per theta."""
+    th = np.ascontiguousarray(thetas, dtype=np.float64)
+    fn = lib().sbslpm_dual_tree_traversal_device_multi
+    counts = (ctypes.c_long * len(th))()
+    _check(fn(levels, panels, len(th), th.ctypes.data_as(_D), None, None, 0, counts), "traversal")
+    total = sum(counts)
+    out = (InteractPair * max(total, 1))()
+    near = ctypes.create_string_buffer(max(total, 1))
+    _check(fn(levels, panels, len(th), th.ctypes.data_as(_D), out, near, total, counts), "traversal")
+    allp = np.ctypeslib.as_array(ctypes.cast(out, ctypes.POINTER(ctypes.c_int)), (max(total, 1), 3))[:total]
+    alln = np.frombuffer(near.raw, np.uint8)[:total]
+    res, o = [], 0
+    for c in counts:
+        res.append((allp[o:o + c].copy(), alln[o:o + c].copy()))
+        o += c
+    return res
 
 
 def interp_vals_bli(xi, eta, min_xi, max_xi, min_eta, max_eta, degree) -> np.ndarray:
@@ -538,6 +582,18 @@ class Context:
         autotuning it."""
         _check(lib().sbslpm_set_cc_tuning(self._h, int(slots), int(chunk_len)), "sbslpm_set_cc_tuning")
 
+    def set_cc_tuning_direct(self, slots: int, chunk_len: int, targets_per_thread: int):
+        """Fix the barrier-free form of the mixed-precision well-separated kernel
+        (sources read through L1 from a pair-transposed copy) and its shape."""
+        _check(lib().sbslpm_set_cc_tuning_direct(self._h, int(slots), int(chunk_len), int(targets_per_thread)),
+               "sbslpm_set_cc_tuning_direct")
+
+    def cc_form(self) -> int:
+        """0: sources staged in shared memory; 1 | 2: barrier-free, targets per thread."""
+        t = ctypes.c_int()
+        _check(lib().sbslpm_cc_form(self._h, ctypes.byref(t)), "sbslpm_cc_form")
+        return t.value
+
     def cc_tuning(self):
         """(slots, chunk length, threads per block, candidates timed, ms per
         well-separated launch)."""
@@ -662,6 +718,17 @@ class Batch:
         """Well-separated interactions: -1 autotuned per proxy-degree group (default for mixed
         precision), 0 CUDA-core pairs, 1 tensor-core 3xTF32 GEMM, 2 tensor-core single-pass TF32 GEMM."""
         _check(lib().sbslpm_batch_set_cc_mode(self._h, int(mode)), "sbslpm_batch_set_cc_mode")
+
+    def setup_times(self) -> dict:
+        """Wall time (s) of the creation's list build (every member's traversal on the GPU)."""
+        t = ctypes.c_double()
+        _check(lib().sbslpm_batch_setup_times(self._h, ctypes.byref(t)), "sbslpm_batch_setup_times")
+        return {"lists_s": t.value}
+
+    def set_wait_test(self, on: bool):
+        """Test of the tensor-core kernel's bounded waits: with on, its steps
+        in modes 1 and 2 report SBSLPM_ERR_TIMEOUT (sbslpm_batch_set_wait_test)."""
+        _check(lib().sbslpm_batch_set_wait_test(self._h, int(bool(on))), "sbslpm_batch_set_wait_test")
 
     def cc_info(self):
         """(mode, union cluster pairs over the degree groups, MMA flops per velocity evaluation)."""

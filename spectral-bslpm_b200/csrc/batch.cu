@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -25,6 +26,7 @@ struct sbslpm_batch {
   long N = 0;
   std::vector<double> theta;
   std::vector<int> degree;
+  double lists_s = 0;  // wall time of the members' list build at creation
   std::vector<sbslpm_panel> panels;
   cudaStream_t user_stream = nullptr, own_stream = nullptr;
   // the members' tree passes run on aux_stream (higher priority) beside the
@@ -202,13 +204,20 @@ sbslpm_status batch_setup(sbslpm_batch* b) {
   std::vector<int> by_theta(b->M);
   for (int m = 0; m < b->M; m++) by_theta[m] = m;
   std::stable_sort(by_theta.begin(), by_theta.end(), [&](int u, int v) { return b->theta[u] < b->theta[v]; });
+  // every member's traversal on the GPU in one launch series (the degree
+  // groups share the tree: it depends on the leaf size, not on the degree)
+  std::vector<TreeLists> lists;
+  {
+    const auto t0 = std::chrono::steady_clock::now();
+    SB_TRY(device_tree_lists(b->degs[0].t, b->theta, lists, nullptr));
+    b->lists_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  }
   for (int mi = 0; mi < b->M; mi++) {
     const int m = by_theta[mi];
     const size_t k = std::lower_bound(uniq.begin(), uniq.end(), b->degree[m]) - uniq.begin();
     sbslpm_batch::Degree& D = b->degs[k];
     D.members.push_back(m);
-    TreeLists l;
-    build_tree_lists(D.t, b->theta[m], l);
+    TreeLists& l = lists[m];
     hns[m] = l.ns;
     hnsrc[m] = l.nsrc;
     b->near_pairs[m] = l.ns.back();
@@ -711,6 +720,25 @@ sbslpm_status sbslpm_batch_set_cc_mode(sbslpm_batch* b, int mode) {
     b->graph = nullptr;
   }
   b->cc_mode = mode;
+  return SBSLPM_OK;
+}
+
+sbslpm_status sbslpm_batch_set_wait_test(sbslpm_batch* b, int on) {
+  if (!b) return SBSLPM_ERR_ARG;
+  for (auto& D : b->degs) {
+    D.tc.withhold = on ? 1 : 0;
+    D.tc.wait_ns = on ? 2000000ull : 1000000000ull;
+  }
+  if (b->graph) {  // the groups are kernel arguments captured in the graph
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  return SBSLPM_OK;
+}
+
+sbslpm_status sbslpm_batch_setup_times(const sbslpm_batch* b, double* lists_s) {
+  if (!b || !lists_s) return SBSLPM_ERR_ARG;
+  *lists_s = b->lists_s;
   return SBSLPM_OK;
 }
 

@@ -1040,7 +1040,10 @@ __global__ void k_reduce_groups(const double* __restrict__ partial, int groups, 
 // combination.  bve_departure_to_target (src/bve_time_step.cpp:15-67):
 // new vorticity = BLI(vor)(dep) + 2 Omega dep_z - 2 Omega z, tracers by BLI.
 // mode bit 1: compute departure points (else read dep); bit 2: remap (else
-// write dep).
+// write dep).  The locations use locate_basis_rcp (one division per
+// direction of the barycentric basis, reciprocals in the projections): the
+// kernel is bound by float64 division and atan latency, not by its 136 bytes
+// of traffic per particle.
 
 template <int D>
 __device__ __forceinline__ void depart_remap_body(const StepGeom& g, const BliTable& tab, long o,
@@ -1059,28 +1062,28 @@ __device__ __forceinline__ void depart_remap_body(const StepGeom& g, const BliTa
     const double x0 = x[o], y0 = y[o], z0 = z[o];
     const double k1x = v3[o], k1y = v3[n + o], k1z = v3[2 * n + o];
     double xx = x0 - 0.5 * dt * k1x, yy = y0 - 0.5 * dt * k1y, zz = z0 - 0.5 * dt * k1z;
-    project_to_sphere(xx, yy, zz);
-    locate_basis<D>(g, tab, xx, yy, zz, b, err);
+    project_to_sphere_rcp(xx, yy, zz);
+    locate_basis_rcp<D>(g, tab, xx, yy, zz, b, err);
     double k2x, k2y, k2z;
     gather3<D>(b, v2, n, k2x, k2y, k2z);
     xx = x0 - 0.5 * dt * k2x, yy = y0 - 0.5 * dt * k2y, zz = z0 - 0.5 * dt * k2z;
-    project_to_sphere(xx, yy, zz);
-    locate_basis<D>(g, tab, xx, yy, zz, b, err);
+    project_to_sphere_rcp(xx, yy, zz);
+    locate_basis_rcp<D>(g, tab, xx, yy, zz, b, err);
     double k3x, k3y, k3z;
     gather3<D>(b, v1, n, k3x, k3y, k3z);
     xx = x0 - dt * k3x, yy = y0 - dt * k3y, zz = z0 - dt * k3z;
-    project_to_sphere(xx, yy, zz);
-    locate_basis<D>(g, tab, xx, yy, zz, b, err);
+    project_to_sphere_rcp(xx, yy, zz);
+    locate_basis_rcp<D>(g, tab, xx, yy, zz, b, err);
     double k4x, k4y, k4z;
     gather3<D>(b, v0, n, k4x, k4y, k4z);
     xx = x0 - 1.0 / 6.0 * dt * k1x, yy = y0 - 1.0 / 6.0 * dt * k1y, zz = z0 - 1.0 / 6.0 * dt * k1z;
-    project_to_sphere(xx, yy, zz);
+    project_to_sphere_rcp(xx, yy, zz);
     xx -= -1.0 / 3.0 * dt * k2x, yy -= -1.0 / 3.0 * dt * k2y, zz -= -1.0 / 3.0 * dt * k2z;
-    project_to_sphere(xx, yy, zz);
+    project_to_sphere_rcp(xx, yy, zz);
     xx -= -1.0 / 3.0 * dt * k3x, yy -= -1.0 / 3.0 * dt * k3y, zz -= -1.0 / 3.0 * dt * k3z;
-    project_to_sphere(xx, yy, zz);
+    project_to_sphere_rcp(xx, yy, zz);
     xx -= -1.0 / 6.0 * dt * k4x, yy -= -1.0 / 6.0 * dt * k4y, zz -= -1.0 / 6.0 * dt * k4z;
-    project_to_sphere(xx, yy, zz);
+    project_to_sphere_rcp(xx, yy, zz);
     dx = xx;
     dy = yy;
     dz = zz;
@@ -1095,7 +1098,7 @@ __device__ __forceinline__ void depart_remap_body(const StepGeom& g, const BliTa
     dz = dep[2 * n + o];
   }
   if (mode & 2) {
-    locate_basis<D>(g, tab, dx, dy, dz, b, err);
+    locate_basis_rcp<D>(g, tab, dx, dy, dz, b, err);
     double vor = gather<D>(b, vors);
     for (int k = 0; k < T; k++) new_tracers[o * T + k] = gather<D>(b, tracers, T, k);
     vor += 2 * g.omega * dz;

@@ -116,12 +116,18 @@ void launch_inv_lap(long n, const double* x, const double* y, const double* z, c
 // chunk's raw sums to partial[chunk][3][q], then a reduction adds each
 // target's chunks in list order into tgt ([3][panels*q]).  chunks[c] =
 // (target, first entry, end entry, 0); cstart[panels+1] is the CSR of chunks
-// by target.
+// by target.  Mixed precision with direct_tpt = 1 or 2: the barrier-free
+// form (k_cc32d: direct_tpt target proxies per thread, sources read through
+// L1 from the pair-transposed copy srcp that launch_cc_pair_sources makes of
+// the packed proxy sources; cc_direct_shape_ok).
 bool cc_chunk_supported(int q);
 bool cc_chunk_shape_ok(int q, int slots);
-int cc_chunk_threads(int q, int slots);
+bool cc_direct_shape_ok(int q, int slots, int tpt);
+int cc_chunk_threads(int q, int slots, int direct_tpt = 0);
+void launch_cc_pair_sources(const float4* srcf, int q, int panels, float4* srcp, cudaStream_t st);
 void launch_cc_chunks(const StepGeom& g, int precision, int slots, const int4* chunks, int nchunks, const int* cstart,
-                      const double4* src, double* partial, double* tgt, cudaStream_t st);
+                      const double4* src, double* partial, double* tgt, cudaStream_t st, int direct_tpt = 0,
+                      const float4* srcp = nullptr);
 void build_cc_chunks(const std::vector<int>& start, int chunk_len, std::vector<int4>& chunks,
                      std::vector<int>& cstart);
 

@@ -123,6 +123,99 @@ __global__ void __launch_bounds__(CcShape<Q, S>::NT)
   }
 }
 
+// Mixed precision without shared-memory staging: the source proxies are read
+// straight from a pair-transposed copy (srcp: per panel, proxies (2k, 2k+1)
+// as (x0,x1,y0,y1),(z0,z1,w0,w1), a zero-strength partner after an odd
+// count) through the L1 cache, where a warp's lanes share every 16-byte
+// load, so a slot walks its chunk with no barrier at all.  A thread holds TPT
+// target proxies (j, j + QT, ...), so each pair of source loads feeds TPT
+// targets.
+template <int Q, int S, int TPT>
+struct CcDirectShape {
+  static constexpr int QT = (Q + TPT - 1) / TPT;  // threads per slot
+  static constexpr int NT = (S * QT + 31) / 32 * 32;
+  static constexpr bool ok = NT <= 512 && 5 * S * QT >= 4 * NT;  // at most a fifth of the lanes idle
+};
+
+template <int Q, int S, int TPT, bool GUARD>
+__global__ void __launch_bounds__(CcDirectShape<Q, S, TPT>::NT)
+    k_cc32d(StepGeom g, const int4* __restrict__ chunks, int nchunks, const float4* __restrict__ srcp,
+            double* __restrict__ partial) {
+  constexpr int Q2 = (Q + 1) / 2, QT = CcDirectShape<Q, S, TPT>::QT;
+  const int h = threadIdx.x / QT, jt = threadIdx.x - h * QT;
+  const int c = blockIdx.x * S + h;
+  if (h >= S || c >= nchunks) return;  // no barrier below: idle lanes leave
+  const int4 ch = chunks[c];
+  const long pn = (long)g.panels * Q;
+  const double* ct = g.pd_centre + 4 * (long)ch.x;
+  const double cx = ct[0], cy = ct[1], cz = ct[2];
+  float dtx[TPT], dty[TPT], dtz[TPT];
+  double ax[TPT], ay[TPT], az[TPT];
+#pragma unroll
+  for (int r = 0; r < TPT; r++) {
+    const int j = jt + r * QT;
+    const long o = (long)ch.x * Q + (j < Q ? j : 0);
+    dtx[r] = (float)((g.px[o] - cx) * kPackScale);
+    dty[r] = (float)((g.px[pn + o] - cy) * kPackScale);
+    dtz[r] = (float)((g.px[2 * pn + o] - cz) * kPackScale);
+    ax[r] = ay[r] = az[r] = 0;
+  }
+  const float feps = (float)g.eps;
+  const float2 eps2 = make_float2(feps, feps);
+  for (int e = ch.y; e < ch.z; e++) {
+    const int sp = __ldg(g.src_panel + e);
+    const double* cs = g.pd_centre + 4 * (long)sp;
+    const float bx0 = (float)((cs[0] - cx) * kPackScale), by0 = (float)((cs[1] - cy) * kPackScale),
+                bz0 = (float)((cs[2] - cz) * kPackScale);
+    float2 bx[TPT], by[TPT], bz[TPT], fx[TPT], fy[TPT], fz[TPT];
+#pragma unroll
+    for (int r = 0; r < TPT; r++) {
+      const float b0 = bx0 - dtx[r], b1 = by0 - dty[r], b2 = bz0 - dtz[r];
+      bx[r] = make_float2(b0, b0);
+      by[r] = make_float2(b1, b1);
+      bz[r] = make_float2(b2, b2);
+      fx[r] = fy[r] = fz[r] = make_float2(0.f, 0.f);
+    }
+    const float4* sb = srcp + (long)sp * 2 * Q2;
+#pragma unroll 8
+    for (int k2 = 0; k2 < Q2; k2++) {
+      const float4 A = __ldg(sb + 2 * k2), B = __ldg(sb + 2 * k2 + 1);
+      const float2 sx = make_float2(A.x, A.y), sy = make_float2(A.z, A.w), sz = make_float2(B.x, B.y),
+                   sw = make_float2(B.z, B.w);
+#pragma unroll
+      for (int r = 0; r < TPT; r++) pair32x2<GUARD>(bx[r], by[r], bz[r], sx, sy, sz, sw, eps2, fx[r], fy[r], fz[r]);
+    }
+#pragma unroll
+    for (int r = 0; r < TPT; r++) {
+      ax[r] += (double)fx[r].x + (double)fx[r].y;
+      ay[r] += (double)fy[r].x + (double)fy[r].y;
+      az[r] += (double)fz[r].x + (double)fz[r].y;
+    }
+  }
+  double* p = partial + (long)c * 3 * Q;
+#pragma unroll
+  for (int r = 0; r < TPT; r++) {
+    const int j = jt + r * QT;
+    if (j >= Q) continue;
+    p[j] = ax[r];
+    p[Q + j] = ay[r];
+    p[2 * Q + j] = az[r];
+  }
+}
+
+// The pair-transposed copy of the packed proxy sources that k_cc32d reads.
+__global__ void k_cc_pair_sources(const float4* __restrict__ srcf, int q, long pairs, float4* __restrict__ srcp) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= pairs) return;
+  const int q2 = (q + 1) / 2;
+  const long p = i / q2;
+  const int k = (int)(i - p * q2);
+  const float4 s0 = srcf[p * q + 2 * k];
+  const float4 s1 = 2 * k + 1 < q ? srcf[p * q + 2 * k + 1] : make_float4(0.f, 0.f, 0.f, 0.f);
+  srcp[2 * i] = make_float4(s0.x, s1.x, s0.y, s1.y);
+  srcp[2 * i + 1] = make_float4(s0.z, s1.z, s0.w, s1.w);
+}
+
 // Float64: the same slots and chunks with absolute proxy positions (pair64).
 template <int Q, int S, bool GUARD>
 __global__ void __launch_bounds__(CcShape<Q, S>::NT)
@@ -322,6 +415,43 @@ void launch_q_s(const StepGeom& g, bool mixed, const int4* chunks, int nchunks, 
   }
 }
 
+template <int Q, int S, int TPT>
+void launch_direct_s(const StepGeom& g, const int4* chunks, int nchunks, const float4* srcp, double* partial,
+                     cudaStream_t st) {
+  if constexpr (CcDirectShape<Q, S, TPT>::ok) {
+    constexpr int NT = CcDirectShape<Q, S, TPT>::NT;
+    const unsigned grid = (unsigned)((nchunks + S - 1) / S);
+    if (!(g.eps > 0)) SB_LAUNCH((k_cc32d<Q, S, TPT, true>), grid, NT, 0, st, g, chunks, nchunks, srcp, partial);
+    else SB_LAUNCH((k_cc32d<Q, S, TPT, false>), grid, NT, 0, st, g, chunks, nchunks, srcp, partial);
+  }
+}
+
+template <int Q, int TPT>
+void launch_direct_t(const StepGeom& g, int slots, const int4* chunks, int nchunks, const float4* srcp,
+                     double* partial, cudaStream_t st) {
+  switch (slots) {
+    case 1: launch_direct_s<Q, 1, TPT>(g, chunks, nchunks, srcp, partial, st); break;
+    case 2: launch_direct_s<Q, 2, TPT>(g, chunks, nchunks, srcp, partial, st); break;
+    case 3: launch_direct_s<Q, 3, TPT>(g, chunks, nchunks, srcp, partial, st); break;
+    case 4: launch_direct_s<Q, 4, TPT>(g, chunks, nchunks, srcp, partial, st); break;
+    case 6: launch_direct_s<Q, 6, TPT>(g, chunks, nchunks, srcp, partial, st); break;
+    default: launch_direct_s<Q, 8, TPT>(g, chunks, nchunks, srcp, partial, st); break;
+  }
+}
+
+template <int Q, int TPT>
+bool direct_ok_t(int slots) {
+  switch (slots) {
+    case 1: return CcDirectShape<Q, 1, TPT>::ok;
+    case 2: return CcDirectShape<Q, 2, TPT>::ok;
+    case 3: return CcDirectShape<Q, 3, TPT>::ok;
+    case 4: return CcDirectShape<Q, 4, TPT>::ok;
+    case 6: return CcDirectShape<Q, 6, TPT>::ok;
+    case 8: return CcDirectShape<Q, 8, TPT>::ok;
+    default: return false;
+  }
+}
+
 template <int Q>
 void launch_q(const StepGeom& g, bool mixed, int slots, const int4* chunks, int nchunks, const double4* src,
               double* partial, cudaStream_t st) {
@@ -364,12 +494,38 @@ bool cc_chunk_shape_ok(int q, int slots) {
   }
 }
 
-int cc_chunk_threads(int q, int slots) { return (slots * q + 31) / 32 * 32; }
+int cc_chunk_threads(int q, int slots, int direct_tpt) {
+  const int qt = direct_tpt > 0 ? (q + direct_tpt - 1) / direct_tpt : q;
+  return (slots * qt + 31) / 32 * 32;
+}
+
+bool cc_direct_shape_ok(int q, int slots, int tpt) {
+  if (tpt != 1 && tpt != 2) return false;
+#define SB_DOK(Q)                                                         \
+  case Q:                                                                 \
+    return tpt == 1 ? direct_ok_t<Q, 1>(slots) : direct_ok_t<Q, 2>(slots);
+  switch (q) { SB_DOK(36) SB_DOK(49) SB_DOK(64) SB_DOK(81) SB_DOK(100) SB_DOK(121) default: return false; }
+#undef SB_DOK
+}
+
+void launch_cc_pair_sources(const float4* srcf, int q, int panels, float4* srcp, cudaStream_t st) {
+  const long pairs = (long)panels * ((q + 1) / 2);
+  SB_LAUNCH(k_cc_pair_sources, blocks_for(pairs, 256), 256, 0, st, srcf, q, pairs, srcp);
+}
 
 void launch_cc_chunks(const StepGeom& g, int precision, int slots, const int4* chunks, int nchunks, const int* cstart,
-                      const double4* src, double* partial, double* out, cudaStream_t st) {
+                      const double4* src, double* partial, double* out, cudaStream_t st, int direct_tpt,
+                      const float4* srcp) {
   const bool mixed = precision == SBSLPM_MIXED;
-  if (nchunks > 0) {
+  if (nchunks > 0 && mixed && direct_tpt > 0) {
+#define SB_DQ(Q)                                                                          \
+  case Q:                                                                                 \
+    if (direct_tpt == 1) launch_direct_t<Q, 1>(g, slots, chunks, nchunks, srcp, partial, st); \
+    else launch_direct_t<Q, 2>(g, slots, chunks, nchunks, srcp, partial, st);                 \
+    break;
+    switch (g.q) { SB_DQ(36) SB_DQ(49) SB_DQ(64) SB_DQ(81) SB_DQ(100) SB_DQ(121) default: break; }
+#undef SB_DQ
+  } else if (nchunks > 0) {
     switch (g.q) {
       case 36: launch_q<36>(g, mixed, slots, chunks, nchunks, src, partial, st); break;
       case 49: launch_q<49>(g, mixed, slots, chunks, nchunks, src, partial, st); break;

@@ -31,9 +31,9 @@
 // 8-wide K step) and stride byte offset KC * 32 (consecutive 8-row groups).
 // Every operand address the MMAs can form stays inside its chunk image.
 //
-// Every wait is bounded (one second of %globaltimer); a wait that runs out
-// sets kErrTimeout, waits (bounded) for the MMAs already issued, frees the
-// tensor memory and returns.
+// Every wait is bounded (one second of %globaltimer, CcTcGroup::wait_ns); a
+// wait that runs out sets kErrTimeout, waits (bounded) for the MMAs already
+// issued, frees the tensor memory and returns.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -45,7 +45,6 @@ namespace sbslpm {
 namespace {
 
 constexpr int kCcThreads = 512;  // producer threads; one more warp issues the MMAs
-constexpr unsigned long long kWaitNs = 1000000000ull;  // bound of every mbarrier wait
 
 __host__ __device__ constexpr int cc_rows(int Q) { return (3 * Q + 127) / 128 * 128; }
 
@@ -81,7 +80,7 @@ __device__ __forceinline__ void mma_commit(uint32_t bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" : : "r"(bar) : "memory");
 }
 
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, unsigned long long bound_ns) {
   const unsigned long long t0 = global_ns();
   while (true) {
     uint32_t done;
@@ -93,7 +92,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
         : "r"(bar), "r"(parity)
         : "memory");
     if (done) return true;
-    if (global_ns() - t0 > kWaitNs) return false;
+    if (global_ns() - t0 > bound_ns) return false;
   }
 }
 
@@ -142,8 +141,9 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
 }
 
 // Waits for the phase of the given parity, or until the CTA's abort flag is
-// set (by another thread's expired wait) or one second passes (sets it).
-__device__ __forceinline__ bool mbar_wait_abortable(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
+// set (by another thread's expired wait) or bound_ns pass (sets it).
+__device__ __forceinline__ bool mbar_wait_abortable(uint32_t bar, uint32_t parity, volatile int* abort_flag,
+                                                    unsigned long long bound_ns) {
   const unsigned long long t0 = global_ns();
   while (true) {
     uint32_t done;
@@ -156,7 +156,7 @@ __device__ __forceinline__ bool mbar_wait_abortable(uint32_t bar, uint32_t parit
         : "memory");
     if (done) return true;
     if (*abort_flag) return false;
-    if (global_ns() - t0 > kWaitNs) {
+    if (global_ns() - t0 > bound_ns) {
       *abort_flag = 1;
       return false;
     }
@@ -253,7 +253,8 @@ __global__ void __launch_bounds__(kCcThreads + 32, 1) k_cc_tc(CcTcGroup g) {
     int c = 0;
     for (; c < total; c++) {
       // warp-uniform decision, so that the warp stays converged for the exit path
-      if (!__all_sync(0xffffffffu, mbar_wait_abortable(smem_u32(&full[c & 1]), (uint32_t)((c >> 1) & 1), abort_flag)))
+      if (!__all_sync(0xffffffffu, mbar_wait_abortable(smem_u32(&full[c & 1]), (uint32_t)((c >> 1) & 1), abort_flag,
+                                                       g.wait_ns)))
         break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       if (lane == 0) {
@@ -325,8 +326,8 @@ __global__ void __launch_bounds__(kCcThreads + 32, 1) k_cc_tc(CcTcGroup g) {
       const int slot = i & 1, ring = i % kRing;
       if (i >= 2) {
         // warp-uniform decision: the flush below needs the whole warp
-        if (!__all_sync(0xffffffffu,
-                        mbar_wait_abortable(smem_u32(&empty[slot]), (uint32_t)(((i >> 1) - 1) & 1), abort_flag)))
+        if (!__all_sync(0xffffffffu, mbar_wait_abortable(smem_u32(&empty[slot]), (uint32_t)(((i >> 1) - 1) & 1),
+                                                         abort_flag, g.wait_ns)))
           break;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         // chunk i - 2 is complete: if it closed a source cluster, fold that cluster in
@@ -389,7 +390,7 @@ __global__ void __launch_bounds__(kCcThreads + 32, 1) k_cc_tc(CcTcGroup g) {
         }
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      mbar_arrive(smem_u32(&full[slot]));
+      if (!(g.withhold && i == 0 && tid == 0)) mbar_arrive(smem_u32(&full[slot]));
     }
     asm volatile("cp.async.wait_all;" ::: "memory");
   }
@@ -397,7 +398,7 @@ __global__ void __launch_bounds__(kCcThreads + 32, 1) k_cc_tc(CcTcGroup g) {
   // every MMA committed is complete before the sums are read and the memory freed
   int good = 1;
   if (tid == 0 && s_last >= 0)
-    good = mbar_wait(smem_u32(&empty[s_last & 1]), (uint32_t)((s_last >> 1) & 1));
+    good = mbar_wait(smem_u32(&empty[s_last & 1]), (uint32_t)((s_last >> 1) & 1), g.wait_ns);
   const bool ok = __syncthreads_and(good && !s_abort && s_last == total - 1);
   if (!ok && tid == 0) dev::flag(g.err, kErrTimeout);
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");

@@ -43,6 +43,11 @@ struct CcTcGroup {
   const BatchMember* mem;
   unsigned* err;
   size_t smem3, smem1;  // dynamic shared memory of the 3xTF32 / TF32 kernels (cc_tc_prepare)
+  // bound of every mbarrier wait (ns); withhold = 1 keeps one producer
+  // thread of every CTA from arriving on the first chunk's barrier, so that
+  // the MMA warp's wait runs out (the timeout path's test; no MMA is issued)
+  unsigned long long wait_ns = 1000000000ull;
+  int withhold = 0;
 };
 
 // Kernel attributes and launch shared memory of a group; call once, outside

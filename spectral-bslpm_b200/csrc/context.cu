@@ -180,8 +180,10 @@ sbslpm_status precompute_tree(sbslpm_ctx* c) {
   SB_TRY(upload(&c->flx, t.lx));
   SB_TRY(upload(&c->fly, t.ly));
 
-  TreeLists l;
-  build_tree_lists(t, c->cfg.fmm_theta, l);
+  // the traversal of the tree on the GPU (the same list, in the same order, as on the host)
+  std::vector<TreeLists> lv;
+  SB_TRY(device_tree_lists(t, std::vector<double>{c->cfg.fmm_theta}, lv, nullptr));
+  TreeLists& l = lv[0];
   c->n_near = l.ns.back();
   c->n_cc = l.cs.back();
   c->list = l.list;
@@ -222,6 +224,7 @@ sbslpm_status precompute_tree(sbslpm_ctx* c) {
   if (c->cfg.precision == SBSLPM_MIXED) {
     SB_TRY(dalloc(&c->fsrcf, pn));
     SB_TRY(dalloc(&c->psrcf, N));
+    if (c->cc_partial) SB_TRY(dalloc(&c->fsrcp, (size_t)t.Pf * 2 * ((t.qx + 1) / 2)));
   }
   return SBSLPM_OK;
 }
@@ -308,8 +311,9 @@ namespace sbslpm {
 void launch_tree_cc(sbslpm_ctx* c, cudaStream_t st) {
   if (c->cc_partial && c->cc_slots > 0) {
     const int k = c->cc_len - 1;
+    if (c->cc_tpt > 0) launch_cc_pair_sources(c->fsrcf, c->qx, c->Pf, c->fsrcp, st);
     launch_cc_chunks(c->fgeom, c->cfg.precision, c->cc_slots, c->cc_chunks[k], c->cc_nchunks[k], c->cc_cstart[k],
-                     c->fsrc, c->cc_partial, c->ftgt, st);
+                     c->fsrc, c->cc_partial, c->ftgt, st, c->cc_tpt, c->fsrcp);
   } else {
     launch_interactions_only(c->fgeom, c->cfg.precision, c->fsrc, c->ftgt, st);
   }
@@ -447,13 +451,17 @@ sbslpm_status cc_autotune(sbslpm_ctx* c) {
   SB_CUDA(cudaEventCreate(&e1));
   double best = 1e30;
   int cand = 0;
-  const int keep_slots = c->cc_slots, keep_len = c->cc_len;
-  int best_slots = keep_slots, best_len = keep_len;
-  for (int sl = 0; sl <= 8; sl++) {  // chunk slots per block; 0: one block per target panel
-    if (sl > 0 && !cc_chunk_shape_ok(c->qx, sl)) continue;
+  const int keep_slots = c->cc_slots, keep_len = c->cc_len, keep_tpt = c->cc_tpt;
+  int best_slots = keep_slots, best_len = keep_len, best_tpt = keep_tpt;
+  // kernel form: 0 staged in shared memory, 1 | 2 barrier-free (mixed precision)
+  const int max_tpt = c->cfg.precision == SBSLPM_MIXED && c->fsrcp ? 2 : 0;
+  for (int tpt = 0; tpt <= max_tpt; tpt++)
+  for (int sl = tpt > 0 ? 1 : 0; sl <= 8; sl++) {  // chunk slots per block; 0: one block per target panel
+    if (sl > 0 && !(tpt > 0 ? cc_direct_shape_ok(c->qx, sl, tpt) : cc_chunk_shape_ok(c->qx, sl))) continue;
     for (int len = sl > 0 ? 1 : 0; len <= (sl > 0 ? 4 : 0); len++) {
       c->cc_slots = sl;
       c->cc_len = len;
+      c->cc_tpt = tpt;
       launch_tree_cc(c, st);
       SB_CUDA(cudaEventRecord(e0, st));
       for (int r = 0; r < 5; r++) launch_tree_cc(c, st);
@@ -466,6 +474,7 @@ sbslpm_status cc_autotune(sbslpm_ctx* c) {
         best = ms / 5;
         best_slots = sl;
         best_len = len;
+        best_tpt = tpt;
       }
     }
   }
@@ -473,6 +482,7 @@ sbslpm_status cc_autotune(sbslpm_ctx* c) {
   cudaEventDestroy(e1);
   c->cc_slots = best_slots;
   c->cc_len = best_len;
+  c->cc_tpt = best_tpt;
   c->cc_candidates = cand;
   c->cc_tuned_ms = best;
   c->cc_tuned = true;
@@ -625,6 +635,20 @@ sbslpm_status sbslpm_dual_tree_traversal(int levels, const sbslpm_panel* panels,
   return SBSLPM_OK;
 }
 
+sbslpm_status sbslpm_dual_tree_traversal_flagged(int levels, const sbslpm_panel* panels, double theta,
+                                                 sbslpm_interact_pair* out, char* near, long cap, long* count) {
+  if (!panels || !count || levels < 1 || levels > 12) return SBSLPM_ERR_ARG;
+  std::vector<sbslpm_panel> p(panels, panels + sbslpm_panel_count(levels));
+  std::vector<sbslpm_interact_pair> list;
+  std::vector<char> flags;
+  build_interactions_flagged(levels, p, theta, list, flags);
+  *count = (long)list.size();
+  const size_t n = std::min<size_t>(cap > 0 ? (size_t)cap : 0, list.size());
+  if (out && n) std::memcpy(out, list.data(), sizeof(sbslpm_interact_pair) * n);
+  if (near && n) std::memcpy(near, flags.data(), n);
+  return SBSLPM_OK;
+}
+
 sbslpm_status sbslpm_interp_vals_bli(double* basis, double xi, double eta, double min_xi, double max_xi,
                                      double min_eta, double max_eta, int degree) {
   if (!basis || degree < 0 || degree > kMaxDegree) return SBSLPM_ERR_ARG;
@@ -720,7 +744,7 @@ sbslpm_status sbslpm_destroy(sbslpm_ctx* c) {
                   c->s_ntan, c->s_pow15, c->s_filt, c->s_ptan, c->s_pface, c->s_ustart, c->s_umem, c->src2,
                   c->srcf2, c->tend, c->avor, c->adj_src, c->adj_vbar, c->adj_q, c->adj_y, c->adj_part,
                   c->adj_w, c->adj_vel, c->adj_near_ts, c->adj_near_tt, c->adj_cc_ts, c->adj_cc_tt, c->adj_tbar,
-                  c->adj_qbl, c->self, c->force, c->d_time, c->cc_partial, c->entry32, c->fentry32};
+                  c->adj_qbl, c->self, c->force, c->d_time, c->cc_partial, c->entry32, c->fentry32, c->fsrcp};
   for (void* b : bufs)
     if (b) cudaFree(b);
   for (int k = 0; k < 4; k++) {
@@ -1054,6 +1078,7 @@ sbslpm_status sbslpm_set_cc_tuning(sbslpm_ctx* c, int slots, int chunk_len) {
     return set_last_error("unsupported well-separated launch shape"), SBSLPM_ERR_ARG;
   c->cc_slots = slots;
   c->cc_len = chunk_len;
+  c->cc_tpt = 0;
   c->cc_candidates = 0;
   c->cc_tuned_ms = 0;
   c->cc_tuned = true;
@@ -1064,13 +1089,33 @@ sbslpm_status sbslpm_set_cc_tuning(sbslpm_ctx* c, int slots, int chunk_len) {
   return SBSLPM_OK;
 }
 
+sbslpm_status sbslpm_set_cc_tuning_direct(sbslpm_ctx* c, int slots, int chunk_len, int targets_per_thread) {
+  if (!c || !c->tree) return SBSLPM_ERR_ARG;
+  if (!c->cc_partial || !c->fsrcp)
+    return set_last_error("the barrier-free well-separated kernel needs mixed precision and 36..121 proxies"),
+           SBSLPM_ERR_CONFIG;
+  if (!cc_direct_shape_ok(c->qx, slots, targets_per_thread) || chunk_len < 1 || chunk_len > 4)
+    return set_last_error("unsupported well-separated launch shape"), SBSLPM_ERR_ARG;
+  SB_TRY(sbslpm_set_cc_tuning(c, 0, 0));
+  c->cc_slots = slots;
+  c->cc_len = chunk_len;
+  c->cc_tpt = targets_per_thread;
+  return SBSLPM_OK;
+}
+
 sbslpm_status sbslpm_cc_tuning(const sbslpm_ctx* c, int* shape, double* ms_per_launch) {
   if (!c || !c->tree || !shape || !ms_per_launch) return SBSLPM_ERR_ARG;
   shape[0] = c->cc_partial && c->cc_slots > 0 ? c->cc_slots : 0;
   shape[1] = c->cc_partial && c->cc_slots > 0 ? c->cc_len : 0;
-  shape[2] = c->cc_partial && c->cc_slots > 0 ? cc_chunk_threads(c->qx, c->cc_slots) : 128;
+  shape[2] = c->cc_partial && c->cc_slots > 0 ? cc_chunk_threads(c->qx, c->cc_slots, c->cc_tpt) : 128;
   shape[3] = c->cc_candidates;
   *ms_per_launch = c->cc_tuned_ms;
+  return SBSLPM_OK;
+}
+
+sbslpm_status sbslpm_cc_form(const sbslpm_ctx* c, int* targets_per_thread) {
+  if (!c || !c->tree || !targets_per_thread) return SBSLPM_ERR_ARG;
+  *targets_per_thread = c->cc_partial && c->cc_slots > 0 ? c->cc_tpt : 0;
   return SBSLPM_OK;
 }
 

@@ -76,6 +76,8 @@ struct sbslpm_ctx {
   int cc_nchunks[4] = {};
   double* cc_partial = nullptr;  // [n_cc][3][qx] chunk sums
   int cc_slots = 1, cc_len = 2;  // chunk slots per block (0: one block per target panel), entries per chunk
+  int cc_tpt = 0;                 // 0: sources staged in shared memory; 1 | 2: barrier-free, targets per thread
+  float4* fsrcp = nullptr;        // pair-transposed packed proxy sources (barrier-free mixed kernel)
   bool cc_tuned = false;
   int cc_candidates = 0;
   double cc_tuned_ms = 0;
@@ -173,7 +175,16 @@ void child_basis_1d(const std::vector<sbslpm_panel>& P, const BliTable& tab, int
 void bli_table(int n, BliTable& t);
 sbslpm_status build_tree_tables(int L, int d, const std::vector<sbslpm_panel>& grid, int leaf_size, int n,
                                 TreeTables& t);
+// The treecode's lists from the traversal of its tree (list in traversal
+// order, near[e] = 1 for pairs that failed the MAC): on the host
+// (build_tree_lists) or from a traversal made elsewhere (tree_lists_from;
+// device_tree_lists runs the members' traversals on the GPU in one launch
+// series).
 void build_tree_lists(const TreeTables& t, double theta, TreeLists& l);
+void tree_lists_from(const TreeTables& t, std::vector<sbslpm_interact_pair>&& list, const std::vector<char>& near,
+                     TreeLists& l);
+sbslpm_status device_tree_lists(const TreeTables& t, const std::vector<double>& theta, std::vector<TreeLists>& out,
+                                cudaStream_t st);
 sbslpm_status near_autotune(sbslpm_ctx* c, const double* x, const double* y, const double* z, const double* area,
                             const double* vors);
 // The treecode's well-separated interactions into ftgt (chunked kernels where q allows).

@@ -131,6 +131,107 @@ __device__ __forceinline__ void locate_basis(const StepGeom& g, const BliTable& 
   b.row = (long)(leaf - g.offset) * g.q;
 }
 
+// The same basis with fewer float64 divisions, for the departure / remap
+// kernel (one thread per particle, four locations each): the projection and
+// the face coordinates multiply by one reciprocal, and the barycentric basis
+// uses the common-denominator form f_i = w_i P_i / sum_k w_k P_k with
+// P_i = prod_{j != i} (t - c_j) -- the second barycentric form multiplied
+// through by prod_j (t - c_j): one division per direction instead of 2(D+1).
+// Nodes within 1e-15 are hit exactly as in bli_1d; results differ from
+// locate_basis by rounding only.
+template <int D>
+__device__ __forceinline__ void bli_1d_common(double t, double lo, double hi, const BliTable& tab, double* f,
+                                              unsigned& err) {
+  const double range = 0.5 * (hi - lo), offset = 0.5 * (hi + lo);
+  if (t < lo - 1e-15 || t > hi + 1e-15) err |= kErrOutOfPanel;
+  if (D == 0) {
+    f[0] = 1;
+    return;
+  }
+  double dl[D + 1];
+  int hit = -1;
+#pragma unroll
+  for (int i = 0; i <= D; i++) {
+    dl[i] = t - (tab.cosv[i] * range + offset);
+    if (hit < 0 && fabs(dl[i]) < 1e-15) hit = i;
+  }
+  if (hit >= 0) {
+#pragma unroll
+    for (int i = 0; i <= D; i++) f[i] = (i == hit) ? 1.0 : 0.0;
+    return;
+  }
+  double pre[D + 1], suf = 1.0, den = 0.0;
+  pre[0] = 1.0;
+#pragma unroll
+  for (int i = 1; i <= D; i++) pre[i] = pre[i - 1] * dl[i - 1];
+#pragma unroll
+  for (int i = D; i >= 0; i--) {
+    f[i] = tab.w[i] * (pre[i] * suf);
+    den += f[i];
+    suf *= dl[i];
+  }
+  const double inv = 1.0 / den;
+#pragma unroll
+  for (int i = 0; i <= D; i++) f[i] *= inv;
+}
+
+__device__ __forceinline__ void project_to_sphere_rcp(double& x, double& y, double& z) {
+  const double inv = 1.0 / sqrt(x * x + y * y + z * z);
+  x *= inv;
+  y *= inv;
+  z *= inv;
+}
+
+template <int D>
+__device__ __forceinline__ void locate_basis_rcp(const StepGeom& g, const BliTable& tab, double x, double y, double z,
+                                                 Basis<D>& b, unsigned& err) {
+  const int face = face_from_xyz(x, y, z);
+  double xi, eta;
+  switch (face) {  // xieta_from_xyz_face with one reciprocal of the face's axis coordinate
+    case 0: { const double r = 1.0 / x; xi = atan(y * r); eta = atan(z * r); break; }
+    case 1: { const double r = 1.0 / y; xi = atan(-x * r); eta = atan(z * r); break; }
+    case 2: { const double r = 1.0 / x; xi = atan(y * r); eta = atan(-z * r); break; }
+    case 3: { const double r = 1.0 / y; xi = atan(-x * r); eta = atan(-z * r); break; }
+    case 4: { const double r = 1.0 / z; xi = atan(y * r); eta = atan(-x * r); break; }
+    default: { const double r = 1.0 / z; xi = atan(-y * r); eta = atan(-x * r); break; }
+  }
+  // tree descent of locate_leaf from the face's coordinates
+  Bounds bd{-1, 1, -1, 1};
+  int id = face;
+  for (int lev = 0; lev < g.levels - 1; lev++) {
+    const double mid_xi = 0.5 * kPi / 4.0 * (bd.max_xi + bd.min_xi);
+    const double mid_eta = 0.5 * kPi / 4.0 * (bd.max_eta + bd.min_eta);
+    const double ux = 0.5 * (bd.max_xi + bd.min_xi), ue = 0.5 * (bd.max_eta + bd.min_eta);
+    int c;
+    if ((xi >= mid_xi) && (eta >= mid_eta)) {
+      c = 0;
+      bd.min_xi = ux;
+      bd.min_eta = ue;
+    } else if ((xi <= mid_xi) && (eta >= mid_eta)) {
+      c = 1;
+      bd.max_xi = ux;
+      bd.min_eta = ue;
+    } else if ((xi <= mid_xi) && (eta <= mid_eta)) {
+      c = 2;
+      bd.max_xi = ux;
+      bd.max_eta = ue;
+    } else if ((xi >= mid_xi) && (eta <= mid_eta)) {
+      c = 3;
+      bd.min_xi = ux;
+      bd.max_eta = ue;
+    } else {
+      err |= kErrNonFinite;  // NaN coordinates
+      c = 0;
+      bd.min_xi = ux;
+      bd.min_eta = ue;
+    }
+    id = level_start(lev + 1) + 4 * (id - level_start(lev)) + c;
+  }
+  bli_1d_common<D>(xi, kPi / 4.0 * bd.min_xi, kPi / 4.0 * bd.max_xi, tab, b.fx, err);
+  bli_1d_common<D>(eta, kPi / 4.0 * bd.min_eta, kPi / 4.0 * bd.max_eta, tab, b.fe, err);
+  b.row = (long)(id - g.offset) * g.q;
+}
+
 // sum_m field[row + m] * fx[i] fe[j] with m = i (D+1) + j, in m order.
 template <int D>
 __device__ __forceinline__ double gather(const Basis<D>& b, const double* __restrict__ f, long stride = 1,

@@ -46,8 +46,14 @@ void build_swe_tables(int degree, const std::vector<sbslpm_panel>& panels, int o
 
 void set_last_error(const std::string& msg);
 
-// traversal.cu: dual_tree_traversal on the device (same list, same order as build_interactions)
+// traversal.cu: dual_tree_traversal on the device (same list, same order as build_interactions);
+// the multi form runs one traversal per theta in one launch series and, with
+// near, records per pair whether it failed the MAC (build_interactions_flagged)
 sbslpm_status device_dual_tree_traversal(int levels, const std::vector<sbslpm_panel>& P, double theta,
                                          std::vector<sbslpm_interact_pair>& out, cudaStream_t st);
+sbslpm_status device_dual_tree_traversal_multi(int levels, const std::vector<sbslpm_panel>& P,
+                                               const std::vector<double>& theta,
+                                               std::vector<std::vector<sbslpm_interact_pair>>& out,
+                                               std::vector<std::vector<char>>* near, cudaStream_t st);
 
 }  // namespace sbslpm

@@ -115,9 +115,26 @@ sbslpm_status build_tree_tables(int L, int d, const std::vector<sbslpm_panel>& g
 // to the first leaf) and well-separated pairs (proxy x proxy, CSR by target
 // panel), each in traversal order within a target.
 void build_tree_lists(const TreeTables& t, double theta, TreeLists& l) {
-  const int Pf = t.Pf, Af = t.Af, offf = Pf - Af;
+  std::vector<sbslpm_interact_pair> list;
   std::vector<char> near;
-  build_interactions_flagged(t.Lf, t.fpanels, theta, l.list, near);
+  build_interactions_flagged(t.Lf, t.fpanels, theta, list, near);
+  tree_lists_from(t, std::move(list), near, l);
+}
+
+sbslpm_status device_tree_lists(const TreeTables& t, const std::vector<double>& theta, std::vector<TreeLists>& out,
+                                cudaStream_t st) {
+  std::vector<std::vector<sbslpm_interact_pair>> lists;
+  std::vector<std::vector<char>> near;
+  SB_TRY(device_dual_tree_traversal_multi(t.Lf, t.fpanels, theta, lists, &near, st));
+  out.resize(theta.size());
+  for (size_t m = 0; m < theta.size(); m++) tree_lists_from(t, std::move(lists[m]), near[m], out[m]);
+  return SBSLPM_OK;
+}
+
+void tree_lists_from(const TreeTables& t, std::vector<sbslpm_interact_pair>&& list, const std::vector<char>& near,
+                     TreeLists& l) {
+  const int Pf = t.Pf, Af = t.Af, offf = Pf - Af;
+  l.list = std::move(list);
   l.ns.assign(Af + 1, 0);
   l.cs.assign(Pf + 1, 0);
   for (size_t e = 0; e < l.list.size(); e++) {

@@ -16,7 +16,10 @@ scale-free, so it compares directly with the unit-sphere run.
 
 Prints, every 10 steps, the area-weighted relative L2 height drift
 |h - h0| / |h0| until the run becomes non-finite or reaches the last step,
-and writes the curve to tests/golden/swe_drift_reference_L<levels>.json.
+and writes the curve so far to tests/golden/swe_drift_reference_L<levels>.json
+after every 10 steps (the reference stops the process with Kokkos::abort when
+a non-finite departure point reaches its point location, so the file holds
+the curve up to the last finite state; "stopped" records the abort).
 
 Usage:  make -C oracle ref REF=<checkout> &&
         OMP_NUM_THREADS=<n> python tests/golden/swe_drift_reference.py <levels> [<steps>]
@@ -66,22 +69,26 @@ def main():
     w = area / area.sum()
     h0 = height.copy()
     l2 = lambda a: float(np.sqrt((w * a * a).sum()))
-    curve, done, t0 = [], 0, time.time()
+    out = {"levels": levels, "particles": int(x.size), "threads": ref.lib.ref_num_threads(), "dt": 0.002,
+           "time_scale": S, "theta": 0.7, "degree": 3, "kernel_eps": EPS, "noise_seed": 4, "curve": [],
+           "stopped": f"Kokkos::abort (point location of a non-finite point) before step {nsteps}"}
+    path = os.path.join(HERE, f"swe_drift_reference_L{levels}.json")
+    done, t0 = 0, time.time()
     while done < nsteps:
         vors, divs, height, vel, _ = ref.swe_step(c, vors, divs, height, base, smap, vel=vel, time=float(done),
                                                    nsteps=10, driver_unify=True)
         done += 10
         finite = bool(np.isfinite(height).all())
         drift = l2(height - h0) / l2(h0) if finite else None
-        curve.append({"step": done, "height_l2_drift": drift})
+        out["curve"].append({"step": done, "height_l2_drift": drift})
+        if done >= nsteps or not finite:
+            out["stopped"] = None if finite else f"non-finite height at step {done}"
         print(f"levels {levels} step {done}: drift {drift}  ({time.time() - t0:.0f} s)", flush=True)
+        with open(path, "w") as f:
+            json.dump(out, f, indent=1)
         if not finite:
             break
     ref.destroy(c)
-    out = {"levels": levels, "particles": int(x.size), "threads": ref.lib.ref_num_threads(), "dt": 0.002,
-           "time_scale": S, "theta": 0.7, "degree": 3, "kernel_eps": EPS, "noise_seed": 4, "curve": curve}
-    with open(os.path.join(HERE, f"swe_drift_reference_L{levels}.json"), "w") as f:
-        json.dump(out, f, indent=1)
 
 
 if __name__ == "__main__":

@@ -214,6 +214,26 @@ def test_tensor_core_cc_matches_cuda_core_pairs(sb, mode, tol):
         assert rel(vt[k], vr[k]) <= tol, k
 
 
+def test_tensor_core_wait_runs_out_and_the_batch_recovers(sb):
+    """The tensor-core kernel's failure path: with one producer arrival
+    withheld in every CTA (sbslpm_batch_set_wait_test), the MMA warp's
+    bounded wait runs out before any MMA is issued, the CTA frees its tensor
+    memory and returns, and the step reports SBSLPM_ERR_TIMEOUT.  The next
+    step with the test off gives the normal result bit for bit."""
+    g, xyza, vors = grid_and_vors(sb, len(THETA))
+    tc = sb.Batch(base_cfg(sb, sb.MIXED), THETA, PDEG)
+    tc.set_tuning(128, 2, 2)
+    tc.set_cc_mode(1)
+    v0, vel0 = batch_step(sb, tc, xyza, vors)  # a normal step first (and the first-step timing)
+    tc.set_wait_test(True)
+    with pytest.raises(sb.SbslpmError) as err:
+        batch_step(sb, tc, xyza, vors)
+    assert err.value.status == 7  # SBSLPM_ERR_TIMEOUT
+    tc.set_wait_test(False)
+    v1, vel1 = batch_step(sb, tc, xyza, vors)
+    assert torch.equal(v1, v0) and torch.equal(vel1, vel0)
+
+
 def test_cc_autotuner_times_every_mode(sb):
     g, xyza, vors = grid_and_vors(sb, len(THETA))
     batch = sb.Batch(base_cfg(sb, sb.MIXED), THETA, PDEG)

@@ -1,7 +1,9 @@
 """GPU tests of the treecode's well-separated (cluster-cluster) launch shapes:
 every chunked shape (1..8 chunk slots per block, 1..4 list entries per
 chunk) against the whole-panel kernel, for every proxy count with a chunked
-kernel, in both precisions, through the C ABI (sbslpm_set_cc_tuning).
+kernel, in both precisions, and the barrier-free mixed-precision form against
+the staged one, through the C ABI (sbslpm_set_cc_tuning,
+sbslpm_set_cc_tuning_direct).
 
 The shapes evaluate the same pairs with the same per-source-panel arithmetic
 and differ only in the order in which a target's float64 sums are added, so
@@ -38,6 +40,18 @@ def shapes(q):
     return out
 
 
+def direct_shapes(q, tpt):
+    """(slots, chunk length) of the barrier-free form with tpt target proxies
+    per thread: ceil(q / tpt) threads per slot, the same block rule."""
+    qt = -(-q // tpt)
+    out = []
+    for s in (1, 2, 3, 4, 6, 8):
+        nt = -(-s * qt // 32) * 32
+        if nt <= 512 and 5 * s * qt >= 4 * nt:
+            out += [(s, k) for k in (1, 2, 3, 4)]
+    return out
+
+
 @pytest.fixture(scope="module")
 def grid(sb):
     g = sb.build_grid(5, 3, exact_cc=True)
@@ -68,14 +82,44 @@ def test_chunked_shapes_match_whole_panel_kernel(sb, grid, n, precision):
         by_len.setdefault(k, f)
 
 
+@pytest.mark.parametrize("n", [5, 6, 7, 8, 9, 10])
+def test_barrier_free_form_matches_staged_form(sb, grid, n):
+    """The barrier-free kernel (sources read through L1 from a pair-transposed
+    copy, 1 or 2 target proxies per thread) runs the same per-source-panel
+    float32 arithmetic in the same order as the staged kernel: with the same
+    chunk length the step is bit-identical."""
+    g, vor = grid
+    ctx = tree_ctx(sb, n, sb.MIXED)
+    ctx.set_near_tuning(128, 2, 2)
+    q = (n + 1) ** 2
+    staged = {}
+    for k in (1, 2, 3, 4):
+        ctx.set_cc_tuning(shapes(q)[0][0], k)
+        staged[k] = unit_fields(g, vor)
+        step(ctx, staged[k])
+    for tpt in (1, 2):
+        for sl, k in direct_shapes(q, tpt):
+            ctx.set_cc_tuning_direct(sl, k, tpt)
+            assert ctx.cc_form() == tpt
+            assert ctx.cc_tuning()[:3] == (sl, k, -(-sl * -(-q // tpt) // 32) * 32)
+            f = unit_fields(g, vor)
+            step(ctx, f)
+            assert torch.equal(f["vors"], staged[k]["vors"]), (tpt, sl, k)
+            assert all(torch.equal(a, b) for a, b in zip(f["vel"], staged[k]["vel"])), (tpt, sl, k)
+
+
 def test_autotuner_times_every_shape(sb, grid):
     g, vor = grid
     ctx = tree_ctx(sb, 8, sb.MIXED)
     f = unit_fields(g, vor)
     step(ctx, f)
     sl, k, threads, cand, ms = ctx.cc_tuning()
-    assert cand == 1 + len(shapes(81)) and ms > 0
-    assert (sl, k, threads) == (0, 0, 128) or ((sl, k) in shapes(81) and threads == -(-sl * 81 // 32) * 32)
+    assert cand == 1 + len(shapes(81)) + len(direct_shapes(81, 1)) + len(direct_shapes(81, 2)) and ms > 0
+    tpt = ctx.cc_form()
+    if tpt:
+        assert (sl, k) in direct_shapes(81, tpt) and threads == -(-sl * -(-81 // tpt) // 32) * 32
+    else:
+        assert (sl, k, threads) == (0, 0, 128) or ((sl, k) in shapes(81) and threads == -(-sl * 81 // 32) * 32)
     again = unit_fields(g, vor)
     step(ctx, again)
     assert torch.equal(again["vors"], f["vors"])  # a fixed shape is deterministic
@@ -97,6 +141,11 @@ def test_rejects_unsupported_shapes(sb):
     for sl, k in ((1, 1), (2, 2), (5, 1), (3, 0), (3, 5), (9, 1), (0, 1), (-1, 1)):
         with pytest.raises(sb.SbslpmError):
             ctx.set_cc_tuning(sl, k)
+    for sl, k, tpt in ((1, 1, 3), (3, 1, 0), (3, 0, 1), (5, 1, 1)):
+        with pytest.raises(sb.SbslpmError):
+            ctx.set_cc_tuning_direct(sl, k, tpt)
+    with pytest.raises(sb.SbslpmError):  # float64: no barrier-free form
+        tree_ctx(sb, 6, sb.FP64).set_cc_tuning_direct(6, 1, 1)
     small = tree_ctx(sb, 3, sb.MIXED)  # 16 proxies: whole-panel kernel only
     with pytest.raises(sb.SbslpmError):
         small.set_cc_tuning(1, 1)

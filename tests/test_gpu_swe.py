@@ -258,3 +258,45 @@ def test_swe_needs_degree_two(sb):
     z = torch.zeros(A, q, dtype=torch.float64, device="cuda")
     with pytest.raises(sb.SbslpmError):
         ctx.unify_boundary_vals(z)
+
+
+@pytest.mark.parametrize("levels", [6, 7])
+def test_height_drift_follows_the_reference(sb, levels):
+    """The benchmark's SWE flow (steady geostrophic solid-body rotation with
+    N(0, 1e-4^2) noise on g h, dt 0.002, spectral FMM at theta 0.7, exact
+    Clenshaw-Curtis weights): the float64 path's relative L2 height drift
+    every 10 steps against the reference's own step run to the same steps
+    (tests/golden/swe_drift_reference_L<levels>.json, made by
+    tests/golden/swe_drift_reference.py).  The reference's forward-Euler
+    divergence and height update amplifies the noise until its point location
+    meets a non-finite point, so both runs grow together; the drift values
+    agree to 1e-8 relative while they are finite."""
+    import json
+
+    with open(os.path.join(GOLDEN, f"swe_drift_reference_L{levels}.json")) as f:
+        ref = json.load(f)
+    g = sb.build_grid(levels, 3, exact_cc=True)
+    om, u0 = 2 * np.pi, 2 * np.pi / 12
+    lat = np.arcsin(np.clip(g.z, -1, 1))
+    h0 = 2.94 - (om * u0 + 0.5 * u0 * u0) * np.sin(lat) ** 2
+    h0 = h0 + 1e-4 * np.random.default_rng(ref["noise_seed"]).standard_normal(h0.shape)
+    ctx = sb.Context(sb.config_default(levels=levels, interp_degree=3, fmm_theta=ref["theta"],
+                                       kernel_eps=ref["kernel_eps"], omega=om, dt=ref["dt"], g_over_a=1.0))
+    f = [cuda(g.x), cuda(g.y), cuda(g.z), cuda(g.area), cuda(2 * u0 * np.sin(lat)), cuda(np.zeros_like(h0)),
+         cuda(h0)]
+    vel = [torch.zeros_like(f[0]) for _ in range(3)]
+    base = [torch.zeros_like(f[0]) for _ in range(3)]
+    ctx.swe_init(*f, *vel, *base)
+    w = g.area / g.area.sum()
+    l2 = lambda a: float(np.sqrt((w * a * a).sum()))
+    done, checked = 0, 0
+    for row in ref["curve"]:
+        if row["height_l2_drift"] is None:
+            break
+        ctx.swe_run(*f, *vel, None, *base, nsteps=row["step"] - done)
+        done = row["step"]
+        d = l2(f[6].cpu().numpy() - h0) / l2(h0)
+        print(f"levels {levels} step {done}: drift {d:.6e} (reference {row['height_l2_drift']:.6e})")
+        assert abs(d - row["height_l2_drift"]) <= 1e-8 * row["height_l2_drift"]
+        checked += 1
+    assert checked >= 5

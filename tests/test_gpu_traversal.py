@@ -26,3 +26,25 @@ def test_device_traversal_equals_reference_order(sb, levels, theta):
     assert np.array_equal(dev, host)
     if (levels, theta) == (7, 0.7):
         assert len(host) == 1224342
+
+
+@pytest.mark.parametrize("levels", [3, 4, 5])
+def test_treecode_lists_of_many_members_in_one_launch_series(sb, levels):
+    """The treecode's traversal (its tree is the grid's quadtree truncated at
+    the leaf size: levels 3..5 here, the ensemble's tree at 98,304 particles
+    being levels 4) for 128 members with their own theta, on the GPU in one
+    launch series: every member's list, order and near flags equal the host
+    traversal's, bit for bit."""
+    panels = sb.cubed_sphere_panels_init(levels)
+    thetas = np.random.default_rng(2026).uniform(0.5, 0.8, 128)
+    t0 = time.perf_counter()
+    dev = sb.dual_tree_traversal_device_multi(levels, panels, thetas)
+    t1 = time.perf_counter()
+    host = [sb.dual_tree_traversal_flagged(levels, panels, th) for th in thetas]
+    t2 = time.perf_counter()
+    print("levels %d, 128 members: %d pairs, device %.3f s, host %.3f s"
+          % (levels, sum(len(h[0]) for h in host), t1 - t0, t2 - t1))
+    for (dl, dn), (hl, hn), th in zip(dev, host, thetas):
+        assert np.array_equal(dl, hl), th
+        assert np.array_equal(dn, hn), th
+        assert np.array_equal(hl, sb.dual_tree_traversal(levels, panels, th))  # the same list as the unflagged one
