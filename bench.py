@@ -275,6 +275,15 @@ def swe_bench(sb, torch, dev, flush, steps):
 ENS_MEMBERS, ENS_LEVELS, ENS_SH_DEGREE = 128, 6, 20
 
 
+def tree_levels_for(levels, degree=DEGREE, leaf=LEAF_SIZE):
+    """Levels of the treecode's tree: the grid's quadtree truncated so that a
+    leaf holds at most `leaf` particles."""
+    npl, m = (degree + 1) ** 2, 0
+    while npl * 4 <= leaf and m < levels - 1:
+        npl, m = npl * 4, m + 1
+    return levels - m
+
+
 def sh_basis(g, lmax):
     """Real orthonormal spherical harmonics of degrees 1..lmax at the grid points
     ([functions][leaf*q]); degree 0 is left out because relative vorticity
@@ -320,7 +329,20 @@ def ensemble_bench(sb, torch, dev, flush, steps):
     xyza = [T(g.x), T(g.y), T(g.z), T(g.area)]
     cfg = sb.config_default(levels=ENS_LEVELS, interp_degree=DEGREE, kernel_eps=EPS, omega=OMEGA, dt=DT,
                             precision=sb.MIXED, leaf_size=LEAF_SIZE)
+    t_create = time.perf_counter()
     batch = sb.Batch(cfg, theta, pdeg)
+    create_s = time.perf_counter() - t_create
+    lists_s = batch.setup_times()["lists_s"]
+    # the same members' traversals on the host, for comparison (the batch builds them on the GPU)
+    tree_levels = tree_levels_for(ENS_LEVELS)
+    panels = sb.cubed_sphere_panels_init(tree_levels)
+    t_host = time.perf_counter()
+    for th in theta:
+        sb.dual_tree_traversal_flagged(tree_levels, panels, float(th))
+    host_lists_s = time.perf_counter() - t_host
+    t_dev = time.perf_counter()
+    sb.dual_tree_traversal_device_multi(tree_levels, panels, theta)
+    device_lists_s = time.perf_counter() - t_dev
     v = T(vors)
     vel = torch.zeros((ENS_MEMBERS, 3) + base.shape, dtype=torch.float64, device=dev)
     st = torch.cuda.current_stream()
@@ -395,6 +417,13 @@ def ensemble_bench(sb, torch, dev, flush, steps):
                            "ms_per_step_cuda_core_pairs": ms_cuda_cores, "ms_per_step_tensor_core_3xtf32": ms_tc3,
                            "ms_per_step_tensor_core_tf32_single_pass": ms_tf32,
                            "ms_per_step_cuda_core_shared_pairs": ms_shared},
+        "setup_s": {"batch_create": create_s, "member_lists_in_create": lists_s,
+                    "traversals_gpu_one_launch_series": device_lists_s,
+                    "traversals_host_one_by_one": host_lists_s,
+                    "note": "member_lists_in_create: the 128 members' traversals on the GPU plus the lists' CSR "
+                            "assembly inside sbslpm_batch_create (the first GPU work of the process's batch); "
+                            "the other two: the same traversals (flagged lists copied to the host) through the C "
+                            "ABI, on the GPU in one launch series and on the host one by one"},
         "fp64_plain_single_member_steps_per_s": fp64_sps,
         "speedup_member_steps_vs_fp64_plain": member_sps / fp64_sps,
         "accuracy_step1_vs_fp64_direct": acc,
@@ -450,6 +479,8 @@ def profile_run(sb, torch, dev, args):
         if proxy:  # the first-step autotuner's choice on this workload, fixed so that the capture sees steps only
             ctx.set_near_tuning(*[int(v) for v in args.near_shape.split(",")])
             ctx.set_cc_tuning(*[int(v) for v in args.cc_shape.split(",")])
+            if args.near_mutual and prec == sb.MIXED:
+                ctx.set_near_mutual(True)
         f = [T(g.x), T(g.y), T(g.z), T(g.area), T(rh4(g)), *[torch.zeros_like(T(g.x)) for _ in range(3)], None]
         for _ in range(n):
             ctx.bve_back_rk4_step(*f)
@@ -639,6 +670,8 @@ def main():
     ap.add_argument("--cc-shape", default="3,3",
                     help="--profile treecode/treecode64: well-separated chunk slots per block,chunk length (0,0: "
                          "one block per target panel)")
+    ap.add_argument("--near-mutual", action="store_true",
+                    help="--profile treecode: the first stage's near field two-sided (sbslpm_set_near_mutual)")
     ap.add_argument("--degree", type=int, default=0,
                     help="--profile ensemble: one proxy degree for every member (0: drawn from {6, 8, 10})")
     args = ap.parse_args()
@@ -811,6 +844,8 @@ def main():
     share = 4 * ms_int / ms_per_step
     tune32, tune64 = ctx32.near_tuning(), ctx64.near_tuning()
     cc32, cc64 = ctx32.cc_tuning(), ctx64.cc_tuning()
+    cc32_form = ctx32.cc_form()
+    mutual_on, mutual_ms = ctx32.near_mutual()
     well_sep_pairs = 4 * 52566 * 81 * 81  # per step: well-separated tree-panel pairs x 81 x 81 proxies
 
     # ---- batched ensemble ----------------------------------------------------
@@ -881,7 +916,16 @@ def main():
                          "ms_per_launch": ms_int, "step_share": share,
                          "peak_source": "measured f32 FMA-chain throughput on this GPU (sbslpm_measure_fma_peak); "
                                         "MEASURED_PEAKS.json has no CUDA-core peak"},
-            "well_separated_kernel": {"slots": cc32[0], "chunk_len": cc32[1], "threads": cc32[2],
+            "first_stage_near_field": {"two_sided": mutual_on, "ms_per_launch_two_sided": mutual_ms,
+                                       "ms_per_launch_one_sided": tune32[4] if len(tune32) > 4 else None,
+                                       "note": "at the first RK stage the sources are the grid particles, so each "
+                                               "unordered near leaf pair can be evaluated once for both "
+                                               "directions; the first-step timing keeps the faster kernel for "
+                                               "that stage (the later stages' sources are displaced and need the "
+                                               "one-sided kernel)"},
+            "well_separated_kernel": {"form": "barrier-free, %d target proxies per thread" % cc32_form if cc32_form
+                                      else "sources staged in shared memory",
+                                      "slots": cc32[0], "chunk_len": cc32[1], "threads": cc32[2],
                                       "candidates_timed": cc32[3], "ms_per_launch": cc32[4],
                                       "pairs_per_launch": well_sep_pairs / 4,
                                       "pairs_per_s": well_sep_pairs / 4 / (cc32[4] * 1e-3) if cc32[4] else None,

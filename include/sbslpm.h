@@ -519,6 +519,17 @@ sbslpm_status sbslpm_time_interactions(sbslpm_ctx* ctx, int reps, double* ms_per
  * candidates timed. */
 sbslpm_status sbslpm_set_near_tuning(sbslpm_ctx* ctx, int threads, int targets_per_thread, int splits);
 sbslpm_status sbslpm_near_tuning(const sbslpm_ctx* ctx, int* shape, double* ms_per_launch);
+/* Mixed-precision treecode contexts with 256-particle leaves: the first RK
+ * stage's near field can run two-sided.  At that stage the sources are the
+ * grid particles themselves, so a leaf pair's distances and reciprocals
+ * serve both directions: one CTA per unordered near leaf pair (diagonal and
+ * unmirrored pairs one-sided) writes float32 sums per list entry, added per
+ * leaf in list order.  The first-step timing keeps it for stage 0 when it
+ * beats the chosen shape; sbslpm_set_near_mutual turns it on or off (it
+ * changes the order of float32 additions only).  *ms_per_launch: its timed
+ * launch (with the per-leaf sums). */
+sbslpm_status sbslpm_set_near_mutual(sbslpm_ctx* ctx, int on);
+sbslpm_status sbslpm_near_mutual(const sbslpm_ctx* ctx, int* on, double* ms_per_launch);
 /* Treecode contexts with 36..121 proxies (proxy_degree 5..10): the launch
  * shape of the well-separated (cluster-cluster) interactions, either one
  * block of four warps per target panel (slots 0, chunk length 0, the kernel
@@ -538,11 +549,18 @@ sbslpm_status sbslpm_cc_tuning(const sbslpm_ctx* ctx, int* shape, double* ms_per
  * form of the chunked kernel: each slot reads its source proxies straight
  * from a pair-transposed copy through the L1 cache instead of staging them in
  * shared memory, with targets_per_thread (1 | 2) target proxies per thread.
- * The first-step timing includes it; sbslpm_set_cc_tuning_direct fixes it
- * (the chunk length sets the order of the float64 additions, as above);
- * sbslpm_cc_form reports 0 for the staged form, else its targets per
- * thread. */
+ * A third form keeps the staged form's slots but brings each slot's source
+ * panels into shared memory with bulk copies (the TMA engine's
+ * cp.async.bulk), double-buffered through mbarriers so that the next panel
+ * arrives while the current one is evaluated and no barrier spans the block;
+ * its waits are bounded (a copy that never lands gives SBSLPM_ERR_TIMEOUT).
+ * The first-step timing includes both; sbslpm_set_cc_tuning_direct and
+ * sbslpm_set_cc_tuning_bulk fix one (the chunk length sets the order of the
+ * float64 additions, as above); sbslpm_cc_form reports 0 for the staged
+ * form, 1 | 2 (targets per thread) for the barrier-free one, 3 for the
+ * bulk-copy one. */
 sbslpm_status sbslpm_set_cc_tuning_direct(sbslpm_ctx* ctx, int slots, int chunk_len, int targets_per_thread);
+sbslpm_status sbslpm_set_cc_tuning_bulk(sbslpm_ctx* ctx, int slots, int chunk_len);
 sbslpm_status sbslpm_cc_form(const sbslpm_ctx* ctx, int* targets_per_thread);
 /* CUDA-core fused multiply-add throughput of this GPU, measured with
  * independent FMA chains on every SM for about ms milliseconds: kind 0 =

@@ -178,6 +178,9 @@ def lib() -> ctypes.CDLL:
     L.sbslpm_batch_set_stage0_shared.argtypes = [_VP, ctypes.c_int]
     L.sbslpm_cc_tuning.argtypes = [_VP, _I, _D]
     L.sbslpm_set_cc_tuning_direct.argtypes = [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    L.sbslpm_set_near_mutual.argtypes = [_VP, ctypes.c_int]
+    L.sbslpm_set_cc_tuning_bulk.argtypes = [_VP, ctypes.c_int, ctypes.c_int]
+    L.sbslpm_near_mutual.argtypes = [_VP, _I, _D]
     L.sbslpm_cc_form.argtypes = [_VP, _I]
     L.sbslpm_measure_fma_peak.argtypes = [ctypes.c_int, ctypes.c_double, _D]
     _lib = L
@@ -582,14 +585,29 @@ class Context:
         autotuning it."""
         _check(lib().sbslpm_set_cc_tuning(self._h, int(slots), int(chunk_len)), "sbslpm_set_cc_tuning")
 
+    def set_near_mutual(self, on: bool):
+        """The first stage's two-sided near-field kernel on or off (mixed, 256-particle leaves)."""
+        _check(lib().sbslpm_set_near_mutual(self._h, int(bool(on))), "sbslpm_set_near_mutual")
+
+    def near_mutual(self):
+        """(in use for stage 0, ms per launch of the two-sided kernel from the first-step timing)."""
+        on, ms = ctypes.c_int(), ctypes.c_double()
+        _check(lib().sbslpm_near_mutual(self._h, ctypes.byref(on), ctypes.byref(ms)), "sbslpm_near_mutual")
+        return bool(on.value), ms.value
+
     def set_cc_tuning_direct(self, slots: int, chunk_len: int, targets_per_thread: int):
         """Fix the barrier-free form of the mixed-precision well-separated kernel
         (sources read through L1 from a pair-transposed copy) and its shape."""
         _check(lib().sbslpm_set_cc_tuning_direct(self._h, int(slots), int(chunk_len), int(targets_per_thread)),
                "sbslpm_set_cc_tuning_direct")
 
+    def set_cc_tuning_bulk(self, slots: int, chunk_len: int):
+        """Fix the bulk-copy form of the mixed-precision well-separated kernel (each slot's
+        source panels copied into shared memory by cp.async.bulk, double-buffered)."""
+        _check(lib().sbslpm_set_cc_tuning_bulk(self._h, int(slots), int(chunk_len)), "sbslpm_set_cc_tuning_bulk")
+
     def cc_form(self) -> int:
-        """0: sources staged in shared memory; 1 | 2: barrier-free, targets per thread."""
+        """0: sources staged in shared memory; 1 | 2: barrier-free, targets per thread; 3: bulk copies."""
         t = ctypes.c_int()
         _check(lib().sbslpm_cc_form(self._h, ctypes.byref(t)), "sbslpm_cc_form")
         return t.value

@@ -39,29 +39,43 @@ constexpr int kThreads = 256;
 
 // Barycentric Lagrange basis of degree n on Chebyshev extrema of [lo, hi]
 // without the reference's range check: displaced sources may sit slightly
-// outside their leaf, where the interpolant extrapolates smoothly.
+// outside their leaf, where the interpolant extrapolates smoothly.  The
+// second barycentric form multiplied through by prod_j (t - c_j):
+// f_i = w_i P_i / sum_k w_k P_k with P_i = prod_{j != i} (t - c_j), one
+// division instead of n + 2 (nodes within 1e-15 are hit exactly).
 __device__ __forceinline__ void bli_1d_free(double t, double lo, double hi, int n, const double* cosv,
                                             const double* w, double* f) {
   if (n == 0) {
     f[0] = 1;
     return;
   }
-  double range = 0.5 * (hi - lo), offset = 0.5 * (hi + lo);
+  const double range = 0.5 * (hi - lo), offset = 0.5 * (hi + lo);
+  double dl[kMaxDegree + 1];
   int hit = -1;
-  for (int i = 0; i <= n; i++)
-    if (hit < 0 && fabs(t - (cosv[i] * range + offset)) < 1e-15) hit = i;
+#pragma unroll
+  for (int i = 0; i <= kMaxDegree; i++) {
+    dl[i] = i <= n ? t - (cosv[i] * range + offset) : 1.0;
+    if (i <= n && hit < 0 && fabs(dl[i]) < 1e-15) hit = i;
+  }
   if (hit >= 0) {
     for (int i = 0; i <= n; i++) f[i] = (i == hit) ? 1.0 : 0.0;
     return;
   }
-  double den = 0;
-  for (int i = 0; i <= n; i++) {
-    double v = w[i] / (t - (cosv[i] * range + offset));
-    f[i] = v;
-    den += v;
+  double pre[kMaxDegree + 1];
+  pre[0] = 1.0;
+#pragma unroll
+  for (int i = 1; i <= kMaxDegree; i++) pre[i] = pre[i - 1] * dl[i - 1];
+  double suf = 1.0, den = 0.0, v[kMaxDegree + 1];
+#pragma unroll
+  for (int i = kMaxDegree; i >= 0; i--) {
+    v[i] = i <= n ? w[i] * (pre[i] * suf) : 0.0;
+    den += v[i];
+    suf *= dl[i];
   }
-  double inv = 1.0 / den;
-  for (int i = 0; i <= n; i++) f[i] *= inv;
+  const double inv = 1.0 / den;
+#pragma unroll
+  for (int i = 0; i <= kMaxDegree; i++)
+    if (i <= n) f[i] = v[i] * inv;
 }
 
 __device__ __forceinline__ void bltc_sources_body(const TreeGeom& tg, const StepGeom& fg, const BliTable& tab, int f,
@@ -430,6 +444,140 @@ __global__ void __launch_bounds__(NT)
   }
 }
 
+// The first stage's near field with each leaf pair evaluated once for both
+// directions.  At stage 0 the sources sit on the grid (psrcf holds the
+// particles themselves, packed relative to their leaf's centre), so for
+// particle i of leaf T and j of leaf S the differences are opposite, d_ji =
+// -d_ij, and the distance and reciprocal are shared: one evaluation gives
+// w_j r d to i and -w_i r d to j -- 7 paired float32 operations per pair
+// instead of 10, and one reciprocal instead of two.  One CTA of 256 threads
+// per unit (T, S, eT, eS) of 256-particle leaves: warp w takes S's particles
+// 32w..32w+31 (shared memory), lane l T's particles 8l..8l+7 (registers, in
+// pairs for FFMA2).  In step r lane l meets source 32w + (l + r) mod 32, so
+// the 32 lanes of a warp update 32 different source accumulators (shared
+// memory) and each source sees the lanes in a fixed order; after 32 steps the
+// warps' target partials are added in warp order.  The float32 sums of the
+// unit go to slot eT (what T's particles receive from S, [3][256]) and, for
+// eS >= 0, slot eS (what S's receive from T); units with eS < 0 -- the
+// diagonal pairs (T, T) and pairs whose mirror is not in the list -- evaluate
+// T's side only.  k_near_slot_sum adds a leaf's slots in list order.
+template <bool GUARD>
+__global__ void __launch_bounds__(256, 2)
+    k_bltc_near32_mutual(StepGeom fg, const int4* __restrict__ units, const float4* __restrict__ psrcf, float eps,
+                         float* __restrict__ slot) {
+  constexpr int L = kMutualLeaf;
+  __shared__ float4 src[L];        // S's particles: packed position, strength
+  __shared__ float4 sacc[L];       // what S's particles receive from T
+  __shared__ float red[8][3][L];   // the warps' target partials
+  const int4 u = units[blockIdx.x];
+  const int T = u.x, S = u.y, eT = u.z, eS = u.w;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const bool both = eS >= 0;
+  src[tid] = psrcf[(long)S * L + tid];
+  sacc[tid] = make_float4(0.f, 0.f, 0.f, 0.f);
+  const double* ct = fg.pd_centre + 4 * (long)(fg.offset + T);
+  const double* cs = fg.pd_centre + 4 * (long)(fg.offset + S);
+  const float bx0 = (float)((cs[0] - ct[0]) * kPackScale), by0 = (float)((cs[1] - ct[1]) * kPackScale),
+              bz0 = (float)((cs[2] - ct[2]) * kPackScale);
+  float2 bx[4], by[4], bz[4], wt[4], ax[4], ay[4], az[4];
+#pragma unroll
+  for (int p = 0; p < 4; p++) {
+    const float4 t0 = psrcf[(long)T * L + 8 * lane + 2 * p], t1 = psrcf[(long)T * L + 8 * lane + 2 * p + 1];
+    bx[p] = make_float2(bx0 - t0.x, bx0 - t1.x);
+    by[p] = make_float2(by0 - t0.y, by0 - t1.y);
+    bz[p] = make_float2(bz0 - t0.z, bz0 - t1.z);
+    wt[p] = make_float2(t0.w, t1.w);
+    ax[p] = ay[p] = az[p] = make_float2(0.f, 0.f);
+  }
+  const float2 eps2 = make_float2(eps, eps);
+  __syncthreads();
+#pragma unroll 2
+  for (int r = 0; r < 32; r++) {
+    const int j = 32 * warp + ((lane + r) & 31);
+    const float4 sj = src[j];
+    const float2 sx = make_float2(sj.x, sj.x), sy = make_float2(sj.y, sj.y), sz = make_float2(sj.z, sj.z),
+                 sw = make_float2(sj.w, sj.w);
+    float2 gx = make_float2(0.f, 0.f), gy = gx, gz = gx;
+#pragma unroll
+    for (int p = 0; p < 4; p++) {
+      const float2 dx = __fadd2_rn(bx[p], sx), dy = __fadd2_rn(by[p], sy), dz = __fadd2_rn(bz[p], sz);
+      const float2 den = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, eps2)));
+      float r0 = recip_f32(den.x), r1 = recip_f32(den.y);
+      if (GUARD) {
+        r0 = den.x > 0.0f ? r0 : 0.0f;
+        r1 = den.y > 0.0f ? r1 : 0.0f;
+      }
+      const float2 rr = make_float2(r0, r1);
+      const float2 g = __fmul2_rn(sw, rr);
+      ax[p] = __ffma2_rn(g, dx, ax[p]);
+      ay[p] = __ffma2_rn(g, dy, ay[p]);
+      az[p] = __ffma2_rn(g, dz, az[p]);
+      if (both) {
+        const float2 h = __fmul2_rn(wt[p], rr);
+        gx = __ffma2_rn(h, dx, gx);
+        gy = __ffma2_rn(h, dy, gy);
+        gz = __ffma2_rn(h, dz, gz);
+      }
+    }
+    if (both) {  // source j receives -(sum of h d): the difference points the other way
+      float4 a = sacc[j];
+      a.x -= gx.x + gx.y;
+      a.y -= gy.x + gy.y;
+      a.z -= gz.x + gz.y;
+      sacc[j] = a;
+    }
+    __syncwarp();
+  }
+#pragma unroll
+  for (int p = 0; p < 4; p++) {
+    const int k = 8 * lane + 2 * p;
+    red[warp][0][k] = ax[p].x;
+    red[warp][0][k + 1] = ax[p].y;
+    red[warp][1][k] = ay[p].x;
+    red[warp][1][k + 1] = ay[p].y;
+    red[warp][2][k] = az[p].x;
+    red[warp][2][k + 1] = az[p].y;
+  }
+  __syncthreads();
+  float* o = slot + (long)eT * 3 * L;
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    float a = red[0][c][tid];
+#pragma unroll
+    for (int w = 1; w < 8; w++) a += red[w][c][tid];
+    o[c * L + tid] = a;
+  }
+  if (both) {
+    float* q = slot + (long)eS * 3 * L;
+    const float4 a = sacc[tid];
+    q[tid] = a.x;
+    q[L + tid] = a.y;
+    q[2 * L + tid] = a.z;
+  }
+}
+
+// Near-field sums of every particle from the unit slots: leaf T's slots in
+// its near-list order (float32 sums added in float64), then u = cb t x a as
+// the per-leaf-pair kernel's epilogue; written as split 0 of the near buffer.
+__global__ void k_near_slot_sum(TreeGeom tg, const float* __restrict__ slot, const double* __restrict__ x,
+                                const double* __restrict__ y, const double* __restrict__ z, double* __restrict__ near) {
+  constexpr int L = kMutualLeaf;
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= tg.N) return;
+  const int T = (int)(i / L), k = (int)(i - (long)T * L);
+  double a0 = 0, a1 = 0, a2 = 0;
+  for (int e = tg.near_start[T]; e < tg.near_start[T + 1]; e++) {
+    const float* p = slot + (long)e * 3 * L;
+    a0 += (double)p[k];
+    a1 += (double)p[L + k];
+    a2 += (double)p[2 * L + k];
+  }
+  const double tx = x[i], ty = y[i], tz = z[i];
+  near[i] = kBiotSavartPacked * (ty * a2 - tz * a1);
+  near[tg.N + i] = kBiotSavartPacked * (tz * a0 - tx * a2);
+  near[2 * tg.N + i] = kBiotSavartPacked * (tx * a1 - ty * a0);
+}
+
 // Leaf proxy targets -> particles: v_i = (near-field splits summed in order)
 // + sum_a lx[k][a] sum_b ly[k][b] T[a][b], with the leaf-box basis of
 // particle k of the (uniform) leaf.
@@ -574,6 +722,17 @@ void launch_bltc_near_multi(const BatchMember* mem, const int* perm, int members
     if (guard) SB_LAUNCH((k_bltc_near32_multi<256, MB, true>), grid, 256, smem, st, mem, perm, members, ustart, uent, x, y, z, psrcf, near);
     else SB_LAUNCH((k_bltc_near32_multi<256, MB, false>), grid, 256, smem, st, mem, perm, members, ustart, uent, x, y, z, psrcf, near);
   }
+}
+
+void launch_bltc_near_mutual(const TreeGeom& tg, const StepGeom& fg, const int4* units, int nunits,
+                             const float4* psrcf, float* slot, const double* x, const double* y, const double* z,
+                             double* near, cudaStream_t st) {
+  if (nunits > 0) {
+    if (!(tg.eps > 0)) SB_LAUNCH(k_bltc_near32_mutual<true>, (unsigned)nunits, 256, 0, st, fg, units, psrcf,
+                                 (float)tg.eps, slot);
+    else SB_LAUNCH(k_bltc_near32_mutual<false>, (unsigned)nunits, 256, 0, st, fg, units, psrcf, (float)tg.eps, slot);
+  }
+  SB_LAUNCH(k_near_slot_sum, blocks_for(tg.N, 256), 256, 0, st, tg, slot, x, y, z, near);
 }
 
 void launch_bltc_to_particles_batch(const BatchMember* mem, int members, int leaves, int nmax, const double* near,

@@ -119,7 +119,11 @@ void launch_inv_lap(long n, const double* x, const double* y, const double* z, c
 // by target.  Mixed precision with direct_tpt = 1 or 2: the barrier-free
 // form (k_cc32d: direct_tpt target proxies per thread, sources read through
 // L1 from the pair-transposed copy srcp that launch_cc_pair_sources makes of
-// the packed proxy sources; cc_direct_shape_ok).
+// the packed proxy sources; cc_direct_shape_ok); with direct_tpt =
+// kCcBulkForm: the same slots as the staged form with each slot's source
+// panels brought into shared memory by bulk copies (k_cc32t, double-buffered
+// through mbarriers; cc_chunk_shape_ok).
+constexpr int kCcBulkForm = 3;
 bool cc_chunk_supported(int q);
 bool cc_chunk_shape_ok(int q, int slots);
 bool cc_direct_shape_ok(int q, int slots, int tpt);
@@ -145,6 +149,15 @@ void launch_bltc_sources(const TreeGeom& tg, const StepGeom& fg, const BliTable&
 // v = near splits summed + far field interpolated from the leaf proxies
 void launch_bltc_to_particles(const TreeGeom& tg, const StepGeom& fg, const double* tgt, const double* near,
                               int splits, double* v, cudaStream_t st);
+// The first stage's near field with each leaf pair evaluated once for both
+// directions (kMutualLeaf-particle leaves, mixed precision): units (T, S,
+// slot of T <- S, slot of S <- T or -1), float32 slot sums [near entries][3][leaf]
+// added per leaf in list order into split 0 of near.
+constexpr int kMutualLeaf = 256;
+void launch_bltc_near_mutual(const TreeGeom& tg, const StepGeom& fg, const int4* units, int nunits,
+                             const float4* psrcf, float* slot, const double* x, const double* y, const double* z,
+                             double* near, cudaStream_t st);
+void build_mutual_units(const std::vector<int>& ns, const std::vector<int>& nsrc, std::vector<int4>& units);
 
 // Batched treecode (members on one particle grid; one launch per phase over
 // all members, the cc launch once per proxy degree).  mem: device array of

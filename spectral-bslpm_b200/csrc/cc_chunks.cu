@@ -16,6 +16,7 @@
 // float64 additions), not on S.
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <vector>
 
 #include "../../include/sbslpm.h"
@@ -201,6 +202,137 @@ __global__ void __launch_bounds__(CcDirectShape<Q, S, TPT>::NT)
     p[Q + j] = ay[r];
     p[2 * Q + j] = az[r];
   }
+}
+
+// Mixed precision with the source proxies brought into shared memory by the
+// bulk-copy engine (TMA, cp.async.bulk): each slot owns two buffers of one
+// source panel's pair-transposed proxies (Q2 x 32 bytes, contiguous in srcp)
+// and two pairs of mbarriers.  The slot's first thread issues the copies of
+// its chunk's first two entries at once and each later one as soon as all
+// the slot's threads have released the buffer (empty barrier), so the next
+// panel arrives while the current one is evaluated, and no barrier spans the
+// block.  Every wait is bounded (0.2 s of %globaltimer): one that runs out
+// sets kErrTimeout and the slot stops.
+__device__ __forceinline__ unsigned long long cc_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ bool cc_mbar_wait(uint32_t bar, uint32_t parity) {
+  const unsigned long long t0 = cc_ns();
+  while (true) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (cc_ns() - t0 > 200000000ull) return false;
+  }
+}
+
+__device__ __forceinline__ void cc_bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" : : "r"(bar), "r"(bytes) : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+               :
+               : "r"(dst), "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+
+template <int Q, int S, bool GUARD>
+__global__ void __launch_bounds__(CcShape<Q, S>::NT)
+    k_cc32t(StepGeom g, const int4* __restrict__ chunks, int nchunks, const float4* __restrict__ srcp,
+            double* __restrict__ partial) {
+  constexpr int Q2 = (Q + 1) / 2;
+  constexpr uint32_t kBytes = Q2 * 32;
+  __shared__ __align__(128) float4 buf[S][2][2 * Q2];
+  __shared__ __align__(8) unsigned long long full[S][2], empty[S][2];
+  const int h = threadIdx.x / Q, j = threadIdx.x - h * Q;
+  const int c = blockIdx.x * S + h;
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < S; k++)
+      for (int b = 0; b < 2; b++) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" : : "r"((uint32_t)__cvta_generic_to_shared(&full[k][b]))
+                     : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;"
+                     :
+                     : "r"((uint32_t)__cvta_generic_to_shared(&empty[k][b])), "r"(Q)
+                     : "memory");
+      }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (h >= S || c >= nchunks) return;  // no block-wide barrier below
+  const int4 ch = chunks[c];
+  const int n = ch.z - ch.y;
+  const bool producer = j == 0;
+  // shared-memory addresses of buffer / barrier b of this slot: base + b * stride
+  const uint32_t f0 = (uint32_t)__cvta_generic_to_shared(&full[h][0]);
+  const uint32_t e0 = (uint32_t)__cvta_generic_to_shared(&empty[h][0]);
+  const uint32_t d0 = (uint32_t)__cvta_generic_to_shared(&buf[h][0][0]);
+  auto fb = [&](int b) { return f0 + 8u * (uint32_t)b; };
+  auto eb = [&](int b) { return e0 + 8u * (uint32_t)b; };
+  auto db = [&](int b) { return d0 + kBytes * (uint32_t)b; };
+  if (producer) {
+    for (int e = 0; e < n && e < 2; e++)
+      cc_bulk_load(db(e), srcp + (long)__ldg(g.src_panel + ch.y + e) * 2 * Q2, kBytes, fb(e));
+  }
+  const long pn = (long)g.panels * Q;
+  const double* ct = g.pd_centre + 4 * (long)ch.x;
+  const double cx = ct[0], cy = ct[1], cz = ct[2];
+  const long o = (long)ch.x * Q + j;
+  const float dtx = (float)((g.px[o] - cx) * kPackScale), dty = (float)((g.px[pn + o] - cy) * kPackScale),
+              dtz = (float)((g.px[2 * pn + o] - cz) * kPackScale);
+  const float feps = (float)g.eps;
+  const float2 eps2 = make_float2(feps, feps);
+  double ax = 0, ay = 0, az = 0;
+  bool ok = true;
+  for (int e = 0; e < n; e++) {
+    const int b = e & 1;
+    const uint32_t par = (uint32_t)((e >> 1) & 1);
+    if (!cc_mbar_wait(fb(b), par)) {
+      ok = false;
+      break;
+    }
+    const int sp = __ldg(g.src_panel + ch.y + e);
+    const double* cs = g.pd_centre + 4 * (long)sp;
+    const float b0 = (float)((cs[0] - cx) * kPackScale) - dtx, b1 = (float)((cs[1] - cy) * kPackScale) - dty,
+                b2 = (float)((cs[2] - cz) * kPackScale) - dtz;
+    const float2 bx = make_float2(b0, b0), by = make_float2(b1, b1), bz = make_float2(b2, b2);
+    float2 fx = make_float2(0.f, 0.f), fy = fx, fz = fx;
+    const float4* tb = buf[h][b];
+#pragma unroll 8
+    for (int k2 = 0; k2 < Q2; k2++) {
+      const float4 A = tb[2 * k2], B = tb[2 * k2 + 1];
+      pair32x2<GUARD>(bx, by, bz, make_float2(A.x, A.y), make_float2(A.z, A.w), make_float2(B.x, B.y),
+                      make_float2(B.z, B.w), eps2, fx, fy, fz);
+    }
+    ax += (double)fx.x + (double)fx.y;
+    ay += (double)fy.x + (double)fy.y;
+    az += (double)fz.x + (double)fz.y;
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" : : "r"(eb(b)) : "memory");
+    if (producer && e + 2 < n) {  // refill this buffer once the slot has released it
+      if (!cc_mbar_wait(eb(b), par)) {
+        // the copy of entry e + 1 may still be in flight: let it land (bounded) before leaving
+        cc_mbar_wait(fb(b ^ 1), (uint32_t)(((e + 1) >> 1) & 1));
+        ok = false;
+        break;
+      }
+      cc_bulk_load(db(b), srcp + (long)__ldg(g.src_panel + ch.y + e + 2) * 2 * Q2, kBytes, fb(b));
+    }
+  }
+  if (!ok) {
+    dev::flag(g.err, kErrTimeout);
+    return;
+  }
+  double* p = partial + (long)c * 3 * Q;
+  p[j] = ax;
+  p[Q + j] = ay;
+  p[2 * Q + j] = az;
 }
 
 // The pair-transposed copy of the packed proxy sources that k_cc32d reads.
@@ -439,6 +571,30 @@ void launch_direct_t(const StepGeom& g, int slots, const int4* chunks, int nchun
   }
 }
 
+template <int Q, int S>
+void launch_bulk_s(const StepGeom& g, const int4* chunks, int nchunks, const float4* srcp, double* partial,
+                   cudaStream_t st) {
+  if constexpr (CcShape<Q, S>::ok) {
+    constexpr int NT = CcShape<Q, S>::NT;
+    const unsigned grid = (unsigned)((nchunks + S - 1) / S);
+    if (!(g.eps > 0)) SB_LAUNCH((k_cc32t<Q, S, true>), grid, NT, 0, st, g, chunks, nchunks, srcp, partial);
+    else SB_LAUNCH((k_cc32t<Q, S, false>), grid, NT, 0, st, g, chunks, nchunks, srcp, partial);
+  }
+}
+
+template <int Q>
+void launch_bulk_q(const StepGeom& g, int slots, const int4* chunks, int nchunks, const float4* srcp,
+                   double* partial, cudaStream_t st) {
+  switch (slots) {
+    case 1: launch_bulk_s<Q, 1>(g, chunks, nchunks, srcp, partial, st); break;
+    case 2: launch_bulk_s<Q, 2>(g, chunks, nchunks, srcp, partial, st); break;
+    case 3: launch_bulk_s<Q, 3>(g, chunks, nchunks, srcp, partial, st); break;
+    case 4: launch_bulk_s<Q, 4>(g, chunks, nchunks, srcp, partial, st); break;
+    case 6: launch_bulk_s<Q, 6>(g, chunks, nchunks, srcp, partial, st); break;
+    default: launch_bulk_s<Q, 8>(g, chunks, nchunks, srcp, partial, st); break;
+  }
+}
+
 template <int Q, int TPT>
 bool direct_ok_t(int slots) {
   switch (slots) {
@@ -495,7 +651,7 @@ bool cc_chunk_shape_ok(int q, int slots) {
 }
 
 int cc_chunk_threads(int q, int slots, int direct_tpt) {
-  const int qt = direct_tpt > 0 ? (q + direct_tpt - 1) / direct_tpt : q;
+  const int qt = direct_tpt > 0 && direct_tpt != kCcBulkForm ? (q + direct_tpt - 1) / direct_tpt : q;
   return (slots * qt + 31) / 32 * 32;
 }
 
@@ -517,7 +673,12 @@ void launch_cc_chunks(const StepGeom& g, int precision, int slots, const int4* c
                       const double4* src, double* partial, double* out, cudaStream_t st, int direct_tpt,
                       const float4* srcp) {
   const bool mixed = precision == SBSLPM_MIXED;
-  if (nchunks > 0 && mixed && direct_tpt > 0) {
+  if (nchunks > 0 && mixed && direct_tpt == kCcBulkForm) {
+#define SB_BQ(Q) \
+  case Q: launch_bulk_q<Q>(g, slots, chunks, nchunks, srcp, partial, st); break;
+    switch (g.q) { SB_BQ(36) SB_BQ(49) SB_BQ(64) SB_BQ(81) SB_BQ(100) SB_BQ(121) default: break; }
+#undef SB_BQ
+  } else if (nchunks > 0 && mixed && direct_tpt > 0) {
 #define SB_DQ(Q)                                                                          \
   case Q:                                                                                 \
     if (direct_tpt == 1) launch_direct_t<Q, 1>(g, slots, chunks, nchunks, srcp, partial, st); \

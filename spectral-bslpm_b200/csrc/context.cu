@@ -192,6 +192,13 @@ sbslpm_status precompute_tree(sbslpm_ctx* c) {
   SB_TRY(upload(&c->cc_start, l.cs));
   SB_TRY(upload(&c->cc_src, l.csrc));
   if (c->cfg.precision == SBSLPM_MIXED && t.qx <= 32) SB_TRY(upload(&c->fentry32, entry_table(l.cs, l.csrc, t.centre)));
+  if (c->cfg.precision == SBSLPM_MIXED && t.npl == kMutualLeaf && c->n_near > 0) {
+    std::vector<int4> units;
+    build_mutual_units(l.ns, l.nsrc, units);
+    c->n_mutual = (int)units.size();
+    SB_TRY(upload(&c->mutual_units, units));
+    SB_TRY(dalloc(&c->near_slot, (size_t)c->n_near * 3 * kMutualLeaf));
+  }
   if (c->n_cc > 0 && cc_chunk_supported(t.qx)) {
     for (int k = 0; k < 4; k++) {
       std::vector<int4> chunks;
@@ -346,10 +353,17 @@ void velocity_eval(sbslpm_ctx* c, int stage, double dt_s, const double* vprev, c
     launch_tree_cc(c, tree_st);
     launch_downward_fused(fg, c->ftgt, nullptr, tree_st);
     if (c->aux_stream) cudaEventRecord(c->ev_join, tree_st);
-    launch_bltc_near_batch(c->self, 1, fg.leaves, c->npl, c->cfg.kernel_eps, c->cfg.precision, x, y, z, c->psrc,
-                           c->psrcf, c->near, c->near_splits, c->near_nt, c->near_tpt, st);
+    int splits = c->near_splits;
+    if (stage == 0 && c->near_mutual) {  // sources on the grid: each leaf pair once for both directions
+      launch_bltc_near_mutual(c->tgeom, fg, c->mutual_units, c->n_mutual, c->psrcf, c->near_slot, x, y, z, c->near,
+                              st);
+      splits = 1;
+    } else {
+      launch_bltc_near_batch(c->self, 1, fg.leaves, c->npl, c->cfg.kernel_eps, c->cfg.precision, x, y, z, c->psrc,
+                             c->psrcf, c->near, c->near_splits, c->near_nt, c->near_tpt, st);
+    }
     if (c->aux_stream) cudaStreamWaitEvent(st, c->ev_join, 0);
-    launch_bltc_to_particles(c->tgeom, fg, c->ftgt, c->near, c->near_splits, v, st);
+    launch_bltc_to_particles(c->tgeom, fg, c->ftgt, c->near, splits, v, st);
     return;
   }
   launch_upward_fused(g, 0, stage, dt_s, vprev, x, y, z, vors, area, c->src, mixed, st);
@@ -402,6 +416,8 @@ sbslpm_status finish(sbslpm_ctx* c) {
   if (e) {
     SB_CUDA(cudaMemsetAsync(c->err, 0, sizeof(unsigned), st));
     SB_CUDA(cudaStreamSynchronize(st));
+    if (e & kErrTimeout)
+      return set_last_error("a well-separated kernel's bounded copy wait ran out"), SBSLPM_ERR_TIMEOUT;
     if (e & kErrNonFinite) return set_last_error("non-finite point in a location step"), SBSLPM_ERR_NONFINITE;
     return set_last_error("interpolation point outside its panel"), SBSLPM_ERR_OUT_OF_PANEL;
   }
@@ -453,11 +469,12 @@ sbslpm_status cc_autotune(sbslpm_ctx* c) {
   int cand = 0;
   const int keep_slots = c->cc_slots, keep_len = c->cc_len, keep_tpt = c->cc_tpt;
   int best_slots = keep_slots, best_len = keep_len, best_tpt = keep_tpt;
-  // kernel form: 0 staged in shared memory, 1 | 2 barrier-free (mixed precision)
-  const int max_tpt = c->cfg.precision == SBSLPM_MIXED && c->fsrcp ? 2 : 0;
+  // kernel form: 0 staged in shared memory, 1 | 2 barrier-free, 3 bulk copies (mixed precision)
+  const int max_tpt = c->cfg.precision == SBSLPM_MIXED && c->fsrcp ? kCcBulkForm : 0;
   for (int tpt = 0; tpt <= max_tpt; tpt++)
   for (int sl = tpt > 0 ? 1 : 0; sl <= 8; sl++) {  // chunk slots per block; 0: one block per target panel
-    if (sl > 0 && !(tpt > 0 ? cc_direct_shape_ok(c->qx, sl, tpt) : cc_chunk_shape_ok(c->qx, sl))) continue;
+    const bool direct = tpt == 1 || tpt == 2;
+    if (sl > 0 && !(direct ? cc_direct_shape_ok(c->qx, sl, tpt) : cc_chunk_shape_ok(c->qx, sl))) continue;
     for (int len = sl > 0 ? 1 : 0; len <= (sl > 0 ? 4 : 0); len++) {
       c->cc_slots = sl;
       c->cc_len = len;
@@ -533,6 +550,24 @@ sbslpm_status near_autotune(sbslpm_ctx* c, const double* x, const double* y, con
         c->near_splits = sp;
       }
     }
+  }
+  // the first stage's two-sided kernel, where it applies: kept for stage 0
+  // if it beats the chosen shape on these (stage-0) sources
+  c->near_mutual = false;
+  if (c->n_mutual > 0) {
+    auto run = [&] {
+      launch_bltc_near_mutual(c->tgeom, c->fgeom, c->mutual_units, c->n_mutual, c->psrcf, c->near_slot, x, y, z,
+                              c->near, st);
+    };
+    run();
+    SB_CUDA(cudaEventRecord(e0, st));
+    for (int r = 0; r < 5; r++) run();
+    SB_CUDA(cudaEventRecord(e1, st));
+    SB_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    SB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    c->near_mutual_ms = ms / 5;
+    c->near_mutual = c->near_mutual_ms < best;
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -744,7 +779,8 @@ sbslpm_status sbslpm_destroy(sbslpm_ctx* c) {
                   c->s_ntan, c->s_pow15, c->s_filt, c->s_ptan, c->s_pface, c->s_ustart, c->s_umem, c->src2,
                   c->srcf2, c->tend, c->avor, c->adj_src, c->adj_vbar, c->adj_q, c->adj_y, c->adj_part,
                   c->adj_w, c->adj_vel, c->adj_near_ts, c->adj_near_tt, c->adj_cc_ts, c->adj_cc_tt, c->adj_tbar,
-                  c->adj_qbl, c->self, c->force, c->d_time, c->cc_partial, c->entry32, c->fentry32, c->fsrcp};
+                  c->adj_qbl, c->self, c->force, c->d_time, c->cc_partial, c->entry32, c->fentry32, c->fsrcp,
+                  c->mutual_units, c->near_slot};
   for (void* b : bufs)
     if (b) cudaFree(b);
   for (int k = 0; k < 4; k++) {
@@ -1113,9 +1149,43 @@ sbslpm_status sbslpm_cc_tuning(const sbslpm_ctx* c, int* shape, double* ms_per_l
   return SBSLPM_OK;
 }
 
+sbslpm_status sbslpm_set_cc_tuning_bulk(sbslpm_ctx* c, int slots, int chunk_len) {
+  if (!c || !c->tree) return SBSLPM_ERR_ARG;
+  if (!c->cc_partial || !c->fsrcp)
+    return set_last_error("the bulk-copy well-separated kernel needs mixed precision and 36..121 proxies"),
+           SBSLPM_ERR_CONFIG;
+  if (!cc_chunk_shape_ok(c->qx, slots) || chunk_len < 1 || chunk_len > 4)
+    return set_last_error("unsupported well-separated launch shape"), SBSLPM_ERR_ARG;
+  SB_TRY(sbslpm_set_cc_tuning(c, 0, 0));
+  c->cc_slots = slots;
+  c->cc_len = chunk_len;
+  c->cc_tpt = kCcBulkForm;
+  return SBSLPM_OK;
+}
+
 sbslpm_status sbslpm_cc_form(const sbslpm_ctx* c, int* targets_per_thread) {
   if (!c || !c->tree || !targets_per_thread) return SBSLPM_ERR_ARG;
   *targets_per_thread = c->cc_partial && c->cc_slots > 0 ? c->cc_tpt : 0;
+  return SBSLPM_OK;
+}
+
+sbslpm_status sbslpm_set_near_mutual(sbslpm_ctx* c, int on) {
+  if (!c || !c->tree) return SBSLPM_ERR_ARG;
+  if (on && c->n_mutual == 0)
+    return set_last_error("the two-sided near-field kernel needs mixed precision and 256-particle leaves"),
+           SBSLPM_ERR_CONFIG;
+  c->near_mutual = on != 0;
+  if (c->graph) {
+    cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+  }
+  return SBSLPM_OK;
+}
+
+sbslpm_status sbslpm_near_mutual(const sbslpm_ctx* c, int* on, double* ms_per_launch) {
+  if (!c || !c->tree || !on || !ms_per_launch) return SBSLPM_ERR_ARG;
+  *on = c->near_mutual ? 1 : 0;
+  *ms_per_launch = c->near_mutual_ms;
   return SBSLPM_OK;
 }
 

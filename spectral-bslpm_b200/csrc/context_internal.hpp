@@ -68,6 +68,13 @@ struct sbslpm_ctx {
   bool near_tuned = false;
   int near_candidates = 0;
   double near_tuned_ms = 0;
+  // the first stage's two-sided near-field kernel (mixed, 256-particle leaves):
+  // its units, float32 slot sums, and whether the first-step timing chose it
+  int4* mutual_units = nullptr;
+  int n_mutual = 0;
+  float* near_slot = nullptr;
+  bool near_mutual = false;
+  double near_mutual_ms = 0;
   // the well-separated list cut into chunks of 1..4 entries per target panel
   // (k = chunk length - 1), used for q >= 36; threads and chunk length are
   // autotuned with the near field

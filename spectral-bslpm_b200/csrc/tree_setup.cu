@@ -152,4 +152,23 @@ void tree_lists_from(const TreeTables& t, std::vector<sbslpm_interact_pair>&& li
   }
 }
 
+// Units of the first stage's two-sided near-field kernel from the near lists
+// (CSR by target leaf): (T, S, e, e') for every entry e = (T <- S) with S > T
+// whose mirror e' = (S <- T) is in S's list, (T, S, e, -1) for the diagonal
+// entries and for entries without a mirror (evaluated one-sidedly).
+void build_mutual_units(const std::vector<int>& ns, const std::vector<int>& nsrc, std::vector<int4>& units) {
+  units.clear();
+  const int leaves = (int)ns.size() - 1;
+  for (int T = 0; T < leaves; T++)
+    for (int e = ns[T]; e < ns[T + 1]; e++) {
+      const int S = nsrc[e];
+      int mirror = -1;
+      if (S != T)
+        for (int f = ns[S]; f < ns[S + 1]; f++)
+          if (nsrc[f] == T) mirror = f;
+      if (S == T || mirror < 0) units.push_back(make_int4(T, S, e, -1));
+      else if (S > T) units.push_back(make_int4(T, S, e, mirror));
+    }
+}
+
 }  // namespace sbslpm

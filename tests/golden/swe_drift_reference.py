@@ -70,11 +70,15 @@ def main():
     h0 = height.copy()
     l2 = lambda a: float(np.sqrt((w * a * a).sum()))
     out = {"levels": levels, "particles": int(x.size), "threads": ref.lib.ref_num_threads(), "dt": 0.002,
-           "time_scale": S, "theta": 0.7, "degree": 3, "kernel_eps": EPS, "noise_seed": 4, "curve": [],
-           "stopped": f"Kokkos::abort (point location of a non-finite point) before step {nsteps}"}
+           "time_scale": S, "theta": 0.7, "degree": 3, "kernel_eps": EPS, "noise_seed": 4, "curve": []}
     path = os.path.join(HERE, f"swe_drift_reference_L{levels}.json")
     done, t0 = 0, time.time()
     while done < nsteps:
+        # what the file says if the reference stops the process in this chunk
+        out["stopped"] = (f"Kokkos::abort (point location of a non-finite departure point) after step {done}, "
+                          f"before step {done + 10}")
+        with open(path, "w") as f:
+            json.dump(out, f, indent=1)
         vors, divs, height, vel, _ = ref.swe_step(c, vors, divs, height, base, smap, vel=vel, time=float(done),
                                                    nsteps=10, driver_unify=True)
         done += 10

@@ -1,9 +1,9 @@
 """GPU tests of the treecode's well-separated (cluster-cluster) launch shapes:
 every chunked shape (1..8 chunk slots per block, 1..4 list entries per
 chunk) against the whole-panel kernel, for every proxy count with a chunked
-kernel, in both precisions, and the barrier-free mixed-precision form against
-the staged one, through the C ABI (sbslpm_set_cc_tuning,
-sbslpm_set_cc_tuning_direct).
+kernel, in both precisions, and the barrier-free and bulk-copy (TMA)
+mixed-precision forms against the staged one, through the C ABI
+(sbslpm_set_cc_tuning, sbslpm_set_cc_tuning_direct, sbslpm_set_cc_tuning_bulk).
 
 The shapes evaluate the same pairs with the same per-source-panel arithmetic
 and differ only in the order in which a target's float64 sums are added, so
@@ -106,6 +106,16 @@ def test_barrier_free_form_matches_staged_form(sb, grid, n):
             step(ctx, f)
             assert torch.equal(f["vors"], staged[k]["vors"]), (tpt, sl, k)
             assert all(torch.equal(a, b) for a, b in zip(f["vel"], staged[k]["vel"])), (tpt, sl, k)
+    # the bulk-copy form: the staged form's slots, each slot's source panels
+    # copied into shared memory by cp.async.bulk (double-buffered)
+    for sl, k in shapes(q):
+        ctx.set_cc_tuning_bulk(sl, k)
+        assert ctx.cc_form() == 3
+        assert ctx.cc_tuning()[:3] == (sl, k, -(-sl * q // 32) * 32)
+        f = unit_fields(g, vor)
+        step(ctx, f)
+        assert torch.equal(f["vors"], staged[k]["vors"]), ("bulk", sl, k)
+        assert all(torch.equal(a, b) for a, b in zip(f["vel"], staged[k]["vel"])), ("bulk", sl, k)
 
 
 def test_autotuner_times_every_shape(sb, grid):
@@ -114,11 +124,11 @@ def test_autotuner_times_every_shape(sb, grid):
     f = unit_fields(g, vor)
     step(ctx, f)
     sl, k, threads, cand, ms = ctx.cc_tuning()
-    assert cand == 1 + len(shapes(81)) + len(direct_shapes(81, 1)) + len(direct_shapes(81, 2)) and ms > 0
+    assert cand == 1 + 2 * len(shapes(81)) + len(direct_shapes(81, 1)) + len(direct_shapes(81, 2)) and ms > 0
     tpt = ctx.cc_form()
-    if tpt:
+    if tpt in (1, 2):
         assert (sl, k) in direct_shapes(81, tpt) and threads == -(-sl * -(-81 // tpt) // 32) * 32
-    else:
+    else:  # staged or bulk copies: the same shapes
         assert (sl, k, threads) == (0, 0, 128) or ((sl, k) in shapes(81) and threads == -(-sl * 81 // 32) * 32)
     again = unit_fields(g, vor)
     step(ctx, again)
@@ -146,6 +156,10 @@ def test_rejects_unsupported_shapes(sb):
             ctx.set_cc_tuning_direct(sl, k, tpt)
     with pytest.raises(sb.SbslpmError):  # float64: no barrier-free form
         tree_ctx(sb, 6, sb.FP64).set_cc_tuning_direct(6, 1, 1)
+    with pytest.raises(sb.SbslpmError):  # nor a bulk-copy one
+        tree_ctx(sb, 6, sb.FP64).set_cc_tuning_bulk(3, 1)
+    with pytest.raises(sb.SbslpmError):
+        ctx.set_cc_tuning_bulk(1, 1)  # 49 proxies: slots 3, 4, 6, 8
     small = tree_ctx(sb, 3, sb.MIXED)  # 16 proxies: whole-panel kernel only
     with pytest.raises(sb.SbslpmError):
         small.set_cc_tuning(1, 1)

@@ -112,3 +112,43 @@ def test_headline_configuration_meets_the_bar(sb):
         v, vel = gpu_step(sb, g, vor, levels=7, fmm_theta=0.7, proxy_degree=8, leaf_size=256, precision=prec)
         print(f"levels 7 prec={prec}: vorticity error {rel(v, dv):.3e}, velocity error {rel(vel, dvel):.3e}")
         assert rel(v, dv) <= BAR
+
+
+@pytest.mark.parametrize("levels", [5, 6])
+def test_two_sided_first_stage_near_field(sb, port, levels):
+    """The first stage's near field evaluated once per unordered leaf pair for
+    both directions (sbslpm_set_near_mutual): the same step within the
+    mixed-precision bar of the oracle's treecode and of the one-sided kernel,
+    and deterministic."""
+    g = sb.build_grid(levels, 3, exact_cc=True)
+    vor = rh4(g.x, g.y, g.z, g.area)
+    out = {}
+    for on in (False, True, True):
+        cfg = sb.config_default(levels=levels, interp_degree=3, kernel_eps=EPS, omega=OMEGA, dt=DT, fmm_theta=0.7,
+                                proxy_degree=8, leaf_size=256, precision=sb.MIXED)
+        ctx = sb.Context(cfg)
+        ctx.set_near_tuning(128, 2, 4)
+        ctx.set_near_mutual(on)
+        assert ctx.near_mutual()[0] == on
+        v = cuda(vor)
+        vel = [torch.zeros_like(v) for _ in range(3)]
+        ctx.bve_back_rk4_step(cuda(g.x), cuda(g.y), cuda(g.z), cuda(g.area), v, *vel)
+        if on in out:
+            assert torch.equal(v, out[on][0]) and torch.equal(torch.stack(vel), out[on][1])
+        out[on] = (v, torch.stack(vel))
+    assert rel(out[True][1], out[False][1]) <= MIXED_TOL
+    assert rel(out[True][0], out[False][0]) <= MIXED_TOL
+    if levels == 5:
+        og = port.build(levels, 3, None, exact_cc=True)
+        ov, ovel, _ = port.bve_step(og, vor, None, dt=DT, omega=OMEGA, eps=EPS, mode=2, tree=(8, 256, 0.7, 0))
+        assert rel(out[True][1], np.stack(ovel)) <= MIXED_TOL
+        assert rel(out[True][0], ov) <= MIXED_TOL
+
+
+def test_two_sided_kernel_refused_where_it_does_not_apply(sb):
+    for kw in (dict(precision=sb.FP64, leaf_size=256), dict(precision=sb.MIXED, leaf_size=64)):
+        cfg = sb.config_default(levels=5, interp_degree=3, kernel_eps=EPS, omega=OMEGA, dt=DT, fmm_theta=0.7,
+                                proxy_degree=8, **kw)
+        ctx = sb.Context(cfg)
+        with pytest.raises(sb.SbslpmError):
+            ctx.set_near_mutual(True)

@@ -80,3 +80,54 @@ def test_reference_arm_other_ranks_do_nothing(capsys):
 
     bench.run_reference(Args(), 1)  # rank 1 returns without work or output
     assert capsys.readouterr().out == ""
+
+
+def _lists_rank(rank, world, port, thetas, out):
+    """An ensemble sharded over ranks: each rank builds the treecode lists of
+    its members (every world-th theta) through the library's host API, and
+    the ranks gather them."""
+    import datetime
+
+    import torch.distributed as dist
+
+    from conftest import load_package
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=30))
+    try:
+        sb = load_package()
+        panels = sb.cubed_sphere_panels_init(4)
+        mine = {m: sb.dual_tree_traversal_flagged(4, panels, th) for m, th in enumerate(thetas) if m % world == rank}
+        mine = {m: (l.tolist(), n.tolist()) for m, (l, n) in mine.items()}
+        gathered = [None] * world
+        dist.all_gather_object(gathered, mine)
+        out.put((rank, gathered))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_ensemble_lists_sharded_over_two_ranks():
+    """The library's host traversal called on two gloo ranks, members split
+    between them: the gathered lists equal one process's build of every
+    member, and the same on both ranks."""
+    from conftest import load_package
+
+    thetas = [0.5, 0.55, 0.6, 0.65, 0.7, 0.8]
+    ctx = torch.multiprocessing.get_context("spawn")
+    q = ctx.Queue()
+    port = free_port()
+    procs = [ctx.Process(target=_lists_rank, args=(r, 2, port, thetas, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted((q.get(timeout=120) for _ in procs), key=lambda r: r[0])
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert res[0][1] == res[1][1]
+    merged = {m: v for part in res[0][1] for m, v in part.items()}
+    sb = load_package()
+    panels = sb.cubed_sphere_panels_init(4)
+    for m, th in enumerate(thetas):
+        lst, near = sb.dual_tree_traversal_flagged(4, panels, th)
+        assert merged[m] == (lst.tolist(), near.tolist())
+        assert np.array_equal(lst, sb.dual_tree_traversal(4, panels, th))
