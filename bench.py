@@ -266,6 +266,58 @@ def swe_bench(sb, torch, dev, flush, steps):
         drift.append(row)
     out["drift"] = drift
     out["speedup_mixed_vs_fp64"] = out["mixed"]["steps_per_s"] / out["fp64"]["steps_per_s"]
+
+    # the treecode velocity (theta 0.7, degree-8 proxies, 256-particle leaves)
+    # in both precisions, and every path's state after one step against the
+    # float64 direct-sum step
+    def one_step(ctx):
+        f = [T(g.x), T(g.y), T(g.z), T(g.area), T(vors), torch.zeros_like(T(vors)), T(h0)]
+        vel = [torch.zeros_like(f[0]) for _ in range(3)]
+        base = [torch.zeros_like(f[0]) for _ in range(3)]
+        ctx.swe_init(*f, *vel, *base)
+        ctx.swe_run(*f, *vel, None, *base, nsteps=1)
+        return f[4], f[5], f[6]
+
+    def swe_ctx(prec, **kw):
+        return sb.Context(sb.config_default(levels=LEVELS, interp_degree=DEGREE, kernel_eps=EPS, omega=om, dt=SWE_DT,
+                                            precision=prec, g_over_a=1.0, **kw))
+
+    for name, prec in (("tree_fp64", sb.FP64), ("tree_mixed", sb.MIXED)):
+        ctx = swe_ctx(prec, fmm_theta=THETA, proxy_degree=PROXY_DEGREE, leaf_size=LEAF_SIZE)
+        f = [T(g.x), T(g.y), T(g.z), T(g.area), T(vors), torch.zeros_like(T(vors)), T(h0)]
+        vel = [torch.zeros_like(f[0]) for _ in range(3)]
+        base = [torch.zeros_like(f[0]) for _ in range(3)]
+        ctx.swe_init(*f, *vel, *base)
+        args = (*f, *vel, None, *base)
+        ctx.swe_run(*args, nsteps=3)
+        torch.cuda.synchronize()
+        st = torch.cuda.current_stream()
+        ts = []
+        for _ in range(steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            ctx.swe_run(*args, nsteps=1)
+            e1.record(st)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        out[name] = {"steps_per_s": 1e3 / (sum(ts) / len(ts)), "ms_per_step": sum(ts) / len(ts)}
+        del ctx
+    ref1 = one_step(swe_ctx(sb.FP64, velocity=sb.VEL_DIRECT))
+    acc = {}
+    for name, kw in (("spectral_fmm_fp64", dict(fmm_theta=THETA)),
+                     ("spectral_fmm_mixed", dict(fmm_theta=THETA, precision=sb.MIXED)),
+                     ("treecode_fp64", dict(fmm_theta=THETA, proxy_degree=PROXY_DEGREE, leaf_size=LEAF_SIZE)),
+                     ("treecode_mixed", dict(fmm_theta=THETA, proxy_degree=PROXY_DEGREE, leaf_size=LEAF_SIZE,
+                                             precision=sb.MIXED))):
+        prec = kw.pop("precision", sb.FP64)
+        res = one_step(swe_ctx(prec, **kw))
+        acc[name] = {k: float((a - b).abs().max() / b.abs().max()) for k, a, b in
+                     zip(("rel_linf_vort", "rel_linf_div", "rel_linf_height"), res, ref1)}
+    out["accuracy_step1_vs_fp64_direct"] = acc
+    out["treecode_note"] = ("the treecode velocity of the SWE step: near leaf pairs of both fields particle x "
+                            "particle, every well-separated pair proxy x proxy (theta 0.7, degree-8 proxies, "
+                            "256-particle leaves), the irregular-point FMM design of the reference")
     out["config"] = {"workload": "SWE v2 RK4, 393,216 particles, steady geostrophic flow + N(0,1e-4^2) height "
                                  "noise, spectral FMM theta 0.7 (proxy degree 3)", "dt": SWE_DT,
                      "drift_steps": SWE_STEPS, "g_over_a": 1.0, "omega": om, "u0": u0, "gh0": 2.94}
@@ -478,7 +530,13 @@ def profile_run(sb, torch, dev, args):
                                            leaf_size=LEAF_SIZE))
         if proxy:  # the first-step autotuner's choice on this workload, fixed so that the capture sees steps only
             ctx.set_near_tuning(*[int(v) for v in args.near_shape.split(",")])
-            ctx.set_cc_tuning(*[int(v) for v in args.cc_shape.split(",")])
+            cc = args.cc_shape.split(",")
+            if len(cc) > 2 and cc[2] == "bulk":
+                ctx.set_cc_tuning_bulk(int(cc[0]), int(cc[1]))
+            elif len(cc) > 2:
+                ctx.set_cc_tuning_direct(int(cc[0]), int(cc[1]), int(cc[2]))
+            else:
+                ctx.set_cc_tuning(int(cc[0]), int(cc[1]))
             if args.near_mutual and prec == sb.MIXED:
                 ctx.set_near_mutual(True)
         f = [T(g.x), T(g.y), T(g.z), T(g.area), T(rh4(g)), *[torch.zeros_like(T(g.x)) for _ in range(3)], None]
@@ -669,7 +727,7 @@ def main():
                     help="--profile treecode/treecode64: near-field threads,targets per thread,splits")
     ap.add_argument("--cc-shape", default="3,3",
                     help="--profile treecode/treecode64: well-separated chunk slots per block,chunk length (0,0: "
-                         "one block per target panel)")
+                         "one block per target panel)[,bulk | ,targets per thread of the barrier-free form]")
     ap.add_argument("--near-mutual", action="store_true",
                     help="--profile treecode: the first stage's near field two-sided (sbslpm_set_near_mutual)")
     ap.add_argument("--degree", type=int, default=0,

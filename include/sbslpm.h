@@ -287,6 +287,18 @@ sbslpm_status sbslpm_swe_tendencies(sbslpm_ctx* ctx, const double* xcos, const d
  * every copy of a grid point shared by several panels gets the mean of the
  * copies (summed in [leaf][q] order). */
 sbslpm_status sbslpm_unify_boundary_vals(sbslpm_ctx* ctx, double* vals);
+/* The shallow-water velocity on the treecode (contexts with proxy_degree > 0
+ * and leaves of at most 256 particles; the SWE step uses it then): vorticity
+ * sources at the grid points displaced by (dx, dy, dz) (re-projected), with
+ * strengths w_vor, and divergence sources at the grid points with strengths
+ * w_div (A x q each), near leaf pairs particle x particle, every
+ * well-separated pair proxy x proxy -- the design of the reference's
+ * irregular-point FMM (swe_vel_panel_interaction_ll,
+ * src/fmm_interactions/swe_vel_impl.hpp:149-288).  u_* (A x q) receive the
+ * velocity at the grid points. */
+sbslpm_status sbslpm_swe_tree_velocity(sbslpm_ctx* ctx, const double* dx, const double* dy, const double* dz,
+                                       const double* w_vor, const double* w_div, double* u_x, double* u_y,
+                                       double* u_z);
 /* Replaces swe_vel_interactions_2 (src/fmm_interactions/swe_vel.cpp:39-67):
  * proxy-target velocities of vorticity sources at proj(proxy + disp) and
  * divergence sources at the fixed proxies; [panel][q] inputs; target_1..3

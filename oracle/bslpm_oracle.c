@@ -773,24 +773,44 @@ static int bltc_well_separated(const orc_panel* p, int t, int s, double theta) {
   return sep < theta;
 }
 
-/* One list entry of swe_vel_panel_interaction_ll, rotational part
+/* One list entry of swe_vel_panel_interaction_ll
  * (src/fmm_interactions/swe_vel_impl.hpp:256-284): targets j in order, sources
- * k in order; out receives 3 strided sums per target. */
+ * k in order; out receives 3 strided sums per target.  Rotational part with
+ * sources s (strengths sv); with sd, the divergent part with sources s2
+ * (strengths sd).  The reference's sources of both fields coincide; here the
+ * vorticity sources may be displaced while the divergence sources stay on the
+ * grid (swe_vel_panel_interaction_2, src/fmm_interactions/swe_vel_impl.hpp:124-141),
+ * and where they coincide the arithmetic is the reference's. */
+typedef struct {
+  const double* xyz;                 /* interleaved positions, or NULL */
+  const double *x, *y, *z, *w;       /* positions (when xyz is NULL) and strengths */
+} bltc_src;
+
 static void bltc_block(int nt, const double* txyz, size_t tstride, const double* tx, const double* ty,
-                       const double* tz, int ns, const double* sxyz, const double* sx, const double* sy,
-                       const double* sz, const double* sv, double eps, double* o1, double* o2, double* o3) {
+                       const double* tz, int ns, bltc_src s1, const bltc_src* s2, double eps, double* o1, double* o2,
+                       double* o3) {
   for (int j = 0; j < nt; j++) {
     double x_t = txyz ? txyz[3 * j] : tx[j], y_t = txyz ? txyz[3 * j + 1] : ty[j], z_t = txyz ? txyz[3 * j + 2] : tz[j];
     double a1 = o1[j * tstride], a2 = o2[j * tstride], a3 = o3[j * tstride];
     for (int k = 0; k < ns; k++) {
-      double x_s = sxyz ? sxyz[3 * k] : sx[k], y_s = sxyz ? sxyz[3 * k + 1] : sy[k],
-             z_s = sxyz ? sxyz[3 * k + 2] : sz[k];
+      double x_s = s1.xyz ? s1.xyz[3 * k] : s1.x[k], y_s = s1.xyz ? s1.xyz[3 * k + 1] : s1.y[k],
+             z_s = s1.xyz ? s1.xyz[3 * k + 2] : s1.z[k];
       double dp = x_t * x_s + y_t * y_s + z_t * z_s;
       double gf = 0.07957747154594767 / (1.0 - dp + eps);
-      double gf1 = -gf * sv[k];
-      a1 += gf1 * (y_t * z_s - z_t * y_s);
-      a2 += gf1 * (z_t * x_s - x_t * z_s);
-      a3 += gf1 * (x_t * y_s - y_t * x_s);
+      double gf1 = -gf * s1.w[k];
+      if (s2) {
+        double x2 = s2->xyz ? s2->xyz[3 * k] : s2->x[k], y2 = s2->xyz ? s2->xyz[3 * k + 1] : s2->y[k],
+               z2 = s2->xyz ? s2->xyz[3 * k + 2] : s2->z[k];
+        double dp2 = x_t * x2 + y_t * y2 + z_t * z2;
+        double gf2 = 0.07957747154594767 / (1.0 - dp2 + eps) * s2->w[k];
+        a1 += gf1 * (y_t * z_s - z_t * y_s) + gf2 * (x2 - x_t * dp2);
+        a2 += gf1 * (z_t * x_s - x_t * z_s) + gf2 * (y2 - y_t * dp2);
+        a3 += gf1 * (x_t * y_s - y_t * x_s) + gf2 * (z2 - z_t * dp2);
+      } else {
+        a1 += gf1 * (y_t * z_s - z_t * y_s);
+        a2 += gf1 * (z_t * x_s - x_t * z_s);
+        a3 += gf1 * (x_t * y_s - y_t * x_s);
+      }
     }
     o1[j * tstride] = a1;
     o2[j * tstride] = a2;
@@ -800,11 +820,12 @@ static void bltc_block(int nt, const double* txyz, size_t tstride, const double*
 
 /* The interaction list on the tree: entries grouped by target panel (stable,
  * so each target sees its sources in list order), target panels in parallel.
- * u (3 x N) receives particle-target sums, T (3 x Pf x qx) proxy-target sums. */
+ * u (3 x N) receives particle-target sums, T (3 x Pf x qx) proxy-target sums.
+ * Particle sources p1 (rotational) and, for the SWE, p2 (divergent), proxy
+ * strengths S and S2 at the fixed proxies. */
 static void bltc_interactions(const bltc_tree* t, long nl, const int* list, double theta, int typed,
-                              const double* tx, const double* ty, const double* tz, const double* sx,
-                              const double* sy, const double* sz, const double* w, const double* S, double eps,
-                              double* u, double* T) {
+                              const double* tx, const double* ty, const double* tz, bltc_src p1, const double* S,
+                              const bltc_src* p2, const double* S2, double eps, double* u, double* T) {
   int Pf = t->Pf, qx = t->qx, npl = t->npl;
   size_t pn = (size_t)Pf * qx, N = (size_t)t->Af * npl;
   long* start = (long*)calloc((size_t)Pf + 1, sizeof(long));
@@ -825,13 +846,20 @@ static void bltc_interactions(const bltc_tree* t, long nl, const int* list, doub
       size_t t0 = (size_t)(tp - t->offf) * npl, s0 = (size_t)(s - t->offf) * npl;
       double* o = tpart ? u + t0 : T + (size_t)tp * qx;
       size_t stride = tpart ? N : pn;
-      if (spart)
-        bltc_block(tpart ? npl : qx, tpart ? NULL : t->px + 3 * (size_t)tp * qx, 1, tx + t0, ty + t0, tz + t0, npl,
-                   NULL, sx + s0, sy + s0, sz + s0, w + s0, eps, o, o + stride, o + 2 * stride);
-      else
-        bltc_block(tpart ? npl : qx, tpart ? NULL : t->px + 3 * (size_t)tp * qx, 1, tx + t0, ty + t0, tz + t0, qx,
-                   t->px + 3 * (size_t)s * qx, NULL, NULL, NULL, S + (size_t)s * qx, eps, o, o + stride,
+      const double* txyz = tpart ? NULL : t->px + 3 * (size_t)tp * qx;
+      int nt = tpart ? npl : qx;
+      if (spart) {
+        bltc_src a = {NULL, p1.x + s0, p1.y + s0, p1.z + s0, p1.w + s0}, b;
+        if (p2) b = (bltc_src){NULL, p2->x + s0, p2->y + s0, p2->z + s0, p2->w + s0};
+        bltc_block(nt, txyz, 1, tx + t0, ty + t0, tz + t0, npl, a, p2 ? &b : NULL, eps, o, o + stride,
                    o + 2 * stride);
+      } else {
+        const double* sxyz = t->px + 3 * (size_t)s * qx;
+        bltc_src a = {sxyz, NULL, NULL, NULL, S + (size_t)s * qx}, b = {sxyz, NULL, NULL, NULL, NULL};
+        if (p2) b.w = S2 + (size_t)s * qx;
+        bltc_block(nt, txyz, 1, tx + t0, ty + t0, tz + t0, qx, a, p2 ? &b : NULL, eps, o, o + stride,
+                   o + 2 * stride);
+      }
     }
   }
   free(start);
@@ -876,9 +904,36 @@ void orc_bltc_velocity(int levels, int degree, int leaf_size, int n, double thet
   double* T = (double*)calloc(3 * pn, sizeof(double));
   memset(u, 0, sizeof(double) * 3 * N);
   bltc_upward(&t, sx, sy, sz, w, S);
-  bltc_interactions(&t, nl, list, theta, typed, tx, ty, tz, sx, sy, sz, w, S, eps, u, T);
+  bltc_src p1 = {NULL, sx, sy, sz, w};
+  bltc_interactions(&t, nl, list, theta, typed, tx, ty, tz, p1, S, NULL, NULL, eps, u, T);
   bltc_downward(&t, tx, ty, tz, T, u);
   free(S);
+  free(T);
+  free(list);
+  bltc_tree_free(&t);
+}
+
+void orc_bltc_velocity_swe(int levels, int degree, int leaf_size, int n, double theta, double eps, int typed,
+                           const double* tx, const double* ty, const double* tz, const double* sx, const double* sy,
+                           const double* sz, const double* w, const double* dx, const double* dy, const double* dz,
+                           const double* wd, double* u) {
+  bltc_tree t;
+  bltc_tree_init(levels, degree, leaf_size, n, &t);
+  size_t pn = (size_t)t.Pf * t.qx, N = (size_t)t.Af * t.npl;
+  long nl = orc_dual_tree_traversal(t.Lf, t.tp, theta, NULL, 0);
+  int* list = (int*)malloc(sizeof(int) * 3 * (size_t)(nl > 0 ? nl : 1));
+  orc_dual_tree_traversal(t.Lf, t.tp, theta, list, nl);
+  double* S = (double*)calloc(pn, sizeof(double));
+  double* S2 = (double*)calloc(pn, sizeof(double));
+  double* T = (double*)calloc(3 * pn, sizeof(double));
+  memset(u, 0, sizeof(double) * 3 * N);
+  bltc_upward(&t, sx, sy, sz, w, S);
+  bltc_upward(&t, dx, dy, dz, wd, S2);
+  bltc_src p1 = {NULL, sx, sy, sz, w}, p2 = {NULL, dx, dy, dz, wd};
+  bltc_interactions(&t, nl, list, theta, typed, tx, ty, tz, p1, S, &p2, S2, eps, u, T);
+  bltc_downward(&t, tx, ty, tz, T, u);
+  free(S);
+  free(S2);
   free(T);
   free(list);
   bltc_tree_free(&t);

@@ -98,6 +98,13 @@ void orc_bltc_downward(int levels, int degree, int leaf_size, int n, double* T, 
 void orc_bltc_velocity(int levels, int degree, int leaf_size, int n, double theta, double eps, int typed,
                        const double* tx, const double* ty, const double* tz, const double* sx, const double* sy,
                        const double* sz, const double* w, double* u);
+/* The shallow-water form: vorticity sources s (strengths w, rotational part)
+ * and divergence sources d (strengths wd, divergent part of
+ * swe_vel_panel_interaction_ll, src/fmm_interactions/swe_vel_impl.hpp:256-284). */
+void orc_bltc_velocity_swe(int levels, int degree, int leaf_size, int n, double theta, double eps, int typed,
+                           const double* tx, const double* ty, const double* tz, const double* sx, const double* sy,
+                           const double* sz, const double* w, const double* dx, const double* dy, const double* dz,
+                           const double* wd, double* u);
 
 /* direct_sum_inv_lap (src/direct_sum_impl.hpp:20-27) over n points. */
 void orc_direct_sum_inv_lap(int n, const double* x, const double* y, const double* z, const double* area,

@@ -223,6 +223,15 @@ class Port:
         self.lib.orc_bltc_downward(levels, degree, leaf_size, n, _dp(t), *[_dp(v) for v in a], _dp(u))
         return t, u
 
+    def bltc_velocity_swe(self, levels, degree, leaf_size, n, theta, eps, typed, t, s, w, d, wd):
+        """Shallow-water treecode velocity (3 x N): vorticity sources s (strengths w), divergence
+        sources d (strengths wd)."""
+        a = [np.ascontiguousarray(v, dtype=np.float64).ravel() for v in (*t, *s, w, *d, wd)]
+        u = np.zeros((3, a[0].size))
+        self.lib.orc_bltc_velocity_swe(levels, degree, leaf_size, n, ctypes.c_double(theta), ctypes.c_double(eps),
+                                       int(typed), *[_dp(v) for v in a], _dp(u))
+        return u
+
     def bltc_velocity(self, levels, degree, leaf_size, n, theta, eps, typed, t, s, w):
         """Treecode velocity (3 x N) at targets t = (x, y, z) of sources s with strengths w."""
         a = [np.ascontiguousarray(v, dtype=np.float64).ravel() for v in (*t, *s, w)]
@@ -453,9 +462,10 @@ class Ref:
         self.lib.ref_ll_downward(c["h"], *[_dp(v) for v in t], *[_dp(v) for v in s])
         return s
 
-    def ll_velocity(self, c, vors):
+    def ll_velocity(self, c, vors, divs=None):
         out = [np.zeros((c["A"], c["q"])) for _ in range(3)]
-        self.lib.ref_ll_velocity(c["h"], _dp(np.ascontiguousarray(vors, dtype=np.float64)), *[_dp(v) for v in out])
+        d = None if divs is None else _dp(np.ascontiguousarray(divs, dtype=np.float64))
+        self.lib.ref_ll_velocity(c["h"], _dp(np.ascontiguousarray(vors, dtype=np.float64)), d, *[_dp(v) for v in out])
         return out
 
     def swe_map(self, c):

@@ -9,8 +9,8 @@
 //   upward_pass_ll                 (src/fmm_funcs.cpp:394-405; base_pots_ll,
 //                                   child_to_parent_ll src/fmm_funcs_impl.hpp:190-268)
 //   swe_vel_interactions_ll        (src/fmm_interactions/swe_vel.cpp:69-100,
-//                                   swe_vel_panel_interaction_ll swe_vel_impl.hpp:149-288)
-//                                  with zero divergence: the rotational part
+//                                   swe_vel_panel_interaction_ll swe_vel_impl.hpp:149-288),
+//                                  rotational and divergent parts
 //   downward_pass_3_ll             (src/fmm_funcs.cpp:407-419; parent_to_child_3_ll,
 //                                   child_panel_interp_3_ll src/fmm_funcs_impl.hpp:270-364)
 // The tree table is built as initialize_cube_sphere_irreg_points builds its
@@ -174,9 +174,10 @@ void ref_ll_downward(void* h, const double* t1, const double* t2, const double* 
   copy_out(w, s3);
 }
 
-// The irregular-point FMM velocity of vorticity vors (A x q; zero divergence):
-// upward_pass_ll, swe_vel_interactions_ll, downward_pass_3_ll.
-void ref_ll_velocity(void* h, const double* vors, double* vel_x, double* vel_y, double* vel_z) {
+// The irregular-point FMM velocity of vorticity vors and divergence divs
+// (A x q; divs may be NULL: zero divergence): upward_pass_ll of both fields,
+// swe_vel_interactions_ll, downward_pass_3_ll.
+void ref_ll_velocity(void* h, const double* vors, const double* divs, double* vel_x, double* vel_y, double* vel_z) {
   LLCtx* c = static_cast<LLCtx*>(h);
   RefCtx* g = c->grid;
   int A = g->rc.active_panel_count, q = g->q;
@@ -184,6 +185,10 @@ void ref_ll_velocity(void* h, const double* vors, double* vel_x, double* vel_y, 
       t2("t2", c->Pf, c->qx), t3("t3", c->Pf, c->qx), vx("vx", A, q), vy("vy", A, q), vz("vz", A, q);
   copy_in(v, vors);
   upward_pass_ll(c->rc, g->xcos, g->ycos, g->zcos, c->tree, g->area, v, psv, c->lpp);
+  if (divs) {
+    copy_in(d, divs);
+    upward_pass_ll(c->rc, g->xcos, g->ycos, g->zcos, c->tree, g->area, d, psd, c->lpp);
+  }
   swe_vel_interactions_ll(c->rc, g->xcos, g->ycos, g->zcos, t1, t2, t3, vx, vy, vz, psv, psd, v, d, g->area, c->list,
                           c->tree, c->lpp);
   downward_pass_3_ll(c->rc, g->xcos, g->ycos, g->zcos, c->tree, t1, t2, t3, vx, vy, vz, c->lpp);

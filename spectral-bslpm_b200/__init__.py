@@ -153,6 +153,7 @@ def lib() -> ctypes.CDLL:
     L.sbslpm_swe_tendencies.argtypes = [_VP] * 14
     L.sbslpm_unify_boundary_vals.argtypes = [_VP] * 2
     L.sbslpm_swe_vel_interactions.argtypes = [_VP] * 9
+    L.sbslpm_swe_tree_velocity.argtypes = [_VP] * 9
     L.sbslpm_cubed_sphere_2d_to_1d.argtypes = [ctypes.c_long, ctypes.c_int, _D, _D, _D, _I, _I,
                                                ctypes.POINTER(ctypes.c_long)]
     L.sbslpm_bve_adjoint_step.argtypes = [_VP] * 8
@@ -557,6 +558,15 @@ class Context:
         self._sync_stream()
         _check(lib().sbslpm_swe_vel_interactions(self._h, *[_dev(t, "field") for t in (
             disp_x, disp_y, disp_z, source_vor, source_div, t1, t2, t3)]), "sbslpm_swe_vel_interactions")
+
+    def swe_tree_velocity(self, disp_x, disp_y, disp_z, w_vor, w_div, u_x, u_y, u_z):
+        """Treecode SWE velocity at the grid: vorticity sources displaced by disp (strengths
+        w_vor), divergence sources at the grid (strengths w_div); u_* written."""
+        lq = (self.leaf_count, self.q)
+        self._sync_stream()
+        _check(lib().sbslpm_swe_tree_velocity(self._h, *[_dev(t, n, lq) for t, n in (
+            (disp_x, "disp_x"), (disp_y, "disp_y"), (disp_z, "disp_z"), (w_vor, "w_vor"), (w_div, "w_div"),
+            (u_x, "u_x"), (u_y, "u_y"), (u_z, "u_z"))]), "sbslpm_swe_tree_velocity")
 
     # -- adjoint -----------------------------------------------------------
     def bve_adjoint_step(self, xcos, ycos, zcos, area, vors, vors_bar_next, vors_bar):

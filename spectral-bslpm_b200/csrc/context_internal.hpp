@@ -62,6 +62,9 @@ struct sbslpm_ctx {
   int *fface = nullptr, *near_start = nullptr, *near_src = nullptr, *cc_start = nullptr, *cc_src = nullptr;
   int4* fentry32 = nullptr;  // the same entry table over the well-separated list (mixed, q <= 32)
   double4 *fsrc = nullptr, *psrc = nullptr;
+  // SWE on the treecode: the divergence field's particle sources and proxies
+  double4 *fsrc2 = nullptr, *psrc2 = nullptr;
+  float4 *fsrcf2 = nullptr, *psrcf2 = nullptr;
   double* gx = nullptr;  // [3][particles]: the particle grid, for timing the near kernel alone
   double* near = nullptr;  // [4][3][particles] near-field partial sums (near_splits in use)
   int near_splits = 2, near_nt = 128, near_tpt = 2;  // near-field launch shape (autotuned on the first step)

@@ -22,9 +22,8 @@ sbslpm_status swe_setup(sbslpm_ctx* c) {
   if (c->swe_ready) return SBSLPM_OK;
   if (c->d < 2)
     return set_last_error("the shallow-water step needs interp_degree >= 2 (three-node stencils)"), SBSLPM_ERR_CONFIG;
-  if (c->tree)
-    return set_last_error("the shallow-water step runs on the spectral FMM (proxy_degree 0) or direct velocity"),
-           SBSLPM_ERR_CONFIG;
+  if (c->tree && c->npl > 256)
+    return set_last_error("the shallow-water treecode takes leaves of at most 256 particles"), SBSLPM_ERR_CONFIG;
   const long ln = (long)c->A * c->q;
   std::vector<double> interp, g(3 * ln), area(ln);
   build_interp(c->d, false, interp);
@@ -50,14 +49,29 @@ sbslpm_status swe_setup(sbslpm_ctx* c) {
   SB_TRY(upload(&c->s_pface, pface));
   SB_TRY(upload(&c->s_ustart, ustart));
   SB_TRY(upload(&c->s_umem, umem));
-  const size_t pn = (size_t)c->P * c->q;
-  if (!c->src) SB_TRY(dalloc(&c->src, pn));
-  SB_TRY(dalloc(&c->src2, pn));
-  if (c->cfg.precision == SBSLPM_MIXED) {
-    if (!c->srcf) SB_TRY(dalloc(&c->srcf, pn));
-    SB_TRY(dalloc(&c->srcf2, pn));
+  if (c->tree) {  // the divergence field on the treecode: particle sources and proxies
+    const size_t fpn = (size_t)c->Pf * c->qx;
+    SB_TRY(dalloc(&c->psrc2, (size_t)ln));
+    SB_TRY(dalloc(&c->fsrc2, fpn));
+    std::vector<double4> init(fpn);
+    std::vector<double> fpx(3 * fpn);
+    SB_CUDA(cudaMemcpy(fpx.data(), c->fpx, sizeof(double) * 3 * fpn, cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < fpn; i++) init[i] = make_double4(fpx[i], fpx[fpn + i], fpx[2 * fpn + i], 0.0);
+    SB_CUDA(cudaMemcpy(c->fsrc2, init.data(), sizeof(double4) * fpn, cudaMemcpyHostToDevice));
+    if (c->cfg.precision == SBSLPM_MIXED) {
+      SB_TRY(dalloc(&c->psrcf2, (size_t)ln));
+      SB_TRY(dalloc(&c->fsrcf2, fpn));
+    }
+  } else {
+    const size_t pn = (size_t)c->P * c->q;
+    if (!c->src) SB_TRY(dalloc(&c->src, pn));
+    SB_TRY(dalloc(&c->src2, pn));
+    if (c->cfg.precision == SBSLPM_MIXED) {
+      if (!c->srcf) SB_TRY(dalloc(&c->srcf, pn));
+      SB_TRY(dalloc(&c->srcf2, pn));
+    }
+    if (!c->tgt) SB_TRY(dalloc(&c->tgt, 3 * pn));
   }
-  if (!c->tgt) SB_TRY(dalloc(&c->tgt, 3 * pn));
   SB_TRY(dalloc(&c->tend, 9 * (size_t)ln));
   SB_TRY(dalloc(&c->avor, (size_t)ln));
 
@@ -72,10 +86,44 @@ sbslpm_status swe_setup(sbslpm_ctx* c) {
   s.pface = c->s_pface;
   s.ustart = c->s_ustart;
   s.umem = c->s_umem;
-  s.srcf2 = c->srcf2;
-  c->geom.srcf = c->srcf;
+  s.srcf2 = c->tree ? c->fsrcf2 : c->srcf2;
+  if (!c->tree) c->geom.srcf = c->srcf;
   c->swe_ready = true;
   return SBSLPM_OK;
+}
+
+// The treecode velocity of both fields (bltc_swe.cu): leaf sources and their
+// anterpolation, then, on the auxiliary stream, the upward pass of each
+// field, the SWE proxy kernel over the well-separated list and the downward
+// pass, beside the near field of both fields; the leaf interpolation adds
+// the two.  Piecewise mode with explicit displacements and strengths.
+void swe_tree_velocity(sbslpm_ctx* c, int stage, double dtd, double dts, const double* vprev, const double* tprev,
+                       const double* x, const double* y, const double* z, const double* area, const double* vors,
+                       const double* divs, const double* dispx, const double* dispy, const double* dispz,
+                       const double* wv, const double* wd, double* v) {
+  cudaStream_t st = c->stream();
+  const bool mixed = c->cfg.precision == SBSLPM_MIXED;
+  const StepGeom& fg = c->fgeom;
+  launch_bltc_swe_sources(c->tgeom, fg, c->ftab, stage, dtd, dts, vprev, tprev, x, y, z, vors, divs, area, dispx,
+                          dispy, dispz, wv, wd, c->psrc, c->psrcf, c->psrc2, c->psrcf2, c->fsrc, c->fsrc2, mixed, st);
+  cudaStream_t tree_st = c->aux_stream ? c->aux_stream : st;
+  if (c->aux_stream) {
+    cudaEventRecord(c->ev_fork, st);
+    cudaStreamWaitEvent(tree_st, c->ev_fork, 0);
+  }
+  launch_upward_fused(fg, 2, 0, 0.0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, c->fsrc, mixed, tree_st);
+  StepGeom fg2 = fg;  // the divergence proxies pack into their own buffer
+  fg2.srcf = c->fsrcf2;
+  launch_upward_fused(fg2, 2, 0, 0.0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, c->fsrc2, mixed,
+                      tree_st);
+  launch_swe_interactions(fg, c->sgeom, c->cfg.precision, c->fsrc, c->fsrc2, c->ftgt, tree_st);
+  launch_downward_fused(fg, c->ftgt, nullptr, tree_st);
+  if (c->aux_stream) cudaEventRecord(c->ev_join, tree_st);
+  constexpr int kSplits = 4;
+  launch_bltc_swe_near(c->tgeom, fg, c->cfg.precision, x, y, z, c->psrc, c->psrc2, c->psrcf, c->psrcf2, c->near,
+                       kSplits, st);
+  if (c->aux_stream) cudaStreamWaitEvent(st, c->ev_join, 0);
+  launch_bltc_to_particles(c->tgeom, fg, c->ftgt, c->near, kSplits, v, st);
 }
 
 // One velocity evaluation of both source fields (stage 0 undisplaced;
@@ -86,6 +134,11 @@ void swe_velocity_eval(sbslpm_ctx* c, int stage, double dtd, double dts, const d
   cudaStream_t st = c->stream();
   const StepGeom& g = c->geom;
   const bool mixed = c->cfg.precision == SBSLPM_MIXED;
+  if (c->tree) {
+    swe_tree_velocity(c, stage, dtd, dts, vprev, tprev, x, y, z, area, vors, divs, nullptr, nullptr, nullptr, nullptr,
+                      nullptr, v);
+    return;
+  }
   if (c->cfg.velocity == SBSLPM_VEL_DIRECT) {
     launch_swe_leaf_sources(g, c->sgeom, stage, dtd, dts, vprev, tprev, vors, divs, area, c->src, c->src2, mixed, st);
     launch_swe_direct(g, c->sgeom, c->cfg.precision, c->src, c->src2, v, c->partial, c->groups, st);
@@ -254,12 +307,34 @@ sbslpm_status sbslpm_swe_vel_interactions(sbslpm_ctx* c, const double* dx, const
     return SBSLPM_ERR_ARG;
   if (c->cfg.velocity != SBSLPM_VEL_FMM)
     return set_last_error("the interaction list exists only with FMM velocity"), SBSLPM_ERR_CONFIG;
+  if (c->tree)
+    return set_last_error("a treecode context has no spectral interaction list (sbslpm_swe_tree_velocity)"),
+           SBSLPM_ERR_CONFIG;
   SB_TRY(swe_setup(c));
   cudaStream_t st = c->stream();
   launch_swe_sources_from_disp(c->geom, c->sgeom, dx, dy, dz, sv, sd, c->src, c->src2,
                                c->cfg.precision == SBSLPM_MIXED, st);
   launch_swe_interactions(c->geom, c->sgeom, c->cfg.precision, c->src, c->src2, c->tgt, st);
   launch_add3(c->tgt, (long)c->P * c->q, t1, t2, t3, st);
+  return finish(c);
+}
+
+sbslpm_status sbslpm_swe_tree_velocity(sbslpm_ctx* c, const double* dx, const double* dy, const double* dz,
+                                       const double* w_vor, const double* w_div, double* u_x, double* u_y,
+                                       double* u_z) {
+  if (!c || bad(dx) || bad(dy) || bad(dz) || bad(w_vor) || bad(w_div) || bad(u_x) || bad(u_y) || bad(u_z))
+    return SBSLPM_ERR_ARG;
+  if (any_on_host({dx, dy, dz, w_vor, w_div, u_x, u_y, u_z}))
+    return set_last_error("device pointers expected"), SBSLPM_ERR_ARG;
+  if (!c->tree) return set_last_error("the context has no treecode (proxy_degree 0)"), SBSLPM_ERR_CONFIG;
+  SB_TRY(swe_setup(c));
+  cudaStream_t st = c->stream();
+  const size_t ln = (size_t)c->A * c->q;
+  double* v = c->vbuf;
+  swe_tree_velocity(c, 0, 0.0, 0.0, nullptr, nullptr, c->gx, c->gx + ln, c->gx + 2 * ln, nullptr, nullptr, nullptr,
+                    dx, dy, dz, w_vor, w_div, v);
+  double* outs[3] = {u_x, u_y, u_z};
+  for (int k = 0; k < 3; k++) SB_CUDA(cudaMemcpyAsync(outs[k], v + k * ln, sizeof(double) * ln, cudaMemcpyDeviceToDevice, st));
   return finish(c);
 }
 

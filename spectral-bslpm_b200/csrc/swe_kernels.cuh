@@ -66,4 +66,21 @@ void launch_unify(const SweGeom& s, double* f0, double* f1, double* f2, int roun
 void launch_swe_arrival(const StepGeom& g, const double* tend1, double dt, const double* vors, double* divs,
                         double* height, double* avor, cudaStream_t st);
 
+// Treecode velocity of the SWE step (bltc_swe.cu).  Leaf sources of both
+// fields and their anterpolation onto the tree leaves' proxies (proxy: the
+// vorticity proxies' .w, proxy2: the divergence proxies' .w): step mode from
+// (stage, dtd, dts, vprev, tprev, vors, divs, area) as launch_swe_upward, or,
+// with dispx/dispy/dispz, positions x + disp and strengths wv / wd given.
+void launch_bltc_swe_sources(const TreeGeom& tg, const StepGeom& fg, const BliTable& tab, int stage, double dtd,
+                             double dts, const double* vprev, const double* tprev, const double* x, const double* y,
+                             const double* z, const double* vors, const double* divs, const double* area,
+                             const double* dispx, const double* dispy, const double* dispz, const double* wv,
+                             const double* wd, double4* psrc, float4* psrcf, double4* psrc2, float4* psrcf2,
+                             double4* proxy, double4* proxy2, bool mixed, cudaStream_t st);
+// Near leaf pairs of both fields into splits x 3 x N velocity partials
+// (leaves of at most 256 particles).
+void launch_bltc_swe_near(const TreeGeom& tg, const StepGeom& fg, int precision, const double* x, const double* y,
+                          const double* z, const double4* psrc, const double4* psrc2, const float4* psrcf,
+                          const float4* psrcf2, double* near, int splits, cudaStream_t st);
+
 }  // namespace sbslpm

@@ -18,3 +18,8 @@ def down_in(Pf, qx):
     """Three proxy-target fields, smooth in the panel and proxy indices."""
     p, k = np.meshgrid(np.arange(Pf), np.arange(qx), indexing="ij")
     return [np.cos(0.37 * p + 1.3 * k + f) for f in range(3)]
+
+
+def divs_of(x, y, z):
+    """A smooth divergence-like field on the grid."""
+    return 0.4 * np.cos(2 * x - z) + 0.2 * y * z

@@ -15,6 +15,8 @@ and stores small cases as tests/golden/bltc_<name>.npz:
              into zero particle values (3 x A x q)
   vel        the velocity of the vorticity pots (3 x A x q): upward pass,
              typed interactions, downward pass
+  vel_swe    the same with the divergence divs_of as the second source
+             field (the rotational and divergent parts)
 
 The inputs are smooth functions of the grid (pots) and of the panel and
 proxy indices (down_in), defined in tests/golden/bltc_inputs.py and
@@ -34,7 +36,7 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 import numpy as np  # noqa: E402
 
 from oracle.pyoracle import Ref  # noqa: E402
-from tests.golden.bltc_inputs import CASES, EPS, down_in, pots_of  # noqa: E402
+from tests.golden.bltc_inputs import CASES, EPS, divs_of, down_in, pots_of  # noqa: E402
 
 def main():
     ref = Ref()
@@ -47,7 +49,8 @@ def main():
         out = dict(levels=levels, degree=degree, leaf_size=leaf, proxy_degree=n, theta=theta, eps=EPS,
                    tree_levels=ll["Lf"], npl=ll["npl"], list=ref.ll_list(ll), upward=ref.ll_upward(ll, pots),
                    down_out=np.stack(ref.ll_downward(ll, *down_in(ll["Pf"], ll["qx"]))),
-                   vel=np.stack(ref.ll_velocity(ll, pots)))
+                   vel=np.stack(ref.ll_velocity(ll, pots)),
+                   vel_swe=np.stack(ref.ll_velocity(ll, pots, divs_of(x, y, z))))
         ref.ll_destroy(ll)
         np.savez_compressed(os.path.join(HERE, f"bltc_{name}.npz"), **out)
         print(name, {k: getattr(v, "shape", v) for k, v in out.items()})

@@ -1,0 +1,100 @@
+"""The shallow-water velocity and step on the treecode (proxy_degree > 0),
+through the C ABI.
+
+Checker: the oracle's shallow-water treecode (orc_bltc_velocity_swe,
+oracle/bslpm_oracle.c) with every well-separated pair proxy x proxy, built
+from the reference's irregular-point FMM functions and pinned to them with
+both source fields by tests/test_oracle_bltc.py.  Tolerances: float64
+velocity <= 1e-12 relative L-infinity, mixed <= 1e-6; the treecode step
+against the float64 direct-sum step within the treecode's own error.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+EPS = 1e-4
+
+
+def rel(a, b):
+    a = a.detach().cpu().numpy() if hasattr(a, "detach") else np.asarray(a)
+    b = b.detach().cpu().numpy() if hasattr(b, "detach") else np.asarray(b)
+    return float(np.abs(a - b).max() / np.abs(b).max())
+
+
+def cuda(a):
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).cuda()
+
+
+def tree_ctx(sb, levels, n, leaf, theta, precision, **kw):
+    return sb.Context(sb.config_default(levels=levels, interp_degree=3, fmm_theta=theta, kernel_eps=EPS,
+                                        omega=2 * np.pi, dt=0.002, proxy_degree=n, leaf_size=leaf,
+                                        precision=precision, g_over_a=1.0, **kw))
+
+
+@pytest.mark.parametrize("levels,leaf,n,theta", [(5, 256, 8, 0.7), (4, 64, 6, 0.5), (4, 16, 5, 0.8)])
+def test_swe_tree_velocity_matches_oracle(sb, port, levels, leaf, n, theta):
+    g = sb.build_grid(levels, 3, exact_cc=True)
+    rng = np.random.default_rng(7)
+    d = [2e-3 * rng.standard_normal(g.x.shape) for _ in range(3)]
+    lat, lon = np.arcsin(np.clip(g.z, -1, 1)), np.arctan2(g.y, g.x)
+    wv = g.area * (np.sin(lat) - 0.5 * np.sin(lat) * np.cos(lat) ** 4 * 30 * np.cos(4 * lon))
+    wd = g.area * 0.3 * np.cos(2 * g.x - g.z)
+    s = np.stack([g.x + d[0], g.y + d[1], g.z + d[2]])
+    s /= np.linalg.norm(s, axis=0)
+    p = (g.x, g.y, g.z)
+    want = port.bltc_velocity_swe(levels, 3, leaf, n, theta, EPS, 0, p, (s[0], s[1], s[2]), wv, p, wd)
+    for prec, tol in ((sb.FP64, 1e-12), (sb.MIXED, 1e-6)):
+        ctx = tree_ctx(sb, levels, n, leaf, theta, prec)
+        u = [torch.zeros(g.x.shape, dtype=torch.float64, device="cuda") for _ in range(3)]
+        ctx.swe_tree_velocity(*[cuda(a) for a in d], cuda(wv), cuda(wd), *u)
+        err = rel(torch.stack(u).reshape(3, -1), want)
+        print(f"levels {levels} leaf {leaf} n {n} theta {theta} prec {prec}: {err:.2e}")
+        assert err <= tol
+
+
+def swe_state(sb, levels):
+    g = sb.build_grid(levels, 3, exact_cc=True)
+    om, u0 = 2 * np.pi, 2 * np.pi / 12
+    lat = np.arcsin(np.clip(g.z, -1, 1))
+    vor = 2 * u0 * np.sin(lat)
+    h0 = 2.94 - (om * u0 + 0.5 * u0 * u0) * np.sin(lat) ** 2
+    h0 = h0 + 1e-4 * np.random.default_rng(4).standard_normal(h0.shape)
+    return g, vor, h0
+
+
+def swe_steps(sb, ctx, g, vor, h0, nsteps):
+    f = [cuda(g.x), cuda(g.y), cuda(g.z), cuda(g.area), cuda(vor), cuda(np.zeros_like(h0)), cuda(h0)]
+    vel = [torch.zeros_like(f[0]) for _ in range(3)]
+    base = [torch.zeros_like(f[0]) for _ in range(3)]
+    ctx.swe_init(*f, *vel, *base)
+    ctx.swe_run(*f, *vel, None, *base, nsteps=nsteps)
+    return f[4], f[5], f[6], torch.stack(vel)
+
+
+@pytest.mark.parametrize("n,theta", [(8, 0.7), (6, 0.5)])
+def test_swe_tree_step_against_the_direct_sum(sb, n, theta):
+    """The benchmark's SWE flow at 24,576 particles, 5 steps: the treecode
+    step (float64 and mixed) against the float64 direct-sum step; the mixed
+    treecode against the float64 treecode within 1e-6."""
+    g, vor, h0 = swe_state(sb, 5)
+    dctx = sb.Context(sb.config_default(levels=5, interp_degree=3, kernel_eps=EPS, omega=2 * np.pi, dt=0.002,
+                                        velocity=sb.VEL_DIRECT, g_over_a=1.0))
+    dv, dd, dh, dvel = swe_steps(sb, dctx, g, vor, h0, 5)
+    out = {}
+    for prec in (sb.FP64, sb.MIXED):
+        v, d, h, vel = swe_steps(sb, tree_ctx(sb, 5, n, 256, theta, prec), g, vor, h0, 5)
+        out[prec] = (v, d, h, vel)
+        print(f"n {n} theta {theta} prec {prec}: vorticity {rel(v, dv):.2e}, divergence {rel(d, dd):.2e}, "
+              f"height {rel(h, dh):.2e}, velocity {rel(vel, dvel):.2e}")
+        assert rel(v, dv) <= 1e-6 and rel(h, dh) <= 1e-6 and rel(vel, dvel) <= 1e-5
+    for a, b in zip(out[sb.MIXED], out[sb.FP64]):
+        assert rel(a, b) <= 1e-6
+
+
+def test_spectral_piecewise_entry_refused_on_treecode(sb):
+    ctx = tree_ctx(sb, 4, 6, 64, 0.7, sb.FP64)
+    t = [torch.zeros(sb.panel_count(4) * 16, dtype=torch.float64, device="cuda") for _ in range(8)]
+    with pytest.raises(sb.SbslpmError):
+        ctx.swe_vel_interactions(*t)

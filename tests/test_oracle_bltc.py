@@ -18,7 +18,7 @@ import numpy as np
 import pytest
 
 from conftest import GOLDEN
-from tests.golden.bltc_inputs import CASES, EPS, down_in, pots_of
+from tests.golden.bltc_inputs import CASES, EPS, divs_of, down_in, pots_of
 
 TOL = 1e-13
 
@@ -65,6 +65,17 @@ def test_typed_velocity(case, port):
     w = pots_of(*p) * g["area"]
     u = port.bltc_velocity(levels, degree, leaf, n, theta, EPS, 1, p, p, w)
     assert rel(u, gd["vel"].reshape(3, -1)) <= TOL
+
+
+def test_typed_shallow_water_velocity(case, port):
+    """Both fields (vorticity and divergence at the grid points): the
+    rotational and divergent parts of swe_vel_panel_interaction_ll."""
+    gd, g, (levels, degree, leaf, n, theta) = case
+    p = (g["x"], g["y"], g["z"])
+    w = pots_of(*p) * g["area"]
+    wd = divs_of(*p) * g["area"]
+    u = port.bltc_velocity_swe(levels, degree, leaf, n, theta, EPS, 1, p, p, w, p, wd)
+    assert rel(u, gd["vel_swe"].reshape(3, -1)) <= TOL
 
 
 def test_untyped_velocity_within_the_treecode_error(case, port):
