@@ -609,6 +609,22 @@ def adjoint_bench(sb, torch, dev, directions=8):
     t2.synchronize()
     tree = {"forward_ms": t0.elapsed_time(t1), "backward_ms": t1.elapsed_time(t2),
             "grad_rel_l2_vs_direct_sum_adjoint": float((xt.grad - grad).norm() / grad.norm())}
+    # and through the mixed-precision treecode's adjoint (float32 transposed pair sums)
+    ctxm = sb.Context(sb.config_default(levels=ADJ_LEVELS, interp_degree=DEGREE, kernel_eps=EPS, omega=OMEGA,
+                                        dt=ADJ_DT, precision=sb.MIXED, fmm_theta=THETA, proxy_degree=PROXY_DEGREE,
+                                        leaf_size=LEAF_SIZE))
+    xm = T(wn).requires_grad_()
+    sb.bve_rollout(ctxm, *f, T(wn), 1)  # first-step launch-shape timing outside the timed region
+    t0.record(st)
+    outm = sb.bve_rollout(ctxm, *f, xm, ADJ_STEPS)
+    lossm = 0.5 * (area * (outm - wstar) ** 2).sum()
+    t1.record(st)
+    lossm.backward()
+    t2.record(st)
+    t2.synchronize()
+    tree["mixed"] = {"forward_ms": t0.elapsed_time(t1), "backward_ms": t1.elapsed_time(t2),
+                     "grad_rel_l2_vs_direct_sum_adjoint": float((xm.grad - grad).norm() / grad.norm()),
+                     "grad_rel_l2_vs_fp64_treecode_adjoint": float((xm.grad - xt.grad).norm() / xt.grad.norm())}
     return {"forward_ms": e0.elapsed_time(e1), "backward_ms": e1.elapsed_time(e2), "steps": ADJ_STEPS,
             "treecode": tree,
             "particles": int(g.x.size), "J": float(loss.detach()), "grad_norm": float(grad.norm()),
@@ -703,6 +719,100 @@ def timed_steps(torch, ctx, f, steps, flush):
     return ts
 
 
+def shard_bench(sb, torch, dev, dist, args, rank, world, local_rank):
+    """The 393,216-particle problem sharded over the ranks (owner-computes over
+    the treecode's leaves, one NCCL all-gather of the stage velocity per RK
+    stage): steps/s of the ONE problem (strong scaling).  Rank 0 checks that
+    the sharded steps are bit-identical to the same steps on one GPU."""
+    g = sb.build_grid(LEVELS, DEGREE, exact_cc=True)
+    vor0 = rh4(g)
+
+    def T(a):
+        return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
+    def fields():
+        return [T(g.x), T(g.y), T(g.z), T(g.area), T(vor0), *[torch.zeros_like(T(g.x)) for _ in range(3)], None]
+
+    def ctx_new():
+        return sb.Context(sb.config_default(levels=LEVELS, interp_degree=DEGREE, fmm_theta=THETA, kernel_eps=EPS,
+                                            omega=OMEGA, dt=DT, precision=sb.MIXED, proxy_degree=PROXY_DEGREE,
+                                            leaf_size=LEAF_SIZE))
+
+    ctx = ctx_new()
+    if world > 1:
+        ctx.shard_over(timeout=120.0)
+    else:
+        ctx.shard(0, 1, sb.shard_unique_id(), timeout=120.0)
+    ctx.set_near_mutual(False)
+    f = fields()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    for _ in range(args.warmup):
+        ctx.bve_run(*f, nsteps=1)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    launches0 = sb.kernel_launches()
+    with ClockSampler(local_rank) as clk:
+        ts = timed_steps(torch, ctx, f, args.steps, flush)
+    launches = sb.kernel_launches() - launches0
+    t_total = job_time(dist, torch, sum(ts), dev)
+    # the same steps on one GPU (rank 0): bit-identical vorticity expected
+    same = None
+    if rank == 0:
+        one = ctx_new()
+        near, cc = ctx.near_tuning(), ctx.cc_tuning()
+        one.set_near_tuning(*near[:3])
+        one.set_near_mutual(False)
+        if ctx.cc_form() == 3:
+            one.set_cc_tuning_bulk(*cc[:2])
+        elif ctx.cc_form():
+            one.set_cc_tuning_direct(cc[0], cc[1], ctx.cc_form())
+        else:
+            one.set_cc_tuning(*cc[:2])
+        fo = fields()
+        for _ in range(args.warmup + args.steps):
+            one.bve_run(*fo, nsteps=1)
+        torch.cuda.synchronize()
+        same = bool(torch.equal(fo[4], f[4]))
+        del one
+    if dist:
+        dist.barrier()
+    # end to end with host buffers (every rank copies the whole problem in and out)
+    host = [torch.from_numpy(np.array(a, dtype=np.float64, copy=True)).pin_memory() for a in (g.x, g.y, g.z, g.area)]
+    vors_h = torch.from_numpy(np.array(vor0, dtype=np.float64, copy=True)).pin_memory()
+    vel_h = [torch.zeros(g.x.shape, dtype=torch.float64).pin_memory() for _ in range(3)]
+    ctx.bve_back_rk4_step_host(*host, vors_h, *vel_h)
+    st = torch.cuda.current_stream()
+    te = []
+    for _ in range(args.steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        ctx.bve_back_rk4_step_host(*host, vors_h, *vel_h)
+        e1.record(st)
+        e1.synchronize()
+        te.append(e0.elapsed_time(e1))
+    e2e_total = job_time(dist, torch, sum(te), dev)
+    first, count = ctx.shard_range()
+    ctx.shard_release()
+    if rank == 0:
+        h2d = (len(host) + 1) * vors_h.numel() * 8
+        line = {
+            "metric": METRIC, "value": args.steps / (t_total * 1e-3), "unit": "steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_total / args.steps,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f32 pairs / f64 positions+remap", "data": "synthetic",
+            "config": dict(workload_config(), parallelism=f"one problem sharded over {world} GPU(s): owner-computes "
+                           "over the treecode's leaves, NCCL all-gather of each stage's velocity"),
+            "e2e": {"value": args.steps / (e2e_total * 1e-3), "unit": "steps/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": 4 * vors_h.numel() * 8},
+            "gpu_launches": launches, "clocks": clk.summary(),
+            "shard": {"rank0_particles": [first, count], "bit_identical_to_one_gpu": same,
+                      "all_gather_bytes_per_step": 4 * 3 * vors_h.numel() * 8 * (world - 1) // max(world, 1)},
+        }
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -730,6 +840,8 @@ def main():
                          "one block per target panel)[,bulk | ,targets per thread of the barrier-free form]")
     ap.add_argument("--near-mutual", action="store_true",
                     help="--profile treecode: the first stage's near field two-sided (sbslpm_set_near_mutual)")
+    ap.add_argument("--shard", action="store_true",
+                    help="one problem sharded over the --gpus ranks (strong scaling) instead of one replica per rank")
     ap.add_argument("--degree", type=int, default=0,
                     help="--profile ensemble: one proxy degree for every member (0: drawn from {6, 8, 10})")
     args = ap.parse_args()
@@ -757,6 +869,11 @@ def main():
     dev = torch.device("cuda", local_rank)
     if args.profile:
         profile_run(sb, torch, dev, args)
+        return
+    if args.shard:
+        shard_bench(sb, torch, dev, dist, args, rank, world, local_rank)
+        if dist:
+            dist.destroy_process_group()
         return
 
     g = sb.build_grid(LEVELS, DEGREE, exact_cc=True)

@@ -210,6 +210,48 @@ int sbslpm_pointer_on_device(const void* p);
 sbslpm_status sbslpm_bve_run(sbslpm_ctx* ctx, const double* xcos, const double* ycos, const double* zcos,
                              const double* area, double* vors, double* vel_x, double* vel_y, double* vel_z,
                              double* tracers, double time, int nsteps);
+/* One velocity evaluation of the step (its first stage, sources on the grid)
+ * into vel_x/y/z ([leaf][q]): the Biot-Savart velocity of vors by the
+ * context's method -- the velocity part of bve_back_rk4_step
+ * (src/bve_time_step.cpp:333-350).  On a sharded context without a
+ * communicator only the rank's own slice (sbslpm_shard_range) is written.
+ * Refused on a forced context (its velocity includes the step's forcing). */
+sbslpm_status sbslpm_bve_velocity(sbslpm_ctx* ctx, const double* xcos, const double* ycos, const double* zcos,
+                                  const double* area, const double* vors, double* vel_x, double* vel_y,
+                                  double* vel_z);
+
+/* ---------------- one problem over several GPUs (treecode) ----------------
+ *
+ * Replaces the reference's MPI split of the velocity work
+ * (src/fmm_interactions/bve_vel.cpp:15-33: each rank takes a slice of the
+ * interaction list; src/bve_time_step.cpp:346-348: MPI_Allreduce of the
+ * velocity).  One process per GPU, each with its own context on the same
+ * problem.  Rank r of nranks owns the particles of a contiguous slice of the
+ * tree leaves (sbslpm_shard_range): it evaluates the near field, the
+ * well-separated pairs that land on its slice and its particles' velocities;
+ * after every RK stage an NCCL all-gather gives every rank the whole
+ * velocity, and the remap runs on every rank.  The result is bit-identical to
+ * the one-GPU step.  The adjoint and shallow-water paths refuse a context of
+ * more than one rank. */
+
+/* A fresh NCCL unique id (128 bytes) for sbslpm_set_shard; rank 0 makes it and
+ * the host sends it to the other ranks (NCCL is loaded at run time:
+ * SBSLPM_ERR_NO_DEVICE when libnccl.so.2 cannot be loaded). */
+sbslpm_status sbslpm_shard_unique_id(unsigned char* id);
+/* Makes the context rank `rank` of `nranks` (nranks must divide the tree's
+ * leaf count; 1 restores the whole problem).  With nccl_id (128 bytes, the
+ * same on every rank) it joins the ranks' communicator -- every rank calls it
+ * together; a rank missing for timeout_s seconds (<= 0: 300) ends it with
+ * SBSLPM_ERR_TIMEOUT.  Without nccl_id a context of more than one rank only
+ * evaluates its own slice (sbslpm_bve_velocity) and refuses whole steps.
+ * Launch shapes are timed again on the next call. */
+sbslpm_status sbslpm_set_shard(sbslpm_ctx* ctx, int rank, int nranks, const unsigned char* nccl_id,
+                               double timeout_s);
+/* The rank's particles: indices [first, first + count) of a [leaf][q] field. */
+sbslpm_status sbslpm_shard_range(const sbslpm_ctx* ctx, long* first, long* count);
+/* Ends the context's communicator (also done by sbslpm_destroy); every rank
+ * calls it together. */
+sbslpm_status sbslpm_shard_release(sbslpm_ctx* ctx);
 
 /* ---------------- pieces of the step (device pointers) ---------------- */
 
@@ -324,9 +366,12 @@ sbslpm_status sbslpm_cubed_sphere_2d_to_1d(long n_leaves, int degree, const doub
  * the adjoint of the input vorticity, vors_bar = (d vors_next / d vors)^T
  * vors_bar_next, through the four velocity evaluations (source positions and
  * strengths), the departure search and the remap.  The forward step is
- * recomputed from the checkpoint inside the call.  Needs a float64 context
- * with direct-sum or treecode (proxy_degree > 0) velocity and no tracers.
- * Locating points in panels is piecewise constant and is not differentiated. */
+ * recomputed from the checkpoint inside the call.  Needs a context with the
+ * float64 direct-sum velocity, or the treecode (proxy_degree > 0) in float64
+ * or mixed precision (the forward recomputed in mixed precision, the
+ * transposed near and well-separated pair sums in float32 on packed
+ * coordinates, the rest float64), and no tracers or forcing.  Locating
+ * points in panels is piecewise constant and is not differentiated. */
 sbslpm_status sbslpm_bve_adjoint_step(sbslpm_ctx* ctx, const double* xcos, const double* ycos, const double* zcos,
                                       const double* area, const double* vors, const double* vors_bar_next,
                                       double* vors_bar);

@@ -184,6 +184,11 @@ def lib() -> ctypes.CDLL:
     L.sbslpm_near_mutual.argtypes = [_VP, _I, _D]
     L.sbslpm_cc_form.argtypes = [_VP, _I]
     L.sbslpm_measure_fma_peak.argtypes = [ctypes.c_int, ctypes.c_double, _D]
+    L.sbslpm_bve_velocity.argtypes = [_VP] * 9
+    L.sbslpm_shard_unique_id.argtypes = [_VP]
+    L.sbslpm_set_shard.argtypes = [_VP, ctypes.c_int, ctypes.c_int, _VP, ctypes.c_double]
+    L.sbslpm_shard_range.argtypes = [_VP, ctypes.POINTER(ctypes.c_long), ctypes.POINTER(ctypes.c_long)]
+    L.sbslpm_shard_release.argtypes = [_VP]
     _lib = L
     return L
 
@@ -197,6 +202,37 @@ def _check(status: int, where: str):
 
 def kernel_launches() -> int:
     return int(lib().sbslpm_kernel_launches())
+
+
+def shard_unique_id() -> bytes:
+    """A fresh NCCL unique id (128 bytes) for Context.shard (sbslpm_shard_unique_id)."""
+    buf = (ctypes.c_ubyte * 128)()
+    _check(lib().sbslpm_shard_unique_id(buf), "sbslpm_shard_unique_id")
+    return bytes(buf)
+
+
+def exchange_shard_id(group=None, make=shard_unique_id) -> bytes:
+    """The id every rank of a torch.distributed group passes to Context.shard:
+    made by the group's first rank (make()) and broadcast to the others -- the
+    host side of the reference's MPI communicator set-up."""
+    import torch.distributed as dist
+
+    first = dist.get_global_rank(group, 0) if group is not None else 0
+    obj = [make() if dist.get_rank(group) == 0 else None]
+    dist.broadcast_object_list(obj, src=first, group=group)
+    ident = obj[0]
+    if not isinstance(ident, bytes) or len(ident) != 128:
+        raise ValueError("a shard id is 128 bytes")
+    return ident
+
+
+def shard_slice(leaf_count: int, q: int, tree_leaves: int, rank: int, nranks: int):
+    """(first, count) of rank's particles in a [leaf][q] field when tree_leaves
+    tree leaves are split into nranks equal contiguous slices (sbslpm_shard_range)."""
+    if nranks < 1 or not 0 <= rank < nranks or tree_leaves % nranks:
+        raise ValueError("nranks must divide the tree's leaves and 0 <= rank < nranks")
+    count = leaf_count * q // nranks
+    return rank * count, count
 
 
 # ---------------------------------------------------------------- config ----
@@ -504,6 +540,47 @@ class Context:
             (xcos, "xcos"), (ycos, "ycos"), (zcos, "zcos"), (area, "area"), (vors, "vors"), (vel_x, "vel_x"),
             (vel_y, "vel_y"), (vel_z, "vel_z"))], _dev(tracers, "tracers"), float(time), int(nsteps)),
             "sbslpm_bve_run")
+
+    def bve_velocity(self, xcos, ycos, zcos, area, vors, vel_x, vel_y, vel_z):
+        """The step's first-stage velocity of vors into vel_* (sbslpm_bve_velocity); a
+        sharded context without a communicator writes only its own slice."""
+        lq = (self.leaf_count, self.q)
+        self._sync_stream()
+        _check(lib().sbslpm_bve_velocity(self._h, *[_dev(t, n, lq) for t, n in (
+            (xcos, "xcos"), (ycos, "ycos"), (zcos, "zcos"), (area, "area"), (vors, "vors"), (vel_x, "vel_x"),
+            (vel_y, "vel_y"), (vel_z, "vel_z"))]), "sbslpm_bve_velocity")
+
+    # -- one problem over several GPUs -----------------------------------
+    def shard(self, rank: int, nranks: int, nccl_id: bytes = None, timeout: float = 300.0):
+        """Make this context rank `rank` of `nranks` of one sharded treecode problem
+        (sbslpm_set_shard).  With nccl_id (exchange_shard_id) every rank joins the
+        communicator together and whole steps all-gather each stage's velocity;
+        without it the context evaluates only its own slice (bve_velocity)."""
+        ident = None
+        if nccl_id is not None:
+            if len(nccl_id) != 128:
+                raise ValueError("a shard id is 128 bytes")
+            ident = (ctypes.c_ubyte * 128).from_buffer_copy(nccl_id)
+        self._sync_stream()
+        _check(lib().sbslpm_set_shard(self._h, int(rank), int(nranks), ident, float(timeout)), "sbslpm_set_shard")
+
+    def shard_over(self, group=None, timeout: float = 300.0):
+        """Shard over the ranks of a torch.distributed group (one GPU per rank)."""
+        import torch.distributed as dist
+
+        nranks = dist.get_world_size(group)
+        ident = exchange_shard_id(group) if nranks > 1 else None
+        self.shard(dist.get_rank(group), nranks, ident, timeout)
+
+    def shard_range(self):
+        """(first, count): this rank's particles in a [leaf][q] field."""
+        first, count = ctypes.c_long(), ctypes.c_long()
+        _check(lib().sbslpm_shard_range(self._h, ctypes.byref(first), ctypes.byref(count)), "sbslpm_shard_range")
+        return first.value, count.value
+
+    def shard_release(self):
+        """End the context's communicator (every rank together)."""
+        _check(lib().sbslpm_shard_release(self._h), "sbslpm_shard_release")
 
     # -- shallow water (SWE v2) ------------------------------------------
     def swe_back_rk4_step_2(self, xcos, ycos, zcos, area, vors, divs, height, vel_x, vel_y, vel_z, tracers,
@@ -887,7 +964,8 @@ def direct_sum_bve_autograd(tx, ty, tz, sx, sy, sz, strength, eps):
 
 def bve_rollout(context, xcos, ycos, zcos, area, vors0, nsteps):
     """nsteps BVE steps as a differentiable torch function of the initial
-    vorticity (float64 direct-sum context), adjoint with per-step checkpoints."""
+    vorticity (a float64 direct-sum context, or a treecode context in float64
+    or mixed precision), adjoint with per-step checkpoints."""
     return _autograd()[1].apply(vors0, context, xcos, ycos, zcos, area, int(nsteps))
 
 

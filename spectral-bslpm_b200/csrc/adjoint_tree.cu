@@ -197,6 +197,162 @@ __global__ void __launch_bounds__(512) k_tree_near_T(TreeGeom tg, const int* __r
   }
 }
 
+// Mixed precision (float32 pairs on packed coordinates, as the forward
+// kernels): d' = (y - x) kPackScale = a - x', a = y' + (c_S - c_T) kPackScale
+// with y', x' relative to the source and target panels' centres, so
+// |d'|^2 + eps = |d|^2/2 + eps and, with g = 1/(|d'|^2 + eps),
+//   qbar = K sqrt2 sum g (c.d'),   ybar = K q sum [g c - 2 g^2 (c.d') d'].
+// One source against two targets per instruction (paired FP32): A = (-x0, -x1,
+// -y0, -y1), B = (-z0, -z1, cx0, cx1), C = (cy0, cy1, cz0, cz1) of the two
+// targets; u = g (c.d') feeds q, g c feeds bc and u g d' feeds bd.
+template <bool GUARD>
+__device__ __forceinline__ void adj_pair32x2(const float2 ax, const float2 ay, const float2 az, const float4 A,
+                                             const float4 B, const float4 C, const float2 eps2, float2& q,
+                                             float2& bcx, float2& bcy, float2& bcz, float2& bdx, float2& bdy,
+                                             float2& bdz) {
+  const float2 dx = __fadd2_rn(ax, make_float2(A.x, A.y)), dy = __fadd2_rn(ay, make_float2(A.z, A.w)),
+               dz = __fadd2_rn(az, make_float2(B.x, B.y));
+  const float2 den = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, eps2)));
+  float2 g = make_float2(recip_f32(den.x), recip_f32(den.y));
+  if (GUARD) {
+    g.x = den.x > 0.0f ? g.x : 0.0f;
+    g.y = den.y > 0.0f ? g.y : 0.0f;
+  }
+  const float2 cx = make_float2(B.z, B.w), cy = make_float2(C.x, C.y), cz = make_float2(C.z, C.w);
+  const float2 cd = __ffma2_rn(cx, dx, __ffma2_rn(cy, dy, __fmul2_rn(cz, dz)));
+  const float2 u = __fmul2_rn(g, cd);
+  q = __fadd2_rn(q, u);
+  const float2 ug = __fmul2_rn(u, g);
+  bcx = __ffma2_rn(g, cx, bcx);
+  bcy = __ffma2_rn(g, cy, bcy);
+  bcz = __ffma2_rn(g, cz, bcz);
+  bdx = __ffma2_rn(ug, dx, bdx);
+  bdy = __ffma2_rn(ug, dy, bdy);
+  bdz = __ffma2_rn(ug, dz, bdz);
+}
+
+// Stages target k of a tile as half of a pair slot (see adj_pair32x2): its
+// packed position relative to the target panel's centre ct, negated, and
+// c = w x x (w: the adjoint three-vector at the target, x: its position).
+__device__ __forceinline__ void adj_stage(float4* tile, int k, double x, double y, double z, double wa, double wb,
+                                          double wc, const double* ct) {
+  float* A = reinterpret_cast<float*>(tile + 3 * (k >> 1));
+  const int h = k & 1;
+  A[h] = (float)((ct[0] - x) * kPackScale);
+  A[2 + h] = (float)((ct[1] - y) * kPackScale);
+  A[4 + h] = (float)((ct[2] - z) * kPackScale);
+  A[6 + h] = (float)(wb * z - wc * y);
+  A[8 + h] = (float)(wc * x - wa * z);
+  A[10 + h] = (float)(wa * y - wb * x);
+}
+
+// The zero partner of an odd target count: c = 0 contributes nothing.
+__device__ __forceinline__ void adj_stage_zero(float4* tile, int k) {
+  float* A = reinterpret_cast<float*>(tile + 3 * (k >> 1));
+  const int h = k & 1;
+  for (int m = 0; m < 6; m++) A[2 * m + h] = 0.0f;
+}
+
+// Mixed-precision transposed near field: source leaf sl (blockIdx.x), one
+// thread per source particle; per target leaf of the transposed list the
+// float32 sums are added into float64.
+template <bool GUARD>
+__global__ void __launch_bounds__(512) k_tree_near_T32(TreeGeom tg, StepGeom fg, const int* __restrict__ tstart,
+                                                     const int* __restrict__ ttgt, const double* __restrict__ x,
+                                                     const double* __restrict__ y, const double* __restrict__ z,
+                                                     const double* __restrict__ vbar,
+                                                     const double4* __restrict__ psrc, double* __restrict__ qbar,
+                                                     double* __restrict__ ybar) {
+  extern __shared__ float4 tile32[];  // [(npl+1)/2][3]
+  const int sl = blockIdx.x, npl = tg.npl, np2 = (npl + 1) >> 1;
+  const long N = tg.N;
+  const int j = threadIdx.x;
+  const long oj = (long)sl * npl + (j < npl ? j : 0);
+  const double4 s = psrc[oj];
+  const double* cs = fg.pd_centre + 4 * (long)(fg.offset + sl);
+  const float sx = (float)((s.x - cs[0]) * kPackScale), sy = (float)((s.y - cs[1]) * kPackScale),
+              sz = (float)((s.z - cs[2]) * kPackScale);
+  const float feps = (float)tg.eps;
+  const float2 eps2 = make_float2(feps, feps);
+  double qb = 0, bx = 0, by = 0, bz = 0;
+  for (int e = tstart[sl]; e < tstart[sl + 1]; e++) {
+    const int tl = ttgt[e];
+    const long tb = (long)tl * npl;
+    const double* ct = fg.pd_centre + 4 * (long)(fg.offset + tl);
+    __syncthreads();
+    for (int i = threadIdx.x; i < 2 * np2; i += blockDim.x) {
+      if (i < npl)
+        adj_stage(tile32, i, x[tb + i], y[tb + i], z[tb + i], vbar[tb + i], vbar[N + tb + i], vbar[2 * N + tb + i],
+                  ct);
+      else
+        adj_stage_zero(tile32, i);
+    }
+    __syncthreads();
+    const float a0 = sx + (float)((cs[0] - ct[0]) * kPackScale), a1 = sy + (float)((cs[1] - ct[1]) * kPackScale),
+                a2 = sz + (float)((cs[2] - ct[2]) * kPackScale);
+    const float2 ax = make_float2(a0, a0), ay = make_float2(a1, a1), az = make_float2(a2, a2);
+    float2 q = make_float2(0.f, 0.f), cx = q, cy = q, cz = q, dx = q, dy = q, dz = q;
+#pragma unroll 4
+    for (int k2 = 0; k2 < np2; k2++)
+      adj_pair32x2<GUARD>(ax, ay, az, tile32[3 * k2], tile32[3 * k2 + 1], tile32[3 * k2 + 2], eps2, q, cx, cy, cz,
+                          dx, dy, dz);
+    qb += (double)q.x + (double)q.y;
+    bx += ((double)cx.x + (double)cx.y) - 2.0 * ((double)dx.x + (double)dx.y);
+    by += ((double)cy.x + (double)cy.y) - 2.0 * ((double)dy.x + (double)dy.y);
+    bz += ((double)cz.x + (double)cz.y) - 2.0 * ((double)dz.x + (double)dz.y);
+  }
+  if (j < npl) {
+    qbar[oj] = kBiotSavart / kPackScale * qb;
+    ybar[oj] = kBiotSavart * s.w * bx;
+    ybar[N + oj] = kBiotSavart * s.w * by;
+    ybar[2 * N + oj] = kBiotSavart * s.w * bz;
+  }
+}
+
+// Mixed-precision transposed well-separated interactions: source panel s
+// (blockIdx.x), one thread per source proxy, target panels' proxies and
+// c = Tbar x x staged as pairs.
+template <bool GUARD>
+__global__ void __launch_bounds__(kT) k_tree_cc_T32(StepGeom fg, const int* __restrict__ tstart,
+                                                   const int* __restrict__ ttgt, const double* __restrict__ tbar,
+                                                   double* __restrict__ qbar) {
+  __shared__ float4 tile[3 * ((kT + 1) / 2)];
+  const int s = blockIdx.x, q = fg.q, q2 = (q + 1) >> 1;
+  const long pn = (long)fg.panels * q;
+  const int k = threadIdx.x;
+  const long ok = (long)s * q + (k < q ? k : 0);
+  const double* cs = fg.pd_centre + 4 * (long)s;
+  const float sx = (float)((fg.px[ok] - cs[0]) * kPackScale), sy = (float)((fg.px[pn + ok] - cs[1]) * kPackScale),
+              sz = (float)((fg.px[2 * pn + ok] - cs[2]) * kPackScale);
+  const float feps = (float)fg.eps;
+  const float2 eps2 = make_float2(feps, feps);
+  double acc = 0;
+  for (int e = tstart[s]; e < tstart[s + 1]; e++) {
+    const int t = ttgt[e];
+    const long tb = (long)t * q;
+    const double* ct = fg.pd_centre + 4 * (long)t;
+    __syncthreads();
+    for (int i = threadIdx.x; i < 2 * q2; i += blockDim.x) {
+      if (i < q)
+        adj_stage(tile, i, fg.px[tb + i], fg.px[pn + tb + i], fg.px[2 * pn + tb + i], tbar[tb + i], tbar[pn + tb + i],
+                  tbar[2 * pn + tb + i], ct);
+      else
+        adj_stage_zero(tile, i);
+    }
+    __syncthreads();
+    const float a0 = sx + (float)((cs[0] - ct[0]) * kPackScale), a1 = sy + (float)((cs[1] - ct[1]) * kPackScale),
+                a2 = sz + (float)((cs[2] - ct[2]) * kPackScale);
+    const float2 ax = make_float2(a0, a0), ay = make_float2(a1, a1), az = make_float2(a2, a2);
+    float2 qq = make_float2(0.f, 0.f), cx = qq, cy = qq, cz = qq, dx = qq, dy = qq, dz = qq;
+#pragma unroll 4
+    for (int k2 = 0; k2 < q2; k2++)
+      adj_pair32x2<GUARD>(ax, ay, az, tile[3 * k2], tile[3 * k2 + 1], tile[3 * k2 + 2], eps2, qq, cx, cy, cz, dx, dy,
+                          dz);
+    acc += (double)qq.x + (double)qq.y;
+  }
+  if (k < q) qbar[(long)s * q + k] = kBiotSavart / kPackScale * acc;
+}
+
 // 1-D barycentric basis on the leaf's Chebyshev proxies and its derivative,
 // without a range check (displaced particles may leave their leaf).
 __device__ __forceinline__ void bli_free_deriv(double t, double lo, double hi, int n, const BliTable& tab, double* f,
@@ -288,7 +444,7 @@ __global__ void k_tree_sources_T(TreeGeom tg, StepGeom fg, BliTable tab, const d
 void launch_tree_velocity_adjoint(const TreeGeom& tg, const StepGeom& fg, const BliTable& ftab,
                                   const TreeAdjointLists& tl, const double* x, const double* y, const double* z,
                                   const double* vbar, const double4* psrc, double* tbar, double* qbl, double* qbar,
-                                  double* ybar, cudaStream_t st) {
+                                  double* ybar, bool mixed, cudaStream_t st) {
   const int qx = fg.q, Pf = fg.panels;
   const long pn = (long)Pf * qx;
   // leaf interpolation, transposed; non-leaf rows start at zero
@@ -300,10 +456,14 @@ void launch_tree_velocity_adjoint(const TreeGeom& tg, const StepGeom& fg, const 
     SB_LAUNCH(k_tree_up3, blocks_for(work, 256), 256, 0, st, fg, lev, tbar);
   }
   // well-separated interactions, transposed
-  if (fg.eps > 0)
+  if (mixed) {
+    if (fg.eps > 0) SB_LAUNCH(k_tree_cc_T32<false>, (unsigned)Pf, kT, 0, st, fg, tl.cc_tstart, tl.cc_ttgt, tbar, qbl);
+    else SB_LAUNCH(k_tree_cc_T32<true>, (unsigned)Pf, kT, 0, st, fg, tl.cc_tstart, tl.cc_ttgt, tbar, qbl);
+  } else if (fg.eps > 0) {
     SB_LAUNCH(k_tree_cc_T<false>, (unsigned)Pf, kT, 0, st, fg, tl.cc_tstart, tl.cc_ttgt, tbar, qbl);
-  else
+  } else {
     SB_LAUNCH(k_tree_cc_T<true>, (unsigned)Pf, kT, 0, st, fg, tl.cc_tstart, tl.cc_ttgt, tbar, qbl);
+  }
   // upward pass, transposed: interpolate down the tree
   for (int lev = 0; lev < fg.levels - 1; lev++) {
     const long work = (6L << (2 * (lev + 1))) * qx;
@@ -318,7 +478,15 @@ void launch_tree_velocity_adjoint(const TreeGeom& tg, const StepGeom& fg, const 
     attr = true;
   }
   const int nth = tg.npl <= 256 ? 256 : 512;
-  if (tg.eps > 0)
+  if (mixed) {
+    const size_t sm32 = sizeof(float4) * 3 * ((tg.npl + 1) / 2);
+    if (tg.eps > 0)
+      SB_LAUNCH(k_tree_near_T32<false>, (unsigned)fg.leaves, nth, sm32, st, tg, fg, tl.near_tstart, tl.near_ttgt, x, y,
+                z, vbar, psrc, qbar, ybar);
+    else
+      SB_LAUNCH(k_tree_near_T32<true>, (unsigned)fg.leaves, nth, sm32, st, tg, fg, tl.near_tstart, tl.near_ttgt, x, y,
+                z, vbar, psrc, qbar, ybar);
+  } else if (tg.eps > 0)
     SB_LAUNCH(k_tree_near_T<false>, (unsigned)fg.leaves, nth, sm, st, tg, tl.near_tstart, tl.near_ttgt, x, y, z, vbar,
               psrc, qbar, ybar);
   else

@@ -20,10 +20,12 @@ struct TreeAdjointLists {
 // Given vbar [3][N] (adjoint of one stage velocity) and that stage's particle
 // sources psrc (positions, strengths), writes qbar [N] and ybar [3][N], the
 // adjoints of the particle source strengths and positions.  Scratch: tbar
-// [3][tree panels * q], qbl [tree panels * q].
+// [3][tree panels * q], qbl [tree panels * q].  mixed: the transposed near
+// and well-separated pair sums in float32 on packed coordinates (the
+// forward's mixed arithmetic), everything else float64.
 void launch_tree_velocity_adjoint(const TreeGeom& tg, const StepGeom& fg, const BliTable& ftab,
                                   const TreeAdjointLists& tl, const double* x, const double* y, const double* z,
                                   const double* vbar, const double4* psrc, double* tbar, double* qbl, double* qbar,
-                                  double* ybar, cudaStream_t st);
+                                  double* ybar, bool mixed, cudaStream_t st);
 
 }  // namespace sbslpm

@@ -228,7 +228,7 @@ __global__ void __launch_bounds__(NT)
                         const double4* __restrict__ psrc, double* __restrict__ out) {
   const TreeGeom tg = mem[blockIdx.z].tg;
   const long mo = blockIdx.z;
-  bltc_near64_body<NT, TPT, GUARD>(tg, blockIdx.x, blockIdx.y, gridDim.y, x, y, z, psrc + mo * tg.N,
+  bltc_near64_body<NT, TPT, GUARD>(tg, tg.leaf0 + blockIdx.x, blockIdx.y, gridDim.y, x, y, z, psrc + mo * tg.N,
                                    out + mo * gridDim.y * 3 * tg.N);
 }
 
@@ -328,7 +328,7 @@ __global__ void __launch_bounds__(NT, NT >= 256 ? 4 : 1)
   const TreeGeom tg = mem[blockIdx.z].tg;
   const StepGeom fg = mem[blockIdx.z].fg;
   const long mo = blockIdx.z;
-  bltc_near32_body<NT, TPT, GUARD>(tg, fg, blockIdx.x, blockIdx.y, gridDim.y, x, y, z, psrcf + mo * tg.N,
+  bltc_near32_body<NT, TPT, GUARD>(tg, fg, tg.leaf0 + blockIdx.x, blockIdx.y, gridDim.y, x, y, z, psrcf + mo * tg.N,
                                    out + mo * gridDim.y * 3 * tg.N);
 }
 
@@ -635,7 +635,7 @@ __device__ __forceinline__ void bltc_to_particles_body(const TreeGeom& tg, const
 __global__ void __launch_bounds__(kThreads)
     k_bltc_to_particles(TreeGeom tg, StepGeom fg, const double* __restrict__ tgt, const double* __restrict__ near,
                         int splits, double* __restrict__ v) {
-  bltc_to_particles_body(tg, fg, blockIdx.x, tgt, near, splits, v);
+  bltc_to_particles_body(tg, fg, tg.leaf0 + blockIdx.x, tgt, near, splits, v);
 }
 
 __global__ void __launch_bounds__(kThreads)
@@ -745,8 +745,8 @@ void launch_bltc_to_particles_batch(const BatchMember* mem, int members, int lea
 void launch_bltc_to_particles(const TreeGeom& tg, const StepGeom& fg, const double* tgt, const double* near,
                               int splits, double* v, cudaStream_t st) {
   int qx = (tg.n + 1) * (tg.n + 1);
-  SB_LAUNCH(k_bltc_to_particles, (unsigned)fg.leaves, kThreads, sizeof(double) * 3 * qx, st, tg, fg, tgt, near, splits,
-            v);
+  SB_LAUNCH(k_bltc_to_particles, (unsigned)(tg.owned > 0 ? tg.owned : fg.leaves), kThreads, sizeof(double) * 3 * qx,
+            st, tg, fg, tgt, near, splits, v);
 }
 
 }  // namespace sbslpm

@@ -55,6 +55,10 @@ struct TreeGeom {
   const int* fface;       // [tree panels]
   const int* near_start;  // [tree leaves + 1]: CSR of near leaf pairs by target leaf
   const int* near_src;    // source leaf (relative to the first leaf)
+  // owner-computes slice of the target leaves (a sharded problem): the near
+  // field and the particle velocities are evaluated for leaves
+  // [leaf0, leaf0 + owned) only; owned 0 = every leaf
+  int leaf0 = 0, owned = 0;
 };
 
 // One member of a batched ensemble (treecode velocity, shared particle grid):

@@ -187,11 +187,13 @@ sbslpm_status precompute_tree(sbslpm_ctx* c) {
   c->n_near = l.ns.back();
   c->n_cc = l.cs.back();
   c->list = l.list;
+  c->h_ns = l.ns;
+  c->h_cs = l.cs;
+  c->h_csrc = l.csrc;
+  c->h_fcentre = t.centre;
   SB_TRY(upload(&c->near_start, l.ns));
   SB_TRY(upload(&c->near_src, l.nsrc));
-  SB_TRY(upload(&c->cc_start, l.cs));
-  SB_TRY(upload(&c->cc_src, l.csrc));
-  if (c->cfg.precision == SBSLPM_MIXED && t.qx <= 32) SB_TRY(upload(&c->fentry32, entry_table(l.cs, l.csrc, t.centre)));
+  SB_TRY(install_cc_lists(c, l.cs, l.csrc));
   if (c->cfg.precision == SBSLPM_MIXED && t.npl == kMutualLeaf && c->n_near > 0) {
     std::vector<int4> units;
     build_mutual_units(l.ns, l.nsrc, units);
@@ -200,14 +202,6 @@ sbslpm_status precompute_tree(sbslpm_ctx* c) {
     SB_TRY(dalloc(&c->near_slot, (size_t)c->n_near * 3 * kMutualLeaf));
   }
   if (c->n_cc > 0 && cc_chunk_supported(t.qx)) {
-    for (int k = 0; k < 4; k++) {
-      std::vector<int4> chunks;
-      std::vector<int> cstart;
-      build_cc_chunks(l.cs, k + 1, chunks, cstart);
-      c->cc_nchunks[k] = (int)chunks.size();
-      SB_TRY(upload(&c->cc_chunks[k], chunks));
-      SB_TRY(upload(&c->cc_cstart[k], cstart));
-    }
     SB_TRY(dalloc(&c->cc_partial, (size_t)c->n_cc * 3 * t.qx));
   } else {
     c->cc_tuned = true;  // k_interact_wide / k_interact32 over whole target panels
@@ -315,6 +309,42 @@ void fill_geom(sbslpm_ctx* c) {
 
 namespace sbslpm {
 
+// Uploads a well-separated CSR of the treecode (by target tree panel) and what
+// is derived from it: the entry table (mixed precision, q <= 32) and the lists
+// of chunks of 1..4 entries; the arrays of an earlier list are released.
+sbslpm_status install_cc_lists(sbslpm_ctx* c, const std::vector<int>& cs, const std::vector<int>& csrc) {
+  auto drop = [](auto*& p) {
+    if (p) cudaFree(p);
+    p = nullptr;
+  };
+  drop(c->cc_start);
+  drop(c->cc_src);
+  drop(c->fentry32);
+  for (int k = 0; k < 4; k++) {
+    drop(c->cc_chunks[k]);
+    drop(c->cc_cstart[k]);
+    c->cc_nchunks[k] = 0;
+  }
+  SB_TRY(upload(&c->cc_start, cs));
+  SB_TRY(upload(&c->cc_src, csrc));
+  if (c->cfg.precision == SBSLPM_MIXED && c->qx <= 32)
+    SB_TRY(upload(&c->fentry32, entry_table(cs, csrc, c->h_fcentre)));
+  if (c->n_cc > 0 && cc_chunk_supported(c->qx)) {
+    for (int k = 0; k < 4; k++) {
+      std::vector<int4> chunks;
+      std::vector<int> cstart;
+      build_cc_chunks(cs, k + 1, chunks, cstart);
+      c->cc_nchunks[k] = (int)chunks.size();
+      SB_TRY(upload(&c->cc_chunks[k], chunks));
+      SB_TRY(upload(&c->cc_cstart[k], cstart));
+    }
+  }
+  c->fgeom.tgt_start = c->cc_start;
+  c->fgeom.src_panel = c->cc_src;
+  c->fgeom.entry = c->fentry32;
+  return SBSLPM_OK;
+}
+
 void launch_tree_cc(sbslpm_ctx* c, cudaStream_t st) {
   if (c->cc_partial && c->cc_slots > 0) {
     const int k = c->cc_len - 1;
@@ -359,7 +389,7 @@ void velocity_eval(sbslpm_ctx* c, int stage, double dt_s, const double* vprev, c
                               st);
       splits = 1;
     } else {
-      launch_bltc_near_batch(c->self, 1, fg.leaves, c->npl, c->cfg.kernel_eps, c->cfg.precision, x, y, z, c->psrc,
+      launch_bltc_near_batch(c->self, 1, owned_leaves(c), c->npl, c->cfg.kernel_eps, c->cfg.precision, x, y, z, c->psrc,
                              c->psrcf, c->near, c->near_splits, c->near_nt, c->near_tpt, st);
     }
     if (c->aux_stream) cudaStreamWaitEvent(st, c->ev_join, 0);
@@ -390,6 +420,7 @@ void enqueue_step(sbslpm_ctx* c, const double* x, const double* y, const double*
   if (c->force) launch_ssw_forcing(c->A, c->q, c->cfg.forcing, c->cfg.omega, c->d_time, x, y, z, c->force, st);
   for (int s = 0; s < 4; s++) {
     velocity_eval(c, s, stage_dt[s], s ? v[s - 1] : nullptr, x, y, z, area, vors, v[s]);
+    shard_exchange(c, v[s]);  // every rank's slice into every rank's copy (sharded contexts)
     if (s == 0 && stage0) cudaEventRecord(stage0, st);
   }
   if (c->force) launch_time_advance(c->d_time, dt, st);
@@ -413,6 +444,11 @@ sbslpm_status finish(sbslpm_ctx* c) {
   SB_CUDA(cudaMemcpyAsync(c->h_err, c->err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
   SB_CUDA(cudaStreamSynchronize(st));
   unsigned e = *c->h_err;
+  if (c->shard_status != SBSLPM_OK) {
+    const sbslpm_status s = c->shard_status;
+    c->shard_status = SBSLPM_OK;
+    return set_last_error(c->shard_error), s;
+  }
   if (e) {
     SB_CUDA(cudaMemsetAsync(c->err, 0, sizeof(unsigned), st));
     SB_CUDA(cudaStreamSynchronize(st));
@@ -532,7 +568,7 @@ sbslpm_status near_autotune(sbslpm_ctx* c, const double* x, const double* y, con
     if (sh[0] * sh[1] < c->npl || sh[0] * sh[1] >= 4 * c->npl) continue;
     for (int sp = 1; sp <= 4; sp++) {
       auto run = [&] {
-        launch_bltc_near_batch(c->self, 1, c->fgeom.leaves, c->npl, c->cfg.kernel_eps, prec, x, y, z, c->psrc,
+        launch_bltc_near_batch(c->self, 1, owned_leaves(c), c->npl, c->cfg.kernel_eps, prec, x, y, z, c->psrc,
                                c->psrcf, c->near, sp, sh[0], sh[1], st);
       };
       run();
@@ -554,7 +590,7 @@ sbslpm_status near_autotune(sbslpm_ctx* c, const double* x, const double* y, con
   // the first stage's two-sided kernel, where it applies: kept for stage 0
   // if it beats the chosen shape on these (stage-0) sources
   c->near_mutual = false;
-  if (c->n_mutual > 0) {
+  if (c->n_mutual > 0 && c->shard_n == 1) {  // a unit writes both of its leaves: unsharded contexts only
     auto run = [&] {
       launch_bltc_near_mutual(c->tgeom, c->fgeom, c->mutual_units, c->n_mutual, c->psrcf, c->near_slot, x, y, z,
                               c->near, st);
@@ -770,6 +806,10 @@ sbslpm_status sbslpm_create(const sbslpm_config* cfg, sbslpm_ctx** out) {
 
 sbslpm_status sbslpm_destroy(sbslpm_ctx* c) {
   if (!c) return SBSLPM_OK;
+  if (c->nccl_comm) {
+    cudaStreamSynchronize(c->stream());
+    shard_release(c);
+  }
   if (c->graph) cudaGraphExecDestroy(c->graph);
   if (c->swe_graph) cudaGraphExecDestroy(c->swe_graph);
   void* bufs[] = {c->px, c->il_basis, c->child_mat, c->centre, c->tgt_start, c->src_panel, c->il_row, c->src,
@@ -837,6 +877,7 @@ sbslpm_status sbslpm_bve_step(sbslpm_ctx* c, const double* x, const double* y, c
     return SBSLPM_ERR_ARG;
   if (any_on_host({x, y, z, area, vors, vel_x, vel_y, vel_z, tracers}))
     return set_last_error("device-pointer step given host memory (sbslpm_bve_step_host takes host arrays)"), SBSLPM_ERR_ARG;
+  SB_TRY(shard_allows(c, true, "a step"));
   SB_TRY(near_autotune(c, x, y, z, area, vors));
   if (c->force) SB_CUDA(cudaMemcpyAsync(c->d_time, &time, sizeof(double), cudaMemcpyHostToDevice, c->stream()));
   enqueue_step(c, x, y, z, area, vors, vel_x, vel_y, vel_z, tracers);
@@ -849,6 +890,7 @@ sbslpm_status sbslpm_bve_step_host(sbslpm_ctx* c, const double* x, const double*
   if (!c || bad(x) || bad(y) || bad(z) || bad(area) || bad(vors) || bad(vel_x) || bad(vel_y) || bad(vel_z) ||
       (c->cfg.tracer_count > 0 && bad(tracers)) || !std::isfinite(time))
     return SBSLPM_ERR_ARG;
+  SB_TRY(shard_allows(c, true, "a step"));
   const int T = c->cfg.tracer_count;
   const size_t ln = (size_t)c->A * c->q, bytes = sizeof(double) * ln;
   if (!c->hio) {
@@ -897,11 +939,17 @@ sbslpm_status sbslpm_bve_run(sbslpm_ctx* c, const double* x, const double* y, co
     return SBSLPM_ERR_ARG;
   if (any_on_host({x, y, z, area, vors, vel_x, vel_y, vel_z, tracers}))
     return set_last_error("device-pointer step given host memory (sbslpm_bve_step_host takes host arrays)"), SBSLPM_ERR_ARG;
+  SB_TRY(shard_allows(c, true, "a step"));
   SB_TRY(near_autotune(c, x, y, z, area, vors));
   GraphKey key{{x, y, z, area, vors, vel_x, vel_y, vel_z, tracers}};
   cudaStream_t st = c->stream();
   // step n of the replays runs at time + n dt (each step advances the device time)
   if (c->force) SB_CUDA(cudaMemcpyAsync(c->d_time, &time, sizeof(double), cudaMemcpyHostToDevice, st));
+  if (c->nccl_comm) {  // a sharded run enqueues its steps (and their all-gathers) one by one, uncaptured
+    for (int s = 0; s < nsteps && c->shard_status == SBSLPM_OK; s++)
+      enqueue_step(c, x, y, z, area, vors, vel_x, vel_y, vel_z, tracers);
+    return finish(c);
+  }
   if (!c->graph || !(key == c->graph_key)) {
     SB_TRY(capture_graph(c, &c->graph, [&] { enqueue_step(c, x, y, z, area, vors, vel_x, vel_y, vel_z, tracers); }));
     c->graph_key = key;
@@ -910,6 +958,29 @@ sbslpm_status sbslpm_bve_run(sbslpm_ctx* c, const double* x, const double* y, co
     SB_CUDA(cudaGraphLaunch(c->graph, st));
     launch_counter() += c->launches_per_step;
   }
+  return finish(c);
+}
+
+sbslpm_status sbslpm_bve_velocity(sbslpm_ctx* c, const double* x, const double* y, const double* z,
+                                  const double* area, const double* vors, double* vel_x, double* vel_y,
+                                  double* vel_z) {
+  if (!c || bad(x) || bad(y) || bad(z) || bad(area) || bad(vors) || bad(vel_x) || bad(vel_y) || bad(vel_z))
+    return SBSLPM_ERR_ARG;
+  if (any_on_host({x, y, z, area, vors, vel_x, vel_y, vel_z}))
+    return set_last_error("device pointers expected"), SBSLPM_ERR_ARG;
+  if (c->force)
+    return set_last_error("a forced context's velocity includes the step's forcing: use the step"), SBSLPM_ERR_CONFIG;
+  SB_TRY(near_autotune(c, x, y, z, area, vors));
+  cudaStream_t st = c->stream();
+  velocity_eval(c, 0, 0.0, nullptr, x, y, z, area, vors, c->vbuf);
+  shard_exchange(c, c->vbuf);
+  long first = 0, count = (long)c->A * c->q;
+  if (!c->nccl_comm) sbslpm_shard_range(c, &first, &count);  // a rank without exchange: its own slice
+  const size_t ln = (size_t)c->A * c->q;
+  double* out[3] = {vel_x, vel_y, vel_z};
+  for (int k = 0; k < 3; k++)
+    SB_CUDA(cudaMemcpyAsync(out[k] + first, c->vbuf + k * ln + first, sizeof(double) * count, cudaMemcpyDeviceToDevice,
+                            st));
   return finish(c);
 }
 
@@ -1056,7 +1127,7 @@ sbslpm_status sbslpm_time_interactions(sbslpm_ctx* c, int reps, double* ms_per_l
     SB_CUDA(cudaEventCreate(&b));
     SB_CUDA(cudaEventRecord(a, st));
     for (int r = 0; r < reps; r++)
-      launch_bltc_near_batch(c->self, 1, c->fgeom.leaves, c->npl, c->cfg.kernel_eps, c->cfg.precision, c->gx,
+      launch_bltc_near_batch(c->self, 1, owned_leaves(c), c->npl, c->cfg.kernel_eps, c->cfg.precision, c->gx,
                              c->gx + c->tgeom.N, c->gx + 2 * c->tgeom.N, c->psrc, c->psrcf, c->near, c->near_splits,
                              c->near_nt, c->near_tpt, st);
     SB_CUDA(cudaEventRecord(b, st));
@@ -1066,7 +1137,9 @@ sbslpm_status sbslpm_time_interactions(sbslpm_ctx* c, int reps, double* ms_per_l
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     *ms_per_launch = tms / reps;
-    if (pairs) *pairs = (double)c->n_near * c->npl * c->npl;
+    const long owned_near = c->tgeom.owned > 0 ? c->h_ns[c->tgeom.leaf0 + c->tgeom.owned] - c->h_ns[c->tgeom.leaf0]
+                                                : c->n_near;
+    if (pairs) *pairs = (double)owned_near * c->npl * c->npl;
     return finish(c);
   }
   if (c->cfg.precision == SBSLPM_MIXED) launch_pack_mixed(c->geom, c->src, st);
@@ -1173,6 +1246,9 @@ sbslpm_status sbslpm_set_near_mutual(sbslpm_ctx* c, int on) {
   if (!c || !c->tree) return SBSLPM_ERR_ARG;
   if (on && c->n_mutual == 0)
     return set_last_error("the two-sided near-field kernel needs mixed precision and 256-particle leaves"),
+           SBSLPM_ERR_CONFIG;
+  if (on && c->shard_n > 1)
+    return set_last_error("the two-sided near-field kernel writes both leaves of a pair: one rank only"),
            SBSLPM_ERR_CONFIG;
   c->near_mutual = on != 0;
   if (c->graph) {

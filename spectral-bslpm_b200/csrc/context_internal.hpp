@@ -132,6 +132,18 @@ struct sbslpm_ctx {
   int *adj_near_ts = nullptr, *adj_near_tt = nullptr, *adj_cc_ts = nullptr, *adj_cc_tt = nullptr;
   double *adj_tbar = nullptr, *adj_qbl = nullptr;
 
+  // owner-computes sharding of one treecode problem over ranks (shard.cpp):
+  // this rank's slice of the tree leaves, the unfiltered well-separated CSR
+  // (rebuilt per slice), and the communicator that all-gathers each stage's
+  // velocity (null: the rank computes its own slice only)
+  int shard_rank = 0, shard_n = 1;
+  std::vector<int> h_ns, h_cs, h_csrc;
+  std::vector<double> h_fcentre;  // [tree panels][4] panel centres (entry tables)
+  void* nccl_comm = nullptr;
+  double shard_timeout_s = 300.0;
+  sbslpm_status shard_status = SBSLPM_OK;  // a failed exchange inside an enqueued step
+  std::string shard_error;
+
   cudaStream_t stream() const { return user_stream_set ? user_stream : own_stream; }
 };
 
@@ -167,6 +179,15 @@ void enqueue_step(sbslpm_ctx* c, const double* x, const double* y, const double*
 void velocity_eval(sbslpm_ctx* c, int stage, double dt_s, const double* vprev, const double* x, const double* y,
                    const double* z, const double* area, const double* vors, double* v);
 void launch_add3(const double* t, long n, double* a, double* b, double* cc, cudaStream_t st);
+sbslpm_status install_cc_lists(sbslpm_ctx* c, const std::vector<int>& cs, const std::vector<int>& csrc);
+// shard.cpp: all-gathers a stage velocity [3][particles] over the context's
+// ranks (a no-op on an unsharded context); failures land in shard_status
+void shard_exchange(sbslpm_ctx* c, double* v);
+void shard_release(sbslpm_ctx* c);
+// Entry points that run a whole step: a sharded context (more than one rank)
+// needs its communicator; the adjoint and the shallow-water step are not
+// sharded.  Returns SBSLPM_OK or the refusal (with its message set).
+sbslpm_status shard_allows(const sbslpm_ctx* c, bool step_needs_exchange, const char* what);
 
 // tree_setup.cu: host tables of the decoupled-degree treecode.
 struct TreeTables {
@@ -199,6 +220,8 @@ sbslpm_status near_autotune(sbslpm_ctx* c, const double* x, const double* y, con
                             const double* vors);
 // The treecode's well-separated interactions into ftgt (chunked kernels where q allows).
 void launch_tree_cc(sbslpm_ctx* c, cudaStream_t st);
+// Target leaves the near-field launches cover: this rank's slice when sharded.
+inline int owned_leaves(const sbslpm_ctx* c) { return c->tgeom.owned > 0 ? c->tgeom.owned : c->fgeom.leaves; }
 sbslpm_status capture_graph(sbslpm_ctx* c, cudaGraphExec_t* graph, const std::function<void()>& body);
 
 }  // namespace sbslpm

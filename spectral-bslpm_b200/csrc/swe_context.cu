@@ -218,6 +218,7 @@ sbslpm_status sbslpm_swe_step(sbslpm_ctx* c, const double* x, const double* y, c
     return SBSLPM_ERR_ARG;
   if (any_on_host({x, y, z, area, vors, divs, height, vel_x, vel_y, vel_z, tracers, bv, bd, bh}))
     return set_last_error("device-pointer step given host memory"), SBSLPM_ERR_ARG;
+  SB_TRY(shard_allows(c, false, "the shallow-water path"));
   SB_TRY(swe_setup(c));
   swe_enqueue_step(c, x, y, z, area, vors, divs, height, vel_x, vel_y, vel_z, tracers, bv, bd, bh);
   return finish(c);
@@ -233,6 +234,7 @@ sbslpm_status sbslpm_swe_run(sbslpm_ctx* c, const double* x, const double* y, co
     return SBSLPM_ERR_ARG;
   if (any_on_host({x, y, z, area, vors, divs, height, vel_x, vel_y, vel_z, tracers, bv, bd, bh}))
     return set_last_error("device-pointer step given host memory"), SBSLPM_ERR_ARG;
+  SB_TRY(shard_allows(c, false, "the shallow-water path"));
   SB_TRY(swe_setup(c));
   GraphKey key{{x, y, z, area, vors, divs, height, vel_x, vel_y, vel_z, tracers, bv, bd, bh}};
   if (!c->swe_graph || !(key == c->swe_graph_key)) {
@@ -257,6 +259,7 @@ sbslpm_status sbslpm_swe_init(sbslpm_ctx* c, const double* x, const double* y, c
   if (!c || bad(x) || bad(y) || bad(z) || bad(area) || bad(vors) || bad(divs) || bad(height) || bad(vel_x) ||
       bad(vel_y) || bad(vel_z) || bad(bv) || bad(bd) || bad(bh))
     return SBSLPM_ERR_ARG;
+  SB_TRY(shard_allows(c, false, "the shallow-water path"));
   SB_TRY(swe_setup(c));
   cudaStream_t st = c->stream();
   const size_t ln = (size_t)c->A * c->q;
@@ -310,6 +313,7 @@ sbslpm_status sbslpm_swe_vel_interactions(sbslpm_ctx* c, const double* dx, const
   if (c->tree)
     return set_last_error("a treecode context has no spectral interaction list (sbslpm_swe_tree_velocity)"),
            SBSLPM_ERR_CONFIG;
+  SB_TRY(shard_allows(c, false, "the shallow-water path"));
   SB_TRY(swe_setup(c));
   cudaStream_t st = c->stream();
   launch_swe_sources_from_disp(c->geom, c->sgeom, dx, dy, dz, sv, sd, c->src, c->src2,
@@ -327,6 +331,7 @@ sbslpm_status sbslpm_swe_tree_velocity(sbslpm_ctx* c, const double* dx, const do
   if (any_on_host({dx, dy, dz, w_vor, w_div, u_x, u_y, u_z}))
     return set_last_error("device pointers expected"), SBSLPM_ERR_ARG;
   if (!c->tree) return set_last_error("the context has no treecode (proxy_degree 0)"), SBSLPM_ERR_CONFIG;
+  SB_TRY(shard_allows(c, false, "the shallow-water path"));
   SB_TRY(swe_setup(c));
   cudaStream_t st = c->stream();
   const size_t ln = (size_t)c->A * c->q;

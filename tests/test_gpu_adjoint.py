@@ -132,9 +132,10 @@ def test_twenty_step_gradient_matches_finite_differences(sb):
     assert big.sum() >= 56 and (np.abs(fds - ads)[big] / np.abs(ads[big])).max() <= 1e-5
 
 
-def tree_ctx(sb, levels, dt, theta=0.7, degree=8):
+def tree_ctx(sb, levels, dt, theta=0.7, degree=8, precision=None):
     cfg = sb.config_default(levels=levels, interp_degree=3, kernel_eps=1e-4, omega=2 * np.pi, dt=dt,
-                            precision=sb.FP64, fmm_theta=theta, proxy_degree=degree, leaf_size=256)
+                            precision=sb.FP64 if precision is None else precision, fmm_theta=theta,
+                            proxy_degree=degree, leaf_size=256)
     return sb.Context(cfg)
 
 
@@ -180,3 +181,52 @@ def test_treecode_gradient_matches_direct_sum_adjoint(sb):
     rel = float((gt - gd).norm() / gd.norm())
     print("treecode vs direct-sum adjoint gradient: relative L2 %.2e" % rel)
     assert rel <= 1e-5, rel
+
+
+def test_mixed_treecode_adjoint_step_matches_float64(sb):
+    """One reverse step on the mixed-precision treecode (the forward recomputed
+    in mixed precision, the transposed pair sums in float32 on packed
+    coordinates) against the same step in float64: the float32 rounding of
+    the pair sums, 1e-6 relative L2 at most (measured ~1e-8)."""
+    _, f, w0, wn = gaussian_vortex_state(sb, 5, 0.01, 1e-2)
+    wbar_next = torch.from_numpy(np.random.default_rng(9).standard_normal(tuple(wn.shape))).cuda()
+    out = []
+    for prec in (sb.FP64, sb.MIXED):
+        ctx = tree_ctx(sb, 5, 0.01, precision=prec)
+        wbar = torch.empty_like(wn)
+        ctx.bve_adjoint_step(*f, wn, wbar_next, wbar)
+        out.append(wbar)
+    rel = float((out[1] - out[0]).norm() / out[0].norm())
+    print("mixed vs float64 treecode adjoint step: relative L2 %.2e" % rel)
+    assert rel <= 1e-6, rel
+
+
+def test_mixed_treecode_gradient_matches_direct_sum_adjoint(sb):
+    """The 20-step loss gradient through the mixed-precision treecode's
+    adjoint against the float64 direct-sum adjoint's: within the treecode's
+    approximation error, as the float64 treecode."""
+    ctxd, f, w0, wn = gaussian_vortex_state(sb, 5, 0.01, 1e-2)
+    ctxm = tree_ctx(sb, 5, 0.01, precision=sb.MIXED)
+    area = f[3]
+    grads = []
+    for ctx in (ctxd, ctxm):
+        v = w0.clone()
+        vel = [torch.zeros_like(v) for _ in range(3)]
+        ctxd.bve_run(*f, v, *vel, nsteps=20)
+        x = wn.clone().requires_grad_()
+        out = sb.bve_rollout(ctx, *f, x, 20)
+        (0.5 * (area * (out - v) ** 2).sum()).backward()
+        grads.append(x.grad.clone())
+    gd, gm = grads
+    rel = float((gm - gd).norm() / gd.norm())
+    print("mixed treecode vs direct-sum adjoint gradient: relative L2 %.2e" % rel)
+    assert rel <= 1e-5, rel
+
+
+def test_mixed_direct_sum_adjoint_is_refused(sb):
+    _, f, w0, wn = gaussian_vortex_state(sb, 4, 0.01, 1e-2)
+    ctx = sb.Context(sb.config_default(levels=4, interp_degree=3, kernel_eps=1e-4, omega=2 * np.pi, dt=0.01,
+                                       velocity=sb.VEL_DIRECT, precision=sb.MIXED))
+    with pytest.raises(sb.SbslpmError) as e:
+        ctx.bve_adjoint_step(*f, wn, torch.ones_like(wn), torch.empty_like(wn))
+    assert e.value.status == 1

@@ -131,3 +131,51 @@ def test_ensemble_lists_sharded_over_two_ranks():
         lst, near = sb.dual_tree_traversal_flagged(4, panels, th)
         assert merged[m] == (lst.tolist(), near.tolist())
         assert np.array_equal(lst, sb.dual_tree_traversal(4, panels, th))
+
+
+def _shard_id_rank(rank, world, port, out):
+    """The host side of a sharded problem: the group's first rank makes the
+    NCCL id through the library, every rank receives it, and each takes its
+    slice of the particles."""
+    import datetime
+
+    import torch.distributed as dist
+
+    from conftest import load_package
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=30))
+    try:
+        sb = load_package()
+        ident = sb.exchange_shard_id()
+        out.put((rank, ident, sb.shard_slice(24576, 16, 1536, rank, world)))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_shard_id_and_slices_over_two_ranks():
+    ctx = torch.multiprocessing.get_context("spawn")
+    q = ctx.Queue()
+    port = free_port()
+    procs = [ctx.Process(target=_shard_id_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted((q.get(timeout=120) for _ in procs), key=lambda r: r[0])
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    (_, id0, s0), (_, id1, s1) = res
+    assert len(id0) == 128 and id0 == id1  # one communicator id for both ranks
+    assert s0 == (0, 196608) and s1 == (196608, 196608)  # disjoint, covering 24,576 x 16 particles
+
+
+def test_shard_slices_partition_the_particles():
+    from conftest import load_package
+
+    sb = load_package()
+    for ranks in (1, 2, 3, 4, 6, 8):
+        s = [sb.shard_slice(384, 16, 96, r, ranks) for r in range(ranks)]
+        assert s[0][0] == 0 and all(a[0] + a[1] == b[0] for a, b in zip(s, s[1:]))
+        assert s[-1][0] + s[-1][1] == 384 * 16
+    with pytest.raises(ValueError):
+        sb.shard_slice(384, 16, 96, 0, 5)
