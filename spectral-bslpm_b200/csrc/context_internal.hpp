@@ -123,6 +123,11 @@ struct sbslpm_ctx {
   double* hio = nullptr;  // [5 + T][leaves*q]: x, y, z, area, vors, tracers
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t ev_stage0 = nullptr, ev_copied = nullptr;
+  // the same step with its copies captured as one CUDA graph, for pinned host
+  // arrays (keyed by the host pointers)
+  cudaGraphExec_t host_graph = nullptr;
+  GraphKey host_graph_key{};
+  long host_launches_per_step = 0;
 
   // adjoint workspace, allocated on first use
   double4* adj_src = nullptr;  // [4 stages][panels*q] stage sources (positions, strengths)
@@ -223,5 +228,8 @@ void launch_tree_cc(sbslpm_ctx* c, cudaStream_t st);
 // Target leaves the near-field launches cover: this rank's slice when sharded.
 inline int owned_leaves(const sbslpm_ctx* c) { return c->tgeom.owned > 0 ? c->tgeom.owned : c->fgeom.leaves; }
 sbslpm_status capture_graph(sbslpm_ctx* c, cudaGraphExec_t* graph, const std::function<void()>& body);
+// Releases the captured BVE steps (device-array and host-array forms): their
+// launch shapes or lists changed.
+void drop_step_graphs(sbslpm_ctx* c);
 
 }  // namespace sbslpm

@@ -200,8 +200,7 @@ sbslpm_status sbslpm_set_shard(sbslpm_ctx* c, int rank, int nranks, const unsign
   // earlier work ends first; the captured step and the old communicator go
   SB_CUDA(cudaStreamSynchronize(c->stream()));
   shard_release(c);
-  if (c->graph) cudaGraphExecDestroy(c->graph);
-  c->graph = nullptr;
+  drop_step_graphs(c);
   if (c->swe_graph) cudaGraphExecDestroy(c->swe_graph);
   c->swe_graph = nullptr;
   c->shard_status = SBSLPM_OK;

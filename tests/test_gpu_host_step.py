@@ -76,6 +76,46 @@ def test_host_step_is_the_device_step(sb, case, pinned):
     assert np.array_equal(c[0], d[0])
 
 
+@pytest.mark.parametrize("case", ["treecode_mixed", "spectral_fp64_tracers"])
+def test_repeated_pinned_host_steps_replay_as_a_graph(sb, case):
+    """The same pinned arrays stepped again and again: after the first (eager)
+    call the step and its copies replay as one captured CUDA graph; every
+    step stays bit-identical to the device step, also after the launch shape
+    changes (the captured graph is dropped and captured again)."""
+    levels = 5 if case == "treecode_mixed" else 4
+    g = sb.build_grid(levels, 3, exact_cc=True)
+    vor = unit_sphere_rh4(g)
+    kw = dict(levels=levels, interp_degree=3, fmm_theta=0.7, kernel_eps=1e-4, omega=2 * np.pi, dt=0.005)
+    tracers = None
+    if case == "treecode_mixed":
+        kw.update(precision=sb.MIXED, proxy_degree=8, leaf_size=256)
+    else:
+        kw.update(tracer_count=2)
+        tracers = np.stack([g.z, g.x * g.y], axis=-1)
+    ctx = sb.Context(sb.config_default(**kw))
+    if case == "treecode_mixed":
+        ctx.set_near_tuning(128, 2, 2)
+        ctx.set_cc_tuning(3, 2)
+    P = lambda a: torch.from_numpy(np.array(a, dtype=np.float64, order="C", copy=True)).pin_memory()
+    hv, hvel = P(vor), [P(np.zeros_like(vor)) for _ in range(3)]
+    htr = P(tracers) if tracers is not None else None
+    hx = [P(a) for a in (g.x, g.y, g.z, g.area)]
+    dv, dtr = vor.copy(), (tracers.copy() if tracers is not None else None)
+    launches = []
+    for k in range(4):
+        if k == 2 and case == "treecode_mixed":
+            ctx.set_near_tuning(256, 1, 3)
+        l0 = sb.kernel_launches()
+        ctx.bve_back_rk4_step_host(*hx, hv, *hvel, htr)
+        launches.append(sb.kernel_launches() - l0)
+        dv, dvel, dtr = device_step(ctx, g, dv, dtr)
+        assert np.array_equal(hv.numpy(), dv), k
+        assert all(np.array_equal(h.numpy(), u) for h, u in zip(hvel, dvel)), k
+        if tracers is not None:
+            assert np.array_equal(htr.numpy(), dtr), k
+    assert launches[1] == launches[0] > 0  # a replay counts the captured kernels
+
+
 def test_host_step_rejects_device_and_misshaped_arrays(sb):
     g = sb.build_grid(3, 3, exact_cc=True)
     ctx = sb.Context(sb.config_default(levels=3, interp_degree=3, kernel_eps=1e-4))
