@@ -79,6 +79,7 @@ sbslpm_status sbslpm_bve_adjoint_step(sbslpm_ctx* c, const double* x, const doub
   if (c->cfg.tracer_count != 0 || c->cfg.forcing != SBSLPM_FORCING_NONE)
     return set_last_error("the adjoint step needs a context without tracers or forcing"), SBSLPM_ERR_CONFIG;
   SB_TRY(shard_allows(c, false, "the adjoint step"));
+  NvtxRange range("sbslpm bve adjoint step");
   SB_TRY(adjoint_setup(c));
   SB_TRY(near_autotune(c, x, y, z, area, vors));
   cudaStream_t st = c->stream();

@@ -432,6 +432,7 @@ void batch_velocity(sbslpm_batch* b, int stage, double dt_s, const double* vprev
 
 void batch_enqueue_step(sbslpm_batch* b, const double* x, const double* y, const double* z, const double* area,
                         double* vors, double* vel) {
+  NvtxRange step_range("sbslpm batch step");
   cudaStream_t st = b->stream();
   const size_t MN = (size_t)b->M * b->N;
   const double dt = b->cfg.dt;

@@ -417,14 +417,24 @@ void enqueue_step(sbslpm_ctx* c, const double* x, const double* y, const double*
   for (int k = 0; k < 4; k++) v[k] = c->vbuf + (size_t)k * 3 * ln;
   const double stage_dt[4] = {0.0, 0.5 * dt, 0.5 * dt, dt};
   // bve_forcing at the step's time, the same for all four stages (src/bve_time_step.cpp:323-395)
+  NvtxRange step_range("sbslpm bve step");
   if (c->force) launch_ssw_forcing(c->A, c->q, c->cfg.forcing, c->cfg.omega, c->d_time, x, y, z, c->force, st);
+  static const char* const stage_name[4] = {"sbslpm stage 0 velocity", "sbslpm stage 1 velocity",
+                                            "sbslpm stage 2 velocity", "sbslpm stage 3 velocity"};
   for (int s = 0; s < 4; s++) {
-    velocity_eval(c, s, stage_dt[s], s ? v[s - 1] : nullptr, x, y, z, area, vors, v[s]);
-    shard_exchange(c, v[s]);  // every rank's slice into every rank's copy (sharded contexts)
+    {
+      NvtxRange r(stage_name[s]);
+      velocity_eval(c, s, stage_dt[s], s ? v[s - 1] : nullptr, x, y, z, area, vors, v[s]);
+    }
+    if (c->nccl_comm) {
+      NvtxRange r("sbslpm stage velocity all-gather");
+      shard_exchange(c, v[s]);  // every rank's slice into every rank's copy (sharded contexts)
+    }
     if (s == 0 && stage0) cudaEventRecord(stage0, st);
   }
   if (c->force) launch_time_advance(c->d_time, dt, st);
   const int T = c->cfg.tracer_count;
+  NvtxRange remap_range("sbslpm departure + remap");
   launch_depart_remap(c->geom, &c->tab, x, y, z, v[0], v[1], v[2], v[3], dt, c->dep, vors, tracers, T, c->newvor,
                       c->newtr, 3, st);
   cudaMemcpyAsync(vors, c->newvor, sizeof(double) * ln, cudaMemcpyDeviceToDevice, st);
@@ -555,6 +565,7 @@ sbslpm_status cc_autotune(sbslpm_ctx* c) {
 sbslpm_status near_autotune(sbslpm_ctx* c, const double* x, const double* y, const double* z, const double* area,
                             const double* vors) {
   if (!c->tree || (c->near_tuned && c->cc_tuned)) return SBSLPM_OK;
+  NvtxRange r("sbslpm launch-shape timing");
   cudaStream_t st = c->stream();
   const int prec = c->cfg.precision;
   launch_bltc_sources(c->tgeom, c->fgeom, c->ftab, 0, 0.0, nullptr, x, y, z, vors, area, c->psrc, c->psrcf, c->fsrc,
@@ -993,6 +1004,7 @@ sbslpm_status sbslpm_bve_run(sbslpm_ctx* c, const double* x, const double* y, co
     SB_TRY(capture_graph(c, &c->graph, [&] { enqueue_step(c, x, y, z, area, vors, vel_x, vel_y, vel_z, tracers); }));
     c->graph_key = key;
   }
+  NvtxRange r("sbslpm bve run (graph replays)");
   for (int s = 0; s < nsteps; s++) {
     SB_CUDA(cudaGraphLaunch(c->graph, st));
     launch_counter() += c->launches_per_step;

@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <array>
 #include <initializer_list>
@@ -12,6 +13,16 @@
 #include "../../include/sbslpm.h"
 
 namespace sbslpm {
+
+// An NVTX range over a scope of host code (the enqueueing of a step's
+// phases): profilers show the stages on the CPU timeline and correlate them
+// with their kernels; without a profiler attached a range costs a branch.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // True when any non-null pointer is host memory: the entry points that take
 // device pointers reject those arguments instead of handing them to kernels.

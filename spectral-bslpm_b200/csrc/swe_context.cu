@@ -165,6 +165,7 @@ void swe_velocity_eval(sbslpm_ctx* c, int stage, double dtd, double dts, const d
 void swe_enqueue_step(sbslpm_ctx* c, const double* x, const double* y, const double* z, const double* area,
                       double* vors, double* divs, double* height, double* vel_x, double* vel_y, double* vel_z,
                       double* tracers, const double* bv, const double* bd, const double* bh) {
+  NvtxRange step_range("sbslpm swe step");
   (void)bv;  // modify_tendencies leaves the vorticity tendency alone (src/swe_time_step_2.cpp:778-782)
   cudaStream_t st = c->stream();
   const size_t ln = (size_t)c->A * c->q;
