@@ -242,7 +242,8 @@ sbslpm_status sbslpm_shard_unique_id(unsigned char* id);
  * leaf count; 1 restores the whole problem).  With nccl_id (128 bytes, the
  * same on every rank) it joins the ranks' communicator -- every rank calls it
  * together; a rank missing for timeout_s seconds (<= 0: 300) ends it with
- * SBSLPM_ERR_TIMEOUT.  Without nccl_id a context of more than one rank only
+ * SBSLPM_ERR_TIMEOUT and leaves the context as it was.  Without nccl_id a
+ * context of more than one rank only
  * evaluates its own slice (sbslpm_bve_velocity) and refuses whole steps.
  * Launch shapes are timed again on the next call. */
 sbslpm_status sbslpm_set_shard(sbslpm_ctx* ctx, int rank, int nranks, const unsigned char* nccl_id,

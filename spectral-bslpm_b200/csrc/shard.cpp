@@ -197,14 +197,37 @@ sbslpm_status sbslpm_set_shard(sbslpm_ctx* c, int rank, int nranks, const unsign
   if (c->Af % nranks)
     return set_last_error("nranks must divide the tree's " + std::to_string(c->Af) + " leaves"), SBSLPM_ERR_ARG;
   if (!(timeout_s > 0)) timeout_s = 300.0;
-  // earlier work ends first; the captured step and the old communicator go
+  // earlier work ends first
   SB_CUDA(cudaStreamSynchronize(c->stream()));
+  // the new communicator first: a set-up that fails leaves the context as it was
+  ncclComm_t comm = nullptr;
+  if (id) {  // one rank works too: its all-gather is a copy in place
+    const NcclApi& n = nccl();
+    if (!n.ok) return set_last_error(n.why), SBSLPM_ERR_NO_DEVICE;
+    ncclUniqueId u;
+    std::memcpy(u.internal, id, 128);
+    ncclConfig_t cfg = NCCL_CONFIG_INITIALIZER;
+    cfg.blocking = 0;
+    const ncclResult_t r = n.init_rank_config(&comm, nranks, u, rank, &cfg);
+    if (r != ncclSuccess && r != ncclInProgress) {
+      if (comm) n.abort_comm(comm);
+      return set_last_error("ncclCommInitRankConfig: " + nccl_error(n, r)), SBSLPM_ERR_CUDA;
+    }
+    std::string msg;
+    const sbslpm_status s = wait_comm(n, comm, timeout_s, "communicator set-up", msg);
+    if (s != SBSLPM_OK) {
+      n.abort_comm(comm);
+      return set_last_error(msg), s;
+    }
+  }
+  // the old communicator and the captured steps go
   shard_release(c);
   drop_step_graphs(c);
   if (c->swe_graph) cudaGraphExecDestroy(c->swe_graph);
   c->swe_graph = nullptr;
   c->shard_status = SBSLPM_OK;
   c->shard_timeout_s = timeout_s;
+  c->nccl_comm = comm;
 
   // leaves [lo, hi) of this rank; a tree panel's leaf range from its children
   const int per = c->Af / nranks, lo = rank * per, hi = lo + per, off = c->Pf - c->Af;
@@ -249,28 +272,6 @@ sbslpm_status sbslpm_set_shard(sbslpm_ctx* c, int rank, int nranks, const unsign
   c->near_tuned = false;
   c->near_mutual = false;
   if (c->cc_partial) c->cc_tuned = false;
-
-  if (id) {  // one rank works too: its all-gather is a copy in place
-    const NcclApi& n = nccl();
-    if (!n.ok) return set_last_error(n.why), SBSLPM_ERR_NO_DEVICE;
-    ncclUniqueId u;
-    std::memcpy(u.internal, id, 128);
-    ncclConfig_t cfg = NCCL_CONFIG_INITIALIZER;
-    cfg.blocking = 0;
-    ncclComm_t comm = nullptr;
-    const ncclResult_t r = n.init_rank_config(&comm, nranks, u, rank, &cfg);
-    if (r != ncclSuccess && r != ncclInProgress) {
-      if (comm) n.abort_comm(comm);
-      return set_last_error("ncclCommInitRankConfig: " + nccl_error(n, r)), SBSLPM_ERR_CUDA;
-    }
-    std::string msg;
-    const sbslpm_status s = wait_comm(n, comm, timeout_s, "communicator set-up", msg);
-    if (s != SBSLPM_OK) {
-      n.abort_comm(comm);
-      return set_last_error(msg), s;
-    }
-    c->nccl_comm = comm;
-  }
   return SBSLPM_OK;
 }
 

@@ -159,14 +159,14 @@ def test_one_rank_communicator_steps_are_the_unsharded_steps(sb, grids, prec):
 
 def test_a_rank_that_never_joins_times_out(sb, grids):
     """Rank 0 of 2 with no rank 1: the communicator's set-up is polled on the
-    host and gives up after the limit with SBSLPM_ERR_TIMEOUT; the context then
-    runs unsharded as before."""
+    host and gives up after the limit with SBSLPM_ERR_TIMEOUT, leaving the
+    context as it was (unsharded): it steps as before."""
     g, vor = grids[4]
     ctx = make_ctx(sb, 4, 64, 8, 0.7, sb.FP64)
     with pytest.raises(sb.SbslpmError) as e:
         ctx.shard(0, 2, sb.shard_unique_id(), timeout=3.0)
     assert e.value.status == 7  # SBSLPM_ERR_TIMEOUT
-    ctx.shard(0, 1)
+    assert ctx.shard_range() == (0, ctx.leaf_count * ctx.q)
     f = [cuda(g.x), cuda(g.y), cuda(g.z), cuda(g.area), cuda(vor)]
     vel = [torch.zeros_like(f[0]) for _ in range(3)]
     ctx.bve_back_rk4_step(*f, *vel)
