@@ -625,8 +625,21 @@ def adjoint_bench(sb, torch, dev, directions=8):
     tree["mixed"] = {"forward_ms": t0.elapsed_time(t1), "backward_ms": t1.elapsed_time(t2),
                      "grad_rel_l2_vs_direct_sum_adjoint": float((xm.grad - grad).norm() / grad.norm()),
                      "grad_rel_l2_vs_fp64_treecode_adjoint": float((xm.grad - xt.grad).norm() / xt.grad.norm())}
+    # the direct sum in mixed precision (float32 pairs on leaf-packed coordinates, both directions)
+    ctxdm = sb.Context(sb.config_default(levels=ADJ_LEVELS, interp_degree=DEGREE, kernel_eps=EPS, omega=OMEGA,
+                                         dt=ADJ_DT, velocity=sb.VEL_DIRECT, precision=sb.MIXED))
+    xd = T(wn).requires_grad_()
+    t0.record(st)
+    outd = sb.bve_rollout(ctxdm, *f, xd, ADJ_STEPS)
+    lossd = 0.5 * (area * (outd - wstar) ** 2).sum()
+    t1.record(st)
+    lossd.backward()
+    t2.record(st)
+    t2.synchronize()
+    direct_mixed = {"forward_ms": t0.elapsed_time(t1), "backward_ms": t1.elapsed_time(t2),
+                    "grad_rel_l2_vs_fp64_direct_sum_adjoint": float((xd.grad - grad).norm() / grad.norm())}
     return {"forward_ms": e0.elapsed_time(e1), "backward_ms": e1.elapsed_time(e2), "steps": ADJ_STEPS,
-            "treecode": tree,
+            "treecode": tree, "direct_mixed": direct_mixed,
             "particles": int(g.x.size), "J": float(loss.detach()), "grad_norm": float(grad.norm()),
             "fd_directions": directions, "fd_max_err_over_rms": float(np.abs(fds - ads).max() / rms),
             "fd_max_rel_err": float((np.abs(fds - ads) / np.abs(ads)).max()),

@@ -19,6 +19,7 @@
 
 #include "../../include/sbslpm.h"
 #include "adjoint.cuh"
+#include "adjoint_pair32.cuh"
 #include "device_common.cuh"
 
 namespace sbslpm {
@@ -76,6 +77,69 @@ __global__ void __launch_bounds__(kAdjThreads)
   if (j < ns) {
     double* p = partial + (long)blockIdx.y * 4 * ns;
     p[j] = kBiotSavart * qb;
+    p[ns + j] = kBiotSavart * s.w * bx;
+    p[2 * ns + j] = kBiotSavart * s.w * by;
+    p[3 * ns + j] = kBiotSavart * s.w * bz;
+  }
+}
+
+// The same VJP in mixed precision for the step's own particles (targets and
+// sources both [leaf][q]; leaf centres g.pd_centre): one thread per source,
+// packed relative to its leaf's centre; target tiles of whole leaves staged
+// as pairs (adj_stage), the offset between the two leaves' centres rounded
+// to float32 once per (source, target leaf), the float32 sums of a target
+// leaf added into float64 -- the arithmetic of the forward's mixed leaf-pair
+// kernels.  gridDim.y groups of target leaves write partials [group][4][ns].
+template <bool GUARD>
+__global__ void __launch_bounds__(kAdjThreads)
+    k_bs_vjp32_leaves(StepGeom g, const double* __restrict__ tx, const double* __restrict__ ty,
+                      const double* __restrict__ tz, const double* __restrict__ ux, const double* __restrict__ uy,
+                      const double* __restrict__ uz, const double4* __restrict__ src, double* __restrict__ partial) {
+  __shared__ float4 tile[3 * (kAdjThreads / 2)];  // TL leaves x qh target pairs x 3
+  const int q = g.q, qh = (q + 1) >> 1, TL = max(1, kAdjThreads / (2 * qh));
+  const long ns = (long)g.leaves * q;
+  const long j = blockIdx.x * (long)kAdjThreads + threadIdx.x;
+  const int per = (g.leaves + gridDim.y - 1) / gridDim.y;
+  const int l0 = blockIdx.y * per, l1 = min(g.leaves, l0 + per);
+  const double4 s = src[j < ns ? j : 0];
+  const double* cs = g.pd_centre + 4 * (long)(g.offset + (j < ns ? j / q : 0));
+  const float sx = (float)((s.x - cs[0]) * kPackScale), sy = (float)((s.y - cs[1]) * kPackScale),
+              sz = (float)((s.z - cs[2]) * kPackScale);
+  const float feps = (float)g.eps;
+  const float2 eps2 = make_float2(feps, feps);
+  double qb = 0, bx = 0, by = 0, bz = 0;
+  for (int L = l0; L < l1; L += TL) {
+    const int nl = min(TL, l1 - L);
+    __syncthreads();
+    for (int k = threadIdx.x; k < nl * 2 * qh; k += blockDim.x) {
+      const int ll = k / (2 * qh), idx = k - ll * 2 * qh;
+      float4* lt = tile + 3 * qh * ll;
+      if (idx < q) {
+        const long i = (long)(L + ll) * q + idx;
+        adj_stage(lt, idx, tx[i], ty[i], tz[i], ux[i], uy[i], uz[i], g.pd_centre + 4 * (long)(g.offset + L + ll));
+      } else {
+        adj_stage_zero(lt, idx);
+      }
+    }
+    __syncthreads();
+    for (int ll = 0; ll < nl; ll++) {
+      const double* ct = g.pd_centre + 4 * (long)(g.offset + L + ll);
+      const float a0 = sx + (float)((cs[0] - ct[0]) * kPackScale), a1 = sy + (float)((cs[1] - ct[1]) * kPackScale),
+                  a2 = sz + (float)((cs[2] - ct[2]) * kPackScale);
+      const float2 ax = make_float2(a0, a0), ay = make_float2(a1, a1), az = make_float2(a2, a2);
+      float2 qq = make_float2(0.f, 0.f), cx = qq, cy = qq, cz = qq, dx = qq, dy = qq, dz = qq;
+      const float4* lt = tile + 3 * qh * ll;
+      for (int k2 = 0; k2 < qh; k2++)
+        adj_pair32x2<GUARD>(ax, ay, az, lt[3 * k2], lt[3 * k2 + 1], lt[3 * k2 + 2], eps2, qq, cx, cy, cz, dx, dy, dz);
+      qb += (double)qq.x + (double)qq.y;
+      bx += ((double)cx.x + (double)cx.y) - 2.0 * ((double)dx.x + (double)dx.y);
+      by += ((double)cy.x + (double)cy.y) - 2.0 * ((double)dy.x + (double)dy.y);
+      bz += ((double)cz.x + (double)cz.y) - 2.0 * ((double)dz.x + (double)dz.y);
+    }
+  }
+  if (j < ns) {
+    double* p = partial + (long)blockIdx.y * 4 * ns;
+    p[j] = kBiotSavart / kPackScale * qb;
     p[ns + j] = kBiotSavart * s.w * bx;
     p[2 * ns + j] = kBiotSavart * s.w * by;
     p[3 * ns + j] = kBiotSavart * s.w * bz;
@@ -371,6 +435,22 @@ void launch_bs_vjp(long nt, const double* tx, const double* ty, const double* tz
   SB_LAUNCH(k_sum_groups, blocks_for(ns, 256), 256, 0, st, partial, groups, ns, 4 * ns, qbar);
   for (int c = 0; c < 3; c++)
     SB_LAUNCH(k_sum_groups, blocks_for(ns, 256), 256, 0, st, partial + (long)(c + 1) * ns, groups, ns, 4 * ns,
+              ybar + (long)c * ns);
+}
+
+void launch_bs_vjp_leaves32(const StepGeom& g, const double* tx, const double* ty, const double* tz,
+                            const double* ux, const double* uy, const double* uz, const double4* src, double* partial,
+                            int groups, double* qbar, double* ybar, cudaStream_t st) {
+  const long ns = (long)g.leaves * g.q;
+  const int gl = groups < g.leaves ? groups : g.leaves;
+  const dim3 grid(blocks_for(ns, kAdjThreads), (unsigned)gl);
+  if (g.eps > 0)
+    SB_LAUNCH(k_bs_vjp32_leaves<false>, grid, kAdjThreads, 0, st, g, tx, ty, tz, ux, uy, uz, src, partial);
+  else
+    SB_LAUNCH(k_bs_vjp32_leaves<true>, grid, kAdjThreads, 0, st, g, tx, ty, tz, ux, uy, uz, src, partial);
+  SB_LAUNCH(k_sum_groups, blocks_for(ns, 256), 256, 0, st, partial, gl, ns, 4 * ns, qbar);
+  for (int c = 0; c < 3; c++)
+    SB_LAUNCH(k_sum_groups, blocks_for(ns, 256), 256, 0, st, partial + (long)(c + 1) * ns, gl, ns, 4 * ns,
               ybar + (long)c * ns);
 }
 

@@ -15,6 +15,12 @@ int adjoint_groups(long n_targets, long n_sources);
 void launch_bs_vjp(long nt, const double* tx, const double* ty, const double* tz, const double* ux,
                    const double* uy, const double* uz, long ns, const double4* src, double eps, double* partial,
                    int groups, double* qbar, double* ybar, cudaStream_t st);
+// The same for the step's particles in mixed precision (targets x and sources
+// src both the context's [leaf][q] particles; float32 pairs on coordinates
+// packed relative to their leaves' centres; groups of target leaves).
+void launch_bs_vjp_leaves32(const StepGeom& g, const double* tx, const double* ty, const double* tz,
+                            const double* ux, const double* uy, const double* uz, const double4* src, double* partial,
+                            int groups, double* qbar, double* ybar, cudaStream_t st);
 void launch_pack_sources(long n, const double* x, const double* y, const double* z, const double* q, double4* s,
                          cudaStream_t st);
 // Adjoint of a stage's leaf sources (strength a (w + 2 Omega z - 2 Omega y_z),

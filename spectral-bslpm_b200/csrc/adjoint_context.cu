@@ -72,10 +72,8 @@ sbslpm_status sbslpm_bve_adjoint_step(sbslpm_ctx* c, const double* x, const doub
                                       double* vors_bar) {
   if (!c || bad(x) || bad(y) || bad(z) || bad(area) || bad(vors) || bad(vors_bar_next) || bad(vors_bar))
     return SBSLPM_ERR_ARG;
-  if (!(c->cfg.velocity == SBSLPM_VEL_DIRECT || c->tree) || (c->cfg.precision != SBSLPM_FP64 && !c->tree))
-    return set_last_error("the adjoint step runs on the float64 direct-sum or the treecode velocity (float64 or "
-                          "mixed)"),
-           SBSLPM_ERR_CONFIG;
+  if (!(c->cfg.velocity == SBSLPM_VEL_DIRECT || c->tree))
+    return set_last_error("the adjoint step runs on the direct-sum or the treecode velocity"), SBSLPM_ERR_CONFIG;
   if (c->cfg.tracer_count != 0 || c->cfg.forcing != SBSLPM_FORCING_NONE)
     return set_last_error("the adjoint step needs a context without tracers or forcing"), SBSLPM_ERR_CONFIG;
   SB_TRY(shard_allows(c, false, "the adjoint step"));
@@ -109,6 +107,9 @@ sbslpm_status sbslpm_bve_adjoint_step(sbslpm_ctx* c, const double* x, const doub
                           nullptr, c->fsrc, false, st);
       launch_tree_velocity_adjoint(c->tgeom, c->fgeom, c->ftab, tl, x, y, z, vb[s], c->psrc, c->adj_tbar, c->adj_qbl,
                                    c->adj_q, c->adj_y, c->cfg.precision == SBSLPM_MIXED, st);
+    } else if (c->cfg.precision == SBSLPM_MIXED) {
+      launch_bs_vjp_leaves32(c->geom, x, y, z, vb[s], vb[s] + ln, vb[s] + 2 * ln, c->adj_src + s * pn + off,
+                             c->adj_part, c->adj_groups, c->adj_q, c->adj_y, st);
     } else {
       launch_bs_vjp((long)ln, x, y, z, vb[s], vb[s] + ln, vb[s] + 2 * ln, (long)ln, c->adj_src + s * pn + off,
                     c->cfg.kernel_eps, c->adj_part, c->adj_groups, c->adj_q, c->adj_y, st);
