@@ -756,7 +756,6 @@ def shard_bench(sb, torch, dev, dist, args, rank, world, local_rank):
         ctx.shard_over(timeout=120.0)
     else:
         ctx.shard(0, 1, sb.shard_unique_id(), timeout=120.0)
-    ctx.set_near_mutual(False)
     f = fields()
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
     for _ in range(args.warmup):
@@ -775,7 +774,7 @@ def shard_bench(sb, torch, dev, dist, args, rank, world, local_rank):
         one = ctx_new()
         near, cc = ctx.near_tuning(), ctx.cc_tuning()
         one.set_near_tuning(*near[:3])
-        one.set_near_mutual(False)
+        one.set_near_mutual(ctx.near_mutual()[0])  # a one-rank context may keep the two-sided first stage
         if ctx.cc_form() == 3:
             one.set_cc_tuning_bulk(*cc[:2])
         elif ctx.cc_form():

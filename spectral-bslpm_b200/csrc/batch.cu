@@ -658,7 +658,7 @@ sbslpm_status sbslpm_batch_run(sbslpm_batch* b, const double* x, const double* y
     b->launches_per_step = launch_counter() - before;
     launch_counter() = before;
     SB_CUDA(ce);
-    SB_CUDA(cudaGraphInstantiate(&b->graph, gr, 0));
+    SB_CUDA(cudaGraphInstantiateWithFlags(&b->graph, gr, cudaGraphInstantiateFlagUseNodePriority));
     cudaGraphDestroy(gr);
     std::memcpy(b->key, key, sizeof key);
   }

@@ -82,7 +82,8 @@ __global__ void __launch_bounds__(kThreads)
                        const double* __restrict__ dispy, const double* __restrict__ dispz,
                        const double* __restrict__ wv_in, const double* __restrict__ wd_in, double4* __restrict__ psrc,
                        float4* __restrict__ psrcf, double4* __restrict__ psrc2, float4* __restrict__ psrcf2,
-                       double4* __restrict__ proxy, double4* __restrict__ proxy2, int mixed) {
+                       double4* __restrict__ proxy, double4* __restrict__ proxy2, int mixed,
+                       const double* __restrict__ gcentre, int gq) {
   extern __shared__ double sh[];
   const int f = blockIdx.x, n1 = tg.n + 1, npl = tg.npl;
   double* lx = sh;              // [npl][n1] basis of the displaced vorticity sources
@@ -93,7 +94,6 @@ __global__ void __launch_bounds__(kThreads)
   const int panel = fg.offset + f;
   const double* bd = tg.fbounds + 4 * panel;
   const int face = tg.fface[panel];
-  const double* cc = fg.pd_centre + 4 * (long)panel;
   const long N = tg.N;
   for (int k = threadIdx.x; k < npl; k += blockDim.x) {
     const long i = (long)f * npl + k;
@@ -121,11 +121,12 @@ __global__ void __launch_bounds__(kThreads)
     project_to_sphere(xx, yy, zz);
     psrc[i] = make_double4(xx, yy, zz, wv);
     psrc2[i] = make_double4(gx, gy, gz, wd);
-    if (mixed) {
-      psrcf[i] = make_float4((float)((xx - cc[0]) * kPackScale), (float)((yy - cc[1]) * kPackScale),
-                             (float)((zz - cc[2]) * kPackScale), (float)wv);
-      psrcf2[i] = make_float4((float)((gx - cc[0]) * kPackScale), (float)((gy - cc[1]) * kPackScale),
-                              (float)((gz - cc[2]) * kPackScale), (float)wd);
+    if (mixed) {  // packed relative to the particle's grid leaf (see k_bltc_swe_near)
+      const double* gc = gcentre + 4 * (i / gq);
+      psrcf[i] = make_float4((float)((xx - gc[0]) * kPackScale), (float)((yy - gc[1]) * kPackScale),
+                             (float)((zz - gc[2]) * kPackScale), (float)wv);
+      psrcf2[i] = make_float4((float)((gx - gc[0]) * kPackScale), (float)((gy - gc[1]) * kPackScale),
+                              (float)((gz - gc[2]) * kPackScale), (float)wd);
     }
     double xi, eta;
     xieta_from_xyz_face(xx, yy, zz, face, xi, eta);
@@ -174,13 +175,19 @@ __device__ __forceinline__ void swe_tree_epilogue(double K, double tx, double ty
 // split), TPT targets per thread, the source leaf's particles of both fields
 // staged in shared memory.  Split y takes every gridDim.y-th source leaf and
 // writes the velocity of its partial sums to out + y 3N.  float64: pair64 on
-// absolute positions; mixed: pair32 on positions relative to the leaves'
-// centres, per-source-leaf float32 sums added into float64.
+// absolute positions.  Mixed: pair32 with the sources packed relative to
+// their own grid leaf (gq particles) and, per source grid leaf, the target's
+// offset from that leaf's centre formed in float64 and rounded once, so that
+// d' = (c_sub - t) kPackScale + (s - c_sub) kPackScale carries the rounding
+// of grid-leaf-sized terms rather than tree-leaf-sized ones (the divergence
+// tendency differentiates the velocity twice and amplifies that rounding);
+// float32 sums per source grid leaf added into float64.
 template <int NT, int TPT, bool GUARD, bool MIXED>
 __global__ void __launch_bounds__(NT)
     k_bltc_swe_near(TreeGeom tg, StepGeom fg, const double* __restrict__ x, const double* __restrict__ y,
                     const double* __restrict__ z, const double4* __restrict__ psrc, const double4* __restrict__ psrc2,
-                    const float4* __restrict__ psrcf, const float4* __restrict__ psrcf2, double* __restrict__ out) {
+                    const float4* __restrict__ psrcf, const float4* __restrict__ psrcf2, double* __restrict__ out,
+                    const double* __restrict__ gcentre, int gq) {
   using Src = typename std::conditional<MIXED, float4, double4>::type;
   extern __shared__ __align__(16) unsigned char smem[];
   Src* t1 = reinterpret_cast<Src*>(smem);
@@ -189,7 +196,6 @@ __global__ void __launch_bounds__(NT)
   double* v = out + (long)split * 3 * tg.N;
   const double* ct = fg.pd_centre + 4 * (long)(fg.offset + f);
   double tx[TPT], ty[TPT], tz[TPT], ax[TPT], ay[TPT], az[TPT], bx[TPT], by[TPT], bz[TPT];
-  float dtx[TPT], dty[TPT], dtz[TPT];
 #pragma unroll
   for (int r = 0; r < TPT; r++) {
     const int k = threadIdx.x + r * NT;
@@ -197,11 +203,9 @@ __global__ void __launch_bounds__(NT)
     tx[r] = x[i];
     ty[r] = y[i];
     tz[r] = z[i];
-    dtx[r] = (float)((tx[r] - ct[0]) * kPackScale);
-    dty[r] = (float)((ty[r] - ct[1]) * kPackScale);
-    dtz[r] = (float)((tz[r] - ct[2]) * kPackScale);
     ax[r] = ay[r] = az[r] = bx[r] = by[r] = bz[r] = 0;
   }
+  (void)ct;
   const float feps = (float)tg.eps;
   for (int e = tg.near_start[f] + split; e < tg.near_start[f + 1]; e += nsplit) {
     const int sl = tg.near_src[e];
@@ -218,34 +222,34 @@ __global__ void __launch_bounds__(NT)
     }
     __syncthreads();
     if constexpr (MIXED) {
-      const double* cs = fg.pd_centre + 4 * (long)(fg.offset + sl);
-      const float c0 = (float)((cs[0] - ct[0]) * kPackScale), c1 = (float)((cs[1] - ct[1]) * kPackScale),
-                  c2 = (float)((cs[2] - ct[2]) * kPackScale);
-      float b0[TPT], b1[TPT], b2[TPT], fa[TPT][3], fb[TPT][3];
-#pragma unroll
-      for (int r = 0; r < TPT; r++) {
-        b0[r] = c0 - dtx[r];
-        b1[r] = c1 - dty[r];
-        b2[r] = c2 - dtz[r];
-        fa[r][0] = fa[r][1] = fa[r][2] = fb[r][0] = fb[r][1] = fb[r][2] = 0.f;
-      }
-#pragma unroll 4
-      for (int k = 0; k < npl; k++) {
-        const float4 s1 = t1[k], s2 = t2[k];
+      for (int k0 = 0; k0 < npl; k0 += gq) {
+        const double* cs = gcentre + 4 * ((sb + k0) / gq);
+        float b0[TPT], b1[TPT], b2[TPT], fa[TPT][3], fb[TPT][3];
 #pragma unroll
         for (int r = 0; r < TPT; r++) {
-          pair32<GUARD>(b0[r], b1[r], b2[r], s1, feps, fa[r][0], fa[r][1], fa[r][2]);
-          pair32<GUARD>(b0[r], b1[r], b2[r], s2, feps, fb[r][0], fb[r][1], fb[r][2]);
+          b0[r] = (float)((cs[0] - tx[r]) * kPackScale);
+          b1[r] = (float)((cs[1] - ty[r]) * kPackScale);
+          b2[r] = (float)((cs[2] - tz[r]) * kPackScale);
+          fa[r][0] = fa[r][1] = fa[r][2] = fb[r][0] = fb[r][1] = fb[r][2] = 0.f;
         }
-      }
+#pragma unroll 4
+        for (int k = k0; k < k0 + gq; k++) {
+          const float4 s1 = t1[k], s2 = t2[k];
 #pragma unroll
-      for (int r = 0; r < TPT; r++) {
-        ax[r] += fa[r][0];
-        ay[r] += fa[r][1];
-        az[r] += fa[r][2];
-        bx[r] += fb[r][0];
-        by[r] += fb[r][1];
-        bz[r] += fb[r][2];
+          for (int r = 0; r < TPT; r++) {
+            pair32<GUARD>(b0[r], b1[r], b2[r], s1, feps, fa[r][0], fa[r][1], fa[r][2]);
+            pair32<GUARD>(b0[r], b1[r], b2[r], s2, feps, fb[r][0], fb[r][1], fb[r][2]);
+          }
+        }
+#pragma unroll
+        for (int r = 0; r < TPT; r++) {
+          ax[r] += fa[r][0];
+          ay[r] += fa[r][1];
+          az[r] += fa[r][2];
+          bx[r] += fb[r][0];
+          by[r] += fb[r][1];
+          bz[r] += fb[r][2];
+        }
       }
     } else {
 #pragma unroll 4
@@ -281,7 +285,7 @@ void launch_bltc_swe_sources(const TreeGeom& tg, const StepGeom& fg, const BliTa
                              const double* dispx, const double* dispy, const double* dispz, const double* wv,
                              const double* wd, double4* psrc, float4* psrcf,
                              double4* psrc2, float4* psrcf2, double4* proxy, double4* proxy2, bool mixed,
-                             cudaStream_t st) {
+                             const double* gcentre, int gq, cudaStream_t st) {
   const int n1 = tg.n + 1, qx = n1 * n1, G = kThreads / qx > 0 ? kThreads / qx : 1;
   const size_t smem = sizeof(double) * ((size_t)tg.npl * n1 * 2 + 2 * (size_t)tg.npl + 2 * (size_t)G * qx);
   static bool attr = false;
@@ -291,12 +295,13 @@ void launch_bltc_swe_sources(const TreeGeom& tg, const StepGeom& fg, const BliTa
   }
   SB_LAUNCH(k_bltc_swe_sources, (unsigned)fg.leaves, kThreads, smem, st, tg, fg, tab, stage, dtd, dts, vprev, tprev,
             x, y, z, vors, divs, area, dispx, dispy, dispz, wv, wd, psrc, psrcf, psrc2, psrcf2, proxy, proxy2,
-            mixed ? 1 : 0);
+            mixed ? 1 : 0, gcentre, gq);
 }
 
 void launch_bltc_swe_near(const TreeGeom& tg, const StepGeom& fg, int precision, const double* x, const double* y,
                           const double* z, const double4* psrc, const double4* psrc2, const float4* psrcf,
-                          const float4* psrcf2, double* near, int splits, cudaStream_t st) {
+                          const float4* psrcf2, double* near, int splits, const double* gcentre, int gq,
+                          cudaStream_t st) {
   const dim3 grid((unsigned)fg.leaves, (unsigned)splits);
   const bool guard = !(tg.eps > 0), mixed = precision == SBSLPM_MIXED;
   constexpr int NT = 128;
@@ -306,14 +311,14 @@ void launch_bltc_swe_near(const TreeGeom& tg, const StepGeom& fg, int precision,
   do {                                                                                                            \
     if (mixed) {                                                                                                  \
       if (guard) SB_LAUNCH((k_bltc_swe_near<NT, TPT, true, true>), grid, NT, smem, st, tg, fg, x, y, z, psrc,     \
-                           psrc2, psrcf, psrcf2, near);                                                           \
+                           psrc2, psrcf, psrcf2, near, gcentre, gq);                                                           \
       else SB_LAUNCH((k_bltc_swe_near<NT, TPT, false, true>), grid, NT, smem, st, tg, fg, x, y, z, psrc, psrc2,   \
-                     psrcf, psrcf2, near);                                                                        \
+                     psrcf, psrcf2, near, gcentre, gq);                                                                        \
     } else {                                                                                                      \
       if (guard) SB_LAUNCH((k_bltc_swe_near<NT, TPT, true, false>), grid, NT, smem, st, tg, fg, x, y, z, psrc,    \
-                           psrc2, psrcf, psrcf2, near);                                                           \
+                           psrc2, psrcf, psrcf2, near, gcentre, gq);                                                           \
       else SB_LAUNCH((k_bltc_swe_near<NT, TPT, false, false>), grid, NT, smem, st, tg, fg, x, y, z, psrc, psrc2,  \
-                     psrcf, psrcf2, near);                                                                        \
+                     psrcf, psrcf2, near, gcentre, gq);                                                                        \
     }                                                                                                             \
   } while (0)
   if (tpt <= 1) SB_SN(1);

@@ -505,7 +505,10 @@ sbslpm_status capture_graph(sbslpm_ctx* c, cudaGraphExec_t* graph, const std::fu
   c->launches_per_step = launch_counter() - before;
   launch_counter() = before;
   SB_CUDA(ce);
-  SB_CUDA(cudaGraphInstantiate(graph, g, 0));
+  // kernels captured from the higher-priority auxiliary stream keep that
+  // priority on replay (otherwise a graph runs every node at its launch
+  // stream's priority and the tree passes queue behind the near field)
+  SB_CUDA(cudaGraphInstantiateWithFlags(graph, g, cudaGraphInstantiateFlagUseNodePriority));
   cudaGraphDestroy(g);
   return SBSLPM_OK;
 }

@@ -105,7 +105,8 @@ void swe_tree_velocity(sbslpm_ctx* c, int stage, double dtd, double dts, const d
   const bool mixed = c->cfg.precision == SBSLPM_MIXED;
   const StepGeom& fg = c->fgeom;
   launch_bltc_swe_sources(c->tgeom, fg, c->ftab, stage, dtd, dts, vprev, tprev, x, y, z, vors, divs, area, dispx,
-                          dispy, dispz, wv, wd, c->psrc, c->psrcf, c->psrc2, c->psrcf2, c->fsrc, c->fsrc2, mixed, st);
+                          dispy, dispz, wv, wd, c->psrc, c->psrcf, c->psrc2, c->psrcf2, c->fsrc, c->fsrc2, mixed,
+                          c->centre + 4 * (size_t)c->off, c->q, st);
   cudaStream_t tree_st = c->aux_stream ? c->aux_stream : st;
   if (c->aux_stream) {
     cudaEventRecord(c->ev_fork, st);
@@ -121,7 +122,7 @@ void swe_tree_velocity(sbslpm_ctx* c, int stage, double dtd, double dts, const d
   if (c->aux_stream) cudaEventRecord(c->ev_join, tree_st);
   constexpr int kSplits = 4;
   launch_bltc_swe_near(c->tgeom, fg, c->cfg.precision, x, y, z, c->psrc, c->psrc2, c->psrcf, c->psrcf2, c->near,
-                       kSplits, st);
+                       kSplits, c->centre + 4 * (size_t)c->off, c->q, st);
   if (c->aux_stream) cudaStreamWaitEvent(st, c->ev_join, 0);
   launch_bltc_to_particles(c->tgeom, fg, c->ftgt, c->near, kSplits, v, st);
 }

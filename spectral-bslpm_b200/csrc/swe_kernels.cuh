@@ -76,11 +76,15 @@ void launch_bltc_swe_sources(const TreeGeom& tg, const StepGeom& fg, const BliTa
                              const double* z, const double* vors, const double* divs, const double* area,
                              const double* dispx, const double* dispy, const double* dispz, const double* wv,
                              const double* wd, double4* psrc, float4* psrcf, double4* psrc2, float4* psrcf2,
-                             double4* proxy, double4* proxy2, bool mixed, cudaStream_t st);
+                             double4* proxy, double4* proxy2, bool mixed, const double* gcentre, int gq,
+                             cudaStream_t st);
 // Near leaf pairs of both fields into splits x 3 x N velocity partials
-// (leaves of at most 256 particles).
+// (leaves of at most 256 particles).  gcentre: the grid leaves' centres
+// ([grid leaves][4], gq particles each): mixed precision packs the particle
+// sources relative to them.
 void launch_bltc_swe_near(const TreeGeom& tg, const StepGeom& fg, int precision, const double* x, const double* y,
                           const double* z, const double4* psrc, const double4* psrc2, const float4* psrcf,
-                          const float4* psrcf2, double* near, int splits, cudaStream_t st);
+                          const float4* psrcf2, double* near, int splits, const double* gcentre, int gq,
+                          cudaStream_t st);
 
 }  // namespace sbslpm
