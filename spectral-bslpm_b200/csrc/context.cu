@@ -78,6 +78,17 @@ sbslpm_status precompute(sbslpm_ctx* c) {
   build_interp(d, false, interp);
 
   bli_table(d, c->tab);
+  // panel centres for the mixed-precision relative coordinates (the treecode's
+  // shallow-water near field packs its particles by grid leaf as well)
+  std::vector<double> centre((size_t)4 * P, 0.0);
+  for (int p = 0; p < P; p++) {
+    const sbslpm_panel& pp = c->panels[p];
+    double xyz[3];
+    xyz_from_xieta(kPi / 4.0 * 0.5 * (pp.min_xi + pp.max_xi), kPi / 4.0 * 0.5 * (pp.min_eta + pp.max_eta), pp.face,
+                   xyz);
+    for (int k = 0; k < 3; k++) centre[4 * (size_t)p + k] = xyz[k];
+  }
+  SB_TRY(upload(&c->centre, centre));
   if (c->tree) return SBSLPM_OK;  // the treecode has its own set-up
 
   // proxy positions, exactly as the reference's interaction kernel places them
@@ -93,16 +104,6 @@ sbslpm_status precompute(sbslpm_ctx* c) {
     }
   SB_TRY(upload(&c->px, px));
 
-  // panel centres for the mixed-precision relative coordinates
-  std::vector<double> centre((size_t)4 * P, 0.0);
-  for (int p = 0; p < P; p++) {
-    const sbslpm_panel& pp = c->panels[p];
-    double xyz[3];
-    xyz_from_xieta(kPi / 4.0 * 0.5 * (pp.min_xi + pp.max_xi), kPi / 4.0 * 0.5 * (pp.min_eta + pp.max_eta), pp.face,
-                   xyz);
-    for (int k = 0; k < 3; k++) centre[4 * (size_t)p + k] = xyz[k];
-  }
-  SB_TRY(upload(&c->centre, centre));
   if (c->cfg.velocity != SBSLPM_VEL_FMM) return SBSLPM_OK;
 
   // displacement interpolation at non-leaf proxies (bve_disp_interp,
