@@ -510,6 +510,22 @@ def profile_run(sb, torch, dev, args):
         vel = torch.zeros((M, 3) + g.x.shape, dtype=torch.float64, device=dev)
         for _ in range(n):
             batch.step(T(g.x), T(g.y), T(g.z), T(g.area), v, vel)
+    elif args.profile in ("adjoint", "adjoint64"):
+        # reverse steps of the treecode (the benchmark's tree, 393,216 particles) from the RH4 state
+        g = sb.build_grid(LEVELS, DEGREE, exact_cc=True)
+        prec = sb.MIXED if args.profile == "adjoint" else sb.FP64
+        ctx = sb.Context(sb.config_default(levels=LEVELS, interp_degree=DEGREE, fmm_theta=THETA, kernel_eps=EPS,
+                                           omega=OMEGA, dt=DT, precision=prec, proxy_degree=PROXY_DEGREE,
+                                           leaf_size=LEAF_SIZE))
+        ctx.set_near_tuning(*[int(v) for v in args.near_shape.split(",")])
+        cc = args.cc_shape.split(",")
+        ctx.set_cc_tuning(int(cc[0]), int(cc[1]))
+        f = [T(g.x), T(g.y), T(g.z), T(g.area)]
+        w = T(rh4(g))
+        wbar_next = T(np.random.default_rng(9).standard_normal(g.x.shape))
+        wbar = torch.empty_like(w)
+        for _ in range(n):
+            ctx.bve_adjoint_step(*f, w, wbar_next, wbar)
     elif args.profile in ("swe", "swe64"):
         g = sb.build_grid(LEVELS, DEGREE, exact_cc=True)
         om, u0 = 2 * np.pi, 2 * np.pi / 12
@@ -842,7 +858,8 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint measurement")
     ap.add_argument("--no-at-bar", action="store_true",
                     help="skip the search for the fastest treecode settings that meet the 1e-6 bar")
-    ap.add_argument("--profile", choices=["treecode", "treecode64", "spectral", "swe", "swe64", "ensemble"],
+    ap.add_argument("--profile", choices=["treecode", "treecode64", "spectral", "swe", "swe64", "ensemble", "adjoint",
+                                          "adjoint64"],
                     help="run --warmup + --steps steps of one path and exit (for profiler captures; no timing)")
     ap.add_argument("--members", type=int, default=ENS_MEMBERS, help="ensemble members in --profile ensemble")
     ap.add_argument("--cc-mode", type=int, default=3, choices=[0, 1, 2, 3],
