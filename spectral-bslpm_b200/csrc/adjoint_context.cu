@@ -57,6 +57,18 @@ sbslpm_status adjoint_setup(sbslpm_ctx* c) {
     SB_TRY(upload(&c->adj_cc_tt, ctt));
     SB_TRY(dalloc(&c->adj_tbar, (size_t)3 * t.Pf * t.qx));
     SB_TRY(dalloc(&c->adj_qbl, (size_t)t.Pf * t.qx));
+  } else if (c->cfg.velocity == SBSLPM_VEL_FMM) {
+    // the spectral interaction list transposed: target panels by source panel, in list order
+    std::vector<int> ts(c->P + 1, 0), tt(c->list.size());
+    for (const auto& e : c->list) ts[e.source_panel + 1]++;
+    for (int p = 0; p < c->P; p++) ts[p + 1] += ts[p];
+    std::vector<int> fill(ts.begin(), ts.end() - 1);
+    for (const auto& e : c->list) tt[fill[e.source_panel]++] = e.target_panel;
+    SB_TRY(upload(&c->adj_cc_ts, ts));
+    SB_TRY(upload(&c->adj_cc_tt, tt));
+    SB_TRY(dalloc(&c->adj_tbar, 3 * pn));
+    SB_TRY(dalloc(&c->adj_qbl, pn));
+    SB_TRY(dalloc(&c->adj_ynl, (size_t)3 * c->off * c->q));
   }
   return SBSLPM_OK;
 }
@@ -72,8 +84,8 @@ sbslpm_status sbslpm_bve_adjoint_step(sbslpm_ctx* c, const double* x, const doub
                                       double* vors_bar) {
   if (!c || bad(x) || bad(y) || bad(z) || bad(area) || bad(vors) || bad(vors_bar_next) || bad(vors_bar))
     return SBSLPM_ERR_ARG;
-  if (!(c->cfg.velocity == SBSLPM_VEL_DIRECT || c->tree))
-    return set_last_error("the adjoint step runs on the direct-sum or the treecode velocity"), SBSLPM_ERR_CONFIG;
+  if (c->cfg.velocity == SBSLPM_VEL_FMM && !c->tree && c->cfg.precision != SBSLPM_FP64)
+    return set_last_error("the adjoint step of the spectral FMM runs in float64"), SBSLPM_ERR_CONFIG;
   if (c->cfg.tracer_count != 0 || c->cfg.forcing != SBSLPM_FORCING_NONE)
     return set_last_error("the adjoint step needs a context without tracers or forcing"), SBSLPM_ERR_CONFIG;
   SB_TRY(shard_allows(c, false, "the adjoint step"));
@@ -89,7 +101,12 @@ sbslpm_status sbslpm_bve_adjoint_step(sbslpm_ctx* c, const double* x, const doub
   const double* v[4];
   for (int k = 0; k < 4; k++) v[k] = c->vbuf + (size_t)k * 3 * ln;
   const double h[4] = {0.0, 0.5 * dt, 0.5 * dt, dt};
-  if (!c->tree)
+  const bool spectral = !c->tree && c->cfg.velocity == SBSLPM_VEL_FMM;
+  if (spectral)  // every panel's stage sources: displaced proxies and anterpolated strengths
+    for (int s = 0; s < 4; s++)
+      launch_upward_fused(c->geom, 0, s, h[s], s ? v[s - 1] : nullptr, x, y, z, vors, area, c->adj_src + s * pn,
+                          false, st);
+  else if (!c->tree)
     for (int s = 0; s < 4; s++)
       launch_leaf_sources(c->geom, s, h[s], s ? v[s - 1] : nullptr, x, y, z, vors, area, c->adj_src + s * pn, st);
   // reverse: departure search and remap, then the stages from the last
@@ -107,6 +124,10 @@ sbslpm_status sbslpm_bve_adjoint_step(sbslpm_ctx* c, const double* x, const doub
                           nullptr, c->fsrc, false, st);
       launch_tree_velocity_adjoint(c->tgeom, c->fgeom, c->ftab, tl, x, y, z, vb[s], c->psrc, c->adj_tbar, c->adj_qbl,
                                    c->adj_q, c->adj_y, c->cfg.precision == SBSLPM_MIXED, st);
+    } else if (spectral) {
+      launch_spectral_velocity_adjoint(c->geom, c->adj_cc_ts, c->adj_cc_tt, vb[s], c->adj_src + s * pn,
+                                       c->adj_tbar, c->adj_qbl, c->adj_y, c->adj_ynl, st);
+      if (s > 0) launch_nonleaf_positions_adjoint(c->geom, h[s], v[s - 1], c->adj_ynl, vb[s - 1], st);
     } else if (c->cfg.precision == SBSLPM_MIXED) {
       launch_bs_vjp_leaves32(c->geom, x, y, z, vb[s], vb[s] + ln, vb[s] + 2 * ln, c->adj_src + s * pn + off,
                              c->adj_part, c->adj_groups, c->adj_q, c->adj_y, st);
@@ -114,8 +135,8 @@ sbslpm_status sbslpm_bve_adjoint_step(sbslpm_ctx* c, const double* x, const doub
       launch_bs_vjp((long)ln, x, y, z, vb[s], vb[s] + ln, vb[s] + 2 * ln, (long)ln, c->adj_src + s * pn + off,
                     c->cfg.kernel_eps, c->adj_part, c->adj_groups, c->adj_q, c->adj_y, st);
     }
-    launch_src_adjoint((long)ln, s, h[s], c->cfg.omega, s ? v[s - 1] : nullptr, x, y, z, area, c->adj_q, c->adj_y,
-                       vors_bar, s ? vb[s - 1] : nullptr, st);
+    launch_src_adjoint((long)ln, s, h[s], c->cfg.omega, s ? v[s - 1] : nullptr, x, y, z, area,
+                       spectral ? c->adj_qbl + off : c->adj_q, c->adj_y, vors_bar, s ? vb[s - 1] : nullptr, st);
   }
   return finish(c);
 }

@@ -15,6 +15,14 @@
 // well-separated list); Qbar = U^T Qbar (a downward accumulation); then per
 // particle qbar_j = [A^T Qbar]_j + near^T, ybar_j = q_j grad_y(A^T Qbar) +
 // near^T, with near^T the source-owned sum over the transposed near list.
+//
+// The reference's own spectral FMM (proxies = the panels' interp_degree
+// points, displaced and re-projected at every stage; bve_vel_impl.hpp:85-122,
+// bve_time_step.cpp:69-170) reverses the same way on the panel quadtree, with
+// two differences: the interactions' sources move, so their transpose also
+// gives position adjoints, and a non-leaf proxy's displacement is the BLI
+// interpolation of its containing leaf's (bve_disp_interp), whose transpose
+// scatters back onto the leaf velocities.
 #include <cuda_runtime.h>
 
 #include "adjoint_pair32.cuh"
@@ -384,7 +392,133 @@ __global__ void k_tree_sources_T(TreeGeom tg, StepGeom fg, BliTable tab, const d
   }
 }
 
+// Transposed spectral-FMM interactions: source panel s (blockIdx.x), one
+// thread per source proxy k, over the target panels whose list holds s:
+// Qbar_s,k = K sum g c.d and ybar_s,k = K S_s,k sum [g c - g^2 (c.d) d],
+// c = Tbar_t,i x x_t,i, d = y_s,k - x_t,i (y: the stage's displaced proxy).
+// Writes qbar [panels*q]; the position adjoints of leaf proxies go to
+// ybar_leaf [3][leaves*q], of non-leaf proxies to ybar_nl [3][offset*q].
+template <bool GUARD>
+__global__ void __launch_bounds__(kT) k_spec_interact_T(StepGeom g, const int* __restrict__ tstart,
+                                                       const int* __restrict__ ttgt, const double* __restrict__ tbar,
+                                                       const double4* __restrict__ src, double* __restrict__ qbar,
+                                                       double* __restrict__ ybar_leaf, double* __restrict__ ybar_nl) {
+  __shared__ double sx[kT], sy[kT], sz[kT], cx[kT], cy[kT], cz[kT];
+  const int s = blockIdx.x, q = g.q;
+  const long pn = (long)g.panels * q;
+  const int k = threadIdx.x;
+  const double4 y = src[(long)s * q + (k < q ? k : 0)];
+  double qb = 0, bx = 0, by = 0, bz = 0;
+  for (int e = tstart[s]; e < tstart[s + 1]; e++) {
+    const long tb = (long)ttgt[e] * q;
+    __syncthreads();
+    if (k < q) {
+      const double x = g.px[tb + k], yy = g.px[pn + tb + k], z = g.px[2 * pn + tb + k];
+      const double a = tbar[tb + k], b = tbar[pn + tb + k], c = tbar[2 * pn + tb + k];
+      sx[k] = x;
+      sy[k] = yy;
+      sz[k] = z;
+      cx[k] = b * z - c * yy;
+      cy[k] = c * x - a * z;
+      cz[k] = a * yy - b * x;
+    }
+    __syncthreads();
+    if (k < q)
+      for (int i = 0; i < q; i++) {
+        const double dx = y.x - sx[i], dy = y.y - sy[i], dz = y.z - sz[i];
+        const double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+        double gg = recip_nr(fma(0.5, r2, g.eps));
+        if (GUARD) gg = r2 > 0.0 ? gg : 0.0;
+        const double sd = fma(cx[i], dx, fma(cy[i], dy, cz[i] * dz));
+        qb = fma(gg, sd, qb);
+        const double t = gg * gg * sd;
+        bx = fma(gg, cx[i], fma(-t, dx, bx));
+        by = fma(gg, cy[i], fma(-t, dy, by));
+        bz = fma(gg, cz[i], fma(-t, dz, bz));
+      }
+  }
+  if (k >= q) return;
+  const long o = (long)s * q + k;
+  qbar[o] = kBiotSavart * qb;
+  if (s >= g.offset) {
+    const long ln = (long)g.leaves * q, l = o - (long)g.offset * q;
+    ybar_leaf[l] = kBiotSavart * y.w * bx;
+    ybar_leaf[ln + l] = kBiotSavart * y.w * by;
+    ybar_leaf[2 * ln + l] = kBiotSavart * y.w * bz;
+  } else {
+    const long nn = (long)g.offset * q;
+    ybar_nl[o] = kBiotSavart * y.w * bx;
+    ybar_nl[nn + o] = kBiotSavart * y.w * by;
+    ybar_nl[2 * nn + o] = kBiotSavart * y.w * bz;
+  }
+}
+
+// Non-leaf proxy positions, reversed: y_i = proj(p_i + h sum_m B_mi v[row_i + m])
+// (k_nonleaf_positions); vbar[c][row_i + m] += h B_mi J(p)^T ybar_i with
+// J(p)^T ybar = (ybar - yhat (yhat.ybar)) / |p|.  Proxies of one leaf row add
+// into the same velocity entries: double atomics.
+__global__ void k_nonleaf_positions_T(StepGeom g, double h, const double* __restrict__ vprev,
+                                      const double* __restrict__ ybar_nl, double* __restrict__ vbar) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const int q = g.q;
+  const long np = (long)g.offset * q;
+  if (i >= np) return;
+  const long pn = (long)g.panels * q, ln = (long)g.leaves * q;
+  const long row = (long)g.il_row[i] * q;
+  double px = g.px[i], py = g.px[pn + i], pz = g.px[2 * pn + i];
+  for (int m = 0; m < q; m++) {
+    const double bm = g.il_basis[m * np + i];
+    px += (h * vprev[row + m]) * bm;
+    py += (h * vprev[ln + row + m]) * bm;
+    pz += (h * vprev[2 * ln + row + m]) * bm;
+  }
+  const double r = sqrt(px * px + py * py + pz * pz), ir = 1.0 / r;
+  const double hx = px * ir, hy = py * ir, hz = pz * ir;
+  const double gx = ybar_nl[i], gy = ybar_nl[np + i], gz = ybar_nl[2 * np + i];
+  const double dd = hx * gx + hy * gy + hz * gz;
+  const double ax = h * (gx - hx * dd) * ir, ay = h * (gy - hy * dd) * ir, az = h * (gz - hz * dd) * ir;
+  for (int m = 0; m < q; m++) {
+    const double bm = g.il_basis[m * np + i];
+    atomicAdd(vbar + row + m, ax * bm);
+    atomicAdd(vbar + ln + row + m, ay * bm);
+    atomicAdd(vbar + 2 * ln + row + m, az * bm);
+  }
+}
+
 }  // namespace
+
+void launch_spectral_velocity_adjoint(const StepGeom& g, const int* tstart, const int* ttgt, const double* vbar,
+                                      const double4* src, double* tbar, double* qbar, double* ybar_leaf,
+                                      double* ybar_nl, cudaStream_t st) {
+  const int q = g.q, P = g.panels;
+  const long pn = (long)P * q, ln = (long)g.leaves * q, off = (long)g.offset * q;
+  // the leaf targets' adjoint is vbar itself (leaf proxies = particles); the
+  // downward pass transposed accumulates it up the tree
+  cudaMemsetAsync(tbar, 0, sizeof(double) * 3 * pn, st);
+  for (int c = 0; c < 3; c++)
+    cudaMemcpyAsync(tbar + c * pn + off, vbar + c * ln, sizeof(double) * ln, cudaMemcpyDeviceToDevice, st);
+  for (int lev = g.levels - 2; lev >= 0; lev--) {
+    const long work = (6L << (2 * lev)) * q * 3;
+    SB_LAUNCH(k_tree_up3, blocks_for(work, 256), 256, 0, st, g, lev, tbar);
+  }
+  if (g.eps > 0)
+    SB_LAUNCH(k_spec_interact_T<false>, (unsigned)P, kT, 0, st, g, tstart, ttgt, tbar, src, qbar, ybar_leaf,
+              ybar_nl);
+  else
+    SB_LAUNCH(k_spec_interact_T<true>, (unsigned)P, kT, 0, st, g, tstart, ttgt, tbar, src, qbar, ybar_leaf,
+              ybar_nl);
+  // the strengths' upward pass transposed: interpolate their adjoints down
+  for (int lev = 0; lev < g.levels - 1; lev++) {
+    const long work = (6L << (2 * (lev + 1))) * q;
+    SB_LAUNCH(k_tree_down1, blocks_for(work, 256), 256, 0, st, g, lev, qbar);
+  }
+}
+
+void launch_nonleaf_positions_adjoint(const StepGeom& g, double h, const double* vprev, const double* ybar_nl,
+                                      double* vbar, cudaStream_t st) {
+  const long np = (long)g.offset * g.q;
+  if (np > 0) SB_LAUNCH(k_nonleaf_positions_T, blocks_for(np, 256), 256, 0, st, g, h, vprev, ybar_nl, vbar);
+}
 
 void launch_tree_velocity_adjoint(const TreeGeom& tg, const StepGeom& fg, const BliTable& ftab,
                                   const TreeAdjointLists& tl, const double* x, const double* y, const double* z,

@@ -136,6 +136,7 @@ struct sbslpm_ctx {
   int adj_groups = 1;
   int *adj_near_ts = nullptr, *adj_near_tt = nullptr, *adj_cc_ts = nullptr, *adj_cc_tt = nullptr;
   double *adj_tbar = nullptr, *adj_qbl = nullptr;
+  double* adj_ynl = nullptr;  // spectral FMM: [3][non-leaf proxies] position adjoints
 
   // owner-computes sharding of one treecode problem over ranks (shard.cpp):
   // this rank's slice of the tree leaves, the unfiltered well-separated CSR

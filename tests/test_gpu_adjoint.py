@@ -250,3 +250,55 @@ def test_mixed_direct_sum_adjoint_matches_float64(sb):
     rel20 = float((grads[1] - grads[0]).norm() / grads[0].norm())
     print("mixed vs float64 direct-sum adjoint: step %.2e, 20-step gradient %.2e" % (rel1, rel20))
     assert rel1 <= 1e-6 and rel20 <= 1e-6, (rel1, rel20)
+
+
+def spectral_ctx(sb, levels, dt, theta=0.7):
+    return sb.Context(sb.config_default(levels=levels, interp_degree=3, kernel_eps=1e-4, omega=2 * np.pi, dt=dt,
+                                        precision=sb.FP64, fmm_theta=theta))
+
+
+@pytest.mark.parametrize("levels", [3, 4])
+def test_spectral_fmm_adjoint_step_dot_product(sb, levels):
+    """One reverse step through the reference's own spectral FMM (displaced
+    proxies on every panel, non-leaf displacements interpolated from the
+    leaves) against central differences of the forward step."""
+    _, f, w0, wn = gaussian_vortex_state(sb, levels, 0.01, 1e-2)
+    ctx = spectral_ctx(sb, levels, 0.01)
+    wbar_next = torch.from_numpy(np.random.default_rng(9).standard_normal(tuple(wn.shape))).cuda()
+    wbar = torch.empty_like(wn)
+    ctx.bve_adjoint_step(*f, wn, wbar_next, wbar)
+
+    def step(w):
+        v = w.clone()
+        vel = [torch.zeros_like(v) for _ in range(3)]
+        ctx.bve_back_rk4_step(*f, v, *vel)
+        return v
+
+    for seed in range(3):
+        d = torch.from_numpy(np.random.default_rng(70 + seed).standard_normal(tuple(wn.shape))).cuda()
+        h = 1e-6
+        fd = float((wbar_next * (step(wn + h * d) - step(wn - h * d))).sum()) / (2 * h)
+        ad = float((wbar * d).sum())
+        print(f"levels {levels} seed {seed}: fd {fd:.10e} adjoint {ad:.10e}")
+        assert abs(fd - ad) <= 1e-6 * abs(ad), (seed, fd, ad)
+
+
+def test_spectral_fmm_gradient_close_to_direct_sum_adjoint(sb):
+    """The 20-step loss gradient through the spectral FMM's adjoint against the
+    float64 direct-sum adjoint's: they differ by the FMM's approximation
+    error (theta 0.5 here)."""
+    ctxd, f, w0, wn = gaussian_vortex_state(sb, 5, 0.01, 1e-2)
+    ctxs = spectral_ctx(sb, 5, 0.01, theta=0.5)
+    area = f[3]
+    v = w0.clone()
+    vel = [torch.zeros_like(v) for _ in range(3)]
+    ctxd.bve_run(*f, v, *vel, nsteps=20)
+    grads = []
+    for ctx in (ctxd, ctxs):
+        x = wn.clone().requires_grad_()
+        out = sb.bve_rollout(ctx, *f, x, 20)
+        (0.5 * (area * (out - v) ** 2).sum()).backward()
+        grads.append(x.grad.clone())
+    rel = float((grads[1] - grads[0]).norm() / grads[0].norm())
+    print("spectral FMM vs direct-sum adjoint gradient: relative L2 %.2e" % rel)
+    assert rel <= 1e-4, rel
