@@ -367,11 +367,13 @@ sbslpm_status sbslpm_cubed_sphere_2d_to_1d(long n_leaves, int degree, const doub
  * the adjoint of the input vorticity, vors_bar = (d vors_next / d vors)^T
  * vors_bar_next, through the four velocity evaluations (source positions and
  * strengths), the departure search and the remap.  The forward step is
- * recomputed from the checkpoint inside the call.  Needs a context with the
- * direct-sum or the treecode (proxy_degree > 0) velocity, in float64 or mixed
- * precision (mixed: the forward recomputed in mixed precision and the
+ * recomputed from the checkpoint inside the call.  Runs on every velocity
+ * method: the direct sum and the treecode (proxy_degree > 0) in float64 or
+ * mixed precision (mixed: the forward recomputed in mixed precision and the
  * transposed pair sums in float32 on coordinates packed relative to their
- * leaves' or panels' centres, the rest float64), and no tracers or forcing.
+ * leaves' or panels' centres, the rest float64), and the reference's
+ * spectral FMM in float64 (displaced proxies on every panel; the non-leaf
+ * displacement interpolation reversed).  Needs no tracers or forcing.
  * Locating points in panels is piecewise constant and is not
  * differentiated. */
 sbslpm_status sbslpm_bve_adjoint_step(sbslpm_ctx* ctx, const double* xcos, const double* ycos, const double* zcos,
