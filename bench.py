@@ -657,8 +657,21 @@ def adjoint_bench(sb, torch, dev, directions=8):
     t2.synchronize()
     direct_mixed = {"forward_ms": t0.elapsed_time(t1), "backward_ms": t1.elapsed_time(t2),
                     "grad_rel_l2_vs_fp64_direct_sum_adjoint": float((xd.grad - grad).norm() / grad.norm())}
+    # the reference's own spectral FMM (float64, theta 0.7): displaced proxies on every panel
+    ctxs = sb.Context(sb.config_default(levels=ADJ_LEVELS, interp_degree=DEGREE, kernel_eps=EPS, omega=OMEGA,
+                                        dt=ADJ_DT, precision=sb.FP64, fmm_theta=THETA))
+    xs = T(wn).requires_grad_()
+    t0.record(st)
+    outs = sb.bve_rollout(ctxs, *f, xs, ADJ_STEPS)
+    losss = 0.5 * (area * (outs - wstar) ** 2).sum()
+    t1.record(st)
+    losss.backward()
+    t2.record(st)
+    t2.synchronize()
+    spectral = {"forward_ms": t0.elapsed_time(t1), "backward_ms": t1.elapsed_time(t2), "theta": THETA,
+                "grad_rel_l2_vs_direct_sum_adjoint": float((xs.grad - grad).norm() / grad.norm())}
     return {"forward_ms": e0.elapsed_time(e1), "backward_ms": e1.elapsed_time(e2), "steps": ADJ_STEPS,
-            "treecode": tree, "direct_mixed": direct_mixed,
+            "treecode": tree, "direct_mixed": direct_mixed, "spectral_fmm": spectral,
             "particles": int(g.x.size), "J": float(loss.detach()), "grad_norm": float(grad.norm()),
             "fd_directions": directions, "fd_max_err_over_rms": float(np.abs(fds - ads).max() / rms),
             "fd_max_rel_err": float((np.abs(fds - ads) / np.abs(ads)).max()),
