@@ -84,8 +84,6 @@ sbslpm_status sbslpm_bve_adjoint_step(sbslpm_ctx* c, const double* x, const doub
                                       double* vors_bar) {
   if (!c || bad(x) || bad(y) || bad(z) || bad(area) || bad(vors) || bad(vors_bar_next) || bad(vors_bar))
     return SBSLPM_ERR_ARG;
-  if (c->cfg.velocity == SBSLPM_VEL_FMM && !c->tree && c->cfg.precision != SBSLPM_FP64)
-    return set_last_error("the adjoint step of the spectral FMM runs in float64"), SBSLPM_ERR_CONFIG;
   if (c->cfg.tracer_count != 0 || c->cfg.forcing != SBSLPM_FORCING_NONE)
     return set_last_error("the adjoint step needs a context without tracers or forcing"), SBSLPM_ERR_CONFIG;
   SB_TRY(shard_allows(c, false, "the adjoint step"));
@@ -126,7 +124,8 @@ sbslpm_status sbslpm_bve_adjoint_step(sbslpm_ctx* c, const double* x, const doub
                                    c->adj_q, c->adj_y, c->cfg.precision == SBSLPM_MIXED, st);
     } else if (spectral) {
       launch_spectral_velocity_adjoint(c->geom, c->adj_cc_ts, c->adj_cc_tt, vb[s], c->adj_src + s * pn,
-                                       c->adj_tbar, c->adj_qbl, c->adj_y, c->adj_ynl, st);
+                                       c->adj_tbar, c->adj_qbl, c->adj_y, c->adj_ynl,
+                                       c->cfg.precision == SBSLPM_MIXED, st);
       if (s > 0) launch_nonleaf_positions_adjoint(c->geom, h[s], v[s - 1], c->adj_ynl, vb[s - 1], st);
     } else if (c->cfg.precision == SBSLPM_MIXED) {
       launch_bs_vjp_leaves32(c->geom, x, y, z, vb[s], vb[s] + ln, vb[s] + 2 * ln, c->adj_src + s * pn + off,

@@ -392,54 +392,100 @@ __global__ void k_tree_sources_T(TreeGeom tg, StepGeom fg, BliTable tab, const d
   }
 }
 
-// Transposed spectral-FMM interactions: source panel s (blockIdx.x), one
-// thread per source proxy k, over the target panels whose list holds s:
-// Qbar_s,k = K sum g c.d and ybar_s,k = K S_s,k sum [g c - g^2 (c.d) d],
-// c = Tbar_t,i x x_t,i, d = y_s,k - x_t,i (y: the stage's displaced proxy).
-// Writes qbar [panels*q]; the position adjoints of leaf proxies go to
-// ybar_leaf [3][leaves*q], of non-leaf proxies to ybar_nl [3][offset*q].
-template <bool GUARD>
+// Transposed spectral-FMM interactions: one group of G lanes per source panel
+// s (kT / G groups per block; G = q rounded up to a power of two for q <= 32,
+// the whole block above), lane k its proxy k, over the target panels whose
+// list holds s: Qbar_s,k = K sum g c.d and ybar_s,k = K S_s,k sum [g c -
+// g^2 (c.d) d], c = Tbar_t,i x x_t,i, d = y_s,k - x_t,i (y: the stage's
+// displaced proxy).  Float64, or mixed: d' = d kPackScale from coordinates
+// packed relative to the two panels' centres (their offset rounded once per
+// entry), one source against two targets per paired FP32 instruction
+// (adj_pair32x2), per-entry float32 sums added into float64.  Writes qbar
+// [panels*q]; position adjoints of leaf proxies to ybar_leaf [3][leaves*q],
+// of non-leaf proxies to ybar_nl [3][offset*q].
+template <int G, bool GUARD, bool MIXED>
 __global__ void __launch_bounds__(kT) k_spec_interact_T(StepGeom g, const int* __restrict__ tstart,
                                                        const int* __restrict__ ttgt, const double* __restrict__ tbar,
                                                        const double4* __restrict__ src, double* __restrict__ qbar,
                                                        double* __restrict__ ybar_leaf, double* __restrict__ ybar_nl) {
-  __shared__ double sx[kT], sy[kT], sz[kT], cx[kT], cy[kT], cz[kT];
-  const int s = blockIdx.x, q = g.q;
+  constexpr int S = kT / G;
+  __shared__ double sd64[6][kT];                  // float64: x, y, z, c of each group's target panel
+  __shared__ float4 sd32[S][3 * ((G + 1) / 2)];  // mixed: pairs of packed targets and c
+  const int gi = threadIdx.x / G, k = threadIdx.x % G, base = gi * G;
+  const int s = blockIdx.x * S + gi, q = g.q, qh = (q + 1) >> 1;
   const long pn = (long)g.panels * q;
-  const int k = threadIdx.x;
-  const double4 y = src[(long)s * q + (k < q ? k : 0)];
+  const bool panel = s < g.panels;
+  const bool act = panel && k < q;
+  const unsigned lanes = G >= 32 ? 0xffffffffu : (((1u << G) - 1u) << (threadIdx.x & 31 & ~(G - 1)));
+  auto sync = [&] {
+    if (G > 32) __syncthreads();
+    else __syncwarp(lanes);
+  };
+  const double4 y = src[panel ? (long)s * q + (k < q ? k : 0) : 0];
+  const double* cs = g.pd_centre + 4 * (long)(panel ? s : 0);
+  const float ysx = (float)((y.x - cs[0]) * kPackScale), ysy = (float)((y.y - cs[1]) * kPackScale),
+              ysz = (float)((y.z - cs[2]) * kPackScale);
+  const float feps = (float)g.eps;
+  const float2 eps2 = make_float2(feps, feps);
   double qb = 0, bx = 0, by = 0, bz = 0;
-  for (int e = tstart[s]; e < tstart[s + 1]; e++) {
+  const int e0 = panel ? tstart[s] : 0, e1 = panel ? tstart[s + 1] : 0;
+  for (int e = e0; e < e1; e++) {
     const long tb = (long)ttgt[e] * q;
-    __syncthreads();
-    if (k < q) {
-      const double x = g.px[tb + k], yy = g.px[pn + tb + k], z = g.px[2 * pn + tb + k];
-      const double a = tbar[tb + k], b = tbar[pn + tb + k], c = tbar[2 * pn + tb + k];
-      sx[k] = x;
-      sy[k] = yy;
-      sz[k] = z;
-      cx[k] = b * z - c * yy;
-      cy[k] = c * x - a * z;
-      cz[k] = a * yy - b * x;
-    }
-    __syncthreads();
-    if (k < q)
-      for (int i = 0; i < q; i++) {
-        const double dx = y.x - sx[i], dy = y.y - sy[i], dz = y.z - sz[i];
-        const double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
-        double gg = recip_nr(fma(0.5, r2, g.eps));
-        if (GUARD) gg = r2 > 0.0 ? gg : 0.0;
-        const double sd = fma(cx[i], dx, fma(cy[i], dy, cz[i] * dz));
-        qb = fma(gg, sd, qb);
-        const double t = gg * gg * sd;
-        bx = fma(gg, cx[i], fma(-t, dx, bx));
-        by = fma(gg, cy[i], fma(-t, dy, by));
-        bz = fma(gg, cz[i], fma(-t, dz, bz));
+    sync();
+    if constexpr (MIXED) {
+      const double* ct = g.pd_centre + 4 * (long)ttgt[e];
+      for (int i = k; i < 2 * qh; i += G) {
+        if (i < q)
+          adj_stage(sd32[gi], i, g.px[tb + i], g.px[pn + tb + i], g.px[2 * pn + tb + i], tbar[tb + i],
+                    tbar[pn + tb + i], tbar[2 * pn + tb + i], ct);
+        else
+          adj_stage_zero(sd32[gi], i);
       }
+      sync();
+      if (act) {
+        const float a0 = ysx + (float)((cs[0] - ct[0]) * kPackScale), a1 = ysy + (float)((cs[1] - ct[1]) * kPackScale),
+                    a2 = ysz + (float)((cs[2] - ct[2]) * kPackScale);
+        const float2 ax = make_float2(a0, a0), ay = make_float2(a1, a1), az = make_float2(a2, a2);
+        float2 qq = make_float2(0.f, 0.f), cx = qq, cy = qq, cz = qq, dx = qq, dy = qq, dz = qq;
+        for (int k2 = 0; k2 < qh; k2++)
+          adj_pair32x2<GUARD>(ax, ay, az, sd32[gi][3 * k2], sd32[gi][3 * k2 + 1], sd32[gi][3 * k2 + 2], eps2, qq, cx,
+                              cy, cz, dx, dy, dz);
+        qb += (double)qq.x + (double)qq.y;
+        bx += ((double)cx.x + (double)cx.y) - 2.0 * ((double)dx.x + (double)dx.y);
+        by += ((double)cy.x + (double)cy.y) - 2.0 * ((double)dy.x + (double)dy.y);
+        bz += ((double)cz.x + (double)cz.y) - 2.0 * ((double)dz.x + (double)dz.y);
+      }
+    } else {
+      for (int i = k; i < q; i += G) {
+        const double x = g.px[tb + i], yy = g.px[pn + tb + i], z = g.px[2 * pn + tb + i];
+        const double a = tbar[tb + i], b = tbar[pn + tb + i], c = tbar[2 * pn + tb + i];
+        sd64[0][base + i] = x;
+        sd64[1][base + i] = yy;
+        sd64[2][base + i] = z;
+        sd64[3][base + i] = b * z - c * yy;
+        sd64[4][base + i] = c * x - a * z;
+        sd64[5][base + i] = a * yy - b * x;
+      }
+      sync();
+      if (act)
+        for (int i = 0; i < q; i++) {
+          const double dx = y.x - sd64[0][base + i], dy = y.y - sd64[1][base + i], dz = y.z - sd64[2][base + i];
+          const double cx = sd64[3][base + i], cy = sd64[4][base + i], cz = sd64[5][base + i];
+          const double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+          double gg = recip_nr(fma(0.5, r2, g.eps));
+          if (GUARD) gg = r2 > 0.0 ? gg : 0.0;
+          const double sdot = fma(cx, dx, fma(cy, dy, cz * dz));
+          qb = fma(gg, sdot, qb);
+          const double t = gg * gg * sdot;
+          bx = fma(gg, cx, fma(-t, dx, bx));
+          by = fma(gg, cy, fma(-t, dy, by));
+          bz = fma(gg, cz, fma(-t, dz, bz));
+        }
+    }
   }
-  if (k >= q) return;
+  if (!act) return;
   const long o = (long)s * q + k;
-  qbar[o] = kBiotSavart * qb;
+  qbar[o] = (MIXED ? kBiotSavart / kPackScale : kBiotSavart) * qb;
   if (s >= g.offset) {
     const long ln = (long)g.leaves * q, l = o - (long)g.offset * q;
     ybar_leaf[l] = kBiotSavart * y.w * bx;
@@ -450,6 +496,20 @@ __global__ void __launch_bounds__(kT) k_spec_interact_T(StepGeom g, const int* _
     ybar_nl[o] = kBiotSavart * y.w * bx;
     ybar_nl[nn + o] = kBiotSavart * y.w * by;
     ybar_nl[2 * nn + o] = kBiotSavart * y.w * bz;
+  }
+}
+
+template <int G>
+void launch_spec_interact_T_g(const StepGeom& g, bool mixed, const int* tstart, const int* ttgt, const double* tbar,
+                              const double4* src, double* qbar, double* ybar_leaf, double* ybar_nl, cudaStream_t st) {
+  const unsigned blocks = (unsigned)((g.panels + kT / G - 1) / (kT / G));
+  const bool guard = !(g.eps > 0);
+  if (mixed) {
+    if (guard) SB_LAUNCH((k_spec_interact_T<G, true, true>), blocks, kT, 0, st, g, tstart, ttgt, tbar, src, qbar, ybar_leaf, ybar_nl);
+    else SB_LAUNCH((k_spec_interact_T<G, false, true>), blocks, kT, 0, st, g, tstart, ttgt, tbar, src, qbar, ybar_leaf, ybar_nl);
+  } else {
+    if (guard) SB_LAUNCH((k_spec_interact_T<G, true, false>), blocks, kT, 0, st, g, tstart, ttgt, tbar, src, qbar, ybar_leaf, ybar_nl);
+    else SB_LAUNCH((k_spec_interact_T<G, false, false>), blocks, kT, 0, st, g, tstart, ttgt, tbar, src, qbar, ybar_leaf, ybar_nl);
   }
 }
 
@@ -489,9 +549,9 @@ __global__ void k_nonleaf_positions_T(StepGeom g, double h, const double* __rest
 
 void launch_spectral_velocity_adjoint(const StepGeom& g, const int* tstart, const int* ttgt, const double* vbar,
                                       const double4* src, double* tbar, double* qbar, double* ybar_leaf,
-                                      double* ybar_nl, cudaStream_t st) {
-  const int q = g.q, P = g.panels;
-  const long pn = (long)P * q, ln = (long)g.leaves * q, off = (long)g.offset * q;
+                                      double* ybar_nl, bool mixed, cudaStream_t st) {
+  const int q = g.q;
+  const long pn = (long)g.panels * q, ln = (long)g.leaves * q, off = (long)g.offset * q;
   // the leaf targets' adjoint is vbar itself (leaf proxies = particles); the
   // downward pass transposed accumulates it up the tree
   cudaMemsetAsync(tbar, 0, sizeof(double) * 3 * pn, st);
@@ -501,12 +561,10 @@ void launch_spectral_velocity_adjoint(const StepGeom& g, const int* tstart, cons
     const long work = (6L << (2 * lev)) * q * 3;
     SB_LAUNCH(k_tree_up3, blocks_for(work, 256), 256, 0, st, g, lev, tbar);
   }
-  if (g.eps > 0)
-    SB_LAUNCH(k_spec_interact_T<false>, (unsigned)P, kT, 0, st, g, tstart, ttgt, tbar, src, qbar, ybar_leaf,
-              ybar_nl);
-  else
-    SB_LAUNCH(k_spec_interact_T<true>, (unsigned)P, kT, 0, st, g, tstart, ttgt, tbar, src, qbar, ybar_leaf,
-              ybar_nl);
+  if (q <= 4) launch_spec_interact_T_g<4>(g, mixed, tstart, ttgt, tbar, src, qbar, ybar_leaf, ybar_nl, st);
+  else if (q <= 16) launch_spec_interact_T_g<16>(g, mixed, tstart, ttgt, tbar, src, qbar, ybar_leaf, ybar_nl, st);
+  else if (q <= 32) launch_spec_interact_T_g<32>(g, mixed, tstart, ttgt, tbar, src, qbar, ybar_leaf, ybar_nl, st);
+  else launch_spec_interact_T_g<kT>(g, mixed, tstart, ttgt, tbar, src, qbar, ybar_leaf, ybar_nl, st);
   // the strengths' upward pass transposed: interpolate their adjoints down
   for (int lev = 0; lev < g.levels - 1; lev++) {
     const long work = (6L << (2 * (lev + 1))) * q;

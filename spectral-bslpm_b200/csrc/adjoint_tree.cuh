@@ -28,7 +28,8 @@ void launch_tree_velocity_adjoint(const TreeGeom& tg, const StepGeom& fg, const 
                                   const double* vbar, const double4* psrc, double* tbar, double* qbl, double* qbar,
                                   double* ybar, bool mixed, cudaStream_t st);
 
-// The reference's spectral FMM (proxy = particle degree), float64: given vbar
+// The reference's spectral FMM (proxy = particle degree; float64, or mixed:
+// float32 transposed pairs on packed coordinates): given vbar
 // [3][leaves*q] and the stage's sources src [panels*q] (displaced proxies,
 // strengths), writes qbar [panels*q] (strength adjoints, leaves final after
 // the strengths' transposed upward pass), ybar_leaf [3][leaves*q] and ybar_nl
@@ -37,7 +38,7 @@ void launch_tree_velocity_adjoint(const TreeGeom& tg, const StepGeom& fg, const 
 // Scratch: tbar [3][panels*q].
 void launch_spectral_velocity_adjoint(const StepGeom& g, const int* tstart, const int* ttgt, const double* vbar,
                                       const double4* src, double* tbar, double* qbar, double* ybar_leaf,
-                                      double* ybar_nl, cudaStream_t st);
+                                      double* ybar_nl, bool mixed, cudaStream_t st);
 // The non-leaf proxies' displacement interpolation reversed: vbar [3][leaves*q]
 // += the adjoint of the previous stage's velocity through ybar_nl (atomics).
 void launch_nonleaf_positions_adjoint(const StepGeom& g, double h, const double* vprev, const double* ybar_nl,

@@ -310,3 +310,21 @@ def test_spectral_fmm_gradient_close_to_direct_sum_adjoint(sb):
     rel_fwd = float((fwd[1] - fwd[0]).norm() / fwd[0].norm())
     print("spectral FMM vs direct sum after 20 steps: vorticity %.2e, adjoint gradient %.2e" % (rel_fwd, rel))
     assert rel <= 1e-3, rel
+
+
+def test_mixed_spectral_fmm_adjoint_step_matches_float64(sb):
+    """The spectral FMM's reverse step in mixed precision (forward recomputed in
+    mixed precision, the transposed interactions in float32 on coordinates
+    packed relative to the panels' centres) against the float64 one."""
+    _, f, w0, wn = gaussian_vortex_state(sb, 5, 0.01, 1e-2)
+    wbar_next = torch.from_numpy(np.random.default_rng(9).standard_normal(tuple(wn.shape))).cuda()
+    out = []
+    for prec in (sb.FP64, sb.MIXED):
+        ctx = sb.Context(sb.config_default(levels=5, interp_degree=3, kernel_eps=1e-4, omega=2 * np.pi, dt=0.01,
+                                           precision=prec, fmm_theta=0.7))
+        wbar = torch.empty_like(wn)
+        ctx.bve_adjoint_step(*f, wn, wbar_next, wbar)
+        out.append(wbar)
+    rel = float((out[1] - out[0]).norm() / out[0].norm())
+    print("mixed vs float64 spectral FMM adjoint step: relative L2 %.2e" % rel)
+    assert rel <= 1e-6, rel
