@@ -194,7 +194,6 @@ __global__ void __launch_bounds__(NT)
   Src* t2 = t1 + tg.npl;
   const int f = blockIdx.x, split = blockIdx.y, nsplit = gridDim.y, npl = tg.npl;
   double* v = out + (long)split * 3 * tg.N;
-  const double* ct = fg.pd_centre + 4 * (long)(fg.offset + f);
   double tx[TPT], ty[TPT], tz[TPT], ax[TPT], ay[TPT], az[TPT], bx[TPT], by[TPT], bz[TPT];
 #pragma unroll
   for (int r = 0; r < TPT; r++) {
@@ -205,7 +204,6 @@ __global__ void __launch_bounds__(NT)
     tz[r] = z[i];
     ax[r] = ay[r] = az[r] = bx[r] = by[r] = bz[r] = 0;
   }
-  (void)ct;
   const float feps = (float)tg.eps;
   for (int e = tg.near_start[f] + split; e < tg.near_start[f + 1]; e += nsplit) {
     const int sl = tg.near_src[e];

@@ -29,7 +29,7 @@ def rh4(x, y, z, area):
     return vor - (vor * area).sum() / (4 * np.pi)
 
 
-def make_ctx(sb, levels, leaf, n, theta, prec, form="staged"):
+def make_ctx(sb, levels, leaf, n, theta, prec):
     cfg = sb.config_default(levels=levels, interp_degree=3, kernel_eps=EPS, omega=OMEGA, dt=DT, fmm_theta=theta,
                             proxy_degree=n, leaf_size=leaf, precision=prec)
     return sb.Context(cfg)
