@@ -128,3 +128,26 @@ def test_config_validation(sb):
         sb.Context(sb.config_default(levels=0))
     with pytest.raises(sb.SbslpmError):
         sb.Context(sb.config_default(precision=sb.MIXED, interp_degree=8))
+
+
+@pytest.mark.parametrize("degree", [1, 2, 3, 4, 6, 8, 10])
+def test_bli_reproduces_polynomials(sb, degree):
+    """Known answer: the barycentric Lagrange basis on a panel's Chebyshev
+    nodes (sbslpm_interp_vals_bli, src/interp_funcs_impl.hpp:11-142)
+    reproduces every tensor-product polynomial of degree <= d exactly."""
+    rng = np.random.default_rng(degree)
+    it = sb.interp_init(degree)
+    lo_x, hi_x, lo_y, hi_y = -0.3, 0.5, -0.2, 0.2
+    X = lo_x + (it[:, 0] + 1) / 2 * (hi_x - lo_x)
+    Y = lo_y + (it[:, 1] + 1) / 2 * (hi_y - lo_y)
+    for _ in range(4):
+        a = rng.standard_normal((degree + 1, degree + 1))
+
+        def p(x, y):
+            return sum(a[i, j] * x ** i * y ** j for i in range(degree + 1) for j in range(degree + 1))
+
+        vals = p(X, Y)
+        for _ in range(8):
+            xi, eta = rng.uniform(lo_x, hi_x), rng.uniform(lo_y, hi_y)
+            b = sb.interp_vals_bli(xi, eta, lo_x, hi_x, lo_y, hi_y, degree)
+            assert abs(b @ vals - p(xi, eta)) <= 1e-12 * max(1.0, abs(p(xi, eta)))
