@@ -46,7 +46,7 @@ PROXY_DEGREE, LEAF_SIZE = 8, 256
 PAIR_FLOP = 17  # FLOP per Biot-Savart pair (division counted as 1)
 # DRAM bytes (read + write) of one near-field launch at this workload, from an
 # ncu capture of one launch (dram__bytes_read.sum + dram__bytes_write.sum)
-NEAR_TRAFFIC = 15.889920e6 + 0.548096e6
+NEAR_TRAFFIC = 15.889664e6 + 0.428032e6
 # The reference's own method (its spectral FMM, proxy degree = particle degree
 # 3, float64) meets the 1e-6 vorticity bar on this workload from theta 0.45
 # down (theta 0.5: 1.35e-6, 0.45: 6.3e-7 after one step against the float64
@@ -1063,6 +1063,7 @@ def main():
     peak64 = sb.measure_fma_peak(1, 50.0) / 1e12
     share = 4 * ms_int / ms_per_step
     tune32, tune64 = ctx32.near_tuning(), ctx64.near_tuning()
+    near_form32 = ctx32.near_form()
     cc32, cc64 = ctx32.cc_tuning(), ctx64.cc_tuning()
     cc32_form = ctx32.cc_form()
     mutual_on, mutual_ms = ctx32.near_mutual()
@@ -1129,6 +1130,8 @@ def main():
                          "leaf tiles, one-member table)",
                          "launch_shape": {"threads": tune32[0], "targets_per_thread": tune32[1],
                                           "splits": tune32[2], "candidates_timed": tune32[3]},
+                         "pair_form": "expanded (8 float32 operations per pair)" if near_form32 else
+                                      "difference (10 float32 operations per pair)",
                          "achieved": achieved, "peak": peak_meas, "unit": "TFLOP/s", "frac": achieved / peak_meas,
                          "traffic": NEAR_TRAFFIC, "traffic_source": "ncu capture of one launch of this kernel on "
                          "this workload (dram__bytes_read.sum + dram__bytes_write.sum)",

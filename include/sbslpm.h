@@ -453,6 +453,12 @@ sbslpm_status sbslpm_batch_set_cc_mode(sbslpm_batch* batch, int mode);
  * in the order of float32 additions.  SBSLPM_ERR_CONFIG for float64 batches.
  * Replaces nothing in the reference (one problem per process there). */
 sbslpm_status sbslpm_batch_set_stage0_shared(sbslpm_batch* batch, int shared);
+/* Mixed-precision batches: the near-field pair form of the members' own near
+ * kernel, as sbslpm_set_near_form (set-up chooses the expanded form when every
+ * member's near list allows it).  A member is bit-exact with a single context
+ * only when both use the same form. */
+sbslpm_status sbslpm_batch_set_near_form(sbslpm_batch* batch, int expanded);
+sbslpm_status sbslpm_batch_near_form(const sbslpm_batch* batch, int* expanded);
 sbslpm_status sbslpm_batch_cc_info(const sbslpm_batch* batch, int* mode, double* union_pairs, double* mma_flops);
 /* Wall time (seconds) of sbslpm_batch_create's list build: every member's
  * tree traversal on the GPU in one launch series, with the lists' CSR
@@ -590,6 +596,19 @@ sbslpm_status sbslpm_near_tuning(const sbslpm_ctx* ctx, int* shape, double* ms_p
  * changes the order of float32 additions only).  *ms_per_launch: its timed
  * launch (with the per-leaf sums). */
 sbslpm_status sbslpm_set_near_mutual(sbslpm_ctx* ctx, int on);
+/* Mixed-precision treecode contexts: the arithmetic of the near-field pair
+ * kernel.  0 = difference form: d = (source - target) in packed float32,
+ * |d|^2 + eps, g d accumulated (10 float32 operations per pair).  1 =
+ * expanded form: |d|^2 + eps = (|s|^2 + eps) + |b|^2 + 2 b.s with the
+ * source's offset s from its leaf centre and b = the target's offset to that
+ * centre, and sum g d = sum r (w s) + b sum r w (8 operations per pair).  The
+ * expanded form rounds the denominator relative to (|b| + |s|)^2 rather than
+ * to |d|; set-up chooses it when eps is at least 3 * 2^-14 times the largest
+ * (|c_S - c_T| + 2 r_T + 2 r_S)^2 / 2 over the near leaf pairs (rounding at
+ * most 2^-10 of eps), else the difference form.  This call overrides the
+ * choice (1 needs kernel_eps > 0). */
+sbslpm_status sbslpm_set_near_form(sbslpm_ctx* ctx, int expanded);
+sbslpm_status sbslpm_near_form(const sbslpm_ctx* ctx, int* expanded);
 sbslpm_status sbslpm_near_mutual(const sbslpm_ctx* ctx, int* on, double* ms_per_launch);
 /* Treecode contexts with 36..121 proxies (proxy_degree 5..10): the launch
  * shape of the well-separated (cluster-cluster) interactions, either one

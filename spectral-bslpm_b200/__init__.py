@@ -182,6 +182,10 @@ def lib() -> ctypes.CDLL:
     L.sbslpm_set_near_mutual.argtypes = [_VP, ctypes.c_int]
     L.sbslpm_set_cc_tuning_bulk.argtypes = [_VP, ctypes.c_int, ctypes.c_int]
     L.sbslpm_near_mutual.argtypes = [_VP, _I, _D]
+    L.sbslpm_set_near_form.argtypes = [_VP, ctypes.c_int]
+    L.sbslpm_near_form.argtypes = [_VP, _I]
+    L.sbslpm_batch_set_near_form.argtypes = [_VP, ctypes.c_int]
+    L.sbslpm_batch_near_form.argtypes = [_VP, _I]
     L.sbslpm_cc_form.argtypes = [_VP, _I]
     L.sbslpm_measure_fma_peak.argtypes = [ctypes.c_int, ctypes.c_double, _D]
     L.sbslpm_bve_velocity.argtypes = [_VP] * 9
@@ -682,6 +686,17 @@ class Context:
         _check(lib().sbslpm_near_mutual(self._h, ctypes.byref(on), ctypes.byref(ms)), "sbslpm_near_mutual")
         return bool(on.value), ms.value
 
+    def set_near_form(self, expanded: bool):
+        """Mixed precision: the near-field pair arithmetic, expanded (8 float32
+        operations per pair; needs kernel_eps > 0) or difference form (10)."""
+        _check(lib().sbslpm_set_near_form(self._h, int(bool(expanded))), "sbslpm_set_near_form")
+
+    def near_form(self) -> bool:
+        """True when the near field runs the expanded pair form."""
+        on = ctypes.c_int()
+        _check(lib().sbslpm_near_form(self._h, ctypes.byref(on)), "sbslpm_near_form")
+        return bool(on.value)
+
     def set_cc_tuning_direct(self, slots: int, chunk_len: int, targets_per_thread: int):
         """Fix the barrier-free form of the mixed-precision well-separated kernel
         (sources read through L1 from a pair-transposed copy) and its shape."""
@@ -818,6 +833,15 @@ class Batch:
         groups of members (True, the default) or run per member (False: bit-exact
         with single contexts)."""
         _check(lib().sbslpm_batch_set_stage0_shared(self._h, 1 if shared else 0), "sbslpm_batch_set_stage0_shared")
+
+    def set_near_form(self, expanded: bool):
+        """The members' near-field pair arithmetic (as Context.set_near_form)."""
+        _check(lib().sbslpm_batch_set_near_form(self._h, int(bool(expanded))), "sbslpm_batch_set_near_form")
+
+    def near_form(self) -> bool:
+        on = ctypes.c_int()
+        _check(lib().sbslpm_batch_near_form(self._h, ctypes.byref(on)), "sbslpm_batch_near_form")
+        return bool(on.value)
 
     def set_cc_mode(self, mode: int):
         """Well-separated interactions: -1 autotuned per proxy-degree group (default for mixed

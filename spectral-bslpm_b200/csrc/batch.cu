@@ -79,6 +79,8 @@ struct sbslpm_batch {
   bool tuned = false;
   int nt = 128, tpt = 2, splits = 2, candidates = 0;
   double tuned_ms = 0;
+  // the mixed near field's pair form (near_expanded_ok for every member's list)
+  bool near_expanded = false;
   static constexpr int kMaxSplits = 4;
 
   cudaGraphExec_t graph = nullptr;
@@ -212,6 +214,9 @@ sbslpm_status batch_setup(sbslpm_batch* b) {
     SB_TRY(device_tree_lists(b->degs[0].t, b->theta, lists, nullptr));
     b->lists_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   }
+  b->near_expanded = mixed;
+  for (int m = 0; m < b->M && b->near_expanded; m++)
+    b->near_expanded = near_expanded_ok(b->degs[0].t, lists[m], b->cfg.kernel_eps);
   for (int mi = 0; mi < b->M; mi++) {
     const int m = by_theta[mi];
     const size_t k = std::lower_bound(uniq.begin(), uniq.end(), b->degree[m]) - uniq.begin();
@@ -425,7 +430,7 @@ void batch_velocity(sbslpm_batch* b, int stage, double dt_s, const double* vprev
                            b->d_gent, x, y, z, b->psrcf, b->near, b->splits, st);
   else
     launch_bltc_near_batch(b->d_mem, b->M, b->Af, b->npl, b->cfg.kernel_eps, prec, x, y, z, b->psrc, b->psrcf,
-                           b->near, b->splits, b->nt, b->tpt, st);
+                           b->near, b->splits, b->nt, b->tpt, b->near_expanded, st);
   if (b->aux_stream) cudaStreamWaitEvent(st, b->ev_join, 0);
   launch_bltc_to_particles_batch(b->d_mem, b->M, b->Af, b->nmax, b->near, b->splits, v, st);
 }
@@ -465,11 +470,11 @@ sbslpm_status batch_autotune(sbslpm_batch* b, const double* x, const double* y, 
     if (sh[0] * sh[1] < b->npl || sh[0] * sh[1] >= 4 * b->npl) continue;
     for (int sp = 1; sp <= sbslpm_batch::kMaxSplits; sp++) {
       launch_bltc_near_batch(b->d_mem, b->M, b->Af, b->npl, b->cfg.kernel_eps, prec, x, y, z, b->psrc, b->psrcf,
-                             b->near, sp, sh[0], sh[1], st);  // warm-up
+                             b->near, sp, sh[0], sh[1], b->near_expanded, st);  // warm-up
       SB_CUDA(cudaEventRecord(e0, st));
       for (int r = 0; r < 3; r++)
         launch_bltc_near_batch(b->d_mem, b->M, b->Af, b->npl, b->cfg.kernel_eps, prec, x, y, z, b->psrc, b->psrcf,
-                               b->near, sp, sh[0], sh[1], st);
+                               b->near, sp, sh[0], sh[1], b->near_expanded, st);
       SB_CUDA(cudaEventRecord(e1, st));
       SB_CUDA(cudaEventSynchronize(e1));
       float ms = 0;
@@ -696,6 +701,25 @@ sbslpm_status sbslpm_batch_set_tuning(sbslpm_batch* b, int threads, int targets_
     cudaGraphExecDestroy(b->graph);
     b->graph = nullptr;
   }
+  return SBSLPM_OK;
+}
+
+sbslpm_status sbslpm_batch_set_near_form(sbslpm_batch* b, int expanded) {
+  if (!b || (expanded != 0 && expanded != 1)) return SBSLPM_ERR_ARG;
+  if (expanded && (b->cfg.precision != SBSLPM_MIXED || !(b->cfg.kernel_eps > 0)))
+    return set_last_error("the expanded near-field form needs mixed precision and kernel_eps > 0"),
+           SBSLPM_ERR_CONFIG;
+  if ((bool)expanded != b->near_expanded && b->graph) {
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  b->near_expanded = expanded != 0;
+  return SBSLPM_OK;
+}
+
+sbslpm_status sbslpm_batch_near_form(const sbslpm_batch* b, int* expanded) {
+  if (!b || !expanded) return SBSLPM_ERR_ARG;
+  *expanded = b->near_expanded ? 1 : 0;
   return SBSLPM_OK;
 }
 

@@ -238,14 +238,16 @@ __global__ void __launch_bounds__(NT)
 // (x0,x1,y0,y1),(z0,z1,w0,w1), so that every operand of the pair arithmetic
 // is a register pair and the paired FP32 instructions of sm_100
 // (FADD2 / FFMA2 / FMUL2) evaluate two pairs per instruction; a missing
-// partner of an odd source count has zero strength (pair32x2).
-template <int NT, int TPT, bool GUARD>
+// partner of an odd source count has zero strength (pair32x2).  EXP: the
+// expanded form (pair32x2_expanded), sources staged as four float4 per two.
+template <int NT, int TPT, bool GUARD, bool EXP>
 __device__ __forceinline__ void bltc_near32_body(const TreeGeom& tg, const StepGeom& fg, int f, int split,
                                                  int nsplit, const double* __restrict__ x,
                                                  const double* __restrict__ y, const double* __restrict__ z,
                                                  const float4* __restrict__ psrcf, double* __restrict__ out) {
+  static_assert(!(GUARD && EXP), "the expanded form needs eps > 0");
   double* v = out + (long)split * 3 * tg.N;  // partial sums of this source split
-  extern __shared__ float4 tilef[];  // [(npl+1)/2][2]
+  extern __shared__ float4 tilef[];  // [(npl+1)/2][EXP ? 4 : 2]
   const int npl = tg.npl, npl2 = (npl + 1) >> 1;
   const double* ct = fg.pd_centre + 4 * (long)(fg.offset + f);
   const double cx = ct[0], cy = ct[1], cz = ct[2];
@@ -272,36 +274,62 @@ __device__ __forceinline__ void bltc_near32_body(const TreeGeom& tg, const StepG
                 bz0 = (float)((cs[2] - cz) * kPackScale);
     __syncthreads();
     for (int k2 = threadIdx.x; k2 < npl2; k2 += NT) {
-      const float4 s0 = psrcf[sb + 2 * k2];
-      const float4 s1 = (2 * k2 + 1 < npl) ? psrcf[sb + 2 * k2 + 1] : make_float4(0.f, 0.f, 0.f, 0.f);
-      tilef[2 * k2] = make_float4(s0.x, s1.x, s0.y, s1.y);
-      tilef[2 * k2 + 1] = make_float4(s0.z, s1.z, s0.w, s1.w);
+      if constexpr (EXP) {
+        dev::stage_expanded(psrcf + sb, k2, npl, feps, tilef + 4 * k2);
+      } else {
+        const float4 s0 = psrcf[sb + 2 * k2];
+        const float4 s1 = (2 * k2 + 1 < npl) ? psrcf[sb + 2 * k2 + 1] : make_float4(0.f, 0.f, 0.f, 0.f);
+        tilef[2 * k2] = make_float4(s0.x, s1.x, s0.y, s1.y);
+        tilef[2 * k2 + 1] = make_float4(s0.z, s1.z, s0.w, s1.w);
+      }
     }
     __syncthreads();
-    float2 fx[TPT], fy[TPT], fz[TPT], bx[TPT], by[TPT], bz[TPT];
+    float2 fx[TPT], fy[TPT], fz[TPT], fw[TPT], bx[TPT], by[TPT], bz[TPT], bb[TPT];
 #pragma unroll
     for (int r = 0; r < TPT; r++) {
-      fx[r] = fy[r] = fz[r] = make_float2(0.f, 0.f);
+      fx[r] = fy[r] = fz[r] = fw[r] = make_float2(0.f, 0.f);
       const float b0 = bx0 - dtx[r], b1 = by0 - dty[r], b2 = bz0 - dtz[r];
-      bx[r] = make_float2(b0, b0);
-      by[r] = make_float2(b1, b1);
-      bz[r] = make_float2(b2, b2);
+      if constexpr (EXP) {  // m = 2b (exact), |b|^2
+        bx[r] = make_float2(2.f * b0, 2.f * b0);
+        by[r] = make_float2(2.f * b1, 2.f * b1);
+        bz[r] = make_float2(2.f * b2, 2.f * b2);
+        const float q = fmaf(b0, b0, fmaf(b1, b1, b2 * b2));
+        bb[r] = make_float2(q, q);
+      } else {
+        bx[r] = make_float2(b0, b0);
+        by[r] = make_float2(b1, b1);
+        bz[r] = make_float2(b2, b2);
+      }
     }
     // unrolled 8 deep (measured: 2.4% faster than 4 for the 128 x 2 shape on the
     // 393,216-particle treecode, 16 no better, 2 slower), registers permitting
 #pragma unroll 8
     for (int k2 = 0; k2 < npl2; k2++) {
-      const float4 A = tilef[2 * k2], B = tilef[2 * k2 + 1];
-      const float2 sx = make_float2(A.x, A.y), sy = make_float2(A.z, A.w), sz = make_float2(B.x, B.y),
-                   sw = make_float2(B.z, B.w);
+      if constexpr (EXP) {
+        const float4 A = tilef[4 * k2], B = tilef[4 * k2 + 1], C = tilef[4 * k2 + 2], D = tilef[4 * k2 + 3];
 #pragma unroll
-      for (int r = 0; r < TPT; r++) pair32x2<GUARD>(bx[r], by[r], bz[r], sx, sy, sz, sw, eps2, fx[r], fy[r], fz[r]);
+        for (int r = 0; r < TPT; r++)
+          dev::pair32x2_expanded(bx[r], by[r], bz[r], bb[r], A, B, C, D, fx[r], fy[r], fz[r], fw[r]);
+      } else {
+        const float4 A = tilef[2 * k2], B = tilef[2 * k2 + 1];
+        const float2 sx = make_float2(A.x, A.y), sy = make_float2(A.z, A.w), sz = make_float2(B.x, B.y),
+                     sw = make_float2(B.z, B.w);
+#pragma unroll
+        for (int r = 0; r < TPT; r++)
+          pair32x2<GUARD>(bx[r], by[r], bz[r], sx, sy, sz, sw, eps2, fx[r], fy[r], fz[r]);
+      }
     }
 #pragma unroll
     for (int r = 0; r < TPT; r++) {
       ax[r] += (double)fx[r].x + (double)fx[r].y;
       ay[r] += (double)fy[r].x + (double)fy[r].y;
       az[r] += (double)fz[r].x + (double)fz[r].y;
+      if constexpr (EXP) {  // + b sum r w, b = m / 2 exactly
+        const double sw = (double)fw[r].x + (double)fw[r].y;
+        ax[r] = fma(0.5 * (double)bx[r].x, sw, ax[r]);
+        ay[r] = fma(0.5 * (double)by[r].x, sw, ay[r]);
+        az[r] = fma(0.5 * (double)bz[r].x, sw, az[r]);
+      }
     }
   }
 #pragma unroll
@@ -318,17 +346,20 @@ __device__ __forceinline__ void bltc_near32_body(const TreeGeom& tg, const StepG
 
 // 256-thread shapes are held to 64 registers (four blocks per SM): on the
 // 393,216-particle treecode the (256 x 1) shape then ran 535 us per launch
-// against 555 us uncapped; the smaller shapes measured slower when capped, so
-// they keep their registers.  The autotuner chooses among all of them.
-template <int NT, int TPT, bool GUARD>
-__global__ void __launch_bounds__(NT, NT >= 256 ? 4 : 1)
+// against 555 us uncapped; the smaller shapes of the difference form measured
+// slower when capped, so they keep their registers.  The 128-thread shapes of
+// the expanded form are held to 128 registers (four blocks per SM: 495.5 us
+// per launch for 128 x 2 against 502.2 us at 138 registers).  The autotuner
+// chooses among all of them.
+template <int NT, int TPT, bool GUARD, bool EXP>
+__global__ void __launch_bounds__(NT, NT >= 256 ? 4 : (EXP && NT == 128 ? 4 : 1))
     k_bltc_near32_batch(const BatchMember* __restrict__ mem, const double* __restrict__ x,
                         const double* __restrict__ y, const double* __restrict__ z,
                         const float4* __restrict__ psrcf, double* __restrict__ out) {
   const TreeGeom tg = mem[blockIdx.z].tg;
   const StepGeom fg = mem[blockIdx.z].fg;
   const long mo = blockIdx.z;
-  bltc_near32_body<NT, TPT, GUARD>(tg, fg, tg.leaf0 + blockIdx.x, blockIdx.y, gridDim.y, x, y, z, psrcf + mo * tg.N,
+  bltc_near32_body<NT, TPT, GUARD, EXP>(tg, fg, tg.leaf0 + blockIdx.x, blockIdx.y, gridDim.y, x, y, z, psrcf + mo * tg.N,
                                    out + mo * gridDim.y * 3 * tg.N);
 }
 
@@ -682,15 +713,20 @@ void launch_bltc_sources_batch(const BatchMember* mem, int members, int leaves, 
 
 void launch_bltc_near_batch(const BatchMember* mem, int members, int leaves, int npl, double eps, int precision,
                             const double* x, const double* y, const double* z, const double4* psrc,
-                            const float4* psrcf, double* near, int splits, int nt, int tpt, cudaStream_t st) {
+                            const float4* psrcf, double* near, int splits, int nt, int tpt, bool expanded,
+                            cudaStream_t st) {
   const bool guard = !(eps > 0);
   const dim3 grid((unsigned)leaves, (unsigned)splits, (unsigned)members);
 #define SB_NEARB(NT, TPT)                                                                                         \
   do {                                                                                                            \
     if (precision == SBSLPM_MIXED) {                                                                              \
-      const size_t sm32 = sizeof(float4) * 2 * ((npl + 1) / 2);                                                  \
-      if (guard) SB_LAUNCH((k_bltc_near32_batch<NT, TPT, true>), grid, NT, sm32, st, mem, x, y, z, psrcf, near);  \
-      else SB_LAUNCH((k_bltc_near32_batch<NT, TPT, false>), grid, NT, sm32, st, mem, x, y, z, psrcf, near);       \
+      const size_t sm32 = sizeof(float4) * (expanded && !guard ? 4 : 2) * ((npl + 1) / 2);                       \
+      if (guard)                                                                                                  \
+        SB_LAUNCH((k_bltc_near32_batch<NT, TPT, true, false>), grid, NT, sm32, st, mem, x, y, z, psrcf, near);    \
+      else if (expanded)                                                                                          \
+        SB_LAUNCH((k_bltc_near32_batch<NT, TPT, false, true>), grid, NT, sm32, st, mem, x, y, z, psrcf, near);    \
+      else                                                                                                        \
+        SB_LAUNCH((k_bltc_near32_batch<NT, TPT, false, false>), grid, NT, sm32, st, mem, x, y, z, psrcf, near);   \
     } else {                                                                                                      \
       const size_t sm64 = sizeof(double4) * npl;                                                                 \
       if (guard) SB_LAUNCH((k_bltc_near64_batch<NT, TPT, true>), grid, NT, sm64, st, mem, x, y, z, psrc, near);   \

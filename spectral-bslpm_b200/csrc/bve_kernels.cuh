@@ -182,9 +182,11 @@ void launch_bltc_near_multi(const BatchMember* mem, const int* perm, int members
 void launch_cc_batch(const BatchMember* mem, const int* idx, int count, int q, int tree_panels, double eps,
                      int precision, cudaStream_t st);
 void launch_downward_batch(const BatchMember* mem, int members, int levels, int qmax, cudaStream_t st);
+// expanded: the mixed kernel's expanded pair form (pair32x2_expanded; eps > 0 only)
 void launch_bltc_near_batch(const BatchMember* mem, int members, int leaves, int npl, double eps, int precision,
                             const double* x, const double* y, const double* z, const double4* psrc,
-                            const float4* psrcf, double* near, int splits, int nt, int tpt, cudaStream_t st);
+                            const float4* psrcf, double* near, int splits, int nt, int tpt, bool expanded,
+                            cudaStream_t st);
 void launch_bltc_to_particles_batch(const BatchMember* mem, int members, int leaves, int nmax, const double* near,
                                     int splits, double* v, cudaStream_t st);
 void launch_depart_remap_batch(const StepGeom& g, const BliTable* tab, int members, const double* x,

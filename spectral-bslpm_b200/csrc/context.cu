@@ -192,6 +192,7 @@ sbslpm_status precompute_tree(sbslpm_ctx* c) {
   c->h_cs = l.cs;
   c->h_csrc = l.csrc;
   c->h_fcentre = t.centre;
+  c->near_expanded = c->cfg.precision == SBSLPM_MIXED && near_expanded_ok(t, l, c->cfg.kernel_eps);
   SB_TRY(upload(&c->near_start, l.ns));
   SB_TRY(upload(&c->near_src, l.nsrc));
   SB_TRY(install_cc_lists(c, l.cs, l.csrc));
@@ -391,7 +392,7 @@ void velocity_eval(sbslpm_ctx* c, int stage, double dt_s, const double* vprev, c
       splits = 1;
     } else {
       launch_bltc_near_batch(c->self, 1, owned_leaves(c), c->npl, c->cfg.kernel_eps, c->cfg.precision, x, y, z, c->psrc,
-                             c->psrcf, c->near, c->near_splits, c->near_nt, c->near_tpt, st);
+                             c->psrcf, c->near, c->near_splits, c->near_nt, c->near_tpt, c->near_expanded, st);
     }
     if (c->aux_stream) cudaStreamWaitEvent(st, c->ev_join, 0);
     launch_bltc_to_particles(c->tgeom, fg, c->ftgt, c->near, splits, v, st);
@@ -591,7 +592,7 @@ sbslpm_status near_autotune(sbslpm_ctx* c, const double* x, const double* y, con
     for (int sp = 1; sp <= 4; sp++) {
       auto run = [&] {
         launch_bltc_near_batch(c->self, 1, owned_leaves(c), c->npl, c->cfg.kernel_eps, prec, x, y, z, c->psrc,
-                               c->psrcf, c->near, sp, sh[0], sh[1], st);
+                               c->psrcf, c->near, sp, sh[0], sh[1], c->near_expanded, st);
       };
       run();
       SB_CUDA(cudaEventRecord(e0, st));
@@ -1184,7 +1185,7 @@ sbslpm_status sbslpm_time_interactions(sbslpm_ctx* c, int reps, double* ms_per_l
     for (int r = 0; r < reps; r++)
       launch_bltc_near_batch(c->self, 1, owned_leaves(c), c->npl, c->cfg.kernel_eps, c->cfg.precision, c->gx,
                              c->gx + c->tgeom.N, c->gx + 2 * c->tgeom.N, c->psrc, c->psrcf, c->near, c->near_splits,
-                             c->near_nt, c->near_tpt, st);
+                             c->near_nt, c->near_tpt, c->near_expanded, st);
     SB_CUDA(cudaEventRecord(b, st));
     SB_CUDA(cudaEventSynchronize(b));
     float tms = 0;
@@ -1301,6 +1302,22 @@ sbslpm_status sbslpm_set_near_mutual(sbslpm_ctx* c, int on) {
            SBSLPM_ERR_CONFIG;
   c->near_mutual = on != 0;
   drop_step_graphs(c);
+  return SBSLPM_OK;
+}
+
+sbslpm_status sbslpm_set_near_form(sbslpm_ctx* c, int expanded) {
+  if (!c || !c->tree || (expanded != 0 && expanded != 1)) return SBSLPM_ERR_ARG;
+  if (expanded && (c->cfg.precision != SBSLPM_MIXED || !(c->cfg.kernel_eps > 0)))
+    return set_last_error("the expanded near-field form needs mixed precision and kernel_eps > 0"),
+           SBSLPM_ERR_CONFIG;
+  c->near_expanded = expanded != 0;
+  drop_step_graphs(c);
+  return SBSLPM_OK;
+}
+
+sbslpm_status sbslpm_near_form(const sbslpm_ctx* c, int* expanded) {
+  if (!c || !c->tree || !expanded) return SBSLPM_ERR_ARG;
+  *expanded = c->near_expanded ? 1 : 0;
   return SBSLPM_OK;
 }
 

@@ -68,6 +68,9 @@ struct sbslpm_ctx {
   double* gx = nullptr;  // [3][particles]: the particle grid, for timing the near kernel alone
   double* near = nullptr;  // [4][3][particles] near-field partial sums (near_splits in use)
   int near_splits = 2, near_nt = 128, near_tpt = 2;  // near-field launch shape (autotuned on the first step)
+  // the mixed near field's pair form: expanded (near_expanded_ok at set-up,
+  // or sbslpm_set_near_form) or difference
+  bool near_expanded = false;
   bool near_tuned = false;
   int near_candidates = 0;
   double near_tuned_ms = 0;
@@ -218,6 +221,10 @@ sbslpm_status build_tree_tables(int L, int d, const std::vector<sbslpm_panel>& g
 // device_tree_lists runs the members' traversals on the GPU in one launch
 // series).
 void build_tree_lists(const TreeTables& t, double theta, TreeLists& l);
+// The mixed near field's pair form for these lists and kernel eps: true = the
+// expanded form (8 paired operations per two pairs), false = the difference
+// form (10); the expanded form only where its rounding stays far below eps.
+bool near_expanded_ok(const TreeTables& t, const TreeLists& l, double eps);
 void tree_lists_from(const TreeTables& t, std::vector<sbslpm_interact_pair>&& list, const std::vector<char>& near,
                      TreeLists& l);
 sbslpm_status device_tree_lists(const TreeTables& t, const std::vector<double>& theta, std::vector<TreeLists>& out,

@@ -81,6 +81,45 @@ __device__ __forceinline__ void pair32x2(const float2 bx, const float2 by, const
   az = __ffma2_rn(g, dz, az);
 }
 
+// Two pairs in the expanded form: with b = base (target side, as above) and
+// s the source's packed offset, |b + s|^2 + eps = (|s|^2 + eps) + |b|^2 +
+// 2 b.s, and sum g (b + s) = sum r (w s) + b sum r w with r = 1/den.  The
+// source side is staged as (x0,x1,y0,y1) (z0,z1,q0,q1) (w0x0,w1x1,w0y0,w1y1)
+// (w0z0,w1z1,w0,w1) with q = |s|^2 + eps, the target side as m = 2b and
+// bb = |b|^2: 4 paired operations for the denominator and 4 for the sums, 8
+// per two pairs against 10 in pair32x2.  The expansion rounds the
+// denominator to u (|b| + |s|)^2 instead of u |b + s| (|b| + |s|), so it is
+// used only where eps dominates that (a coincident pair still adds nothing:
+// its s = -b cancels in the final b sum r w + sum r w s up to rounding of
+// w s / eps).  fx, fy, fz accumulate sum r w s; fw accumulates sum r w.
+__device__ __forceinline__ void pair32x2_expanded(const float2 mx, const float2 my, const float2 mz, const float2 bb,
+                                                  const float4 A, const float4 B, const float4 C, const float4 D,
+                                                  float2& fx, float2& fy, float2& fz, float2& fw) {
+  float2 den = __fadd2_rn(make_float2(B.z, B.w), bb);
+  den = __ffma2_rn(mz, make_float2(B.x, B.y), den);
+  den = __ffma2_rn(my, make_float2(A.z, A.w), den);
+  den = __ffma2_rn(mx, make_float2(A.x, A.y), den);
+  const float2 r = make_float2(recip_f32(den.x), recip_f32(den.y));
+  fx = __ffma2_rn(r, make_float2(C.x, C.y), fx);
+  fy = __ffma2_rn(r, make_float2(C.z, C.w), fy);
+  fz = __ffma2_rn(r, make_float2(D.x, D.y), fz);
+  fw = __ffma2_rn(r, make_float2(D.z, D.w), fw);
+}
+
+// Stages the sources 2k, 2k+1 of a packed float4 array (x, y, z, w) in the
+// expanded form's four float4 (a missing partner past n has zero strength).
+__device__ __forceinline__ void stage_expanded(const float4* __restrict__ src, int k2, int n, float eps,
+                                               float4* __restrict__ out) {
+  const float4 s0 = src[2 * k2];
+  const float4 s1 = (2 * k2 + 1 < n) ? src[2 * k2 + 1] : make_float4(0.f, 0.f, 0.f, 0.f);
+  const float q0 = fmaf(s0.x, s0.x, fmaf(s0.y, s0.y, fmaf(s0.z, s0.z, eps)));
+  const float q1 = fmaf(s1.x, s1.x, fmaf(s1.y, s1.y, fmaf(s1.z, s1.z, eps)));
+  out[0] = make_float4(s0.x, s1.x, s0.y, s1.y);
+  out[1] = make_float4(s0.z, s1.z, q0, q1);
+  out[2] = make_float4(s0.w * s0.x, s1.w * s1.x, s0.w * s0.y, s1.w * s1.y);
+  out[3] = make_float4(s0.w * s0.z, s1.w * s1.z, s0.w, s1.w);
+}
+
 // First panel id of the k-th level below the subtree root (level, root_rel).
 __device__ __forceinline__ int subtree_first(int level, int root_rel, int k) {
   return level_start(level + k) + (root_rel << (2 * k));

@@ -152,6 +152,33 @@ void tree_lists_from(const TreeTables& t, std::vector<sbslpm_interact_pair>&& li
   }
 }
 
+// Whether the mixed near field may evaluate its pairs in the expanded form
+// (pair32x2_expanded).  That form rounds the denominator |b + s|^2 + eps to
+// about 3u (|b| + |s|)^2 (u = 2^-24) where the difference form rounds it
+// relative to |b + s|, so it is chosen only where that rounding stays below
+// 2^-10 of eps for every near pair: eps >= 3 u 2^10 M with M the largest
+// (|c_S - c_T| + 2 r_T + 2 r_S)^2 / 2 over the near leaf pairs (packed
+// coordinates carry the factor 1/sqrt(2); twice the leaf radii leave room for
+// the displaced sources of the later RK stages).  eps = 0 needs the
+// difference form (its coincident pairs are skipped by a test of the
+// denominator).
+bool near_expanded_ok(const TreeTables& t, const TreeLists& l, double eps) {
+  if (!(eps > 0)) return false;
+  const int offf = t.Pf - t.Af;
+  double m = 0;
+  for (int T = 0; T < t.Af; T++)
+    for (int e = l.ns[T]; e < l.ns[T + 1]; e++) {
+      const int S = l.nsrc[e];
+      const double* a = &t.centre[4 * (size_t)(offf + T)];
+      const double* b = &t.centre[4 * (size_t)(offf + S)];
+      const double dx = a[0] - b[0], dy = a[1] - b[1], dz = a[2] - b[2];
+      const double r = std::sqrt(dx * dx + dy * dy + dz * dz) +
+                       2.0 * (t.fpanels[offf + T].radius + t.fpanels[offf + S].radius);
+      m = std::fmax(m, 0.5 * r * r);
+    }
+  return eps >= 3.0 * std::ldexp(1.0, -14) * m;
+}
+
 // Units of the first stage's two-sided near-field kernel from the near lists
 // (CSR by target leaf): (T, S, e, e') for every entry e = (T <- S) with S > T
 // whose mirror e' = (S <- T) is in S's list, (T, S, e, -1) for the diagonal

@@ -47,8 +47,10 @@ def base_cfg(sb, precision, **kw):
                              precision=precision, leaf_size=256, **kw)
 
 
-def single_step(sb, precision, theta, pdeg, xyza, vor, tuning=(128, 2, 2)):
+def single_step(sb, precision, theta, pdeg, xyza, vor, tuning=(128, 2, 2), near_form=None):
     ctx = sb.Context(base_cfg(sb, precision, fmm_theta=theta, proxy_degree=pdeg))
+    if near_form is not None:
+        ctx.set_near_form(near_form)  # the batch's near-field pair arithmetic
     if tuning:
         ctx.set_near_tuning(*tuning)
         ctx.set_cc_tuning(0, 0)  # one block per target panel, the batch's CUDA-core kernel
@@ -70,8 +72,9 @@ def test_batch_equals_single_contexts(sb, precision):
     v = vors.clone()
     vel = torch.zeros((len(THETA), 3) + v.shape[1:], dtype=torch.float64, device="cuda")
     batch.step(*xyza, v, vel)
+    form = batch.near_form() if prec == sb.MIXED else None
     for m in range(len(THETA)):
-        sv, svel = single_step(sb, prec, THETA[m], PDEG[m], xyza, vors[m].contiguous())
+        sv, svel = single_step(sb, prec, THETA[m], PDEG[m], xyza, vors[m].contiguous(), near_form=form)
         assert torch.equal(v[m], sv), m
         assert torch.equal(vel[m], svel), m
 

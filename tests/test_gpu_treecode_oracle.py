@@ -46,9 +46,11 @@ def rh4(x, y, z, area):
     return vor - (vor * area).sum() / (4 * np.pi)
 
 
-def gpu_step(sb, g, vor, **kw):
+def gpu_step(sb, g, vor, near_form=None, **kw):
     cfg = sb.config_default(levels=kw.pop("levels"), interp_degree=3, kernel_eps=EPS, omega=OMEGA, dt=DT, **kw)
     ctx = sb.Context(cfg)
+    if near_form is not None:
+        ctx.set_near_form(near_form)
     v = cuda(vor)
     vel = [torch.zeros_like(v) for _ in range(3)]
     ctx.bve_back_rk4_step(cuda(g.x), cuda(g.y), cuda(g.z), cuda(g.area), v, *vel)
@@ -101,16 +103,58 @@ def test_treecode_error_against_the_direct_sum(sb, port, grid5, n, theta):
         assert err <= 2 * ref_err + slack
 
 
+@pytest.mark.parametrize("levels,leaf,n,theta", [(6, 256, 8, 0.7), (6, 64, 8, 0.7)])
+def test_expanded_near_form_matches_oracle(sb, port, levels, leaf, n, theta):
+    """The mixed near field in the expanded pair form (8 float32 operations per
+    pair: the denominator as (|s|^2 + eps) + |b|^2 + 2 b.s about the source
+    leaf's centre), which set-up chooses at 98,304 particles: within the
+    mixed-precision bar of the oracle's treecode, and of the difference
+    form."""
+    g = sb.build_grid(levels, 3, exact_cc=True)
+    og = port.build(levels, 3, None, exact_cc=True)
+    vor = rh4(g.x, g.y, g.z, g.area)
+    ov, ovel, _ = port.bve_step(og, vor, None, dt=DT, omega=OMEGA, eps=EPS, mode=2, tree=(n, leaf, theta, 0))
+    ovel = np.stack(ovel)
+    kw = dict(levels=levels, fmm_theta=theta, proxy_degree=n, leaf_size=leaf, precision=sb.MIXED)
+    v1, vel1 = gpu_step(sb, g, vor, **kw)  # set-up's choice: the expanded form
+    v0, vel0 = gpu_step(sb, g, vor, near_form=False, **kw)
+    print(f"levels {levels} leaf {leaf}: expanded vs oracle velocity {rel(vel1, ovel):.2e}, vorticity "
+          f"{rel(v1, ov):.2e}; difference form {rel(vel0, ovel):.2e}, {rel(v0, ov):.2e}")
+    assert rel(vel1, ovel) <= MIXED_TOL and rel(v1, ov) <= MIXED_TOL
+    assert rel(vel1, vel0) <= MIXED_TOL and rel(v1, v0) <= MIXED_TOL
+
+
+def test_near_form_chosen_at_set_up(sb):
+    """Set-up keeps the difference form where eps does not dominate the
+    expanded form's rounding (256-particle leaves at 24,576 particles) and
+    takes the expanded one at the headline size; float64 never uses it, and
+    eps = 0 refuses it."""
+    def ctx(levels, **kw):
+        return sb.Context(sb.config_default(levels=levels, interp_degree=3, omega=OMEGA, dt=DT, fmm_theta=0.7,
+                                            proxy_degree=8, leaf_size=256, **kw))
+    assert not ctx(5, kernel_eps=EPS, precision=sb.MIXED).near_form()
+    assert ctx(6, kernel_eps=EPS, precision=sb.MIXED).near_form()
+    assert ctx(7, kernel_eps=EPS, precision=sb.MIXED).near_form()
+    assert not ctx(7, kernel_eps=EPS, precision=sb.FP64).near_form()
+    assert not ctx(7, kernel_eps=0.0, precision=sb.MIXED).near_form()
+    with pytest.raises(sb.SbslpmError):
+        ctx(5, kernel_eps=0.0, precision=sb.MIXED).set_near_form(True)
+    with pytest.raises(sb.SbslpmError):
+        ctx(5, kernel_eps=EPS, precision=sb.FP64).set_near_form(True)
+
+
 def test_headline_configuration_meets_the_bar(sb):
     """393,216 particles, theta 0.7, degree-8 proxies, 256-particle leaves:
-    the mixed and float64 treecode steps within 1e-6 (vorticity) of the
-    float64 direct sum."""
+    the mixed (both near-field pair forms) and float64 treecode steps within
+    1e-6 (vorticity) of the float64 direct sum."""
     g = sb.build_grid(7, 3, exact_cc=True)
     vor = rh4(g.x, g.y, g.z, g.area)
     dv, dvel = gpu_step(sb, g, vor, levels=7, velocity=sb.VEL_DIRECT)
-    for prec in (sb.MIXED, sb.FP64):
-        v, vel = gpu_step(sb, g, vor, levels=7, fmm_theta=0.7, proxy_degree=8, leaf_size=256, precision=prec)
-        print(f"levels 7 prec={prec}: vorticity error {rel(v, dv):.3e}, velocity error {rel(vel, dvel):.3e}")
+    for prec, form in ((sb.MIXED, True), (sb.MIXED, False), (sb.FP64, None)):
+        v, vel = gpu_step(sb, g, vor, near_form=form, levels=7, fmm_theta=0.7, proxy_degree=8, leaf_size=256,
+                          precision=prec)
+        print(f"levels 7 prec={prec} expanded={form}: vorticity error {rel(v, dv):.3e}, "
+              f"velocity error {rel(vel, dvel):.3e}")
         assert rel(v, dv) <= BAR
 
 
