@@ -634,13 +634,21 @@ sbslpm_status sbslpm_cc_tuning(const sbslpm_ctx* ctx, int* shape, double* ms_per
  * cp.async.bulk), double-buffered through mbarriers so that the next panel
  * arrives while the current one is evaluated and no barrier spans the block;
  * its waits are bounded (a copy that never lands gives SBSLPM_ERR_TIMEOUT).
- * The first-step timing includes both; sbslpm_set_cc_tuning_direct and
- * sbslpm_set_cc_tuning_bulk fix one (the chunk length sets the order of the
+ * A fourth form runs one warp per chunk: the lanes hold the target panel's
+ * proxies, ceil(q / 32) per lane, so every staged source pair feeds that many
+ * targets, and each warp stages its own source panels with cp.async into two
+ * buffers of its own (the next entry's panel in flight during the current
+ * one), synchronising with __syncwarp only; `warps` (1, 2, 4 or 8) warps per
+ * block.  All four forms give bit-identical results for the same chunk
+ * length.  The first-step timing includes all of them;
+ * sbslpm_set_cc_tuning_direct, sbslpm_set_cc_tuning_bulk and
+ * sbslpm_set_cc_tuning_warp fix one (the chunk length sets the order of the
  * float64 additions, as above); sbslpm_cc_form reports 0 for the staged
  * form, 1 | 2 (targets per thread) for the barrier-free one, 3 for the
- * bulk-copy one. */
+ * bulk-copy one, 4 for the warp-per-chunk one. */
 sbslpm_status sbslpm_set_cc_tuning_direct(sbslpm_ctx* ctx, int slots, int chunk_len, int targets_per_thread);
 sbslpm_status sbslpm_set_cc_tuning_bulk(sbslpm_ctx* ctx, int slots, int chunk_len);
+sbslpm_status sbslpm_set_cc_tuning_warp(sbslpm_ctx* ctx, int warps, int chunk_len);
 sbslpm_status sbslpm_cc_form(const sbslpm_ctx* ctx, int* targets_per_thread);
 /* CUDA-core fused multiply-add throughput of this GPU, measured with
  * independent FMA chains on every SM for about ms milliseconds: kind 0 =

@@ -181,6 +181,7 @@ def lib() -> ctypes.CDLL:
     L.sbslpm_set_cc_tuning_direct.argtypes = [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     L.sbslpm_set_near_mutual.argtypes = [_VP, ctypes.c_int]
     L.sbslpm_set_cc_tuning_bulk.argtypes = [_VP, ctypes.c_int, ctypes.c_int]
+    L.sbslpm_set_cc_tuning_warp.argtypes = [_VP, ctypes.c_int, ctypes.c_int]
     L.sbslpm_near_mutual.argtypes = [_VP, _I, _D]
     L.sbslpm_set_near_form.argtypes = [_VP, ctypes.c_int]
     L.sbslpm_near_form.argtypes = [_VP, _I]
@@ -708,8 +709,14 @@ class Context:
         source panels copied into shared memory by cp.async.bulk, double-buffered)."""
         _check(lib().sbslpm_set_cc_tuning_bulk(self._h, int(slots), int(chunk_len)), "sbslpm_set_cc_tuning_bulk")
 
+    def set_cc_tuning_warp(self, warps: int, chunk_len: int):
+        """Fix the warp-per-chunk form of the mixed-precision well-separated kernel
+        (ceil(q / 32) target proxies per lane, warp-private cp.async staging)."""
+        _check(lib().sbslpm_set_cc_tuning_warp(self._h, int(warps), int(chunk_len)), "sbslpm_set_cc_tuning_warp")
+
     def cc_form(self) -> int:
-        """0: sources staged in shared memory; 1 | 2: barrier-free, targets per thread; 3: bulk copies."""
+        """0: sources staged in shared memory; 1 | 2: barrier-free, targets per thread; 3: bulk copies;
+        4: warp per chunk."""
         t = ctypes.c_int()
         _check(lib().sbslpm_cc_form(self._h, ctypes.byref(t)), "sbslpm_cc_form")
         return t.value

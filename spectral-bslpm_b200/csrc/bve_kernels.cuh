@@ -126,8 +126,13 @@ void launch_inv_lap(long n, const double* x, const double* y, const double* z, c
 // the packed proxy sources; cc_direct_shape_ok); with direct_tpt =
 // kCcBulkForm: the same slots as the staged form with each slot's source
 // panels brought into shared memory by bulk copies (k_cc32t, double-buffered
-// through mbarriers; cc_chunk_shape_ok).
+// through mbarriers; cc_chunk_shape_ok); with direct_tpt = kCcWarpForm: one
+// warp per chunk, ceil(q / 32) target proxies per lane, `slots` warps per
+// block (1, 2, 4 or 8; cc_warp_shape_ok), each warp staging its source panels
+// from srcp with cp.async and __syncwarp only (k_cc32w).
 constexpr int kCcBulkForm = 3;
+constexpr int kCcWarpForm = 4;
+bool cc_warp_shape_ok(int q, int warps);
 bool cc_chunk_supported(int q);
 bool cc_chunk_shape_ok(int q, int slots);
 bool cc_direct_shape_ok(int q, int slots, int tpt);

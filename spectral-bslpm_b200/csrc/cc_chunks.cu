@@ -335,6 +335,112 @@ __global__ void __launch_bounds__(CcShape<Q, S>::NT)
   p[2 * Q + j] = az;
 }
 
+// Mixed precision, one warp per chunk: the warp's lanes hold the target
+// panel's Q proxies, TPT = ceil(Q / 32) per lane (j = lane + 32 r), so that
+// every staged source pair feeds TPT targets; each warp stages its chunk's
+// source panels in its own two shared-memory buffers with cp.async (16 bytes
+// per lane, the next entry's panel in flight while the current one is
+// evaluated) and synchronises with __syncwarp only -- no barrier spans the
+// block, and warps of a block never wait for each other.  The pair
+// arithmetic and the order of every target's sums are those of k_cc32, so
+// the result is bit-identical to the staged form's.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;"
+               :
+               : "r"((uint32_t)__cvta_generic_to_shared(smem)), "l"(gmem)
+               : "memory");
+}
+
+template <int Q>
+struct CcWarpShape {
+  static constexpr int TPT = (Q + 31) / 32;  // target proxies per lane
+  static constexpr int Q2 = (Q + 1) / 2;
+  static constexpr int NF4 = 2 * Q2;  // float4 per staged source panel
+};
+
+template <int Q, int WPB, bool GUARD>
+__global__ void __launch_bounds__(32 * WPB)
+    k_cc32w(StepGeom g, const int4* __restrict__ chunks, int nchunks, const float4* __restrict__ srcp,
+            double* __restrict__ partial) {
+  using Sh = CcWarpShape<Q>;
+  constexpr int TPT = Sh::TPT, Q2 = Sh::Q2, NF4 = Sh::NF4;
+  __shared__ __align__(16) float4 buf[WPB][2][NF4];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int c = blockIdx.x * WPB + warp;
+  if (c >= nchunks) return;  // the whole warp: nothing below waits on other warps
+  const int4 ch = chunks[c];
+  const int n = ch.z - ch.y;
+  const long pn = (long)g.panels * Q;
+  const double* ct = g.pd_centre + 4 * (long)ch.x;
+  const double cx = ct[0], cy = ct[1], cz = ct[2];
+  float dtx[TPT], dty[TPT], dtz[TPT];
+  double ax[TPT], ay[TPT], az[TPT];
+#pragma unroll
+  for (int r = 0; r < TPT; r++) {
+    const int j = lane + 32 * r;
+    const long o = (long)ch.x * Q + (j < Q ? j : 0);
+    dtx[r] = (float)((g.px[o] - cx) * kPackScale);
+    dty[r] = (float)((g.px[pn + o] - cy) * kPackScale);
+    dtz[r] = (float)((g.px[2 * pn + o] - cz) * kPackScale);
+    ax[r] = ay[r] = az[r] = 0;
+  }
+  auto stage = [&](int e) {  // entry e's source panel into buffer e & 1 (one cp.async group per call)
+    if (e < n) {
+      const float4* s = srcp + (long)__ldg(g.src_panel + ch.y + e) * NF4;
+      float4* d = buf[warp][e & 1];
+      for (int k = lane; k < NF4; k += 32) cp_async16(d + k, s + k);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  stage(0);
+  const float feps = (float)g.eps;
+  const float2 eps2 = make_float2(feps, feps);
+  for (int e = 0; e < n; e++) {
+    stage(e + 1);  // the next panel flies while this one is evaluated
+    asm volatile("cp.async.wait_group 1;" ::: "memory");
+    __syncwarp();
+    const int sp = __ldg(g.src_panel + ch.y + e);
+    const double* cs = g.pd_centre + 4 * (long)sp;
+    const float bx0 = (float)((cs[0] - cx) * kPackScale), by0 = (float)((cs[1] - cy) * kPackScale),
+                bz0 = (float)((cs[2] - cz) * kPackScale);
+    float2 bx[TPT], by[TPT], bz[TPT], fx[TPT], fy[TPT], fz[TPT];
+#pragma unroll
+    for (int r = 0; r < TPT; r++) {
+      const float b0 = bx0 - dtx[r], b1 = by0 - dty[r], b2 = bz0 - dtz[r];
+      bx[r] = make_float2(b0, b0);
+      by[r] = make_float2(b1, b1);
+      bz[r] = make_float2(b2, b2);
+      fx[r] = fy[r] = fz[r] = make_float2(0.f, 0.f);
+    }
+    const float4* tb = buf[warp][e & 1];
+#pragma unroll 4
+    for (int k2 = 0; k2 < Q2; k2++) {
+      const float4 A = tb[2 * k2], B = tb[2 * k2 + 1];
+      const float2 sx = make_float2(A.x, A.y), sy = make_float2(A.z, A.w), sz = make_float2(B.x, B.y),
+                   sw = make_float2(B.z, B.w);
+#pragma unroll
+      for (int r = 0; r < TPT; r++) pair32x2<GUARD>(bx[r], by[r], bz[r], sx, sy, sz, sw, eps2, fx[r], fy[r], fz[r]);
+    }
+#pragma unroll
+    for (int r = 0; r < TPT; r++) {
+      ax[r] += (double)fx[r].x + (double)fx[r].y;
+      ay[r] += (double)fy[r].x + (double)fy[r].y;
+      az[r] += (double)fz[r].x + (double)fz[r].y;
+    }
+    __syncwarp();  // every lane is done with this buffer before stage(e + 2) refills it
+  }
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+  double* p = partial + (long)c * 3 * Q;
+#pragma unroll
+  for (int r = 0; r < TPT; r++) {
+    const int j = lane + 32 * r;
+    if (j >= Q) continue;
+    p[j] = ax[r];
+    p[Q + j] = ay[r];
+    p[2 * Q + j] = az[r];
+  }
+}
+
 // The pair-transposed copy of the packed proxy sources that k_cc32d reads.
 __global__ void k_cc_pair_sources(const float4* __restrict__ srcf, int q, long pairs, float4* __restrict__ srcp) {
   const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
@@ -583,6 +689,21 @@ void launch_bulk_s(const StepGeom& g, const int4* chunks, int nchunks, const flo
 }
 
 template <int Q>
+void launch_warp_q(const StepGeom& g, int warps, const int4* chunks, int nchunks, const float4* srcp,
+                   double* partial, cudaStream_t st) {
+  const bool guard = !(g.eps > 0);
+#define SB_WQ(W)                                                                                          \
+  case W: {                                                                                               \
+    const unsigned grid = (unsigned)((nchunks + W - 1) / W);                                              \
+    if (guard) SB_LAUNCH((k_cc32w<Q, W, true>), grid, 32 * W, 0, st, g, chunks, nchunks, srcp, partial);  \
+    else SB_LAUNCH((k_cc32w<Q, W, false>), grid, 32 * W, 0, st, g, chunks, nchunks, srcp, partial);       \
+    break;                                                                                                \
+  }
+  switch (warps) { SB_WQ(1) SB_WQ(2) SB_WQ(4) default: SB_WQ(8) }
+#undef SB_WQ
+}
+
+template <int Q>
 void launch_bulk_q(const StepGeom& g, int slots, const int4* chunks, int nchunks, const float4* srcp,
                    double* partial, cudaStream_t st) {
   switch (slots) {
@@ -650,7 +771,12 @@ bool cc_chunk_shape_ok(int q, int slots) {
   }
 }
 
+bool cc_warp_shape_ok(int q, int warps) {
+  return cc_chunk_supported(q) && (warps == 1 || warps == 2 || warps == 4 || warps == 8);
+}
+
 int cc_chunk_threads(int q, int slots, int direct_tpt) {
+  if (direct_tpt == kCcWarpForm) return 32 * slots;
   const int qt = direct_tpt > 0 && direct_tpt != kCcBulkForm ? (q + direct_tpt - 1) / direct_tpt : q;
   return (slots * qt + 31) / 32 * 32;
 }
@@ -673,7 +799,12 @@ void launch_cc_chunks(const StepGeom& g, int precision, int slots, const int4* c
                       const double4* src, double* partial, double* out, cudaStream_t st, int direct_tpt,
                       const float4* srcp) {
   const bool mixed = precision == SBSLPM_MIXED;
-  if (nchunks > 0 && mixed && direct_tpt == kCcBulkForm) {
+  if (nchunks > 0 && mixed && direct_tpt == kCcWarpForm) {
+#define SB_WQQ(Q) \
+  case Q: launch_warp_q<Q>(g, slots, chunks, nchunks, srcp, partial, st); break;
+    switch (g.q) { SB_WQQ(36) SB_WQQ(49) SB_WQQ(64) SB_WQQ(81) SB_WQQ(100) SB_WQQ(121) default: break; }
+#undef SB_WQQ
+  } else if (nchunks > 0 && mixed && direct_tpt == kCcBulkForm) {
 #define SB_BQ(Q) \
   case Q: launch_bulk_q<Q>(g, slots, chunks, nchunks, srcp, partial, st); break;
     switch (g.q) { SB_BQ(36) SB_BQ(49) SB_BQ(64) SB_BQ(81) SB_BQ(100) SB_BQ(121) default: break; }

@@ -527,12 +527,15 @@ sbslpm_status cc_autotune(sbslpm_ctx* c) {
   int cand = 0;
   const int keep_slots = c->cc_slots, keep_len = c->cc_len, keep_tpt = c->cc_tpt;
   int best_slots = keep_slots, best_len = keep_len, best_tpt = keep_tpt;
-  // kernel form: 0 staged in shared memory, 1 | 2 barrier-free, 3 bulk copies (mixed precision)
-  const int max_tpt = c->cfg.precision == SBSLPM_MIXED && c->fsrcp ? kCcBulkForm : 0;
+  // kernel form: 0 staged in shared memory, 1 | 2 barrier-free, 3 bulk copies, 4 warp per chunk (mixed precision)
+  const int max_tpt = c->cfg.precision == SBSLPM_MIXED && c->fsrcp ? kCcWarpForm : 0;
   for (int tpt = 0; tpt <= max_tpt; tpt++)
-  for (int sl = tpt > 0 ? 1 : 0; sl <= 8; sl++) {  // chunk slots per block; 0: one block per target panel
+  for (int sl = tpt > 0 ? 1 : 0; sl <= 8; sl++) {  // chunk slots (warps) per block; 0: one block per target panel
     const bool direct = tpt == 1 || tpt == 2;
-    if (sl > 0 && !(direct ? cc_direct_shape_ok(c->qx, sl, tpt) : cc_chunk_shape_ok(c->qx, sl))) continue;
+    const bool shape_ok = tpt == kCcWarpForm ? cc_warp_shape_ok(c->qx, sl)
+                          : direct          ? cc_direct_shape_ok(c->qx, sl, tpt)
+                                            : cc_chunk_shape_ok(c->qx, sl);
+    if (sl > 0 && !shape_ok) continue;
     for (int len = sl > 0 ? 1 : 0; len <= (sl > 0 ? 4 : 0); len++) {
       c->cc_slots = sl;
       c->cc_len = len;
@@ -1283,6 +1286,20 @@ sbslpm_status sbslpm_set_cc_tuning_bulk(sbslpm_ctx* c, int slots, int chunk_len)
   c->cc_slots = slots;
   c->cc_len = chunk_len;
   c->cc_tpt = kCcBulkForm;
+  return SBSLPM_OK;
+}
+
+sbslpm_status sbslpm_set_cc_tuning_warp(sbslpm_ctx* c, int warps, int chunk_len) {
+  if (!c || !c->tree) return SBSLPM_ERR_ARG;
+  if (!c->cc_partial || !c->fsrcp)
+    return set_last_error("the warp-per-chunk well-separated kernel needs mixed precision and 36..121 proxies"),
+           SBSLPM_ERR_CONFIG;
+  if (!cc_warp_shape_ok(c->qx, warps) || chunk_len < 1 || chunk_len > 4)
+    return set_last_error("unsupported well-separated launch shape"), SBSLPM_ERR_ARG;
+  SB_TRY(sbslpm_set_cc_tuning(c, 0, 0));
+  c->cc_slots = warps;
+  c->cc_len = chunk_len;
+  c->cc_tpt = kCcWarpForm;
   return SBSLPM_OK;
 }
 

@@ -1,9 +1,10 @@
 """GPU tests of the treecode's well-separated (cluster-cluster) launch shapes:
 every chunked shape (1..8 chunk slots per block, 1..4 list entries per
 chunk) against the whole-panel kernel, for every proxy count with a chunked
-kernel, in both precisions, and the barrier-free and bulk-copy (TMA)
-mixed-precision forms against the staged one, through the C ABI
-(sbslpm_set_cc_tuning, sbslpm_set_cc_tuning_direct, sbslpm_set_cc_tuning_bulk).
+kernel, in both precisions, and the barrier-free, bulk-copy (TMA) and
+warp-per-chunk mixed-precision forms against the staged one, through the C
+ABI (sbslpm_set_cc_tuning, sbslpm_set_cc_tuning_direct,
+sbslpm_set_cc_tuning_bulk, sbslpm_set_cc_tuning_warp).
 
 The shapes evaluate the same pairs with the same per-source-panel arithmetic
 and differ only in the order in which a target's float64 sums are added, so
@@ -20,6 +21,7 @@ pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
 
 ORDER_TOL = 1e-13
+WARPS = (1, 2, 4, 8)  # warps per block of the warp-per-chunk form
 
 
 def tree_ctx(sb, n, precision, leaf=64):
@@ -116,6 +118,17 @@ def test_barrier_free_form_matches_staged_form(sb, grid, n):
         step(ctx, f)
         assert torch.equal(f["vors"], staged[k]["vors"]), ("bulk", sl, k)
         assert all(torch.equal(a, b) for a, b in zip(f["vel"], staged[k]["vel"])), ("bulk", sl, k)
+    # the warp-per-chunk form: ceil(q / 32) target proxies per lane, warp-private
+    # cp.async staging, __syncwarp only
+    for w in WARPS:
+        for k in (1, 2, 3, 4):
+            ctx.set_cc_tuning_warp(w, k)
+            assert ctx.cc_form() == 4
+            assert ctx.cc_tuning()[:3] == (w, k, 32 * w)
+            f = unit_fields(g, vor)
+            step(ctx, f)
+            assert torch.equal(f["vors"], staged[k]["vors"]), ("warp", w, k)
+            assert all(torch.equal(a, b) for a, b in zip(f["vel"], staged[k]["vel"])), ("warp", w, k)
 
 
 def test_autotuner_times_every_shape(sb, grid):
@@ -124,10 +137,13 @@ def test_autotuner_times_every_shape(sb, grid):
     f = unit_fields(g, vor)
     step(ctx, f)
     sl, k, threads, cand, ms = ctx.cc_tuning()
-    assert cand == 1 + 2 * len(shapes(81)) + len(direct_shapes(81, 1)) + len(direct_shapes(81, 2)) and ms > 0
+    assert cand == (1 + 2 * len(shapes(81)) + len(direct_shapes(81, 1)) + len(direct_shapes(81, 2))
+                    + 4 * len(WARPS)) and ms > 0
     tpt = ctx.cc_form()
     if tpt in (1, 2):
         assert (sl, k) in direct_shapes(81, tpt) and threads == -(-sl * -(-81 // tpt) // 32) * 32
+    elif tpt == 4:
+        assert sl in WARPS and 1 <= k <= 4 and threads == 32 * sl
     else:  # staged or bulk copies: the same shapes
         assert (sl, k, threads) == (0, 0, 128) or ((sl, k) in shapes(81) and threads == -(-sl * 81 // 32) * 32)
     again = unit_fields(g, vor)
@@ -160,6 +176,11 @@ def test_rejects_unsupported_shapes(sb):
         tree_ctx(sb, 6, sb.FP64).set_cc_tuning_bulk(3, 1)
     with pytest.raises(sb.SbslpmError):
         ctx.set_cc_tuning_bulk(1, 1)  # 49 proxies: slots 3, 4, 6, 8
+    for w, k in ((3, 1), (0, 1), (16, 1), (4, 0), (4, 5)):
+        with pytest.raises(sb.SbslpmError):
+            ctx.set_cc_tuning_warp(w, k)
+    with pytest.raises(sb.SbslpmError):  # float64: no warp-per-chunk form
+        tree_ctx(sb, 6, sb.FP64).set_cc_tuning_warp(4, 1)
     small = tree_ctx(sb, 3, sb.MIXED)  # 16 proxies: whole-panel kernel only
     with pytest.raises(sb.SbslpmError):
         small.set_cc_tuning(1, 1)
