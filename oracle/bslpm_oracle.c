@@ -1,4 +1,4 @@
-/* CPU restatement of the reference's BVE backward semi-Lagrangian hot path.
+/* CPU restatement of the reference's BVE and SWE backward semi-Lagrangian hot path.
  *
  * TEST INFRASTRUCTURE ONLY: the checker for the CUDA path and the "port"
  * CPU baseline.  The product library never links or calls this file.
@@ -1310,4 +1310,425 @@ void orc_downward_pass(int levels, int degree, const orc_panel* p, const double*
   orc_downward_pass_3(levels, degree, p, interp, t, z, z + (size_t)P * q, s, zs, zs + (size_t)orc_leaf_count(levels) * q);
   free(z);
   free(zs);
+}
+
+/* ---------------- shallow water v2 ---------------- */
+
+/* One panel-pair block of swe_vel_panel_interaction_2
+ * (src/fmm_interactions/swe_vel_impl.hpp:104-146): the rotational term at the
+ * displaced, re-projected source points, the divergent term at the fixed
+ * source points; per target, the two terms of source k are added in that
+ * order (the reference's two atomic adds per component). */
+static void swe_pair_block(const orc_panel* p, const double* interp, int q, int t, int s, const double* dx,
+                           const double* dy, const double* dz, const double* sv, const double* sd, double eps,
+                           double* t1, double* t2, double* t3) {
+  double fx[MAXQ][3], mv[MAXQ][3];
+  for (int k = 0; k < q; k++) {
+    proxy_point(p, s, interp, k, fx[k]);
+    double x_s = fx[k][0] + dx[(size_t)s * q + k], y_s = fx[k][1] + dy[(size_t)s * q + k],
+           z_s = fx[k][2] + dz[(size_t)s * q + k];
+    project_to_sphere(&x_s, &y_s, &z_s);
+    mv[k][0] = x_s;
+    mv[k][1] = y_s;
+    mv[k][2] = z_s;
+  }
+  for (int j = 0; j < q; j++) {
+    double xt[3];
+    proxy_point(p, t, interp, j, xt);
+    double a1 = t1[(size_t)t * q + j], a2 = t2[(size_t)t * q + j], a3 = t3[(size_t)t * q + j];
+    for (int k = 0; k < q; k++) {
+      const double* m = mv[k];
+      const double* f = fx[k];
+      double dp = xt[0] * m[0] + xt[1] * m[1] + xt[2] * m[2];
+      double dp2 = xt[0] * f[0] + xt[1] * f[1] + xt[2] * f[2];
+      double g1 = -(0.07957747154594767 / (1.0 - dp + eps)) * sv[(size_t)s * q + k];
+      double g2 = 0.07957747154594767 / (1.0 - dp2 + eps) * sd[(size_t)s * q + k];
+      a1 += g1 * (xt[1] * m[2] - xt[2] * m[1]);
+      a2 += g1 * (xt[2] * m[0] - xt[0] * m[2]);
+      a3 += g1 * (xt[0] * m[1] - xt[1] * m[0]);
+      a1 += g2 * (f[0] - xt[0] * dp2);
+      a2 += g2 * (f[1] - xt[1] * dp2);
+      a3 += g2 * (f[2] - xt[2] * dp2);
+    }
+    t1[(size_t)t * q + j] = a1;
+    t2[(size_t)t * q + j] = a2;
+    t3[(size_t)t * q + j] = a3;
+  }
+}
+
+/* swe_vel_interactions_2: src/fmm_interactions/swe_vel.cpp:39-67 with one
+ * rank; grouped by target panel as orc_bve_vel_interactions. */
+void orc_swe_vel_interactions(int levels, int degree, const orc_panel* p, const double* interp, long n_list,
+                              const int* list, const double* disp_x, const double* disp_y, const double* disp_z,
+                              const double* src_vor, const double* src_div, double eps, double* t1, double* t2,
+                              double* t3) {
+  int q = (degree + 1) * (degree + 1), P = orc_panel_count(levels);
+  long* start = (long*)calloc((size_t)P + 1, sizeof(long));
+  long* order = (long*)malloc(sizeof(long) * (size_t)(n_list > 0 ? n_list : 1));
+  long* fill = (long*)malloc(sizeof(long) * (size_t)P);
+  for (long i = 0; i < n_list; i++) start[list[3 * i] + 1]++;
+  for (int i = 0; i < P; i++) start[i + 1] += start[i];
+  for (int i = 0; i < P; i++) fill[i] = start[i];
+  for (long i = 0; i < n_list; i++) order[fill[list[3 * i]]++] = i;
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int t = 0; t < P; t++)
+    for (long e = start[t]; e < start[t + 1]; e++)
+      swe_pair_block(p, interp, q, t, list[3 * order[e] + 1], disp_x, disp_y, disp_z, src_vor, src_div, eps, t1, t2,
+                     t3);
+  free(start);
+  free(order);
+  free(fill);
+}
+
+/* The three-point finite-difference derivative along one direction of a
+ * (d+1) x (d+1) panel grid, fd_deriv_xi / fd_deriv_eta
+ * (src/deriv_funcs_impl.hpp:94-185): node k at cos(k pi / d) scaled to
+ * [lo, hi], one-sided second-order weights at the two end nodes, the
+ * non-uniform centred weights inside (the shorter neighbouring gap is h).
+ * Values of the line are f[base + k * stride]; xi lines have stride d + 1
+ * (base = the eta index), eta lines stride 1 (base = xi index * (d + 1)). */
+static void fd_line(double* out, const double* f, int d, double lo, double hi, int base, int stride) {
+  const double scale = 0.5 * (hi - lo), off = 0.5 * (hi + lo);
+  {
+    const double n0 = hi, n1 = cos(ORC_PI / d) * scale + off, n2 = cos(ORC_PI * 2.0 / d) * scale + off;
+    const double h = n0 - n1, ratio = (n0 - n2) / (n0 - n1);
+    const double w0 = -1.0 - 1.0 / ratio, w1 = ratio / (ratio - 1.0), w2 = -1.0 / (ratio * ratio - ratio);
+    int a = base;
+    out[a] = (w0 * f[a] + w1 * f[a + stride] + w2 * f[a + 2 * stride]) / h;
+    a = base + d * stride;
+    out[a] = -(w0 * f[a] + w1 * f[a - stride] + w2 * f[a - 2 * stride]) / h;
+  }
+  for (int k = 1; k < d; k++) {
+    const double n0 = cos((k - 1) * ORC_PI / d) * scale + off, n1 = cos(k * ORC_PI / d) * scale + off,
+                 n2 = cos((k + 1) * ORC_PI / d) * scale + off;
+    const double g1 = n0 - n1, g2 = n1 - n2, h = fmin(g1, g2), ratio = fmax(g1 / h, g2 / h);
+    double w0, w1, w2;
+    if (g1 < g2) {
+      w0 = -ratio / (ratio + 1.0);
+      w1 = (ratio - 1.0) / ratio;
+      w2 = 1.0 / (ratio * ratio + ratio);
+    } else {
+      w0 = -1.0 / (ratio * ratio + ratio);
+      w1 = (1.0 - ratio) / ratio;
+      w2 = ratio / (ratio + 1.0);
+    }
+    const int a = base + k * stride;
+    out[a] = (w0 * f[a - stride] + w1 * f[a] + w2 * f[a + stride]) / h;
+  }
+}
+
+static void fd_xi(double* out, const double* f, int d, double lo, double hi) {
+  for (int j = 0; j <= d; j++) fd_line(out, f, d, lo, hi, j, d + 1);
+}
+
+static void fd_eta(double* out, const double* f, int d, double lo, double hi) {
+  for (int i = 0; i <= d; i++) fd_line(out, f, d, lo, hi, i * (d + 1), 1);
+}
+
+/* spatial_filter_vals (src/deriv_funcs_impl.hpp:391-441): each value takes
+ * (1 - c) of itself plus c / 4 of a distance-weighted pair of neighbours in
+ * each direction (the two nearer nodes on the reference interval [-1, 1]),
+ * c = 0.0005. */
+static void spatial_filter(double* out, const double* f, int d) {
+  const double c = 0.0005;
+  for (int i = 0; i <= d; i++) {
+    const double xi = cos(ORC_PI * i / d);
+    const int ia = i == 0 ? 1 : i - 1, ib = i == 0 ? 2 : (i == d ? i - 2 : i + 1);
+    const double xd1 = fabs(xi - cos(ORC_PI * ia / d)), xd2 = fabs(xi - cos(ORC_PI * ib / d));
+    for (int j = 0; j <= d; j++) {
+      const double eta = cos(ORC_PI * j / d);
+      const int ja = j == 0 ? 1 : j - 1, jb = j == 0 ? 2 : (j == d ? j - 2 : j + 1);
+      const double ed1 = fabs(eta - cos(ORC_PI * ja / d)), ed2 = fabs(eta - cos(ORC_PI * jb / d));
+      const int k = i * (d + 1) + j;
+      const double f1 = f[ia * (d + 1) + j], f2 = f[ib * (d + 1) + j], f3 = f[i * (d + 1) + ja],
+                   f4 = f[i * (d + 1) + jb];
+      double v = (1.0 - c) * f[k];
+      v += 0.25 * c / (xd1 + xd2) * xd1 * f2;
+      v += 0.25 * c / (xd1 + xd2) * xd2 * f1;
+      v += 0.25 * c / (ed1 + ed2) * ed1 * f4;
+      v += 0.25 * c / (ed1 + ed2) * ed2 * f3;
+      out[k] = v;
+    }
+  }
+}
+
+/* The panel's node tangents X = tan(xi), Y = tan(eta) at node (i, j). */
+static void node_tan(int d, int i, int j, double min_xi, double max_xi, double min_eta, double max_eta, double* X,
+                     double* Y) {
+  const double xi = cos(ORC_PI * i / d) * (0.5 * (max_xi - min_xi)) + 0.5 * (min_xi + max_xi);
+  const double eta = cos(ORC_PI * j / d) * (0.5 * (max_eta - min_eta)) + 0.5 * (min_eta + max_eta);
+  *X = tan(xi);
+  *Y = tan(eta);
+}
+
+/* single_panel_lap_fd (src/deriv_funcs_impl.hpp:510-560): the surface
+ * Laplacian in gnomonic coordinates from the finite differences (the mixed
+ * derivative as the mean of the two orders), then the spatial filter. */
+static void panel_lap(double* out, const double* f, double mnx, double mxx, double mne, double mxe, int d) {
+  double fx[MAXQ], fe[MAXQ], fxx[MAXQ], fee[MAXQ], fxe[MAXQ], fex[MAXQ], lap[MAXQ];
+  fd_xi(fx, f, d, mnx, mxx);
+  fd_eta(fe, f, d, mne, mxe);
+  fd_xi(fxx, fx, d, mnx, mxx);
+  fd_eta(fee, fe, d, mne, mxe);
+  fd_eta(fxe, fx, d, mne, mxe);
+  fd_xi(fex, fe, d, mnx, mxx);
+  for (int i = 0; i <= d; i++)
+    for (int j = 0; j <= d; j++) {
+      const int k = i * (d + 1) + j;
+      double X, Y;
+      node_tan(d, i, j, mnx, mxx, mne, mxe, &X, &Y);
+      const double C2 = 1 + X * X, D2 = 1 + Y * Y, delta = 1 + X * X + Y * Y;
+      const double mix = 0.5 * (fxe[k] + fex[k]);
+      lap[k] = delta * (fxx[k] / C2 + fee[k] / D2 + 2.0 * X * Y / (C2 * D2) * mix);
+    }
+  spatial_filter(out, lap, d);
+}
+
+/* single_panel_curl_rad_comp_fd (src/deriv_funcs_impl.hpp:591-619): the
+ * radial component of the curl of the tangent field (a, b) given by its
+ * gnomonic components, then the spatial filter. */
+static void panel_curl_rad(double* out, const double* a, const double* b, double mnx, double mxx, double mne,
+                           double mxe, int d) {
+  double ax[MAXQ], bx[MAXQ], ae[MAXQ], be[MAXQ], curl[MAXQ];
+  fd_xi(ax, a, d, mnx, mxx);
+  fd_xi(bx, b, d, mnx, mxx);
+  fd_eta(ae, a, d, mne, mxe);
+  fd_eta(be, b, d, mne, mxe);
+  for (int i = 0; i <= d; i++)
+    for (int j = 0; j <= d; j++) {
+      const int k = i * (d + 1) + j;
+      double X, Y;
+      node_tan(d, i, j, mnx, mxx, mne, mxe, &X, &Y);
+      const double C = sqrt(1 + X * X), D = sqrt(1 + Y * Y), delta = 1 + X * X + Y * Y;
+      curl[k] = -sqrt(delta) * (X * Y / (C * D) * (be[k] / D - ax[k] / C) - ae[k] / D + bx[k] / C);
+    }
+  spatial_filter(out, curl, d);
+}
+
+/* single_panel_div_fd (src/deriv_funcs_impl.hpp:661-698): the divergence of
+ * the tangent field (a, b), no filter. */
+static void panel_div(double* out, const double* a, const double* b, double mnx, double mxx, double mne, double mxe,
+                      int d) {
+  double as[MAXQ], bs[MAXQ], ax[MAXQ], be[MAXQ];
+  for (int i = 0; i <= d; i++)
+    for (int j = 0; j <= d; j++) {
+      const int k = i * (d + 1) + j;
+      double X, Y;
+      node_tan(d, i, j, mnx, mxx, mne, mxe, &X, &Y);
+      const double delta = 1 + X * X + Y * Y;
+      as[k] = a[k] / sqrt(delta);
+      bs[k] = b[k] / sqrt(delta);
+    }
+  fd_xi(ax, as, d, mnx, mxx);
+  fd_eta(be, bs, d, mne, mxe);
+  for (int i = 0; i <= d; i++)
+    for (int j = 0; j <= d; j++) {
+      const int k = i * (d + 1) + j;
+      double X, Y;
+      node_tan(d, i, j, mnx, mxx, mne, mxe, &X, &Y);
+      const double C = sqrt(1 + X * X), D = sqrt(1 + Y * Y), delta = 1 + X * X + Y * Y;
+      out[k] = pow(delta, 1.5) / (C * D) * (ax[k] / C + be[k] / D);
+    }
+}
+
+/* xietavec_from_xyzvec (src/cubed_sphere_transforms_impl.hpp:242-276): a
+ * tangent vector's gnomonic components at (x, y, z), from its longitude and
+ * colatitude components; within 1e-16 of a pole the x and y components. */
+static void xieta_vec(double* xc, double* ec, double vx, double vy, double vz, double x, double y, double z) {
+  double xe[2];
+  xieta_from_xyz(x, y, z, xe);
+  const int face = face_from_xyz(x, y, z);
+  if (!(fabs(z) < 1 - 1e-16)) {
+    *xc = vx;
+    *ec = vy;
+    return;
+  }
+  const double lon = (-y * vx + x * vy) / sqrt(x * x + y * y);
+  const double colat = ((x * vx + y * vy) * z - (x * x + y * y) * vz) / sqrt(x * x + y * y);
+  const double X = tan(xe[0]), Y = tan(xe[1]), X2 = X * X, Y2 = Y * Y;
+  const double C = sqrt(1 + X2), D = sqrt(1 + Y2), delta = 1 + X2 + Y2;
+  if (face <= 3) {
+    *xc = C * D / sqrt(delta) * lon;
+    *ec = -1.0 * colat + X * Y / sqrt(delta) * lon;
+  } else {
+    const double sg = face == 4 ? 1.0 : -1.0;
+    *xc = sg / sqrt(X2 + Y2) * (D * X * colat - D * Y / sqrt(delta) * lon);
+    *ec = sg / sqrt(X2 + Y2) * (C * Y * colat + C * X / sqrt(delta) * lon);
+  }
+}
+
+/* swe_tendency_computation_2 (src/swe_time_step_2_impl.hpp:41-127): per leaf
+ * panel, the vorticity tendency -delta (zeta + 2 Omega z) - 2 Omega v_z, the
+ * divergence tendency curl_r((zeta + 2 Omega z) v) - (g/a) lap(surface) -
+ * lap(|v|^2 / 2) and the height tendency div(h v), the last two zero within
+ * 1e-5 of the poles.  The reference hard-codes g/a = 9.81 / 6371000. */
+void orc_swe_tendencies(int levels, int degree, const orc_panel* p, const double* x, const double* y,
+                        const double* z, const double* vx, const double* vy, const double* vz, const double* vors,
+                        const double* divs, const double* height, const double* surface, double omega,
+                        double g_over_a, double* vor_t, double* div_t, double* h_t) {
+  const int d = degree, q = (d + 1) * (d + 1), P = orc_panel_count(levels), A = orc_leaf_count(levels);
+  const int off = P - A;
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < A; i++) {
+    const orc_panel* pp = &p[i + off];
+    const double mnx = ORC_PI / 4.0 * pp->min_xi, mxx = ORC_PI / 4.0 * pp->max_xi;
+    const double mne = ORC_PI / 4.0 * pp->min_eta, mxe = ORC_PI / 4.0 * pp->max_eta;
+    double va[MAXQ], vb[MAXQ], ha[MAXQ], hb[MAXQ], sf[MAXQ], ke[MAXQ];
+    double curl[MAXQ], hlap[MAXQ], klap[MAXQ], hdiv[MAXQ];
+    for (int j = 0; j < q; j++) {
+      const size_t o = (size_t)i * q + j;
+      xieta_vec(&va[j], &vb[j], vx[o], vy[o], vz[o], x[o], y[o], z[o]);
+      ha[j] = height[o] * va[j];
+      hb[j] = height[o] * vb[j];
+      const double zetaf = vors[o] + 2 * omega * z[o];
+      va[j] *= zetaf;
+      vb[j] *= zetaf;
+      sf[j] = surface[o];
+      ke[j] = 0.5 * (vx[o] * vx[o] + vy[o] * vy[o] + vz[o] * vz[o]);
+    }
+    panel_curl_rad(curl, va, vb, mnx, mxx, mne, mxe, d);
+    panel_lap(hlap, sf, mnx, mxx, mne, mxe, d);
+    panel_lap(klap, ke, mnx, mxx, mne, mxe, d);
+    panel_div(hdiv, ha, hb, mnx, mxx, mne, mxe, d);
+    for (int j = 0; j < q; j++) {
+      const size_t o = (size_t)i * q + j;
+      const double abs_vor = vors[o] + 2.0 * omega * z[o];
+      vor_t[o] = -divs[o] * abs_vor - 2.0 * omega * vz[o];
+      div_t[o] = curl[j] - hlap[j] * g_over_a - klap[j];
+      h_t[o] = hdiv[j];
+      if (1.0 - fabs(z[o]) < 1e-5) {
+        div_t[o] = 0.0;
+        h_t[o] = 0.0;
+      }
+    }
+  }
+}
+
+/* unify_boundary_vals (src/initialize_cubed_sphere.cpp:364-370): every copy
+ * of a point shared by panels takes the mean of the copies (sums in panel
+ * order).  map: [leaf][q] -> distinct point, counts: copies per point. */
+void orc_swe_unify(int n, const int* map, const int* counts, int points, double* vals) {
+  double* acc = (double*)calloc((size_t)points, sizeof(double));
+  for (int i = 0; i < n; i++) acc[map[i]] += vals[i];
+  for (int i = 0; i < n; i++) vals[i] = acc[map[i]] / counts[map[i]];
+  free(acc);
+}
+
+/* One velocity evaluation of the SWE step: vorticity strengths (area_v x
+ * vor) and divergence strengths (area x div) up, the two-field interactions
+ * at the displacement (dx, dy, dz), down into vel (3 x A x q). */
+static void swe_velocity(const orc_swe_problem* pb, const double* area_v, const double* vor, const double* div,
+                         const double* dx, const double* dy, const double* dz, double* sv, double* sd, double* t1,
+                         double* t2, double* t3, double* vel) {
+  const int q = (pb->degree + 1) * (pb->degree + 1), P = orc_panel_count(pb->levels), A = orc_leaf_count(pb->levels);
+  const size_t n = (size_t)A * q, pq = (size_t)P * q;
+  orc_upward_pass(pb->levels, pb->degree, pb->panels, pb->interp, area_v, vor, sv);
+  orc_upward_pass(pb->levels, pb->degree, pb->panels, pb->interp, pb->area, div, sd);
+  memset(t1, 0, sizeof(double) * pq);
+  memset(t2, 0, sizeof(double) * pq);
+  memset(t3, 0, sizeof(double) * pq);
+  orc_swe_vel_interactions(pb->levels, pb->degree, pb->panels, pb->interp, pb->n_list, pb->list, dx, dy, dz, sv, sd,
+                           pb->kernel_eps, t1, t2, t3);
+  memset(vel, 0, sizeof(double) * 3 * n);
+  orc_downward_pass_3(pb->levels, pb->degree, pb->panels, pb->interp, t1, t2, t3, vel, vel + n, vel + 2 * n);
+}
+
+/* swe_back_rk4_step_2 (src/swe_time_step_2.cpp:785-1035), topography none
+ * (the effective height is the height).  Stage s > 0 displaces the sources
+ * by dt_s times the previous stage's velocity (dt/2, dt/2, dt; leaves, then
+ * the non-leaf proxies interpolated, swe_displacement_upward_pass_2
+ * :486-496) and evaluates the velocity of the sources with the previous
+ * stage's tendencies applied over dt/2 (swe_apply_tendencies_2 :384-414, the
+ * vorticity strength with the area scaled by 1 + dt/2 div); after every
+ * stage the reference unifies the first stage's velocity (its
+ * unify_boundary_vals calls name vel_x/y/z), so that velocity is unified four
+ * times and the later ones never.  Tendencies of stages 1-3 (the fourth
+ * reaches no result) use the original vorticity and divergence with the
+ * stage's height, minus the base divergence and height tendencies
+ * (modify_tendencies :765-783), unified.  Arrival values are forward Euler
+ * with the first tendencies (swe_compute_arrival_values_2 :555-626; its
+ * interpolations of the later vorticity tendencies reach no output and are
+ * not evaluated), the departure search is the BVE one on the four stage
+ * velocities (swe_find_departure_points_2 :663-763), and the arrival
+ * vorticity and the tracers are remapped without a planetary term
+ * (swe_departure_to_target_2 :40-64). */
+void orc_swe_step(const orc_swe_problem* pb, double* vors, double* divs, double* height, double* vel_x,
+                  double* vel_y, double* vel_z, double* tracers) {
+  const int d = pb->degree, q = (d + 1) * (d + 1), P = orc_panel_count(pb->levels), A = orc_leaf_count(pb->levels);
+  const int off = P - A, T = pb->tracer_count;
+  const size_t n = (size_t)A * q, pq = (size_t)P * q;
+  double* dx = (double*)calloc(pq, sizeof(double));
+  double* dy = (double*)calloc(pq, sizeof(double));
+  double* dz = (double*)calloc(pq, sizeof(double));
+  double* sv = (double*)calloc(pq, sizeof(double));
+  double* sd = (double*)calloc(pq, sizeof(double));
+  double* t1 = (double*)calloc(pq, sizeof(double));
+  double* t2 = (double*)calloc(pq, sizeof(double));
+  double* t3 = (double*)calloc(pq, sizeof(double));
+  double* v[4];
+  double* tend[3];
+  for (int k = 0; k < 4; k++) v[k] = (double*)calloc(3 * n, sizeof(double));
+  for (int k = 0; k < 3; k++) tend[k] = (double*)calloc(3 * n, sizeof(double));
+  double* dvor = (double*)calloc(n, sizeof(double));
+  double* ddiv = (double*)calloc(n, sizeof(double));
+  double* dh = (double*)calloc(n, sizeof(double));
+  double* darea = (double*)calloc(n, sizeof(double));
+  double* dep = (double*)calloc(3 * n, sizeof(double));
+  double* nv = (double*)calloc(n, sizeof(double));
+  double* ntr = (double*)calloc(n * (T > 0 ? T : 1), sizeof(double));
+  const double fr[3] = {0.5, 0.5, 1.0};
+  for (int s = 0; s < 4; s++) {
+    const double* hs = height;  /* the stage's height (and surface) */
+    if (s == 0) {
+      swe_velocity(pb, pb->area, vors, divs, dx, dy, dz, sv, sd, t1, t2, t3, v[0]);
+    } else {
+      const double h = fr[s - 1] * pb->dt, ha = 0.5 * pb->dt;
+      const double* vp = v[s - 1];
+      for (int i = 0; i < A; i++)
+        for (int j = 0; j < q; j++) {
+          const size_t o = (size_t)i * q + j, g = (size_t)(i + off) * q + j;
+          dx[g] = h * vp[o];
+          dy[g] = h * vp[n + o];
+          dz[g] = h * vp[2 * n + o];
+        }
+      disp_interp(pb->panels, off, d, pb->interp, dx, dy, dz);
+      const double* tp = tend[s - 1];
+      for (size_t o = 0; o < n; o++) {
+        dvor[o] = vors[o] + ha * tp[o];
+        ddiv[o] = divs[o] + ha * tp[n + o];
+        dh[o] = height[o] + ha * tp[2 * n + o];
+        darea[o] = pb->area[o] * (1.0 + ha * divs[o]);
+      }
+      swe_velocity(pb, darea, dvor, ddiv, dx, dy, dz, sv, sd, t1, t2, t3, v[s]);
+      hs = dh;
+    }
+    for (int c = 0; c < 3; c++) orc_swe_unify((int)n, pb->map, pb->counts, pb->point_count, v[0] + c * n);
+    if (s < 3) {
+      double* tq = tend[s];
+      orc_swe_tendencies(pb->levels, d, pb->panels, pb->x, pb->y, pb->z, v[s], v[s] + n, v[s] + 2 * n, vors, divs,
+                         hs, hs, pb->omega, pb->g_over_a, tq, tq + n, tq + 2 * n);
+      for (size_t o = 0; o < n; o++) {
+        tq[n + o] -= pb->base_div[o];
+        tq[2 * n + o] -= pb->base_h[o];
+      }
+      for (int c = 0; c < 3; c++) orc_swe_unify((int)n, pb->map, pb->counts, pb->point_count, tq + c * n);
+    }
+  }
+  /* arrival values and the departure search */
+  for (size_t o = 0; o < n; o++) {
+    nv[o] = vors[o] + pb->dt * tend[0][o];
+    divs[o] = divs[o] + pb->dt * tend[0][n + o];
+    height[o] = height[o] + pb->dt * tend[0][2 * n + o];
+  }
+  orc_bve_departure(pb->levels, d, pb->panels, pb->x, pb->y, pb->z, v[0], v[1], v[2], v[3], pb->dt, dep, dep + n,
+                    dep + 2 * n);
+  orc_bve_remap(pb->levels, d, pb->panels, pb->z, dep, dep + n, dep + 2 * n, nv, T, tracers, 0.0, vors, ntr);
+  if (T > 0) memcpy(tracers, ntr, sizeof(double) * n * T);
+  memcpy(vel_x, v[0], sizeof(double) * n);
+  memcpy(vel_y, v[0] + n, sizeof(double) * n);
+  memcpy(vel_z, v[0] + 2 * n, sizeof(double) * n);
+  free(dx); free(dy); free(dz); free(sv); free(sd); free(t1); free(t2); free(t3);
+  for (int k = 0; k < 4; k++) free(v[k]);
+  for (int k = 0; k < 3; k++) free(tend[k]);
+  free(dvor); free(ddiv); free(dh); free(darea); free(dep); free(nv); free(ntr);
 }

@@ -106,6 +106,38 @@ void orc_bltc_velocity_swe(int levels, int degree, int leaf_size, int n, double 
                            const double* sz, const double* w, const double* dx, const double* dy, const double* dz,
                            const double* wd, double* u);
 
+/* Shallow water v2.  swe_vel_interactions_2 (src/fmm_interactions/swe_vel.cpp:39-67,
+ * accumulating into t1..t3), swe_tendency_computation_2
+ * (src/swe_time_step_2_impl.hpp:41-127, outputs overwritten; the reference's
+ * g/a is 9.81 / 6371000), unify_boundary_vals (src/initialize_cubed_sphere.cpp:364-370)
+ * over n values with the [leaf][q] -> point map and the copies per point,
+ * and one swe_back_rk4_step_2 (src/swe_time_step_2.cpp:785-1035, topography
+ * none): vors, divs, height, tracers in-out, vel_* out (the first stage's
+ * velocity). */
+void orc_swe_vel_interactions(int levels, int degree, const orc_panel* p, const double* interp, long n_list,
+                              const int* list, const double* disp_x, const double* disp_y, const double* disp_z,
+                              const double* src_vor, const double* src_div, double eps, double* t1, double* t2,
+                              double* t3);
+void orc_swe_tendencies(int levels, int degree, const orc_panel* p, const double* x, const double* y,
+                        const double* z, const double* vx, const double* vy, const double* vz, const double* vors,
+                        const double* divs, const double* height, const double* surface, double omega,
+                        double g_over_a, double* vor_t, double* div_t, double* h_t);
+void orc_swe_unify(int n, const int* map, const int* counts, int points, double* vals);
+typedef struct {
+  int levels, degree, tracer_count;
+  double kernel_eps, omega, dt, g_over_a;
+  const orc_panel* panels;
+  const double* interp;
+  const double *x, *y, *z, *area;
+  long n_list;
+  const int* list;
+  const int *map, *counts; /* the grid's point map (cubed_sphere_2d_to_1d) */
+  int point_count;
+  const double *base_div, *base_h; /* base tendencies (the vorticity's is not used by the reference) */
+} orc_swe_problem;
+void orc_swe_step(const orc_swe_problem* pb, double* vors, double* divs, double* height, double* vel_x,
+                  double* vel_y, double* vel_z, double* tracers);
+
 /* direct_sum_inv_lap (src/direct_sum_impl.hpp:20-27) over n points. */
 void orc_direct_sum_inv_lap(int n, const double* x, const double* y, const double* z, const double* area,
                             const double* pots, double* soln);

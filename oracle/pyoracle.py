@@ -1,7 +1,7 @@
 """ctypes access to the two oracle libraries (test infrastructure only).
 
 * ``Port``: oracle/liboracle_port.so, the plain-C restatement of the
-  reference's BVE hot path (oracle/bslpm_oracle.c).  Builds from this
+  reference's BVE and SWE hot path (oracle/bslpm_oracle.c).  Builds from this
   repository alone, so it is the checker on machines without the reference.
 * ``Ref``: oracle/_ref/libsbslpm_ref.so, the reference's own src/*.cpp built
   against the shim headers by oracle/Makefile (present where it was built).
@@ -68,6 +68,31 @@ class OrcProblem(ctypes.Structure):
     ]
 
 
+class OrcSweProblem(ctypes.Structure):
+    _fields_ = [
+        ("levels", ctypes.c_int),
+        ("degree", ctypes.c_int),
+        ("tracer_count", ctypes.c_int),
+        ("kernel_eps", ctypes.c_double),
+        ("omega", ctypes.c_double),
+        ("dt", ctypes.c_double),
+        ("g_over_a", ctypes.c_double),
+        ("panels", ctypes.POINTER(OrcPanel)),
+        ("interp", _D),
+        ("x", _D),
+        ("y", _D),
+        ("z", _D),
+        ("area", _D),
+        ("n_list", ctypes.c_long),
+        ("list", _I),
+        ("map", _I),
+        ("counts", _I),
+        ("point_count", ctypes.c_int),
+        ("base_div", _D),
+        ("base_h", _D),
+    ]
+
+
 def panels_to_arrays(panels) -> tuple[np.ndarray, np.ndarray]:
     """(ints P x 13, dbls P x 6) in the column order of ref_get_panels."""
     P = len(panels)
@@ -93,6 +118,7 @@ class Port:
         L.orc_bve_step.argtypes = [ctypes.POINTER(OrcProblem), _D, _D, _D, _D, _D]
         L.orc_interp_to_latlon.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(OrcPanel), _D, ctypes.c_int,
                                            _D, ctypes.c_int, _D, _D]
+        L.orc_swe_step.argtypes = [ctypes.POINTER(OrcSweProblem)] + [_D] * 7
 
     # ---- setup -------------------------------------------------------------
     def build(self, levels: int, degree: int, theta: float | None, exact_cc: bool = False):
@@ -191,6 +217,57 @@ class Port:
             pb.time = float(time) + k * dt
             self.lib.orc_bve_step(ctypes.byref(pb), _dp(v), _dp(vx), _dp(vy), _dp(vz), _dp(tr))
         return v, (vx, vy, vz), (tr if T else None)
+
+    # ---- shallow water v2 --------------------------------------------------
+    def swe_vel_interactions(self, g, dx, dy, dz, src_vor, src_div, eps):
+        P, q = src_vor.shape
+        t = [np.zeros((P, q)) for _ in range(3)]
+        lst = np.ascontiguousarray(g["list"], dtype=np.int32)
+        a = [np.ascontiguousarray(v, dtype=np.float64) for v in (dx, dy, dz, src_vor, src_div)]
+        self.lib.orc_swe_vel_interactions(g["levels"], g["degree"], g["panels"], _dp(g["interp"]),
+                                          ctypes.c_long(len(lst)), _ip(lst), *[_dp(v) for v in a],
+                                          ctypes.c_double(eps), _dp(t[0]), _dp(t[1]), _dp(t[2]))
+        return t
+
+    def swe_tendencies(self, g, vel, vors, divs, height, surface, omega, g_over_a):
+        A, q = g["x"].shape
+        out = [np.zeros((A, q)) for _ in range(3)]
+        a = [np.ascontiguousarray(v, dtype=np.float64) for v in (*vel, vors, divs, height, surface)]
+        self.lib.orc_swe_tendencies(g["levels"], g["degree"], g["panels"], _dp(g["x"]), _dp(g["y"]), _dp(g["z"]),
+                                    *[_dp(v) for v in a], ctypes.c_double(omega), ctypes.c_double(g_over_a),
+                                    *[_dp(o) for o in out])
+        return out
+
+    def swe_unify(self, vals, smap, counts):
+        v = np.array(vals, dtype=np.float64, order="C")
+        m = np.ascontiguousarray(smap, dtype=np.int32)
+        c = np.ascontiguousarray(counts, dtype=np.int32)
+        self.lib.orc_swe_unify(ctypes.c_int(v.size), _ip(m), _ip(c), ctypes.c_int(c.size), _dp(v))
+        return v
+
+    def swe_step(self, g, vors, divs, height, base, smap, counts, tracers=None, *, dt, omega, eps, g_over_a,
+                 nsteps=1, driver_unify=False):
+        """nsteps of swe_back_rk4_step_2 (base = the three base tendencies);
+        driver_unify: the driver's unify of vors, divs and height after each
+        step.  Returns (vors, divs, height, (vx, vy, vz), tracers)."""
+        A, q = g["x"].shape
+        T = 0 if tracers is None else tracers.shape[2]
+        lst = np.ascontiguousarray(g["list"], dtype=np.int32)
+        m = np.ascontiguousarray(smap, dtype=np.int32)
+        c = np.ascontiguousarray(counts, dtype=np.int32)
+        bd, bh = (np.ascontiguousarray(b, dtype=np.float64) for b in (base[1], base[2]))
+        pb = OrcSweProblem(g["levels"], g["degree"], T, eps, omega, dt, g_over_a, g["panels"], _dp(g["interp"]),
+                           _dp(g["x"]), _dp(g["y"]), _dp(g["z"]), _dp(g["area"]), len(lst), _ip(lst), _ip(m),
+                           _ip(c), int(c.size), _dp(bd), _dp(bh))
+        v, d, h = (np.array(a, dtype=np.float64, order="C") for a in (vors, divs, height))
+        tr = np.zeros(1) if tracers is None else np.array(tracers, dtype=np.float64, order="C")
+        vel = [np.zeros((A, q)) for _ in range(3)]
+        for _ in range(nsteps):
+            self.lib.orc_swe_step(ctypes.byref(pb), _dp(v), _dp(d), _dp(h), *[_dp(a) for a in vel], _dp(tr))
+            if driver_unify:
+                for a in (v, d, h):
+                    self.lib.orc_swe_unify(ctypes.c_int(a.size), _ip(m), _ip(c), ctypes.c_int(c.size), _dp(a))
+        return v, d, h, tuple(vel), (tr if T else None)
 
     # ---- treecode (decoupled proxy degree) ---------------------------------
     def bltc_shape(self, levels, degree, leaf_size):

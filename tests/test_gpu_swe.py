@@ -1,7 +1,9 @@
 """GPU parity tests of the shallow-water (SWE v2) step, through the C ABI.
 
-Checker: golden vectors made by the reference itself (tests/golden/swe_*.npz,
-tests/golden/make_golden_swe.py).  Tolerances (relative L-infinity, scaled by
+Checkers: golden vectors made by the reference itself (tests/golden/swe_*.npz,
+tests/golden/make_golden_swe.py), and at 24,576 particles the oracle's C
+restatement of swe_back_rk4_step_2 (oracle/bslpm_oracle.c, pinned bit for
+bit to those vectors by tests/test_oracle_swe.py).  Tolerances (relative L-infinity, scaled by
 the largest reference magnitude of the field):
   float64 path            <= 1e-12 (step, tendencies, interactions, set-up)
   unify_boundary_vals     bit-exact (same summation order, IEEE operations)
@@ -225,6 +227,32 @@ def test_swe_mixed_close_to_fp64_other_degrees(sb, degree):
     c32.swe_run(*s32.args(), nsteps=3)
     assert rel(s32.vors, s64.vors) <= MIXED_TOL
     assert rel(s32.height, s64.height) <= MIXED_TOL
+
+
+@pytest.mark.parametrize("precision,tol", [("FP64", FP64_TOL), ("MIXED", MIXED_TOL)])
+def test_swe_steps_match_c_oracle_levels5(sb, port, precision, tol):
+    """24,576 particles (beyond the golden fixtures), the benchmark's unit-sphere
+    flow: one step, then two more of the driver's loop (step + unify), against
+    the oracle's restatement on the same inputs and base tendencies."""
+    ctx, s = unit_sphere_state(sb, 5, getattr(sb, precision))
+    g = port.build(5, 3, 0.7, exact_cc=True)
+    host = lambda t: t.detach().cpu().numpy()
+    assert np.array_equal(g["x"], host(s.x)) and np.array_equal(g["area"], host(s.area))
+    smap, counts = sb.cubed_sphere_2d_to_1d(g["x"], g["y"], g["z"], 3)
+    base = [host(b) for b in s.base]
+    kw = dict(dt=0.002, omega=2 * np.pi, eps=1e-4, g_over_a=1.0)
+    ov, od, oh, ovel, _ = port.swe_step(g, host(s.vors), host(s.divs), host(s.height), base, smap, counts, **kw)
+    ctx.swe_back_rk4_step_2(*s.args())
+    errs = [rel(s.vors, ov), rel(s.divs, od), rel(s.height, oh), rel(torch.stack(s.vel), np.stack(ovel))]
+    print(f"{precision} one step vs the C oracle: vorticity {errs[0]:.2e}, divergence {errs[1]:.2e}, "
+          f"height {errs[2]:.2e}, velocity {errs[3]:.2e}")
+    assert max(errs) <= tol
+    for f in (s.vors, s.divs, s.height):
+        ctx.unify_boundary_vals(f)
+    ov, od, oh = (port.swe_unify(a, smap, counts) for a in (ov, od, oh))
+    ctx.swe_run(*s.args(), nsteps=2)
+    ov, od, oh, ovel, _ = port.swe_step(g, ov, od, oh, base, smap, counts, nsteps=2, driver_unify=True, **kw)
+    assert rel(s.vors, ov) <= 10 * tol and rel(s.height, oh) <= 10 * tol
 
 
 def test_swe_steady_flow_stays_steady(sb):
