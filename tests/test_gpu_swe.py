@@ -233,7 +233,10 @@ def test_swe_mixed_close_to_fp64_other_degrees(sb, degree):
 def test_swe_steps_match_c_oracle_levels5(sb, port, precision, tol):
     """24,576 particles (beyond the golden fixtures), the benchmark's unit-sphere
     flow: one step, then two more of the driver's loop (step + unify), against
-    the oracle's restatement on the same inputs and base tendencies."""
+    the oracle's restatement on the same inputs and base tendencies.  The
+    divergence of this balanced flow is the difference of nearly equal
+    tendencies (a rounding-level field after the first step), so its error is
+    measured on the vorticity's scale."""
     ctx, s = unit_sphere_state(sb, 5, getattr(sb, precision))
     g = port.build(5, 3, 0.7, exact_cc=True)
     host = lambda t: t.detach().cpu().numpy()
@@ -243,7 +246,8 @@ def test_swe_steps_match_c_oracle_levels5(sb, port, precision, tol):
     kw = dict(dt=0.002, omega=2 * np.pi, eps=1e-4, g_over_a=1.0)
     ov, od, oh, ovel, _ = port.swe_step(g, host(s.vors), host(s.divs), host(s.height), base, smap, counts, **kw)
     ctx.swe_back_rk4_step_2(*s.args())
-    errs = [rel(s.vors, ov), rel(s.divs, od), rel(s.height, oh), rel(torch.stack(s.vel), np.stack(ovel))]
+    on_vor = lambda a, b: float(np.abs(host(a) - b).max() / np.abs(ov).max())
+    errs = [rel(s.vors, ov), on_vor(s.divs, od), rel(s.height, oh), rel(torch.stack(s.vel), np.stack(ovel))]
     print(f"{precision} one step vs the C oracle: vorticity {errs[0]:.2e}, divergence {errs[1]:.2e}, "
           f"height {errs[2]:.2e}, velocity {errs[3]:.2e}")
     assert max(errs) <= tol
@@ -252,7 +256,7 @@ def test_swe_steps_match_c_oracle_levels5(sb, port, precision, tol):
     ov, od, oh = (port.swe_unify(a, smap, counts) for a in (ov, od, oh))
     ctx.swe_run(*s.args(), nsteps=2)
     ov, od, oh, ovel, _ = port.swe_step(g, ov, od, oh, base, smap, counts, nsteps=2, driver_unify=True, **kw)
-    assert rel(s.vors, ov) <= 10 * tol and rel(s.height, oh) <= 10 * tol
+    assert rel(s.vors, ov) <= 10 * tol and rel(s.height, oh) <= 10 * tol and on_vor(s.divs, od) <= 10 * tol
 
 
 def test_swe_steady_flow_stays_steady(sb):
