@@ -608,12 +608,8 @@ void launch_tree_velocity_adjoint(const TreeGeom& tg, const StepGeom& fg, const 
   }
   // near field, transposed (writes qbar, ybar), then the anterpolation adjoint (adds)
   const size_t sm = sizeof(double) * 6 * tg.npl;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_tree_near_T<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
-    cudaFuncSetAttribute(k_tree_near_T<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
-    attr = true;
-  }
+  static std::atomic<unsigned long long> attr{0};
+  raise_smem_once(attr, 64 * 1024, k_tree_near_T<false>, k_tree_near_T<true>);
   const int nth = tg.npl <= 256 ? 256 : 512;
   if (mixed) {
     const size_t sm32 = sizeof(float4) * 3 * ((tg.npl + 1) / 2);

@@ -688,11 +688,8 @@ void launch_bltc_sources(const TreeGeom& tg, const StepGeom& fg, const BliTable&
                          const double* area, double4* psrc, float4* psrcf, double4* proxy, bool mixed,
                          cudaStream_t st) {
   size_t smem = sizeof(double) * ((size_t)tg.npl * (tg.n + 1) * 2 + tg.npl + kThreads);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_bltc_sources, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr = true;
-  }
+  static std::atomic<unsigned long long> attr{0};
+  raise_smem_once(attr, 200 * 1024, k_bltc_sources);
   SB_LAUNCH(k_bltc_sources, (unsigned)fg.leaves, kThreads, smem, st, tg, fg, tab, stage, dt_s, vprev, x, y, z, vors,
             area, psrc, psrcf, proxy, mixed ? 1 : 0);
 }
@@ -702,11 +699,8 @@ void launch_bltc_sources_batch(const BatchMember* mem, int members, int leaves, 
                                const double* vors, const double* area, double4* psrc, float4* psrcf, bool mixed,
                                cudaStream_t st) {
   size_t smem = sizeof(double) * ((size_t)npl * (nmax + 1) * 2 + npl + kThreads);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_bltc_sources_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr = true;
-  }
+  static std::atomic<unsigned long long> attr{0};
+  raise_smem_once(attr, 200 * 1024, k_bltc_sources_batch);
   SB_LAUNCH(k_bltc_sources_batch, dim3((unsigned)leaves, (unsigned)members), kThreads, smem, st, mem, stage, dt_s,
             vprev, x, y, z, vors, area, psrc, mixed ? psrcf : nullptr, mixed ? 1 : 0);
 }

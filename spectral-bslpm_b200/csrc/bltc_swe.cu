@@ -286,11 +286,8 @@ void launch_bltc_swe_sources(const TreeGeom& tg, const StepGeom& fg, const BliTa
                              const double* gcentre, int gq, cudaStream_t st) {
   const int n1 = tg.n + 1, qx = n1 * n1, G = kThreads / qx > 0 ? kThreads / qx : 1;
   const size_t smem = sizeof(double) * ((size_t)tg.npl * n1 * 2 + 2 * (size_t)tg.npl + 2 * (size_t)G * qx);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_bltc_swe_sources, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr = true;
-  }
+  static std::atomic<unsigned long long> attr{0};
+  raise_smem_once(attr, 200 * 1024, k_bltc_swe_sources);
   SB_LAUNCH(k_bltc_swe_sources, (unsigned)fg.leaves, kThreads, smem, st, tg, fg, tab, stage, dtd, dts, vprev, tprev,
             x, y, z, vors, divs, area, dispx, dispy, dispz, wv, wd, psrc, psrcf, psrc2, psrcf2, proxy, proxy2,
             mixed ? 1 : 0, gcentre, gq);

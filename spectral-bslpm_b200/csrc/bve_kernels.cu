@@ -20,8 +20,8 @@
 
 namespace sbslpm {
 
-long& launch_counter() {
-  static long n = 0;
+std::atomic<long>& launch_counter() {
+  static std::atomic<long> n{0};
   return n;
 }
 
@@ -1328,11 +1328,8 @@ static size_t subtree_smem(int q, int fields, int D) {
 void launch_upward_fused(const StepGeom& g, int mode, int stage, double dt_s, const double* vprev, const double* x,
                          const double* y, const double* z, const double* vors, const double* area, double4* src,
                          bool mixed, cudaStream_t st) {
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_upward_subtree, cudaFuncAttributeMaxDynamicSharedMemorySize, 164 * 1024);
-    attr = true;
-  }
+  static std::atomic<unsigned long long> attr{0};
+  raise_smem_once(attr, 164 * 1024, k_upward_subtree);
   const int Dmax = subtree_depth(g.q);
   int r = g.levels - 1;  // the bottom of the next subtree
   const long nl = (long)g.offset * g.q;  // non-leaf proxy points
@@ -1353,11 +1350,8 @@ void launch_upward_fused(const StepGeom& g, int mode, int stage, double dt_s, co
 }
 
 void launch_upward_batch(const BatchMember* mem, int members, int levels, int qmax, bool mixed, cudaStream_t st) {
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_upward_subtree_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, 164 * 1024);
-    attr = true;
-  }
+  static std::atomic<unsigned long long> attr{0};
+  raise_smem_once(attr, 164 * 1024, k_upward_subtree_batch);
   const int Dmax = subtree_depth(qmax);
   int r = levels - 1;
   do {
@@ -1370,11 +1364,8 @@ void launch_upward_batch(const BatchMember* mem, int members, int levels, int qm
 }
 
 void launch_downward_batch(const BatchMember* mem, int members, int levels, int qmax, cudaStream_t st) {
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_downward_subtree_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, 164 * 1024);
-    attr = true;
-  }
+  static std::atomic<unsigned long long> attr{0};
+  raise_smem_once(attr, 164 * 1024, k_downward_subtree_batch);
   const int Dmax = subtree_depth(qmax);
   int r = 0;
   while (r < levels - 1) {
@@ -1407,11 +1398,8 @@ void launch_cc_batch(const BatchMember* mem, const int* idx, int count, int q, i
 }
 
 void launch_downward_fused(const StepGeom& g, double* tgt, double* leaf_out, cudaStream_t st) {
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_downward_subtree, cudaFuncAttributeMaxDynamicSharedMemorySize, 164 * 1024);
-    attr = true;
-  }
+  static std::atomic<unsigned long long> attr{0};
+  raise_smem_once(attr, 164 * 1024, k_downward_subtree);
   const int Dmax = subtree_depth(g.q);
   int r = 0;
   while (r < g.levels - 1) {

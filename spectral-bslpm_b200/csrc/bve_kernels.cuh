@@ -4,6 +4,8 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include <vector>
 
 #include "geometry.cuh"
@@ -200,6 +202,7 @@ void launch_depart_remap_batch(const StepGeom& g, const BliTable* tab, int membe
                                cudaStream_t st);
 
 // Counts every kernel launched through the wrappers above.
-long& launch_counter();
+// Kernel launches made by the library (a process-wide diagnostic count).
+std::atomic<long>& launch_counter();
 
 }  // namespace sbslpm

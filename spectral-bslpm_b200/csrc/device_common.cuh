@@ -5,6 +5,8 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include "bve_kernels.cuh"
 
 namespace sbslpm {
@@ -306,7 +308,22 @@ inline unsigned blocks_for(long n, int t) { return (unsigned)((n + t - 1) / t); 
 
 }  // namespace dev
 
-long& launch_counter();
+// Kernel launches made by the library (a process-wide diagnostic count).
+std::atomic<long>& launch_counter();
+
+// Raises kernels' dynamic shared-memory limit on the current device, once per
+// device (the attribute is per device: a process that drives several GPUs
+// must set it on each).  done: the caller's static record of the devices set
+// (device ordinals >= 64 are set on every call).
+template <typename... K>
+inline void raise_smem_once(std::atomic<unsigned long long>& done, int bytes, K... kernels) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return;
+  const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
+  if (bit && (done.load(std::memory_order_acquire) & bit)) return;
+  (cudaFuncSetAttribute(kernels, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes), ...);
+  if (bit) done.fetch_or(bit, std::memory_order_acq_rel);
+}
 
 }  // namespace sbslpm
 

@@ -617,11 +617,8 @@ void launch_swe_upward(const StepGeom& g, const SweGeom& s, int stage, double dt
                        const double* tprev, const double*, const double*, const double*, const double* vors,
                        const double* divs, const double* area, double4* src, double4* src2, bool mixed,
                        cudaStream_t st) {
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_swe_upward_subtree, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr = true;
-  }
+  static std::atomic<unsigned long long> attr{0};
+  raise_smem_once(attr, 200 * 1024, k_swe_upward_subtree);
   const int Dmax = g.q <= 25 ? 3 : 1;
   int r = g.levels - 1;
   const long nl = (long)g.offset * g.q;  // non-leaf proxy points
