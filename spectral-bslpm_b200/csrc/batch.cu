@@ -22,6 +22,7 @@ using namespace sbslpm;
 
 struct sbslpm_batch {
   sbslpm_config cfg{};
+  int device = 0;  // the device current at creation: buffers and streams live there
   int M = 0, L = 0, d = 0, q = 0, P = 0, A = 0, off = 0;
   long N = 0;
   std::vector<double> theta;
@@ -581,6 +582,7 @@ sbslpm_status sbslpm_batch_create(const sbslpm_config* base, int members, const 
     return SBSLPM_ERR_NO_DEVICE;
   }
   sbslpm_batch* b = new sbslpm_batch();
+  cudaGetDevice(&b->device);
   b->cfg = c;
   b->M = members;
   b->theta.assign(theta, theta + members);
@@ -626,6 +628,7 @@ sbslpm_status sbslpm_batch_step(sbslpm_batch* b, const double* x, const double* 
   if (!b || bad(x) || bad(y) || bad(z) || bad(area) || bad(vors) || bad(vel)) return SBSLPM_ERR_ARG;
   if (any_on_host({x, y, z, area, vors, vel}))
     return set_last_error("device-pointer step given host memory"), SBSLPM_ERR_ARG;
+  SB_TRY(on_device(b->device, "the batch"));
   SB_TRY(batch_autotune(b, x, y, z, area, vors));
   batch_enqueue_step(b, x, y, z, area, vors, vel);
   return batch_finish(b);
@@ -636,6 +639,7 @@ sbslpm_status sbslpm_batch_run(sbslpm_batch* b, const double* x, const double* y
   if (!b || bad(x) || bad(y) || bad(z) || bad(area) || bad(vors) || bad(vel) || nsteps < 0) return SBSLPM_ERR_ARG;
   if (any_on_host({x, y, z, area, vors, vel}))
     return set_last_error("device-pointer step given host memory"), SBSLPM_ERR_ARG;
+  SB_TRY(on_device(b->device, "the batch"));
   SB_TRY(batch_autotune(b, x, y, z, area, vors));
   const void* key[7] = {x, y, z, area, vors, vel, nullptr};
   cudaStream_t st = b->stream();

@@ -777,6 +777,7 @@ sbslpm_status sbslpm_create(const sbslpm_config* cfg, sbslpm_ctx** out) {
   }
   sbslpm_ctx* c = new sbslpm_ctx();
   c->cfg = *cfg;
+  cudaGetDevice(&c->device);
   c->L = cfg->levels;
   c->d = cfg->interp_degree;
   c->q = (c->d + 1) * (c->d + 1);
@@ -1027,6 +1028,7 @@ sbslpm_status sbslpm_bve_velocity(sbslpm_ctx* c, const double* x, const double* 
     return SBSLPM_ERR_ARG;
   if (any_on_host({x, y, z, area, vors, vel_x, vel_y, vel_z}))
     return set_last_error("device pointers expected"), SBSLPM_ERR_ARG;
+  SB_TRY(on_device(c->device, "the context"));
   if (c->force)
     return set_last_error("a forced context's velocity includes the step's forcing: use the step"), SBSLPM_ERR_CONFIG;
   SB_TRY(near_autotune(c, x, y, z, area, vors));

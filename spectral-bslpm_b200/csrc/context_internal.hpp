@@ -30,6 +30,7 @@ struct GraphKey {
 
 struct sbslpm_ctx {
   sbslpm_config cfg{};
+  int device = 0;  // the device current at creation: buffers and streams live there
   int L = 0, d = 0, q = 0, P = 0, A = 0, off = 0;
   long I = 0;
   std::vector<sbslpm_panel> panels;

@@ -57,6 +57,19 @@ void build_swe_tables(int degree, const std::vector<sbslpm_panel>& panels, int o
 
 void set_last_error(const std::string& msg);
 
+// OK when the current device is `device` (the one a context or batch was
+// created on, which owns its buffers and streams); otherwise an argument
+// error naming both, so that no kernel is launched on another GPU with this
+// device's memory.
+inline sbslpm_status on_device(int device, const char* what) {
+  int cur = -1;
+  if (cudaGetDevice(&cur) != cudaSuccess) return set_last_error("cudaGetDevice failed"), SBSLPM_ERR_CUDA;
+  if (cur == device) return SBSLPM_OK;
+  set_last_error(std::string(what) + " was created on device " + std::to_string(device) + " but device " +
+                 std::to_string(cur) + " is current: make its device current (cudaSetDevice) first");
+  return SBSLPM_ERR_ARG;
+}
+
 // traversal.cu: dual_tree_traversal on the device (same list, same order as build_interactions);
 // the multi form runs one traversal per theta in one launch series and, with
 // near, records per pair whether it failed the MAC (build_interactions_flagged)

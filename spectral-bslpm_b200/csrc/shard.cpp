@@ -140,6 +140,7 @@ void shard_release(sbslpm_ctx* c) {
 }
 
 sbslpm_status shard_allows(const sbslpm_ctx* c, bool step_needs_exchange, const char* what) {
+  SB_TRY(on_device(c->device, "the context"));
   if (c->shard_n <= 1) return SBSLPM_OK;
   if (!step_needs_exchange)
     return set_last_error(std::string(what) + " is not sharded: set one rank (sbslpm_set_shard(ctx, 0, 1, ...))"),
