@@ -60,8 +60,11 @@ def single_step(sb, precision, theta, pdeg, xyza, vor, tuning=(128, 2, 2), near_
     return v, torch.stack(vel)
 
 
-@pytest.mark.parametrize("precision", ["FP64", "MIXED"])
-def test_batch_equals_single_contexts(sb, precision):
+@pytest.mark.parametrize("precision,expanded", [("FP64", None), ("MIXED", None), ("MIXED", True)])
+def test_batch_equals_single_contexts(sb, precision, expanded):
+    """expanded = True forces the expanded near-field pair form on the batch
+    (set-up keeps the difference form at this size); the single contexts
+    follow the batch's form either way."""
     prec = getattr(sb, precision)
     g, xyza, vors = grid_and_vors(sb, len(THETA))
     batch = sb.Batch(base_cfg(sb, prec), THETA, PDEG)
@@ -69,6 +72,9 @@ def test_batch_equals_single_contexts(sb, precision):
     if prec == sb.MIXED:
         batch.set_cc_mode(batch.CC_CUDA_CORES)  # the single context's float32 pair arithmetic
         batch.set_stage0_shared(False)  # and its per-member stage-0 near field
+        if expanded is not None:
+            batch.set_near_form(expanded)
+            assert batch.near_form() == expanded
     v = vors.clone()
     vel = torch.zeros((len(THETA), 3) + v.shape[1:], dtype=torch.float64, device="cuda")
     batch.step(*xyza, v, vel)
@@ -141,6 +147,9 @@ def test_stage0_shared_refused_in_float64(sb):
     with pytest.raises(sb.SbslpmError):
         batch.set_stage0_shared(True)
     batch.set_stage0_shared(False)
+    with pytest.raises(sb.SbslpmError):  # nor the expanded near-field form
+        batch.set_near_form(True)
+    assert not batch.near_form()
 
 
 def test_batch_autotuned_close_to_single(sb):
