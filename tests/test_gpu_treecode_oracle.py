@@ -87,6 +87,24 @@ def test_treecode_step_matches_oracle(sb, port, levels, leaf, n, theta):
         assert rel(v, ov) <= tol, (prec, rel(v, ov))
 
 
+def test_treecode_step_with_tracers_matches_oracle(sb, port, grid5):
+    """Two passive tracers carried by a treecode step (the remap of
+    bve_departure_to_target at the treecode's departure points) against the
+    oracle's treecode step with the same tracers."""
+    g, og, vor, _, _ = grid5
+    tr = np.ascontiguousarray(np.stack([g.z, g.x * g.y], axis=2))
+    ov, _, otr = port.bve_step(og, vor, tr, dt=DT, omega=OMEGA, eps=EPS, mode=2, tree=(8, 256, 0.7, 0))
+    for prec, tol in ((sb.FP64, FP64_TOL), (sb.MIXED, MIXED_TOL)):
+        cfg = sb.config_default(levels=5, interp_degree=3, kernel_eps=EPS, omega=OMEGA, dt=DT, fmm_theta=0.7,
+                                proxy_degree=8, leaf_size=256, precision=prec, tracer_count=2)
+        ctx = sb.Context(cfg)
+        v, t = cuda(vor), cuda(tr)
+        vel = [torch.zeros_like(v) for _ in range(3)]
+        ctx.bve_back_rk4_step(cuda(g.x), cuda(g.y), cuda(g.z), cuda(g.area), v, *vel, t)
+        assert rel(v, ov) <= tol, prec
+        assert rel(t, otr) <= tol, prec
+
+
 @pytest.mark.parametrize("n,theta", [(8, 0.7), (6, 0.5), (10, 0.8)])
 def test_treecode_error_against_the_direct_sum(sb, port, grid5, n, theta):
     """Vorticity after one step within the bar of the oracle's float64 direct
