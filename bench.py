@@ -526,14 +526,15 @@ def profile_run(sb, torch, dev, args):
         wbar = torch.empty_like(w)
         for _ in range(n):
             ctx.bve_adjoint_step(*f, w, wbar_next, wbar)
-    elif args.profile in ("swe", "swe64"):
+    elif args.profile in ("swe", "swe64", "swe-tree", "swe-tree64"):
         g = sb.build_grid(LEVELS, DEGREE, exact_cc=True)
         om, u0 = 2 * np.pi, 2 * np.pi / 12
         lat = np.arcsin(np.clip(g.z, -1, 1))
         h0 = 2.94 - (om * u0 + 0.5 * u0 * u0) * np.sin(lat) ** 2
-        prec = sb.MIXED if args.profile == "swe" else sb.FP64
+        prec = sb.FP64 if args.profile.endswith("64") else sb.MIXED
+        tree = dict(proxy_degree=PROXY_DEGREE, leaf_size=LEAF_SIZE) if args.profile.startswith("swe-tree") else {}
         ctx = sb.Context(sb.config_default(levels=LEVELS, interp_degree=DEGREE, fmm_theta=THETA, kernel_eps=EPS,
-                                           omega=om, dt=SWE_DT, precision=prec, g_over_a=1.0))
+                                           omega=om, dt=SWE_DT, precision=prec, g_over_a=1.0, **tree))
         f = [T(g.x), T(g.y), T(g.z), T(g.area), T(2 * u0 * np.sin(lat)), torch.zeros_like(T(g.x)), T(h0)]
         vel = [torch.zeros_like(f[0]) for _ in range(3)]
         base = [torch.zeros_like(f[0]) for _ in range(3)]
@@ -871,8 +872,8 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint measurement")
     ap.add_argument("--no-at-bar", action="store_true",
                     help="skip the search for the fastest treecode settings that meet the 1e-6 bar")
-    ap.add_argument("--profile", choices=["treecode", "treecode64", "spectral", "swe", "swe64", "ensemble", "adjoint",
-                                          "adjoint64"],
+    ap.add_argument("--profile", choices=["treecode", "treecode64", "spectral", "swe", "swe64", "swe-tree",
+                                          "swe-tree64", "ensemble", "adjoint", "adjoint64"],
                     help="run --warmup + --steps steps of one path and exit (for profiler captures; no timing)")
     ap.add_argument("--members", type=int, default=ENS_MEMBERS, help="ensemble members in --profile ensemble")
     ap.add_argument("--cc-mode", type=int, default=3, choices=[0, 1, 2, 3],

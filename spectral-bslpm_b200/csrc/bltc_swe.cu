@@ -175,13 +175,15 @@ __device__ __forceinline__ void swe_tree_epilogue(double K, double tx, double ty
 // split), TPT targets per thread, the source leaf's particles of both fields
 // staged in shared memory.  Split y takes every gridDim.y-th source leaf and
 // writes the velocity of its partial sums to out + y 3N.  float64: pair64 on
-// absolute positions.  Mixed: pair32 with the sources packed relative to
-// their own grid leaf (gq particles) and, per source grid leaf, the target's
+// absolute positions.  Mixed: the paired float32 pair (pair32x2, two sources
+// per instruction) with the sources packed relative to their own grid leaf
+// (gq particles) and, per source grid leaf, the target's
 // offset from that leaf's centre formed in float64 and rounded once, so that
 // d' = (c_sub - t) kPackScale + (s - c_sub) kPackScale carries the rounding
 // of grid-leaf-sized terms rather than tree-leaf-sized ones (the divergence
 // tendency differentiates the velocity twice and amplifies that rounding);
-// float32 sums per source grid leaf added into float64.
+// float32 sums per source grid leaf (two interleaved halves) added into
+// float64.
 template <int NT, int TPT, bool GUARD, bool MIXED>
 __global__ void __launch_bounds__(NT)
     k_bltc_swe_near(TreeGeom tg, StepGeom fg, const double* __restrict__ x, const double* __restrict__ y,
@@ -194,59 +196,115 @@ __global__ void __launch_bounds__(NT)
   Src* t2 = t1 + tg.npl;
   const int f = blockIdx.x, split = blockIdx.y, nsplit = gridDim.y, npl = tg.npl;
   double* v = out + (long)split * 3 * tg.N;
-  double tx[TPT], ty[TPT], tz[TPT], ax[TPT], ay[TPT], az[TPT], bx[TPT], by[TPT], bz[TPT];
+  // float64: the targets' positions; mixed: their packed positions t k as
+  // float pairs hi + lo (t k to within u^2), so that the offset from a grid
+  // leaf's centre c, (c - t) k, forms in float32 as (C_hi - T_hi) + (C_lo -
+  // T_lo) with the rounding of the offset itself (no float64 conversions in
+  // the source loop, which would share the reciprocals' pipe)
+  constexpr int TD = MIXED ? 1 : TPT, TF = MIXED ? TPT : 1;
+  double tx[TD], ty[TD], tz[TD];
+  float2 nt[3][TF];
+  double ax[TPT], ay[TPT], az[TPT], bx[TPT], by[TPT], bz[TPT];
 #pragma unroll
   for (int r = 0; r < TPT; r++) {
     const int k = threadIdx.x + r * NT;
     const long i = (long)f * npl + (k < npl ? k : 0);
-    tx[r] = x[i];
-    ty[r] = y[i];
-    tz[r] = z[i];
+    if constexpr (MIXED) {
+      const double p[3] = {x[i] * kPackScale, y[i] * kPackScale, z[i] * kPackScale};
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        const float hi = (float)p[c], lo = (float)(p[c] - (double)hi);
+        nt[c][r] = make_float2(-hi, -lo);
+      }
+    } else {
+      tx[r] = x[i];
+      ty[r] = y[i];
+      tz[r] = z[i];
+    }
     ax[r] = ay[r] = az[r] = bx[r] = by[r] = bz[r] = 0;
   }
   const float feps = (float)tg.eps;
+  const int hq = (gq + 1) / 2, ngl = npl / gq, np2 = ngl * hq;
   for (int e = tg.near_start[f] + split; e < tg.near_start[f + 1]; e += nsplit) {
     const int sl = tg.near_src[e];
     const long sb = (long)sl * npl;
     __syncthreads();
-    for (int k = threadIdx.x; k < npl; k += NT) {
-      if constexpr (MIXED) {
-        t1[k] = psrcf[sb + k];
-        t2[k] = psrcf2[sb + k];
-      } else {
+    if constexpr (MIXED) {
+      // both fields' sources two at a time, transposed so that every operand
+      // of the pair arithmetic is a register pair (x0,x1,y0,y1),(z0,z1,w0,w1)
+      // for the paired float32 instructions (pair32x2); each grid leaf takes
+      // hq = ceil(gq/2) pairs, an odd gq closing on a source of zero strength
+      // at the grid leaf's centre (which adds exactly zero); after them the
+      // grid leaves' packed centres c k as (x_hi, x_lo, y_hi, y_lo),
+      // (z_hi, z_lo, -, -)
+      float4* tp = reinterpret_cast<float4*>(smem);
+      const float4 none = make_float4(0.f, 0.f, 0.f, 0.f);
+      for (int p = threadIdx.x; p < np2; p += NT) {
+        const int gl = p / hq, j = p - gl * hq;
+        const long s0 = sb + (long)gl * gq + 2 * j;
+        const bool two = 2 * j + 1 < gq;
+        const float4 a0 = psrcf[s0], a1 = two ? psrcf[s0 + 1] : none;
+        const float4 c0 = psrcf2[s0], c1 = two ? psrcf2[s0 + 1] : none;
+        tp[4 * p] = make_float4(a0.x, a1.x, a0.y, a1.y);
+        tp[4 * p + 1] = make_float4(a0.z, a1.z, a0.w, a1.w);
+        tp[4 * p + 2] = make_float4(c0.x, c1.x, c0.y, c1.y);
+        tp[4 * p + 3] = make_float4(c0.z, c1.z, c0.w, c1.w);
+      }
+      for (int gl = threadIdx.x; gl < ngl; gl += NT) {
+        const double* cs = gcentre + 4 * (sb / gq + gl);
+        float hl[6];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          const double pc = cs[c] * kPackScale;
+          hl[2 * c] = (float)pc;
+          hl[2 * c + 1] = (float)(pc - (double)hl[2 * c]);
+        }
+        tp[4 * np2 + 2 * gl] = make_float4(hl[0], hl[1], hl[2], hl[3]);
+        tp[4 * np2 + 2 * gl + 1] = make_float4(hl[4], hl[5], 0.f, 0.f);
+      }
+    } else {
+      for (int k = threadIdx.x; k < npl; k += NT) {
         t1[k] = psrc[sb + k];
         t2[k] = psrc2[sb + k];
       }
     }
     __syncthreads();
     if constexpr (MIXED) {
-      for (int k0 = 0; k0 < npl; k0 += gq) {
-        const double* cs = gcentre + 4 * ((sb + k0) / gq);
-        float b0[TPT], b1[TPT], b2[TPT], fa[TPT][3], fb[TPT][3];
+      const float4* tp = reinterpret_cast<const float4*>(smem);
+      const float2 eps2 = make_float2(feps, feps);
+      for (int gl = 0; gl < ngl; gl++) {
+        const float4 C0 = tp[4 * np2 + 2 * gl], C1 = tp[4 * np2 + 2 * gl + 1];
+        const float2 cc[3] = {make_float2(C0.x, C0.y), make_float2(C0.z, C0.w), make_float2(C1.x, C1.y)};
+        float2 bq[3][TPT], fa[TPT][3], fb[TPT][3];
 #pragma unroll
         for (int r = 0; r < TPT; r++) {
-          b0[r] = (float)((cs[0] - tx[r]) * kPackScale);
-          b1[r] = (float)((cs[1] - ty[r]) * kPackScale);
-          b2[r] = (float)((cs[2] - tz[r]) * kPackScale);
-          fa[r][0] = fa[r][1] = fa[r][2] = fb[r][0] = fb[r][1] = fb[r][2] = 0.f;
+#pragma unroll
+          for (int c = 0; c < 3; c++) {
+            const float2 dd = __fadd2_rn(cc[c], nt[c][r]);
+            const float bc = dd.x + dd.y;
+            bq[c][r] = make_float2(bc, bc);
+          }
+          fa[r][0] = fa[r][1] = fa[r][2] = fb[r][0] = fb[r][1] = fb[r][2] = make_float2(0.f, 0.f);
         }
 #pragma unroll 4
-        for (int k = k0; k < k0 + gq; k++) {
-          const float4 s1 = t1[k], s2 = t2[k];
+        for (int p = gl * hq; p < (gl + 1) * hq; p++) {
+          const float4 A = tp[4 * p], B = tp[4 * p + 1], C = tp[4 * p + 2], D = tp[4 * p + 3];
 #pragma unroll
           for (int r = 0; r < TPT; r++) {
-            pair32<GUARD>(b0[r], b1[r], b2[r], s1, feps, fa[r][0], fa[r][1], fa[r][2]);
-            pair32<GUARD>(b0[r], b1[r], b2[r], s2, feps, fb[r][0], fb[r][1], fb[r][2]);
+            pair32x2<GUARD>(bq[0][r], bq[1][r], bq[2][r], make_float2(A.x, A.y), make_float2(A.z, A.w),
+                            make_float2(B.x, B.y), make_float2(B.z, B.w), eps2, fa[r][0], fa[r][1], fa[r][2]);
+            pair32x2<GUARD>(bq[0][r], bq[1][r], bq[2][r], make_float2(C.x, C.y), make_float2(C.z, C.w),
+                            make_float2(D.x, D.y), make_float2(D.z, D.w), eps2, fb[r][0], fb[r][1], fb[r][2]);
           }
         }
 #pragma unroll
         for (int r = 0; r < TPT; r++) {
-          ax[r] += fa[r][0];
-          ay[r] += fa[r][1];
-          az[r] += fa[r][2];
-          bx[r] += fb[r][0];
-          by[r] += fb[r][1];
-          bz[r] += fb[r][2];
+          ax[r] += (double)(fa[r][0].x + fa[r][0].y);
+          ay[r] += (double)(fa[r][1].x + fa[r][1].y);
+          az[r] += (double)(fa[r][2].x + fa[r][2].y);
+          bx[r] += (double)(fb[r][0].x + fb[r][0].y);
+          by[r] += (double)(fb[r][1].x + fb[r][1].y);
+          bz[r] += (double)(fb[r][2].x + fb[r][2].y);
         }
       }
     } else {
@@ -268,7 +326,7 @@ __global__ void __launch_bounds__(NT)
     if (k >= npl) continue;
     const long i = (long)f * npl + k;
     double ux, uy, uz;
-    swe_tree_epilogue(K, tx[r], ty[r], tz[r], ax[r], ay[r], az[r], bx[r], by[r], bz[r], ux, uy, uz);
+    swe_tree_epilogue(K, x[i], y[i], z[i], ax[r], ay[r], az[r], bx[r], by[r], bz[r], ux, uy, uz);
     v[i] = ux;
     v[tg.N + i] = uy;
     v[2 * tg.N + i] = uz;
@@ -301,7 +359,10 @@ void launch_bltc_swe_near(const TreeGeom& tg, const StepGeom& fg, int precision,
   const bool guard = !(tg.eps > 0), mixed = precision == SBSLPM_MIXED;
   constexpr int NT = 128;
   const int tpt = (tg.npl + NT - 1) / NT;
-  const size_t smem = (mixed ? sizeof(float4) : sizeof(double4)) * 2 * (size_t)tg.npl;
+  // mixed: four float4 per source pair, ceil(gq/2) pairs per grid leaf, and
+  // two float4 per grid leaf for its centre
+  const size_t smem = mixed ? sizeof(float4) * (size_t)(tg.npl / gq) * (4 * ((gq + 1) / 2) + 2)
+                            : sizeof(double4) * 2 * (size_t)tg.npl;
 #define SB_SN(TPT)                                                                                                \
   do {                                                                                                            \
     if (mixed) {                                                                                                  \
@@ -316,10 +377,10 @@ void launch_bltc_swe_near(const TreeGeom& tg, const StepGeom& fg, int precision,
                      psrcf, psrcf2, near, gcentre, gq);                                                                        \
     }                                                                                                             \
   } while (0)
+  // the shallow-water context refuses leaves of more than 256 particles, so
+  // two targets per thread of 128 cover every leaf
   if (tpt <= 1) SB_SN(1);
-  else if (tpt == 2) SB_SN(2);
-  else if (tpt <= 4) SB_SN(4);
-  else SB_SN(8);
+  else SB_SN(2);
 #undef SB_SN
 }
 

@@ -27,15 +27,18 @@ def cuda(a):
     return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).cuda()
 
 
-def tree_ctx(sb, levels, n, leaf, theta, precision, **kw):
-    return sb.Context(sb.config_default(levels=levels, interp_degree=3, fmm_theta=theta, kernel_eps=EPS,
+def tree_ctx(sb, levels, n, leaf, theta, precision, deg=3, **kw):
+    return sb.Context(sb.config_default(levels=levels, interp_degree=deg, fmm_theta=theta, kernel_eps=EPS,
                                         omega=2 * np.pi, dt=0.002, proxy_degree=n, leaf_size=leaf,
                                         precision=precision, g_over_a=1.0, **kw))
 
 
-@pytest.mark.parametrize("levels,leaf,n,theta", [(5, 256, 8, 0.7), (4, 64, 6, 0.5), (4, 16, 5, 0.8)])
-def test_swe_tree_velocity_matches_oracle(sb, port, levels, leaf, n, theta):
-    g = sb.build_grid(levels, 3, exact_cc=True)
+# interp degrees 2 and 4 give grid leaves of 9 and 25 points: an odd count,
+# which the mixed near field closes with a zero-strength source per grid leaf
+@pytest.mark.parametrize("levels,leaf,n,theta,deg", [(5, 256, 8, 0.7, 3), (4, 64, 6, 0.5, 3), (4, 16, 5, 0.8, 3),
+                                                     (4, 256, 8, 0.7, 2), (4, 256, 6, 0.6, 4)])
+def test_swe_tree_velocity_matches_oracle(sb, port, levels, leaf, n, theta, deg):
+    g = sb.build_grid(levels, deg, exact_cc=True)
     rng = np.random.default_rng(7)
     d = [2e-3 * rng.standard_normal(g.x.shape) for _ in range(3)]
     lat, lon = np.arcsin(np.clip(g.z, -1, 1)), np.arctan2(g.y, g.x)
@@ -44,13 +47,13 @@ def test_swe_tree_velocity_matches_oracle(sb, port, levels, leaf, n, theta):
     s = np.stack([g.x + d[0], g.y + d[1], g.z + d[2]])
     s /= np.linalg.norm(s, axis=0)
     p = (g.x, g.y, g.z)
-    want = port.bltc_velocity_swe(levels, 3, leaf, n, theta, EPS, 0, p, (s[0], s[1], s[2]), wv, p, wd)
+    want = port.bltc_velocity_swe(levels, deg, leaf, n, theta, EPS, 0, p, (s[0], s[1], s[2]), wv, p, wd)
     for prec, tol in ((sb.FP64, 1e-12), (sb.MIXED, 1e-6)):
-        ctx = tree_ctx(sb, levels, n, leaf, theta, prec)
+        ctx = tree_ctx(sb, levels, n, leaf, theta, prec, deg)
         u = [torch.zeros(g.x.shape, dtype=torch.float64, device="cuda") for _ in range(3)]
         ctx.swe_tree_velocity(*[cuda(a) for a in d], cuda(wv), cuda(wd), *u)
         err = rel(torch.stack(u).reshape(3, -1), want)
-        print(f"levels {levels} leaf {leaf} n {n} theta {theta} prec {prec}: {err:.2e}")
+        print(f"levels {levels} deg {deg} leaf {leaf} n {n} theta {theta} prec {prec}: {err:.2e}")
         assert err <= tol
 
 
