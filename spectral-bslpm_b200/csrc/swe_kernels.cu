@@ -236,7 +236,9 @@ __global__ void k_swe_sources_from_disp(StepGeom g, SweGeom sw, const double* __
 // Interactions.  One warp per target panel; for q <= 16 the warp's lanes are
 // (32/q source splits) x (q target nodes), for larger q each lane owns
 // ceil(q/32) target nodes.  A source panel's q proxies of both fields are
-// staged in shared memory and every lane sweeps them.  ALL_LEAVES: every
+// staged in shared memory and every lane sweeps them (mixed: two proxies per
+// paired float32 instruction, each panel's two interleaved float32 halves
+// added before the float64 conversion).  ALL_LEAVES: every
 // leaf against every leaf, source leaves split into gridDim.y groups whose
 // partials are reduced in order afterwards.
 
@@ -264,7 +266,11 @@ __global__ void __launch_bounds__(32 * kWarps)
                    double* __restrict__ out, long out_stride) {
   using W = Shape<Q>;
   using Src = typename std::conditional<MIXED, float4, double4>::type;
-  __shared__ Src stage[kWarps][2][W::STAGE];
+  // mixed: a split's Q proxies as ceil(Q/2) source pairs of two float4
+  // (x0,x1,y0,y1),(z0,z1,w0,w1), an odd Q closing on a zero-strength source
+  // at the panel's centre (which adds exactly zero)
+  constexpr int HQ = (Q + 1) / 2, SPLIT = MIXED ? 2 * HQ : Q, STG = MIXED ? W::S * 2 * HQ : W::STAGE;
+  __shared__ Src stage[kWarps][2][STG];
   __shared__ double red[kWarps][6][32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int tp_first = ALL_LEAVES ? g.offset : 0;
@@ -316,55 +322,71 @@ __global__ void __launch_bounds__(32 * kWarps)
     ax[r] = ay[r] = az[r] = bx[r] = by[r] = bz[r] = 0;
   }
   constexpr int STEP = Q <= 32 ? W::S : 1;
+  // a lane's share of the staging: a proxy (float64) or a source pair (mixed)
+  auto stage_one = [&](int sp, int k, int slot) {
+    if constexpr (MIXED) {
+      const long b = (long)sp * Q + 2 * k;
+      const bool two = 2 * k + 1 < Q;
+      const float4 none = make_float4(0.f, 0.f, 0.f, 0.f);
+      const float4 a0 = s1[b], a1 = two ? s1[b + 1] : none, c0 = s2[b], c1 = two ? s2[b + 1] : none;
+      stage[warp][0][slot + 2 * k] = make_float4(a0.x, a1.x, a0.y, a1.y);
+      stage[warp][0][slot + 2 * k + 1] = make_float4(a0.z, a1.z, a0.w, a1.w);
+      stage[warp][1][slot + 2 * k] = make_float4(c0.x, c1.x, c0.y, c1.y);
+      stage[warp][1][slot + 2 * k + 1] = make_float4(c0.z, c1.z, c0.w, c1.w);
+    } else {
+      stage[warp][0][slot + k] = s1[(long)sp * Q + k];
+      stage[warp][1][slot + k] = s2[(long)sp * Q + k];
+    }
+  };
+  constexpr int PER = MIXED ? HQ : Q;  // staging items per source panel
   for (int e = e0; e < e1; e += STEP) {
     int sp = 0;
     if (Q <= 32) {
       if (active && e + h < e1) {
         sp = source_of(e + h);
         const int j = lane % Q;
-        stage[warp][0][h * Q + j] = s1[(long)sp * Q + j];
-        stage[warp][1][h * Q + j] = s2[(long)sp * Q + j];
+        if (j < PER) stage_one(sp, j, h * SPLIT);
       }
     } else {
       sp = source_of(e);
-      for (int k = lane; k < Q; k += 32) {
-        stage[warp][0][k] = s1[(long)sp * Q + k];
-        stage[warp][1][k] = s2[(long)sp * Q + k];
-      }
+      for (int k = lane; k < PER; k += 32) stage_one(sp, k, 0);
     }
     __syncwarp();
     if (active && e + h < e1) {
-      const Src* st1 = &stage[warp][0][h * Q];
-      const Src* st2 = &stage[warp][1][h * Q];
+      const Src* st1 = &stage[warp][0][h * SPLIT];
+      const Src* st2 = &stage[warp][1][h * SPLIT];
       if constexpr (MIXED) {
         const double* cs = g.pd_centre + 4 * (long)sp;
         const float c0 = (float)((cs[0] - ct[0]) * kPackScale), c1 = (float)((cs[1] - ct[1]) * kPackScale),
                     c2 = (float)((cs[2] - ct[2]) * kPackScale);
-        float fa[TPL][3], fb[TPL][3], b0[TPL], b1[TPL], b2[TPL];
+        const float2 eps2 = make_float2(eps32, eps32);
+        float2 fa[TPL][3], fb[TPL][3], b0[TPL], b1[TPL], b2[TPL];
 #pragma unroll
         for (int r = 0; r < TPL; r++) {
-          b0[r] = c0 - dtx[r];
-          b1[r] = c1 - dty[r];
-          b2[r] = c2 - dtz[r];
-          fa[r][0] = fa[r][1] = fa[r][2] = fb[r][0] = fb[r][1] = fb[r][2] = 0.f;
+          b0[r] = make_float2(c0 - dtx[r], c0 - dtx[r]);
+          b1[r] = make_float2(c1 - dty[r], c1 - dty[r]);
+          b2[r] = make_float2(c2 - dtz[r], c2 - dtz[r]);
+          fa[r][0] = fa[r][1] = fa[r][2] = fb[r][0] = fb[r][1] = fb[r][2] = make_float2(0.f, 0.f);
         }
 #pragma unroll 4
-        for (int k = 0; k < Q; k++) {
-          const float4 v1 = st1[k], v2 = st2[k];
+        for (int k = 0; k < HQ; k++) {
+          const float4 A = st1[2 * k], B = st1[2 * k + 1], C = st2[2 * k], D = st2[2 * k + 1];
 #pragma unroll
           for (int r = 0; r < TPL; r++) {
-            pair32<GUARD>(b0[r], b1[r], b2[r], v1, eps32, fa[r][0], fa[r][1], fa[r][2]);
-            pair32<GUARD>(b0[r], b1[r], b2[r], v2, eps32, fb[r][0], fb[r][1], fb[r][2]);
+            pair32x2<GUARD>(b0[r], b1[r], b2[r], make_float2(A.x, A.y), make_float2(A.z, A.w),
+                            make_float2(B.x, B.y), make_float2(B.z, B.w), eps2, fa[r][0], fa[r][1], fa[r][2]);
+            pair32x2<GUARD>(b0[r], b1[r], b2[r], make_float2(C.x, C.y), make_float2(C.z, C.w),
+                            make_float2(D.x, D.y), make_float2(D.z, D.w), eps2, fb[r][0], fb[r][1], fb[r][2]);
           }
         }
 #pragma unroll
         for (int r = 0; r < TPL; r++) {
-          ax[r] += fa[r][0];
-          ay[r] += fa[r][1];
-          az[r] += fa[r][2];
-          bx[r] += fb[r][0];
-          by[r] += fb[r][1];
-          bz[r] += fb[r][2];
+          ax[r] += (double)(fa[r][0].x + fa[r][0].y);
+          ay[r] += (double)(fa[r][1].x + fa[r][1].y);
+          az[r] += (double)(fa[r][2].x + fa[r][2].y);
+          bx[r] += (double)(fb[r][0].x + fb[r][0].y);
+          by[r] += (double)(fb[r][1].x + fb[r][1].y);
+          bz[r] += (double)(fb[r][2].x + fb[r][2].y);
         }
       } else {
 #pragma unroll 4
@@ -405,7 +427,9 @@ __global__ void __launch_bounds__(32 * kWarps)
     const int j = Q <= 32 ? lane % Q : lane + 32 * r;
     if (j >= Q) continue;
     double ux, uy, uz;
-    swe_epilogue(K, tx[r], ty[r], tz[r], ax[r], ay[r], az[r], bx[r], by[r], bz[r], ux, uy, uz);
+    const long ot = (long)t * Q + j;  // the target's position again: not held in registers across the sweep
+    swe_epilogue(K, g.px[ot], g.px[pn + ot], g.px[2 * pn + ot], ax[r], ay[r], az[r], bx[r], by[r], bz[r], ux, uy,
+                 uz);
     const long o = ALL_LEAVES ? (long)blockIdx.y * 3 * out_stride + (long)tix * Q + j : (long)t * Q + j;
     const long s = ALL_LEAVES ? out_stride : pn;
     out[o] = ux;

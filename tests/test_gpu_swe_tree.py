@@ -84,8 +84,8 @@ def test_swe_tree_step_against_the_direct_sum(sb, n, theta):
     velocity).  The divergence starts at zero and stays three orders below
     the vorticity: its error is set by the velocity's float32 rounding
     through the kinetic-energy Laplacian of the divergence tendency, so it is
-    measured on the vorticity's scale (bound 5e-6; measured 1.3e-6 at theta
-    0.7, degree 8 and 4.8e-7 at theta 0.5, degree 6) and printed beside the
+    measured on the vorticity's scale (bound 5e-6; measured 5.5e-7 at theta
+    0.7, degree 8 and 3.7e-7 at theta 0.5, degree 6) and printed beside the
     same error of the mixed spectral-FMM step (1.1e-7 and 1.3e-7: its near
     field is smaller, and its float32 sums shorter)."""
     g, vor, h0 = swe_state(sb, 5)
