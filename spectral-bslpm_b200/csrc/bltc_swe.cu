@@ -333,6 +333,132 @@ __global__ void __launch_bounds__(NT)
   }
 }
 
+// Well-separated pairs of both fields, mixed precision, over chunks of the
+// interaction list: the BVE treecode's chunks of at most C consecutive
+// entries of one target panel, S chunk slots of Q target proxies per block
+// (thread k: target proxy k % Q of slot k / Q).  Per entry a slot stages the
+// source panel's Q proxies of both fields as ceil(Q/2) source pairs (an odd
+// Q closing on a zero-strength proxy at the panel's centre) and every thread
+// runs them on the paired float32 instructions against its target proxy;
+// each source panel's float32 sums are added into float64.  A slot writes
+// its chunk's raw sums of both fields (6 rows of Q) to its own row of
+// partial; k_swe_cc_reduce adds a target's chunks in list order and applies
+// the SWE epilogue.  Against one warp per target panel (k_swe_interact, 81
+// of 96 lanes busy at Q = 81) the slots keep the lanes busy and spread long
+// lists over the GPU.
+template <int Q, int S>
+struct SweCcShape {
+  static constexpr int NT = (S * Q + 31) / 32 * 32;
+  static constexpr int Q2 = (Q + 1) / 2;
+};
+
+template <int Q, int S, bool GUARD>
+__global__ void __launch_bounds__(SweCcShape<Q, S>::NT)
+    k_swe_cc32(StepGeom g, const float4* __restrict__ srcf2, const int4* __restrict__ chunks, int nchunks,
+               double* __restrict__ partial) {
+  constexpr int Q2 = SweCcShape<Q, S>::Q2;
+  __shared__ float4 tile[S][2][2 * Q2];  // per field (x0,x1,y0,y1),(z0,z1,w0,w1)
+  const int h = threadIdx.x / Q, j = threadIdx.x - h * Q;
+  const int c = blockIdx.x * S + h;
+  const bool live = h < S && c < nchunks;
+  int nmax = 0;  // the block's longest chunk: every thread passes the same barriers
+  for (int k = 0; k < S && blockIdx.x * S + k < nchunks; k++) {
+    const int4 ck = chunks[blockIdx.x * S + k];
+    nmax = max(nmax, ck.z - ck.y);
+  }
+  const int4 ch = live ? chunks[c] : make_int4(0, 0, 0, 0);
+  const int n = ch.z - ch.y;
+  const long pn = (long)g.panels * Q;
+  double cx = 0, cy = 0, cz = 0;
+  float dtx = 0, dty = 0, dtz = 0;
+  if (live) {
+    const double* ct = g.pd_centre + 4 * (long)ch.x;
+    cx = ct[0];
+    cy = ct[1];
+    cz = ct[2];
+    const long o = (long)ch.x * Q + j;
+    dtx = (float)((g.px[o] - cx) * kPackScale);
+    dty = (float)((g.px[pn + o] - cy) * kPackScale);
+    dtz = (float)((g.px[2 * pn + o] - cz) * kPackScale);
+  }
+  const float feps = (float)g.eps;
+  const float2 eps2 = make_float2(feps, feps);
+  double ax = 0, ay = 0, az = 0, bx = 0, by = 0, bz = 0;
+  for (int e = 0; e < nmax; e++) {
+    const bool act = live && e < n;
+    const int sp = act ? __ldg(g.src_panel + ch.y + e) : 0;
+    __syncthreads();
+    if (act && j < Q2) {
+      const long sb = (long)sp * Q + 2 * j;
+      const bool two = 2 * j + 1 < Q;
+      const float4 none = make_float4(0.f, 0.f, 0.f, 0.f);
+      const float4 a0 = g.srcf[sb], a1 = two ? g.srcf[sb + 1] : none;
+      const float4 c0 = srcf2[sb], c1 = two ? srcf2[sb + 1] : none;
+      tile[h][0][2 * j] = make_float4(a0.x, a1.x, a0.y, a1.y);
+      tile[h][0][2 * j + 1] = make_float4(a0.z, a1.z, a0.w, a1.w);
+      tile[h][1][2 * j] = make_float4(c0.x, c1.x, c0.y, c1.y);
+      tile[h][1][2 * j + 1] = make_float4(c0.z, c1.z, c0.w, c1.w);
+    }
+    __syncthreads();
+    if (act) {
+      const double* cs = g.pd_centre + 4 * (long)sp;
+      const float b0 = (float)((cs[0] - cx) * kPackScale) - dtx, b1 = (float)((cs[1] - cy) * kPackScale) - dty,
+                  b2 = (float)((cs[2] - cz) * kPackScale) - dtz;
+      const float2 px2 = make_float2(b0, b0), py2 = make_float2(b1, b1), pz2 = make_float2(b2, b2);
+      float2 fa[3], fb[3];
+      fa[0] = fa[1] = fa[2] = fb[0] = fb[1] = fb[2] = make_float2(0.f, 0.f);
+      const float4* t1 = tile[h][0];
+      const float4* t2 = tile[h][1];
+#pragma unroll 4
+      for (int k2 = 0; k2 < Q2; k2++) {
+        const float4 A = t1[2 * k2], B = t1[2 * k2 + 1], C = t2[2 * k2], D = t2[2 * k2 + 1];
+        pair32x2<GUARD>(px2, py2, pz2, make_float2(A.x, A.y), make_float2(A.z, A.w), make_float2(B.x, B.y),
+                        make_float2(B.z, B.w), eps2, fa[0], fa[1], fa[2]);
+        pair32x2<GUARD>(px2, py2, pz2, make_float2(C.x, C.y), make_float2(C.z, C.w), make_float2(D.x, D.y),
+                        make_float2(D.z, D.w), eps2, fb[0], fb[1], fb[2]);
+      }
+      ax += (double)(fa[0].x + fa[0].y);
+      ay += (double)(fa[1].x + fa[1].y);
+      az += (double)(fa[2].x + fa[2].y);
+      bx += (double)(fb[0].x + fb[0].y);
+      by += (double)(fb[1].x + fb[1].y);
+      bz += (double)(fb[2].x + fb[2].y);
+    }
+  }
+  if (live) {
+    double* p = partial + (long)c * 6 * Q;
+    p[j] = ax;
+    p[Q + j] = ay;
+    p[2 * Q + j] = az;
+    p[3 * Q + j] = bx;
+    p[4 * Q + j] = by;
+    p[5 * Q + j] = bz;
+  }
+}
+
+// Each target proxy's chunk sums in list order, then the SWE epilogue with
+// the packed kernel constant (the sums are over packed differences).
+__global__ void k_swe_cc_reduce(StepGeom g, const int* __restrict__ cstart, const double* __restrict__ partial,
+                                double* __restrict__ out) {
+  const int q = g.q;
+  const long pn = (long)g.panels * q;
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= pn) return;
+  const int t = (int)(i / q), j = (int)(i - (long)t * q);
+  double a[6] = {0, 0, 0, 0, 0, 0};
+  for (int c = cstart[t]; c < cstart[t + 1]; c++) {
+    const double* p = partial + (long)c * 6 * q + j;
+#pragma unroll
+    for (int r = 0; r < 6; r++) a[r] += p[r * q];
+  }
+  double ux, uy, uz;
+  swe_tree_epilogue(kBiotSavartPacked, g.px[i], g.px[pn + i], g.px[2 * pn + i], a[0], a[1], a[2], a[3], a[4], a[5],
+                    ux, uy, uz);
+  out[i] = ux;
+  out[pn + i] = uy;
+  out[2 * pn + i] = uz;
+}
+
 }  // namespace
 
 void launch_bltc_swe_sources(const TreeGeom& tg, const StepGeom& fg, const BliTable& tab, int stage, double dtd,
@@ -367,14 +493,14 @@ void launch_bltc_swe_near(const TreeGeom& tg, const StepGeom& fg, int precision,
   do {                                                                                                            \
     if (mixed) {                                                                                                  \
       if (guard) SB_LAUNCH((k_bltc_swe_near<NT, TPT, true, true>), grid, NT, smem, st, tg, fg, x, y, z, psrc,     \
-                           psrc2, psrcf, psrcf2, near, gcentre, gq);                                                           \
+                           psrc2, psrcf, psrcf2, near, gcentre, gq);                                              \
       else SB_LAUNCH((k_bltc_swe_near<NT, TPT, false, true>), grid, NT, smem, st, tg, fg, x, y, z, psrc, psrc2,   \
-                     psrcf, psrcf2, near, gcentre, gq);                                                                        \
+                     psrcf, psrcf2, near, gcentre, gq);                                                           \
     } else {                                                                                                      \
       if (guard) SB_LAUNCH((k_bltc_swe_near<NT, TPT, true, false>), grid, NT, smem, st, tg, fg, x, y, z, psrc,    \
-                           psrc2, psrcf, psrcf2, near, gcentre, gq);                                                           \
+                           psrc2, psrcf, psrcf2, near, gcentre, gq);                                              \
       else SB_LAUNCH((k_bltc_swe_near<NT, TPT, false, false>), grid, NT, smem, st, tg, fg, x, y, z, psrc, psrc2,  \
-                     psrcf, psrcf2, near, gcentre, gq);                                                                        \
+                     psrcf, psrcf2, near, gcentre, gq);                                                           \
     }                                                                                                             \
   } while (0)
   // the shallow-water context refuses leaves of more than 256 particles, so
@@ -382,6 +508,40 @@ void launch_bltc_swe_near(const TreeGeom& tg, const StepGeom& fg, int precision,
   if (tpt <= 1) SB_SN(1);
   else SB_SN(2);
 #undef SB_SN
+}
+
+bool swe_tree_cc_supported(int q) { return q == 36 || q == 49 || q == 64 || q == 81 || q == 100 || q == 121; }
+
+// Slots per block for each proxy count: at most a few lanes of the block idle
+// (36: 7 x 36 of 256, 49: 5 x 49 of 256, 64: 2 x 64 of 128, 81: 3 x 81 of
+// 256, 100: 5 x 100 of 512, 121: 2 x 121 of 256).
+void launch_swe_tree_cc(const StepGeom& fg, const float4* srcf2, const int4* chunks, int nchunks, const int* cstart,
+                        double* partial, double* tgt, cudaStream_t st) {
+  const bool guard = !(fg.eps > 0);
+  if (nchunks > 0) {
+#define SB_SCC(Q, S)                                                                                           \
+  case Q:                                                                                                      \
+    if (guard)                                                                                                 \
+      SB_LAUNCH((k_swe_cc32<Q, S, true>), (unsigned)((nchunks + S - 1) / S), (SweCcShape<Q, S>::NT), 0, st, fg, \
+                srcf2, chunks, nchunks, partial);                                                              \
+    else                                                                                                       \
+      SB_LAUNCH((k_swe_cc32<Q, S, false>), (unsigned)((nchunks + S - 1) / S), (SweCcShape<Q, S>::NT), 0, st,   \
+                fg, srcf2, chunks, nchunks, partial);                                                          \
+    break;
+    switch (fg.q) {
+      SB_SCC(36, 7)
+      SB_SCC(49, 5)
+      SB_SCC(64, 2)
+      SB_SCC(81, 3)
+      SB_SCC(100, 5)
+      SB_SCC(121, 2)
+      default:
+        break;
+    }
+#undef SB_SCC
+  }
+  const long pn = (long)fg.panels * fg.q;
+  SB_LAUNCH(k_swe_cc_reduce, blocks_for(pn, 256), 256, 0, st, fg, cstart, partial, tgt);
 }
 
 }  // namespace sbslpm

@@ -847,7 +847,8 @@ sbslpm_status sbslpm_destroy(sbslpm_ctx* c) {
                   c->srcf2, c->tend, c->avor, c->adj_src, c->adj_vbar, c->adj_q, c->adj_y, c->adj_part,
                   c->adj_w, c->adj_vel, c->adj_near_ts, c->adj_near_tt, c->adj_cc_ts, c->adj_cc_tt, c->adj_tbar,
                   c->adj_qbl, c->self, c->force, c->d_time, c->cc_partial, c->entry32, c->fentry32, c->fsrcp,
-                  c->mutual_units, c->near_slot, c->fsrc2, c->psrc2, c->fsrcf2, c->psrcf2, c->adj_ynl};
+                  c->mutual_units, c->near_slot, c->fsrc2, c->psrc2, c->fsrcf2, c->psrcf2, c->adj_ynl,
+                  c->swe_cc_partial};
   for (void* b : bufs)
     if (b) cudaFree(b);
   for (int k = 0; k < 4; k++) {

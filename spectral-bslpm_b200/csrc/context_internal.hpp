@@ -89,6 +89,7 @@ struct sbslpm_ctx {
   int* cc_cstart[4] = {};
   int cc_nchunks[4] = {};
   double* cc_partial = nullptr;  // [n_cc][3][qx] chunk sums
+  double* swe_cc_partial = nullptr;  // [n_cc][6][qx] chunk sums of both SWE fields (mixed treecode)
   int cc_slots = 1, cc_len = 2;  // chunk slots per block (0: one block per target panel), entries per chunk
   int cc_tpt = 0;                 // 0: sources staged in shared memory; 1 | 2: barrier-free, targets per thread
   float4* fsrcp = nullptr;        // pair-transposed packed proxy sources (barrier-free mixed kernel)

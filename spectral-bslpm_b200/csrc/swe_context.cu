@@ -17,6 +17,10 @@ using namespace sbslpm;
 namespace sbslpm {
 namespace {
 
+// Entries per chunk of the mixed treecode's well-separated list for the SWE
+// (the chunk lists of 1..4 entries are built with the treecode's lists).
+constexpr int kSweCcLen = 2;
+
 // Static tables and workspace of the SWE step, built on the first SWE call.
 sbslpm_status swe_setup(sbslpm_ctx* c) {
   if (c->swe_ready) return SBSLPM_OK;
@@ -61,6 +65,8 @@ sbslpm_status swe_setup(sbslpm_ctx* c) {
     if (c->cfg.precision == SBSLPM_MIXED) {
       SB_TRY(dalloc(&c->psrcf2, (size_t)ln));
       SB_TRY(dalloc(&c->fsrcf2, fpn));
+      if (c->n_cc > 0 && c->cc_chunks[kSweCcLen - 1] && swe_tree_cc_supported(c->qx))
+        SB_TRY(dalloc(&c->swe_cc_partial, (size_t)c->n_cc * 6 * c->qx));
     }
   } else {
     const size_t pn = (size_t)c->P * c->q;
@@ -117,7 +123,11 @@ void swe_tree_velocity(sbslpm_ctx* c, int stage, double dtd, double dts, const d
   fg2.srcf = c->fsrcf2;
   launch_upward_fused(fg2, 2, 0, 0.0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, c->fsrc2, mixed,
                       tree_st);
-  launch_swe_interactions(fg, c->sgeom, c->cfg.precision, c->fsrc, c->fsrc2, c->ftgt, tree_st);
+  if (c->swe_cc_partial)
+    launch_swe_tree_cc(fg, c->fsrcf2, c->cc_chunks[kSweCcLen - 1], c->cc_nchunks[kSweCcLen - 1],
+                       c->cc_cstart[kSweCcLen - 1], c->swe_cc_partial, c->ftgt, tree_st);
+  else
+    launch_swe_interactions(fg, c->sgeom, c->cfg.precision, c->fsrc, c->fsrc2, c->ftgt, tree_st);
   launch_downward_fused(fg, c->ftgt, nullptr, tree_st);
   if (c->aux_stream) cudaEventRecord(c->ev_join, tree_st);
   constexpr int kSplits = 4;

@@ -87,4 +87,12 @@ void launch_bltc_swe_near(const TreeGeom& tg, const StepGeom& fg, int precision,
                           const float4* psrcf2, double* near, int splits, const double* gcentre, int gq,
                           cudaStream_t st);
 
+// Well-separated pairs of both fields on the treecode, mixed precision, over
+// the chunks of the interaction list (cstart: a target panel's first chunk;
+// partial: [chunks][6][q] float64) into tgt (3 x panels*q); proxy counts
+// with swe_tree_cc_supported only.
+bool swe_tree_cc_supported(int q);
+void launch_swe_tree_cc(const StepGeom& fg, const float4* srcf2, const int4* chunks, int nchunks, const int* cstart,
+                        double* partial, double* tgt, cudaStream_t st);
+
 }  // namespace sbslpm

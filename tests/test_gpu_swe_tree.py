@@ -34,9 +34,12 @@ def tree_ctx(sb, levels, n, leaf, theta, precision, deg=3, **kw):
 
 
 # interp degrees 2 and 4 give grid leaves of 9 and 25 points: an odd count,
-# which the mixed near field closes with a zero-strength source per grid leaf
+# which the mixed near field closes with a zero-strength source per grid leaf;
+# proxy degrees 5..10 (36..121 proxies) cover every shape of the mixed
+# well-separated kernel, the odd proxy counts closing on a zero-strength proxy
 @pytest.mark.parametrize("levels,leaf,n,theta,deg", [(5, 256, 8, 0.7, 3), (4, 64, 6, 0.5, 3), (4, 16, 5, 0.8, 3),
-                                                     (4, 256, 8, 0.7, 2), (4, 256, 6, 0.6, 4)])
+                                                     (4, 256, 8, 0.7, 2), (4, 256, 6, 0.6, 4), (4, 64, 7, 0.6, 3),
+                                                     (4, 64, 9, 0.8, 3), (4, 64, 10, 0.8, 3)])
 def test_swe_tree_velocity_matches_oracle(sb, port, levels, leaf, n, theta, deg):
     g = sb.build_grid(levels, deg, exact_cc=True)
     rng = np.random.default_rng(7)
