@@ -365,7 +365,6 @@ __global__ void k_downward_subtree_batch(const BatchMember* __restrict__ mem, in
 template <int Q>
 struct WarpShape {
   static constexpr int S = Q <= 16 ? 32 / Q : 1;          // source splits per warp
-  static constexpr int TPL = Q <= 32 ? 1 : (Q + 31) / 32;  // target nodes per lane
   static constexpr int STAGE = (S * Q > Q ? S * Q : Q);    // staged points per warp
   static constexpr int Q2 = (Q + 1) / 2;                    // source pairs per panel
   static constexpr int STAGE2 = (S > 1 ? S : 1) * 2 * Q2;   // float4 slots per warp, paired layout
@@ -473,7 +472,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_interact64(StepGeom g, 
       out[2 * s + o] = uz;
     }
   } else {
-    constexpr int TPL = W::TPL;
+    constexpr int TPL = Q <= 32 ? 1 : (Q + 31) / 32;  // target nodes per lane
     double tx[TPL], ty[TPL], tz[TPL], ax[TPL], ay[TPL], az[TPL];
 #pragma unroll
     for (int r = 0; r < TPL; r++) {
@@ -698,7 +697,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_interact32(StepGeom g, 
       out[2 * s + o] = kBiotSavartPacked * (tx * ay - ty * ax);
     }
   } else {
-    constexpr int TPL = W::TPL;
+    constexpr int TPL = Q <= 32 ? 1 : (Q + 31) / 32;  // target nodes per lane
     double tx[TPL], ty[TPL], tz[TPL], ax[TPL], ay[TPL], az[TPL];
     float dtx[TPL], dty[TPL], dtz[TPL];
 #pragma unroll

@@ -41,7 +41,6 @@ using dev::pair64;
 template <int Q, int S>
 struct CcShape {
   static constexpr int NT = (S * Q + 31) / 32 * 32;
-  static constexpr int Q2 = (Q + 1) / 2;
   static constexpr bool ok = NT <= 512 && 5 * S * Q >= 4 * NT;  // at most a fifth of the lanes idle
 };
 
@@ -60,7 +59,7 @@ __device__ __forceinline__ int chunk_entries_max(const int4* __restrict__ chunks
 template <int Q, int S, bool GUARD>
 __global__ void __launch_bounds__(CcShape<Q, S>::NT)
     k_cc32(StepGeom g, const int4* __restrict__ chunks, int nchunks, double* __restrict__ partial) {
-  constexpr int Q2 = CcShape<Q, S>::Q2;
+  constexpr int Q2 = (Q + 1) / 2;
   __shared__ float4 tile[S][2 * Q2];  // (x0,x1,y0,y1),(z0,z1,w0,w1); odd q: zero-strength partner
   const int h = threadIdx.x / Q, j = threadIdx.x - h * Q;
   const int c = blockIdx.x * S + h;
